@@ -1,0 +1,332 @@
+"""Benchmark of the ps3D time step on B200.
+
+Workload: the jet-instability case, 256 x 256 x 128, rigid lid, AB3,
+Laplacian viscosity (two opposing Gaussian jets in thermal-wind balance plus
+seeded 1e-3 noise in b; synthetic, seeded).  A step is one call of the
+reference's integrate (tendencies, friction, AB3, FFT pressure projection).
+
+Reported: grid-point-steps/s of the mixed FP32/FP64 path (value) and of the
+plain FP64 path, the relative L2 distance between the two after the run, the
+roofline of the dominant kernel from CUDA events on the engine's stream, an
+end-to-end figure through the public C ABI with host buffers, and the CPU
+oracle restatement timed on this host's cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): every rank runs an independent replica on its own GPU
+(a single grid does not shard here); value = all ranks' grid-point-steps over
+the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 256, 256, 128
+WORKLOAD = "jets 256x256x128 rigid lid AB3 Laplacian friction"
+
+# algorithmic HBM bytes per grid point per launch (SURVEY-style accounting):
+# K1 reads u,v,w,b + 2 AB history slots x 4 fields, writes 4 tendencies + 4 state
+BYTES_PER_POINT = {
+    "fp64": {"step": 160, "fft_fwd": 32, "vsolve": 16, "fft_inv": 16, "correct": 56, "other": 16},
+    "mixed": {"step": 112, "fft_fwd": 28, "vsolve": 8, "fft_inv": 12, "correct": 56, "other": 24},
+}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def jets_state(p):
+    from ps3d_b200 import configs as cf
+    f = cf.jets_fields(p)
+    return cf.add_noise(p, f, "b", rel=1e-3, seed=1)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x, pg, dev):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, dev):
+    import torch
+    if pg is not None:
+        pg.barrier(device_ids=[dev])
+    torch.cuda.synchronize(dev)
+
+
+def time_path(precision, steps, warmup, dev, pg):
+    """Warm up, then time exactly `steps` steps with CUDA events on the engine's stream."""
+    import torch
+    from ps3d_b200 import configs as cf
+    from ps3d_b200.model import Model
+    p = cf.jets_params(NX, NY, NZ, precision=precision)
+    f = jets_state(p)
+    m = Model(p, device=dev)
+    m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+    m.run(warmup)
+    stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    m.profile(True)
+    clocks = ClockSampler(dev)
+    barrier(pg, dev)
+    clocks.start()
+    ev0.record(stream)
+    m.enqueue(steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    kern = m.profile_read()
+    m.profile(False)
+    barrier(pg, dev)
+    ms_max = max_over_ranks(ms, pg, dev)
+    state = m.download(tendencies=False)
+    return m, p, ms, ms_max, kern, clk, state
+
+
+def e2e_run(precision, steps, dev):
+    """main.f90's loop through the public C ABI with host buffers: upload the
+    state, `steps` x (ps3d_step + host rotation), diagnose every 10 steps,
+    download the state.  All host<->device copies are inside the timed region."""
+    import torch
+    from ps3d_b200 import configs as cf
+    from ps3d_b200.model import Model
+    p = cf.jets_params(NX, NY, NZ, precision=precision)
+    f = jets_state(p)
+    m = Model(p, device=dev)
+    m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+    m.run(3)                      # warm the kernels
+    names = ("u", "v", "w", "b", "p")
+    host = {n: np.ascontiguousarray(f.get(n, np.zeros_like(f["u"]))) for n in names}
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    m.upload(**host, itt=0, tau=3, taum1=2, taum2=1)
+    itt, tau, t1, t2 = 0, 3, 2, 1
+    ndiag = 0
+    for n in range(steps):
+        m.integrate(itt, tau, t1, t2)
+        if n % 10 == 0:
+            m.diagnose()
+            ndiag += 1
+        tau, t1, t2 = tau % 3 + 1, t1 % 3 + 1, t2 % 3 + 1
+        itt += 1
+    out = m.download(tendencies=False)
+    t = time.perf_counter() - t0
+    m.close()
+    field_bytes = host["u"].nbytes
+    h2d = 5 * field_bytes
+    d2h = 5 * field_bytes + ndiag * 32
+    return t, h2d / steps, d2h / steps, out
+
+
+def cpu_baseline_run(steps, warmup_steps=1, budget_s=60.0):
+    """The CPU oracle restatement on all host cores, bounded to ~budget_s."""
+    from oracle.binding import Oracle, set_threads
+    from ps3d_b200 import configs as cf
+    cores = os.cpu_count() or 1
+    set_threads(cores)
+    p = cf.jets_params(NX, NY, NZ)
+    f = jets_state(p)
+    o = Oracle(p)
+    for n in ("u", "v", "w", "b"):
+        o.field(n)[...] = f[n]
+    t0 = time.perf_counter()
+    o.integrate(warmup_steps)
+    t_one = (time.perf_counter() - t0) / max(warmup_steps, 1)
+    n = int(max(1, min(steps, budget_s / max(t_one, 1e-6))))
+    t0 = time.perf_counter()
+    o.integrate(n)
+    t = time.perf_counter() - t0
+    return NX * NY * NZ * n / t, cores, n
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    unit = "grid-point-steps/s"
+    metric = "grid-point-steps/s of the ps3D time step, 256x256x128 jets, mixed FP32/FP64 path (FP64 path beside)"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = max(1, args.steps)
+        val, cores, n = cpu_baseline_run(steps, warmup_steps=min(max(args.warmup, 1), 2), budget_s=150.0)
+        sample = f"{n} full steps of {NX}x{NY}x{NZ} (after warm-up) on {cores} threads"
+        line = {"impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus,
+                "steps": n, "warmup": args.warmup, "ms_per_step": NX * NY * NZ / val * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded jets + noise)",
+                "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "reference Fortran/MPI/P3DFFT path is not buildable here; oracle C++ restatement timed"}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    from ps3d_b200 import build as b
+    from ps3d_b200 import abi
+    from ps3d_b200 import configs as cf
+    b.build()
+    torch.cuda.set_device(local)
+    dev = local
+    npts = NX * NY * NZ
+
+    m64, p64, ms64, ms64_max, k64, clk64, s64 = time_path(abi.PS3D_FP64, args.steps, args.warmup, dev, pg)
+    m64.close()
+    mmx, pmx, msmx, msmx_max, kmx, clkmx, smx = time_path(abi.PS3D_MIXED, args.steps, args.warmup, dev, pg)
+    mmx.close()
+    v64 = world * npts * args.steps / (ms64_max * 1e-3)
+    vmx = world * npts * args.steps / (msmx_max * 1e-3)
+    rel = {n: cf.rel_l2(cf.interior(smx[n]), cf.interior(s64[n])) for n in ("u", "v", "w", "b", "p")}
+    u, v, w = smx["u"], smx["v"], smx["w"]
+    div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / pmx.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / pmx.dy
+           + (w[2:-2, 2:-2, 2:-2] - w[1:-3, 2:-2, 2:-2]) / pmx.dz)
+
+    peak, peak_kind = peaks()
+
+    def roof(kern, prec):
+        out = {}
+        for k, (ms, n) in kern.items():
+            if n == 0:
+                continue
+            per = ms / n
+            bpp = BYTES_PER_POINT[prec].get(k, 0)
+            out[k] = {"launches": n, "ms_total": ms, "ms_per_launch": per,
+                      "algorithmic_gb_per_launch": bpp * npts / 1e9,
+                      "achieved_gbs": bpp * npts / (per * 1e-3) / 1e9 if bpp else None}
+        return out
+
+    r64, rmx = roof(k64, "fp64"), roof(kmx, "mixed")
+    dom = max(rmx.items(), key=lambda kv: kv[1]["ms_total"])
+    dom_name, dom_v = dom
+    launches = sum(n for _, n in kmx.values())
+
+    line = {"metric": metric, "value": vmx, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": msmx_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (FP64 state/AB/tridiagonal)",
+            "data": "synthetic (seeded jets + 1e-3 b noise)",
+            "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state ~1.4 GB)"},
+            "fp64": {"value": v64, "ms_per_step": ms64_max / args.steps, "kernels": r64},
+            "mixed_over_fp64": vmx / v64,
+            "rel_l2_mixed_vs_fp64": rel, "max_div_mixed": float(np.abs(div).max()),
+            "kernels": rmx,
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_v["achieved_gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": (dom_v["achieved_gbs"] or 0) / peak, "traffic": None,
+                         "peak_kind": peak_kind},
+            "gpu_launches": int(launches),
+            "clocks": clkmx, "clocks_fp64": clk64}
+    if not args.no_e2e:
+        t, h2d, d2h, _ = e2e_run(abi.PS3D_MIXED, args.steps, dev)
+        t = max_over_ranks(t, pg, dev)
+        line["e2e"] = {"value": world * npts * args.steps / t, "unit": unit, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h,
+                       "path": "public C ABI: upload, ps3d_step per step, diagnose every 10 steps, download"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        val, cores, n = cpu_baseline_run(3, warmup_steps=1, budget_s=30.0)
+        line["cpu_baseline"] = {"value": val, "unit": unit, "cores": cores, "kind": "port",
+                                "sample": f"{n} full steps of {NX}x{NY}x{NZ} after 1 warm-up step, CPU oracle"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,222 @@
+/*
+ * ps3d_gpu.h — C ABI of the B200 (sm_100a) ps3D time-step engine.
+ *
+ * The reference model (ceden/ps3D) keeps its state in Fortran module globals
+ * (for_src/main_module.f90:3-108) and its hot path is a set of argument-less
+ * subroutines: integrate (for_src/integrate.f90:2-115), pressure_solver
+ * (for_src/pressure_solver.f90:2-120), the normal-mode projections
+ * (for_src/diag_opt_balance.f90:263-335, for_src/diag_balance.f90:109-132),
+ * diag_opt_balance (for_src/diag_opt_balance.f90:55-179) and diagnose
+ * (for_src/diagnose.F90:2-61).  This header replaces those with entry points
+ * on an opaque context that owns the device-resident state.  Every entry point
+ * takes plain pointers and sizes, returns an int status (0 = success, negative
+ * = error) and never aborts or traps; a Fortran host binds them through
+ * ISO_C_BINDING (interfaces are listed in INTEGRATION.md).
+ *
+ * Host arrays use the reference's layout: real(8) fields are column-major,
+ * x fastest, with two halo points on every side, i.e. Fortran bounds
+ * (1-2:nx+2, 1-2:ny+2, 1-2:nz+2) -> (nx+4)*(ny+4)*(nz+4) doubles.  Tendency
+ * arrays carry the trailing time-level dimension of 3
+ * (for_src/main_module.f90:124-127): 3*(nx+4)*(ny+4)*(nz+4) doubles.
+ * Time-level indices tau/taum1/taum2 are 1-based as in Fortran.
+ */
+#ifndef PS3D_GPU_H
+#define PS3D_GPU_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define PS3D_API __attribute__((visibility("default")))
+#else
+#define PS3D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PS3D_OK                0
+#define PS3D_ERR_CUDA         -1  /* a CUDA runtime call failed                     */
+#define PS3D_ERR_NONFINITE    -2  /* NaN/Inf found in the state (diagnose.F90:42-45) */
+#define PS3D_ERR_TIMEOUT      -3  /* a bounded device or host wait ran out          */
+#define PS3D_ERR_OOM          -4  /* device allocation or admission budget refused  */
+#define PS3D_ERR_BADPARAM     -5  /* invalid argument, size or configuration        */
+#define PS3D_ERR_UNSUPPORTED  -6  /* valid in the reference, not built here         */
+#define PS3D_ERR_CANCELLED    -7  /* a serving request was cancelled                */
+
+/* ---- parameters (for_src/main_module.f90:16-57) -------------------------- */
+typedef struct ps3d_params {
+    int nx, ny, nz;                       /* grid points                       */
+    double Lx, Ly, Lz;                    /* domain extent (m)                 */
+    double dx, dy, dz;                    /* cell size (m)                     */
+    double dt;                            /* time step (s)                     */
+    double f0, N0;                        /* Coriolis and stability freq.      */
+    double Ro, dsqr;                      /* Rossby number, aspect ratio^2     */
+    double eps_ab;                        /* AB2 weighting (main_module.f90:56)*/
+    double Ah, Av, Kh, Kv;                /* harmonic viscosity / diffusivity  */
+    double Ahbi, Avbi, Khbi, Kvbi;        /* biharmonic coefficients           */
+    int enable_nonlinear;                 /* main_module.f90:16                */
+    int enable_vertical_boundaries;       /* rigid lid (1) or periodic z (0)   */
+    int enable_AB_3_order;                /* AB3 (1) or AB2 (0)                */
+    int precision;                        /* PS3D_FP64 or PS3D_MIXED           */
+} ps3d_params;
+
+#define PS3D_FP64  0   /* every kernel in FP64                                  */
+#define PS3D_MIXED 1   /* FP32 stencils/FFTs, FP64 state, tridiagonal, AB and
+                          eigen-projection, one FP64-residual Poisson refinement */
+
+/* ---- optimal balance knobs (for_src/main_module.f90:24-30) ------------- */
+typedef struct ps3d_optbal {
+    double period;        /* opt_balance_period: ramp length in s            */
+    double average;       /* opt_balance_average (time-averaging variant)    */
+    int max_itts;         /* opt_balance_max_Itts                            */
+    int average_times;    /* opt_balance_average_times                       */
+    double tol;           /* opt_balance_tol                                 */
+    int enable_time_ave;  /* enable_diag_opt_time_ave                        */
+    int adopt;            /* 1: copy the balanced fields into u,v,w,b at the
+                             end, as for_config/test_opt_balance.f90:240-241 */
+} ps3d_optbal;
+
+/* ---- user forcing (set_forcing hook, for_src/integrate.f90:82) ---------- */
+/* Device view handed to a host forcing callback: interior-only device arrays
+ * (x fastest, nx*ny*nz doubles), already friction-updated, and the tendency
+ * slot of the current time level.  The callback may launch its own kernels on
+ * `stream`; it runs between friction and the Adams-Bashforth update.        */
+typedef struct ps3d_device_view {
+    int nx, ny, nz;
+    double *u, *v, *w, *b;                /* state being stepped             */
+    double *du, *dv, *dw, *db;            /* tendencies of time level tau    */
+    double dt, Ro;
+    int itt;
+    void* stream;                         /* cudaStream_t                    */
+} ps3d_device_view;
+
+typedef int (*ps3d_forcing_fn)(void* user, const ps3d_device_view* view);
+
+#define PS3D_FORCE_NONE        0
+#define PS3D_FORCE_WAVEMAKER   1  /* u += dt*(cos(omega t) u_r + sin(omega t) u_i),
+                                     t = dt*itt (for_src/config.f90:224-237)     */
+#define PS3D_FORCE_BACKGROUND  2  /* advection by/of a background flow U(x,y,z)
+                                     and buoyancy B(x,y,z)
+                                     (for_config/lee_wave1.f90:245-312)          */
+#define PS3D_FORCE_CALLBACK    4  /* host callback with device pointers          */
+
+typedef struct ps3d_forcing {
+    int kind;                             /* bitwise OR of PS3D_FORCE_*      */
+    double omega;                         /* wavemaker frequency             */
+    /* wavemaker fields, halo layout, NULL = zero field                       */
+    const double *u_r, *v_r, *w_r, *b_r, *u_i, *v_i, *w_i, *b_i;
+    /* background flow fields, halo layout, NULL = zero field                 */
+    const double *u_back, *b_back;
+    ps3d_forcing_fn fn;                   /* PS3D_FORCE_CALLBACK             */
+    void* user;
+} ps3d_forcing;
+
+typedef struct ps3d_ctx ps3d_ctx;
+
+/* Replaces allocate_main_module (main_module.f90:112-144) and
+ * wavenumber_initialisation (my_fft.f90:87-156) for one rank on one GPU:
+ * allocates the device state, wavenumber and vertical-mode tables.
+ * nx, ny must be even (main.f90:45-55) and nz even in periodic mode; every
+ * FFT length (nx/2, ny and, periodic, nz) must factor into 2, 3 and 5.     */
+PS3D_API int ps3d_create(const ps3d_params* prm, int device, ps3d_ctx** out);
+PS3D_API int ps3d_destroy(ps3d_ctx* ctx);
+
+/* Copy the model state in the reference's halo layout to/from the device
+ * (u,v,w,b,p: main_module.f90:64-68; du..db with their 3 time levels) and set
+ * or read the time-level indices (main_module.f90:55,58).  Any pointer may be
+ * NULL on download to skip that field; on upload a NULL tendency pointer
+ * zero-fills those time levels.                                             */
+PS3D_API int ps3d_upload_state(ps3d_ctx* ctx,
+                      const double* u, const double* v, const double* w,
+                      const double* b, const double* p,
+                      const double* du, const double* dv, const double* dw,
+                      const double* db,
+                      int itt, int tau, int taum1, int taum2);
+PS3D_API int ps3d_download_state(ps3d_ctx* ctx,
+                        double* u, double* v, double* w, double* b, double* p,
+                        double* du, double* dv, double* dw, double* db,
+                        int* itt, int* tau, int* taum1, int* taum2);
+
+/* integrate (integrate.f90:2-115) once, with the caller's time-level indices
+ * and step counter; it does not rotate them (the caller does, as main.f90:156-160). */
+PS3D_API int ps3d_step(ps3d_ctx* ctx, int itt, int tau, int taum1, int taum2);
+
+/* nsteps iterations of the main loop body (main.f90:139-162 without the
+ * diagnostics): integrate, rotate tau/taum1/taum2, time += dt, itt += 1.
+ * Device resident; returns after the work is queued and completed.          */
+PS3D_API int ps3d_integrate(ps3d_ctx* ctx, int nsteps);
+
+/* Change the per-step parameters the balance drivers ramp
+ * (diag_opt_balance.f90:191-198,221-224).                                    */
+PS3D_API int ps3d_set_step_params(ps3d_ctx* ctx, double dt, double Ro,
+                         double Ahbi, double Avbi, double Khbi, double Kvbi);
+
+/* pressure_solver (pressure_solver.f90:2-120) on the current device state.  */
+PS3D_API int ps3d_pressure_solve(ps3d_ctx* ctx);
+
+/* Normal-mode projections on the device state:
+ *  PS3D_PROJ_NORMAL_MODE   normal_mode_projection   (diag_opt_balance.f90:288-310)
+ *  PS3D_PROJ_BASE_POINT    geostrophic_base_point   (diag_opt_balance.f90:263-285):
+ *                          stores g0_base and returns the base point in u_base
+ *  PS3D_PROJ_EXCHANGE      exchange_geostrophic_base_point (diag_opt_balance.f90:313-335)
+ *  PS3D_PROJ_ZERO_ORDER    diag_balance_zero_order  (diag_balance.f90:109-132):
+ *                          writes u0..b0, readable with ps3d_get_fields       */
+#define PS3D_PROJ_NORMAL_MODE 0
+#define PS3D_PROJ_BASE_POINT  1
+#define PS3D_PROJ_EXCHANGE    2
+#define PS3D_PROJ_ZERO_ORDER  3
+PS3D_API int ps3d_project_geostrophic(ps3d_ctx* ctx, int mode);
+
+/* diag_opt_balance (diag_opt_balance.f90:55-179) on the device state.  The
+ * model state is restored on return (as :172-176); the balanced fields are
+ * kept (u_bal) and copied into the state when opt->adopt is set.            */
+PS3D_API int ps3d_opt_balance(ps3d_ctx* ctx, const ps3d_optbal* opt,
+                     double* final_norm, int* iters);
+
+/* Auxiliary field sets in halo layout (u,v,w,b; any may be NULL).          */
+#define PS3D_FIELDS_STATE    0   /* u, v, w, b                         */
+#define PS3D_FIELDS_BALANCED 1   /* u_bal..b_bal  (diag_opt_balance)   */
+#define PS3D_FIELDS_BASE     2   /* u_base..b_base                     */
+#define PS3D_FIELDS_ZERO     3   /* u0..b0 (diag_balance_zero_order)   */
+PS3D_API int ps3d_get_fields(ps3d_ctx* ctx, int which,
+                    double* u, double* v, double* w, double* b);
+
+/* diagnose (diagnose.F90:2-61) reductions: mean KE and PE, max horizontal and
+ * vertical speed.  Returns PS3D_ERR_NONFINITE when any of u,v,w,b,p holds a
+ * NaN or Inf (the reference aborts there, diagnose.F90:42-45).              */
+PS3D_API int ps3d_diagnose(ps3d_ctx* ctx, double* ke, double* pe,
+                  double* umax, double* wmax);
+
+/* Install the set_forcing hook (integrate.f90:82).  Field arrays are copied
+ * to the device during the call.                                            */
+PS3D_API int ps3d_set_forcing(ps3d_ctx* ctx, const ps3d_forcing* f);
+
+PS3D_API const char* ps3d_strerror(int status);
+
+/* ---- engine extensions (no counterpart in the reference) ----------------
+ * The CUDA stream the context queues its kernels on (a cudaStream_t).      */
+PS3D_API int ps3d_get_stream(ps3d_ctx* ctx, void** stream);
+/* ps3d_integrate without the final synchronisation: queues nsteps on the
+ * context's stream and returns; errors of queued work surface at the next
+ * synchronising call.                                                      */
+PS3D_API int ps3d_enqueue(ps3d_ctx* ctx, int nsteps);
+/* Per-kernel CUDA-event timing.  ps3d_profile(ctx, 1) clears and starts
+ * recording an event pair around every launch; ps3d_profile_read waits for
+ * the stream and returns, per kernel class (PS3D_K_*), the summed device
+ * milliseconds and the number of launches.                                 */
+#define PS3D_K_STEP     0   /* fused tendency/friction/AB kernel            */
+#define PS3D_K_FFT_FWD  1   /* divergence + forward plane FFT               */
+#define PS3D_K_VSOLVE   2   /* vertical Thomas / periodic z solve           */
+#define PS3D_K_FFT_INV  3   /* inverse plane FFT                            */
+#define PS3D_K_CORRECT  4   /* pressure-gradient correction                 */
+#define PS3D_K_OTHER    5   /* friction stages, forcing, projections, ...   */
+#define PS3D_K_COUNT    6
+PS3D_API int ps3d_profile(ps3d_ctx* ctx, int enable);
+PS3D_API int ps3d_profile_read(ps3d_ctx* ctx, double* ms, long long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PS3D_GPU_H */

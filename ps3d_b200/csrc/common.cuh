@@ -1,0 +1,67 @@
+// common.cuh — shared device definitions of the ps3D B200 engine.
+//
+// Device layout (differs from the host's halo layout on purpose): every real
+// field is stored interior-only, x fastest, nx*ny*nz elements, and stencils
+// wrap their indices periodically.  On one rank the reference's halo
+// exchange (for_src/parallel_mpi.f90:70-211) makes every halo point an exact
+// periodic copy of an interior point, so the halo carries no extra state;
+// the one place where halos differ from the wrapped interior (friction
+// stages reading pre-friction halos, for_src/integrate.f90:59-78) is
+// reproduced explicitly by the friction kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#define PS3D_HD __host__ __device__ __forceinline__
+
+namespace ps3d {
+
+// ---------------------------------------------------------------------------
+// complex helpers (interleaved re/im, double2/float2 compatible with the
+// reference's complex(8) storage)
+// ---------------------------------------------------------------------------
+template <typename R> struct cpx_t;
+template <> struct cpx_t<double> { using type = double2; };
+template <> struct cpx_t<float> { using type = float2; };
+template <typename R> using cpx = typename cpx_t<R>::type;
+
+template <typename R> PS3D_HD cpx<R> mk(R a, R b) { cpx<R> c; c.x = a; c.y = b; return c; }
+template <typename T> PS3D_HD T cadd(T a, T b) { a.x += b.x; a.y += b.y; return a; }
+template <typename T> PS3D_HD T csub(T a, T b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename T> PS3D_HD T cmul(T a, T b) {
+    T c; c.x = a.x * b.x - a.y * b.y; c.y = a.x * b.y + a.y * b.x; return c;
+}
+template <typename T> PS3D_HD T cconj(T a) { a.y = -a.y; return a; }
+template <typename T, typename S> PS3D_HD T cscale(T a, S s) { a.x *= s; a.y *= s; return a; }
+// multiply by s*i  (s = +-1)
+template <typename T> PS3D_HD T cmul_si(T a, int s) {
+    T c; c.x = -s * a.y; c.y = s * a.x; return c;
+}
+
+// ---------------------------------------------------------------------------
+// FFT plan for one transform length, device side
+// ---------------------------------------------------------------------------
+constexpr int kMaxStages = 16;
+
+struct FFTPlan {
+    int n;                    // transform length
+    int nst;                  // number of stages
+    int r[kMaxStages];        // radices in DIT stage order (product = n)
+    const double2* tw;        // exp(-2 pi i t / n), t = 0..n-1
+    const float2* twf;        // the same, rounded to FP32
+    const int* pos;           // digit-reversal: natural index t -> position
+    const int* ipos;          // inverse of pos
+};
+
+// ---------------------------------------------------------------------------
+// periodic index helpers
+// ---------------------------------------------------------------------------
+PS3D_HD int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// status flags written by kernels (bit mask, OR-ed)
+enum : unsigned {
+    kFlagNonFinite = 1u,
+    kFlagBounds = 2u,
+};
+
+}  // namespace ps3d

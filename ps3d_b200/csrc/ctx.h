@@ -1,0 +1,153 @@
+// ctx.h — the device context of one grid (host-side bookkeeping).
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "engine.h"
+
+// Return PS3D_ERR_CUDA (or PS3D_ERR_OOM) from an int-returning function when a
+// CUDA call fails.
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t ck_e_ = (call);                                                     \
+        if (ck_e_ != cudaSuccess) {                                                     \
+            ps3d::note_cuda_error(ck_e_, #call, __FILE__, __LINE__);                    \
+            return ck_e_ == cudaErrorMemoryAllocation ? PS3D_ERR_OOM : PS3D_ERR_CUDA;   \
+        }                                                                               \
+    } while (0)
+
+namespace ps3d {
+
+void note_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+// owning device (or pinned host) buffer
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool host = false;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    cudaError_t alloc(size_t n) {
+        release();
+        cudaError_t e = cudaMalloc(&p, n ? n : 1);
+        if (e == cudaSuccess) bytes = n; else p = nullptr;
+        return e;
+    }
+    cudaError_t alloc_host(size_t n) {
+        release();
+        cudaError_t e = cudaMallocHost(&p, n ? n : 1);
+        if (e == cudaSuccess) { bytes = n; host = true; } else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) { if (host) cudaFreeHost(p); else cudaFree(p); }
+        p = nullptr; bytes = 0; host = false;
+    }
+};
+
+struct DevPlan {
+    FFTPlan plan{};
+    int n = 0;
+    DevBuf dtw, dtwf, dpos, dipos;
+    cudaError_t build(int len);
+};
+
+bool fft_length_ok(int n);
+
+enum { kSetSave = 10, kSetAve = 11, kSetSave2 = 12 };
+
+struct Ctx {
+    ps3d_params P{};
+    int device = 0;
+    int nx = 0, ny = 0, nz = 0, nxh = 0;
+    long N = 0, M2 = 0, M = 0;
+    bool rigid = true, mixed = false;
+    cudaStream_t stream = nullptr;
+    size_t tsize = 8;
+    // state
+    DevBuf state[4][3];
+    int cur[4] = {0, 0, 0, 0};
+    DevBuf p, p2;
+    DevBuf tend[4];           // 3 time levels each
+    DevBuf FS;                // spectral work array of the Poisson solve
+    // projections
+    DevBuf spec4[4], g0base, qtmp;
+    DevBuf bal[4], base[4], zero[4], save[4], ave[4], save2[4];
+    DevBuf saved_p, saved_tend[4];
+    // tables
+    DevPlan plx, ply, plz;
+    DevBuf twx;
+    DevBuf t_kx, t_ky, t_kz, t_hkx, t_hky, t_hkz, t_ex, t_ey, t_ez, t_px, t_py, t_pz, t_sz, t_cz, t_hkz_ds;
+    DevBuf m_phi, m_psi, m_psib;
+    PlaneArgs pa64{}, pa32{};
+    // forcing
+    int fkind = 0;
+    double omega = 0.0;
+    DevBuf wr[4], wi[4], ub, bb;
+    ps3d_forcing_fn fn = nullptr;
+    void* user = nullptr;
+    // time levels (main_module.f90:55-59)
+    int itt = 0, tau = 3, taum1 = 2, taum2 = 1;
+    double time = 0.0;
+    // per-kernel event timing (ps3d_profile)
+    bool prof = false;
+    struct ProfRec { int kid; cudaEvent_t e0, e1; };
+    std::vector<ProfRec> prof_recs;
+    std::vector<cudaEvent_t> prof_pool;
+    size_t prof_next = 0;
+    long long launches = 0;
+    cudaEvent_t prof_event();
+    void prof_begin(int kid, cudaEvent_t* e0);
+    void prof_end(int kid, cudaEvent_t e0);
+    int prof_read(double* ms, long long* count);
+    // reductions / staging
+    int nred = 0;
+    DevBuf red_partials, red_out, staging;
+
+    ~Ctx() {
+        if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+        for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
+    }
+
+    double* field(int f) { return (double*)state[f][cur[f]].p; }
+    void rotate() {
+        tau = tau % 3 + 1;
+        taum1 = taum1 % 3 + 1;
+        taum2 = taum2 % 3 + 1;
+    }
+    int sync() {
+        CK(cudaStreamSynchronize(stream));
+        CK(cudaGetLastError());
+        return PS3D_OK;
+    }
+
+    int init(const ps3d_params& prm, int dev);
+    int step(int itt, int tau, int taum1, int taum2);
+    int poisson_once(double* out, double beta);
+    int pressure_solve();
+    int forward_transform(const double* const* in);
+    int backward_transform(double* const* out);
+    int project(int mode);
+    int diagnose(double* ke, double* pe, double* umax, double* wmax);
+    int opt_time_ave(int set, int n_end_ave);
+    int opt_balance(const ps3d_optbal& O, double* final_norm, int* iters);
+    int set_forcing(const ps3d_forcing* f);
+
+    cudaError_t ensure_spectral4();
+    cudaError_t ensure_fieldset(int which);
+    cudaError_t ensure_saved_tail();
+    cudaError_t ensure_staging();
+    DevBuf* fieldset(int which);
+    cudaError_t copy_state_to(int set);
+    cudaError_t copy_set_to_state(int set);
+
+    void gather(const double* h, double* dst) const;
+    void scatter(const double* src, double* h, int kind) const;
+    int upload_field(double* dev, const double* h);
+    int download_field(const double* dev, double* h, int kind);
+    int upload_tend(int f, const double* h);
+    int download_tend(int f, double* h);
+};
+
+}  // namespace ps3d

@@ -1,0 +1,1057 @@
+// engine.cu — host side of the ps3D B200 engine and the C ABI of
+// include/ps3d_gpu.h.
+//
+// One context = one grid on one GPU (the reference's single-rank meaning).
+// All model state lives in HBM in the interior-only layout (common.cuh); the
+// host crosses the boundary only in upload/download, which convert to and from
+// the reference's halo layout.  The drivers here restate the control flow of
+//   integrate            for_src/integrate.f90:2-115
+//   pressure_solver      for_src/pressure_solver.f90:2-120
+//   forward/backward_transform  for_src/diag_balance.f90:421-462
+//   diag_opt_balance     for_src/diag_opt_balance.f90:55-378
+//   diagnose             for_src/diagnose.F90:2-61
+// over device kernels.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+#include "engine.h"
+#include "ctx.h"
+
+namespace ps3d {
+
+// Launch a kernel, count it, and bracket it with CUDA events when profiling.
+#define LAUNCH(kid, call)                                  \
+    do {                                                   \
+        cudaEvent_t lp_e0_ = nullptr;                      \
+        if (prof) prof_begin(kid, &lp_e0_);                \
+        CK(call);                                          \
+        ++launches;                                        \
+        if (prof) prof_end(kid, lp_e0_);                   \
+    } while (0)
+
+cudaEvent_t Ctx::prof_event() {
+    if (prof_next < prof_pool.size()) return prof_pool[prof_next++];
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    prof_pool.push_back(e);
+    ++prof_next;
+    return e;
+}
+void Ctx::prof_begin(int, cudaEvent_t* e0) {
+    *e0 = prof_event();
+    if (*e0) cudaEventRecord(*e0, stream);
+}
+void Ctx::prof_end(int kid, cudaEvent_t e0) {
+    cudaEvent_t e1 = prof_event();
+    if (!e0 || !e1) return;
+    cudaEventRecord(e1, stream);
+    prof_recs.push_back({kid, e0, e1});
+}
+int Ctx::prof_read(double* ms, long long* count) {
+    CK(cudaStreamSynchronize(stream));
+    for (int k = 0; k < PS3D_K_COUNT; ++k) { if (ms) ms[k] = 0.0; if (count) count[k] = 0; }
+    for (const ProfRec& r : prof_recs) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, r.e0, r.e1));
+        if (ms) ms[r.kid] += t;
+        if (count) count[r.kid] += 1;
+    }
+    prof_recs.clear();
+    prof_next = 0;
+    return PS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FFT plans (host construction)
+// ---------------------------------------------------------------------------
+static std::vector<int> radices_of(int n) {
+    std::vector<int> r;
+    int m = n;
+    while (m % 4 == 0) { r.push_back(4); m /= 4; }
+    while (m % 2 == 0) { r.push_back(2); m /= 2; }
+    while (m % 3 == 0) { r.push_back(3); m /= 3; }
+    while (m % 5 == 0) { r.push_back(5); m /= 5; }
+    if (m != 1) r.clear();
+    return r;
+}
+bool fft_length_ok(int n) { return n == 1 || !radices_of(n).empty(); }
+
+// exp(-2 pi i t / n) with octant reduction in long double (exact at multiples of pi/4)
+static double2 twiddle_fwd(long t, long n) {
+    t %= n; if (t < 0) t += n;
+    double c, s;
+    if ((8 * t) % n == 0) {
+        static const double r2 = 0.70710678118654752440084436210484904;
+        const double cc[8] = {1, r2, 0, -r2, -1, -r2, 0, r2};
+        const double ss[8] = {0, r2, 1, r2, 0, -r2, -1, -r2};
+        const long o = (8 * t) / n;
+        c = cc[o]; s = ss[o];
+    } else {
+        const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
+        c = (double)cosl(a); s = (double)sinl(a);
+    }
+    return make_double2(c, -s);
+}
+
+static int pos_of(int t, const std::vector<int>& r, int m, int n) {
+    if (m == 0) return 0;
+    const int R = r[m - 1];
+    return (t % R) * (n / R) + pos_of(t / R, r, m - 1, n / R);
+}
+
+cudaError_t DevPlan::build(int len) {
+    n = len;
+    std::vector<int> r = n == 1 ? std::vector<int>{} : radices_of(n);
+    if (n != 1 && r.empty()) return cudaErrorInvalidValue;
+    if ((int)r.size() > kMaxStages) return cudaErrorInvalidValue;
+    std::vector<double2> tw(n);
+    std::vector<float2> twf(n);
+    std::vector<int> pos(n), ipos(n);
+    for (int t = 0; t < n; ++t) {
+        tw[t] = twiddle_fwd(t, n);
+        twf[t] = make_float2((float)tw[t].x, (float)tw[t].y);
+        pos[t] = pos_of(t, r, (int)r.size(), n);
+    }
+    for (int t = 0; t < n; ++t) ipos[pos[t]] = t;
+    cudaError_t e;
+    if ((e = dtw.alloc(n * sizeof(double2)))) return e;
+    if ((e = dtwf.alloc(n * sizeof(float2)))) return e;
+    if ((e = dpos.alloc(n * sizeof(int)))) return e;
+    if ((e = dipos.alloc(n * sizeof(int)))) return e;
+    if ((e = cudaMemcpy(dtw.p, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(dtwf.p, twf.data(), n * sizeof(float2), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(dpos.p, pos.data(), n * sizeof(int), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(dipos.p, ipos.data(), n * sizeof(int), cudaMemcpyHostToDevice))) return e;
+    plan.n = n;
+    plan.nst = (int)r.size();
+    for (int s = 0; s < kMaxStages; ++s) plan.r[s] = s < (int)r.size() ? r[s] : 1;
+    plan.tw = (const double2*)dtw.p;
+    plan.twf = (const float2*)dtwf.p;
+    plan.pos = (const int*)dpos.p;
+    plan.ipos = (const int*)dipos.p;
+    return cudaSuccess;
+}
+
+// Choose the cluster shape of the plane kernels for one element size.
+static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
+    const int nxh = nx / 2 + 1, n2 = nx / 2;
+    for (int pass = 0; pass < 2; ++pass) {
+        const size_t limit = pass == 0 ? 110 * 1024 : 225 * 1024;
+        for (int C : {1, 2, 4, 8, 16}) {
+            if (ny % C) continue;
+            const int R = ny / C;
+            const int cpc = (nxh + C - 1) / C;
+            if ((C - 1) * cpc >= nxh) continue;
+            const int rc = std::min(8, R);
+            const int ldr = rc | 1, ldc = cpc | 1;
+            const size_t sm = ((size_t)ny * ldc + (size_t)n2 * ldr) * es;
+            if (sm > limit) continue;
+            a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rc; a.ldr = ldr; a.ldc = ldc;
+            return true;
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// context construction
+// ---------------------------------------------------------------------------
+static double hat_ksqr(double k, double d) { return 2.0 * (1.0 - std::cos(k * d)) / (d * d); }
+static double hat_epm(double k, double d) { return 0.5 * (1 + std::cos(k * d)); }
+
+int Ctx::init(const ps3d_params& prm, int dev) {
+    P = prm;
+    device = dev;
+    nx = P.nx; ny = P.ny; nz = P.nz; nxh = nx / 2 + 1;
+    N = (long)nx * ny * nz;
+    M2 = (long)nxh * ny;
+    M = M2 * nz;
+    rigid = P.enable_vertical_boundaries != 0;
+    mixed = P.precision == PS3D_MIXED;
+    if (nx < 2 || ny < 2 || nz < 2 || nx % 2 || ny % 2 || (!rigid && nz % 2)) return PS3D_ERR_BADPARAM;
+    if (!fft_length_ok(nx / 2) || !fft_length_ok(ny) || (!rigid && !fft_length_ok(nz))) return PS3D_ERR_BADPARAM;
+    if (P.precision != PS3D_FP64 && P.precision != PS3D_MIXED) return PS3D_ERR_BADPARAM;
+    if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0)) return PS3D_ERR_BADPARAM;
+    if (cudaSetDevice(dev) != cudaSuccess) return PS3D_ERR_CUDA;
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(plane_setup(false));
+    CK(plane_setup(true));
+    // state: 3 buffers per field (fused path ping-pongs two, the generic path needs three)
+    for (int f = 0; f < 4; ++f)
+        for (int q = 0; q < 3; ++q) { CK(state[f][q].alloc(N * sizeof(double))); CK(cudaMemset(state[f][q].p, 0, N * sizeof(double))); }
+    for (int f = 0; f < 4; ++f) cur[f] = 0;
+    CK(p.alloc(N * sizeof(double))); CK(cudaMemset(p.p, 0, N * sizeof(double)));
+    tsize = mixed ? sizeof(float) : sizeof(double);
+    for (int f = 0; f < 4; ++f) { CK(tend[f].alloc(3 * N * tsize)); CK(cudaMemset(tend[f].p, 0, 3 * N * tsize)); }
+    CK(FS.alloc(M * (mixed ? sizeof(float2) : sizeof(double2))));
+    if (mixed) CK(p2.alloc(N * sizeof(double)));
+    // plans and tables
+    CK(plx.build(nx / 2)); CK(ply.build(ny)); CK(plz.build(rigid ? 1 : nz));
+    {
+        std::vector<double2> tw(nxh);
+        for (int t = 0; t < nxh; ++t) tw[t] = twiddle_fwd(t, nx);
+        CK(twx.alloc(nxh * sizeof(double2)));
+        CK(cudaMemcpy(twx.p, tw.data(), nxh * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+    // wavenumbers (my_fft.f90:87-156) and per-axis symbols (eigenvectors.f90:224-268)
+    const double pi = std::acos(0.0) * 2.0;
+    std::vector<double> kx(nxh), ky(ny), kz(nz);
+    for (int i = 1; i <= nx / 2 + 1; ++i) kx[i - 1] = 2 * (i - 1) * pi / P.Lx;
+    for (int j = 1; j <= (ny + 1) / 2; ++j) ky[j - 1] = 2 * (j - 1) * pi / P.Ly;
+    for (int j = (ny + 1) / 2 + 1; j <= ny; ++j) ky[j - 1] = -(2 * (ny - j + 1) * pi / P.Ly);
+    if (rigid) {
+        for (int k = 1; k <= nz; ++k) kz[k - 1] = (double)(k - 1) * pi / P.Lz;
+    } else {
+        for (int k = 1; k <= (nz + 1) / 2; ++k) kz[k - 1] = 2 * (k - 1) * pi / P.Lz;
+        for (int k = (nz + 1) / 2 + 1; k <= nz; ++k) kz[k - 1] = -(2 * (nz - k + 1) * pi / P.Lz);
+    }
+    auto axis = [&](const std::vector<double>& k, double d, std::vector<double>& hk, std::vector<double>& ep,
+                    std::vector<double2>& ex) {
+        hk.resize(k.size()); ep.resize(k.size()); ex.resize(k.size());
+        for (size_t t = 0; t < k.size(); ++t) {
+            hk[t] = hat_ksqr(k[t], d);
+            ep[t] = hat_epm(k[t], d);
+            ex[t] = make_double2(std::cos(k[t] * d), std::sin(k[t] * d));
+        }
+    };
+    std::vector<double> hkx, hky, hkz, ex_, ey_, ez_, sz(nz), cz(nz), hkz_ds(nz);
+    std::vector<double2> px, py, pz;
+    axis(kx, P.dx, hkx, ex_, px);
+    axis(ky, P.dy, hky, ey_, py);
+    axis(kz, P.dz, hkz, ez_, pz);
+    for (int k = 0; k < nz; ++k) {
+        const double arg = kz[k] / 2 * P.dz;
+        sz[k] = std::sin(arg); cz[k] = std::cos(arg);
+        hkz_ds[k] = hkz[k] / P.dsqr;
+    }
+    auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = b.alloc(bytes);
+        if (e) return e;
+        return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+    };
+    CK(up(t_kx, kx.data(), nxh * 8)); CK(up(t_ky, ky.data(), ny * 8)); CK(up(t_kz, kz.data(), nz * 8));
+    CK(up(t_hkx, hkx.data(), nxh * 8)); CK(up(t_hky, hky.data(), ny * 8)); CK(up(t_hkz, hkz.data(), nz * 8));
+    CK(up(t_ex, ex_.data(), nxh * 8)); CK(up(t_ey, ey_.data(), ny * 8)); CK(up(t_ez, ez_.data(), nz * 8));
+    CK(up(t_px, px.data(), nxh * 16)); CK(up(t_py, py.data(), ny * 16)); CK(up(t_pz, pz.data(), nz * 16));
+    CK(up(t_sz, sz.data(), nz * 8)); CK(up(t_cz, cz.data(), nz * 8)); CK(up(t_hkz_ds, hkz_ds.data(), nz * 8));
+    if (rigid) {
+        // vertical modes psi, phi, psib (my_fft.f90:112-127), Fortran column-major (k, mode)
+        std::vector<double> psi((size_t)nz * nz, 0.0), phi((size_t)nz * nz, 0.0), psib((size_t)nz * nz, 0.0);
+        auto A = [&](std::vector<double>& m, int k, int k2) -> double& { return m[(k - 1) + (size_t)nz * (k2 - 1)]; };
+        for (int k = 1; k <= nz; ++k) { A(phi, k, 1) = std::sqrt(1.0 / P.Lz); A(psi, k, 1) = 0.0; A(psib, k, 1) = 0.0; }
+        for (int k2 = 2; k2 <= nz; ++k2) {
+            for (int k = 1; k <= nz; ++k) A(psi, k, k2) = std::sqrt(2.0 / P.Lz) * std::sin((k2 - 1) * k * pi / nz);
+            const double sd = 2 * std::sin((k2 - 1) * pi / (2 * nz));
+            const double cd = 2 * std::cos((k2 - 1) * pi / (2 * nz));
+            A(phi, 1, k2) = A(psi, 1, k2) / sd;
+            A(psib, 1, k2) = A(psi, 1, k2) / cd;
+            for (int k = 2; k <= nz; ++k) {
+                A(phi, k, k2) = (A(psi, k, k2) - A(psi, k - 1, k2)) / sd;
+                A(psib, k, k2) = (A(psi, k, k2) + A(psi, k - 1, k2)) / cd;
+            }
+        }
+        CK(up(m_phi, phi.data(), phi.size() * 8)); CK(up(m_psi, psi.data(), psi.size() * 8));
+        CK(up(m_psib, psib.data(), psib.size() * 8));
+    }
+    // plane kernel shapes
+    PlaneArgs base{};
+    base.nx = nx; base.ny = ny; base.nz = nz; base.nxh = nxh;
+    base.px = plx.plan; base.py = ply.plan; base.twx = (const double2*)twx.p;
+    base.rdx = 1.0 / P.dx; base.rdy = 1.0 / P.dy; base.rdz = 1.0 / P.dz;
+    pa64 = base; pa32 = base;
+    if (!choose_plane_config(nx, ny, sizeof(double2), pa64)) return PS3D_ERR_BADPARAM;
+    if (!choose_plane_config(nx, ny, sizeof(float2), pa32)) return PS3D_ERR_BADPARAM;
+    // reductions
+    nred = 148 * 4;
+    CK(red_partials.alloc((size_t)nred * 5 * sizeof(double)));
+    CK(red_out.alloc(256));   // DiagOut at 0, norm results (4 doubles) at byte 64
+    CK(cudaStreamSynchronize(stream));
+    return PS3D_OK;
+}
+
+cudaError_t Ctx::ensure_spectral4() {
+    if (spec4[0].p) return cudaSuccess;
+    cudaError_t e;
+    for (int f = 0; f < 4; ++f) if ((e = spec4[f].alloc(M * sizeof(double2)))) return e;
+    if ((e = g0base.alloc(M * sizeof(double2)))) return e;
+    if ((e = cudaMemset(g0base.p, 0, M * sizeof(double2)))) return e;
+    if ((e = qtmp.alloc(M * sizeof(double2)))) return e;
+    return cudaSuccess;
+}
+cudaError_t Ctx::ensure_fieldset(int which) {
+    DevBuf* s = fieldset(which);
+    if (!s) return cudaErrorInvalidValue;
+    if (s[0].p) return cudaSuccess;
+    for (int f = 0; f < 4; ++f) {
+        cudaError_t e = s[f].alloc(N * sizeof(double));
+        if (e) return e;
+        if ((e = cudaMemsetAsync(s[f].p, 0, N * sizeof(double), stream))) return e;
+    }
+    return cudaSuccess;
+}
+DevBuf* Ctx::fieldset(int which) {
+    switch (which) {
+        case PS3D_FIELDS_BALANCED: return bal;
+        case PS3D_FIELDS_BASE: return base;
+        case PS3D_FIELDS_ZERO: return zero;
+        case kSetSave: return save;
+        case kSetAve: return ave;
+        case kSetSave2: return save2;
+        default: return nullptr;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// integrate (integrate.f90:2-115)
+// ---------------------------------------------------------------------------
+int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
+    StepArgs a{};
+    a.nx = nx; a.ny = ny; a.nz = nz;
+    a.rigid = rigid; a.nonlinear = P.enable_nonlinear != 0;
+    a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz;
+    a.dt = P.dt; a.dtw = P.dt / P.dsqr;
+    a.Ro = P.Ro; a.dsqr = P.dsqr; a.N0sq = P.N0 * P.N0; a.f0 = P.f0;
+    a.Ah = P.Ah; a.Av = P.Av; a.Kh = P.Kh; a.Kv = P.Kv;
+    a.harm_uvw = (P.Ah > 0. || P.Av > 0.); a.harm_b = (P.Kh > 0. || P.Kv > 0.);
+    if (itt_ == 0) { a.ab0 = 1.0; a.ab1 = 0.0; a.ab2 = 0.0; }
+    else if (itt_ == 1 || !P.enable_AB_3_order) { a.ab0 = 1.5 + P.eps_ab; a.ab1 = -(0.5 + P.eps_ab); a.ab2 = 0.0; }
+    else { a.ab0 = 23.0 / 12.0; a.ab1 = -16.0 / 12.0; a.ab2 = 5.0 / 12.0; }
+    const int s0 = tau_ - 1, s1 = taum1_ - 1, s2 = taum2_ - 1;
+    for (int f = 0; f < 4; ++f) {
+        a.t0[f] = (char*)tend[f].p + (size_t)s0 * N * tsize;
+        a.t1[f] = (const char*)tend[f].p + (size_t)s1 * N * tsize;
+        a.t2[f] = (const char*)tend[f].p + (size_t)s2 * N * tsize;
+    }
+    a.u = field(0); a.v = field(1); a.w = field(2); a.b = field(3);
+    const bool bg = (fkind & PS3D_FORCE_BACKGROUND) != 0;
+    const bool wm = (fkind & PS3D_FORCE_WAVEMAKER) != 0;
+    const bool cb = (fkind & PS3D_FORCE_CALLBACK) != 0 && fn != nullptr;
+    const bool bih = P.Ahbi > 0. || P.Avbi > 0. || P.Khbi > 0. || P.Kvbi > 0.;
+    const bool harm = a.harm_uvw || a.harm_b;
+    if (wm) {
+        const double t = P.dt * itt_;
+        a.wm_on = 1; a.wm_c = std::cos(omega * t); a.wm_s = std::sin(omega * t);
+        for (int f = 0; f < 4; ++f) { a.wr[f] = (const double*)wr[f].p; a.wi[f] = (const double*)wi[f].p; }
+    }
+    const bool fused = !bih && !cb && !(bg && harm);
+    if (fused) {
+        if (bg) { a.ub = (const double*)ub.p; a.bb = (const double*)bb.p; }
+        int nxt[4];
+        for (int f = 0; f < 4; ++f) nxt[f] = (cur[f] + 1) % 3;
+        a.uo = (double*)state[0][nxt[0]].p; a.vo = (double*)state[1][nxt[1]].p;
+        a.wo = (double*)state[2][nxt[2]].p; a.bo = (double*)state[3][nxt[3]].p;
+        a.do_ab = 1;
+        LAUNCH(PS3D_K_STEP, launch_step(a, mixed, stream));
+        for (int f = 0; f < 4; ++f) cur[f] = nxt[f];
+    } else {
+        if (mixed) return PS3D_ERR_UNSUPPORTED;   // generic path keeps FP64 tendencies
+        int old[4], B[4], Cb[4];
+        for (int f = 0; f < 4; ++f) { old[f] = cur[f]; B[f] = (cur[f] + 1) % 3; Cb[f] = (cur[f] + 2) % 3; }
+        a.uo = (double*)state[0][B[0]].p; a.vo = (double*)state[1][B[1]].p;
+        a.wo = (double*)state[2][B[2]].p; a.bo = (double*)state[3][B[3]].p;
+        a.do_ab = 0;
+        a.wm_on = 0;
+        StepArgs k1 = a;
+        LAUNCH(PS3D_K_STEP, launch_step(k1, false, stream));
+        int fin[4] = {B[0], B[1], B[2], B[3]};
+        // biharmonic_h then biharmonic_v per field (integrate.f90:68-78)
+        const double rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
+        for (int f = 0; f < 4; ++f) {
+            const double hb = f < 3 ? P.Ahbi : P.Khbi;
+            const double vb = f < 3 ? P.Avbi : P.Kvbi;
+            int in = B[f], other = Cb[f];
+            if (hb > 0.) {
+                LAUNCH(PS3D_K_OTHER, launch_biharmonic_h((const double*)state[f][in].p, (const double*)state[f][old[f]].p,
+                                       (double*)state[f][other].p, nx, ny, nz, hb, rdx, rdy, P.dt, stream));
+                std::swap(in, other);
+            }
+            if (vb > 0.) {
+                LAUNCH(PS3D_K_OTHER, launch_biharmonic_v((const double*)state[f][in].p, (const double*)state[f][old[f]].p,
+                                       (double*)state[f][other].p, nx, ny, nz, rigid, vb, rdz, P.dt, stream));
+                std::swap(in, other);
+                if (f == 2 && rigid)   // w(:,:,nz:nz+2) = 0 after biharmonic_v(w)
+                    CK(cudaMemsetAsync((double*)state[f][in].p + (size_t)(nz - 1) * nx * ny, 0,
+                                       (size_t)nx * ny * sizeof(double), stream));
+            }
+            fin[f] = in;
+        }
+        // set_forcing (integrate.f90:82) on the friction-updated state
+        StepArgs fa = a;
+        fa.u = (const double*)state[0][fin[0]].p; fa.v = (const double*)state[1][fin[1]].p;
+        fa.w = (const double*)state[2][fin[2]].p; fa.b = (const double*)state[3][fin[3]].p;
+        fa.uo = (double*)state[0][fin[0]].p; fa.vo = (double*)state[1][fin[1]].p;
+        fa.wo = (double*)state[2][fin[2]].p; fa.bo = (double*)state[3][fin[3]].p;
+        if (bg) {
+            fa.ub = (const double*)ub.p; fa.bb = (const double*)bb.p;
+            LAUNCH(PS3D_K_OTHER, launch_forcing_background(fa, stream));
+        }
+        if (cb) {
+            ps3d_device_view view{};
+            view.nx = nx; view.ny = ny; view.nz = nz;
+            view.u = fa.uo; view.v = fa.vo; view.w = fa.wo; view.b = fa.bo;
+            view.du = (double*)a.t0[0]; view.dv = (double*)a.t0[1]; view.dw = (double*)a.t0[2]; view.db = (double*)a.t0[3];
+            view.dt = P.dt; view.Ro = P.Ro; view.itt = itt_; view.stream = (void*)stream;
+            const int rc = fn(user, &view);
+            if (rc != 0) return rc < 0 ? rc : PS3D_ERR_BADPARAM;
+        }
+        if (wm) {
+            fa.wm_on = 1; fa.wm_c = a.wm_c; fa.wm_s = a.wm_s;
+            for (int f = 0; f < 4; ++f) { fa.wr[f] = a.wr[f]; fa.wi[f] = a.wi[f]; }
+        }
+        LAUNCH(PS3D_K_OTHER, launch_wavemaker_ab(fa, wm ? 1 : 0, stream));
+        for (int f = 0; f < 4; ++f) cur[f] = fin[f];
+    }
+    return pressure_solve();
+}
+
+// ---------------------------------------------------------------------------
+// pressure_solver (pressure_solver.f90:2-120)
+// ---------------------------------------------------------------------------
+int Ctx::poisson_once(double* out, double beta) {
+    const bool f32 = mixed;
+    PlaneArgs a = f32 ? pa32 : pa64;
+    a.mode = 0;
+    a.u = field(0); a.v = field(1); a.w = field(2);
+    a.rdt = 1.0 / P.dt;
+    a.scale = P.dx * P.dy;
+    a.spec = FS.p;
+    LAUNCH(PS3D_K_FFT_FWD, launch_plane_fwd(a, f32, stream));
+    ColumnArgs c{};
+    c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = FS.p;
+    c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p; c.hkz = (const double*)t_hkz_ds.p;
+    if (rigid) {
+        c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
+        c.dz2dsqr = P.dz * P.dz * P.dsqr;
+        LAUNCH(PS3D_K_VSOLVE, launch_thomas(c, f32, stream));
+    } else {
+        c.pz = plz.plan; c.scale = P.dz; c.op = 0;
+        LAUNCH(PS3D_K_VSOLVE, launch_zsolve(c, f32, stream));
+    }
+    PlaneArgs b = f32 ? pa32 : pa64;
+    b.spec = FS.p;
+    b.out = out;
+    b.beta = beta;
+    b.scale = rigid ? 1.0 / (P.Lx * P.Ly) : 1.0 / (P.Lx * P.Ly * P.Lz);
+    LAUNCH(PS3D_K_FFT_INV, launch_plane_inv(b, f32, stream));
+    LAUNCH(PS3D_K_CORRECT, launch_correct(field(0), field(1), field(2), out, nx, ny, nz, rigid, P.dt, P.dt / P.dsqr,
+                      1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, stream));
+    return PS3D_OK;
+}
+
+int Ctx::pressure_solve() {
+    int rc = poisson_once((double*)p.p, 0.0);
+    if (rc) return rc;
+    if (mixed) {
+        // one FP64-residual refinement: the divergence of the corrected
+        // velocity is solved again and its pressure added to p
+        rc = poisson_once((double*)p2.p, 0.0);
+        if (rc) return rc;
+        LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N, 1.0, 1.0, stream));
+    }
+    return PS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// forward_transform / backward_transform (diag_balance.f90:421-462)
+// ---------------------------------------------------------------------------
+int Ctx::forward_transform(const double* const* in) {
+    CK(ensure_spectral4());
+    const DevBuf* modes[4] = {&m_phi, &m_phi, &m_psi, &m_psib};
+    for (int f = 0; f < 4; ++f) {
+        PlaneArgs a = pa64;
+        a.mode = 1; a.src = in[f]; a.scale = P.dx * P.dy;
+        a.spec = rigid ? qtmp.p : spec4[f].p;
+        LAUNCH(PS3D_K_OTHER, launch_plane_fwd(a, false, stream));
+        if (rigid) {
+            LAUNCH(PS3D_K_OTHER, launch_vert_mode((const double2*)qtmp.p, (double2*)spec4[f].p, (const double*)modes[f]->p,
+                                nz, M2, P.dz, 0, stream));
+        } else {
+            ColumnArgs c{};
+            c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
+            c.pz = plz.plan; c.scale = P.dz; c.op = 1;
+            LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
+        }
+    }
+    return PS3D_OK;
+}
+int Ctx::backward_transform(double* const* out) {
+    const DevBuf* modes[4] = {&m_phi, &m_phi, &m_psi, &m_psib};
+    for (int f = 0; f < 4; ++f) {
+        void* src = spec4[f].p;
+        if (rigid) {
+            LAUNCH(PS3D_K_OTHER, launch_vert_mode((const double2*)spec4[f].p, (double2*)qtmp.p, (const double*)modes[f]->p,
+                                nz, M2, 1.0, 1, stream));
+            src = qtmp.p;
+        } else {
+            ColumnArgs c{};
+            c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
+            c.pz = plz.plan; c.scale = 1.0; c.op = 2;
+            LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
+        }
+        PlaneArgs b = pa64;
+        b.spec = src; b.out = out[f]; b.beta = 0.0;
+        b.scale = rigid ? 1.0 / (P.Lx * P.Ly) : 1.0 / (P.Lx * P.Ly * P.Lz);
+        LAUNCH(PS3D_K_OTHER, launch_plane_inv(b, false, stream));
+    }
+    return PS3D_OK;
+}
+
+int Ctx::project(int mode) {
+    if (mode < 0 || mode > 3) return PS3D_ERR_BADPARAM;
+    const double* in[4] = {field(0), field(1), field(2), field(3)};
+    int rc = forward_transform(in);
+    if (rc) return rc;
+    ProjArgs a{};
+    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid;
+    a.dx = P.dx; a.dy = P.dy; a.dz = P.dz; a.f0 = P.f0; a.N0 = P.N0; a.dsqr = P.dsqr;
+    a.ax.kx = (const double*)t_kx.p; a.ax.ky = (const double*)t_ky.p; a.ax.kz = (const double*)t_kz.p;
+    a.ax.hkx = (const double*)t_hkx.p; a.ax.hky = (const double*)t_hky.p; a.ax.hkz = (const double*)t_hkz.p;
+    a.ax.ex = (const double*)t_ex.p; a.ax.ey = (const double*)t_ey.p; a.ax.ez = (const double*)t_ez.p;
+    a.ax.px = (const double2*)t_px.p; a.ax.py = (const double2*)t_py.p; a.ax.pz = (const double2*)t_pz.p;
+    a.ax.sz = (const double*)t_sz.p; a.ax.cz = (const double*)t_cz.p;
+    a.US = (double2*)spec4[0].p; a.VS = (double2*)spec4[1].p; a.WS = (double2*)spec4[2].p; a.BS = (double2*)spec4[3].p;
+    a.g0base = (double2*)g0base.p;
+    a.mode = mode;
+    LAUNCH(PS3D_K_OTHER, launch_project(a, stream));
+    double* out[4];
+    if (mode == PS3D_PROJ_NORMAL_MODE || mode == PS3D_PROJ_EXCHANGE) {
+        for (int f = 0; f < 4; ++f) out[f] = field(f);
+    } else {
+        const int set = mode == PS3D_PROJ_BASE_POINT ? PS3D_FIELDS_BASE : PS3D_FIELDS_ZERO;
+        CK(ensure_fieldset(set));
+        DevBuf* s = fieldset(set);
+        for (int f = 0; f < 4; ++f) out[f] = (double*)s[f].p;
+    }
+    return backward_transform(out);
+}
+
+// ---------------------------------------------------------------------------
+// diagnose (diagnose.F90:2-61)
+// ---------------------------------------------------------------------------
+int Ctx::diagnose(double* ke, double* pe, double* umax, double* wmax) {
+    DiagOut* d = (DiagOut*)red_out.p;
+    LAUNCH(PS3D_K_OTHER, launch_diagnose(field(0), field(1), field(2), field(3), (const double*)p.p, nx, ny, nz, P.dsqr, P.N0, P.dz,
+                       (double*)red_partials.p, nred, d, stream));
+    DiagOut h;
+    CK(cudaMemcpyAsync(&h, d, sizeof(DiagOut), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (ke) *ke = h.ke;
+    if (pe) *pe = h.pe;
+    if (umax) *umax = h.umax;
+    if (wmax) *wmax = h.wmax;
+    return (h.flags & kFlagNonFinite) ? PS3D_ERR_NONFINITE : PS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// field-set helpers for the balance drivers
+// ---------------------------------------------------------------------------
+cudaError_t Ctx::copy_state_to(int set) {
+    cudaError_t e = ensure_fieldset(set);
+    if (e) return e;
+    DevBuf* s = fieldset(set);
+    for (int f = 0; f < 4; ++f)
+        if ((e = cudaMemcpyAsync(s[f].p, field(f), N * sizeof(double), cudaMemcpyDeviceToDevice, stream))) return e;
+    return cudaSuccess;
+}
+cudaError_t Ctx::copy_set_to_state(int set) {
+    DevBuf* s = fieldset(set);
+    cudaError_t e;
+    for (int f = 0; f < 4; ++f)
+        if ((e = cudaMemcpyAsync(field(f), s[f].p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream))) return e;
+    return cudaSuccess;
+}
+
+static double ramp(double theta) {   // diag_opt_balance.f90:367-378
+    const double t1 = 1. / std::max(1e-32, theta);
+    const double t2 = 1. / std::max(1e-32, 1.0 - theta);
+    return std::exp(-t1) / (std::exp(-t1) + std::exp(-t2));
+}
+
+// opt_time_ave (diag_opt_balance.f90:234-258): the linear run's time mean into `set`
+int Ctx::opt_time_ave(int set, int n_end_ave) {
+    itt = 0; taum2 = 1; taum1 = 2; tau = 3;
+    P.dt = std::fabs(P.dt);
+    P.Ro = 0.;
+    CK(ensure_fieldset(set));
+    DevBuf* s = fieldset(set);
+    for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(s[f].p, 0, N * sizeof(double), stream));
+    for (int n = 0; n <= n_end_ave - 1; ++n) {
+        int rc = step(itt, tau, taum1, taum2);
+        if (rc) return rc;
+        rotate();
+        for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, field(f), N, 1.0, 1.0, stream));
+    }
+    for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, nullptr, N, 1.0 / n_end_ave, 0.0, stream));
+    return PS3D_OK;
+}
+
+int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
+    if (!(O.period > 0) || O.max_itts < 1 || (O.enable_time_ave && (!(O.average > 0) || O.average_times < 1)))
+        return PS3D_ERR_BADPARAM;
+    // save model state (:78-83)
+    CK(copy_state_to(kSetSave));
+    CK(ensure_saved_tail());
+    CK(cudaMemcpyAsync(saved_p.p, p.p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    for (int f = 0; f < 4; ++f)
+        CK(cudaMemcpyAsync(saved_tend[f].p, tend[f].p, 3 * N * tsize, cudaMemcpyDeviceToDevice, stream));
+    const double Ro_loc = P.Ro, dt_loc = P.dt;
+    const double Ahbi_loc = P.Ahbi, Avbi_loc = P.Avbi, Khbi_loc = P.Khbi, Kvbi_loc = P.Kvbi;
+    const int tau_loc = tau, taum1_loc = taum1, taum2_loc = taum2, itt_loc = itt;
+    CK(copy_state_to(PS3D_FIELDS_BALANCED));
+    const int n_end = (int)(O.period / P.dt) + 1;
+    const int n_end_ave = (int)(O.average / P.dt) + 1;
+    double norm_diff = 1.0;
+    int rc = PS3D_OK, n_done = 0;
+    if (O.enable_time_ave) {
+        for (int m = 1; m <= O.average_times && !rc; ++m) {
+            rc = opt_time_ave(PS3D_FIELDS_BASE, n_end_ave);
+            if (!rc) CK(copy_set_to_state(PS3D_FIELDS_BASE));
+        }
+        if (!rc) CK(copy_set_to_state(PS3D_FIELDS_BALANCED));
+    } else {
+        rc = project(PS3D_PROJ_BASE_POINT);
+    }
+    for (int n = 1; n <= O.max_itts && !rc; ++n) {
+        n_done = n;
+        // opt_backward_integration (:183-209)
+        P.Ahbi = 0; P.Avbi = 0; P.Khbi = 0; P.Kvbi = 0;
+        itt = 0; taum2 = 1; taum1 = 2; tau = 3;
+        P.dt = -std::fabs(P.dt);
+        for (int s = 0; s <= n_end - 1 && !rc; ++s) {
+            P.Ro = (1. - ramp(s * dt_loc / O.period)) * Ro_loc;
+            rc = step(itt, tau, taum1, taum2);
+            rotate();
+        }
+        P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
+        if (rc) break;
+        if (O.enable_time_ave) {
+            for (int m = 1; m <= O.average_times && !rc; ++m) {
+                rc = opt_time_ave(kSetAve, n_end_ave);
+                if (!rc) CK(copy_set_to_state(kSetAve));
+            }
+        } else {
+            rc = project(PS3D_PROJ_NORMAL_MODE);
+        }
+        if (rc) break;
+        // opt_forward_integration (:213-231)
+        itt = 0; taum2 = 1; taum1 = 2; tau = 3;
+        P.dt = std::fabs(P.dt);
+        for (int s = 0; s <= n_end - 1 && !rc; ++s) {
+            P.Ro = ramp(s * dt_loc / O.period) * Ro_loc;
+            rc = step(itt, tau, taum1, taum2);
+            rotate();
+        }
+        if (rc) break;
+        if (O.enable_time_ave) {
+            CK(copy_state_to(kSetSave2));
+            for (int m = 1; m <= O.average_times && !rc; ++m) {
+                rc = opt_time_ave(kSetAve, n_end_ave);
+                if (!rc) CK(copy_set_to_state(kSetAve));
+            }
+            if (rc) break;
+            DevBuf *sv = fieldset(kSetSave2), *av = fieldset(kSetAve), *bs = fieldset(PS3D_FIELDS_BASE);
+            for (int f = 0; f < 4; ++f) {
+                CK(cudaMemcpyAsync(field(f), sv[f].p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+                LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)av[f].p, N, 1.0, -1.0, stream));
+                LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)bs[f].p, N, 1.0, 1.0, stream));
+            }
+        } else {
+            rc = project(PS3D_PROJ_EXCHANGE);
+            if (rc) break;
+        }
+        // opt_balance_norm (:339-362)
+        {
+            DevBuf* bl = fieldset(PS3D_FIELDS_BALANCED);
+            const double* x[4] = {field(0), field(1), field(2), field(3)};
+            const double* y[4] = {(const double*)bl[0].p, (const double*)bl[1].p, (const double*)bl[2].p, (const double*)bl[3].p};
+            double* out = (double*)red_out.p + 8;
+            LAUNCH(PS3D_K_OTHER, launch_norm(x, y, N, P.dsqr, P.N0 * P.N0, (double*)red_partials.p, nred, out, stream));
+            double h[4];
+            CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            norm_diff = h[3];
+        }
+        CK(copy_state_to(PS3D_FIELDS_BALANCED));
+        if (n > 1 && norm_diff < O.tol) break;
+    }
+    // restore model state (:172-176)
+    CK(copy_set_to_state(kSetSave));
+    CK(cudaMemcpyAsync(p.p, saved_p.p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    for (int f = 0; f < 4; ++f)
+        CK(cudaMemcpyAsync(tend[f].p, saved_tend[f].p, 3 * N * tsize, cudaMemcpyDeviceToDevice, stream));
+    P.Ro = Ro_loc; P.dt = dt_loc;
+    P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
+    tau = tau_loc; taum1 = taum1_loc; taum2 = taum2_loc; itt = itt_loc;
+    if (rc) return rc;
+    if (O.adopt) CK(copy_set_to_state(PS3D_FIELDS_BALANCED));
+    CK(cudaStreamSynchronize(stream));
+    if (final_norm) *final_norm = norm_diff;
+    if (iters) *iters = n_done;
+    return PS3D_OK;
+}
+
+cudaError_t Ctx::ensure_saved_tail() {
+    if (saved_p.p) return cudaSuccess;
+    cudaError_t e;
+    if ((e = saved_p.alloc(N * sizeof(double)))) return e;
+    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * tsize))) return e;
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// host <-> device in the reference's halo layout
+// ---------------------------------------------------------------------------
+cudaError_t Ctx::ensure_staging() {
+    if (staging.p) return cudaSuccess;
+    return staging.alloc_host(N * sizeof(double));
+}
+void Ctx::gather(const double* h, double* dst) const {
+    const long sy = nx + 4, sz = (long)(nx + 4) * (ny + 4);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            std::memcpy(dst + ((long)k * ny + j) * nx, h + 2 + sy * (j + 2) + sz * (k + 2), nx * sizeof(double));
+}
+void Ctx::scatter(const double* src, double* h, int kind) const {
+    const long sy = nx + 4, sz = (long)(nx + 4) * (ny + 4);
+    for (int kk = -1; kk <= nz + 2; ++kk) {
+        int k = ((kk - 1) % nz + nz) % nz;   // periodic copy of every halo point
+        if (kind == 1 && rigid) k = kk < 1 ? 0 : (kk > nz ? nz - 1 : kk - 1);   // p ghost levels (:82-93)
+        for (int jj = -1; jj <= ny + 2; ++jj) {
+            const int j = ((jj - 1) % ny + ny) % ny;
+            const double* row = src + ((long)k * ny + j) * nx;
+            double* out = h + sy * (jj + 1) + sz * (kk + 1);
+            out[0] = row[nx - 2]; out[1] = row[nx - 1];
+            std::memcpy(out + 2, row, nx * sizeof(double));
+            out[nx + 2] = row[0]; out[nx + 3] = row[1];
+        }
+    }
+}
+int Ctx::upload_field(double* dev, const double* h) {
+    if (!h) return PS3D_OK;
+    CK(ensure_staging());
+    gather(h, (double*)staging.p);
+    CK(cudaMemcpyAsync(dev, staging.p, N * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    return PS3D_OK;
+}
+int Ctx::download_field(const double* dev, double* h, int kind) {
+    if (!h) return PS3D_OK;
+    CK(ensure_staging());
+    CK(cudaMemcpyAsync(staging.p, dev, N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    scatter((const double*)staging.p, h, kind);
+    return PS3D_OK;
+}
+int Ctx::upload_tend(int f, const double* h) {
+    const long n3 = (long)(nx + 4) * (ny + 4) * (nz + 4);
+    for (int s = 0; s < 3; ++s) {
+        char* dev = (char*)tend[f].p + (size_t)s * N * tsize;
+        if (!h) { CK(cudaMemsetAsync(dev, 0, N * tsize, stream)); continue; }
+        CK(ensure_staging());
+        gather(h + s * n3, (double*)staging.p);
+        if (mixed) {
+            std::vector<float> tmp(N);
+            const double* d = (const double*)staging.p;
+            for (long t = 0; t < N; ++t) tmp[t] = (float)d[t];
+            CK(cudaMemcpy(dev, tmp.data(), N * sizeof(float), cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpyAsync(dev, staging.p, N * sizeof(double), cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+        }
+    }
+    CK(cudaStreamSynchronize(stream));
+    return PS3D_OK;
+}
+int Ctx::download_tend(int f, double* h) {
+    if (!h) return PS3D_OK;
+    const long n3 = (long)(nx + 4) * (ny + 4) * (nz + 4);
+    CK(ensure_staging());
+    for (int s = 0; s < 3; ++s) {
+        const char* dev = (const char*)tend[f].p + (size_t)s * N * tsize;
+        if (mixed) {
+            std::vector<float> tmp(N);
+            CK(cudaMemcpy(tmp.data(), dev, N * sizeof(float), cudaMemcpyDeviceToHost));
+            double* d = (double*)staging.p;
+            for (long t = 0; t < N; ++t) d[t] = tmp[t];
+        } else {
+            CK(cudaMemcpyAsync(staging.p, dev, N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+        }
+        scatter((const double*)staging.p, h + s * n3, 0);
+    }
+    return PS3D_OK;
+}
+
+int Ctx::set_forcing(const ps3d_forcing* f) {
+    fkind = 0; fn = nullptr; user = nullptr;
+    if (!f || f->kind == PS3D_FORCE_NONE) return PS3D_OK;
+    if (f->kind & ~(PS3D_FORCE_WAVEMAKER | PS3D_FORCE_BACKGROUND | PS3D_FORCE_CALLBACK)) return PS3D_ERR_BADPARAM;
+    if ((f->kind & PS3D_FORCE_CALLBACK) && !f->fn) return PS3D_ERR_BADPARAM;
+    if (mixed && (f->kind & PS3D_FORCE_CALLBACK)) return PS3D_ERR_UNSUPPORTED;
+    omega = f->omega;
+    const double* r[4] = {f->u_r, f->v_r, f->w_r, f->b_r};
+    const double* im[4] = {f->u_i, f->v_i, f->w_i, f->b_i};
+    for (int q = 0; q < 4; ++q) {
+        wr[q].release(); wi[q].release();
+        if (!(f->kind & PS3D_FORCE_WAVEMAKER)) continue;
+        if (r[q]) { CK(wr[q].alloc(N * sizeof(double))); int rc = upload_field((double*)wr[q].p, r[q]); if (rc) return rc; }
+        if (im[q]) { CK(wi[q].alloc(N * sizeof(double))); int rc = upload_field((double*)wi[q].p, im[q]); if (rc) return rc; }
+    }
+    ub.release(); bb.release();
+    if (f->kind & PS3D_FORCE_BACKGROUND) {
+        CK(ub.alloc(N * sizeof(double))); CK(bb.alloc(N * sizeof(double)));
+        CK(cudaMemset(ub.p, 0, N * sizeof(double))); CK(cudaMemset(bb.p, 0, N * sizeof(double)));
+        int rc = upload_field((double*)ub.p, f->u_back); if (rc) return rc;
+        rc = upload_field((double*)bb.p, f->b_back); if (rc) return rc;
+    }
+    fn = f->fn; user = f->user;
+    fkind = f->kind;
+    return PS3D_OK;
+}
+
+}  // namespace ps3d
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using ps3d::Ctx;
+
+#define GUARD_BEGIN try {
+#define GUARD_END                                          \
+    }                                                      \
+    catch (const std::bad_alloc&) { return PS3D_ERR_OOM; } \
+    catch (...) { return PS3D_ERR_CUDA; }
+
+struct ps3d_ctx { Ctx impl; };
+
+static inline int ctx_ok(ps3d_ctx* c) { return c ? cudaSetDevice(c->impl.device) == cudaSuccess : 0; }
+
+extern "C" {
+
+int ps3d_create(const ps3d_params* prm, int device, ps3d_ctx** out) {
+    GUARD_BEGIN
+    if (!prm || !out) return PS3D_ERR_BADPARAM;
+    *out = nullptr;
+    std::unique_ptr<ps3d_ctx> c(new ps3d_ctx());
+    int rc = c->impl.init(*prm, device);
+    if (rc) return rc;
+    *out = c.release();
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_destroy(ps3d_ctx* ctx) {
+    GUARD_BEGIN
+    if (!ctx) return PS3D_ERR_BADPARAM;
+    cudaSetDevice(ctx->impl.device);
+    if (ctx->impl.stream) cudaStreamSynchronize(ctx->impl.stream);
+    delete ctx;
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_upload_state(ps3d_ctx* ctx, const double* u, const double* v, const double* w, const double* b,
+                      const double* p, const double* du, const double* dv, const double* dw, const double* db,
+                      int itt, int tau, int taum1, int taum2) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    if (tau < 1 || tau > 3 || taum1 < 1 || taum1 > 3 || taum2 < 1 || taum2 > 3 || itt < 0) return PS3D_ERR_BADPARAM;
+    const double* f[4] = {u, v, w, b};
+    for (int q = 0; q < 4; ++q) { int rc = C.upload_field(C.field(q), f[q]); if (rc) return rc; }
+    int rc = C.upload_field((double*)C.p.p, p); if (rc) return rc;
+    const double* t[4] = {du, dv, dw, db};
+    for (int q = 0; q < 4; ++q) { rc = C.upload_tend(q, t[q]); if (rc) return rc; }
+    C.itt = itt; C.tau = tau; C.taum1 = taum1; C.taum2 = taum2;
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_download_state(ps3d_ctx* ctx, double* u, double* v, double* w, double* b, double* p,
+                        double* du, double* dv, double* dw, double* db, int* itt, int* tau, int* taum1, int* taum2) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    double* f[4] = {u, v, w, b};
+    for (int q = 0; q < 4; ++q) { int rc = C.download_field(C.field(q), f[q], 0); if (rc) return rc; }
+    int rc = C.download_field((const double*)C.p.p, p, 1); if (rc) return rc;
+    double* t[4] = {du, dv, dw, db};
+    for (int q = 0; q < 4; ++q) { rc = C.download_tend(q, t[q]); if (rc) return rc; }
+    if (itt) *itt = C.itt;
+    if (tau) *tau = C.tau;
+    if (taum1) *taum1 = C.taum1;
+    if (taum2) *taum2 = C.taum2;
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_step(ps3d_ctx* ctx, int itt, int tau, int taum1, int taum2) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    if (tau < 1 || tau > 3 || taum1 < 1 || taum1 > 3 || taum2 < 1 || taum2 > 3 || itt < 0) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    C.itt = itt; C.tau = tau; C.taum1 = taum1; C.taum2 = taum2;
+    int rc = C.step(itt, tau, taum1, taum2);
+    if (rc) return rc;
+    return C.sync();
+    GUARD_END
+}
+
+int ps3d_integrate(ps3d_ctx* ctx, int nsteps) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx) || nsteps < 0) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    for (int n = 0; n < nsteps; ++n) {
+        int rc = C.step(C.itt, C.tau, C.taum1, C.taum2);
+        if (rc) return rc;
+        C.rotate();
+        C.time = C.time + C.P.dt;
+        C.itt = C.itt + 1;
+    }
+    return C.sync();
+    GUARD_END
+}
+
+int ps3d_set_step_params(ps3d_ctx* ctx, double dt, double Ro, double Ahbi, double Avbi, double Khbi, double Kvbi) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    if (dt == 0.0 || !std::isfinite(dt) || !std::isfinite(Ro)) return PS3D_ERR_BADPARAM;
+    if (C.mixed && (Ahbi > 0 || Avbi > 0 || Khbi > 0 || Kvbi > 0)) return PS3D_ERR_UNSUPPORTED;
+    C.P.dt = dt; C.P.Ro = Ro; C.P.Ahbi = Ahbi; C.P.Avbi = Avbi; C.P.Khbi = Khbi; C.P.Kvbi = Kvbi;
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_pressure_solve(ps3d_ctx* ctx) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    int rc = ctx->impl.pressure_solve();
+    if (rc) return rc;
+    return ctx->impl.sync();
+    GUARD_END
+}
+
+int ps3d_project_geostrophic(ps3d_ctx* ctx, int mode) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    int rc = ctx->impl.project(mode);
+    if (rc) return rc;
+    return ctx->impl.sync();
+    GUARD_END
+}
+
+int ps3d_opt_balance(ps3d_ctx* ctx, const ps3d_optbal* opt, double* final_norm, int* iters) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx) || !opt) return PS3D_ERR_BADPARAM;
+    int rc = ctx->impl.opt_balance(*opt, final_norm, iters);
+    if (rc) return rc;
+    return ctx->impl.sync();
+    GUARD_END
+}
+
+int ps3d_get_fields(ps3d_ctx* ctx, int which, double* u, double* v, double* w, double* b) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    double* out[4] = {u, v, w, b};
+    for (int q = 0; q < 4; ++q) {
+        const double* src;
+        if (which == PS3D_FIELDS_STATE) src = C.field(q);
+        else {
+            ps3d::DevBuf* s = C.fieldset(which);
+            if (!s) return PS3D_ERR_BADPARAM;
+            if (!s[0].p) return PS3D_ERR_BADPARAM;
+            src = (const double*)s[q].p;
+        }
+        int rc = C.download_field(src, out[q], 0);
+        if (rc) return rc;
+    }
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_diagnose(ps3d_ctx* ctx, double* ke, double* pe, double* umax, double* wmax) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.diagnose(ke, pe, umax, wmax);
+    GUARD_END
+}
+
+int ps3d_set_forcing(ps3d_ctx* ctx, const ps3d_forcing* f) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.set_forcing(f);
+    GUARD_END
+}
+
+int ps3d_get_stream(ps3d_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return PS3D_ERR_BADPARAM;
+    *stream = (void*)ctx->impl.stream;
+    return PS3D_OK;
+}
+
+int ps3d_enqueue(ps3d_ctx* ctx, int nsteps) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx) || nsteps < 0) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    for (int n = 0; n < nsteps; ++n) {
+        int rc = C.step(C.itt, C.tau, C.taum1, C.taum2);
+        if (rc) return rc;
+        C.rotate();
+        C.time = C.time + C.P.dt;
+        C.itt = C.itt + 1;
+    }
+    CK(cudaGetLastError());
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_profile(ps3d_ctx* ctx, int enable) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    Ctx& C = ctx->impl;
+    CK(cudaStreamSynchronize(C.stream));
+    C.prof_recs.clear();
+    C.prof_next = 0;
+    C.prof = enable != 0;
+    return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_profile_read(ps3d_ctx* ctx, double* ms, long long* launches) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.prof_read(ms, launches);
+    GUARD_END
+}
+
+const char* ps3d_strerror(int status) {
+    switch (status) {
+        case PS3D_OK: return "ok";
+        case PS3D_ERR_CUDA: return "CUDA runtime error";
+        case PS3D_ERR_NONFINITE: return "non-finite value in the model state";
+        case PS3D_ERR_TIMEOUT: return "bounded wait ran out";
+        case PS3D_ERR_OOM: return "out of device memory or admission budget";
+        case PS3D_ERR_BADPARAM: return "invalid argument";
+        case PS3D_ERR_UNSUPPORTED: return "configuration not supported by this engine";
+        case PS3D_ERR_CANCELLED: return "request cancelled";
+        default: return "unknown status";
+    }
+}
+
+}  // extern "C"
+
+namespace ps3d {
+// Records the last failing CUDA call; printed to stderr when PS3D_VERBOSE is set.
+void note_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+    static const bool verbose = std::getenv("PS3D_VERBOSE") != nullptr;
+    if (verbose) std::fprintf(stderr, "ps3d: %s failed at %s:%d: %s\n", what, file, line, cudaGetErrorString(e));
+}
+}  // namespace ps3d

@@ -1,0 +1,114 @@
+// engine.h — internal interfaces between the host engine and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <algorithm>
+#include "common.cuh"
+#include "ps3d_gpu.h"
+
+namespace ps3d {
+
+// Arguments of one time step for one grid (K1 and the generic-path kernels).
+// Tendency slots are untyped: FP64 in the plain path, FP32 in the mixed path.
+struct StepArgs {
+    int nx, ny, nz;
+    int rigid, nonlinear;
+    double rdx, rdy, rdz;          // 1/dx, 1/dy, 1/dz
+    double dt, dtw;                // dt and dt/dsqr
+    double Ro, dsqr, N0sq, f0;
+    double Ah, Av, Kh, Kv;
+    int harm_uvw, harm_b;          // (Ah>0 .or. Av>0), (Kh>0 .or. Kv>0)
+    double ab0, ab1, ab2;          // AB weights of slots tau, taum1, taum2
+    int do_ab;                     // 0: stop after friction (generic path)
+    const double *u, *v, *w, *b;   // start-of-step state
+    const double *ub, *bb;         // background flow (NULL: none)
+    double *uo, *vo, *wo, *bo;     // new state
+    void* t0[4];                   // tendencies of time level tau (du,dv,dw,db)
+    const void* t1[4];             // taum1
+    const void* t2[4];             // taum2
+    int wm_on;                     // wavemaker active
+    double wm_c, wm_s;             // cos(omega t), sin(omega t)
+    const double* wr[4];           // wavemaker real parts (NULL = 0)
+    const double* wi[4];           // wavemaker imaginary parts
+};
+
+// Plane-FFT kernels (divergence + forward 2D FFT, inverse 2D FFT) for one grid.
+struct PlaneArgs {
+    int nx, ny, nz, nxh;
+    int C;                         // cluster size (CTAs per z-plane)
+    int rows_per_cta, cols_per_cta, row_chunk, ldc, ldr;
+    // forward source: mode 0 = divergence of (u,v,w)/dt, mode 1 = real field src
+    int mode;
+    const double *u, *v, *w, *src;
+    double rdx, rdy, rdz, rdt;
+    double scale;                  // dx*dy (forward) or 1/(Lx*Ly[*Lz]) (inverse)
+    void* spec;                    // complex spectral array [k][ky][kx]
+    double* out;                   // inverse: real output field
+    double beta;                   // inverse: out = beta*out + result (0: overwrite)
+    FFTPlan px;                    // length nx/2
+    FFTPlan py;                    // length ny
+    const double2* twx;            // exp(-2 pi i t/nx), t = 0..nx/2
+};
+
+struct ColumnArgs {
+    int nx, ny, nz, nxh;
+    void* spec;                    // complex [k][ky][kx]
+    const double* hkx;             // hat_ksqr(kx(i),dx)
+    const double* hky;             // hat_ksqr(ky(j),dy)
+    const double* hkz;             // hat_ksqr(kz(k),dz)/dsqr  (periodic)
+    double fxa;                    // 1/dz^2/dsqr              (rigid lid)
+    double dz2dsqr;                // dz**2*dsqr               (rigid lid, (0,0) column)
+    double scale;                  // periodic forward z scale (dz)
+    FFTPlan pz;                    // length nz (periodic)
+    int op;                        // periodic: 0 solve, 1 forward only, 2 inverse only
+};
+
+cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
+cudaError_t launch_biharmonic_h(const double* cur, const double* old, double* out, int nx, int ny, int nz,
+                                double Hmix, double rdx, double rdy, double dt, cudaStream_t s);
+cudaError_t launch_biharmonic_v(const double* cur, const double* old, double* out, int nx, int ny, int nz,
+                                int rigid, double Vmix, double rdz, double dt, cudaStream_t s);
+cudaError_t launch_forcing_background(const StepArgs& a, cudaStream_t s);
+cudaError_t launch_wavemaker_ab(const StepArgs& a, int do_wm, cudaStream_t s);
+cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int nx, int ny, int nz, int rigid,
+                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s);
+
+// poisson.cu
+size_t plane_fwd_smem(const PlaneArgs& a, bool fp32);
+size_t plane_inv_smem(const PlaneArgs& a, bool fp32);
+cudaError_t plane_setup(bool fp32);
+cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
+cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);
+cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s);
+cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
+
+// modes.cu: eigen tables for one grid and the projections
+struct EigenAxes {
+    // per-axis tables, host-computed with libm (my_fft.f90:87-156, eigenvectors.f90:224-268)
+    const double* kx;  const double* ky;  const double* kz;
+    const double* hkx; const double* hky; const double* hkz;   // hat_ksqr
+    const double* ex;  const double* ey;  const double* ez;    // hat_epm
+    const double2* px; const double2* py; const double2* pz;   // exp(+i k d)
+    const double* sz;  const double* cz;                       // sin/cos(kz/2*dz) (rigid lid)
+};
+struct ProjArgs {
+    int nxh, ny, nz, rigid;
+    double dx, dy, dz, f0, N0, dsqr;
+    EigenAxes ax;
+    double2 *US, *VS, *WS, *BS;
+    double2* g0base;
+    int mode;                      // PS3D_PROJ_*
+};
+cudaError_t launch_project(const ProjArgs& a, cudaStream_t s);
+cudaError_t launch_vert_mode(const double2* in, double2* out, const double* mode, int nz, long ncol,
+                             double scale, int transpose, cudaStream_t s);
+
+// reduce.cu
+struct DiagOut { double ke, pe, umax, wmax; unsigned flags; };
+cudaError_t launch_diagnose(const double* u, const double* v, const double* w, const double* b, const double* p,
+                            int nx, int ny, int nz, double dsqr, double N0, double dz,
+                            double* partials, int nblk, DiagOut* out_dev, cudaStream_t s);
+cudaError_t launch_norm(const double* const* x, const double* const* y, long n, double dsqr, double N0sq,
+                        double* partials, int nblk, double* out_dev, cudaStream_t s);
+cudaError_t launch_axpby(double* y, const double* x, long n, double a, double b, cudaStream_t s);
+
+}  // namespace ps3d

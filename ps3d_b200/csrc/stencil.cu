@@ -1,0 +1,439 @@
+// stencil.cu — tendency, friction, forcing, Adams-Bashforth and pressure
+// gradient kernels of the ps3D time step on sm_100a.
+//
+// K1 (k_step) fuses, per grid point, what the reference does in ~40 full
+// passes over memory:
+//   buoyancy_advection_2nd            advection.f90:2-48
+//   N^2 term                          integrate.f90:21-23
+//   momentum_advection_2nd            advection.f90:53-184
+//   Coriolis and buoyancy force       integrate.f90:37-54
+//   harmonic friction (in place)      mixing.f90:225-274, integrate.f90:59-66
+//   set_forcing (wavemaker and
+//     background-flow advection)      config.f90:224-237, lee_wave1.f90:232-332
+//   Adams-Bashforth 2/3               integrate.f90:87-102
+// The block owns a 32 x BY column tile and marches up in z; the three planes
+// k-1, k, k+1 of u, v, w, b (and of U_back, B_back when present) sit in a
+// shared-memory ring with a one-point halo.  Face fluxes are recomputed per
+// point instead of being stored, so the kernel reads each state word once
+// from HBM and writes tendencies and the new state once.
+#include "engine.h"
+
+namespace ps3d {
+
+constexpr int kTX = 32;
+
+template <int BY, int NF>
+struct StepSmem {
+    double pl[NF][3][(BY + 2) * (kTX + 2)];
+};
+
+// read field f at offsets (di, dj) in ring slot s
+#define SM(fi, s, dj, di) sm.pl[fi][s][(ty + 1 + (dj)) * (kTX + 2) + (tx + 1 + (di))]
+
+template <typename TT, int BY, bool HARM, bool WM, bool BG>
+__global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) {
+    constexpr int NF = BG ? 6 : 4;
+    __shared__ StepSmem<BY, NF> sm;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
+    const int kb = blockIdx.z * kchunk;
+    const int ke = min(nz, kb + kchunk);
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = (i < nx) && (j < ny);
+    const long plane = (long)nx * ny;
+    const double* src[6] = {a.u, a.v, a.w, a.b, a.ub, a.bb};
+    const int tid = ty * kTX + tx;
+    constexpr int TP = (kTX + 2) * (BY + 2);
+
+    auto load_plane = [&](int kk, int slot) {
+        const int kw = wrap(kk, nz);
+        for (int t = tid; t < TP; t += kTX * BY) {
+            const int ti = t % (kTX + 2), tj = t / (kTX + 2);
+            const int gi = wrap(i0 - 1 + ti, nx), gj = wrap(j0 - 1 + tj, ny);
+            const long g = (long)kw * plane + (long)gj * nx + gi;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) sm.pl[f][slot][t] = __ldg(src[f] + g);
+        }
+    };
+
+    load_plane(kb - 1, (kb + 2) % 3);
+    load_plane(kb, kb % 3);
+    const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
+    const bool rigid = a.rigid;
+    for (int k = kb; k < ke; ++k) {
+        load_plane(k + 1, (k + 1) % 3);
+        __syncthreads();
+        if (active) {
+            const int sm1 = (k + 2) % 3, s0 = k % 3, sp1 = (k + 1) % 3;
+#define U(di, dj, dk) SM(0, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
+#define V(di, dj, dk) SM(1, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
+#define W(di, dj, dk) SM(2, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
+#define B(di, dj, dk) SM(3, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
+#define UB(di, dj, dk) SM(4, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
+#define BB(di, dj, dk) SM(5, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
+            const bool top = rigid && (k == nz - 1);   // flux_top(nz) = 0
+            const bool bot = rigid && (k == 0);        // flux_top(0)  = 0
+            const long g = (long)k * plane + (long)j * nx + i;
+            double db_, du_, dv_, dw_;
+            // ---- buoyancy advection + N^2 (advection.f90:12-47, integrate.f90:21-23)
+            if (a.nonlinear) {
+                const double fe = 0.5 * (B(0, 0, 0) + B(1, 0, 0)) * U(0, 0, 0);
+                const double fem = 0.5 * (B(-1, 0, 0) + B(0, 0, 0)) * U(-1, 0, 0);
+                const double fn = 0.5 * (B(0, 0, 0) + B(0, 1, 0)) * V(0, 0, 0);
+                const double fnm = 0.5 * (B(0, -1, 0) + B(0, 0, 0)) * V(0, -1, 0);
+                const double ft = top ? 0.0 : 0.5 * (B(0, 0, 0) + B(0, 0, 1)) * W(0, 0, 0);
+                const double ftm = bot ? 0.0 : 0.5 * (B(0, 0, -1) + B(0, 0, 0)) * W(0, 0, -1);
+                db_ = -Ro * ((fe - fem) * rdx + (fn - fnm) * rdy + (ft - ftm) * rdz);
+                // ---- zonal momentum (advection.f90:65-100)
+                {
+                    const double e = 0.25 * (U(0, 0, 0) + U(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+                    const double em = 0.25 * (U(-1, 0, 0) + U(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
+                    const double n = 0.25 * (U(0, 0, 0) + U(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+                    const double nm = 0.25 * (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+                    const double t = top ? 0.0 : 0.25 * (U(0, 0, 1) + U(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
+                    const double tm = bot ? 0.0 : 0.25 * (U(0, 0, 0) + U(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
+                    du_ = -Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                }
+                // ---- meridional momentum (advection.f90:104-140)
+                {
+                    const double e = 0.25 * (V(0, 0, 0) + V(1, 0, 0)) * (U(0, 1, 0) + U(0, 0, 0));
+                    const double em = 0.25 * (V(-1, 0, 0) + V(0, 0, 0)) * (U(-1, 1, 0) + U(-1, 0, 0));
+                    const double n = 0.25 * (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 1, 0) + V(0, 0, 0));
+                    const double nm = 0.25 * (V(0, -1, 0) + V(0, 0, 0)) * (V(0, 0, 0) + V(0, -1, 0));
+                    const double t = top ? 0.0 : 0.25 * (V(0, 0, 1) + V(0, 0, 0)) * (W(0, 0, 0) + W(0, 1, 0));
+                    const double tm = bot ? 0.0 : 0.25 * (V(0, 0, 0) + V(0, 0, -1)) * (W(0, 0, -1) + W(0, 1, -1));
+                    dv_ = -Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                }
+                // ---- vertical momentum (advection.f90:145-181); rigid lid zeroes
+                //      flux_top(nz-1:nz+2) for w (:167-170)
+                {
+                    const bool wtop = rigid && (k >= nz - 2);
+                    const bool wbot = rigid && (k == 0 || k >= nz - 1);
+                    const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
+                    const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
+                    const double n = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
+                    const double nm = 0.25 * (W(0, -1, 0) + W(0, 0, 0)) * (V(0, -1, 0) + V(0, -1, 1));
+                    const double t = wtop ? 0.0 : 0.25 * (W(0, 0, 1) + W(0, 0, 0)) * (W(0, 0, 0) + W(0, 0, 1));
+                    const double tm = wbot ? 0.0 : 0.25 * (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, -1) + W(0, 0, 0));
+                    dw_ = -a.dsqr * Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                }
+            } else {
+                db_ = du_ = dv_ = dw_ = 0.0;
+            }
+            db_ = db_ - 0.5 * (W(0, 0, 0) + W(0, 0, -1)) * a.N0sq;
+            // ---- Coriolis, buoyancy force, rigid-lid mask (integrate.f90:37-54)
+            du_ = du_ + (V(0, 0, 0) + V(0, -1, 0) + V(1, 0, 0) + V(1, -1, 0)) * 0.25 * a.f0;
+            dv_ = dv_ - (U(-1, 0, 0) + U(0, 0, 0) + U(-1, 1, 0) + U(0, 1, 0)) * 0.25 * a.f0;
+            dw_ = dw_ + 0.5 * (B(0, 0, 0) + B(0, 0, 1));
+            if (top) dw_ = 0.0;
+            // ---- friction, in place before AB (integrate.f90:59-66)
+            double u1 = U(0, 0, 0), v1 = V(0, 0, 0), w1 = W(0, 0, 0), b1 = B(0, 0, 0);
+            if constexpr (HARM) {
+                const double dt = a.dt;
+#define HARMONIC(F, Hm, Vm, out)                                                                   \
+    {                                                                                            \
+        const double e = Hm * (F(1, 0, 0) - F(0, 0, 0)) * rdx;                                   \
+        const double em = Hm * (F(0, 0, 0) - F(-1, 0, 0)) * rdx;                                 \
+        const double n = Hm * (F(0, 1, 0) - F(0, 0, 0)) * rdy;                                   \
+        const double nm = Hm * (F(0, 0, 0) - F(0, -1, 0)) * rdy;                                 \
+        const double t = top ? 0.0 : Vm * (F(0, 0, 1) - F(0, 0, 0)) * rdz;                       \
+        const double tm = bot ? 0.0 : Vm * (F(0, 0, 0) - F(0, 0, -1)) * rdz;                     \
+        out = F(0, 0, 0) + dt * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);              \
+    }
+                if (a.harm_uvw) {
+                    HARMONIC(U, a.Ah, a.Av, u1)
+                    HARMONIC(V, a.Ah, a.Av, v1)
+                    HARMONIC(W, a.Ah, a.Av, w1)
+                    if (top) w1 = 0.0;
+                }
+                if (a.harm_b) HARMONIC(B, a.Kh, a.Kv, b1)
+#undef HARMONIC
+            }
+            // ---- set_forcing: background-flow advection (lee_wave1.f90:245-312)
+            if constexpr (BG) {
+                {
+                    const double e = 2 * 0.25 * (UB(0, 0, 0) + UB(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+                    const double em = 2 * 0.25 * (UB(-1, 0, 0) + UB(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
+                    const double n = 0.25 * (UB(0, 0, 0) + UB(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+                    const double nm = 0.25 * (UB(0, -1, 0) + UB(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+                    const double t = top ? 0.0 : 0.25 * (UB(0, 0, 1) + UB(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
+                    const double tm = bot ? 0.0 : 0.25 * (UB(0, 0, 0) + UB(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
+                    du_ = du_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                }
+                {
+                    const double e = 0.25 * (V(0, 0, 0) + V(1, 0, 0)) * (UB(0, 1, 0) + UB(0, 0, 0));
+                    const double em = 0.25 * (V(-1, 0, 0) + V(0, 0, 0)) * (UB(-1, 1, 0) + UB(-1, 0, 0));
+                    dv_ = dv_ - Ro * (e - em) * rdx;
+                }
+                {
+                    const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (UB(0, 0, 0) + UB(0, 0, 1));
+                    const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (UB(-1, 0, 0) + UB(-1, 0, 1));
+                    dw_ = dw_ - a.dsqr * Ro * (e - em) * rdx;
+                }
+                {
+                    const double e = 0.5 * (B(0, 0, 0) + B(1, 0, 0)) * UB(0, 0, 0) + 0.5 * (BB(0, 0, 0) + BB(1, 0, 0)) * U(0, 0, 0);
+                    const double em = 0.5 * (B(-1, 0, 0) + B(0, 0, 0)) * UB(-1, 0, 0) + 0.5 * (BB(-1, 0, 0) + BB(0, 0, 0)) * U(-1, 0, 0);
+                    const double n = 0.5 * (BB(0, 0, 0) + BB(0, 1, 0)) * V(0, 0, 0);
+                    const double nm = 0.5 * (BB(0, -1, 0) + BB(0, 0, 0)) * V(0, -1, 0);
+                    const double t = top ? 0.0 : 0.5 * (BB(0, 0, 0) + BB(0, 0, 1)) * W(0, 0, 0);
+                    const double tm = bot ? 0.0 : 0.5 * (BB(0, 0, -1) + BB(0, 0, 0)) * W(0, 0, -1);
+                    db_ = db_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                }
+            }
+#undef U
+#undef V
+#undef W
+#undef B
+#undef UB
+#undef BB
+            // ---- set_forcing: wavemaker (config.f90:224-237)
+            if constexpr (WM) {
+                const double dt = a.dt, c = a.wm_c, s = a.wm_s;
+                if (a.wr[0] || a.wi[0]) u1 = u1 + dt * (c * (a.wr[0] ? a.wr[0][g] : 0.0) + s * (a.wi[0] ? a.wi[0][g] : 0.0));
+                if (a.wr[1] || a.wi[1]) v1 = v1 + dt * (c * (a.wr[1] ? a.wr[1][g] : 0.0) + s * (a.wi[1] ? a.wi[1][g] : 0.0));
+                if (a.wr[2] || a.wi[2]) w1 = w1 + dt * (c * (a.wr[2] ? a.wr[2][g] : 0.0) + s * (a.wi[2] ? a.wi[2][g] : 0.0));
+                if (a.wr[3] || a.wi[3]) b1 = b1 + dt * (c * (a.wr[3] ? a.wr[3][g] : 0.0) + s * (a.wi[3] ? a.wi[3][g] : 0.0));
+            }
+            // ---- store tendency of time level tau
+            ((TT*)a.t0[0])[g] = (TT)du_;
+            ((TT*)a.t0[1])[g] = (TT)dv_;
+            ((TT*)a.t0[2])[g] = (TT)dw_;
+            ((TT*)a.t0[3])[g] = (TT)db_;
+            // ---- Adams-Bashforth (integrate.f90:87-102)
+            if (a.do_ab) {
+                const double dt = a.dt, dtw = a.dtw;
+                const double c0 = a.ab0, c1 = a.ab1, c2 = a.ab2;
+                double tu = c0 * (double)(TT)du_, tv = c0 * (double)(TT)dv_, tw = c0 * (double)(TT)dw_, tb = c0 * (double)(TT)db_;
+                if (c1 != 0.0) {
+                    const TT* const* h = (const TT* const*)a.t1;
+                    tu = tu + c1 * (double)h[0][g]; tv = tv + c1 * (double)h[1][g];
+                    tw = tw + c1 * (double)h[2][g]; tb = tb + c1 * (double)h[3][g];
+                }
+                if (c2 != 0.0) {
+                    const TT* const* h = (const TT* const*)a.t2;
+                    tu = tu + c2 * (double)h[0][g]; tv = tv + c2 * (double)h[1][g];
+                    tw = tw + c2 * (double)h[2][g]; tb = tb + c2 * (double)h[3][g];
+                }
+                u1 = u1 + dt * tu; v1 = v1 + dt * tv; w1 = w1 + dtw * tw; b1 = b1 + dt * tb;
+            }
+            a.uo[g] = u1; a.vo[g] = v1; a.wo[g] = w1; a.bo[g] = b1;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Generic friction stages with the reference's stale-halo semantics: the
+// biharmonic operators of mixing.f90:96-217 run after harmonic() without a
+// halo exchange, so any neighbour outside the interior still holds the
+// start-of-step value.  `cur` is the field after the previous stage, `old`
+// the start-of-step field; out = cur + dt*op(.).
+// ---------------------------------------------------------------------------
+__global__ void k_biharmonic_h(const double* __restrict__ cur, const double* __restrict__ old,
+                               double* __restrict__ out, int nx, int ny, int nz,
+                               double Hmix, double rdx, double rdy, double dt) {
+    const long N = (long)nx * ny * nz;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)(g / ((long)nx * ny));
+        const long pk = (long)k * nx * ny;
+        auto P = [&](int di, int dj) -> double {
+            const int ii = i + di, jj = j + dj;
+            const bool in = ii >= 0 && ii < nx && jj >= 0 && jj < ny;
+            const long gg = pk + (long)wrap(jj, ny) * nx + wrap(ii, nx);
+            return in ? cur[gg] : old[gg];
+        };
+        auto del2 = [&](int di, int dj) -> double {
+            const double fe = -Hmix * (P(di + 1, dj) - P(di, dj)) * rdx;
+            const double fem = -Hmix * (P(di, dj) - P(di - 1, dj)) * rdx;
+            const double fn = -Hmix * (P(di, dj + 1) - P(di, dj)) * rdy;
+            const double fnm = -Hmix * (P(di, dj) - P(di, dj - 1)) * rdy;
+            return (fe - fem) * rdx + (fn - fnm) * rdy;
+        };
+        const double d0 = del2(0, 0);
+        const double fe = (del2(1, 0) - d0) * rdx, fem = (d0 - del2(-1, 0)) * rdx;
+        const double fn = (del2(0, 1) - d0) * rdy, fnm = (d0 - del2(0, -1)) * rdy;
+        out[g] = cur[g] + dt * ((fe - fem) * rdx + (fn - fnm) * rdy);
+    }
+}
+
+__global__ void k_biharmonic_v(const double* __restrict__ cur, const double* __restrict__ old,
+                               double* __restrict__ out, int nx, int ny, int nz, int rigid,
+                               double Vmix, double rdz, double dt) {
+    const long N = (long)nx * ny * nz;
+    const long plane = (long)nx * ny;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+        const int k = (int)(g / plane);
+        const long col = g - (long)k * plane;
+        // 1-based level kr = k+1; flux_top(kr) lives between levels kr and kr+1
+        auto P = [&](int kk) -> double {   // kk: 0-based level, may be outside
+            const bool in = kk >= 0 && kk < nz;
+            const long gg = (long)wrap(kk, nz) * plane + col;
+            return in ? cur[gg] : old[gg];
+        };
+        auto ft1 = [&](int kr) -> double {  // first-stage flux at 1-based level kr
+            if (rigid && (kr <= 0 || kr >= nz)) return 0.0;
+            return -Vmix * (P(kr) - P(kr - 1)) * rdz;
+        };
+        auto del2 = [&](int kr) -> double { return (ft1(kr) - ft1(kr - 1)) * rdz; };
+        auto ft2 = [&](int kr) -> double {
+            if (rigid && (kr <= 0 || kr >= nz)) return 0.0;
+            return (del2(kr + 1) - del2(kr)) * rdz;
+        };
+        const int kr = k + 1;
+        out[g] = cur[g] + dt * ((ft2(kr) - ft2(kr - 1)) * rdz);
+    }
+}
+
+// background-flow forcing on the friction-updated state (generic path)
+__global__ void k_forcing_background(StepArgs a) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const long N = (long)nx * ny * nz, plane = (long)nx * ny;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)(g / plane);
+        auto at = [&](const double* f, int di, int dj, int dk) -> double {
+            return f[(long)wrap(k + dk, nz) * plane + (long)wrap(j + dj, ny) * nx + wrap(i + di, nx)];
+        };
+        const double *u = a.u, *v = a.v, *w = a.w, *b = a.b, *ub = a.ub, *bb = a.bb;
+        const bool top = a.rigid && k == nz - 1, bot = a.rigid && k == 0;
+        const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
+        double* const* T0 = (double* const*)a.t0;
+        double du_ = T0[0][g], dv_ = T0[1][g], dw_ = T0[2][g], db_ = T0[3][g];
+        {
+            const double e = 2 * 0.25 * (at(ub, 0, 0, 0) + at(ub, 1, 0, 0)) * (at(u, 1, 0, 0) + at(u, 0, 0, 0));
+            const double em = 2 * 0.25 * (at(ub, -1, 0, 0) + at(ub, 0, 0, 0)) * (at(u, 0, 0, 0) + at(u, -1, 0, 0));
+            const double n = 0.25 * (at(ub, 0, 0, 0) + at(ub, 0, 1, 0)) * (at(v, 1, 0, 0) + at(v, 0, 0, 0));
+            const double nm = 0.25 * (at(ub, 0, -1, 0) + at(ub, 0, 0, 0)) * (at(v, 1, -1, 0) + at(v, 0, -1, 0));
+            const double t = top ? 0.0 : 0.25 * (at(ub, 0, 0, 1) + at(ub, 0, 0, 0)) * (at(w, 0, 0, 0) + at(w, 1, 0, 0));
+            const double tm = bot ? 0.0 : 0.25 * (at(ub, 0, 0, 0) + at(ub, 0, 0, -1)) * (at(w, 0, 0, -1) + at(w, 1, 0, -1));
+            du_ = du_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+        }
+        {
+            const double e = 0.25 * (at(v, 0, 0, 0) + at(v, 1, 0, 0)) * (at(ub, 0, 1, 0) + at(ub, 0, 0, 0));
+            const double em = 0.25 * (at(v, -1, 0, 0) + at(v, 0, 0, 0)) * (at(ub, -1, 1, 0) + at(ub, -1, 0, 0));
+            dv_ = dv_ - Ro * (e - em) * rdx;
+        }
+        {
+            const double e = 0.25 * (at(w, 0, 0, 0) + at(w, 1, 0, 0)) * (at(ub, 0, 0, 0) + at(ub, 0, 0, 1));
+            const double em = 0.25 * (at(w, -1, 0, 0) + at(w, 0, 0, 0)) * (at(ub, -1, 0, 0) + at(ub, -1, 0, 1));
+            dw_ = dw_ - a.dsqr * Ro * (e - em) * rdx;
+        }
+        {
+            const double e = 0.5 * (at(b, 0, 0, 0) + at(b, 1, 0, 0)) * at(ub, 0, 0, 0) + 0.5 * (at(bb, 0, 0, 0) + at(bb, 1, 0, 0)) * at(u, 0, 0, 0);
+            const double em = 0.5 * (at(b, -1, 0, 0) + at(b, 0, 0, 0)) * at(ub, -1, 0, 0) + 0.5 * (at(bb, -1, 0, 0) + at(bb, 0, 0, 0)) * at(u, -1, 0, 0);
+            const double n = 0.5 * (at(bb, 0, 0, 0) + at(bb, 0, 1, 0)) * at(v, 0, 0, 0);
+            const double nm = 0.5 * (at(bb, 0, -1, 0) + at(bb, 0, 0, 0)) * at(v, 0, -1, 0);
+            const double t = top ? 0.0 : 0.5 * (at(bb, 0, 0, 0) + at(bb, 0, 0, 1)) * at(w, 0, 0, 0);
+            const double tm = bot ? 0.0 : 0.5 * (at(bb, 0, 0, -1) + at(bb, 0, 0, 0)) * at(w, 0, 0, -1);
+            db_ = db_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+        }
+        T0[0][g] = du_; T0[1][g] = dv_; T0[2][g] = dw_; T0[3][g] = db_;
+    }
+}
+
+// wavemaker + Adams-Bashforth, pointwise, in place on the state (generic path)
+__global__ void k_wavemaker_ab(StepArgs a, int do_wm) {
+    const long N = (long)a.nx * a.ny * a.nz;
+    double* fld[4] = {a.uo, a.vo, a.wo, a.bo};
+    const double* const* t0 = (const double* const*)a.t0;
+    const double* const* t1 = (const double* const*)a.t1;
+    const double* const* t2 = (const double* const*)a.t2;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            double x = fld[f][g];
+            if (do_wm && (a.wr[f] || a.wi[f]))
+                x = x + a.dt * (a.wm_c * (a.wr[f] ? a.wr[f][g] : 0.0) + a.wm_s * (a.wi[f] ? a.wi[f][g] : 0.0));
+            double t = a.ab0 * t0[f][g];
+            if (a.ab1 != 0.0) t = t + a.ab1 * t1[f][g];
+            if (a.ab2 != 0.0) t = t + a.ab2 * t2[f][g];
+            fld[f][g] = x + (f == 2 ? a.dtw : a.dt) * t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pressure gradient correction, pressure_solver.f90:98-110 (and the rigid-lid
+// ghost levels :82-93, which make the w correction vanish at level nz)
+// ---------------------------------------------------------------------------
+__global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+                          const double* __restrict__ p, int nx, int ny, int nz, int rigid,
+                          double dt, double dtw, double rdx, double rdy, double rdz) {
+    const long plane = (long)nx * ny, N = plane * nz;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)(g / plane);
+        const double p0 = p[g];
+        const double pe = p[g - i + wrap(i + 1, nx)];
+        const double pn = p[g + (long)(wrap(j + 1, ny) - j) * nx];
+        u[g] = u[g] - dt * (pe - p0) * rdx;
+        v[g] = v[g] - dt * (pn - p0) * rdy;
+        if (rigid && k == nz - 1) {
+            w[g] = 0.0;
+        } else {
+            const double pt = p[g + (long)(wrap(k + 1, nz) - k) * plane];
+            w[g] = w[g] - dtw * (pt - p0) * rdz;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename TT, int BY, bool HARM, bool WM, bool BG>
+static cudaError_t launch_step_t(const StepArgs& a, cudaStream_t s) {
+    const int kchunk = a.nz <= 16 ? a.nz : 8;
+    dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, (a.nz + kchunk - 1) / kchunk);
+    k_step<TT, BY, HARM, WM, BG><<<grid, dim3(kTX, BY), 0, s>>>(a, kchunk);
+    return cudaGetLastError();
+}
+
+template <typename TT>
+static cudaError_t launch_step_tt(const StepArgs& a, cudaStream_t s) {
+    const bool harm = a.harm_uvw || a.harm_b;
+    const bool wm = a.wm_on != 0;
+    const bool bg = a.ub != nullptr;
+#define L(H, W, G) return launch_step_t<TT, 8, H, W, G>(a, s)
+    if (harm) { if (wm) { if (bg) L(true, true, true); else L(true, true, false); } else { if (bg) L(true, false, true); else L(true, false, false); } }
+    else { if (wm) { if (bg) L(false, true, true); else L(false, true, false); } else { if (bg) L(false, false, true); else L(false, false, false); } }
+#undef L
+}
+
+cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s) {
+    return fp32_tendencies ? launch_step_tt<float>(a, s) : launch_step_tt<double>(a, s);
+}
+
+static inline int grid_for(long n, int threads) {
+    long b = (n + threads - 1) / threads;
+    return (int)std::min<long>(b, 148L * 16);
+}
+
+cudaError_t launch_biharmonic_h(const double* cur, const double* old, double* out, int nx, int ny, int nz,
+                                double Hmix, double rdx, double rdy, double dt, cudaStream_t s) {
+    const long N = (long)nx * ny * nz;
+    k_biharmonic_h<<<grid_for(N, 256), 256, 0, s>>>(cur, old, out, nx, ny, nz, Hmix, rdx, rdy, dt);
+    return cudaGetLastError();
+}
+cudaError_t launch_biharmonic_v(const double* cur, const double* old, double* out, int nx, int ny, int nz,
+                                int rigid, double Vmix, double rdz, double dt, cudaStream_t s) {
+    const long N = (long)nx * ny * nz;
+    k_biharmonic_v<<<grid_for(N, 256), 256, 0, s>>>(cur, old, out, nx, ny, nz, rigid, Vmix, rdz, dt);
+    return cudaGetLastError();
+}
+cudaError_t launch_forcing_background(const StepArgs& a, cudaStream_t s) {
+    const long N = (long)a.nx * a.ny * a.nz;
+    k_forcing_background<<<grid_for(N, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_wavemaker_ab(const StepArgs& a, int do_wm, cudaStream_t s) {
+    const long N = (long)a.nx * a.ny * a.nz;
+    k_wavemaker_ab<<<grid_for(N, 256), 256, 0, s>>>(a, do_wm);
+    return cudaGetLastError();
+}
+cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int nx, int ny, int nz, int rigid,
+                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s) {
+    const long N = (long)nx * ny * nz;
+    k_correct<<<grid_for(N, 256), 256, 0, s>>>(u, v, w, p, nx, ny, nz, rigid, dt, dtw, rdx, rdy, rdz);
+    return cudaGetLastError();
+}
+
+}  // namespace ps3d

@@ -1,0 +1,252 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+Tolerances are the ones the engine is specified against: relative L2 over
+the interior <= 1e-11 for the FP64 path and <= 1e-5 for the mixed path after
+the stated number of steps; single kernels (one pressure solve, one
+projection) are held to 1e-12.
+"""
+import numpy as np
+import pytest
+
+from oracle.binding import Oracle
+from ps3d_b200 import abi
+from ps3d_b200 import configs as cf
+from ps3d_b200.model import Model, PS3DError
+from tests.helpers import (FIELDS, compare_state, load_oracle, random_state, rel, small_params,
+                           smooth_state, upload_from_oracle)
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-11
+TOL_KERNEL = 1e-12
+TOL_MIXED = 1e-5
+
+
+def _pair(p, fields, pfield=None):
+    o = Oracle(p)
+    load_oracle(o, fields, pfield)
+    m = Model(p)
+    upload_from_oracle(m, o)
+    return o, m
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+@pytest.mark.parametrize("shape", [(32, 32, 16), (48, 40, 12)])
+def test_pressure_solver(rigid, shape):
+    p = small_params(*shape, rigid=rigid)
+    o, m = _pair(p, random_state(p, seed=1))
+    o.pressure_solver()
+    m.pressure_solver()
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL_KERNEL, err
+
+
+def test_pressure_solver_divergence_free():
+    p = small_params(64, 32, 16, rigid=True)
+    _, m = _pair(p, random_state(p, seed=2))
+    m.pressure_solver()
+    s = m.download(tendencies=False)
+    u, v, w = s["u"], s["v"], s["w"]
+    div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / p.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / p.dy
+           + (w[2:-2, 2:-2, 2:-2] - w[1:-3, 2:-2, 2:-2]) / p.dz)
+    scale = np.abs(u).max() / p.dx
+    assert np.abs(div).max() < 1e-12 * scale
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+def test_one_step(rigid):
+    p = small_params(32, 32, 16, rigid=rigid)
+    o, m = _pair(p, smooth_state(p))
+    o.integrate(1)
+    m.run(1)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL_KERNEL, err
+    got = m.download()
+    itt, tau, *_ = o.get_time()
+    # tendency stored in the slot of the step that was just taken
+    slot = (tau - 2) % 3
+    for n in ("du", "dv", "dw", "db"):
+        e = rel(got[n][slot], o.field(n, slot + 1))
+        assert e < TOL_KERNEL, (n, e)
+
+
+def test_eddy_200_steps_fp64():
+    """The 64x64x32 eddy case, AB3, 200 steps."""
+    p = cf.eddy_params(64, 64, 32)
+    f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=0)
+    o, m = _pair(p, f)
+    o.integrate(200)
+    m.run(200)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+    assert m.download(tendencies=False)["itt"] == 200
+
+
+def test_periodic_ab2_eps_nonlinear():
+    p = small_params(32, 32, 16, rigid=False, enable_AB_3_order=0, eps_ab=0.01, Kh=1e-2, Kv=1e-3)
+    o, m = _pair(p, smooth_state(p, seed=3))
+    o.integrate(20)
+    m.run(20)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+
+
+def test_linear_model():
+    p = small_params(32, 32, 16, rigid=True, enable_nonlinear=0)
+    o, m = _pair(p, smooth_state(p, seed=4))
+    o.integrate(20)
+    m.run(20)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+def test_biharmonic_stale_halos(rigid):
+    """harmonic + biharmonic_h + biharmonic_v in sequence without halo
+    exchange (integrate.f90:59-78): the generic friction path."""
+    p = small_params(32, 32, 16, rigid=rigid, Kh=1e-2, Kv=1e-3, Ahbi=1e7, Avbi=1e1, Khbi=1e7, Kvbi=1e1)
+    o, m = _pair(p, random_state(p, seed=5, amp=0.05))
+    o.integrate(5)
+    m.run(5)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+
+
+def test_forcing_background_and_wavemaker():
+    p = small_params(32, 32, 16, rigid=False)
+    p.Ah = p.Av = 0.0
+    fr = cf.lee_wave_forcing(p, amp=1e-6, seed=2)
+    fr["u_back"] += 0.02 * cf.halo_fill(np.sin(np.arange(np.prod(cf.empty_field(p).shape))).reshape(cf.empty_field(p).shape))
+    cf.halo_fill(fr["u_back"])
+    fr["b_back"] = cf.halo_fill(1e-4 * np.cos(np.arange(np.prod(cf.empty_field(p).shape))).reshape(cf.empty_field(p).shape))
+    o, m = _pair(p, smooth_state(p, seed=6))
+    from ps3d_b200.abi import Forcing, dptr
+    kind = abi.PS3D_FORCE_BACKGROUND | abi.PS3D_FORCE_WAVEMAKER
+    f = Forcing()
+    f.kind = kind
+    f.omega = fr["omega"]
+    f.w_r, f.w_i, f.u_back, f.b_back = dptr(fr["w_r"]), dptr(fr["w_i"]), dptr(fr["u_back"]), dptr(fr["b_back"])
+    o.set_forcing(f, keep=fr)
+    m.set_forcing(kind, omega=fr["omega"], w_r=fr["w_r"], w_i=fr["w_i"], u_back=fr["u_back"], b_back=fr["b_back"])
+    o.integrate(10)
+    m.run(10)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+
+
+def test_forcing_with_friction_generic_path():
+    p = small_params(32, 32, 16, rigid=True)
+    fr = cf.lee_wave_forcing(p, amp=1e-6, seed=9)
+    o, m = _pair(p, smooth_state(p, seed=8))
+    from ps3d_b200.abi import Forcing, dptr
+    kind = abi.PS3D_FORCE_BACKGROUND | abi.PS3D_FORCE_WAVEMAKER
+    f = Forcing()
+    f.kind = kind
+    f.omega = fr["omega"]
+    f.w_r, f.w_i, f.u_back = dptr(fr["w_r"]), dptr(fr["w_i"]), dptr(fr["u_back"])
+    o.set_forcing(f, keep=fr)
+    m.set_forcing(kind, omega=fr["omega"], w_r=fr["w_r"], w_i=fr["w_i"], u_back=fr["u_back"])
+    o.integrate(8)
+    m.run(8)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+
+
+def test_step_with_caller_time_levels():
+    """ps3d_step is integrate.f90 as called from main.f90: the host rotates."""
+    p = small_params(32, 32, 16)
+    f = smooth_state(p, seed=10)
+    o, m = _pair(p, f)
+    itt, tau, t1, t2 = 0, 3, 2, 1
+    for _ in range(4):
+        o.set_time(itt, tau, t1, t2)
+        o.step()
+        m.integrate(itt, tau, t1, t2)
+        tau, t1, t2 = tau % 3 + 1, t1 % 3 + 1, t2 % 3 + 1
+        itt += 1
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_projection(rigid, mode):
+    p = small_params(32, 32, 16, rigid=rigid)
+    o, m = _pair(p, smooth_state(p, seed=11))
+    if mode == abi.PS3D_PROJ_EXCHANGE:   # needs a stored base point
+        o.project(abi.PS3D_PROJ_BASE_POINT)
+        m.project(abi.PS3D_PROJ_BASE_POINT)
+        rs = random_state(p, seed=12, amp=0.02)
+        load_oracle(o, rs)
+        m.upload(**{n: rs[n] for n in FIELDS})
+    o.project(mode)
+    m.project(mode)
+    if mode in (abi.PS3D_PROJ_NORMAL_MODE, abi.PS3D_PROJ_EXCHANGE):
+        err = compare_state(m, o, names=FIELDS)
+    else:
+        which = abi.PS3D_FIELDS_BASE if mode == abi.PS3D_PROJ_BASE_POINT else abi.PS3D_FIELDS_ZERO
+        got = m.get_fields(which)
+        suffix = "_base" if mode == abi.PS3D_PROJ_BASE_POINT else "0"
+        err = {n: rel(got[n], o.field(n + suffix)) for n in FIELDS if np.abs(o.field(n + suffix)).max() > 0}
+    assert max(err.values()) < TOL_KERNEL, err
+
+
+@pytest.mark.parametrize("time_ave", [False, True])
+def test_opt_balance(time_ave):
+    p = small_params(32, 32, 8, rigid=True, dt=600.0)
+    f = smooth_state(p, seed=13)
+    o, m = _pair(p, f)
+    opt = abi.OptBal(period=5.5 * p.dt, average=3.5 * p.dt, max_itts=3, average_times=2, tol=0.0,
+                     enable_time_ave=int(time_ave), adopt=0)
+    n_o, it_o = o.opt_balance(opt)
+    n_m, it_m = m.diag_opt_balance(opt)
+    assert it_o == it_m == 3
+    assert abs(n_m - n_o) <= 1e-9 * abs(n_o) + 1e-300
+    got = m.get_fields(abi.PS3D_FIELDS_BALANCED)
+    err = {n: rel(got[n], o.field(n + "_bal")) for n in FIELDS if np.abs(o.field(n + "_bal")).max() > 0}
+    assert max(err.values()) < TOL64, err
+    # the model state is restored
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL_KERNEL, err
+
+
+def test_diagnose_and_nonfinite():
+    p = small_params(32, 32, 16)
+    f = smooth_state(p, seed=14)
+    o, m = _pair(p, f)
+    st, ke, pe, um, wm = o.diagnose()
+    ke2, pe2, um2, wm2 = m.diagnose()
+    assert st == 0
+    assert abs(ke2 - ke) <= 1e-13 * ke and abs(pe2 - pe) <= 1e-13 * pe
+    assert um2 == um and wm2 == wm
+    bad = f["b"].copy()
+    bad[5, 5, 5] = np.nan
+    m.upload(b=bad)
+    with pytest.raises(PS3DError) as ei:
+        m.diagnose()
+    assert ei.value.status == abi.PS3D_ERR_NONFINITE
+
+
+def test_mixed_precision_200_steps():
+    p = cf.eddy_params(64, 64, 32, precision=abi.PS3D_MIXED)
+    f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=0)
+    p64 = p.copy()
+    p64.precision = abi.PS3D_FP64
+    o = Oracle(p64)
+    load_oracle(o, f)
+    m = Model(p)
+    upload_from_oracle(m, o)
+    o.integrate(200)
+    m.run(200)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL_MIXED, err
+
+
+def test_bad_params_rejected():
+    p = small_params(33, 32, 16)
+    with pytest.raises(PS3DError) as ei:
+        Model(p)
+    assert ei.value.status == abi.PS3D_ERR_BADPARAM
+    p = small_params(28, 32, 16)   # nx/2 = 14 = 2*7 has a factor 7
+    with pytest.raises(PS3DError):
+        Model(p)
