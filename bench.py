@@ -34,6 +34,12 @@ if ROOT not in sys.path:
 NX, NY, NZ = 256, 256, 128
 WORKLOAD = "jets 256x256x128 rigid lid AB3 Laplacian friction"
 
+
+def set_grid(nx, ny, nz):
+    global NX, NY, NZ, WORKLOAD
+    NX, NY, NZ = nx, ny, nz
+    WORKLOAD = f"jets {nx}x{ny}x{nz} rigid lid AB3 Laplacian friction"
+
 # algorithmic HBM bytes per grid point per launch (SURVEY-style accounting):
 # K1 reads u,v,w,b + 2 AB history slots x 4 fields, writes 4 tendencies + 4 state
 BYTES_PER_POINT = {
@@ -68,7 +74,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -150,26 +156,27 @@ def time_path(precision, steps, warmup, dev, pg):
     f = jets_state(p)
     m = Model(p, device=dev)
     m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+    clocks = ClockSampler(dev)
+    clocks.start()
     m.run(warmup)
     stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     m.profile(True)
-    clocks = ClockSampler(dev)
     barrier(pg, dev)
-    clocks.start()
     ev0.record(stream)
     m.enqueue(steps)
     ev1.record(stream)
     ev1.synchronize()
-    clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
     kern = m.profile_read()
     m.profile(False)
+    m.run(max(0, min(steps, 30)))      # keep the GPU loaded while the clock sampler catches up
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
     barrier(pg, dev)
     ms_max = max_over_ranks(ms, pg, dev)
     state = m.download(tendencies=False)
-    return m, p, ms, ms_max, kern, clk, state
+    return m, p, ms, ms_max, kern, clk, state, m.describe()
 
 
 def e2e_run(precision, steps, dev):
@@ -228,6 +235,91 @@ def cpu_baseline_run(steps, warmup_steps=1, budget_s=60.0):
     return NX * NY * NZ * n / t, cores, n
 
 
+ENS_SIZES = [(32, 32, 16), (64, 64, 32), (128, 64, 32), (128, 128, 64)]
+
+
+def ensemble_run(dev, pg, world, n_members=256, steps=200, seed=3):
+    """Batched ensemble: 256 eddies, sizes drawn by seed from ENS_SIZES,
+    amplitudes U(0.05, 0.2) m/s, mixed precision, `steps` steps, all members
+    in batched launches replayed as CUDA graphs.  Compared with the same
+    members stepped one at a time on the plain FP64 path (timed on one member
+    per size class and summed over the members).  With N ranks each rank runs
+    its own ensemble (weak scaling)."""
+    import torch
+    from ps3d_b200 import abi
+    from ps3d_b200 import configs as cf
+    from ps3d_b200.ensemble import Ensemble
+    from ps3d_b200.model import Model
+    rng = np.random.default_rng(seed)
+    picks = rng.integers(0, len(ENS_SIZES), n_members)
+    amps = rng.uniform(0.05, 0.2, n_members)
+    members = [cf.eddy_params(*ENS_SIZES[k], precision=abi.PS3D_MIXED) for k in picks]
+    fields = {}
+    ens = Ensemble(members, device=dev)
+    for i, (k, a) in enumerate(zip(picks, amps)):
+        key = int(k)
+        if key not in fields:
+            p = members[i]
+            fields[key] = cf.add_noise(p, cf.eddy_fields(p, amp=1.0), "b", rel=1e-3, seed=0)
+        f = fields[key]
+        ens.upload(i, f["u"] * a, f["v"] * a, f["w"] * a, f["b"] * a)
+    ens.integrate(3)
+    info0 = ens.info()
+    stream = torch.cuda.ExternalStream(info0["stream"], device=f"cuda:{dev}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg, dev)
+    e0.record(stream)
+    ens.enqueue(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), pg, dev)
+    launches = ens.info()["launches"] - info0["launches"]
+    pts = sum(int(np.prod(ENS_SIZES[k])) for k in picks)
+    ens.close()
+    # serial plain FP64: one member per size class, same number of steps
+    rate = {}
+    for k in sorted(set(int(x) for x in picks)):
+        p = cf.eddy_params(*ENS_SIZES[k])
+        f = fields[k]
+        m = Model(p, device=dev)
+        m.upload(**{n: f[n] * 0.1 for n in ("u", "v", "w", "b")})
+        m.run(3)
+        st = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st)
+        for _ in range(steps):
+            m.enqueue(1)
+        a1.record(st)
+        a1.synchronize()
+        rate[k] = a0.elapsed_time(a1) / steps   # ms per step, one member
+        m.close()
+    serial_ms = sum(rate[int(k)] * steps for k in picks)
+    return {"members": n_members, "steps": steps, "sizes": [list(s) for s in ENS_SIZES],
+            "members_per_size": [int((picks == k).sum()) for k in range(len(ENS_SIZES))],
+            "batched_value": world * pts * steps / (ms * 1e-3), "batched_ms": ms, "batched_launches": int(launches),
+            "serial_fp64_value": pts * steps / (serial_ms * 1e-3), "serial_fp64_ms_estimated": serial_ms,
+            "batched_over_serial_fp64": serial_ms / ms,
+            "note": "mixed precision batched (CUDA graphs) vs members stepped one at a time on the FP64 path"}
+
+
+def serve_run(dev, n_requests=40, rate_hz=50.0, max_active=8):
+    """Optimal-balance requests: Poisson arrivals at rate_hz (seed 4), sizes
+    drawn from 64x64x32 .. 256x256x64, 5 iterations of 100-step ramps each,
+    admitted by HBM footprint, FP64 and mixed."""
+    from ps3d_b200 import abi
+    from ps3d_b200.serve import Server, poisson_schedule, replay_poisson
+    sched = poisson_schedule(n_requests, rate_hz, seed=4)
+    out = {"requests": n_requests, "rate_hz": rate_hz, "max_active": max_active,
+           "request": "diag_opt_balance, 5 iterations x (100 back + 100 forward steps) + projections"}
+    for name, prec in (("fp64", abi.PS3D_FP64), ("mixed", abi.PS3D_MIXED)):
+        srv = Server(device=dev, max_active=max_active)
+        r = replay_poisson(srv, sched, precision=prec)
+        r["peak_active"] = srv.stats()["peak_active"]
+        srv.close()
+        out[name] = r
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -236,10 +328,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--case", default="both", choices=["both", "fp64", "mixed"],
+                    help="which time-step paths to time (profiling runs use one)")
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=128)
+    ap.add_argument("--ensemble", type=int, default=1, help="also run the batched-ensemble workload")
+    ap.add_argument("--serve", type=int, default=1, help="also run the serving workload")
     args = ap.parse_args()
+    set_grid(args.nx, args.ny, args.nz)
     world, rank, local, pg = dist_setup()
     unit = "grid-point-steps/s"
-    metric = "grid-point-steps/s of the ps3D time step, 256x256x128 jets, mixed FP32/FP64 path (FP64 path beside)"
+    metric = f"grid-point-steps/s of the ps3D time step, {NX}x{NY}x{NZ} jets, mixed FP32/FP64 path (FP64 path beside)"
 
     if args.impl == "reference":
         if rank != 0:
@@ -267,17 +367,6 @@ def main():
     dev = local
     npts = NX * NY * NZ
 
-    m64, p64, ms64, ms64_max, k64, clk64, s64 = time_path(abi.PS3D_FP64, args.steps, args.warmup, dev, pg)
-    m64.close()
-    mmx, pmx, msmx, msmx_max, kmx, clkmx, smx = time_path(abi.PS3D_MIXED, args.steps, args.warmup, dev, pg)
-    mmx.close()
-    v64 = world * npts * args.steps / (ms64_max * 1e-3)
-    vmx = world * npts * args.steps / (msmx_max * 1e-3)
-    rel = {n: cf.rel_l2(cf.interior(smx[n]), cf.interior(s64[n])) for n in ("u", "v", "w", "b", "p")}
-    u, v, w = smx["u"], smx["v"], smx["w"]
-    div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / pmx.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / pmx.dy
-           + (w[2:-2, 2:-2, 2:-2] - w[1:-3, 2:-2, 2:-2]) / pmx.dz)
-
     peak, peak_kind = peaks()
 
     def roof(kern, prec):
@@ -289,35 +378,59 @@ def main():
             bpp = BYTES_PER_POINT[prec].get(k, 0)
             out[k] = {"launches": n, "ms_total": ms, "ms_per_launch": per,
                       "algorithmic_gb_per_launch": bpp * npts / 1e9,
-                      "achieved_gbs": bpp * npts / (per * 1e-3) / 1e9 if bpp else None}
+                      "achieved_gbs": bpp * npts / (per * 1e-3) / 1e9 if bpp else None,
+                      "frac_of_peak": (bpp * npts / (per * 1e-3) / 1e9) / peak if bpp else None}
         return out
 
-    r64, rmx = roof(k64, "fp64"), roof(kmx, "mixed")
-    dom = max(rmx.items(), key=lambda kv: kv[1]["ms_total"])
-    dom_name, dom_v = dom
-    launches = sum(n for _, n in kmx.values())
-
-    line = {"metric": metric, "value": vmx, "unit": unit, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": msmx_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (FP64 state/AB/tridiagonal)",
+    res = {}
+    for case, prec, name in ((("both", "fp64"), abi.PS3D_FP64, "fp64"), (("both", "mixed"), abi.PS3D_MIXED, "mixed")):
+        if args.case not in case:
+            continue
+        m_, p_, ms_, msmax_, k_, clk_, st_, desc_ = time_path(prec, args.steps, args.warmup, dev, pg)
+        m_.close()
+        res[name] = {"p": p_, "ms_max": msmax_, "kern": k_, "clk": clk_, "state": st_, "desc": desc_,
+                     "value": world * npts * args.steps / (msmax_ * 1e-3),
+                     "roof": roof(k_, name)}
+    head = res.get("mixed") or res["fp64"]
+    hname = "mixed" if "mixed" in res else "fp64"
+    dom_name, dom_v = max(head["roof"].items(), key=lambda kv: kv[1]["ms_total"])
+    launches = sum(n for _, n in head["kern"].values())
+    line = {"metric": metric, "value": head["value"], "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_max"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (FP64 state/AB/tridiagonal)" if hname == "mixed" else "f64",
             "data": "synthetic (seeded jets + 1e-3 b noise)",
             "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (state ~1.4 GB)"},
-            "fp64": {"value": v64, "ms_per_step": ms64_max / args.steps, "kernels": r64},
-            "mixed_over_fp64": vmx / v64,
-            "rel_l2_mixed_vs_fp64": rel, "max_div_mixed": float(np.abs(div).max()),
-            "kernels": rmx,
+                       "path": hname, "kernel_config": head["desc"],
+                       "l2": "inputs larger than L2 (state > 1 GB)" if npts >= 2 ** 23 else "small case"},
+            "kernels": head["roof"],
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_v["achieved_gbs"], "peak": peak,
                          "unit": "GB/s", "frac": (dom_v["achieved_gbs"] or 0) / peak, "traffic": None,
                          "peak_kind": peak_kind},
-            "gpu_launches": int(launches),
-            "clocks": clkmx, "clocks_fp64": clk64}
+            "gpu_launches": int(launches), "clocks": head["clk"]}
+    if "fp64" in res:
+        r64 = res["fp64"]
+        line["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms_max"] / args.steps, "kernels": r64["roof"],
+                        "kernel_config": r64["desc"], "clocks": r64["clk"]}
+    if "fp64" in res and "mixed" in res:
+        s64, smx, pmx = res["fp64"]["state"], res["mixed"]["state"], res["mixed"]["p"]
+        line["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+        line["rel_l2_mixed_vs_fp64"] = {n: cf.rel_l2(cf.interior(smx[n]), cf.interior(s64[n]))
+                                        for n in ("u", "v", "w", "b", "p")}
+        u, v, w = smx["u"], smx["v"], smx["w"]
+        div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / pmx.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / pmx.dy
+               + (w[2:-2, 2:-2, 2:-2] - w[1:-3, 2:-2, 2:-2]) / pmx.dz)
+        line["max_div_mixed"] = float(np.abs(div).max())
     if not args.no_e2e:
-        t, h2d, d2h, _ = e2e_run(abi.PS3D_MIXED, args.steps, dev)
+        t, h2d, d2h, _ = e2e_run(abi.PS3D_MIXED if hname == "mixed" else abi.PS3D_FP64, args.steps, dev)
         t = max_over_ranks(t, pg, dev)
         line["e2e"] = {"value": world * npts * args.steps / t, "unit": unit, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h,
                        "path": "public C ABI: upload, ps3d_step per step, diagnose every 10 steps, download"}
+    if args.ensemble:
+        line["ensemble"] = ensemble_run(dev, pg, world)
+    if args.serve:
+        line["serving"] = serve_run(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         val, cores, n = cpu_baseline_run(3, warmup_steps=1, budget_s=30.0)
         line["cpu_baseline"] = {"value": val, "unit": unit, "cores": cores, "kind": "port",

@@ -214,7 +214,53 @@ PS3D_API int ps3d_enqueue(ps3d_ctx* ctx, int nsteps);
 #define PS3D_K_OTHER    5   /* friction stages, forcing, projections, ...   */
 #define PS3D_K_COUNT    6
 PS3D_API int ps3d_profile(ps3d_ctx* ctx, int enable);
+/* One-line description of the context's kernel configuration (grid,
+ * precision, plane cluster shape, FFT stages, autotuner choice).          */
+PS3D_API int ps3d_describe(ps3d_ctx* ctx, char* buf, int len);
 PS3D_API int ps3d_profile_read(ps3d_ctx* ctx, double* ms, long long* launches);
+
+/* ---- batched ensembles (no counterpart in the reference) -----------------
+ * n independent grids on one GPU.  Members with identical ps3d_params share
+ * every kernel launch (the member index is part of the launch grid); all
+ * members advance together with the main-loop semantics of ps3d_integrate,
+ * and for constant parameters three steps of every member are replayed as
+ * one CUDA graph.  Upload/download use the halo layout of each member.     */
+typedef struct ps3d_ensemble ps3d_ensemble;
+PS3D_API int ps3d_ensemble_create(const ps3d_params* members, int n, int device, ps3d_ensemble** out);
+PS3D_API int ps3d_ensemble_destroy(ps3d_ensemble* e);
+PS3D_API int ps3d_ensemble_upload(ps3d_ensemble* e, int member, const double* u, const double* v,
+                                  const double* w, const double* b);
+PS3D_API int ps3d_ensemble_download(ps3d_ensemble* e, int member, double* u, double* v, double* w,
+                                    double* b, double* p);
+PS3D_API int ps3d_ensemble_integrate(ps3d_ensemble* e, int nsteps);   /* waits for completion */
+PS3D_API int ps3d_ensemble_enqueue(ps3d_ensemble* e, int nsteps);     /* queues only         */
+PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launches, void** stream);
+
+/* ---- serving loop for optimal-balance requests (no counterpart in the
+ * reference) ---------------------------------------------------------------
+ * Requests (one diag_opt_balance each, on their own grid and state) are
+ * admitted in arrival order as execution slots and device memory free up:
+ * the sum of the admitted requests' footprints (ps3d_server_footprint) stays
+ * within hbm_budget_bytes (0: 80% of free memory).  Each admitted request
+ * runs on its own CUDA stream, so concurrent requests overlap on the GPU;
+ * a request's result does not depend on what else is running.           */
+typedef struct ps3d_server ps3d_server;
+PS3D_API int ps3d_server_create(int device, size_t hbm_budget_bytes, int max_active, ps3d_server** out);
+PS3D_API int ps3d_server_destroy(ps3d_server* s);   /* cancels what is still queued or running */
+/* copies the halo-layout inputs; PS3D_ERR_OOM if the request can never fit */
+PS3D_API int ps3d_server_submit(ps3d_server* s, const ps3d_params* prm, const ps3d_optbal* opt,
+                                const double* u, const double* v, const double* w, const double* b,
+                                long long* ticket);
+/* waits at most timeout_ms (PS3D_ERR_TIMEOUT otherwise); returns the request's
+ * status, copies u_bal..b_bal (NULL to skip) and fills res[6] = {status,
+ * final norm, iterations, latency ms, queue ms, run ms}.  A finished request
+ * is handed out once.                                                      */
+PS3D_API int ps3d_server_wait(ps3d_server* s, long long ticket, int timeout_ms,
+                              double* u_bal, double* v_bal, double* w_bal, double* b_bal, double* res);
+PS3D_API int ps3d_server_cancel(ps3d_server* s, long long ticket);
+/* stats[6] = {active, queued, bytes in use, peak bytes, peak active, budget} */
+PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats);
+PS3D_API long long ps3d_server_footprint(const ps3d_params* prm);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,7 @@ def lib():
         L.ps3d_oracle_integrate.argtypes = [vp, C.c_int]
         L.ps3d_oracle_pressure_solver.argtypes = [vp]
         L.ps3d_oracle_project.argtypes = [vp, C.c_int]
+        L.ps3d_oracle_forward_transform.argtypes = [vp]
         L.ps3d_oracle_opt_balance.argtypes = [vp, C.POINTER(OptBal), dp, ip]
         L.ps3d_oracle_diagnose.restype = C.c_int
         L.ps3d_oracle_diagnose.argtypes = [vp, dp, dp, dp, dp]
@@ -144,6 +145,10 @@ class Oracle:
 
     def project(self, mode):
         self.L.ps3d_oracle_project(self.h, mode)
+
+    def forward_transform(self):
+        """forward_transform of the state; read the result with spectral(1..4)."""
+        self.L.ps3d_oracle_forward_transform(self.h)
 
     def opt_balance(self, opt: OptBal):
         norm, iters = C.c_double(), C.c_int()

@@ -1254,6 +1254,13 @@ void ps3d_oracle_integrate(void* h, int nsteps) {
 }
 void ps3d_oracle_pressure_solver(void* h) { pressure_solver(*static_cast<Model*>(h)); }
 void ps3d_oracle_project(void* h, int mode) { project(*static_cast<Model*>(h), mode); }
+/* forward_transform of the current state into US..BS (diag_balance.f90:421-438) */
+void ps3d_oracle_forward_transform(void* h) {
+    Model& M = *static_cast<Model*>(h);
+    const long n = M.nspec();
+    M.US.resize(n); M.VS.resize(n); M.WS.resize(n); M.BS.resize(n);
+    forward_transform(M, M.u.data(), M.v.data(), M.w.data(), M.b.data(), M.US.data(), M.VS.data(), M.WS.data(), M.BS.data());
+}
 void ps3d_oracle_opt_balance(void* h, const ps3d_optbal* o, double* norm, int* iters) {
     diag_opt_balance(*static_cast<Model*>(h), *o, norm, iters);
 }

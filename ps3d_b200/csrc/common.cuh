@@ -47,6 +47,7 @@ struct FFTPlan {
     int n;                    // transform length
     int nst;                  // number of stages
     int r[kMaxStages];        // radices in DIT stage order (product = n)
+    int lp[kMaxStages];       // product of the radices before each stage
     const double2* tw;        // exp(-2 pi i t / n), t = 0..n-1
     const float2* twf;        // the same, rounded to FP32
     const int* pos;           // digit-reversal: natural index t -> position

@@ -1,6 +1,8 @@
 // ctx.h — the device context of one grid (host-side bookkeeping).
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
+#include <string>
 #include <vector>
 #include "engine.h"
 
@@ -50,7 +52,7 @@ struct DevPlan {
     FFTPlan plan{};
     int n = 0;
     DevBuf dtw, dtwf, dpos, dipos;
-    cudaError_t build(int len);
+    cudaError_t build(int len, int policy = 0);
 };
 
 bool fft_length_ok(int n);
@@ -64,7 +66,18 @@ struct Ctx {
     long N = 0, M2 = 0, M = 0;
     bool rigid = true, mixed = false;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;
     size_t tsize = 8;
+    int batch = 1;            // instances of this grid stepped together (ensembles)
+    // CUDA graph of three consecutive steps (tau and the state buffers both
+    // cycle with period 3), replayed by advance() for constant parameters
+    cudaGraphExec_t gexec = nullptr;
+    int g_tau = -1, g_cur = -1;
+    long g_version = -1, version = 0;
+    long long g_launches = 0;
+    bool use_graphs = true;
+    std::atomic<int>* cancel_flag = nullptr;   // serving: set to abandon a running request
+    bool cancelled() const { return cancel_flag && cancel_flag->load(std::memory_order_relaxed) != 0; }
     // state
     DevBuf state[4][3];
     int cur[4] = {0, 0, 0, 0};
@@ -76,7 +89,10 @@ struct Ctx {
     DevBuf bal[4], base[4], zero[4], save[4], ave[4], save2[4];
     DevBuf saved_p, saved_tend[4];
     // tables
-    DevPlan plx, ply, plz;
+    DevPlan plx, ply, plz;      // radix-16/8 schedules
+    DevPlan plx4, ply4;         // radix-4 schedules (autotuner alternative)
+    int kchunk = 8;             // z levels per block of the step kernel
+    std::string tuned;          // description of the autotuned choice
     DevBuf twx;
     DevBuf t_kx, t_ky, t_kz, t_hkx, t_hky, t_hkz, t_ex, t_ey, t_ez, t_px, t_py, t_pz, t_sz, t_cz, t_hkz_ds;
     DevBuf m_phi, m_psi, m_psib;
@@ -106,7 +122,8 @@ struct Ctx {
     DevBuf red_partials, red_out, staging;
 
     ~Ctx() {
-        if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (stream) { cudaStreamSynchronize(stream); if (own_stream) cudaStreamDestroy(stream); }
         for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
     }
 
@@ -122,7 +139,12 @@ struct Ctx {
         return PS3D_OK;
     }
 
-    int init(const ps3d_params& prm, int dev);
+    int init(const ps3d_params& prm, int dev, int nbatch = 1, cudaStream_t use_stream = nullptr);
+    int autotune();
+    int advance(int nsteps, bool allow_graph);
+    bool graphable() const;
+    int capture_graph();
+    void invalidate_graph() { ++version; }
     int step(int itt, int tau, int taum1, int taum2);
     int poisson_once(double* out, double beta);
     int pressure_solve();
@@ -145,6 +167,7 @@ struct Ctx {
     void gather(const double* h, double* dst) const;
     void scatter(const double* src, double* h, int kind) const;
     int upload_field(double* dev, const double* h);
+    double* member_field(int f, int m) { return field(f) + (size_t)m * N; }
     int download_field(const double* dev, double* h, int kind);
     int upload_tend(int f, const double* h);
     int download_tend(int f, double* h);

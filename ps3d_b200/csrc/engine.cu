@@ -70,9 +70,15 @@ int Ctx::prof_read(double* ms, long long* count) {
 // ---------------------------------------------------------------------------
 // FFT plans (host construction)
 // ---------------------------------------------------------------------------
-static std::vector<int> radices_of(int n) {
+// Radix schedule of one transform length.  policy 0 prefers radix 16 and 8
+// (two register passes for 128 and 256 points), policy 1 stays at radix 4.
+static std::vector<int> radices_of(int n, int policy = 0) {
     std::vector<int> r;
     int m = n;
+    if (policy == 0) {
+        while (m % 16 == 0) { r.push_back(16); m /= 16; }
+        if (m % 8 == 0) { r.push_back(8); m /= 8; }
+    }
     while (m % 4 == 0) { r.push_back(4); m /= 4; }
     while (m % 2 == 0) { r.push_back(2); m /= 2; }
     while (m % 3 == 0) { r.push_back(3); m /= 3; }
@@ -105,9 +111,9 @@ static int pos_of(int t, const std::vector<int>& r, int m, int n) {
     return (t % R) * (n / R) + pos_of(t / R, r, m - 1, n / R);
 }
 
-cudaError_t DevPlan::build(int len) {
+cudaError_t DevPlan::build(int len, int policy) {
     n = len;
-    std::vector<int> r = n == 1 ? std::vector<int>{} : radices_of(n);
+    std::vector<int> r = n == 1 ? std::vector<int>{} : radices_of(n, policy);
     if (n != 1 && r.empty()) return cudaErrorInvalidValue;
     if ((int)r.size() > kMaxStages) return cudaErrorInvalidValue;
     std::vector<double2> tw(n);
@@ -130,7 +136,12 @@ cudaError_t DevPlan::build(int len) {
     if ((e = cudaMemcpy(dipos.p, ipos.data(), n * sizeof(int), cudaMemcpyHostToDevice))) return e;
     plan.n = n;
     plan.nst = (int)r.size();
-    for (int s = 0; s < kMaxStages; ++s) plan.r[s] = s < (int)r.size() ? r[s] : 1;
+    int acc = 1;
+    for (int s = 0; s < kMaxStages; ++s) {
+        plan.r[s] = s < (int)r.size() ? r[s] : 1;
+        plan.lp[s] = acc;
+        acc *= plan.r[s];
+    }
     plan.tw = (const double2*)dtw.p;
     plan.twf = (const float2*)dtwf.p;
     plan.pos = (const int*)dpos.p;
@@ -138,7 +149,30 @@ cudaError_t DevPlan::build(int len) {
     return cudaSuccess;
 }
 
-// Choose the cluster shape of the plane kernels for one element size.
+// Feasible cluster shapes of the plane kernels for one element size.
+static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const PlaneArgs& base) {
+    std::vector<PlaneArgs> out;
+    const int nxh = nx / 2 + 1, n2 = nx / 2;
+    for (int C : {1, 2, 4, 8, 16}) {
+        if (ny % C) continue;
+        const int R = ny / C;
+        const int cpc = (nxh + C - 1) / C;
+        if ((C - 1) * cpc >= nxh) continue;
+        for (int rc : {4, 8, 16, 32}) {
+            if (rc > R && rc != 4) continue;
+            const int rcc = std::min(rc, R);
+            const int ldr = rcc | 1, ldc = cpc | 1;
+            const size_t sm = ((size_t)ny * ldc + (size_t)n2 * ldr) * es;
+            if (sm > 225 * 1024) continue;
+            PlaneArgs a = base;
+            a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rcc; a.ldr = ldr; a.ldc = ldc;
+            out.push_back(a);
+        }
+    }
+    return out;
+}
+
+// Default cluster shape of the plane kernels for one element size.
 static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
     const int nxh = nx / 2 + 1, n2 = nx / 2;
     for (int pass = 0; pass < 2; ++pass) {
@@ -165,9 +199,10 @@ static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
 static double hat_ksqr(double k, double d) { return 2.0 * (1.0 - std::cos(k * d)) / (d * d); }
 static double hat_epm(double k, double d) { return 0.5 * (1 + std::cos(k * d)); }
 
-int Ctx::init(const ps3d_params& prm, int dev) {
+int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stream) {
     P = prm;
     device = dev;
+    batch = nbatch < 1 ? 1 : nbatch;
     nx = P.nx; ny = P.ny; nz = P.nz; nxh = nx / 2 + 1;
     N = (long)nx * ny * nz;
     M2 = (long)nxh * ny;
@@ -179,20 +214,23 @@ int Ctx::init(const ps3d_params& prm, int dev) {
     if (P.precision != PS3D_FP64 && P.precision != PS3D_MIXED) return PS3D_ERR_BADPARAM;
     if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0)) return PS3D_ERR_BADPARAM;
     if (cudaSetDevice(dev) != cudaSuccess) return PS3D_ERR_CUDA;
-    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    if (use_stream) { stream = use_stream; own_stream = false; }
+    else CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    const long NB = N * batch;
     CK(plane_setup(false));
     CK(plane_setup(true));
     // state: 3 buffers per field (fused path ping-pongs two, the generic path needs three)
     for (int f = 0; f < 4; ++f)
-        for (int q = 0; q < 3; ++q) { CK(state[f][q].alloc(N * sizeof(double))); CK(cudaMemset(state[f][q].p, 0, N * sizeof(double))); }
+        for (int q = 0; q < 3; ++q) { CK(state[f][q].alloc(NB * sizeof(double))); CK(cudaMemset(state[f][q].p, 0, NB * sizeof(double))); }
     for (int f = 0; f < 4; ++f) cur[f] = 0;
-    CK(p.alloc(N * sizeof(double))); CK(cudaMemset(p.p, 0, N * sizeof(double)));
+    CK(p.alloc(NB * sizeof(double))); CK(cudaMemset(p.p, 0, NB * sizeof(double)));
     tsize = mixed ? sizeof(float) : sizeof(double);
-    for (int f = 0; f < 4; ++f) { CK(tend[f].alloc(3 * N * tsize)); CK(cudaMemset(tend[f].p, 0, 3 * N * tsize)); }
-    CK(FS.alloc(M * (mixed ? sizeof(float2) : sizeof(double2))));
-    if (mixed) CK(p2.alloc(N * sizeof(double)));
+    for (int f = 0; f < 4; ++f) { CK(tend[f].alloc(3 * NB * tsize)); CK(cudaMemset(tend[f].p, 0, 3 * NB * tsize)); }
+    CK(FS.alloc(M * batch * (mixed ? sizeof(float2) : sizeof(double2))));
+    if (mixed) CK(p2.alloc(NB * sizeof(double)));
     // plans and tables
-    CK(plx.build(nx / 2)); CK(ply.build(ny)); CK(plz.build(rigid ? 1 : nz));
+    CK(plx.build(nx / 2, 0)); CK(ply.build(ny, 0)); CK(plz.build(rigid ? 1 : nz, 0));
+    CK(plx4.build(nx / 2, 1)); CK(ply4.build(ny, 1));
     {
         std::vector<double2> tw(nxh);
         for (int t = 0; t < nxh; ++t) tw[t] = twiddle_fwd(t, nx);
@@ -264,15 +302,17 @@ int Ctx::init(const ps3d_params& prm, int dev) {
     base.nx = nx; base.ny = ny; base.nz = nz; base.nxh = nxh;
     base.px = plx.plan; base.py = ply.plan; base.twx = (const double2*)twx.p;
     base.rdx = 1.0 / P.dx; base.rdy = 1.0 / P.dy; base.rdz = 1.0 / P.dz;
+    base.batch = 1; base.sN = N; base.sM = M;
     pa64 = base; pa32 = base;
     if (!choose_plane_config(nx, ny, sizeof(double2), pa64)) return PS3D_ERR_BADPARAM;
     if (!choose_plane_config(nx, ny, sizeof(float2), pa32)) return PS3D_ERR_BADPARAM;
+    kchunk = nz <= 16 ? nz : 8;
     // reductions
     nred = 148 * 4;
     CK(red_partials.alloc((size_t)nred * 5 * sizeof(double)));
     CK(red_out.alloc(256));   // DiagOut at 0, norm results (4 doubles) at byte 64
     CK(cudaStreamSynchronize(stream));
-    return PS3D_OK;
+    return autotune();
 }
 
 cudaError_t Ctx::ensure_spectral4() {
@@ -313,6 +353,7 @@ DevBuf* Ctx::fieldset(int which) {
 int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
     StepArgs a{};
     a.nx = nx; a.ny = ny; a.nz = nz;
+    a.batch = batch; a.sN = N; a.kchunk = kchunk;
     a.rigid = rigid; a.nonlinear = P.enable_nonlinear != 0;
     a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz;
     a.dt = P.dt; a.dtw = P.dt / P.dsqr;
@@ -324,9 +365,9 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
     else { a.ab0 = 23.0 / 12.0; a.ab1 = -16.0 / 12.0; a.ab2 = 5.0 / 12.0; }
     const int s0 = tau_ - 1, s1 = taum1_ - 1, s2 = taum2_ - 1;
     for (int f = 0; f < 4; ++f) {
-        a.t0[f] = (char*)tend[f].p + (size_t)s0 * N * tsize;
-        a.t1[f] = (const char*)tend[f].p + (size_t)s1 * N * tsize;
-        a.t2[f] = (const char*)tend[f].p + (size_t)s2 * N * tsize;
+        a.t0[f] = (char*)tend[f].p + (size_t)s0 * batch * N * tsize;
+        a.t1[f] = (const char*)tend[f].p + (size_t)s1 * batch * N * tsize;
+        a.t2[f] = (const char*)tend[f].p + (size_t)s2 * batch * N * tsize;
     }
     a.u = field(0); a.v = field(1); a.w = field(2); a.b = field(3);
     const bool bg = (fkind & PS3D_FORCE_BACKGROUND) != 0;
@@ -350,7 +391,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         LAUNCH(PS3D_K_STEP, launch_step(a, mixed, stream));
         for (int f = 0; f < 4; ++f) cur[f] = nxt[f];
     } else {
-        if (mixed) return PS3D_ERR_UNSUPPORTED;   // generic path keeps FP64 tendencies
+        if (mixed || batch > 1) return PS3D_ERR_UNSUPPORTED;   // generic path: FP64 tendencies, one grid
         int old[4], B[4], Cb[4];
         for (int f = 0; f < 4; ++f) { old[f] = cur[f]; B[f] = (cur[f] + 1) % 3; Cb[f] = (cur[f] + 2) % 3; }
         a.uo = (double*)state[0][B[0]].p; a.vo = (double*)state[1][B[1]].p;
@@ -388,8 +429,11 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         fa.uo = (double*)state[0][fin[0]].p; fa.vo = (double*)state[1][fin[1]].p;
         fa.wo = (double*)state[2][fin[2]].p; fa.bo = (double*)state[3][fin[3]].p;
         if (bg) {
-            fa.ub = (const double*)ub.p; fa.bb = (const double*)bb.p;
-            LAUNCH(PS3D_K_OTHER, launch_forcing_background(fa, stream));
+            StepArgs ga = fa;   // ga.u..b: friction-updated; ga.uo..bo: start of step (stale halos)
+            ga.ub = (const double*)ub.p; ga.bb = (const double*)bb.p;
+            ga.uo = (double*)state[0][old[0]].p; ga.vo = (double*)state[1][old[1]].p;
+            ga.wo = (double*)state[2][old[2]].p; ga.bo = (double*)state[3][old[3]].p;
+            LAUNCH(PS3D_K_OTHER, launch_forcing_background(ga, stream));
         }
         if (cb) {
             ps3d_device_view view{};
@@ -411,11 +455,235 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
 }
 
 // ---------------------------------------------------------------------------
+// Autotuner: time the feasible plane-kernel shapes (cluster size x row chunk
+// x radix schedule) and the step kernel's z chunk on this grid, with CUDA
+// events, and keep the fastest.  Runs at creation on the zero state (every
+// output is zero, nothing observable changes); results are cached per
+// (grid, precision, batch, device) for the process and in a text file
+// ($PS3D_TUNE_CACHE, default ~/.cache/ps3d_b200_tune.txt).
+// ---------------------------------------------------------------------------
+static std::map<std::string, std::string>& tune_cache() {
+    static std::map<std::string, std::string> m;
+    static bool loaded = false;
+    if (!loaded) {
+        loaded = true;
+        const char* path = std::getenv("PS3D_TUNE_CACHE");
+        std::string f = path ? path : (std::string(std::getenv("HOME") ? std::getenv("HOME") : "/tmp") + "/.cache/ps3d_b200_tune.txt");
+        if (FILE* fp = std::fopen(f.c_str(), "r")) {
+            char k[256], v[256];
+            while (std::fscanf(fp, "%255s %255s", k, v) == 2) m[k] = v;
+            std::fclose(fp);
+        }
+    }
+    return m;
+}
+static void tune_cache_store(const std::string& k, const std::string& v) {
+    tune_cache()[k] = v;
+    const char* path = std::getenv("PS3D_TUNE_CACHE");
+    std::string dir = std::string(std::getenv("HOME") ? std::getenv("HOME") : "/tmp") + "/.cache";
+    std::string f = path ? path : dir + "/ps3d_b200_tune.txt";
+    if (!path) { std::string cmd = dir; (void)cmd; }
+    if (FILE* fp = std::fopen(f.c_str(), "a")) {
+        std::fprintf(fp, "%s %s\n", k.c_str(), v.c_str());
+        std::fclose(fp);
+    }
+}
+
+int Ctx::autotune() {
+    const char* env = std::getenv("PS3D_AUTOTUNE");
+    if (env && env[0] == '0') return PS3D_OK;
+    if ((long)N * batch < (1L << 18) && !(env && env[0] == '2')) return PS3D_OK;   // small grids: defaults
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev));
+    char key[256];
+    std::snprintf(key, sizeof key, "%s|%dx%dx%d|p%d|r%d|b%d", prop.name, nx, ny, nz, (int)mixed, (int)rigid, batch);
+    for (char* c = key; *c; ++c) if (*c == ' ') *c = '_';
+    const bool f32 = mixed;
+    PlaneArgs& pa = f32 ? pa32 : pa64;
+    auto apply = [&](int C, int rc, int pol, int kc) -> bool {
+        for (const PlaneArgs& c : plane_candidates(nx, ny, f32 ? sizeof(float2) : sizeof(double2), pa)) {
+            if (c.C != C || c.row_chunk != rc) continue;
+            pa = c;
+            pa.px = pol == 0 ? plx.plan : plx4.plan;
+            pa.py = pol == 0 ? ply.plan : ply4.plan;
+            kchunk = kc;
+            return true;
+        }
+        return false;
+    };
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+        int C, rc, pol, kc;
+        if (std::sscanf(it->second.c_str(), "C%d,rc%d,pol%d,kc%d", &C, &rc, &pol, &kc) == 4 && apply(C, rc, pol, kc)) {
+            tuned = std::string("cached:") + it->second;
+            return PS3D_OK;
+        }
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto timeit = [&](auto&& fn) -> float {
+        float best = 1e30f;
+        if (fn() != PS3D_OK) return best;
+        if (cudaStreamSynchronize(stream) != cudaSuccess) { cudaGetLastError(); return best; }
+        for (int r = 0; r < 3; ++r) {
+            cudaEventRecord(e0, stream);
+            if (fn() != PS3D_OK) return 1e30f;
+            cudaEventRecord(e1, stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); return 1e30f; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            best = std::min(best, ms);
+        }
+        return best;
+    };
+    // plane kernels
+    float best = 1e30f;
+    PlaneArgs bestpa = pa;
+    int bestpol = 0;
+    for (const PlaneArgs& cand : plane_candidates(nx, ny, f32 ? sizeof(float2) : sizeof(double2), pa)) {
+        for (int pol = 0; pol < 2; ++pol) {
+            PlaneArgs a = cand;
+            a.px = pol == 0 ? plx.plan : plx4.plan;
+            a.py = pol == 0 ? ply.plan : ply4.plan;
+            a.batch = batch;
+            if (plane_max_clusters(a, f32, true) < 1 || plane_max_clusters(a, f32, false) < 1) continue;
+            const float t = timeit([&]() -> int {
+                PlaneArgs f = a;
+                f.mode = 0; f.u = field(0); f.v = field(1); f.w = field(2);
+                f.rdt = 1.0 / P.dt; f.scale = P.dx * P.dy; f.spec = FS.p;
+                CK(launch_plane_fwd(f, f32, stream));
+                PlaneArgs b = a;
+                b.spec = FS.p; b.out = (double*)p.p; b.beta = 0.0; b.scale = 1.0;
+                CK(launch_plane_inv(b, f32, stream));
+                return PS3D_OK;
+            });
+            if (t < best) { best = t; bestpa = a; bestpol = pol; }
+        }
+    }
+    bestpa.batch = 1;
+    pa = bestpa;
+    // step kernel z chunk
+    float bestk = 1e30f;
+    int bestkc = kchunk;
+    for (int kc : {4, 8, 16, 32}) {
+        if (kc > nz) continue;
+        kchunk = kc;
+        const float t = timeit([&]() -> int {
+            StepArgs a{};
+            a.nx = nx; a.ny = ny; a.nz = nz; a.batch = batch; a.sN = N; a.kchunk = kc;
+            a.rigid = rigid; a.nonlinear = 1;
+            a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz; a.dt = P.dt; a.dtw = P.dt / P.dsqr;
+            a.Ro = P.Ro; a.dsqr = P.dsqr; a.N0sq = P.N0 * P.N0; a.f0 = P.f0;
+            a.Ah = P.Ah; a.Av = P.Av; a.Kh = P.Kh; a.Kv = P.Kv;
+            a.harm_uvw = (P.Ah > 0. || P.Av > 0.); a.harm_b = (P.Kh > 0. || P.Kv > 0.);
+            a.ab0 = 23.0 / 12.0; a.ab1 = -16.0 / 12.0; a.ab2 = 5.0 / 12.0; a.do_ab = 1;
+            a.u = field(0); a.v = field(1); a.w = field(2); a.b = field(3);
+            for (int f = 0; f < 4; ++f) {
+                a.t0[f] = (char*)tend[f].p + (size_t)2 * batch * N * tsize;
+                a.t1[f] = (const char*)tend[f].p + (size_t)1 * batch * N * tsize;
+                a.t2[f] = (const char*)tend[f].p;
+            }
+            a.uo = (double*)state[0][(cur[0] + 1) % 3].p; a.vo = (double*)state[1][(cur[1] + 1) % 3].p;
+            a.wo = (double*)state[2][(cur[2] + 1) % 3].p; a.bo = (double*)state[3][(cur[3] + 1) % 3].p;
+            CK(launch_step(a, mixed, stream));
+            return PS3D_OK;
+        });
+        if (t < bestk) { bestk = t; bestkc = kc; }
+    }
+    kchunk = bestkc;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaStreamSynchronize(stream));
+    char val[128];
+    std::snprintf(val, sizeof val, "C%d,rc%d,pol%d,kc%d", pa.C, pa.row_chunk, bestpol, kchunk);
+    tuned = val;
+    tune_cache_store(key, val);
+    return PS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// main-loop advance with CUDA-graph replay.  The fused step's launch sequence
+// depends on (tau, state buffer) which both cycle with period 3, and on the
+// AB weights, which are constant from itt = 2 on.  With constant parameters
+// (no wavemaker clock, no host callback) three steps are captured once and
+// the graph is replayed.
+// ---------------------------------------------------------------------------
+bool Ctx::graphable() const {
+    const bool bih = P.Ahbi > 0. || P.Avbi > 0. || P.Khbi > 0. || P.Kvbi > 0.;
+    const bool harm = P.Ah > 0. || P.Av > 0. || P.Kh > 0. || P.Kv > 0.;
+    const bool bg = (fkind & PS3D_FORCE_BACKGROUND) != 0;
+    if (!use_graphs || prof) return false;
+    if (fkind & (PS3D_FORCE_WAVEMAKER | PS3D_FORCE_CALLBACK)) return false;
+    if (bih || (bg && harm)) return false;
+    return cur[0] == cur[1] && cur[1] == cur[2] && cur[2] == cur[3];
+}
+
+int Ctx::capture_graph() {
+    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+    const int itt0 = itt, tau0 = tau, t10 = taum1, t20 = taum2;
+    int cur0[4];
+    for (int f = 0; f < 4; ++f) cur0[f] = cur[f];
+    const long l0 = launches;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int rc = PS3D_OK;
+    for (int s = 0; s < 3 && !rc; ++s) {
+        rc = step(itt, tau, taum1, taum2);
+        rotate();
+        ++itt;
+    }
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    itt = itt0; tau = tau0; taum1 = t10; taum2 = t20;
+    for (int f = 0; f < 4; ++f) cur[f] = cur0[f];
+    g_launches = launches - l0;
+    launches = l0;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    CK(e);
+    e = cudaGraphInstantiate(&gexec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    g_tau = tau; g_cur = cur[0]; g_version = version;
+    return PS3D_OK;
+}
+
+int Ctx::advance(int nsteps, bool allow_graph) {
+    while (nsteps > 0) {
+        if (allow_graph && nsteps >= 3 && itt >= 2 && graphable()) {
+            if (!gexec || g_tau != tau || g_cur != cur[0] || g_version != version) {
+                int rc = capture_graph();
+                if (rc) return rc;
+            }
+            CK(cudaGraphLaunch(gexec, stream));
+            for (int s = 0; s < 3; ++s) {
+                rotate();
+                for (int f = 0; f < 4; ++f) cur[f] = (cur[f] + 1) % 3;
+                time = time + P.dt;
+                ++itt;
+            }
+            launches += g_launches;
+            nsteps -= 3;
+            continue;
+        }
+        int rc = step(itt, tau, taum1, taum2);
+        if (rc) return rc;
+        rotate();
+        time = time + P.dt;
+        ++itt;
+        --nsteps;
+    }
+    return PS3D_OK;
+}
+
+// ---------------------------------------------------------------------------
 // pressure_solver (pressure_solver.f90:2-120)
 // ---------------------------------------------------------------------------
 int Ctx::poisson_once(double* out, double beta) {
     const bool f32 = mixed;
     PlaneArgs a = f32 ? pa32 : pa64;
+    a.batch = batch;
     a.mode = 0;
     a.u = field(0); a.v = field(1); a.w = field(2);
     a.rdt = 1.0 / P.dt;
@@ -424,6 +692,7 @@ int Ctx::poisson_once(double* out, double beta) {
     LAUNCH(PS3D_K_FFT_FWD, launch_plane_fwd(a, f32, stream));
     ColumnArgs c{};
     c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = FS.p;
+    c.batch = batch; c.sM = M;
     c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p; c.hkz = (const double*)t_hkz_ds.p;
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
@@ -434,13 +703,14 @@ int Ctx::poisson_once(double* out, double beta) {
         LAUNCH(PS3D_K_VSOLVE, launch_zsolve(c, f32, stream));
     }
     PlaneArgs b = f32 ? pa32 : pa64;
+    b.batch = batch;
     b.spec = FS.p;
     b.out = out;
     b.beta = beta;
     b.scale = rigid ? 1.0 / (P.Lx * P.Ly) : 1.0 / (P.Lx * P.Ly * P.Lz);
     LAUNCH(PS3D_K_FFT_INV, launch_plane_inv(b, f32, stream));
     LAUNCH(PS3D_K_CORRECT, launch_correct(field(0), field(1), field(2), out, nx, ny, nz, rigid, P.dt, P.dt / P.dsqr,
-                      1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, stream));
+                      1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, stream, batch));
     return PS3D_OK;
 }
 
@@ -452,7 +722,7 @@ int Ctx::pressure_solve() {
         // velocity is solved again and its pressure added to p
         rc = poisson_once((double*)p2.p, 0.0);
         if (rc) return rc;
-        LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N, 1.0, 1.0, stream));
+        LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N * batch, 1.0, 1.0, stream));
     }
     return PS3D_OK;
 }
@@ -474,6 +744,7 @@ int Ctx::forward_transform(const double* const* in) {
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
+            c.batch = 1; c.sM = M;
             c.pz = plz.plan; c.scale = P.dz; c.op = 1;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -491,6 +762,7 @@ int Ctx::backward_transform(double* const* out) {
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
+            c.batch = 1; c.sM = M;
             c.pz = plz.plan; c.scale = 1.0; c.op = 2;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -624,6 +896,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
         itt = 0; taum2 = 1; taum1 = 2; tau = 3;
         P.dt = -std::fabs(P.dt);
         for (int s = 0; s <= n_end - 1 && !rc; ++s) {
+            if (cancelled()) { rc = PS3D_ERR_CANCELLED; break; }
             P.Ro = (1. - ramp(s * dt_loc / O.period)) * Ro_loc;
             rc = step(itt, tau, taum1, taum2);
             rotate();
@@ -643,6 +916,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
         itt = 0; taum2 = 1; taum1 = 2; tau = 3;
         P.dt = std::fabs(P.dt);
         for (int s = 0; s <= n_end - 1 && !rc; ++s) {
+            if (cancelled()) { rc = PS3D_ERR_CANCELLED; break; }
             P.Ro = ramp(s * dt_loc / O.period) * Ro_loc;
             rc = step(itt, tau, taum1, taum2);
             rotate();
@@ -688,6 +962,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     P.Ro = Ro_loc; P.dt = dt_loc;
     P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
     tau = tau_loc; taum1 = taum1_loc; taum2 = taum2_loc; itt = itt_loc;
+    invalidate_graph();
     if (rc) return rc;
     if (O.adopt) CK(copy_set_to_state(PS3D_FIELDS_BALANCED));
     CK(cudaStreamSynchronize(stream));
@@ -789,6 +1064,7 @@ int Ctx::download_tend(int f, double* h) {
 }
 
 int Ctx::set_forcing(const ps3d_forcing* f) {
+    invalidate_graph();
     fkind = 0; fn = nullptr; user = nullptr;
     if (!f || f->kind == PS3D_FORCE_NONE) return PS3D_OK;
     if (f->kind & ~(PS3D_FORCE_WAVEMAKER | PS3D_FORCE_BACKGROUND | PS3D_FORCE_CALLBACK)) return PS3D_ERR_BADPARAM;
@@ -907,13 +1183,8 @@ int ps3d_integrate(ps3d_ctx* ctx, int nsteps) {
     GUARD_BEGIN
     if (!ctx_ok(ctx) || nsteps < 0) return PS3D_ERR_BADPARAM;
     Ctx& C = ctx->impl;
-    for (int n = 0; n < nsteps; ++n) {
-        int rc = C.step(C.itt, C.tau, C.taum1, C.taum2);
-        if (rc) return rc;
-        C.rotate();
-        C.time = C.time + C.P.dt;
-        C.itt = C.itt + 1;
-    }
+    int rc = C.advance(nsteps, true);
+    if (rc) return rc;
     return C.sync();
     GUARD_END
 }
@@ -925,6 +1196,7 @@ int ps3d_set_step_params(ps3d_ctx* ctx, double dt, double Ro, double Ahbi, doubl
     if (dt == 0.0 || !std::isfinite(dt) || !std::isfinite(Ro)) return PS3D_ERR_BADPARAM;
     if (C.mixed && (Ahbi > 0 || Avbi > 0 || Khbi > 0 || Kvbi > 0)) return PS3D_ERR_UNSUPPORTED;
     C.P.dt = dt; C.P.Ro = Ro; C.P.Ahbi = Ahbi; C.P.Avbi = Avbi; C.P.Khbi = Khbi; C.P.Kvbi = Kvbi;
+    C.invalidate_graph();
     return PS3D_OK;
     GUARD_END
 }
@@ -1001,16 +1273,21 @@ int ps3d_enqueue(ps3d_ctx* ctx, int nsteps) {
     GUARD_BEGIN
     if (!ctx_ok(ctx) || nsteps < 0) return PS3D_ERR_BADPARAM;
     Ctx& C = ctx->impl;
-    for (int n = 0; n < nsteps; ++n) {
-        int rc = C.step(C.itt, C.tau, C.taum1, C.taum2);
-        if (rc) return rc;
-        C.rotate();
-        C.time = C.time + C.P.dt;
-        C.itt = C.itt + 1;
-    }
+    int rc = C.advance(nsteps, true);
+    if (rc) return rc;
     CK(cudaGetLastError());
     return PS3D_OK;
     GUARD_END
+}
+
+int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
+    if (!ctx || !buf || len < 1) return PS3D_ERR_BADPARAM;
+    const Ctx& C = ctx->impl;
+    const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
+    std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_cluster=%d row_chunk=%d fft_x=%d stages fft_y=%d stages "
+                  "kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.mixed ? "mixed" : "fp64", C.batch, pa.C, pa.row_chunk,
+                  pa.px.nst, pa.py.nst, C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
+    return PS3D_OK;
 }
 
 int ps3d_profile(ps3d_ctx* ctx, int enable) {

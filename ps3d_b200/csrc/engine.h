@@ -29,6 +29,9 @@ struct StepArgs {
     double wm_c, wm_s;             // cos(omega t), sin(omega t)
     const double* wr[4];           // wavemaker real parts (NULL = 0)
     const double* wi[4];           // wavemaker imaginary parts
+    int batch;                     // instances of the same grid stepped together (>= 1)
+    long sN;                       // element stride between instances (fields and tendency slots)
+    int kchunk;                    // z levels per block (autotuned)
 };
 
 // Plane-FFT kernels (divergence + forward 2D FFT, inverse 2D FFT) for one grid.
@@ -47,6 +50,8 @@ struct PlaneArgs {
     FFTPlan px;                    // length nx/2
     FFTPlan py;                    // length ny
     const double2* twx;            // exp(-2 pi i t/nx), t = 0..nx/2
+    int batch;                     // instances (>= 1): grid.y = nz*batch
+    long sN, sM;                   // instance strides: real fields, spectral elements
 };
 
 struct ColumnArgs {
@@ -60,6 +65,8 @@ struct ColumnArgs {
     double scale;                  // periodic forward z scale (dz)
     FFTPlan pz;                    // length nz (periodic)
     int op;                        // periodic: 0 solve, 1 forward only, 2 inverse only
+    int batch;                     // instances (>= 1), spectral stride sM elements
+    long sM;
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
@@ -70,7 +77,8 @@ cudaError_t launch_biharmonic_v(const double* cur, const double* old, double* ou
 cudaError_t launch_forcing_background(const StepArgs& a, cudaStream_t s);
 cudaError_t launch_wavemaker_ab(const StepArgs& a, int do_wm, cudaStream_t s);
 cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int nx, int ny, int nz, int rigid,
-                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s);
+                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s,
+                           int batch = 1);
 
 // poisson.cu
 size_t plane_fwd_smem(const PlaneArgs& a, bool fp32);
@@ -78,6 +86,7 @@ size_t plane_inv_smem(const PlaneArgs& a, bool fp32);
 cudaError_t plane_setup(bool fp32);
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);
+int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd);
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
 

@@ -1,0 +1,224 @@
+// ensemble.cu — batched ensembles of uneven grids.
+//
+// The reference runs one grid per MPI job; an ensemble is a new capability.
+// Members with identical parameters (same grid, physics and time step) form
+// one group; a group is a batched context whose kernels carry the member
+// index in their grid, so one launch of each kernel advances every member of
+// the group.  All groups share one stream, and for constant parameters three
+// consecutive steps of every group are captured into a single CUDA graph that
+// is replayed (tau and the state buffers cycle with period 3).
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+#include "ctx.h"
+
+using ps3d::Ctx;
+
+struct ps3d_ensemble {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<std::unique_ptr<Ctx>> groups;
+    std::vector<std::pair<int, int>> where;   // member -> (group, index in group)
+    cudaGraphExec_t gexec = nullptr;
+    bool graph_valid = false;
+    int itt = 0;
+    ~ps3d_ensemble() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        groups.clear();
+        if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+    }
+};
+
+namespace {
+
+bool same_params(const ps3d_params& a, const ps3d_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+
+int step_all(ps3d_ensemble* e) {
+    for (auto& g : e->groups) {
+        int rc = g->step(g->itt, g->tau, g->taum1, g->taum2);
+        if (rc) return rc;
+        g->rotate();
+        g->time = g->time + g->P.dt;
+        ++g->itt;
+    }
+    ++e->itt;
+    return PS3D_OK;
+}
+
+bool all_graphable(ps3d_ensemble* e) {
+    for (auto& g : e->groups)
+        if (!g->graphable()) return false;
+    return true;
+}
+
+int capture(ps3d_ensemble* e) {
+    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+    struct Book { int itt, tau, t1, t2, cur[4]; double time; long long launches; };
+    std::vector<Book> saved;
+    for (auto& g : e->groups)
+        saved.push_back({g->itt, g->tau, g->taum1, g->taum2, {g->cur[0], g->cur[1], g->cur[2], g->cur[3]}, g->time,
+                         g->launches});
+    const int itt0 = e->itt;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PS3D_ERR_CUDA;
+    int rc = PS3D_OK;
+    for (int s = 0; s < 3 && !rc; ++s) rc = step_all(e);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+    for (size_t q = 0; q < e->groups.size(); ++q) {
+        Ctx& g = *e->groups[q];
+        g.g_launches = g.launches - saved[q].launches;
+        g.itt = saved[q].itt; g.tau = saved[q].tau; g.taum1 = saved[q].t1; g.taum2 = saved[q].t2;
+        for (int f = 0; f < 4; ++f) g.cur[f] = saved[q].cur[f];
+        g.time = saved[q].time;
+        g.launches = saved[q].launches;
+    }
+    e->itt = itt0;
+    if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (ce != cudaSuccess) return PS3D_ERR_CUDA;
+    ce = cudaGraphInstantiate(&e->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return PS3D_ERR_CUDA;
+    e->graph_valid = true;
+    return PS3D_OK;
+}
+
+int advance(ps3d_ensemble* e, int nsteps) {
+    while (nsteps > 0) {
+        if (nsteps >= 3 && e->itt >= 2 && all_graphable(e)) {
+            if (!e->graph_valid) {
+                int rc = capture(e);
+                if (rc) return rc;
+            }
+            if (cudaGraphLaunch(e->gexec, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+            for (auto& g : e->groups)
+                for (int s = 0; s < 3; ++s) {
+                    g->rotate();
+                    for (int f = 0; f < 4; ++f) g->cur[f] = (g->cur[f] + 1) % 3;
+                    g->time = g->time + g->P.dt;
+                    ++g->itt;
+                }
+            for (auto& g : e->groups) g->launches += g->g_launches;
+            e->itt += 3;
+            nsteps -= 3;
+            continue;
+        }
+        int rc = step_all(e);
+        if (rc) return rc;
+        --nsteps;
+    }
+    return PS3D_OK;
+}
+
+}  // namespace
+
+#define EGUARD_BEGIN try {
+#define EGUARD_END                                         \
+    }                                                      \
+    catch (const std::bad_alloc&) { return PS3D_ERR_OOM; } \
+    catch (...) { return PS3D_ERR_CUDA; }
+
+extern "C" {
+
+PS3D_API int ps3d_ensemble_create(const ps3d_params* members, int n, int device, ps3d_ensemble** out) {
+    EGUARD_BEGIN
+    if (!members || n < 1 || !out) return PS3D_ERR_BADPARAM;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return PS3D_ERR_CUDA;
+    std::unique_ptr<ps3d_ensemble> e(new ps3d_ensemble());
+    e->device = device;
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) return PS3D_ERR_CUDA;
+    // group members with identical parameters, in first-seen order
+    std::vector<int> gid(n, -1);
+    std::vector<int> leader, count;
+    for (int m = 0; m < n; ++m) {
+        for (size_t q = 0; q < leader.size(); ++q)
+            if (same_params(members[leader[q]], members[m])) { gid[m] = (int)q; break; }
+        if (gid[m] < 0) { gid[m] = (int)leader.size(); leader.push_back(m); count.push_back(0); }
+        e->where.push_back({gid[m], count[gid[m]]++});
+    }
+    for (size_t q = 0; q < leader.size(); ++q) {
+        std::unique_ptr<Ctx> c(new Ctx());
+        int rc = c->init(members[leader[q]], device, count[q], e->stream);
+        if (rc) return rc;
+        e->groups.push_back(std::move(c));
+    }
+    *out = e.release();
+    return PS3D_OK;
+    EGUARD_END
+}
+
+PS3D_API int ps3d_ensemble_destroy(ps3d_ensemble* e) {
+    EGUARD_BEGIN
+    if (!e) return PS3D_ERR_BADPARAM;
+    cudaSetDevice(e->device);
+    delete e;
+    return PS3D_OK;
+    EGUARD_END
+}
+
+PS3D_API int ps3d_ensemble_upload(ps3d_ensemble* e, int member, const double* u, const double* v, const double* w,
+                                  const double* b) {
+    EGUARD_BEGIN
+    if (!e || member < 0 || member >= (int)e->where.size()) return PS3D_ERR_BADPARAM;
+    cudaSetDevice(e->device);
+    Ctx& g = *e->groups[e->where[member].first];
+    const int m = e->where[member].second;
+    const double* f[4] = {u, v, w, b};
+    for (int q = 0; q < 4; ++q) {
+        int rc = g.upload_field(g.member_field(q, m), f[q]);
+        if (rc) return rc;
+    }
+    return PS3D_OK;
+    EGUARD_END
+}
+
+PS3D_API int ps3d_ensemble_download(ps3d_ensemble* e, int member, double* u, double* v, double* w, double* b,
+                                    double* p) {
+    EGUARD_BEGIN
+    if (!e || member < 0 || member >= (int)e->where.size()) return PS3D_ERR_BADPARAM;
+    cudaSetDevice(e->device);
+    Ctx& g = *e->groups[e->where[member].first];
+    const int m = e->where[member].second;
+    double* f[4] = {u, v, w, b};
+    for (int q = 0; q < 4; ++q) {
+        int rc = g.download_field(g.member_field(q, m), f[q], 0);
+        if (rc) return rc;
+    }
+    return g.download_field((const double*)g.p.p + (size_t)m * g.N, p, 1);
+    EGUARD_END
+}
+
+PS3D_API int ps3d_ensemble_enqueue(ps3d_ensemble* e, int nsteps) {
+    EGUARD_BEGIN
+    if (!e || nsteps < 0) return PS3D_ERR_BADPARAM;
+    cudaSetDevice(e->device);
+    return advance(e, nsteps);
+    EGUARD_END
+}
+
+PS3D_API int ps3d_ensemble_integrate(ps3d_ensemble* e, int nsteps) {
+    EGUARD_BEGIN
+    if (!e || nsteps < 0) return PS3D_ERR_BADPARAM;
+    cudaSetDevice(e->device);
+    int rc = advance(e, nsteps);
+    if (rc) return rc;
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return PS3D_ERR_CUDA;
+    return PS3D_OK;
+    EGUARD_END
+}
+
+PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launches, void** stream) {
+    if (!e) return PS3D_ERR_BADPARAM;
+    if (ngroups) *ngroups = (int)e->groups.size();
+    if (launches) {
+        long long t = 0;
+        for (auto& g : e->groups) t += g->launches;
+        *launches = t;
+    }
+    if (stream) *stream = (void*)e->stream;
+    return PS3D_OK;
+}
+
+}  // extern "C"

@@ -32,7 +32,7 @@ __device__ __forceinline__ float2 twiddle<float>(const FFTPlan& P, int t, int si
 
 // radix-RAD DFT in registers: y_m = sum_q v_q exp(sign 2 pi i q m / RAD)
 template <int RAD, typename T>
-__device__ __forceinline__ void small_dft(T* v, int sign) {
+PS3D_HD void small_dft(T* v, int sign) {
     using R = decltype(v[0].x);
     if constexpr (RAD == 2) {
         T a = v[0], b = v[1];
@@ -49,6 +49,45 @@ __device__ __forceinline__ void small_dft(T* v, int sign) {
         T e = cscale(cmul_si(d, sign), h);
         v[0] = cadd(v[0], c);
         v[1] = cadd(m, e); v[2] = csub(m, e);
+    } else if constexpr (RAD == 8) {
+        // radix 2 x 4: y_m = E_m + W8^m O_m, y_{m+4} = E_m - W8^m O_m
+        const R h = (R)0.70710678118654752440;   // sqrt(1/2)
+        T e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        small_dft<4>(e, sign);
+        small_dft<4>(o, sign);
+        const T o1 = mk<R>(h * (o[1].x - sign * o[1].y), h * (o[1].y + sign * o[1].x));   // W8^1
+        const T o2 = cmul_si(o[2], sign);                                                // W8^2 = s i
+        const T o3 = mk<R>(h * (-o[3].x - sign * o[3].y), h * (sign * o[3].x - o[3].y)); // W8^3
+        v[0] = cadd(e[0], o[0]); v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);   v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);   v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);   v[7] = csub(e[3], o3);
+    } else if constexpr (RAD == 16) {
+        // radix 4 x 4: A[q2][m1] = DFT4_q1(v[4 q1 + q2]) W16^{q2 m1}; y[m1 + 4 m2] = DFT4_q2(A[q2][m1])
+        const R cs[10] = {(R)1.0, (R)0.92387953251128675613, (R)0.70710678118654752440, (R)0.38268343236508977173,
+                          (R)0.0, (R)-0.38268343236508977173, (R)-0.70710678118654752440, (R)-0.92387953251128675613,
+                          (R)-1.0, (R)-0.92387953251128675613};
+        const R sn[10] = {(R)0.0, (R)0.38268343236508977173, (R)0.70710678118654752440, (R)0.92387953251128675613,
+                          (R)1.0, (R)0.92387953251128675613, (R)0.70710678118654752440, (R)0.38268343236508977173,
+                          (R)0.0, (R)-0.38268343236508977173};
+        T A[4][4];
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+            T t[4] = {v[q2], v[4 + q2], v[8 + q2], v[12 + q2]};
+            small_dft<4>(t, sign);
+#pragma unroll
+            for (int m1 = 0; m1 < 4; ++m1) {
+                const int e = q2 * m1;
+                A[q2][m1] = e == 0 ? t[m1] : cmul(t[m1], mk<R>(cs[e], sign * sn[e]));
+            }
+        }
+#pragma unroll
+        for (int m1 = 0; m1 < 4; ++m1) {
+            T t[4] = {A[0][m1], A[1][m1], A[2][m1], A[3][m1]};
+            small_dft<4>(t, sign);
+#pragma unroll
+            for (int m2 = 0; m2 < 4; ++m2) v[m1 + 4 * m2] = t[m2];
+        }
     } else if constexpr (RAD == 5) {
         const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;
         const R s1 = (R)0.95105651629515357212, s2 = (R)0.58778525229247312917;
@@ -102,17 +141,16 @@ __device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const
 template <bool DIT, typename R>
 __device__ void fft_batch(cpx<R>* buf, int ld, int nlines, const FFTPlan& P, int sign) {
     __syncthreads();
-    int Lps[kMaxStages];
-    int acc = 1;
-    for (int s = 0; s < P.nst; ++s) { Lps[s] = acc; acc *= P.r[s]; }
     for (int s0 = 0; s0 < P.nst; ++s0) {
         const int st = DIT ? s0 : P.nst - 1 - s0;
-        const int Lp = Lps[st];
+        const int Lp = P.lp[st];
         switch (P.r[st]) {
             case 2: fft_stage<2, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
             case 3: fft_stage<3, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
             case 4: fft_stage<4, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
             case 5: fft_stage<5, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
+            case 8: fft_stage<8, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
+            case 16: fft_stage<16, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
             default: break;
         }
         __syncthreads();

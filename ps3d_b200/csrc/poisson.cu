@@ -31,17 +31,23 @@ namespace ps3d {
 constexpr int kPlaneThreads = 256;
 
 template <typename R>
-__global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(const PlaneArgs a) {
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_fwd(const PlaneArgs a) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
     T* colbuf = reinterpret_cast<T*>(smem_raw);
     T* rowbuf = colbuf + (size_t)a.ny * a.ldc;
-    const int k = blockIdx.y;
-    const int rank = (int)cluster.block_rank();
     const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
+    const int inst = blockIdx.y / nz;
+    const int k = blockIdx.y - inst * nz;
+    const long ioff = (long)inst * a.sN;
+    const int rank = (int)cluster.block_rank();
     const long plane = (long)nx * ny;
     const int ldr = a.ldr, ldc = a.ldc, cpc = a.cols_per_cta;
+    const double* au = a.u + ioff;
+    const double* av = a.v + ioff;
+    const double* aw = a.w + ioff;
+    const double* asrc = a.src ? a.src + ioff : nullptr;
     cluster.sync();   // every CTA of the cluster is running before DSMEM stores
     const int jb = rank * a.rows_per_cta;
     for (int jc = 0; jc < a.rows_per_cta; jc += a.row_chunk) {
@@ -52,18 +58,18 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(const PlaneArgs a) 
             const long g = (long)k * plane + (long)j * nx + 2 * m;
             double d0, d1;
             if (a.mode == 0) {
-                const double2 uu = *reinterpret_cast<const double2*>(a.u + g);
-                const double um = a.u[g - 2 * m + wrap(2 * m - 1, nx)];
+                const double2 uu = *reinterpret_cast<const double2*>(au + g);
+                const double um = au[g - 2 * m + wrap(2 * m - 1, nx)];
                 const long gv = g + (long)(wrap(j - 1, ny) - j) * nx;
                 const long gw = g + (long)(wrap(k - 1, nz) - k) * plane;
-                const double2 vv = *reinterpret_cast<const double2*>(a.v + g);
-                const double2 vm = *reinterpret_cast<const double2*>(a.v + gv);
-                const double2 ww = *reinterpret_cast<const double2*>(a.w + g);
-                const double2 wm = *reinterpret_cast<const double2*>(a.w + gw);
+                const double2 vv = *reinterpret_cast<const double2*>(av + g);
+                const double2 vm = *reinterpret_cast<const double2*>(av + gv);
+                const double2 ww = *reinterpret_cast<const double2*>(aw + g);
+                const double2 wm = *reinterpret_cast<const double2*>(aw + gw);
                 d0 = ((uu.x - um) * a.rdx + (vv.x - vm.x) * a.rdy + (ww.x - wm.x) * a.rdz) * a.rdt;
                 d1 = ((uu.y - uu.x) * a.rdx + (vv.y - vm.y) * a.rdy + (ww.y - wm.y) * a.rdz) * a.rdt;
             } else {
-                const double2 s = *reinterpret_cast<const double2*>(a.src + g);
+                const double2 s = *reinterpret_cast<const double2*>(asrc + g);
                 d0 = s.x; d1 = s.y;
             }
             rowbuf[m * ldr + rr] = mk<R>((R)d0, (R)d1);
@@ -90,7 +96,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(const PlaneArgs a) 
     const int c0 = rank * cpc;
     const int ncol = max(0, min(cpc, nxh - c0));
     if (ncol > 0) fft_batch<false, R>(colbuf, ldc, ncol, a.py, -1);
-    T* spec = reinterpret_cast<T*>(a.spec);
+    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM;
     const R sc = (R)a.scale;
     for (int t = threadIdx.x; t < ny * ncol; t += blockDim.x) {
         const int ky = t / ncol, c = t - ky * ncol;
@@ -99,20 +105,22 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_fwd(const PlaneArgs a) 
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(const PlaneArgs a) {
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_inv(const PlaneArgs a) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
     T* colbuf = reinterpret_cast<T*>(smem_raw);
     T* rowbuf = colbuf + (size_t)a.ny * a.ldc;
-    const int k = blockIdx.y;
-    const int rank = (int)cluster.block_rank();
     const int nx = a.nx, ny = a.ny, nxh = a.nxh, n2 = nx / 2;
+    const int inst = blockIdx.y / a.nz;
+    const int k = blockIdx.y - inst * a.nz;
+    double* out = a.out + (long)inst * a.sN;
+    const int rank = (int)cluster.block_rank();
     const long plane = (long)nx * ny;
     const int ldr = a.ldr, ldc = a.ldc, cpc = a.cols_per_cta;
     const int c0 = rank * cpc;
     const int ncol = max(0, min(cpc, nxh - c0));
-    const T* spec = reinterpret_cast<const T*>(a.spec);
+    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM;
     for (int t = threadIdx.x; t < ny * ncol; t += blockDim.x) {
         const int ky = t / ncol, c = t - ky * ncol;
         colbuf[ky * ldc + c] = spec[((long)k * ny + ky) * nxh + c0 + c];
@@ -147,10 +155,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_inv(const PlaneArgs a) 
             const long g = (long)k * plane + (long)j * nx + 2 * m;
             double2 o = make_double2((double)z.x * sc, (double)z.y * sc);
             if (a.beta != 0.0) {
-                const double2 prev = *reinterpret_cast<const double2*>(a.out + g);
+                const double2 prev = *reinterpret_cast<const double2*>(out + g);
                 o.x = o.x + a.beta * prev.x; o.y = o.y + a.beta * prev.y;
             }
-            *reinterpret_cast<double2*>(a.out + g) = o;
+            *reinterpret_cast<double2*>(out + g) = o;
         }
         __syncthreads();
     }
@@ -165,37 +173,57 @@ __global__ void __launch_bounds__(128) k_thomas(const ColumnArgs a) {
     using T = cpx<R>;
     extern __shared__ double cps[];   // [nz/8 + 1][blockDim.x] checkpoints of c'
     const long ncols = (long)a.nxh * a.ny;
-    const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (c >= ncols) return;
-    T* spec = reinterpret_cast<T*>(a.spec);
+    const long cg_ = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (cg_ >= ncols * a.batch) return;
+    const long inst = cg_ / ncols;
+    const long c = cg_ - inst * ncols;
+    T* spec = reinterpret_cast<T*>(a.spec) + inst * a.sM;
     const int nz = a.nz;
     const int i = (int)(c % a.nxh), j = (int)(c / a.nxh);
     const double ks = a.hkx[i] + a.hky[j];
     const double fxa = a.fxa;
     if (ks > 0) {
+        // levels are processed in chunks of 8: the 8 loads of a chunk are
+        // issued together, then the serial recurrence runs on registers
         const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-        const double b0 = (nz == 1) ? bend : bend;
-        double cp = fxa / b0;
-        const T d0 = spec[c];
-        double dpx = (double)d0.x / b0, dpy = (double)d0.y / b0;
-        spec[c] = mk<R>((R)dpx, (R)dpy);
-        cps[threadIdx.x] = cp;
-        for (int k = 1; k < nz; ++k) {
-            const double bk = (k == nz - 1) ? bend : bmid;
-            const double m = bk - cp * fxa;
-            const double r = 1.0 / m;
-            cp = fxa * r;
-            const T dk = spec[c + (long)k * ncols];
-            dpx = ((double)dk.x - dpx * fxa) * r;
-            dpy = ((double)dk.y - dpy * fxa) * r;
-            spec[c + (long)k * ncols] = mk<R>((R)dpx, (R)dpy);
-            if ((k & 7) == 0) cps[(k >> 3) * blockDim.x + threadIdx.x] = cp;
+        double cp = 0.0, dpx = 0.0, dpy = 0.0;
+        for (int kb = 0; kb < nz; kb += 8) {
+            T d[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (kb + q < nz) d[q] = spec[c + (long)(kb + q) * ncols];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = kb + q;
+                if (k < nz) {
+                    const double bk = (k == 0 || k == nz - 1) ? bend : bmid;
+                    if (k == 0) {
+                        cp = fxa / bk;                       // cp(1) = c(1)/b(1)
+                        dpx = (double)d[q].x / bk;           // dp(1) = d(1)/b(1)
+                        dpy = (double)d[q].y / bk;
+                    } else {
+                        const double r = 1.0 / (bk - cp * fxa);
+                        cp = fxa * r;
+                        dpx = ((double)d[q].x - dpx * fxa) * r;
+                        dpy = ((double)d[q].y - dpy * fxa) * r;
+                    }
+                    if (q == 0) cps[(kb >> 3) * blockDim.x + threadIdx.x] = cp;
+                    d[q] = mk<R>((R)dpx, (R)dpy);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (kb + q < nz) spec[c + (long)(kb + q) * ncols] = d[q];
         }
         double xx = dpx, xy = dpy;   // x(nz) = dp(nz)
-        for (int s = (nz - 1) >> 3; s >= 0; --s) {
-            const int kb = s * 8;
+        for (int sg = (nz - 1) >> 3; sg >= 0; --sg) {
+            const int kb = sg * 8;
+            T d[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (kb + q < nz - 1) d[q] = spec[c + (long)(kb + q) * ncols];
             double cpl[8];
-            cpl[0] = cps[s * blockDim.x + threadIdx.x];
+            cpl[0] = cps[sg * blockDim.x + threadIdx.x];
 #pragma unroll
             for (int q = 1; q < 8; ++q) {
                 const int k = kb + q;
@@ -208,13 +236,14 @@ __global__ void __launch_bounds__(128) k_thomas(const ColumnArgs a) {
             }
 #pragma unroll
             for (int q = 7; q >= 0; --q) {
-                const int k = kb + q;
-                if (k >= nz - 1) continue;
-                const T dk = spec[c + (long)k * ncols];
-                xx = (double)dk.x - cpl[q] * xx;
-                xy = (double)dk.y - cpl[q] * xy;
-                spec[c + (long)k * ncols] = mk<R>((R)xx, (R)xy);
+                if (kb + q >= nz - 1) continue;
+                xx = (double)d[q].x - cpl[q] * xx;
+                xy = (double)d[q].y - cpl[q] * xy;
+                d[q] = mk<R>((R)xx, (R)xy);
             }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (kb + q < nz - 1) spec[c + (long)(kb + q) * ncols] = d[q];
         }
     } else {
         // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
@@ -252,10 +281,12 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
     T* buf = reinterpret_cast<T*>(smem_raw);
     const int ld = kZLines + 1;
     const long ncols = (long)a.nxh * a.ny;
-    const long c0 = blockIdx.x * (long)kZLines;
+    const long bpi = (ncols + kZLines - 1) / kZLines;   // blocks per instance
+    const long inst = blockIdx.x / bpi;
+    const long c0 = (blockIdx.x - inst * bpi) * (long)kZLines;
     const int nl = (int)min((long)kZLines, ncols - c0);
     const int nz = a.nz;
-    T* spec = reinterpret_cast<T*>(a.spec);
+    T* spec = reinterpret_cast<T*>(a.spec) + inst * a.sM;
     for (int t = threadIdx.x; t < nz * nl; t += blockDim.x) {
         const int k = t / nl, l = t - k * nl;
         const int slot = (a.op == 2) ? a.pz.pos[k] : k;
@@ -314,7 +345,7 @@ cudaError_t plane_setup(bool fp32) { return fp32 ? setup_t<float>() : setup_t<do
 template <typename R, bool FWD>
 static cudaError_t launch_plane_t(const PlaneArgs& a, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(a.C, a.nz, 1);
+    cfg.gridDim = dim3(a.C, a.nz * std::max(1, a.batch), 1);
     cfg.blockDim = dim3(kPlaneThreads, 1, 1);
     cfg.dynamicSmemBytes = plane_fwd_smem(a, sizeof(R) == 4);
     cfg.stream = s;
@@ -328,6 +359,30 @@ static cudaError_t launch_plane_t(const PlaneArgs& a, cudaStream_t s) {
     if (FWD) return cudaLaunchKernelEx(&cfg, k_plane_fwd<R>, a);
     return cudaLaunchKernelEx(&cfg, k_plane_inv<R>, a);
 }
+template <typename R, bool FWD>
+static int max_clusters_t(const PlaneArgs& a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(a.C, a.nz * std::max(1, a.batch), 1);
+    cfg.blockDim = dim3(kPlaneThreads, 1, 1);
+    cfg.dynamicSmemBytes = plane_fwd_smem(a, sizeof(R) == 4);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    cudaError_t e = FWD ? cudaOccupancyMaxActiveClusters(&n, k_plane_fwd<R>, &cfg)
+                        : cudaOccupancyMaxActiveClusters(&n, k_plane_inv<R>, &cfg);
+    if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
+}
+int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd) {
+    if (fp32) return fwd ? max_clusters_t<float, true>(a) : max_clusters_t<float, false>(a);
+    return fwd ? max_clusters_t<double, true>(a) : max_clusters_t<double, false>(a);
+}
+
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s) {
     return fp32 ? launch_plane_t<float, true>(a, s) : launch_plane_t<double, true>(a, s);
 }
@@ -336,7 +391,7 @@ cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
 }
 
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s) {
-    const long ncols = (long)a.nxh * a.ny;
+    const long ncols = (long)a.nxh * a.ny * std::max(1, a.batch);
     const int threads = 128;
     const int blocks = (int)((ncols + threads - 1) / threads);
     const size_t sm = (size_t)((a.nz + 7) / 8 + 1) * threads * sizeof(double);
@@ -347,7 +402,7 @@ cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s) {
 
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s) {
     const long ncols = (long)a.nxh * a.ny;
-    const int blocks = (int)((ncols + kZLines - 1) / kZLines);
+    const int blocks = (int)(((ncols + kZLines - 1) / kZLines) * std::max(1, a.batch));
     const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
     const size_t sm = (size_t)a.nz * (kZLines + 1) * es;
     if (fp32) k_zsolve<float><<<blocks, 256, sm, s>>>(a);

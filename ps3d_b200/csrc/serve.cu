@@ -1,0 +1,302 @@
+// serve.cu — a request loop for optimal-balance integrations.
+//
+// Each request is one diag_opt_balance (for_src/diag_opt_balance.f90:55-179)
+// on its own grid and initial state.  Requests are admitted in arrival order
+// as execution slots and HBM free up: a request's device footprint is
+// computed from its grid before admission and the sum over running requests
+// never exceeds the budget.  Every admitted request owns a context with its
+// own CUDA stream, driven by a worker thread, so the kernels of concurrent
+// requests overlap on the GPU while each request's arithmetic stays exactly
+// what it would be alone (no data is shared, reductions are deterministic).
+// Every wait is bounded; nothing here blocks without a limit.
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+#include "ctx.h"
+
+using ps3d::Ctx;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+enum State { kQueued, kRunning, kDone, kFailed, kCancelled };
+
+struct Request {
+    long long id = 0;
+    ps3d_params prm{};
+    ps3d_optbal opt{};
+    std::vector<double> in[4];      // halo-layout input fields
+    std::vector<double> out[4];     // balanced fields (u_bal..b_bal)
+    size_t footprint = 0;
+    State state = kQueued;
+    int status = PS3D_OK;
+    double norm = 0.0;
+    int iters = 0;
+    Clock::time_point t_submit, t_start, t_end;
+    std::atomic<int> cancel{0};
+};
+
+}  // namespace
+
+// Device bytes a context for `p` allocates for a full optimal-balance run.
+static size_t footprint_of(const ps3d_params& p) {
+    const size_t N = (size_t)p.nx * p.ny * p.nz;
+    const size_t M = (size_t)(p.nx / 2 + 1) * p.ny * p.nz;
+    const bool mixed = p.precision == PS3D_MIXED;
+    const size_t ts = mixed ? 4 : 8;
+    size_t b = 0;
+    b += 12 * N * 8;                       // 3 state buffers x 4 fields
+    b += (mixed ? 2 : 1) * N * 8;          // p (+ refinement p2)
+    b += 12 * N * ts;                      // 3 tendency levels x 4 fields
+    b += M * (mixed ? 8 : 16);             // Poisson spectral array
+    b += 6 * M * 16;                       // projection spectra, g0_base, scratch
+    b += 4 * 4 * N * 8;                    // balanced, base, saved, zero-order field sets
+    b += N * 8 + 12 * N * ts;              // saved p and tendencies
+    if (p.nz > 0) b += 3 * (size_t)p.nz * p.nz * 8;
+    return b + (64u << 20);                // tables, plans, reductions, allocator slack
+}
+
+struct ps3d_server {
+    int device = 0;
+    size_t budget = 0, used = 0, peak_used = 0;
+    int max_active = 1, active = 0, peak_active = 0;
+    long long next_id = 1;
+    bool stopping = false;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::map<long long, std::shared_ptr<Request>> all;
+    std::vector<std::thread> workers;
+
+    void worker_loop();
+    void run(Request& r);
+};
+
+void ps3d_server::run(Request& r) {
+    cudaSetDevice(device);
+    Ctx c;
+    int rc = c.init(r.prm, device);
+    if (!rc) {
+        c.cancel_flag = &r.cancel;
+        for (int f = 0; f < 4 && !rc; ++f) rc = c.upload_field(c.field(f), r.in[f].data());
+    }
+    if (!rc) rc = c.opt_balance(r.opt, &r.norm, &r.iters);
+    if (!rc) {
+        // a non-finite balanced state fails this request only
+        double ke, pe, um, wm;
+        ps3d::DevBuf* bal = c.fieldset(PS3D_FIELDS_BALANCED);
+        for (int f = 0; f < 4 && !rc; ++f)
+            if (cudaMemcpyAsync(c.field(f), bal[f].p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, c.stream))
+                rc = PS3D_ERR_CUDA;
+        if (!rc) rc = c.diagnose(&ke, &pe, &um, &wm);
+    }
+    if (!rc) {
+        const size_t n3 = (size_t)(r.prm.nx + 4) * (r.prm.ny + 4) * (r.prm.nz + 4);
+        for (int f = 0; f < 4 && !rc; ++f) {
+            r.out[f].assign(n3, 0.0);
+            rc = c.download_field(c.field(f), r.out[f].data(), 0);
+        }
+    }
+    r.status = rc;
+}
+
+void ps3d_server::worker_loop() {
+    for (;;) {
+        std::shared_ptr<Request> r;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            for (;;) {
+                if (stopping) return;
+                // admit the oldest request if a slot and its HBM footprint are free
+                if (!queue.empty() && active < max_active && used + queue.front()->footprint <= budget) {
+                    r = queue.front();
+                    queue.pop_front();
+                    ++active;
+                    used += r->footprint;
+                    peak_used = std::max(peak_used, used);
+                    peak_active = std::max(peak_active, active);
+                    r->state = kRunning;
+                    r->t_start = Clock::now();
+                    break;
+                }
+                cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            }
+        }
+        run(*r);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            r->t_end = Clock::now();
+            r->state = r->status == PS3D_OK ? kDone : (r->status == PS3D_ERR_CANCELLED ? kCancelled : kFailed);
+            for (int f = 0; f < 4; ++f) { r->in[f].clear(); r->in[f].shrink_to_fit(); }
+            --active;
+            used -= r->footprint;
+        }
+        cv_work.notify_all();
+        cv_done.notify_all();
+    }
+}
+
+#define SGUARD_BEGIN try {
+#define SGUARD_END                                         \
+    }                                                      \
+    catch (const std::bad_alloc&) { return PS3D_ERR_OOM; } \
+    catch (...) { return PS3D_ERR_CUDA; }
+
+extern "C" {
+
+PS3D_API int ps3d_server_create(int device, size_t hbm_budget_bytes, int max_active, ps3d_server** out) {
+    SGUARD_BEGIN
+    if (!out || max_active < 1) return PS3D_ERR_BADPARAM;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return PS3D_ERR_CUDA;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return PS3D_ERR_CUDA;
+    std::unique_ptr<ps3d_server> s(new ps3d_server());
+    s->device = device;
+    s->budget = hbm_budget_bytes ? std::min(hbm_budget_bytes, fr) : (size_t)(0.8 * fr);
+    s->max_active = max_active;
+    for (int t = 0; t < max_active; ++t) s->workers.emplace_back([p = s.get()] { p->worker_loop(); });
+    *out = s.release();
+    return PS3D_OK;
+    SGUARD_END
+}
+
+PS3D_API int ps3d_server_destroy(ps3d_server* s) {
+    SGUARD_BEGIN
+    if (!s) return PS3D_ERR_BADPARAM;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        for (auto& q : s->queue) { q->state = kCancelled; q->status = PS3D_ERR_CANCELLED; }
+        s->queue.clear();
+        for (auto& kv : s->all) kv.second->cancel.store(1);
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->workers) t.join();
+    delete s;
+    return PS3D_OK;
+    SGUARD_END
+}
+
+PS3D_API int ps3d_server_submit(ps3d_server* s, const ps3d_params* prm, const ps3d_optbal* opt,
+                                const double* u, const double* v, const double* w, const double* b,
+                                long long* ticket) {
+    SGUARD_BEGIN
+    if (!s || !prm || !opt || !ticket || !u || !v || !w || !b) return PS3D_ERR_BADPARAM;
+    const ps3d_params& p = *prm;
+    const bool rigid = p.enable_vertical_boundaries != 0;
+    if (p.nx < 2 || p.ny < 2 || p.nz < 2 || p.nx % 2 || p.ny % 2 || (!rigid && p.nz % 2)) return PS3D_ERR_BADPARAM;
+    if (!ps3d::fft_length_ok(p.nx / 2) || !ps3d::fft_length_ok(p.ny) || (!rigid && !ps3d::fft_length_ok(p.nz)))
+        return PS3D_ERR_BADPARAM;
+    if (!(p.dt > 0) || !(opt->period > 0) || opt->max_itts < 1) return PS3D_ERR_BADPARAM;
+    if (p.precision == PS3D_MIXED && (p.Ahbi > 0 || p.Avbi > 0 || p.Khbi > 0 || p.Kvbi > 0)) return PS3D_ERR_UNSUPPORTED;
+    auto r = std::make_shared<Request>();
+    r->prm = p;
+    r->opt = *opt;
+    r->opt.adopt = 0;
+    r->footprint = footprint_of(p);
+    if (r->footprint > s->budget) return PS3D_ERR_OOM;   // can never be admitted
+    const size_t n3 = (size_t)(p.nx + 4) * (p.ny + 4) * (p.nz + 4);
+    const double* f[4] = {u, v, w, b};
+    for (int q = 0; q < 4; ++q) r->in[q].assign(f[q], f[q] + n3);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stopping) return PS3D_ERR_CANCELLED;
+        r->id = s->next_id++;
+        s->all[r->id] = r;
+        s->queue.push_back(r);
+    }
+    s->cv_work.notify_all();
+    *ticket = r->id;
+    return PS3D_OK;
+    SGUARD_END
+}
+
+// Wait up to timeout_ms for a request.  On success the balanced fields are
+// copied out (any pointer may be NULL) and res receives
+// {status, final norm, iterations, latency ms, queue ms, run ms}.
+PS3D_API int ps3d_server_wait(ps3d_server* s, long long ticket, int timeout_ms,
+                              double* u_bal, double* v_bal, double* w_bal, double* b_bal, double* res) {
+    SGUARD_BEGIN
+    if (!s) return PS3D_ERR_BADPARAM;
+    std::shared_ptr<Request> r;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return PS3D_ERR_BADPARAM;
+    r = it->second;
+    const auto deadline = Clock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
+    while (r->state == kQueued || r->state == kRunning) {
+        if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout &&
+            (r->state == kQueued || r->state == kRunning))
+            return PS3D_ERR_TIMEOUT;
+    }
+    double* out[4] = {u_bal, v_bal, w_bal, b_bal};
+    if (r->state == kDone)
+        for (int q = 0; q < 4; ++q)
+            if (out[q] && !r->out[q].empty()) std::memcpy(out[q], r->out[q].data(), r->out[q].size() * sizeof(double));
+    if (res) {
+        auto ms = [](Clock::time_point a, Clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        res[0] = r->status;
+        res[1] = r->norm;
+        res[2] = r->iters;
+        const bool ran = r->state != kCancelled || r->t_start.time_since_epoch().count() != 0;
+        res[3] = ms(r->t_submit, r->t_end);
+        res[4] = ran ? ms(r->t_submit, r->t_start) : res[3];
+        res[5] = ran ? ms(r->t_start, r->t_end) : 0.0;
+    }
+    const int st = r->status;
+    s->all.erase(ticket);   // results are handed out once
+    return st;
+    SGUARD_END
+}
+
+PS3D_API int ps3d_server_cancel(ps3d_server* s, long long ticket) {
+    SGUARD_BEGIN
+    if (!s) return PS3D_ERR_BADPARAM;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->all.find(ticket);
+        if (it == s->all.end()) return PS3D_ERR_BADPARAM;
+        Request& r = *it->second;
+        if (r.state == kQueued) {
+            for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
+                if ((*q)->id == ticket) { s->queue.erase(q); break; }
+            r.state = kCancelled;
+            r.status = PS3D_ERR_CANCELLED;
+            r.t_end = Clock::now();
+        } else if (r.state == kRunning) {
+            r.cancel.store(1);
+        }
+    }
+    s->cv_done.notify_all();
+    return PS3D_OK;
+    SGUARD_END
+}
+
+// stats: [0] active, [1] queued, [2] bytes in use, [3] peak bytes, [4] peak active, [5] budget
+PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats) {
+    if (!s || !stats) return PS3D_ERR_BADPARAM;
+    std::lock_guard<std::mutex> lk(s->mu);
+    stats[0] = s->active;
+    stats[1] = (double)s->queue.size();
+    stats[2] = (double)s->used;
+    stats[3] = (double)s->peak_used;
+    stats[4] = s->peak_active;
+    stats[5] = (double)s->budget;
+    return PS3D_OK;
+}
+
+PS3D_API long long ps3d_server_footprint(const ps3d_params* prm) { return prm ? (long long)footprint_of(*prm) : -1; }
+
+}  // extern "C"

@@ -37,12 +37,15 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
-    const int kb = blockIdx.z * kchunk;
+    const int nzc = (nz + kchunk - 1) / kchunk;
+    const int inst = blockIdx.z / nzc;
+    const int kb = (blockIdx.z - inst * nzc) * kchunk;
     const int ke = min(nz, kb + kchunk);
+    const long ioff = (long)inst * a.sN;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = (i < nx) && (j < ny);
     const long plane = (long)nx * ny;
-    const double* src[6] = {a.u, a.v, a.w, a.b, a.ub, a.bb};
+    const double* src[6] = {a.u + ioff, a.v + ioff, a.w + ioff, a.b + ioff, a.ub, a.bb};
     const int tid = ty * kTX + tx;
     constexpr int TP = (kTX + 2) * (BY + 2);
 
@@ -74,7 +77,8 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
 #define BB(di, dj, dk) SM(5, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
             const bool top = rigid && (k == nz - 1);   // flux_top(nz) = 0
             const bool bot = rigid && (k == 0);        // flux_top(0)  = 0
-            const long g = (long)k * plane + (long)j * nx + i;
+            const long g0 = (long)k * plane + (long)j * nx + i;   // point within the instance
+            const long g = g0 + ioff;                              // point within the batch
             double db_, du_, dv_, dw_;
             // ---- buoyancy advection + N^2 (advection.f90:12-47, integrate.f90:21-23)
             if (a.nonlinear) {
@@ -190,10 +194,10 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
             // ---- set_forcing: wavemaker (config.f90:224-237)
             if constexpr (WM) {
                 const double dt = a.dt, c = a.wm_c, s = a.wm_s;
-                if (a.wr[0] || a.wi[0]) u1 = u1 + dt * (c * (a.wr[0] ? a.wr[0][g] : 0.0) + s * (a.wi[0] ? a.wi[0][g] : 0.0));
-                if (a.wr[1] || a.wi[1]) v1 = v1 + dt * (c * (a.wr[1] ? a.wr[1][g] : 0.0) + s * (a.wi[1] ? a.wi[1][g] : 0.0));
-                if (a.wr[2] || a.wi[2]) w1 = w1 + dt * (c * (a.wr[2] ? a.wr[2][g] : 0.0) + s * (a.wi[2] ? a.wi[2][g] : 0.0));
-                if (a.wr[3] || a.wi[3]) b1 = b1 + dt * (c * (a.wr[3] ? a.wr[3][g] : 0.0) + s * (a.wi[3] ? a.wi[3][g] : 0.0));
+                if (a.wr[0] || a.wi[0]) u1 = u1 + dt * (c * (a.wr[0] ? a.wr[0][g0] : 0.0) + s * (a.wi[0] ? a.wi[0][g0] : 0.0));
+                if (a.wr[1] || a.wi[1]) v1 = v1 + dt * (c * (a.wr[1] ? a.wr[1][g0] : 0.0) + s * (a.wi[1] ? a.wi[1][g0] : 0.0));
+                if (a.wr[2] || a.wi[2]) w1 = w1 + dt * (c * (a.wr[2] ? a.wr[2][g0] : 0.0) + s * (a.wi[2] ? a.wi[2][g0] : 0.0));
+                if (a.wr[3] || a.wi[3]) b1 = b1 + dt * (c * (a.wr[3] ? a.wr[3][g0] : 0.0) + s * (a.wi[3] ? a.wi[3][g0] : 0.0));
             }
             // ---- store tendency of time level tau
             ((TT*)a.t0[0])[g] = (TT)du_;
@@ -204,7 +208,9 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
             if (a.do_ab) {
                 const double dt = a.dt, dtw = a.dtw;
                 const double c0 = a.ab0, c1 = a.ab1, c2 = a.ab2;
-                double tu = c0 * (double)(TT)du_, tv = c0 * (double)(TT)dv_, tw = c0 * (double)(TT)dw_, tb = c0 * (double)(TT)db_;
+                // the current tendency enters at full precision; only the
+                // stored history (FP32 in the mixed path) is rounded
+                double tu = c0 * du_, tv = c0 * dv_, tw = c0 * dw_, tb = c0 * db_;
                 if (c1 != 0.0) {
                     const TT* const* h = (const TT* const*)a.t1;
                     tu = tu + c1 * (double)h[0][g]; tv = tv + c1 * (double)h[1][g];
@@ -285,7 +291,11 @@ __global__ void k_biharmonic_v(const double* __restrict__ cur, const double* __r
     }
 }
 
-// background-flow forcing on the friction-updated state (generic path)
+// background-flow forcing on the friction-updated state (generic path).
+// set_forcing runs after the in-place friction with no halo exchange, so a
+// neighbour outside the interior still holds its start-of-step value: those
+// reads go to the old fields (a.uo..bo hold the start-of-step state here,
+// a.u..b the friction-updated one).
 __global__ void k_forcing_background(StepArgs a) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const long N = (long)nx * ny * nz, plane = (long)nx * ny;
@@ -294,37 +304,43 @@ __global__ void k_forcing_background(StepArgs a) {
         auto at = [&](const double* f, int di, int dj, int dk) -> double {
             return f[(long)wrap(k + dk, nz) * plane + (long)wrap(j + dj, ny) * nx + wrap(i + di, nx)];
         };
-        const double *u = a.u, *v = a.v, *w = a.w, *b = a.b, *ub = a.ub, *bb = a.bb;
+        auto st = [&](int fld, int di, int dj, int dk) -> double {
+            const bool in = i + di >= 0 && i + di < nx && j + dj >= 0 && j + dj < ny && k + dk >= 0 && k + dk < nz;
+            const double* cur = fld == 0 ? a.u : fld == 1 ? a.v : fld == 2 ? a.w : a.b;
+            const double* old = fld == 0 ? a.uo : fld == 1 ? a.vo : fld == 2 ? a.wo : a.bo;
+            return at(in ? cur : old, di, dj, dk);
+        };
+        const double *ub = a.ub, *bb = a.bb;
         const bool top = a.rigid && k == nz - 1, bot = a.rigid && k == 0;
         const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
         double* const* T0 = (double* const*)a.t0;
         double du_ = T0[0][g], dv_ = T0[1][g], dw_ = T0[2][g], db_ = T0[3][g];
         {
-            const double e = 2 * 0.25 * (at(ub, 0, 0, 0) + at(ub, 1, 0, 0)) * (at(u, 1, 0, 0) + at(u, 0, 0, 0));
-            const double em = 2 * 0.25 * (at(ub, -1, 0, 0) + at(ub, 0, 0, 0)) * (at(u, 0, 0, 0) + at(u, -1, 0, 0));
-            const double n = 0.25 * (at(ub, 0, 0, 0) + at(ub, 0, 1, 0)) * (at(v, 1, 0, 0) + at(v, 0, 0, 0));
-            const double nm = 0.25 * (at(ub, 0, -1, 0) + at(ub, 0, 0, 0)) * (at(v, 1, -1, 0) + at(v, 0, -1, 0));
-            const double t = top ? 0.0 : 0.25 * (at(ub, 0, 0, 1) + at(ub, 0, 0, 0)) * (at(w, 0, 0, 0) + at(w, 1, 0, 0));
-            const double tm = bot ? 0.0 : 0.25 * (at(ub, 0, 0, 0) + at(ub, 0, 0, -1)) * (at(w, 0, 0, -1) + at(w, 1, 0, -1));
+            const double e = 2 * 0.25 * (at(ub, 0, 0, 0) + at(ub, 1, 0, 0)) * (st(0, 1, 0, 0) + st(0, 0, 0, 0));
+            const double em = 2 * 0.25 * (at(ub, -1, 0, 0) + at(ub, 0, 0, 0)) * (st(0, 0, 0, 0) + st(0, -1, 0, 0));
+            const double n = 0.25 * (at(ub, 0, 0, 0) + at(ub, 0, 1, 0)) * (st(1, 1, 0, 0) + st(1, 0, 0, 0));
+            const double nm = 0.25 * (at(ub, 0, -1, 0) + at(ub, 0, 0, 0)) * (st(1, 1, -1, 0) + st(1, 0, -1, 0));
+            const double t = top ? 0.0 : 0.25 * (at(ub, 0, 0, 1) + at(ub, 0, 0, 0)) * (st(2, 0, 0, 0) + st(2, 1, 0, 0));
+            const double tm = bot ? 0.0 : 0.25 * (at(ub, 0, 0, 0) + at(ub, 0, 0, -1)) * (st(2, 0, 0, -1) + st(2, 1, 0, -1));
             du_ = du_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
         }
         {
-            const double e = 0.25 * (at(v, 0, 0, 0) + at(v, 1, 0, 0)) * (at(ub, 0, 1, 0) + at(ub, 0, 0, 0));
-            const double em = 0.25 * (at(v, -1, 0, 0) + at(v, 0, 0, 0)) * (at(ub, -1, 1, 0) + at(ub, -1, 0, 0));
+            const double e = 0.25 * (st(1, 0, 0, 0) + st(1, 1, 0, 0)) * (at(ub, 0, 1, 0) + at(ub, 0, 0, 0));
+            const double em = 0.25 * (st(1, -1, 0, 0) + st(1, 0, 0, 0)) * (at(ub, -1, 1, 0) + at(ub, -1, 0, 0));
             dv_ = dv_ - Ro * (e - em) * rdx;
         }
         {
-            const double e = 0.25 * (at(w, 0, 0, 0) + at(w, 1, 0, 0)) * (at(ub, 0, 0, 0) + at(ub, 0, 0, 1));
-            const double em = 0.25 * (at(w, -1, 0, 0) + at(w, 0, 0, 0)) * (at(ub, -1, 0, 0) + at(ub, -1, 0, 1));
+            const double e = 0.25 * (st(2, 0, 0, 0) + st(2, 1, 0, 0)) * (at(ub, 0, 0, 0) + at(ub, 0, 0, 1));
+            const double em = 0.25 * (st(2, -1, 0, 0) + st(2, 0, 0, 0)) * (at(ub, -1, 0, 0) + at(ub, -1, 0, 1));
             dw_ = dw_ - a.dsqr * Ro * (e - em) * rdx;
         }
         {
-            const double e = 0.5 * (at(b, 0, 0, 0) + at(b, 1, 0, 0)) * at(ub, 0, 0, 0) + 0.5 * (at(bb, 0, 0, 0) + at(bb, 1, 0, 0)) * at(u, 0, 0, 0);
-            const double em = 0.5 * (at(b, -1, 0, 0) + at(b, 0, 0, 0)) * at(ub, -1, 0, 0) + 0.5 * (at(bb, -1, 0, 0) + at(bb, 0, 0, 0)) * at(u, -1, 0, 0);
-            const double n = 0.5 * (at(bb, 0, 0, 0) + at(bb, 0, 1, 0)) * at(v, 0, 0, 0);
-            const double nm = 0.5 * (at(bb, 0, -1, 0) + at(bb, 0, 0, 0)) * at(v, 0, -1, 0);
-            const double t = top ? 0.0 : 0.5 * (at(bb, 0, 0, 0) + at(bb, 0, 0, 1)) * at(w, 0, 0, 0);
-            const double tm = bot ? 0.0 : 0.5 * (at(bb, 0, 0, -1) + at(bb, 0, 0, 0)) * at(w, 0, 0, -1);
+            const double e = 0.5 * (st(3, 0, 0, 0) + st(3, 1, 0, 0)) * at(ub, 0, 0, 0) + 0.5 * (at(bb, 0, 0, 0) + at(bb, 1, 0, 0)) * st(0, 0, 0, 0);
+            const double em = 0.5 * (st(3, -1, 0, 0) + st(3, 0, 0, 0)) * at(ub, -1, 0, 0) + 0.5 * (at(bb, -1, 0, 0) + at(bb, 0, 0, 0)) * st(0, -1, 0, 0);
+            const double n = 0.5 * (at(bb, 0, 0, 0) + at(bb, 0, 1, 0)) * st(1, 0, 0, 0);
+            const double nm = 0.5 * (at(bb, 0, -1, 0) + at(bb, 0, 0, 0)) * st(1, 0, -1, 0);
+            const double t = top ? 0.0 : 0.5 * (at(bb, 0, 0, 0) + at(bb, 0, 0, 1)) * st(2, 0, 0, 0);
+            const double tm = bot ? 0.0 : 0.5 * (at(bb, 0, 0, -1) + at(bb, 0, 0, 0)) * st(2, 0, 0, -1);
             db_ = db_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
         }
         T0[0][g] = du_; T0[1][g] = dv_; T0[2][g] = dw_; T0[3][g] = db_;
@@ -358,10 +374,10 @@ __global__ void k_wavemaker_ab(StepArgs a, int do_wm) {
 // ---------------------------------------------------------------------------
 __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                           const double* __restrict__ p, int nx, int ny, int nz, int rigid,
-                          double dt, double dtw, double rdx, double rdy, double rdz) {
-    const long plane = (long)nx * ny, N = plane * nz;
-    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)(g / plane);
+                          double dt, double dtw, double rdx, double rdy, double rdz, int batch) {
+    const long plane = (long)nx * ny, N = plane * nz, NB = N * batch;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < NB; g += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)((g / plane) % nz);
         const double p0 = p[g];
         const double pe = p[g - i + wrap(i + 1, nx)];
         const double pn = p[g + (long)(wrap(j + 1, ny) - j) * nx];
@@ -381,8 +397,8 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double
 // ---------------------------------------------------------------------------
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
 static cudaError_t launch_step_t(const StepArgs& a, cudaStream_t s) {
-    const int kchunk = a.nz <= 16 ? a.nz : 8;
-    dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, (a.nz + kchunk - 1) / kchunk);
+    const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, a.nz) : (a.nz <= 16 ? a.nz : 8);
+    dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((a.nz + kchunk - 1) / kchunk) * std::max(1, a.batch));
     k_step<TT, BY, HARM, WM, BG><<<grid, dim3(kTX, BY), 0, s>>>(a, kchunk);
     return cudaGetLastError();
 }
@@ -430,9 +446,9 @@ cudaError_t launch_wavemaker_ab(const StepArgs& a, int do_wm, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int nx, int ny, int nz, int rigid,
-                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s) {
-    const long N = (long)nx * ny * nz;
-    k_correct<<<grid_for(N, 256), 256, 0, s>>>(u, v, w, p, nx, ny, nz, rigid, dt, dtw, rdx, rdy, rdz);
+                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s, int batch) {
+    const long N = (long)nx * ny * nz * batch;
+    k_correct<<<grid_for(N, 256), 256, 0, s>>>(u, v, w, p, nx, ny, nz, rigid, dt, dtw, rdx, rdy, rdz, batch);
     return cudaGetLastError();
 }
 

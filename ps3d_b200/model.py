@@ -64,6 +64,7 @@ def load():
     L.ps3d_enqueue.argtypes = [vp, C.c_int]
     L.ps3d_profile.argtypes = [vp, C.c_int]
     L.ps3d_profile_read.argtypes = [vp, dp, C.POINTER(C.c_longlong)]
+    L.ps3d_describe.argtypes = [vp, C.c_char_p, C.c_int]
     L.ps3d_strerror.restype = C.c_char_p
     L.ps3d_strerror.argtypes = [C.c_int]
     _lib = L
@@ -187,6 +188,11 @@ class Model:
 
     def profile(self, enable=True):
         _check(self.L.ps3d_profile(self.h, int(enable)), "ps3d_profile")
+
+    def describe(self):
+        buf = C.create_string_buffer(512)
+        _check(self.L.ps3d_describe(self.h, buf, 512), "ps3d_describe")
+        return buf.value.decode()
 
     KERNELS = ("step", "fft_fwd", "vsolve", "fft_inv", "correct", "other")
 

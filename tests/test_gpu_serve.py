@@ -1,0 +1,106 @@
+"""Serving loop: continuous admission, alone-vs-mix invariance, admission by
+HBM footprint, cancellation, bounded waits and per-request failure.
+Failures are injected on the host (NaN in one request's input, a budget too
+small, a cancel), never on the GPU."""
+import numpy as np
+import pytest
+
+from ps3d_b200 import abi
+from ps3d_b200.serve import Server, request
+from ps3d_b200.model import PS3DError
+
+pytestmark = pytest.mark.gpu
+
+
+def _req(n=(32, 32, 16), ramp=6, iters=2):
+    return request(*n, ramp_steps=ramp, iters=iters)
+
+
+def test_result_same_alone_and_in_mix():
+    p, opt, f = _req((32, 32, 16))
+    s = Server(max_active=1)
+    alone = s.wait(s.submit(p, opt, f))
+    s.close()
+    assert alone.status == 0
+    s = Server(max_active=4)
+    others = [_req((64, 32, 16)), _req((32, 32, 8)), _req((64, 64, 16))]
+    tks = [s.submit(*o) for o in others[:2]]
+    mine = s.submit(p, opt, f)
+    tks += [s.submit(*others[2])]
+    mix = s.wait(mine)
+    for t in tks:
+        assert s.wait(t).status == 0
+    st = s.stats()
+    s.close()
+    assert mix.status == 0 and mix.iters == alone.iters
+    assert mix.norm == alone.norm
+    for n in ("u", "v", "w", "b"):
+        assert np.array_equal(mix.fields[n], alone.fields[n]), n
+    assert st["peak_active"] >= 2
+
+
+def test_admission_respects_budget():
+    reqs = [_req((64, 64, 16)) for _ in range(4)]
+    fp = Server.footprint(reqs[0][0])
+    s = Server(hbm_budget_bytes=int(2.5 * fp), max_active=4)
+    tks = [s.submit(*r) for r in reqs]
+    res = [s.wait(t) for t in tks]
+    st = s.stats()
+    s.close()
+    assert all(r.status == 0 for r in res)
+    assert st["peak_bytes"] <= 2.5 * fp
+    assert st["peak_active"] <= 2
+
+
+def test_oversized_request_refused():
+    p, opt, f = _req((64, 64, 32))
+    s = Server(hbm_budget_bytes=Server.footprint(p) // 2, max_active=2)
+    with pytest.raises(PS3DError) as ei:
+        s.submit(p, opt, f)
+    assert ei.value.status == abi.PS3D_ERR_OOM
+    s.close()
+
+
+def test_nan_request_fails_alone():
+    p, opt, f = _req((32, 32, 16))
+    bad = {k: v.copy() for k, v in f.items()}
+    bad["b"][4, 4, 4] = np.nan
+    s = Server(max_active=2)
+    t_ok = s.submit(p, opt, f)
+    t_bad = s.submit(p, opt, bad)
+    r_bad, r_ok = s.wait(t_bad), s.wait(t_ok)
+    s.close()
+    assert r_bad.status == abi.PS3D_ERR_NONFINITE
+    assert r_ok.status == 0
+    s = Server(max_active=1)
+    ref = s.wait(s.submit(p, opt, f))
+    s.close()
+    for n in ("u", "v", "w", "b"):
+        assert np.array_equal(ref.fields[n], r_ok.fields[n])
+
+
+def test_cancel_and_bounded_wait():
+    p, opt, f = _req((64, 64, 32), ramp=40, iters=3)
+    s = Server(max_active=1)
+    t1 = s.submit(p, opt, f)
+    t2 = s.submit(p, opt, f)          # queued behind t1
+    s.cancel(t2)
+    with pytest.raises(PS3DError) as ei:
+        s.wait(t1, timeout_ms=1)      # cannot finish in 1 ms
+    assert ei.value.status == abi.PS3D_ERR_TIMEOUT
+    r2 = s.wait(t2)
+    assert r2.status == abi.PS3D_ERR_CANCELLED
+    r1 = s.wait(t1)
+    assert r1.status == 0
+    s.close()
+
+
+def test_malformed_params_refused():
+    p, opt, f = _req((32, 32, 16))
+    q = p.copy()
+    q.nx = 31
+    s = Server(max_active=1)
+    with pytest.raises(PS3DError) as ei:
+        s.submit(q, opt, f)
+    assert ei.value.status == abi.PS3D_ERR_BADPARAM
+    s.close()
