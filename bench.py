@@ -158,6 +158,11 @@ def time_path(precision, steps, warmup, dev, pg):
     m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
     clocks = ClockSampler(dev)
     clocks.start()
+    t_s = time.perf_counter()
+    m.run(warmup)
+    while time.perf_counter() - t_s < 1.0:   # nvidia-smi needs time to start sampling
+        m.run(3)
+    m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
     m.run(warmup)
     stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -170,12 +175,19 @@ def time_path(precision, steps, warmup, dev, pg):
     ev1.synchronize()
     kern = m.profile_read()
     m.profile(False)
-    m.run(max(0, min(steps, 30)))      # keep the GPU loaded while the clock sampler catches up
-    clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
+    try:
+        diag = list(m.diagnose())
+    except Exception as e:   # non-finite state: reported, not hidden
+        diag = str(e)
+    state = m.download(tendencies=False)   # after warmup + exactly `steps` steps
+    t_s = time.perf_counter()
+    while time.perf_counter() - t_s < 0.5:   # keep the GPU loaded while the sampler catches up
+        m.run(3)
+    clk = clocks.stop()
+    clk["diagnose_after_timed"] = diag
     barrier(pg, dev)
     ms_max = max_over_ranks(ms, pg, dev)
-    state = m.download(tendencies=False)
     return m, p, ms, ms_max, kern, clk, state, m.describe()
 
 

@@ -83,10 +83,15 @@ def eddy_params(nx=64, ny=64, nz=32, precision=PS3D_FP64, rigid=True, dt=None):
 def jets_params(nx=256, ny=256, nz=128, precision=PS3D_FP64):
     """Two opposing zonal jets (template: for_config/jets_unscaled.f90:3-31).
 
-    Lx = Ly = 500 km, Lz = 1000 m, N0 = 2e-3, f0 = 1e-4, dt = 0.5/N0, AB3,
-    Laplacian viscosity 1e-2 m^2/s, rigid lid."""
+    Lx = Ly = 500 km, N0 = 2e-3, f0 = 1e-4, dt = 0.5/N0, AB3, Laplacian
+    viscosity 1e-2 m^2/s, rigid lid.  The depth is Lz = 4000 m rather than the
+    template's 1000 m: with 0.5 m/s jets of width Ly/16 the thermal-wind
+    buoyancy gives b_z ~ f U W pi^2 / Lz^2, which at Lz = 1000 m exceeds N0^2
+    by a factor of ~6 (statically unstable; the explicit scheme overturns and
+    blows up within ~100 steps, in the CPU restatement as on the GPU).  At
+    Lz = 4000 m the minimum of N0^2 + b_z stays at ~0.6 N0^2."""
     N0, f0 = 2e-3, 1e-4
-    return make_params(nx=nx, ny=ny, nz=nz, Lx=500e3, Ly=500e3, Lz=1000.0, f0=f0, N0=N0,
+    return make_params(nx=nx, ny=ny, nz=nz, Lx=500e3, Ly=500e3, Lz=4000.0, f0=f0, N0=N0,
                        dt=0.5 / N0, Ah=1e-2, Av=1e-2, enable_vertical_boundaries=1,
                        enable_AB_3_order=1, precision=precision)
 

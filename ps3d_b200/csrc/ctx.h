@@ -75,6 +75,10 @@ struct Ctx {
     int g_tau = -1, g_cur = -1;
     long g_version = -1, version = 0;
     long long g_launches = 0;
+    bool g_pend_in = false, g_pend_out = false;
+    const double* g_pcor_in = nullptr;
+    const double* g_pcor_out = nullptr;
+    double g_dtp_in = 0.0, g_dtp_out = 0.0;
     bool use_graphs = true;
     std::atomic<int>* cancel_flag = nullptr;   // serving: set to abandon a running request
     bool cancelled() const { return cancel_flag && cancel_flag->load(std::memory_order_relaxed) != 0; }
@@ -91,6 +95,8 @@ struct Ctx {
     // tables
     DevPlan plx, ply, plz;      // radix-16/8 schedules
     DevPlan plx4, ply4;         // radix-4 schedules (autotuner alternative)
+    DevPlan plx8, ply8;         // radix-8 schedules (autotuner alternative)
+    int plane_force = -1;       // PS3D_PLANE_IMPL: -1 free, 0 cluster, 1 rows + y-lines
     int kchunk = 8;             // z levels per block of the step kernel
     std::string tuned;          // description of the autotuned choice
     DevBuf twx;
@@ -106,6 +112,13 @@ struct Ctx {
     // time levels (main_module.f90:55-59)
     int itt = 0, tau = 3, taum1 = 2, taum2 = 1;
     double time = 0.0;
+    // pending pressure-gradient correction (lazy K5): the state arrays hold
+    // u'' and the true velocity is u'' - dtp*grad(*pcor); the next step's
+    // stencil kernel applies it while loading
+    bool pending = false;
+    const double* pcor = nullptr;
+    double dtp = 0.0;
+    bool lazy_correction = true;
     // per-kernel event timing (ps3d_profile)
     bool prof = false;
     struct ProfRec { int kid; cudaEvent_t e0, e1; };
@@ -146,8 +159,9 @@ struct Ctx {
     int capture_graph();
     void invalidate_graph() { ++version; }
     int step(int itt, int tau, int taum1, int taum2);
-    int poisson_once(double* out, double beta);
-    int pressure_solve();
+    int poisson_once(double* out, double beta, bool lazy = false);
+    int pressure_solve(bool lazy = false);
+    int materialize();        // apply a pending correction so the state arrays hold the true state
     int forward_transform(const double* const* in);
     int backward_transform(double* const* out);
     int project(int mode);

@@ -71,13 +71,16 @@ int Ctx::prof_read(double* ms, long long* count) {
 // FFT plans (host construction)
 // ---------------------------------------------------------------------------
 // Radix schedule of one transform length.  policy 0 prefers radix 16 and 8
-// (two register passes for 128 and 256 points), policy 1 stays at radix 4.
+// (two register passes for 128 and 256 points), policy 1 stays at radix 4,
+// policy 2 prefers radix 8 (fewer registers than 16 in FP64).
 static std::vector<int> radices_of(int n, int policy = 0) {
     std::vector<int> r;
     int m = n;
     if (policy == 0) {
         while (m % 16 == 0) { r.push_back(16); m /= 16; }
         if (m % 8 == 0) { r.push_back(8); m /= 8; }
+    } else if (policy == 2) {
+        while (m % 8 == 0) { r.push_back(8); m /= 8; }
     }
     while (m % 4 == 0) { r.push_back(4); m /= 4; }
     while (m % 2 == 0) { r.push_back(2); m /= 2; }
@@ -166,6 +169,19 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
             if (sm > 225 * 1024) continue;
             PlaneArgs a = base;
             a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rcc; a.ldr = ldr; a.ldc = ldc;
+            a.impl = 0;
+            out.push_back(a);
+        }
+    }
+    // rows pass + y-lines pass
+    for (int tj : {8, 16, 32}) {
+        if (ny % tj) continue;
+        if ((size_t)n2 * (tj | 1) * es > 200 * 1024) continue;
+        for (int ly : {8, 16, 32}) {
+            if ((size_t)ny * (ly | 1) * es > 200 * 1024) continue;
+            PlaneArgs a = base;
+            a.impl = 1; a.tj = tj; a.ly = ly;
+            a.C = 1; a.rows_per_cta = ny; a.cols_per_cta = nxh; a.row_chunk = 8; a.ldr = 9; a.ldc = nxh | 1;
             out.push_back(a);
         }
     }
@@ -187,6 +203,21 @@ static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
             const size_t sm = ((size_t)ny * ldc + (size_t)n2 * ldr) * es;
             if (sm > limit) continue;
             a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rc; a.ldr = ldr; a.ldc = ldc;
+            a.impl = 0; a.tj = 8; a.ly = 8;
+            return true;
+        }
+    }
+    return false;
+}
+
+// Default shape of the rows + y-lines plane kernels for one element size.
+static bool choose_split_config(int nx, int ny, size_t es, PlaneArgs& a) {
+    for (const PlaneArgs& c : plane_candidates(nx, ny, es, a)) {
+        if (c.impl != 1 || c.ly != 16) continue;
+        if (c.tj == 16 || (c.tj == 8 && ny % 16)) {
+            const FFTPlan px = a.px, py = a.py;
+            a = c;
+            a.px = px; a.py = py;
             return true;
         }
     }
@@ -231,6 +262,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     // plans and tables
     CK(plx.build(nx / 2, 0)); CK(ply.build(ny, 0)); CK(plz.build(rigid ? 1 : nz, 0));
     CK(plx4.build(nx / 2, 1)); CK(ply4.build(ny, 1));
+    CK(plx8.build(nx / 2, 2)); CK(ply8.build(ny, 2));
     {
         std::vector<double2> tw(nxh);
         for (int t = 0; t < nxh; ++t) tw[t] = twiddle_fwd(t, nx);
@@ -306,6 +338,14 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     pa64 = base; pa32 = base;
     if (!choose_plane_config(nx, ny, sizeof(double2), pa64)) return PS3D_ERR_BADPARAM;
     if (!choose_plane_config(nx, ny, sizeof(float2), pa32)) return PS3D_ERR_BADPARAM;
+    // PS3D_PLANE_IMPL=0|1 pins the plane implementation (cluster, or rows +
+    // y-lines) for the defaults and the autotuner; grids the rows + y-lines
+    // kernels cannot take keep the cluster kernels
+    if (const char* pi = std::getenv("PS3D_PLANE_IMPL")) plane_force = pi[0] == '1' ? 1 : pi[0] == '0' ? 0 : -1;
+    if (plane_force == 1) {
+        choose_split_config(nx, ny, sizeof(double2), pa64);
+        choose_split_config(nx, ny, sizeof(float2), pa32);
+    }
     kchunk = nz <= 16 ? nz : 8;
     // reductions
     nred = 148 * 4;
@@ -381,6 +421,15 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         for (int f = 0; f < 4; ++f) { a.wr[f] = (const double*)wr[f].p; a.wi[f] = (const double*)wi[f].p; }
     }
     const bool fused = !bih && !cb && !(bg && harm);
+    if (!fused) {
+        int rc = materialize();
+        if (rc) return rc;
+    }
+    if (fused && pending) {
+        a.pc = pcor;
+        a.dtp = dtp;
+        a.dtwp = dtp / P.dsqr;
+    }
     if (fused) {
         if (bg) { a.ub = (const double*)ub.p; a.bb = (const double*)bb.p; }
         int nxt[4];
@@ -390,6 +439,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         a.do_ab = 1;
         LAUNCH(PS3D_K_STEP, launch_step(a, mixed, stream));
         for (int f = 0; f < 4; ++f) cur[f] = nxt[f];
+        pending = false;   // consumed by the step kernel
     } else {
         if (mixed || batch > 1) return PS3D_ERR_UNSUPPORTED;   // generic path: FP64 tendencies, one grid
         int old[4], B[4], Cb[4];
@@ -450,8 +500,9 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         }
         LAUNCH(PS3D_K_OTHER, launch_wavemaker_ab(fa, wm ? 1 : 0, stream));
         for (int f = 0; f < 4; ++f) cur[f] = fin[f];
+        return pressure_solve(false);
     }
-    return pressure_solve();
+    return pressure_solve(lazy_correction);
 }
 
 // ---------------------------------------------------------------------------
@@ -498,16 +549,22 @@ int Ctx::autotune() {
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, dev));
     char key[256];
-    std::snprintf(key, sizeof key, "%s|%dx%dx%d|p%d|r%d|b%d", prop.name, nx, ny, nz, (int)mixed, (int)rigid, batch);
+    std::snprintf(key, sizeof key, "%s|%dx%dx%d|p%d|r%d|b%d|i%d", prop.name, nx, ny, nz, (int)mixed, (int)rigid, batch,
+                  plane_force);
     for (char* c = key; *c; ++c) if (*c == ' ') *c = '_';
     const bool f32 = mixed;
     PlaneArgs& pa = f32 ? pa32 : pa64;
-    auto apply = [&](int C, int rc, int pol, int kc) -> bool {
+    auto plans_of = [&](int pol, PlaneArgs& a) {
+        a.px = pol == 0 ? plx.plan : pol == 1 ? plx4.plan : plx8.plan;
+        a.py = pol == 0 ? ply.plan : pol == 1 ? ply4.plan : ply8.plan;
+    };
+    auto apply = [&](int im, int C, int rc, int tj, int ly, int pol, int kc) -> bool {
         for (const PlaneArgs& c : plane_candidates(nx, ny, f32 ? sizeof(float2) : sizeof(double2), pa)) {
-            if (c.C != C || c.row_chunk != rc) continue;
+            if (c.impl != im) continue;
+            if (im == 0 && (c.C != C || c.row_chunk != rc)) continue;
+            if (im == 1 && (c.tj != tj || c.ly != ly)) continue;
             pa = c;
-            pa.px = pol == 0 ? plx.plan : plx4.plan;
-            pa.py = pol == 0 ? ply.plan : ply4.plan;
+            plans_of(pol, pa);
             kchunk = kc;
             return true;
         }
@@ -515,8 +572,9 @@ int Ctx::autotune() {
     };
     auto it = tune_cache().find(key);
     if (it != tune_cache().end()) {
-        int C, rc, pol, kc;
-        if (std::sscanf(it->second.c_str(), "C%d,rc%d,pol%d,kc%d", &C, &rc, &pol, &kc) == 4 && apply(C, rc, pol, kc)) {
+        int im, C, rc, tj, ly, pol, kc;
+        if (std::sscanf(it->second.c_str(), "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d", &im, &C, &rc, &tj, &ly, &pol, &kc) == 7 &&
+            apply(im, C, rc, tj, ly, pol, kc)) {
             tuned = std::string("cached:") + it->second;
             return PS3D_OK;
         }
@@ -544,12 +602,12 @@ int Ctx::autotune() {
     PlaneArgs bestpa = pa;
     int bestpol = 0;
     for (const PlaneArgs& cand : plane_candidates(nx, ny, f32 ? sizeof(float2) : sizeof(double2), pa)) {
-        for (int pol = 0; pol < 2; ++pol) {
+        for (int pol = 0; pol < 3; ++pol) {
             PlaneArgs a = cand;
-            a.px = pol == 0 ? plx.plan : plx4.plan;
-            a.py = pol == 0 ? ply.plan : ply4.plan;
+            plans_of(pol, a);
             a.batch = batch;
-            if (plane_max_clusters(a, f32, true) < 1 || plane_max_clusters(a, f32, false) < 1) continue;
+            if (plane_force >= 0 && a.impl != plane_force) continue;
+            if (a.impl == 0 && (plane_max_clusters(a, f32, true) < 1 || plane_max_clusters(a, f32, false) < 1)) continue;
             const float t = timeit([&]() -> int {
                 PlaneArgs f = a;
                 f.mode = 0; f.u = field(0); f.v = field(1); f.w = field(2);
@@ -598,7 +656,8 @@ int Ctx::autotune() {
     cudaEventDestroy(e1);
     CK(cudaStreamSynchronize(stream));
     char val[128];
-    std::snprintf(val, sizeof val, "C%d,rc%d,pol%d,kc%d", pa.C, pa.row_chunk, bestpol, kchunk);
+    std::snprintf(val, sizeof val, "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d", pa.impl, pa.C, pa.row_chunk, pa.tj, pa.ly,
+                  bestpol, kchunk);
     tuned = val;
     tune_cache_store(key, val);
     return PS3D_OK;
@@ -627,6 +686,9 @@ int Ctx::capture_graph() {
     int cur0[4];
     for (int f = 0; f < 4; ++f) cur0[f] = cur[f];
     const long l0 = launches;
+    const bool pend0 = pending;
+    const double* pcor0 = pcor;
+    const double dtp0 = dtp;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     int rc = PS3D_OK;
@@ -636,8 +698,10 @@ int Ctx::capture_graph() {
         ++itt;
     }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
+    g_pend_out = pending; g_pcor_out = pcor; g_dtp_out = dtp;
     itt = itt0; tau = tau0; taum1 = t10; taum2 = t20;
     for (int f = 0; f < 4; ++f) cur[f] = cur0[f];
+    pending = pend0; pcor = pcor0; dtp = dtp0;
     g_launches = launches - l0;
     launches = l0;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -646,13 +710,15 @@ int Ctx::capture_graph() {
     cudaGraphDestroy(g);
     CK(e);
     g_tau = tau; g_cur = cur[0]; g_version = version;
+    g_pend_in = pending; g_pcor_in = pcor; g_dtp_in = dtp;
     return PS3D_OK;
 }
 
 int Ctx::advance(int nsteps, bool allow_graph) {
     while (nsteps > 0) {
         if (allow_graph && nsteps >= 3 && itt >= 2 && graphable()) {
-            if (!gexec || g_tau != tau || g_cur != cur[0] || g_version != version) {
+            if (!gexec || g_tau != tau || g_cur != cur[0] || g_version != version || g_pend_in != pending ||
+                g_pcor_in != pcor || g_dtp_in != dtp) {
                 int rc = capture_graph();
                 if (rc) return rc;
             }
@@ -663,6 +729,7 @@ int Ctx::advance(int nsteps, bool allow_graph) {
                 time = time + P.dt;
                 ++itt;
             }
+            pending = g_pend_out; pcor = g_pcor_out; dtp = g_dtp_out;
             launches += g_launches;
             nsteps -= 3;
             continue;
@@ -680,7 +747,7 @@ int Ctx::advance(int nsteps, bool allow_graph) {
 // ---------------------------------------------------------------------------
 // pressure_solver (pressure_solver.f90:2-120)
 // ---------------------------------------------------------------------------
-int Ctx::poisson_once(double* out, double beta) {
+int Ctx::poisson_once(double* out, double beta, bool lazy) {
     const bool f32 = mixed;
     PlaneArgs a = f32 ? pa32 : pa64;
     a.batch = batch;
@@ -692,7 +759,7 @@ int Ctx::poisson_once(double* out, double beta) {
     LAUNCH(PS3D_K_FFT_FWD, launch_plane_fwd(a, f32, stream));
     ColumnArgs c{};
     c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = FS.p;
-    c.batch = batch; c.sM = M;
+    c.batch = batch; c.sM = M; c.layout = a.impl;
     c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p; c.hkz = (const double*)t_hkz_ds.p;
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
@@ -709,21 +776,39 @@ int Ctx::poisson_once(double* out, double beta) {
     b.beta = beta;
     b.scale = rigid ? 1.0 / (P.Lx * P.Ly) : 1.0 / (P.Lx * P.Ly * P.Lz);
     LAUNCH(PS3D_K_FFT_INV, launch_plane_inv(b, f32, stream));
+    if (lazy) {
+        pending = true;
+        pcor = out;
+        dtp = P.dt;
+        return PS3D_OK;
+    }
     LAUNCH(PS3D_K_CORRECT, launch_correct(field(0), field(1), field(2), out, nx, ny, nz, rigid, P.dt, P.dt / P.dsqr,
                       1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, stream, batch));
     return PS3D_OK;
 }
 
-int Ctx::pressure_solve() {
-    int rc = poisson_once((double*)p.p, 0.0);
-    if (rc) return rc;
-    if (mixed) {
-        // one FP64-residual refinement: the divergence of the corrected
-        // velocity is solved again and its pressure added to p
-        rc = poisson_once((double*)p2.p, 0.0);
-        if (rc) return rc;
+int Ctx::materialize() {
+    if (!pending) return PS3D_OK;
+    LAUNCH(PS3D_K_CORRECT, launch_correct(field(0), field(1), field(2), pcor, nx, ny, nz, rigid, dtp, dtp / P.dsqr,
+                      1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, stream, batch));
+    if (mixed && pcor == (const double*)p2.p)
         LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N * batch, 1.0, 1.0, stream));
-    }
+    pending = false;
+    return PS3D_OK;
+}
+
+int Ctx::pressure_solve(bool lazy) {
+    int rc = materialize();
+    if (rc) return rc;
+    if (!mixed) return poisson_once((double*)p.p, 0.0, lazy);
+    // one FP64-residual refinement: the divergence of the corrected velocity
+    // is solved again and its pressure added to p (lazily: p += p2 when the
+    // state is next observed; the next step applies the p2 correction)
+    rc = poisson_once((double*)p.p, 0.0, false);
+    if (rc) return rc;
+    rc = poisson_once((double*)p2.p, 0.0, lazy);
+    if (rc) return rc;
+    if (!lazy) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N * batch, 1.0, 1.0, stream));
     return PS3D_OK;
 }
 
@@ -744,7 +829,7 @@ int Ctx::forward_transform(const double* const* in) {
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
-            c.batch = 1; c.sM = M;
+            c.batch = 1; c.sM = M; c.layout = pa64.impl;
             c.pz = plz.plan; c.scale = P.dz; c.op = 1;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -762,7 +847,7 @@ int Ctx::backward_transform(double* const* out) {
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
-            c.batch = 1; c.sM = M;
+            c.batch = 1; c.sM = M; c.layout = pa64.impl;
             c.pz = plz.plan; c.scale = 1.0; c.op = 2;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -776,11 +861,15 @@ int Ctx::backward_transform(double* const* out) {
 
 int Ctx::project(int mode) {
     if (mode < 0 || mode > 3) return PS3D_ERR_BADPARAM;
+    {
+        int rc = materialize();
+        if (rc) return rc;
+    }
     const double* in[4] = {field(0), field(1), field(2), field(3)};
     int rc = forward_transform(in);
     if (rc) return rc;
     ProjArgs a{};
-    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid;
+    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid; a.layout = pa64.impl;
     a.dx = P.dx; a.dy = P.dy; a.dz = P.dz; a.f0 = P.f0; a.N0 = P.N0; a.dsqr = P.dsqr;
     a.ax.kx = (const double*)t_kx.p; a.ax.ky = (const double*)t_ky.p; a.ax.kz = (const double*)t_kz.p;
     a.ax.hkx = (const double*)t_hkx.p; a.ax.hky = (const double*)t_hky.p; a.ax.hkz = (const double*)t_hkz.p;
@@ -807,6 +896,10 @@ int Ctx::project(int mode) {
 // diagnose (diagnose.F90:2-61)
 // ---------------------------------------------------------------------------
 int Ctx::diagnose(double* ke, double* pe, double* umax, double* wmax) {
+    {
+        int rc = materialize();
+        if (rc) return rc;
+    }
     DiagOut* d = (DiagOut*)red_out.p;
     LAUNCH(PS3D_K_OTHER, launch_diagnose(field(0), field(1), field(2), field(3), (const double*)p.p, nx, ny, nz, P.dsqr, P.N0, P.dz,
                        (double*)red_partials.p, nred, d, stream));
@@ -824,6 +917,7 @@ int Ctx::diagnose(double* ke, double* pe, double* umax, double* wmax) {
 // field-set helpers for the balance drivers
 // ---------------------------------------------------------------------------
 cudaError_t Ctx::copy_state_to(int set) {
+    if (materialize() != PS3D_OK) return cudaErrorUnknown;
     cudaError_t e = ensure_fieldset(set);
     if (e) return e;
     DevBuf* s = fieldset(set);
@@ -832,6 +926,7 @@ cudaError_t Ctx::copy_state_to(int set) {
     return cudaSuccess;
 }
 cudaError_t Ctx::copy_set_to_state(int set) {
+    pending = false;   // the state arrays now hold a true state
     DevBuf* s = fieldset(set);
     cudaError_t e;
     for (int f = 0; f < 4; ++f)
@@ -857,6 +952,8 @@ int Ctx::opt_time_ave(int set, int n_end_ave) {
         int rc = step(itt, tau, taum1, taum2);
         if (rc) return rc;
         rotate();
+        rc = materialize();
+        if (rc) return rc;
         for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, field(f), N, 1.0, 1.0, stream));
     }
     for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, nullptr, N, 1.0 / n_end_ave, 0.0, stream));
@@ -941,6 +1038,8 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
         }
         // opt_balance_norm (:339-362)
         {
+            rc = materialize();
+            if (rc) break;
             DevBuf* bl = fieldset(PS3D_FIELDS_BALANCED);
             const double* x[4] = {field(0), field(1), field(2), field(3)};
             const double* y[4] = {(const double*)bl[0].p, (const double*)bl[1].p, (const double*)bl[2].p, (const double*)bl[3].p};
@@ -1139,9 +1238,10 @@ int ps3d_upload_state(ps3d_ctx* ctx, const double* u, const double* v, const dou
     if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
     Ctx& C = ctx->impl;
     if (tau < 1 || tau > 3 || taum1 < 1 || taum1 > 3 || taum2 < 1 || taum2 > 3 || itt < 0) return PS3D_ERR_BADPARAM;
+    int rc = C.materialize(); if (rc) return rc;   // fields not uploaded keep their true values
     const double* f[4] = {u, v, w, b};
-    for (int q = 0; q < 4; ++q) { int rc = C.upload_field(C.field(q), f[q]); if (rc) return rc; }
-    int rc = C.upload_field((double*)C.p.p, p); if (rc) return rc;
+    for (int q = 0; q < 4; ++q) { rc = C.upload_field(C.field(q), f[q]); if (rc) return rc; }
+    rc = C.upload_field((double*)C.p.p, p); if (rc) return rc;
     const double* t[4] = {du, dv, dw, db};
     for (int q = 0; q < 4; ++q) { rc = C.upload_tend(q, t[q]); if (rc) return rc; }
     C.itt = itt; C.tau = tau; C.taum1 = taum1; C.taum2 = taum2;
@@ -1154,9 +1254,10 @@ int ps3d_download_state(ps3d_ctx* ctx, double* u, double* v, double* w, double* 
     GUARD_BEGIN
     if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
     Ctx& C = ctx->impl;
+    int rc = C.materialize(); if (rc) return rc;
     double* f[4] = {u, v, w, b};
-    for (int q = 0; q < 4; ++q) { int rc = C.download_field(C.field(q), f[q], 0); if (rc) return rc; }
-    int rc = C.download_field((const double*)C.p.p, p, 1); if (rc) return rc;
+    for (int q = 0; q < 4; ++q) { rc = C.download_field(C.field(q), f[q], 0); if (rc) return rc; }
+    rc = C.download_field((const double*)C.p.p, p, 1); if (rc) return rc;
     double* t[4] = {du, dv, dw, db};
     for (int q = 0; q < 4; ++q) { rc = C.download_tend(q, t[q]); if (rc) return rc; }
     if (itt) *itt = C.itt;
@@ -1232,6 +1333,7 @@ int ps3d_get_fields(ps3d_ctx* ctx, int which, double* u, double* v, double* w, d
     GUARD_BEGIN
     if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
     Ctx& C = ctx->impl;
+    { int rc = C.materialize(); if (rc) return rc; }
     double* out[4] = {u, v, w, b};
     for (int q = 0; q < 4; ++q) {
         const double* src;
@@ -1284,9 +1386,10 @@ int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
     if (!ctx || !buf || len < 1) return PS3D_ERR_BADPARAM;
     const Ctx& C = ctx->impl;
     const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
-    std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_cluster=%d row_chunk=%d fft_x=%d stages fft_y=%d stages "
-                  "kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.mixed ? "mixed" : "fp64", C.batch, pa.C, pa.row_chunk,
-                  pa.px.nst, pa.py.nst, C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
+    std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_impl=%s plane_cluster=%d row_chunk=%d tj=%d ly=%d "
+                  "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.mixed ? "mixed" : "fp64",
+                  C.batch, pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
+                  C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
     return PS3D_OK;
 }
 

@@ -32,6 +32,10 @@ struct StepArgs {
     int batch;                     // instances of the same grid stepped together (>= 1)
     long sN;                       // element stride between instances (fields and tendency slots)
     int kchunk;                    // z levels per block (autotuned)
+    // pending pressure correction of the previous step (NULL: state is final):
+    // the state arrays hold u'' and the true velocity is u'' - dtp*grad(pc)
+    const double* pc;
+    double dtp, dtwp;
 };
 
 // Plane-FFT kernels (divergence + forward 2D FFT, inverse 2D FFT) for one grid.
@@ -52,6 +56,9 @@ struct PlaneArgs {
     const double2* twx;            // exp(-2 pi i t/nx), t = 0..nx/2
     int batch;                     // instances (>= 1): grid.y = nz*batch
     long sN, sM;                   // instance strides: real fields, spectral elements
+    int impl;                      // 0: one cluster per plane (DSMEM), 1: rows pass + y-lines pass
+    int tj;                        // impl 1: rows per CTA of the rows passes
+    int ly;                        // impl 1: lines per CTA of the y-lines passes
 };
 
 struct ColumnArgs {
@@ -67,6 +74,7 @@ struct ColumnArgs {
     int op;                        // periodic: 0 solve, 1 forward only, 2 inverse only
     int batch;                     // instances (>= 1), spectral stride sM elements
     long sM;
+    int layout;                    // spectral layout: 0 [k][ky][kx], 1 [k][kx][ky]
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
@@ -101,6 +109,7 @@ struct EigenAxes {
 };
 struct ProjArgs {
     int nxh, ny, nz, rigid;
+    int layout;                    // spectral layout: 0 [k][ky][kx], 1 [k][kx][ky]
     double dx, dy, dz, f0, N0, dsqr;
     EigenAxes ax;
     double2 *US, *VS, *WS, *BS;

@@ -54,11 +54,11 @@ bool all_graphable(ps3d_ensemble* e) {
 
 int capture(ps3d_ensemble* e) {
     if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
-    struct Book { int itt, tau, t1, t2, cur[4]; double time; long long launches; };
+    struct Book { int itt, tau, t1, t2, cur[4]; double time; long long launches; bool pend; const double* pcor; double dtp; };
     std::vector<Book> saved;
     for (auto& g : e->groups)
         saved.push_back({g->itt, g->tau, g->taum1, g->taum2, {g->cur[0], g->cur[1], g->cur[2], g->cur[3]}, g->time,
-                         g->launches});
+                         g->launches, g->pending, g->pcor, g->dtp});
     const int itt0 = e->itt;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PS3D_ERR_CUDA;
@@ -72,6 +72,9 @@ int capture(ps3d_ensemble* e) {
         for (int f = 0; f < 4; ++f) g.cur[f] = saved[q].cur[f];
         g.time = saved[q].time;
         g.launches = saved[q].launches;
+        g.g_pend_out = g.pending; g.g_pcor_out = g.pcor; g.g_dtp_out = g.dtp;
+        g.pending = saved[q].pend; g.pcor = saved[q].pcor; g.dtp = saved[q].dtp;
+        g.g_pend_in = g.pending; g.g_pcor_in = g.pcor; g.g_dtp_in = g.dtp;
     }
     e->itt = itt0;
     if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -86,7 +89,10 @@ int capture(ps3d_ensemble* e) {
 int advance(ps3d_ensemble* e, int nsteps) {
     while (nsteps > 0) {
         if (nsteps >= 3 && e->itt >= 2 && all_graphable(e)) {
-            if (!e->graph_valid) {
+            bool same = true;
+            for (auto& g : e->groups)
+                same = same && g->g_pend_in == g->pending && g->g_pcor_in == g->pcor && g->g_dtp_in == g->dtp;
+            if (!e->graph_valid || !same) {
                 int rc = capture(e);
                 if (rc) return rc;
             }
@@ -98,7 +104,10 @@ int advance(ps3d_ensemble* e, int nsteps) {
                     g->time = g->time + g->P.dt;
                     ++g->itt;
                 }
-            for (auto& g : e->groups) g->launches += g->g_launches;
+            for (auto& g : e->groups) {
+                g->launches += g->g_launches;
+                g->pending = g->g_pend_out; g->pcor = g->g_pcor_out; g->dtp = g->g_dtp_out;
+            }
             e->itt += 3;
             nsteps -= 3;
             continue;
@@ -164,6 +173,8 @@ PS3D_API int ps3d_ensemble_upload(ps3d_ensemble* e, int member, const double* u,
     cudaSetDevice(e->device);
     Ctx& g = *e->groups[e->where[member].first];
     const int m = e->where[member].second;
+    { int rc = g.materialize(); if (rc) return rc; }
+    e->graph_valid = false;
     const double* f[4] = {u, v, w, b};
     for (int q = 0; q < 4; ++q) {
         int rc = g.upload_field(g.member_field(q, m), f[q]);
@@ -180,6 +191,8 @@ PS3D_API int ps3d_ensemble_download(ps3d_ensemble* e, int member, double* u, dou
     cudaSetDevice(e->device);
     Ctx& g = *e->groups[e->where[member].first];
     const int m = e->where[member].second;
+    { int rc = g.materialize(); if (rc) return rc; }
+    e->graph_valid = false;
     double* f[4] = {u, v, w, b};
     for (int q = 0; q < 4; ++q) {
         int rc = g.download_field(g.member_field(q, m), f[q], 0);

@@ -149,8 +149,8 @@ __global__ void k_project(const ProjArgs a) {
     const long M = (long)a.nxh * a.ny * a.nz;
     const Phys P{a.f0, a.N0, a.dsqr, a.dz};
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < M; t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % a.nxh);
-        const int j = (int)((t / a.nxh) % a.ny);
+        const int i = a.layout ? (int)((t / a.ny) % a.nxh) : (int)(t % a.nxh);
+        const int j = a.layout ? (int)(t % a.ny) : (int)((t / a.nxh) % a.ny);
         const int k = (int)(t / ((long)a.nxh * a.ny));
         Ax x{a.ax.kx[i], a.ax.hkx[i], a.ax.ex[i], ld(a.ax.px + i), a.dx};
         Ax y{a.ax.ky[j], a.ax.hky[j], a.ax.ey[j], ld(a.ax.py + j), a.dy};

@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(128) k_thomas(const ColumnArgs a) {
     const long c = cg_ - inst * ncols;
     T* spec = reinterpret_cast<T*>(a.spec) + inst * a.sM;
     const int nz = a.nz;
-    const int i = (int)(c % a.nxh), j = (int)(c / a.nxh);
+    const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
+    const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
     const double ks = a.hkx[i] + a.hky[j];
     const double fxa = a.fxa;
     if (ks > 0) {
@@ -302,7 +303,8 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
             T v = cscale(buf[p * ld + l], sc);
             if (a.op == 0) {
                 const long c = c0 + l;
-                const int i = (int)(c % a.nxh), j = (int)(c / a.nxh);
+                const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
+                const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
                 const int k = a.pz.ipos[p];
                 const double ks = a.hkx[i] + a.hky[j] + a.hkz[k];
                 if (ks > 0.0) { v.x = (R)(-(double)v.x / ks); v.y = (R)(-(double)v.y / ks); }
@@ -321,8 +323,159 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Plane transforms, second implementation: a rows pass and a y-lines pass.
+// The spectral array is [k][kx][ky], so every kx line is contiguous in ky:
+// the rows pass writes each kx as one coalesced run of tj rows, the y-lines
+// pass loads and stores whole lines, and the vertical solves read columns
+// with consecutive threads on consecutive ky.  The intermediate makes one
+// extra trip through memory (largely L2-resident), in exchange for
+// independent CTAs with small shared memory and no cluster barriers.
+// Digit-reversed data are always read in shared-memory order and scattered
+// to global memory instead, which keeps the shared-memory accesses free of
+// bank conflicts.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256, 2) k_rows_fwd(const PlaneArgs a) {
+    using T = cpx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
+    const int tj = a.tj, ld = tj | 1;
+    const int jb = blockIdx.x * tj;
+    const int inst = blockIdx.y / nz;
+    const int k = blockIdx.y - inst * nz;
+    const long ioff = (long)inst * a.sN;
+    const long plane = (long)nx * ny;
+    const double* au = a.u + ioff;
+    const double* av = a.v + ioff;
+    const double* aw = a.w + ioff;
+    const double* asrc = a.src ? a.src + ioff : nullptr;
+    for (int t = threadIdx.x; t < tj * n2; t += blockDim.x) {
+        const int rr = t / n2, m = t - rr * n2;
+        const int j = jb + rr;
+        const long g = (long)k * plane + (long)j * nx + 2 * m;
+        double d0, d1;
+        if (a.mode == 0) {
+            const double2 uu = *reinterpret_cast<const double2*>(au + g);
+            const double um = au[g - 2 * m + wrap(2 * m - 1, nx)];
+            const long gv = g + (long)(wrap(j - 1, ny) - j) * nx;
+            const long gw = g + (long)(wrap(k - 1, nz) - k) * plane;
+            const double2 vv = *reinterpret_cast<const double2*>(av + g);
+            const double2 vm = *reinterpret_cast<const double2*>(av + gv);
+            const double2 ww = *reinterpret_cast<const double2*>(aw + g);
+            const double2 wm = *reinterpret_cast<const double2*>(aw + gw);
+            d0 = ((uu.x - um) * a.rdx + (vv.x - vm.x) * a.rdy + (ww.x - wm.x) * a.rdz) * a.rdt;
+            d1 = ((uu.y - uu.x) * a.rdx + (vv.y - vm.y) * a.rdy + (ww.y - wm.y) * a.rdz) * a.rdt;
+        } else {
+            const double2 sv = *reinterpret_cast<const double2*>(asrc + g);
+            d0 = sv.x; d1 = sv.y;
+        }
+        buf[m * ld + rr] = mk<R>((R)d0, (R)d1);
+    }
+    fft_batch<false, R>(buf, ld, tj, a.px, -1);
+    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
+    for (int t = threadIdx.x; t < tj * (n2 + 1); t += blockDim.x) {
+        const int kx = t / tj, rr = t - kx * tj;
+        const int k1 = (kx == n2) ? 0 : kx;
+        const int k2 = (kx == 0) ? 0 : n2 - kx;
+        const T Zk = buf[a.px.pos[k1] * ld + rr];
+        const T Zc = cconj(buf[a.px.pos[k2] * ld + rr]);
+        const T E = cscale(cadd(Zk, Zc), (R)0.5);
+        const T H = cscale(cmul_si(csub(Zk, Zc), -1), (R)0.5);
+        const double2 wd = __ldg(a.twx + kx);
+        spec[(long)kx * ny + jb + rr] = cadd(E, cmul(mk<R>((R)wd.x, (R)wd.y), H));
+    }
+}
+
+// one y transform of every kx line of a plane, in place on [k][kx][ky]
+template <typename R>
+__global__ void __launch_bounds__(256, 2) k_ylines(const PlaneArgs a, int sign, double scale) {
+    using T = cpx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    const int ny = a.ny, nz = a.nz, nxh = a.nxh;
+    const int ly = a.ly, ld = ly | 1;
+    const int inst = blockIdx.y / nz;
+    const int k = blockIdx.y - inst * nz;
+    const int l0 = blockIdx.x * ly;
+    const int nl = min(ly, nxh - l0);
+    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + ((long)k * nxh + l0) * ny;
+    for (int t = threadIdx.x; t < nl * ny; t += blockDim.x) {
+        const int line = t / ny, e = t - line * ny;
+        buf[e * ld + line] = spec[(long)line * ny + e];
+    }
+    fft_batch<false, R>(buf, ld, nl, a.py, sign);
+    const R sc = (R)scale;
+    for (int t = threadIdx.x; t < nl * ny; t += blockDim.x) {
+        const int line = t / ny, q = t - line * ny;   // q: position in shared memory
+        spec[(long)line * ny + a.py.ipos[q]] = cscale(buf[q * ld + line], sc);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, 2) k_rows_inv(const PlaneArgs a) {
+    using T = cpx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
+    const int tj = a.tj, ld = tj | 1;
+    const int jb = blockIdx.x * tj;
+    const int inst = blockIdx.y / nz;
+    const int k = blockIdx.y - inst * nz;
+    const long plane = (long)nx * ny;
+    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
+    double* out = a.out + (long)inst * a.sN;
+    for (int t = threadIdx.x; t < tj * n2; t += blockDim.x) {
+        const int kk = t / tj, rr = t - kk * tj;
+        T Xk = spec[(long)kk * ny + jb + rr];
+        T Xc = spec[(long)(n2 - kk) * ny + jb + rr];
+        if (kk == 0) { Xk.y = (R)0; Xc.y = (R)0; }   // c2r ignores Im of DC and Nyquist
+        Xc = cconj(Xc);
+        const double2 wd = __ldg(a.twx + kk);
+        const T wb = mk<R>((R)wd.x, (R)-wd.y);
+        buf[kk * ld + rr] = cadd(cadd(Xk, Xc), cmul_si(cmul(wb, csub(Xk, Xc)), +1));
+    }
+    fft_batch<false, R>(buf, ld, tj, a.px, +1);
+    const double sc = a.scale;
+    for (int t = threadIdx.x; t < tj * n2; t += blockDim.x) {
+        const int rr = t / n2, q = t - rr * n2;
+        const int m = a.px.ipos[q];
+        const T z = buf[q * ld + rr];
+        const long g = (long)k * plane + (long)(jb + rr) * nx + 2 * m;
+        double2 o = make_double2((double)z.x * sc, (double)z.y * sc);
+        if (a.beta != 0.0) {
+            const double2 prev = *reinterpret_cast<const double2*>(out + g);
+            o.x = o.x + a.beta * prev.x; o.y = o.y + a.beta * prev.y;
+        }
+        *reinterpret_cast<double2*>(out + g) = o;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+size_t rows_smem(const PlaneArgs& a, bool fp32) {
+    return (size_t)(a.nx / 2) * (a.tj | 1) * (fp32 ? sizeof(float2) : sizeof(double2));
+}
+size_t ylines_smem(const PlaneArgs& a, bool fp32) {
+    return (size_t)a.ny * (a.ly | 1) * (fp32 ? sizeof(float2) : sizeof(double2));
+}
+
+template <typename R>
+static cudaError_t launch_split_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
+    const int nb = std::max(1, a.batch);
+    const dim3 grows(a.ny / a.tj, a.nz * nb), glines((a.nxh + a.ly - 1) / a.ly, a.nz * nb);
+    const size_t smr = rows_smem(a, sizeof(R) == 4), sml = ylines_smem(a, sizeof(R) == 4);
+    if (fwd) {
+        k_rows_fwd<R><<<grows, 256, smr, s>>>(a);
+        k_ylines<R><<<glines, 256, sml, s>>>(a, -1, a.scale);
+    } else {
+        k_ylines<R><<<glines, 256, sml, s>>>(a, +1, 1.0);
+        k_rows_inv<R><<<grows, 256, smr, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 size_t plane_fwd_smem(const PlaneArgs& a, bool fp32) {
     const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
     return ((size_t)a.ny * a.ldc + (size_t)(a.nx / 2) * a.ldr) * es;
@@ -338,6 +491,9 @@ static cudaError_t setup_t() {
     if ((e = cudaFuncSetAttribute(k_plane_fwd<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
     if ((e = cudaFuncSetAttribute(k_plane_inv<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_fwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_inv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_ylines<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
     return cudaSuccess;
 }
 cudaError_t plane_setup(bool fp32) { return fp32 ? setup_t<float>() : setup_t<double>(); }
@@ -384,9 +540,11 @@ int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd) {
 }
 
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s) {
+    if (a.impl == 1) return fp32 ? launch_split_t<float>(a, true, s) : launch_split_t<double>(a, true, s);
     return fp32 ? launch_plane_t<float, true>(a, s) : launch_plane_t<double, true>(a, s);
 }
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
+    if (a.impl == 1) return fp32 ? launch_split_t<float>(a, false, s) : launch_split_t<double>(a, false, s);
     return fp32 ? launch_plane_t<float, false>(a, s) : launch_plane_t<double, false>(a, s);
 }
 

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
     const int tid = ty * kTX + tx;
     constexpr int TP = (kTX + 2) * (BY + 2);
 
+    const double* pc = a.pc ? a.pc + ioff : nullptr;
     auto load_plane = [&](int kk, int slot) {
         const int kw = wrap(kk, nz);
         for (int t = tid; t < TP; t += kTX * BY) {
@@ -57,6 +58,21 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
             const long g = (long)kw * plane + (long)gj * nx + gi;
 #pragma unroll
             for (int f = 0; f < NF; ++f) sm.pl[f][slot][t] = __ldg(src[f] + g);
+            if (pc) {
+                // the previous step's pressure-gradient correction
+                // (pressure_solver.f90:98-110), applied where the state is read
+                const double p0 = __ldg(pc + g);
+                const double pe = __ldg(pc + g - gi + wrap(gi + 1, nx));
+                const double pn = __ldg(pc + g + (long)(wrap(gj + 1, ny) - gj) * nx);
+                sm.pl[0][slot][t] = sm.pl[0][slot][t] - a.dtp * (pe - p0) * a.rdx;
+                sm.pl[1][slot][t] = sm.pl[1][slot][t] - a.dtp * (pn - p0) * a.rdy;
+                if (a.rigid && kw == nz - 1) {
+                    sm.pl[2][slot][t] = 0.0;
+                } else {
+                    const double pt = __ldg(pc + g + (long)(wrap(kw + 1, nz) - kw) * plane);
+                    sm.pl[2][slot][t] = sm.pl[2][slot][t] - a.dtwp * (pt - p0) * a.rdz;
+                }
+            }
         }
     };
 

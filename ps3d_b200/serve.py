@@ -111,8 +111,12 @@ SIZES = [(64, 64, 32), (64, 64, 64), (128, 128, 32), (128, 128, 64), (256, 256, 
 def request(nx, ny, nz, precision=abi.PS3D_FP64, ramp_steps=100, iters=5):
     """One opt-balance request on the eddy initial state (for_config/eddy1.f90
     template): ramp of n_end = int(T/dt)+1 = ramp_steps steps, `iters`
-    iterations, tolerance 0 so that all iterations run."""
+    iterations, tolerance 0 so that all iterations run.  No harmonic friction,
+    as in for_config/test_opt_balance.f90: the backward integration runs with
+    dt < 0 and keeps harmonic friction on (diag_opt_balance.f90:190-192 only
+    switches the biharmonic terms off), which would make it anti-diffusive."""
     p = cf.eddy_params(nx, ny, nz, precision=precision)
+    p.Ah = p.Av = p.Kh = p.Kv = 0.0
     f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=0)
     opt = OptBal(period=(ramp_steps - 0.5) * p.dt, average=0.0, max_itts=iters, average_times=1,
                  tol=0.0, enable_time_ave=0, adopt=0)
@@ -147,6 +151,11 @@ def replay_poisson(server, schedule, precision=abi.PS3D_FP64, ramp_steps=100, it
     ok = [r for r in results if r.status == 0]
     steps = sum(2 * r.iters * ramp_steps for r in ok)
     pts = sum(2 * r.iters * ramp_steps * np.prod(s) for (_, s), r in zip(schedule, results) if r.status == 0)
-    return {"requests": len(results), "ok": len(ok), "p50_ms": float(np.percentile(lat, 50)),
+    failed = {}
+    for (_, size), r in zip(schedule, results):
+        if r.status != 0:
+            key = f"{size[0]}x{size[1]}x{size[2]}:{r.status}"
+            failed[key] = failed.get(key, 0) + 1
+    return {"requests": len(results), "ok": len(ok), "failed": failed, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "wall_s": wall,
             "throughput_req_s": len(ok) / wall, "grid_point_steps_s": float(pts / wall), "steps": steps}

@@ -22,6 +22,14 @@ TOL_KERNEL = 1e-12
 TOL_MIXED = 1e-5
 
 
+@pytest.fixture(autouse=True, params=["cluster", "rows+lines"])
+def plane_impl(request, monkeypatch):
+    """Every parity case runs on both plane-transform implementations: the
+    one-cluster-per-plane kernels and the rows pass + y-lines pass."""
+    monkeypatch.setenv("PS3D_PLANE_IMPL", "0" if request.param == "cluster" else "1")
+    return request.param
+
+
 def _pair(p, fields, pfield=None):
     o = Oracle(p)
     load_oracle(o, fields, pfield)
@@ -31,10 +39,11 @@ def _pair(p, fields, pfield=None):
 
 
 @pytest.mark.parametrize("rigid", [True, False])
-@pytest.mark.parametrize("shape", [(32, 32, 16), (48, 40, 12)])
-def test_pressure_solver(rigid, shape):
+@pytest.mark.parametrize("shape", [(32, 32, 16), (48, 40, 12), (256, 256, 8), (128, 64, 8), (64, 256, 4)])
+def test_pressure_solver(rigid, shape, plane_impl):
     p = small_params(*shape, rigid=rigid)
     o, m = _pair(p, random_state(p, seed=1))
+    assert "plane_impl=" + plane_impl in m.describe()
     o.pressure_solver()
     m.pressure_solver()
     err = compare_state(m, o)
@@ -225,6 +234,44 @@ def test_diagnose_and_nonfinite():
     with pytest.raises(PS3DError) as ei:
         m.diagnose()
     assert ei.value.status == abi.PS3D_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("precision", [abi.PS3D_FP64, abi.PS3D_MIXED])
+def test_long_lines_steps(precision):
+    """FFT lengths 128 (radix 16 x 8) and 256 (16 x 16) in a short run."""
+    p = small_params(256, 256, 16, rigid=True, Lx=256e3, Ly=256e3)
+    p.precision = precision
+    p64 = p.copy()
+    p64.precision = abi.PS3D_FP64
+    o = Oracle(p64)
+    load_oracle(o, smooth_state(p64, seed=21))
+    m = Model(p)
+    upload_from_oracle(m, o)
+    o.integrate(6)
+    m.run(6)
+    err = compare_state(m, o)
+    assert max(err.values()) < (TOL64 if precision == abi.PS3D_FP64 else TOL_MIXED), err
+
+
+def test_lazy_correction_observers():
+    """The pressure-gradient correction is applied by the next step's stencil
+    kernel; every observer (download, diagnose, projection, a later explicit
+    pressure solve) must see the corrected state."""
+    p = small_params(32, 32, 16)
+    o, m = _pair(p, smooth_state(p, seed=22))
+    o.integrate(5)
+    m.run(5)
+    st, ke, pe, um, wm = o.diagnose()
+    ke2, pe2, um2, wm2 = m.diagnose()
+    assert abs(ke2 - ke) <= 1e-12 * ke and abs(um2 - um) <= 1e-12 * um
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL64, err
+    o.integrate(3)
+    m.run(3)
+    o.project(abi.PS3D_PROJ_NORMAL_MODE)
+    m.project(abi.PS3D_PROJ_NORMAL_MODE)
+    err = compare_state(m, o, names=FIELDS)
+    assert max(err.values()) < TOL64, err
 
 
 def test_mixed_precision_200_steps():
