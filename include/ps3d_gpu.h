@@ -44,6 +44,7 @@ extern "C" {
 #define PS3D_ERR_BADPARAM     -5  /* invalid argument, size or configuration        */
 #define PS3D_ERR_UNSUPPORTED  -6  /* valid in the reference, not built here         */
 #define PS3D_ERR_CANCELLED    -7  /* a serving request was cancelled                */
+#define PS3D_ERR_TOOLARGE     -8  /* grid exceeds ps3d_pressure_solve_noalloc's static scratch */
 
 /* ---- parameters (for_src/main_module.f90:16-57) -------------------------- */
 typedef struct ps3d_params {
@@ -218,6 +219,24 @@ PS3D_API int ps3d_profile(ps3d_ctx* ctx, int enable);
  * precision, plane cluster shape, FFT stages, autotuner choice).          */
 PS3D_API int ps3d_describe(ps3d_ctx* ctx, char* buf, int len);
 PS3D_API int ps3d_profile_read(ps3d_ctx* ctx, double* ms, long long* launches);
+
+/* ---- pressure projection without device allocation -----------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they need the projection (they own their device arrays through CUDA
+ * Fortran, OpenACC or their own pool, must not allocate inside a locked or
+ * captured region, or must keep a fixed device footprint): the same
+ * computation as ps3d_pressure_solve (pressure_solver.f90:2-120, FP64) on the
+ * caller's device arrays u, v, w (updated in place) and p (written), each
+ * nx*ny*nz doubles, x fastest, interior points only, queued on `stream`
+ * (a cudaStream_t, NULL for the default stream) and waited for.  The
+ * spectral work array and the FFT tables are file-scope static device arrays
+ * (about 16.1 MiB, held on every GPU that loads the library until exit):
+ * (nx/2+1)*ny*nz must not exceed 1048576 and nx/2, ny, nz not 1024, else
+ * PS3D_ERR_TOOLARGE.  The first call on a device looks up those arrays with
+ * that device current; make it before any stream capture.  Every call
+ * shares the arrays: calls that overlap on the GPU race.                    */
+PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, double* v, double* w, double* p,
+                                         void* stream);
 
 /* ---- batched ensembles (no counterpart in the reference) -----------------
  * n independent grids on one GPU.  Members with identical ps3d_params share

@@ -13,6 +13,7 @@ PS3D_ERR_OOM = -4
 PS3D_ERR_BADPARAM = -5
 PS3D_ERR_UNSUPPORTED = -6
 PS3D_ERR_CANCELLED = -7
+PS3D_ERR_TOOLARGE = -8
 
 PS3D_FP64 = 0
 PS3D_MIXED = 1

@@ -1422,6 +1422,7 @@ const char* ps3d_strerror(int status) {
         case PS3D_ERR_BADPARAM: return "invalid argument";
         case PS3D_ERR_UNSUPPORTED: return "configuration not supported by this engine";
         case PS3D_ERR_CANCELLED: return "request cancelled";
+        case PS3D_ERR_TOOLARGE: return "grid exceeds the static scratch of ps3d_pressure_solve_noalloc";
         default: return "unknown status";
     }
 }
