@@ -40,11 +40,18 @@ def set_grid(nx, ny, nz):
     NX, NY, NZ = nx, ny, nz
     WORKLOAD = f"jets {nx}x{ny}x{nz} rigid lid AB3 Laplacian friction"
 
-# algorithmic HBM bytes per grid point per launch (SURVEY-style accounting):
-# K1 reads u,v,w,b + 2 AB history slots x 4 fields, writes 4 tendencies + 4 state
+# algorithmic HBM bytes per grid point per launch.  The step kernel reads
+# u,v,w,b, 2 AB history slots x 4 fields and the pending pressure (the
+# previous projection's gradient is applied while loading), and writes 4
+# tendencies + 4 state fields.  FP64: 32 + 64 + 8 + 32 + 32 = 168.  Mixed
+# (u,v,b history FP32, w history FP64): 32 + 40 + 8 + 20 + 32 = 132.
+# The mixed step runs two forward transforms: the divergence of u (24 B read,
+# 4 B complex64 written) and the refinement residual, which also reads p
+# (36 B): 32 B per launch on average.  Its inverse transforms write p
+# (4 + 8 B) and, for the refinement, read it back (+8 B): 16 on average.
 BYTES_PER_POINT = {
-    "fp64": {"step": 160, "fft_fwd": 32, "vsolve": 16, "fft_inv": 16, "correct": 56, "other": 16},
-    "mixed": {"step": 112, "fft_fwd": 28, "vsolve": 8, "fft_inv": 12, "correct": 56, "other": 24},
+    "fp64": {"step": 168, "fft_fwd": 32, "vsolve": 16, "fft_inv": 16, "correct": 56, "other": 16},
+    "mixed": {"step": 132, "fft_fwd": 32, "vsolve": 8, "fft_inv": 16, "correct": 56, "other": 24},
 }
 
 

@@ -67,7 +67,11 @@ struct Ctx {
     bool rigid = true, mixed = false;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
-    size_t tsize = 8;
+    // bytes per stored tendency of field f: FP32 history in the mixed path,
+    // except w, whose tendency is dominated by the buoyancy term b/dsqr that
+    // the pressure gradient nearly cancels (rounding it to FP32 costs ~1e-5
+    // relative in w within 100 steps)
+    size_t tsz(int f) const { return (mixed && f != 2) ? sizeof(float) : sizeof(double); }
     int batch = 1;            // instances of this grid stepped together (ensembles)
     // CUDA graph of three consecutive steps (tau and the state buffers both
     // cycle with period 3), replayed by advance() for constant parameters
@@ -85,7 +89,7 @@ struct Ctx {
     // state
     DevBuf state[4][3];
     int cur[4] = {0, 0, 0, 0};
-    DevBuf p, p2;
+    DevBuf p;
     DevBuf tend[4];           // 3 time levels each
     DevBuf FS;                // spectral work array of the Poisson solve
     // projections
@@ -159,7 +163,7 @@ struct Ctx {
     int capture_graph();
     void invalidate_graph() { ++version; }
     int step(int itt, int tau, int taum1, int taum2);
-    int poisson_once(double* out, double beta, bool lazy = false);
+    int poisson_once(double* out, double beta, bool lazy = false, const double* pc = nullptr);
     int pressure_solve(bool lazy = false);
     int materialize();        // apply a pending correction so the state arrays hold the true state
     int forward_transform(const double* const* in);

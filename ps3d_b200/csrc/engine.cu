@@ -152,10 +152,12 @@ cudaError_t DevPlan::build(int len, int policy) {
     return cudaSuccess;
 }
 
-// Feasible cluster shapes of the plane kernels for one element size.
+constexpr size_t kMaxSmem = 227 * 1024;   // dynamic shared memory a block may opt in to
+
+// Feasible shapes of the plane kernels for one element size.
 static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const PlaneArgs& base) {
     std::vector<PlaneArgs> out;
-    const int nxh = nx / 2 + 1, n2 = nx / 2;
+    const int nxh = nx / 2 + 1;
     for (int C : {1, 2, 4, 8, 16}) {
         if (ny % C) continue;
         const int R = ny / C;
@@ -165,23 +167,21 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
             if (rc > R && rc != 4) continue;
             const int rcc = std::min(rc, R);
             const int ldr = rcc | 1, ldc = cpc | 1;
-            const size_t sm = ((size_t)ny * ldc + (size_t)n2 * ldr) * es;
-            if (sm > 225 * 1024) continue;
             PlaneArgs a = base;
             a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rcc; a.ldr = ldr; a.ldc = ldc;
             a.impl = 0;
+            if (plane_smem(a, es == sizeof(float2)) > kMaxSmem) continue;
             out.push_back(a);
         }
     }
     // rows pass + y-lines pass
     for (int tj : {8, 16, 32}) {
         if (ny % tj) continue;
-        if ((size_t)n2 * (tj | 1) * es > 200 * 1024) continue;
         for (int ly : {8, 16, 32}) {
-            if ((size_t)ny * (ly | 1) * es > 200 * 1024) continue;
             PlaneArgs a = base;
             a.impl = 1; a.tj = tj; a.ly = ly;
             a.C = 1; a.rows_per_cta = ny; a.cols_per_cta = nxh; a.row_chunk = 8; a.ldr = 9; a.ldc = nxh | 1;
+            if (plane_smem(a, es == sizeof(float2)) > kMaxSmem) continue;
             out.push_back(a);
         }
     }
@@ -190,9 +190,9 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
 
 // Default cluster shape of the plane kernels for one element size.
 static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
-    const int nxh = nx / 2 + 1, n2 = nx / 2;
+    const int nxh = nx / 2 + 1;
     for (int pass = 0; pass < 2; ++pass) {
-        const size_t limit = pass == 0 ? 110 * 1024 : 225 * 1024;
+        const size_t limit = pass == 0 ? 110 * 1024 : kMaxSmem;
         for (int C : {1, 2, 4, 8, 16}) {
             if (ny % C) continue;
             const int R = ny / C;
@@ -200,10 +200,11 @@ static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
             if ((C - 1) * cpc >= nxh) continue;
             const int rc = std::min(8, R);
             const int ldr = rc | 1, ldc = cpc | 1;
-            const size_t sm = ((size_t)ny * ldc + (size_t)n2 * ldr) * es;
-            if (sm > limit) continue;
-            a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rc; a.ldr = ldr; a.ldc = ldc;
-            a.impl = 0; a.tj = 8; a.ly = 8;
+            PlaneArgs c = a;
+            c.C = C; c.rows_per_cta = R; c.cols_per_cta = cpc; c.row_chunk = rc; c.ldr = ldr; c.ldc = ldc;
+            c.impl = 0; c.tj = 8; c.ly = 8;
+            if (plane_smem(c, es == sizeof(float2)) > limit) continue;
+            a = c;
             return true;
         }
     }
@@ -250,15 +251,14 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     const long NB = N * batch;
     CK(plane_setup(false));
     CK(plane_setup(true));
+    CK(step_setup());
     // state: 3 buffers per field (fused path ping-pongs two, the generic path needs three)
     for (int f = 0; f < 4; ++f)
         for (int q = 0; q < 3; ++q) { CK(state[f][q].alloc(NB * sizeof(double))); CK(cudaMemset(state[f][q].p, 0, NB * sizeof(double))); }
     for (int f = 0; f < 4; ++f) cur[f] = 0;
     CK(p.alloc(NB * sizeof(double))); CK(cudaMemset(p.p, 0, NB * sizeof(double)));
-    tsize = mixed ? sizeof(float) : sizeof(double);
-    for (int f = 0; f < 4; ++f) { CK(tend[f].alloc(3 * NB * tsize)); CK(cudaMemset(tend[f].p, 0, 3 * NB * tsize)); }
+    for (int f = 0; f < 4; ++f) { CK(tend[f].alloc(3 * NB * tsz(f))); CK(cudaMemset(tend[f].p, 0, 3 * NB * tsz(f))); }
     CK(FS.alloc(M * batch * (mixed ? sizeof(float2) : sizeof(double2))));
-    if (mixed) CK(p2.alloc(NB * sizeof(double)));
     // plans and tables
     CK(plx.build(nx / 2, 0)); CK(ply.build(ny, 0)); CK(plz.build(rigid ? 1 : nz, 0));
     CK(plx4.build(nx / 2, 1)); CK(ply4.build(ny, 1));
@@ -405,9 +405,9 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
     else { a.ab0 = 23.0 / 12.0; a.ab1 = -16.0 / 12.0; a.ab2 = 5.0 / 12.0; }
     const int s0 = tau_ - 1, s1 = taum1_ - 1, s2 = taum2_ - 1;
     for (int f = 0; f < 4; ++f) {
-        a.t0[f] = (char*)tend[f].p + (size_t)s0 * batch * N * tsize;
-        a.t1[f] = (const char*)tend[f].p + (size_t)s1 * batch * N * tsize;
-        a.t2[f] = (const char*)tend[f].p + (size_t)s2 * batch * N * tsize;
+        a.t0[f] = (char*)tend[f].p + (size_t)s0 * batch * N * tsz(f);
+        a.t1[f] = (const char*)tend[f].p + (size_t)s1 * batch * N * tsz(f);
+        a.t2[f] = (const char*)tend[f].p + (size_t)s2 * batch * N * tsz(f);
     }
     a.u = field(0); a.v = field(1); a.w = field(2); a.b = field(3);
     const bool bg = (fkind & PS3D_FORCE_BACKGROUND) != 0;
@@ -542,13 +542,14 @@ static void tune_cache_store(const std::string& k, const std::string& v) {
 
 int Ctx::autotune() {
     const char* env = std::getenv("PS3D_AUTOTUNE");
-    if (env && env[0] == '0') return PS3D_OK;
-    if ((long)N * batch < (1L << 18) && !(env && env[0] == '2')) return PS3D_OK;   // small grids: defaults
+    const bool pinned = std::getenv("PS3D_TUNE") != nullptr;
+    if (env && env[0] == '0' && !pinned) return PS3D_OK;
+    if ((long)N * batch < (1L << 18) && !(env && env[0] == '2') && !pinned) return PS3D_OK;   // small grids: defaults
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, dev));
-    char key[256];
+    char key[384];
     std::snprintf(key, sizeof key, "%s|%dx%dx%d|p%d|r%d|b%d|i%d", prop.name, nx, ny, nz, (int)mixed, (int)rigid, batch,
                   plane_force);
     for (char* c = key; *c; ++c) if (*c == ' ') *c = '_';
@@ -570,6 +571,17 @@ int Ctx::autotune() {
         }
         return false;
     };
+    // PS3D_TUNE pins a configuration in the cache's format, e.g.
+    // "im1,C1,rc8,tj16,ly8,pol2,kc8" (reproducible profiling, no timing runs)
+    if (const char* pin = std::getenv("PS3D_TUNE")) {
+        int im, C, rc, tj, ly, pol, kc;
+        if (std::sscanf(pin, "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d", &im, &C, &rc, &tj, &ly, &pol, &kc) == 7 &&
+            apply(im, C, rc, tj, ly, pol, kc)) {
+            tuned = std::string("pinned:") + pin;
+            return PS3D_OK;
+        }
+        return PS3D_ERR_BADPARAM;
+    }
     auto it = tune_cache().find(key);
     if (it != tune_cache().end()) {
         int im, C, rc, tj, ly, pol, kc;
@@ -640,8 +652,8 @@ int Ctx::autotune() {
             a.ab0 = 23.0 / 12.0; a.ab1 = -16.0 / 12.0; a.ab2 = 5.0 / 12.0; a.do_ab = 1;
             a.u = field(0); a.v = field(1); a.w = field(2); a.b = field(3);
             for (int f = 0; f < 4; ++f) {
-                a.t0[f] = (char*)tend[f].p + (size_t)2 * batch * N * tsize;
-                a.t1[f] = (const char*)tend[f].p + (size_t)1 * batch * N * tsize;
+                a.t0[f] = (char*)tend[f].p + (size_t)2 * batch * N * tsz(f);
+                a.t1[f] = (const char*)tend[f].p + (size_t)1 * batch * N * tsz(f);
                 a.t2[f] = (const char*)tend[f].p;
             }
             a.uo = (double*)state[0][(cur[0] + 1) % 3].p; a.vo = (double*)state[1][(cur[1] + 1) % 3].p;
@@ -747,12 +759,13 @@ int Ctx::advance(int nsteps, bool allow_graph) {
 // ---------------------------------------------------------------------------
 // pressure_solver (pressure_solver.f90:2-120)
 // ---------------------------------------------------------------------------
-int Ctx::poisson_once(double* out, double beta, bool lazy) {
+int Ctx::poisson_once(double* out, double beta, bool lazy, const double* pc) {
     const bool f32 = mixed;
     PlaneArgs a = f32 ? pa32 : pa64;
     a.batch = batch;
-    a.mode = 0;
+    a.mode = pc ? 2 : 0;
     a.u = field(0); a.v = field(1); a.w = field(2);
+    a.pc = pc; a.dtp = P.dt; a.dtwp = P.dt / P.dsqr; a.rigid = rigid;
     a.rdt = 1.0 / P.dt;
     a.scale = P.dx * P.dy;
     a.spec = FS.p;
@@ -791,8 +804,6 @@ int Ctx::materialize() {
     if (!pending) return PS3D_OK;
     LAUNCH(PS3D_K_CORRECT, launch_correct(field(0), field(1), field(2), pcor, nx, ny, nz, rigid, dtp, dtp / P.dsqr,
                       1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, stream, batch));
-    if (mixed && pcor == (const double*)p2.p)
-        LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N * batch, 1.0, 1.0, stream));
     pending = false;
     return PS3D_OK;
 }
@@ -801,15 +812,14 @@ int Ctx::pressure_solve(bool lazy) {
     int rc = materialize();
     if (rc) return rc;
     if (!mixed) return poisson_once((double*)p.p, 0.0, lazy);
-    // one FP64-residual refinement: the divergence of the corrected velocity
-    // is solved again and its pressure added to p (lazily: p += p2 when the
-    // state is next observed; the next step applies the p2 correction)
-    rc = poisson_once((double*)p.p, 0.0, false);
+    // one FP64-residual refinement: the divergence of u - dt grad p1 (formed
+    // on the fly from u and p1, in FP64) is solved again and the inverse
+    // transform adds its pressure to p, so p = p1 + p2 and one correction
+    // with p (lazy or not) projects the velocity
+    rc = poisson_once((double*)p.p, 0.0, true);
     if (rc) return rc;
-    rc = poisson_once((double*)p2.p, 0.0, lazy);
-    if (rc) return rc;
-    if (!lazy) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)p.p, (const double*)p2.p, N * batch, 1.0, 1.0, stream));
-    return PS3D_OK;
+    pending = false;
+    return poisson_once((double*)p.p, 1.0, lazy, (const double*)p.p);
 }
 
 // ---------------------------------------------------------------------------
@@ -968,7 +978,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     CK(ensure_saved_tail());
     CK(cudaMemcpyAsync(saved_p.p, p.p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     for (int f = 0; f < 4; ++f)
-        CK(cudaMemcpyAsync(saved_tend[f].p, tend[f].p, 3 * N * tsize, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(saved_tend[f].p, tend[f].p, 3 * N * tsz(f), cudaMemcpyDeviceToDevice, stream));
     const double Ro_loc = P.Ro, dt_loc = P.dt;
     const double Ahbi_loc = P.Ahbi, Avbi_loc = P.Avbi, Khbi_loc = P.Khbi, Kvbi_loc = P.Kvbi;
     const int tau_loc = tau, taum1_loc = taum1, taum2_loc = taum2, itt_loc = itt;
@@ -1057,7 +1067,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     CK(copy_set_to_state(kSetSave));
     CK(cudaMemcpyAsync(p.p, saved_p.p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     for (int f = 0; f < 4; ++f)
-        CK(cudaMemcpyAsync(tend[f].p, saved_tend[f].p, 3 * N * tsize, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(tend[f].p, saved_tend[f].p, 3 * N * tsz(f), cudaMemcpyDeviceToDevice, stream));
     P.Ro = Ro_loc; P.dt = dt_loc;
     P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
     tau = tau_loc; taum1 = taum1_loc; taum2 = taum2_loc; itt = itt_loc;
@@ -1074,7 +1084,7 @@ cudaError_t Ctx::ensure_saved_tail() {
     if (saved_p.p) return cudaSuccess;
     cudaError_t e;
     if ((e = saved_p.alloc(N * sizeof(double)))) return e;
-    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * tsize))) return e;
+    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * tsz(f)))) return e;
     return cudaSuccess;
 }
 
@@ -1125,11 +1135,11 @@ int Ctx::download_field(const double* dev, double* h, int kind) {
 int Ctx::upload_tend(int f, const double* h) {
     const long n3 = (long)(nx + 4) * (ny + 4) * (nz + 4);
     for (int s = 0; s < 3; ++s) {
-        char* dev = (char*)tend[f].p + (size_t)s * N * tsize;
-        if (!h) { CK(cudaMemsetAsync(dev, 0, N * tsize, stream)); continue; }
+        char* dev = (char*)tend[f].p + (size_t)s * N * tsz(f);
+        if (!h) { CK(cudaMemsetAsync(dev, 0, N * tsz(f), stream)); continue; }
         CK(ensure_staging());
         gather(h + s * n3, (double*)staging.p);
-        if (mixed) {
+        if (tsz(f) == sizeof(float)) {
             std::vector<float> tmp(N);
             const double* d = (const double*)staging.p;
             for (long t = 0; t < N; ++t) tmp[t] = (float)d[t];
@@ -1147,8 +1157,8 @@ int Ctx::download_tend(int f, double* h) {
     const long n3 = (long)(nx + 4) * (ny + 4) * (nz + 4);
     CK(ensure_staging());
     for (int s = 0; s < 3; ++s) {
-        const char* dev = (const char*)tend[f].p + (size_t)s * N * tsize;
-        if (mixed) {
+        const char* dev = (const char*)tend[f].p + (size_t)s * N * tsz(f);
+        if (tsz(f) == sizeof(float)) {
             std::vector<float> tmp(N);
             CK(cudaMemcpy(tmp.data(), dev, N * sizeof(float), cudaMemcpyDeviceToHost));
             double* d = (double*)staging.p;

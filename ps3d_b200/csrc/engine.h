@@ -43,9 +43,14 @@ struct PlaneArgs {
     int nx, ny, nz, nxh;
     int C;                         // cluster size (CTAs per z-plane)
     int rows_per_cta, cols_per_cta, row_chunk, ldc, ldr;
-    // forward source: mode 0 = divergence of (u,v,w)/dt, mode 1 = real field src
+    // forward source: mode 0 = divergence of (u,v,w)/dt, mode 1 = real field
+    // src, mode 2 = divergence of (u,v,w) - dtp grad(pc), the correction of a
+    // pending pressure pc applied on the fly
     int mode;
     const double *u, *v, *w, *src;
+    const double* pc;
+    double dtp, dtwp;
+    int rigid;
     double rdx, rdy, rdz, rdt;
     double scale;                  // dx*dy (forward) or 1/(Lx*Ly[*Lz]) (inverse)
     void* spec;                    // complex spectral array [k][ky][kx]
@@ -78,6 +83,7 @@ struct ColumnArgs {
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
+cudaError_t step_setup();   // opts the step kernels in to their dynamic shared memory
 cudaError_t launch_biharmonic_h(const double* cur, const double* old, double* out, int nx, int ny, int nz,
                                 double Hmix, double rdx, double rdy, double dt, cudaStream_t s);
 cudaError_t launch_biharmonic_v(const double* cur, const double* old, double* out, int nx, int ny, int nz,
@@ -91,6 +97,7 @@ cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int
 // poisson.cu
 size_t plane_fwd_smem(const PlaneArgs& a, bool fp32);
 size_t plane_inv_smem(const PlaneArgs& a, bool fp32);
+size_t plane_smem(const PlaneArgs& a, bool fp32);   // largest dynamic shared memory of the configuration
 cudaError_t plane_setup(bool fp32);
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);

@@ -15,19 +15,35 @@
 
 namespace ps3d {
 
+// Shared-memory copy of one plan's tables: the twiddles in the working
+// precision, the digit-reversal permutation and its inverse.  Staging them
+// once per block keeps the butterflies off the L1/L2 load path.
 template <typename R>
-__device__ __forceinline__ cpx<R> twiddle(const FFTPlan& P, int t, int sign);
-template <>
-__device__ __forceinline__ double2 twiddle<double>(const FFTPlan& P, int t, int sign) {
-    double2 w = __ldg(P.tw + t);
-    if (sign > 0) w.y = -w.y;
-    return w;
+struct PlanTables {
+    const cpx<R>* tw;
+    const int* pos;
+    const int* ipos;
+};
+
+PS3D_HD constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+PS3D_HD size_t plan_tables_bytes(int n, size_t es) {
+    return align16((size_t)n * es) + 2 * align16((size_t)n * sizeof(int));
 }
-template <>
-__device__ __forceinline__ float2 twiddle<float>(const FFTPlan& P, int t, int sign) {
-    float2 w = __ldg(P.twf + t);
-    if (sign > 0) w.y = -w.y;
-    return w;
+
+// Block-cooperative copy into dst (16-byte aligned, plan_tables_bytes long).
+// The caller synchronises the block before the tables are read.
+template <typename R>
+__device__ PlanTables<R> stage_plan(const FFTPlan& P, unsigned char* dst) {
+    cpx<R>* t = reinterpret_cast<cpx<R>*>(dst);
+    int* p = reinterpret_cast<int*>(dst + align16((size_t)P.n * sizeof(cpx<R>)));
+    int* q = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(p) + align16((size_t)P.n * sizeof(int)));
+    for (int e = threadIdx.x; e < P.n; e += blockDim.x) {
+        if constexpr (sizeof(R) == 8) t[e] = __ldg(P.tw + e);
+        else t[e] = __ldg(P.twf + e);
+        p[e] = __ldg(P.pos + e);
+        q[e] = __ldg(P.ipos + e);
+    }
+    return {t, p, q};
 }
 
 // radix-RAD DFT in registers: y_m = sum_q v_q exp(sign 2 pi i q m / RAD)
@@ -106,7 +122,7 @@ PS3D_HD void small_dft(T* v, int sign) {
 
 template <int RAD, bool DIT, typename R>
 __device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const FFTPlan& P,
-                                          int Lp, int sign) {
+                                          int Lp, int sign, const cpx<R>* tw) {
     using T = cpx<R>;
     const int n = P.n;
     const int L = Lp * RAD;
@@ -124,12 +140,20 @@ __device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const
         for (int q = 0; q < RAD; ++q) v[q] = buf[(base + q * Lp) * ld + line];
         if (DIT && j) {
 #pragma unroll
-            for (int q = 1; q < RAD; ++q) v[q] = cmul(v[q], twiddle<R>(P, q * j * tstride, sign));
+            for (int q = 1; q < RAD; ++q) {
+                T w = tw[q * j * tstride];
+                if (sign > 0) w.y = -w.y;
+                v[q] = cmul(v[q], w);
+            }
         }
         small_dft<RAD>(v, sign);
         if (!DIT && j) {
 #pragma unroll
-            for (int q = 1; q < RAD; ++q) v[q] = cmul(v[q], twiddle<R>(P, q * j * tstride, sign));
+            for (int q = 1; q < RAD; ++q) {
+                T w = tw[q * j * tstride];
+                if (sign > 0) w.y = -w.y;
+                v[q] = cmul(v[q], w);
+            }
         }
 #pragma unroll
         for (int q = 0; q < RAD; ++q) buf[(base + q * Lp) * ld + line] = v[q];
@@ -137,24 +161,36 @@ __device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const
 }
 
 // Whole-block batched FFT.  Must be called by every thread of the block; it
-// synchronises the block before returning.
-template <bool DIT, typename R>
-__device__ void fft_batch(cpx<R>* buf, int ld, int nlines, const FFTPlan& P, int sign) {
+// synchronises the block before returning.  tw: the plan's twiddles staged
+// in shared memory (stage_plan).  MAXR is the largest radix instantiated:
+// kernels built with MAXR = 8 hold fewer registers and run more blocks per
+// SM, and only take plans without radix-16 stages.
+template <bool DIT, typename R, int MAXR = 16>
+__device__ void fft_batch(cpx<R>* buf, int ld, int nlines, const FFTPlan& P, int sign, const cpx<R>* tw) {
     __syncthreads();
     for (int s0 = 0; s0 < P.nst; ++s0) {
         const int st = DIT ? s0 : P.nst - 1 - s0;
         const int Lp = P.lp[st];
         switch (P.r[st]) {
-            case 2: fft_stage<2, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
-            case 3: fft_stage<3, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
-            case 4: fft_stage<4, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
-            case 5: fft_stage<5, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
-            case 8: fft_stage<8, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
-            case 16: fft_stage<16, DIT, R>(buf, ld, nlines, P, Lp, sign); break;
+            case 2: fft_stage<2, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
+            case 3: fft_stage<3, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
+            case 4: fft_stage<4, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
+            case 5: fft_stage<5, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
+            case 8: fft_stage<8, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
+            case 16:
+                if constexpr (MAXR >= 16) fft_stage<16, DIT, R>(buf, ld, nlines, P, Lp, sign, tw);
+                break;
             default: break;
         }
         __syncthreads();
     }
+}
+
+// largest radix of a plan (host side): selects the MAXR instantiation
+inline int plan_max_radix(const FFTPlan& P) {
+    int m = 1;
+    for (int s = 0; s < P.nst; ++s) m = P.r[s] > m ? P.r[s] : m;
+    return m;
 }
 
 }  // namespace ps3d

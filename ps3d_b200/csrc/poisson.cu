@@ -30,62 +30,159 @@ namespace ps3d {
 
 constexpr int kPlaneThreads = 256;
 
+// blocks per SM the plane kernels are built for: the radix-16 instantiation
+// needs ~128 FP64 registers, the radix-8 one fits in 80
+template <int MAXR> constexpr int plane_min_blocks() { return MAXR >= 16 ? 2 : 3; }
+template <int MAXR> constexpr int lines_min_blocks() { return MAXR >= 16 ? 2 : 4; }
+
+// Divergence of the pair of points (2m, 2m+1) of row j in plane k, divided by
+// dt (pressure_solver.f90:16-24), or the pair of source values (mode 1).
+__device__ __forceinline__ double2 plane_source_pair(const PlaneArgs& a, const double* au, const double* av,
+                                                     const double* aw, const double* asrc, int k, int j, int m) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const long plane = (long)nx * ny;
+    const long g = (long)k * plane + (long)j * nx + 2 * m;
+    if (a.mode == 1) return __ldg(reinterpret_cast<const double2*>(asrc + g));
+    const long gum = g - 2 * m + wrap(2 * m - 1, nx);
+    const long gv = g + (long)(wrap(j - 1, ny) - j) * nx;
+    const long gw = g + (long)(wrap(k - 1, nz) - k) * plane;
+    double2 uu = __ldg(reinterpret_cast<const double2*>(au + g));
+    double um = __ldg(au + gum);
+    double2 vv = __ldg(reinterpret_cast<const double2*>(av + g));
+    double2 vm = __ldg(reinterpret_cast<const double2*>(av + gv));
+    double2 ww = __ldg(reinterpret_cast<const double2*>(aw + g));
+    double2 wm = __ldg(reinterpret_cast<const double2*>(aw + gw));
+    if (a.mode == 2) {
+        // u - dt grad p at the points the divergence reads (pressure_solver.f90:98-110)
+        const double* pc = a.pc + (au - a.u);   // same instance offset as the fields
+        const long gpe = g - 2 * m + wrap(2 * m + 2, nx);
+        const long gpn = g + (long)(wrap(j + 1, ny) - j) * nx;
+        const long gpu = g + (long)(wrap(k + 1, nz) - k) * plane;
+        const double2 p0 = __ldg(reinterpret_cast<const double2*>(pc + g));
+        const double pw = __ldg(pc + gum), pe = __ldg(pc + gpe);
+        const double2 ps = __ldg(reinterpret_cast<const double2*>(pc + gv));
+        const double2 pn = __ldg(reinterpret_cast<const double2*>(pc + gpn));
+        const double2 pd = __ldg(reinterpret_cast<const double2*>(pc + gw));
+        const double2 pu = __ldg(reinterpret_cast<const double2*>(pc + gpu));
+        const double dt = a.dtp, dtw = a.dtwp;
+        um = um - dt * (p0.x - pw) * a.rdx;
+        uu.x = uu.x - dt * (p0.y - p0.x) * a.rdx;
+        uu.y = uu.y - dt * (pe - p0.y) * a.rdx;
+        vv.x = vv.x - dt * (pn.x - p0.x) * a.rdy;
+        vv.y = vv.y - dt * (pn.y - p0.y) * a.rdy;
+        vm.x = vm.x - dt * (p0.x - ps.x) * a.rdy;
+        vm.y = vm.y - dt * (p0.y - ps.y) * a.rdy;
+        if (a.rigid && k == nz - 1) {
+            ww.x = 0.0; ww.y = 0.0;
+        } else {
+            ww.x = ww.x - dtw * (pu.x - p0.x) * a.rdz;
+            ww.y = ww.y - dtw * (pu.y - p0.y) * a.rdz;
+        }
+        if (a.rigid && wrap(k - 1, nz) == nz - 1) {
+            wm.x = 0.0; wm.y = 0.0;
+        } else {
+            wm.x = wm.x - dtw * (p0.x - pd.x) * a.rdz;
+            wm.y = wm.y - dtw * (p0.y - pd.y) * a.rdz;
+        }
+    }
+    double2 d;
+    d.x = ((uu.x - um) * a.rdx + (vv.x - vm.x) * a.rdy + (ww.x - wm.x) * a.rdz) * a.rdt;
+    d.y = ((uu.y - uu.x) * a.rdx + (vv.y - vm.y) * a.rdy + (ww.y - wm.y) * a.rdz) * a.rdt;
+    return d;
+}
+
+// exp(-2 pi i t / nx), t = 0..nx/2, staged in the working precision
 template <typename R>
-__global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_fwd(const PlaneArgs a) {
+__device__ cpx<R>* stage_twx(const PlaneArgs& a, unsigned char* dst) {
+    cpx<R>* t = reinterpret_cast<cpx<R>*>(dst);
+    for (int e = threadIdx.x; e < a.nxh; e += blockDim.x) {
+        const double2 w = __ldg(a.twx + e);
+        t[e] = mk<R>((R)w.x, (R)w.y);
+    }
+    return t;
+}
+
+// bytes of shared memory after the work buffers: tables of x, of y, twx
+PS3D_HD size_t tables_x_bytes(const PlaneArgs& a, size_t es) {
+    return plan_tables_bytes(a.nx / 2, es) + align16((size_t)a.nxh * es);
+}
+PS3D_HD size_t tables_y_bytes(const PlaneArgs& a, size_t es) { return plan_tables_bytes(a.ny, es); }
+
+// X_k = E_k + W^k O_k from the half-length transform Z (r2c unpack)
+template <typename R>
+__device__ __forceinline__ cpx<R> r2c_unpack(cpx<R> Zk, cpx<R> Zc, cpx<R> w) {
+    using T = cpx<R>;
+    Zc = cconj(Zc);
+    const T E = cscale(cadd(Zk, Zc), (R)0.5);
+    const T H = cscale(cmul_si(csub(Zk, Zc), -1), (R)0.5);   // O_k = -i (Zk - Zc)/2
+    return cadd(E, cmul(w, H));
+}
+// Z_k = (X_k + conj X_{n2-k}) + i W^{-k} (X_k - conj X_{n2-k}) (c2r pack; the
+// factor 1/2 is in the caller's scale)
+template <typename R>
+__device__ __forceinline__ cpx<R> c2r_pack(cpx<R> Xk, cpx<R> Xc, cpx<R> w, bool dc) {
+    using T = cpx<R>;
+    if (dc) { Xk.y = (R)0; Xc.y = (R)0; }   // c2r ignores Im of DC and Nyquist
+    Xc = cconj(Xc);
+    const T wb = mk<R>(w.x, -w.y);           // W^{-k}
+    return cadd(cadd(Xk, Xc), cmul_si(cmul(wb, csub(Xk, Xc)), +1));
+}
+
+// ---------------------------------------------------------------------------
+// K2/K4, first implementation: one thread-block cluster per z-plane
+// ---------------------------------------------------------------------------
+template <typename R, int MAXR>
+__global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_plane_fwd(const PlaneArgs a) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
     T* colbuf = reinterpret_cast<T*>(smem_raw);
     T* rowbuf = colbuf + (size_t)a.ny * a.ldc;
+    unsigned char* tail = smem_raw + align16(((size_t)a.ny * a.ldc + (size_t)(a.nx / 2) * a.ldr) * sizeof(T));
+    const PlanTables<R> tx = stage_plan<R>(a.px, tail);
+    const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(a.nx / 2, sizeof(T)));
+    const PlanTables<R> ty = stage_plan<R>(a.py, tail + tables_x_bytes(a, sizeof(T)));
     const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
     const int inst = blockIdx.y / nz;
     const int k = blockIdx.y - inst * nz;
     const long ioff = (long)inst * a.sN;
     const int rank = (int)cluster.block_rank();
-    const long plane = (long)nx * ny;
     const int ldr = a.ldr, ldc = a.ldc, cpc = a.cols_per_cta;
     const double* au = a.u + ioff;
     const double* av = a.v + ioff;
     const double* aw = a.w + ioff;
     const double* asrc = a.src ? a.src + ioff : nullptr;
-    cluster.sync();   // every CTA of the cluster is running before DSMEM stores
+    cluster.sync();   // every CTA of the cluster is running before DSMEM stores; tables staged
     const int jb = rank * a.rows_per_cta;
+    constexpr int LB = 2;
     for (int jc = 0; jc < a.rows_per_cta; jc += a.row_chunk) {
         const int nr = min(a.row_chunk, a.rows_per_cta - jc);
-        for (int t = threadIdx.x; t < nr * n2; t += blockDim.x) {
-            const int rr = t / n2, m = t - rr * n2;
-            const int j = jb + jc + rr;
-            const long g = (long)k * plane + (long)j * nx + 2 * m;
-            double d0, d1;
-            if (a.mode == 0) {
-                const double2 uu = *reinterpret_cast<const double2*>(au + g);
-                const double um = au[g - 2 * m + wrap(2 * m - 1, nx)];
-                const long gv = g + (long)(wrap(j - 1, ny) - j) * nx;
-                const long gw = g + (long)(wrap(k - 1, nz) - k) * plane;
-                const double2 vv = *reinterpret_cast<const double2*>(av + g);
-                const double2 vm = *reinterpret_cast<const double2*>(av + gv);
-                const double2 ww = *reinterpret_cast<const double2*>(aw + g);
-                const double2 wm = *reinterpret_cast<const double2*>(aw + gw);
-                d0 = ((uu.x - um) * a.rdx + (vv.x - vm.x) * a.rdy + (ww.x - wm.x) * a.rdz) * a.rdt;
-                d1 = ((uu.y - uu.x) * a.rdx + (vv.y - vm.y) * a.rdy + (ww.y - wm.y) * a.rdz) * a.rdt;
-            } else {
-                const double2 s = *reinterpret_cast<const double2*>(asrc + g);
-                d0 = s.x; d1 = s.y;
+        const int total = nr * n2;
+        for (int t0 = threadIdx.x; t0 < total; t0 += LB * blockDim.x) {
+            double2 d[LB];
+#pragma unroll
+            for (int q = 0; q < LB; ++q) {
+                const int t = t0 + q * blockDim.x;
+                if (t < total) {
+                    const int rr = t / n2, m = t - rr * n2;
+                    d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + jc + rr, m);
+                }
             }
-            rowbuf[m * ldr + rr] = mk<R>((R)d0, (R)d1);
+#pragma unroll
+            for (int q = 0; q < LB; ++q) {
+                const int t = t0 + q * blockDim.x;
+                if (t < total) {
+                    const int rr = t / n2, m = t - rr * n2;
+                    rowbuf[m * ldr + rr] = mk<R>((R)d[q].x, (R)d[q].y);
+                }
+            }
         }
-        fft_batch<false, R>(rowbuf, ldr, nr, a.px, -1);
-        // unpack the half-length transform: X_k = E_k + W^k O_k
+        fft_batch<false, R, MAXR>(rowbuf, ldr, nr, a.px, -1, tx.tw);
         for (int t = threadIdx.x; t < nr * (n2 + 1); t += blockDim.x) {
             const int kx = t / nr, rr = t - kx * nr;
             const int k1 = (kx == n2) ? 0 : kx;
             const int k2 = (kx == 0) ? 0 : n2 - kx;
-            const T Zk = rowbuf[a.px.pos[k1] * ldr + rr];
-            const T Zc = cconj(rowbuf[a.px.pos[k2] * ldr + rr]);
-            const T E = cscale(cadd(Zk, Zc), (R)0.5);
-            const T H = cscale(cmul_si(csub(Zk, Zc), -1), (R)0.5);   // O_k = -i (Zk - Zc)/2
-            const double2 wd = __ldg(a.twx + kx);
-            const T X = cadd(E, cmul(mk<R>((R)wd.x, (R)wd.y), H));
+            const T X = r2c_unpack<R>(rowbuf[tx.pos[k1] * ldr + rr], rowbuf[tx.pos[k2] * ldr + rr], twx[kx]);
             const int owner = kx / cpc, c = kx - owner * cpc;
             T* dst = cluster.map_shared_rank(colbuf, owner);
             dst[(jb + jc + rr) * ldc + c] = X;
@@ -95,22 +192,26 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_fwd(const PlaneArgs 
     cluster.sync();   // all rows delivered
     const int c0 = rank * cpc;
     const int ncol = max(0, min(cpc, nxh - c0));
-    if (ncol > 0) fft_batch<false, R>(colbuf, ldc, ncol, a.py, -1);
+    fft_batch<false, R, MAXR>(colbuf, ldc, ncol, a.py, -1, ty.tw);
     T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM;
     const R sc = (R)a.scale;
     for (int t = threadIdx.x; t < ny * ncol; t += blockDim.x) {
         const int ky = t / ncol, c = t - ky * ncol;
-        spec[((long)k * ny + ky) * nxh + c0 + c] = cscale(colbuf[a.py.pos[ky] * ldc + c], sc);
+        spec[((long)k * ny + ky) * nxh + c0 + c] = cscale(colbuf[ty.pos[ky] * ldc + c], sc);
     }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_inv(const PlaneArgs a) {
+template <typename R, int MAXR>
+__global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_plane_inv(const PlaneArgs a) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
     T* colbuf = reinterpret_cast<T*>(smem_raw);
     T* rowbuf = colbuf + (size_t)a.ny * a.ldc;
+    unsigned char* tail = smem_raw + align16(((size_t)a.ny * a.ldc + (size_t)(a.nx / 2) * a.ldr) * sizeof(T));
+    const PlanTables<R> tx = stage_plan<R>(a.px, tail);
+    const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(a.nx / 2, sizeof(T)));
+    const PlanTables<R> ty = stage_plan<R>(a.py, tail + tables_x_bytes(a, sizeof(T)));
     const int nx = a.nx, ny = a.ny, nxh = a.nxh, n2 = nx / 2;
     const int inst = blockIdx.y / a.nz;
     const int k = blockIdx.y - inst * a.nz;
@@ -121,37 +222,48 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_inv(const PlaneArgs 
     const int c0 = rank * cpc;
     const int ncol = max(0, min(cpc, nxh - c0));
     const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM;
-    for (int t = threadIdx.x; t < ny * ncol; t += blockDim.x) {
-        const int ky = t / ncol, c = t - ky * ncol;
-        colbuf[ky * ldc + c] = spec[((long)k * ny + ky) * nxh + c0 + c];
+    constexpr int LB = sizeof(R) == 8 ? 4 : 8;
+    const int total = ny * ncol;
+    for (int t0 = threadIdx.x; t0 < total; t0 += LB * blockDim.x) {
+        T v[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int ky = t / ncol, c = t - ky * ncol;
+                v[q] = spec[((long)k * ny + ky) * nxh + c0 + c];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int ky = t / ncol, c = t - ky * ncol;
+                colbuf[ky * ldc + c] = v[q];
+            }
+        }
     }
-    if (ncol > 0) fft_batch<false, R>(colbuf, ldc, ncol, a.py, +1);
+    fft_batch<false, R, MAXR>(colbuf, ldc, ncol, a.py, +1, ty.tw);   // also orders the staged tables
     cluster.sync();   // every column transformed; gather rows from the owners
     const int jb = rank * a.rows_per_cta;
     for (int jc = 0; jc < a.rows_per_cta; jc += a.row_chunk) {
         const int nr = min(a.row_chunk, a.rows_per_cta - jc);
         for (int t = threadIdx.x; t < nr * n2; t += blockDim.x) {
             const int kk = t / nr, rr = t - kk * nr;
-            const int prow = a.py.pos[jb + jc + rr];
+            const int prow = ty.pos[jb + jc + rr];
             const int kc = n2 - kk;
             const int o1 = kk / cpc, o2 = kc / cpc;
             const T* s1 = cluster.map_shared_rank(colbuf, o1);
             const T* s2 = cluster.map_shared_rank(colbuf, o2);
-            T Xk = s1[prow * ldc + (kk - o1 * cpc)];
-            T Xc = s2[prow * ldc + (kc - o2 * cpc)];
-            if (kk == 0) { Xk.y = (R)0; Xc.y = (R)0; }   // c2r ignores Im of DC and Nyquist
-            Xc = cconj(Xc);
-            const double2 wd = __ldg(a.twx + kk);
-            const T wb = mk<R>((R)wd.x, (R)-wd.y);      // W^{-k}
-            const T Z = cadd(cadd(Xk, Xc), cmul_si(cmul(wb, csub(Xk, Xc)), +1));
-            rowbuf[kk * ldr + rr] = Z;
+            rowbuf[kk * ldr + rr] = c2r_pack<R>(s1[prow * ldc + (kk - o1 * cpc)], s2[prow * ldc + (kc - o2 * cpc)],
+                                                twx[kk], kk == 0);
         }
-        fft_batch<false, R>(rowbuf, ldr, nr, a.px, +1);
+        fft_batch<false, R, MAXR>(rowbuf, ldr, nr, a.px, +1, tx.tw);
         const double sc = a.scale;
         for (int t = threadIdx.x; t < nr * n2; t += blockDim.x) {
             const int rr = t / n2, m = t - rr * n2;
             const int j = jb + jc + rr;
-            const T z = rowbuf[a.px.pos[m] * ldr + rr];
+            const T z = rowbuf[tx.pos[m] * ldr + rr];
             const long g = (long)k * plane + (long)j * nx + 2 * m;
             double2 o = make_double2((double)z.x * sc, (double)z.y * sc);
             if (a.beta != 0.0) {
@@ -166,103 +278,122 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_plane_inv(const PlaneArgs 
 }
 
 // ---------------------------------------------------------------------------
-// K3, rigid lid: batched Thomas along z (pressure_solver.f90:33-53, 126-162)
+// K3, rigid lid: batched Thomas along z (pressure_solver.f90:33-53, 126-162).
+// The coefficients are real, so the real and imaginary parts of a column
+// are independent recurrences: one thread per (column, part) doubles the
+// threads in flight over one thread per complex column.  Levels move in
+// chunks of KC, and the loads of the next chunk are issued before the
+// recurrence runs over the current one, so memory latency overlaps the
+// serial arithmetic.  c' is checkpointed every KC levels in shared memory
+// and recomputed on the way back (no c' array in HBM).
 // ---------------------------------------------------------------------------
+constexpr int kThomasChunk = 8;
+constexpr int kThomasThreads = 128;
+
 template <typename R>
-__global__ void __launch_bounds__(128) k_thomas(const ColumnArgs a) {
-    using T = cpx<R>;
-    extern __shared__ double cps[];   // [nz/8 + 1][blockDim.x] checkpoints of c'
+__global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a) {
+    constexpr int KC = kThomasChunk;
+    extern __shared__ double cps[];   // [nz/KC + 1][blockDim.x] checkpoints of c'
     const long ncols = (long)a.nxh * a.ny;
-    const long cg_ = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (cg_ >= ncols * a.batch) return;
-    const long inst = cg_ / ncols;
-    const long c = cg_ - inst * ncols;
-    T* spec = reinterpret_cast<T*>(a.spec) + inst * a.sM;
+    const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (gid >= 2 * ncols * a.batch) return;
+    const int part = (int)(gid & 1);
+    const long cb = gid >> 1;
+    const long inst = cb / ncols;
+    const long c = cb - inst * ncols;
+    R* col = reinterpret_cast<R*>(a.spec) + 2 * (inst * a.sM + c) + part;
+    const long ls = 2 * ncols;   // level stride in R
     const int nz = a.nz;
     const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
     const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
     const double ks = a.hkx[i] + a.hky[j];
     const double fxa = a.fxa;
     if (ks > 0) {
-        // levels are processed in chunks of 8: the 8 loads of a chunk are
-        // issued together, then the serial recurrence runs on registers
         const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-        double cp = 0.0, dpx = 0.0, dpy = 0.0;
-        for (int kb = 0; kb < nz; kb += 8) {
-            T d[8];
+        double cp = 0.0, dp = 0.0;
+        R nxt[KC];
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (kb + q < nz) d[q] = spec[c + (long)(kb + q) * ncols];
+        for (int q = 0; q < KC; ++q)
+            if (q < nz) nxt[q] = col[(long)q * ls];
+        for (int kb = 0; kb < nz; kb += KC) {
+            R d[KC];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + KC + q < nz) nxt[q] = col[(long)(kb + KC + q) * ls];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
                 if (k < nz) {
                     const double bk = (k == 0 || k == nz - 1) ? bend : bmid;
                     if (k == 0) {
-                        cp = fxa / bk;                       // cp(1) = c(1)/b(1)
-                        dpx = (double)d[q].x / bk;           // dp(1) = d(1)/b(1)
-                        dpy = (double)d[q].y / bk;
+                        cp = fxa / bk;                   // cp(1) = c(1)/b(1)
+                        dp = (double)d[q] / bk;          // dp(1) = d(1)/b(1)
                     } else {
-                        const double r = 1.0 / (bk - cp * fxa);
+                        const double r = __drcp_rn(bk - cp * fxa);   // == 1.0 / x (both correctly rounded)
                         cp = fxa * r;
-                        dpx = ((double)d[q].x - dpx * fxa) * r;
-                        dpy = ((double)d[q].y - dpy * fxa) * r;
+                        dp = ((double)d[q] - dp * fxa) * r;
                     }
-                    if (q == 0) cps[(kb >> 3) * blockDim.x + threadIdx.x] = cp;
-                    d[q] = mk<R>((R)dpx, (R)dpy);
+                    if (q == 0) cps[(kb / KC) * blockDim.x + threadIdx.x] = cp;
+                    d[q] = (R)dp;
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (kb + q < nz) spec[c + (long)(kb + q) * ncols] = d[q];
+            for (int q = 0; q < KC; ++q)
+                if (kb + q < nz) col[(long)(kb + q) * ls] = d[q];
         }
-        double xx = dpx, xy = dpy;   // x(nz) = dp(nz)
-        for (int sg = (nz - 1) >> 3; sg >= 0; --sg) {
-            const int kb = sg * 8;
-            T d[8];
+        double x = dp;   // x(nz) = dp(nz)
+        const int last = (nz - 1) / KC;
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (kb + q < nz - 1) d[q] = spec[c + (long)(kb + q) * ncols];
-            double cpl[8];
+        for (int q = 0; q < KC; ++q)
+            if (last * KC + q < nz - 1) nxt[q] = col[(long)(last * KC + q) * ls];
+        for (int sg = last; sg >= 0; --sg) {
+            const int kb = sg * KC;
+            R d[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+            if (sg > 0) {
+#pragma unroll
+                for (int q = 0; q < KC; ++q) nxt[q] = col[(long)(kb - KC + q) * ls];
+            }
+            double cpl[KC];
             cpl[0] = cps[sg * blockDim.x + threadIdx.x];
 #pragma unroll
-            for (int q = 1; q < 8; ++q) {
+            for (int q = 1; q < KC; ++q) {
                 const int k = kb + q;
                 if (k < nz) {
                     const double bk = (k == nz - 1) ? bend : bmid;
-                    cpl[q] = fxa * (1.0 / (bk - cpl[q - 1] * fxa));
+                    cpl[q] = fxa * __drcp_rn(bk - cpl[q - 1] * fxa);
                 } else {
                     cpl[q] = 0.0;
                 }
             }
 #pragma unroll
-            for (int q = 7; q >= 0; --q) {
+            for (int q = KC - 1; q >= 0; --q) {
                 if (kb + q >= nz - 1) continue;
-                xx = (double)d[q].x - cpl[q] * xx;
-                xy = (double)d[q].y - cpl[q] * xy;
-                d[q] = mk<R>((R)xx, (R)xy);
+                x = (double)d[q] - cpl[q] * x;
+                d[q] = (R)x;
             }
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (kb + q < nz - 1) spec[c + (long)(kb + q) * ncols] = d[q];
+            for (int q = 0; q < KC; ++q)
+                if (kb + q < nz - 1) col[(long)(kb + q) * ls] = d[q];
         }
     } else {
         // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
         const double h = a.dz2dsqr;
-        T prev_orig = spec[c];
-        spec[c] = mk<R>((R)0, (R)0);
+        const R prev_orig = col[0];
+        col[0] = (R)0;
         if (nz > 1) {
-            double x0x = 0.0, x0y = 0.0;
-            const T o1 = spec[c + ncols];
-            double x1x = (double)prev_orig.x * h, x1y = (double)prev_orig.y * h;
-            spec[c + ncols] = mk<R>((R)x1x, (R)x1y);
-            T orig_km1 = o1;
+            double x0 = 0.0;
+            R orig_km1 = col[ls];
+            double x1 = (double)prev_orig * h;
+            col[ls] = (R)x1;
             for (int k = 2; k < nz; ++k) {
-                const T ok = spec[c + (long)k * ncols];
-                const double xkx = 2 * x1x - x0x + (double)orig_km1.x * h;
-                const double xky = 2 * x1y - x0y + (double)orig_km1.y * h;
-                spec[c + (long)k * ncols] = mk<R>((R)xkx, (R)xky);
-                x0x = x1x; x0y = x1y; x1x = xkx; x1y = xky;
+                const R ok = col[(long)k * ls];
+                const double xk = 2 * x1 - x0 + (double)orig_km1 * h;
+                col[(long)k * ls] = (R)xk;
+                x0 = x1; x1 = xk;
                 orig_km1 = ok;
             }
         }
@@ -281,22 +412,24 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
     const int ld = kZLines + 1;
+    const int nz = a.nz;
+    const PlanTables<R> tz = stage_plan<R>(a.pz, smem_raw + align16((size_t)nz * ld * sizeof(T)));
     const long ncols = (long)a.nxh * a.ny;
     const long bpi = (ncols + kZLines - 1) / kZLines;   // blocks per instance
     const long inst = blockIdx.x / bpi;
     const long c0 = (blockIdx.x - inst * bpi) * (long)kZLines;
     const int nl = (int)min((long)kZLines, ncols - c0);
-    const int nz = a.nz;
     T* spec = reinterpret_cast<T*>(a.spec) + inst * a.sM;
+    __syncthreads();
     for (int t = threadIdx.x; t < nz * nl; t += blockDim.x) {
         const int k = t / nl, l = t - k * nl;
-        const int slot = (a.op == 2) ? a.pz.pos[k] : k;
+        const int slot = (a.op == 2) ? tz.pos[k] : k;
         buf[slot * ld + l] = spec[c0 + l + (long)k * ncols];
     }
     if (a.op == 2) {
-        fft_batch<true, R>(buf, ld, nl, a.pz, +1);
+        fft_batch<true, R>(buf, ld, nl, a.pz, +1, tz.tw);
     } else {
-        fft_batch<false, R>(buf, ld, nl, a.pz, -1);
+        fft_batch<false, R>(buf, ld, nl, a.pz, -1, tz.tw);
         const R sc = (R)a.scale;
         for (int t = threadIdx.x; t < nz * nl; t += blockDim.x) {
             const int p = t / nl, l = t - p * nl;
@@ -305,19 +438,19 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
                 const long c = c0 + l;
                 const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
                 const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
-                const int k = a.pz.ipos[p];
+                const int k = tz.ipos[p];
                 const double ks = a.hkx[i] + a.hky[j] + a.hkz[k];
                 if (ks > 0.0) { v.x = (R)(-(double)v.x / ks); v.y = (R)(-(double)v.y / ks); }
                 else { v.x = (R)0; v.y = (R)0; }
             }
             buf[p * ld + l] = v;
         }
-        if (a.op == 0) fft_batch<true, R>(buf, ld, nl, a.pz, +1);
+        if (a.op == 0) fft_batch<true, R>(buf, ld, nl, a.pz, +1, tz.tw);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < nz * nl; t += blockDim.x) {
         const int k = t / nl, l = t - k * nl;
-        const int slot = (a.op == 1) ? a.pz.pos[k] : k;
+        const int slot = (a.op == 1) ? tz.pos[k] : k;
         spec[c0 + l + (long)k * ncols] = buf[slot * ld + l];
     }
 }
@@ -332,114 +465,144 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
 // independent CTAs with small shared memory and no cluster barriers.
 // Digit-reversed data are always read in shared-memory order and scattered
 // to global memory instead, which keeps the shared-memory accesses free of
-// bank conflicts.
+// bank conflicts.  Global loads are issued in batches (LB per thread)
+// before their shared-memory stores, so each thread keeps several loads in
+// flight.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256, 2) k_rows_fwd(const PlaneArgs a) {
+template <typename R, int MAXR>
+__global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_fwd(const PlaneArgs a) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
     const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
     const int tj = a.tj, ld = tj | 1;
+    unsigned char* tail = smem_raw + align16((size_t)n2 * ld * sizeof(T));
+    const PlanTables<R> tx = stage_plan<R>(a.px, tail);
+    const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(n2, sizeof(T)));
     const int jb = blockIdx.x * tj;
     const int inst = blockIdx.y / nz;
     const int k = blockIdx.y - inst * nz;
     const long ioff = (long)inst * a.sN;
-    const long plane = (long)nx * ny;
     const double* au = a.u + ioff;
     const double* av = a.v + ioff;
     const double* aw = a.w + ioff;
     const double* asrc = a.src ? a.src + ioff : nullptr;
-    for (int t = threadIdx.x; t < tj * n2; t += blockDim.x) {
-        const int rr = t / n2, m = t - rr * n2;
-        const int j = jb + rr;
-        const long g = (long)k * plane + (long)j * nx + 2 * m;
-        double d0, d1;
-        if (a.mode == 0) {
-            const double2 uu = *reinterpret_cast<const double2*>(au + g);
-            const double um = au[g - 2 * m + wrap(2 * m - 1, nx)];
-            const long gv = g + (long)(wrap(j - 1, ny) - j) * nx;
-            const long gw = g + (long)(wrap(k - 1, nz) - k) * plane;
-            const double2 vv = *reinterpret_cast<const double2*>(av + g);
-            const double2 vm = *reinterpret_cast<const double2*>(av + gv);
-            const double2 ww = *reinterpret_cast<const double2*>(aw + g);
-            const double2 wm = *reinterpret_cast<const double2*>(aw + gw);
-            d0 = ((uu.x - um) * a.rdx + (vv.x - vm.x) * a.rdy + (ww.x - wm.x) * a.rdz) * a.rdt;
-            d1 = ((uu.y - uu.x) * a.rdx + (vv.y - vm.y) * a.rdy + (ww.y - wm.y) * a.rdz) * a.rdt;
-        } else {
-            const double2 sv = *reinterpret_cast<const double2*>(asrc + g);
-            d0 = sv.x; d1 = sv.y;
+    constexpr int LB = 2;
+    const int total = tj * n2;
+    for (int t0 = threadIdx.x; t0 < total; t0 += LB * blockDim.x) {
+        double2 d[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int rr = t / n2, m = t - rr * n2;
+                d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + rr, m);
+            }
         }
-        buf[m * ld + rr] = mk<R>((R)d0, (R)d1);
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int rr = t / n2, m = t - rr * n2;
+                buf[m * ld + rr] = mk<R>((R)d[q].x, (R)d[q].y);
+            }
+        }
     }
-    fft_batch<false, R>(buf, ld, tj, a.px, -1);
+    fft_batch<false, R, MAXR>(buf, ld, tj, a.px, -1, tx.tw);   // its first barrier also orders the tables
     T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
     for (int t = threadIdx.x; t < tj * (n2 + 1); t += blockDim.x) {
         const int kx = t / tj, rr = t - kx * tj;
         const int k1 = (kx == n2) ? 0 : kx;
         const int k2 = (kx == 0) ? 0 : n2 - kx;
-        const T Zk = buf[a.px.pos[k1] * ld + rr];
-        const T Zc = cconj(buf[a.px.pos[k2] * ld + rr]);
-        const T E = cscale(cadd(Zk, Zc), (R)0.5);
-        const T H = cscale(cmul_si(csub(Zk, Zc), -1), (R)0.5);
-        const double2 wd = __ldg(a.twx + kx);
-        spec[(long)kx * ny + jb + rr] = cadd(E, cmul(mk<R>((R)wd.x, (R)wd.y), H));
+        spec[(long)kx * ny + jb + rr] = r2c_unpack<R>(buf[tx.pos[k1] * ld + rr], buf[tx.pos[k2] * ld + rr], twx[kx]);
     }
 }
 
 // one y transform of every kx line of a plane, in place on [k][kx][ky]
-template <typename R>
-__global__ void __launch_bounds__(256, 2) k_ylines(const PlaneArgs a, int sign, double scale) {
+template <typename R, int MAXR>
+__global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<MAXR>()) k_ylines(const PlaneArgs a, int sign,
+                                                                                  double scale) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
     const int ny = a.ny, nz = a.nz, nxh = a.nxh;
     const int ly = a.ly, ld = ly | 1;
+    const PlanTables<R> ty = stage_plan<R>(a.py, smem_raw + align16((size_t)ny * ld * sizeof(T)));
     const int inst = blockIdx.y / nz;
     const int k = blockIdx.y - inst * nz;
     const int l0 = blockIdx.x * ly;
     const int nl = min(ly, nxh - l0);
     T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + ((long)k * nxh + l0) * ny;
-    for (int t = threadIdx.x; t < nl * ny; t += blockDim.x) {
-        const int line = t / ny, e = t - line * ny;
-        buf[e * ld + line] = spec[(long)line * ny + e];
+    constexpr int LB = sizeof(R) == 8 ? 4 : 8;
+    const int total = nl * ny;
+    for (int t0 = threadIdx.x; t0 < total; t0 += LB * blockDim.x) {
+        T v[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) v[q] = spec[t];
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int line = t / ny, e = t - line * ny;
+                buf[e * ld + line] = v[q];
+            }
+        }
     }
-    fft_batch<false, R>(buf, ld, nl, a.py, sign);
+    fft_batch<false, R, MAXR>(buf, ld, nl, a.py, sign, ty.tw);
     const R sc = (R)scale;
-    for (int t = threadIdx.x; t < nl * ny; t += blockDim.x) {
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int line = t / ny, q = t - line * ny;   // q: position in shared memory
-        spec[(long)line * ny + a.py.ipos[q]] = cscale(buf[q * ld + line], sc);
+        spec[(long)line * ny + ty.ipos[q]] = cscale(buf[q * ld + line], sc);
     }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256, 2) k_rows_inv(const PlaneArgs a) {
+template <typename R, int MAXR>
+__global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_inv(const PlaneArgs a) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
     const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
     const int tj = a.tj, ld = tj | 1;
+    unsigned char* tail = smem_raw + align16((size_t)n2 * ld * sizeof(T));
+    const PlanTables<R> tx = stage_plan<R>(a.px, tail);
+    const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(n2, sizeof(T)));
     const int jb = blockIdx.x * tj;
     const int inst = blockIdx.y / nz;
     const int k = blockIdx.y - inst * nz;
     const long plane = (long)nx * ny;
     const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
     double* out = a.out + (long)inst * a.sN;
-    for (int t = threadIdx.x; t < tj * n2; t += blockDim.x) {
-        const int kk = t / tj, rr = t - kk * tj;
-        T Xk = spec[(long)kk * ny + jb + rr];
-        T Xc = spec[(long)(n2 - kk) * ny + jb + rr];
-        if (kk == 0) { Xk.y = (R)0; Xc.y = (R)0; }   // c2r ignores Im of DC and Nyquist
-        Xc = cconj(Xc);
-        const double2 wd = __ldg(a.twx + kk);
-        const T wb = mk<R>((R)wd.x, (R)-wd.y);
-        buf[kk * ld + rr] = cadd(cadd(Xk, Xc), cmul_si(cmul(wb, csub(Xk, Xc)), +1));
+    __syncthreads();   // twx staged
+    constexpr int LB = sizeof(R) == 8 ? 2 : 4;
+    const int total = tj * n2;
+    for (int t0 = threadIdx.x; t0 < total; t0 += LB * blockDim.x) {
+        T xk[LB], xc[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int kk = t / tj, rr = t - kk * tj;
+                xk[q] = spec[(long)kk * ny + jb + rr];
+                xc[q] = spec[(long)(n2 - kk) * ny + jb + rr];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * blockDim.x;
+            if (t < total) {
+                const int kk = t / tj, rr = t - kk * tj;
+                buf[kk * ld + rr] = c2r_pack<R>(xk[q], xc[q], twx[kk], kk == 0);
+            }
+        }
     }
-    fft_batch<false, R>(buf, ld, tj, a.px, +1);
+    fft_batch<false, R, MAXR>(buf, ld, tj, a.px, +1, tx.tw);
     const double sc = a.scale;
-    for (int t = threadIdx.x; t < tj * n2; t += blockDim.x) {
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int rr = t / n2, q = t - rr * n2;
-        const int m = a.px.ipos[q];
+        const int m = tx.ipos[q];
         const T z = buf[q * ld + rr];
         const long g = (long)k * plane + (long)(jb + rr) * nx + 2 * m;
         double2 o = make_double2((double)z.x * sc, (double)z.y * sc);
@@ -455,84 +618,113 @@ __global__ void __launch_bounds__(256, 2) k_rows_inv(const PlaneArgs a) {
 // launchers
 // ---------------------------------------------------------------------------
 size_t rows_smem(const PlaneArgs& a, bool fp32) {
-    return (size_t)(a.nx / 2) * (a.tj | 1) * (fp32 ? sizeof(float2) : sizeof(double2));
+    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
+    return align16((size_t)(a.nx / 2) * (a.tj | 1) * es) + tables_x_bytes(a, es);
 }
 size_t ylines_smem(const PlaneArgs& a, bool fp32) {
-    return (size_t)a.ny * (a.ly | 1) * (fp32 ? sizeof(float2) : sizeof(double2));
+    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
+    return align16((size_t)a.ny * (a.ly | 1) * es) + tables_y_bytes(a, es);
+}
+size_t plane_fwd_smem(const PlaneArgs& a, bool fp32) {
+    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
+    return align16(((size_t)a.ny * a.ldc + (size_t)(a.nx / 2) * a.ldr) * es) + tables_x_bytes(a, es) +
+           tables_y_bytes(a, es);
+}
+size_t plane_inv_smem(const PlaneArgs& a, bool fp32) { return plane_fwd_smem(a, fp32); }
+size_t plane_smem(const PlaneArgs& a, bool fp32) {
+    if (a.impl == 1) return std::max(rows_smem(a, fp32), ylines_smem(a, fp32));
+    return plane_fwd_smem(a, fp32);
 }
 
-template <typename R>
-static cudaError_t launch_split_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
+static int maxr_x(const PlaneArgs& a) { return plan_max_radix(a.px) >= 16 ? 16 : 8; }
+static int maxr_y(const PlaneArgs& a) { return plan_max_radix(a.py) >= 16 ? 16 : 8; }
+
+template <typename R, int MX, int MY>
+static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) {
     const int nb = std::max(1, a.batch);
     const dim3 grows(a.ny / a.tj, a.nz * nb), glines((a.nxh + a.ly - 1) / a.ly, a.nz * nb);
     const size_t smr = rows_smem(a, sizeof(R) == 4), sml = ylines_smem(a, sizeof(R) == 4);
     if (fwd) {
-        k_rows_fwd<R><<<grows, 256, smr, s>>>(a);
-        k_ylines<R><<<glines, 256, sml, s>>>(a, -1, a.scale);
+        k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
+        k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
     } else {
-        k_ylines<R><<<glines, 256, sml, s>>>(a, +1, 1.0);
-        k_rows_inv<R><<<grows, 256, smr, s>>>(a);
+        k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, +1, 1.0);
+        k_rows_inv<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
     }
     return cudaGetLastError();
 }
-
-size_t plane_fwd_smem(const PlaneArgs& a, bool fp32) {
-    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
-    return ((size_t)a.ny * a.ldc + (size_t)(a.nx / 2) * a.ldr) * es;
+template <typename R>
+static cudaError_t launch_split_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
+    const int mx = maxr_x(a), my = maxr_y(a);
+    if (mx == 16 && my == 16) return launch_split_m<R, 16, 16>(a, fwd, s);
+    if (mx == 16) return launch_split_m<R, 16, 8>(a, fwd, s);
+    if (my == 16) return launch_split_m<R, 8, 16>(a, fwd, s);
+    return launch_split_m<R, 8, 8>(a, fwd, s);
 }
-size_t plane_inv_smem(const PlaneArgs& a, bool fp32) { return plane_fwd_smem(a, fp32); }
 
+template <typename R, int MAXR>
+static cudaError_t setup_m() {
+    cudaError_t e;
+    const int maxsm = 227 * 1024;
+    if ((e = cudaFuncSetAttribute(k_plane_fwd<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_plane_inv<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_plane_fwd<R, MAXR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
+    if ((e = cudaFuncSetAttribute(k_plane_inv<R, MAXR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_fwd<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_rows_inv<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = cudaFuncSetAttribute(k_ylines<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    return cudaSuccess;
+}
 template <typename R>
 static cudaError_t setup_t() {
     cudaError_t e;
-    const int maxsm = 227 * 1024;
-    if ((e = cudaFuncSetAttribute(k_plane_fwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_plane_inv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_plane_fwd<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
-    if ((e = cudaFuncSetAttribute(k_plane_inv<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
-    if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_rows_fwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_rows_inv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_ylines<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    return cudaSuccess;
+    if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
+    if ((e = setup_m<R, 16>())) return e;
+    return setup_m<R, 8>();
 }
 cudaError_t plane_setup(bool fp32) { return fp32 ? setup_t<float>() : setup_t<double>(); }
 
-template <typename R, bool FWD>
-static cudaError_t launch_plane_t(const PlaneArgs& a, cudaStream_t s) {
+static cudaLaunchConfig_t plane_cfg(const PlaneArgs& a, bool fp32, cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(a.C, a.nz * std::max(1, a.batch), 1);
     cfg.blockDim = dim3(kPlaneThreads, 1, 1);
-    cfg.dynamicSmemBytes = plane_fwd_smem(a, sizeof(R) == 4);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cfg.dynamicSmemBytes = plane_fwd_smem(a, fp32);
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = a.C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (FWD) return cudaLaunchKernelEx(&cfg, k_plane_fwd<R>, a);
-    return cudaLaunchKernelEx(&cfg, k_plane_inv<R>, a);
+    return cfg;
+}
+
+template <typename R, bool FWD, int MAXR>
+static cudaError_t launch_plane_m(const PlaneArgs& a, cudaStream_t s) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = plane_cfg(a, sizeof(R) == 4, attr);
+    cfg.stream = s;
+    if (FWD) return cudaLaunchKernelEx(&cfg, k_plane_fwd<R, MAXR>, a);
+    return cudaLaunchKernelEx(&cfg, k_plane_inv<R, MAXR>, a);
+}
+template <typename R, bool FWD>
+static cudaError_t launch_plane_t(const PlaneArgs& a, cudaStream_t s) {
+    if (std::max(maxr_x(a), maxr_y(a)) >= 16) return launch_plane_m<R, FWD, 16>(a, s);
+    return launch_plane_m<R, FWD, 8>(a, s);
+}
+template <typename R, bool FWD, int MAXR>
+static int max_clusters_m(const PlaneArgs& a) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = plane_cfg(a, sizeof(R) == 4, attr);
+    int n = 0;
+    cudaError_t e = FWD ? cudaOccupancyMaxActiveClusters(&n, k_plane_fwd<R, MAXR>, &cfg)
+                        : cudaOccupancyMaxActiveClusters(&n, k_plane_inv<R, MAXR>, &cfg);
+    if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
 }
 template <typename R, bool FWD>
 static int max_clusters_t(const PlaneArgs& a) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(a.C, a.nz * std::max(1, a.batch), 1);
-    cfg.blockDim = dim3(kPlaneThreads, 1, 1);
-    cfg.dynamicSmemBytes = plane_fwd_smem(a, sizeof(R) == 4);
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = a.C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int n = 0;
-    cudaError_t e = FWD ? cudaOccupancyMaxActiveClusters(&n, k_plane_fwd<R>, &cfg)
-                        : cudaOccupancyMaxActiveClusters(&n, k_plane_inv<R>, &cfg);
-    if (e != cudaSuccess) { cudaGetLastError(); return 0; }
-    return n;
+    if (std::max(maxr_x(a), maxr_y(a)) >= 16) return max_clusters_m<R, FWD, 16>(a);
+    return max_clusters_m<R, FWD, 8>(a);
 }
 int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd) {
     if (fp32) return fwd ? max_clusters_t<float, true>(a) : max_clusters_t<float, false>(a);
@@ -549,12 +741,11 @@ cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
 }
 
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s) {
-    const long ncols = (long)a.nxh * a.ny * std::max(1, a.batch);
-    const int threads = 128;
-    const int blocks = (int)((ncols + threads - 1) / threads);
-    const size_t sm = (size_t)((a.nz + 7) / 8 + 1) * threads * sizeof(double);
-    if (fp32) k_thomas<float><<<blocks, threads, sm, s>>>(a);
-    else k_thomas<double><<<blocks, threads, sm, s>>>(a);
+    const long nthreads = 2 * (long)a.nxh * a.ny * std::max(1, a.batch);
+    const int blocks = (int)((nthreads + kThomasThreads - 1) / kThomasThreads);
+    const size_t sm = (size_t)((a.nz + kThomasChunk - 1) / kThomasChunk + 1) * kThomasThreads * sizeof(double);
+    if (fp32) k_thomas<float><<<blocks, kThomasThreads, sm, s>>>(a);
+    else k_thomas<double><<<blocks, kThomasThreads, sm, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -562,7 +753,7 @@ cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s) {
     const long ncols = (long)a.nxh * a.ny;
     const int blocks = (int)(((ncols + kZLines - 1) / kZLines) * std::max(1, a.batch));
     const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
-    const size_t sm = (size_t)a.nz * (kZLines + 1) * es;
+    const size_t sm = align16((size_t)a.nz * (kZLines + 1) * es) + plan_tables_bytes(a.nz, es);
     if (fp32) k_zsolve<float><<<blocks, 256, sm, s>>>(a);
     else k_zsolve<double><<<blocks, 256, sm, s>>>(a);
     return cudaGetLastError();

@@ -54,12 +54,12 @@ static size_t footprint_of(const ps3d_params& p) {
     const size_t ts = mixed ? 4 : 8;
     size_t b = 0;
     b += 12 * N * 8;                       // 3 state buffers x 4 fields
-    b += (mixed ? 2 : 1) * N * 8;          // p (+ refinement p2)
-    b += 12 * N * ts;                      // 3 tendency levels x 4 fields
+    b += N * 8;                            // p
+    b += 9 * N * ts + 3 * N * 8;           // 3 tendency levels x 4 fields (w always FP64)
     b += M * (mixed ? 8 : 16);             // Poisson spectral array
     b += 6 * M * 16;                       // projection spectra, g0_base, scratch
     b += 4 * 4 * N * 8;                    // balanced, base, saved, zero-order field sets
-    b += N * 8 + 12 * N * ts;              // saved p and tendencies
+    b += N * 8 + 9 * N * ts + 3 * N * 8;   // saved p and tendencies
     if (p.nz > 0) b += 3 * (size_t)p.nz * p.nz * 8;
     return b + (64u << 20);                // tables, plans, reductions, allocator slack
 }

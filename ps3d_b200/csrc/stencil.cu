@@ -13,7 +13,9 @@
 //   Adams-Bashforth 2/3               integrate.f90:87-102
 // The block owns a 32 x BY column tile and marches up in z; the three planes
 // k-1, k, k+1 of u, v, w, b (and of U_back, B_back when present) sit in a
-// shared-memory ring with a one-point halo.  Face fluxes are recomputed per
+// shared-memory ring with a one-point halo.  Each thread's tile elements and
+// their east/north neighbours are located once per block, so a plane load is
+// one offset add per field.  Face fluxes are recomputed per
 // point instead of being stored, so the kernel reads each state word once
 // from HBM and writes tendencies and the new state once.
 #include "engine.h"
@@ -32,6 +34,7 @@ struct StepSmem {
 
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
 __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) {
+    using TW = double;   // stored w tendencies stay FP64 in both paths
     constexpr int NF = BG ? 6 : 4;
     __shared__ StepSmem<BY, NF> sm;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -50,28 +53,43 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
     constexpr int TP = (kTX + 2) * (BY + 2);
 
     const double* pc = a.pc ? a.pc + ioff : nullptr;
+    // per-thread tile elements: plane offsets of the point and of its east and
+    // north neighbours, computed once (full modulo: tiles may be wider than the grid)
+    constexpr int NT = kTX * BY;
+    constexpr int EPT = (TP + NT - 1) / NT;
+    int eo[EPT], eoE[EPT], eoN[EPT];
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+        const int t = tid + e * NT;
+        const int ti = t % (kTX + 2), tj = t / (kTX + 2);
+        const int gi = ((i0 - 1 + ti) % nx + nx) % nx, gj = ((j0 - 1 + tj) % ny + ny) % ny;
+        eo[e] = gj * nx + gi;
+        eoE[e] = gj * nx + wrap(gi + 1, nx);
+        eoN[e] = wrap(gj + 1, ny) * nx + gi;
+    }
     auto load_plane = [&](int kk, int slot) {
         const int kw = wrap(kk, nz);
-        for (int t = tid; t < TP; t += kTX * BY) {
-            const int ti = t % (kTX + 2), tj = t / (kTX + 2);
-            const int gi = wrap(i0 - 1 + ti, nx), gj = wrap(j0 - 1 + tj, ny);
-            const long g = (long)kw * plane + (long)gj * nx + gi;
+        const long po = (long)kw * plane, pu = (long)wrap(kw + 1, nz) * plane;
 #pragma unroll
-            for (int f = 0; f < NF; ++f) sm.pl[f][slot][t] = __ldg(src[f] + g);
-            if (pc) {
-                // the previous step's pressure-gradient correction
-                // (pressure_solver.f90:98-110), applied where the state is read
-                const double p0 = __ldg(pc + g);
-                const double pe = __ldg(pc + g - gi + wrap(gi + 1, nx));
-                const double pn = __ldg(pc + g + (long)(wrap(gj + 1, ny) - gj) * nx);
-                sm.pl[0][slot][t] = sm.pl[0][slot][t] - a.dtp * (pe - p0) * a.rdx;
-                sm.pl[1][slot][t] = sm.pl[1][slot][t] - a.dtp * (pn - p0) * a.rdy;
-                if (a.rigid && kw == nz - 1) {
-                    sm.pl[2][slot][t] = 0.0;
-                } else {
-                    const double pt = __ldg(pc + g + (long)(wrap(kw + 1, nz) - kw) * plane);
-                    sm.pl[2][slot][t] = sm.pl[2][slot][t] - a.dtwp * (pt - p0) * a.rdz;
+        for (int e = 0; e < EPT; ++e) {
+            const int t = tid + e * NT;
+            if (t < TP) {
+                double v[NF];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) v[f] = __ldg(src[f] + po + eo[e]);
+                if (pc) {
+                    // the previous step's pressure-gradient correction
+                    // (pressure_solver.f90:98-110), applied where the state is read
+                    const double p0 = __ldg(pc + po + eo[e]);
+                    const double pe = __ldg(pc + po + eoE[e]);
+                    const double pn = __ldg(pc + po + eoN[e]);
+                    const double pt = __ldg(pc + pu + eo[e]);
+                    v[0] = v[0] - a.dtp * (pe - p0) * a.rdx;
+                    v[1] = v[1] - a.dtp * (pn - p0) * a.rdy;
+                    v[2] = (a.rigid && kw == nz - 1) ? 0.0 : v[2] - a.dtwp * (pt - p0) * a.rdz;
                 }
+#pragma unroll
+                for (int f = 0; f < NF; ++f) sm.pl[f][slot][t] = v[f];
             }
         }
     };
@@ -218,7 +236,7 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
             // ---- store tendency of time level tau
             ((TT*)a.t0[0])[g] = (TT)du_;
             ((TT*)a.t0[1])[g] = (TT)dv_;
-            ((TT*)a.t0[2])[g] = (TT)dw_;
+            ((TW*)a.t0[2])[g] = (TW)dw_;
             ((TT*)a.t0[3])[g] = (TT)db_;
             // ---- Adams-Bashforth (integrate.f90:87-102)
             if (a.do_ab) {
@@ -230,12 +248,12 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
                 if (c1 != 0.0) {
                     const TT* const* h = (const TT* const*)a.t1;
                     tu = tu + c1 * (double)h[0][g]; tv = tv + c1 * (double)h[1][g];
-                    tw = tw + c1 * (double)h[2][g]; tb = tb + c1 * (double)h[3][g];
+                    tw = tw + c1 * (double)((const TW*)a.t1[2])[g]; tb = tb + c1 * (double)h[3][g];
                 }
                 if (c2 != 0.0) {
                     const TT* const* h = (const TT* const*)a.t2;
                     tu = tu + c2 * (double)h[0][g]; tv = tv + c2 * (double)h[1][g];
-                    tw = tw + c2 * (double)h[2][g]; tb = tb + c2 * (double)h[3][g];
+                    tw = tw + c2 * (double)((const TW*)a.t2[2])[g]; tb = tb + c2 * (double)h[3][g];
                 }
                 u1 = u1 + dt * tu; v1 = v1 + dt * tv; w1 = w1 + dtw * tw; b1 = b1 + dt * tb;
             }
@@ -429,6 +447,8 @@ static cudaError_t launch_step_tt(const StepArgs& a, cudaStream_t s) {
     else { if (wm) { if (bg) L(false, true, true); else L(false, true, false); } else { if (bg) L(false, false, true); else L(false, false, false); } }
 #undef L
 }
+
+cudaError_t step_setup() { return cudaSuccess; }   // static shared memory: nothing to opt in to
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s) {
     return fp32_tendencies ? launch_step_tt<float>(a, s) : launch_step_tt<double>(a, s);
