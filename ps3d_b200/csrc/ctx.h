@@ -100,6 +100,7 @@ struct Ctx {
     DevPlan plx, ply, plz;      // radix-16/8 schedules
     DevPlan plx4, ply4;         // radix-4 schedules (autotuner alternative)
     DevPlan plx8, ply8;         // radix-8 schedules (autotuner alternative)
+    DevBuf thomas_r;            // rigid lid: Thomas factors [k][column] (constant for the grid)
     int plane_force = -1;       // PS3D_PLANE_IMPL: -1 free, 0 cluster, 1 rows + y-lines
     int kchunk = 8;             // z levels per block of the step kernel
     std::string tuned;          // description of the autotuned choice

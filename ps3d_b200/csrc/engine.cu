@@ -352,7 +352,20 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     CK(red_partials.alloc((size_t)nred * 5 * sizeof(double)));
     CK(red_out.alloc(256));   // DiagOut at 0, norm results (4 doubles) at byte 64
     CK(cudaStreamSynchronize(stream));
-    return autotune();
+    int rc = autotune();
+    if (rc) return rc;
+    if (rigid && mixed) {
+        // the vertical solve's factors depend only on the grid: built once, in
+        // the spectral column order of the plane kernels the tuner picked
+        ColumnArgs c{};
+        c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.layout = (mixed ? pa32 : pa64).impl;
+        c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p;
+        c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
+        CK(thomas_r.alloc((size_t)M * sizeof(double)));
+        CK(launch_thomas_factor(c, (double*)thomas_r.p, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+    return PS3D_OK;
 }
 
 cudaError_t Ctx::ensure_spectral4() {
@@ -777,6 +790,7 @@ int Ctx::poisson_once(double* out, double beta, bool lazy, const double* pc) {
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         c.dz2dsqr = P.dz * P.dz * P.dsqr;
+        c.rtab = f32 ? (const double*)thomas_r.p : nullptr;   // FP64: the recurrence is cheaper than the table traffic
         LAUNCH(PS3D_K_VSOLVE, launch_thomas(c, f32, stream));
     } else {
         c.pz = plz.plan; c.scale = P.dz; c.op = 0;

@@ -80,6 +80,10 @@ struct ColumnArgs {
     int batch;                     // instances (>= 1), spectral stride sM elements
     long sM;
     int layout;                    // spectral layout: 0 [k][ky][kx], 1 [k][kx][ky]
+    // rigid lid: Thomas factors [k][column] built once by launch_thomas_factor
+    // (level 0: c'(1) = c/b(1); level k >= 1: 1/(b(k) - c'(k-1) a)), or NULL
+    // to compute them on the fly
+    const double* rtab;
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
@@ -103,6 +107,7 @@ cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);
 int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd);
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s);
+cudaError_t launch_thomas_factor(const ColumnArgs& a, double* rtab, cudaStream_t s);
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
 
 // modes.cu: eigen tables for one grid and the projections

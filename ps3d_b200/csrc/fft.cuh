@@ -120,43 +120,73 @@ PS3D_HD void small_dft(T* v, int sign) {
     }
 }
 
+// Work split of one batched stage in fixed-line mode: every thread keeps one
+// line slot (nslots divides the block size) and steps through butterflies,
+// so no per-item division is needed; slots beyond the active lines idle.
+struct StageSplit {
+    int line0, bfly0, bstep;
+};
+__device__ __forceinline__ StageSplit stage_split(int nslots) {
+    StageSplit s;
+    s.line0 = threadIdx.x % nslots;
+    s.bfly0 = threadIdx.x / nslots;
+    s.bstep = blockDim.x / nslots;
+    return s;
+}
+
 template <int RAD, bool DIT, typename R>
-__device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const FFTPlan& P,
-                                          int Lp, int sign, const cpx<R>* tw) {
+__device__ __forceinline__ void fft_butterfly(cpx<R>* buf, int ld, int line, int base, int Lp, int j, int tstride,
+                                              int sign, const cpx<R>* tw) {
     using T = cpx<R>;
+    T v[RAD];
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) v[q] = buf[(base + q * Lp) * ld + line];
+    if (DIT && j) {
+#pragma unroll
+        for (int q = 1; q < RAD; ++q) {
+            T w = tw[q * j * tstride];
+            if (sign > 0) w.y = -w.y;
+            v[q] = cmul(v[q], w);
+        }
+    }
+    small_dft<RAD>(v, sign);
+    if (!DIT && j) {
+#pragma unroll
+        for (int q = 1; q < RAD; ++q) {
+            T w = tw[q * j * tstride];
+            if (sign > 0) w.y = -w.y;
+            v[q] = cmul(v[q], w);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) buf[(base + q * Lp) * ld + line] = v[q];
+}
+
+template <int RAD, bool DIT, bool FIXED, typename R>
+__device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const FFTPlan& P,
+                                          int Lp, int sign, const cpx<R>* tw, const StageSplit& sp) {
     const int n = P.n;
     const int L = Lp * RAD;
     const int tstride = n / L;
     const int nb = n / RAD;
-    const int total = nb * nlines;
-    for (int item = threadIdx.x; item < total; item += blockDim.x) {
-        const int bfly = item / nlines;
-        const int line = item - bfly * nlines;
-        const int blk = bfly / Lp;
-        const int j = bfly - blk * Lp;
-        const int base = blk * L + j;
-        T v[RAD];
-#pragma unroll
-        for (int q = 0; q < RAD; ++q) v[q] = buf[(base + q * Lp) * ld + line];
-        if (DIT && j) {
-#pragma unroll
-            for (int q = 1; q < RAD; ++q) {
-                T w = tw[q * j * tstride];
-                if (sign > 0) w.y = -w.y;
-                v[q] = cmul(v[q], w);
-            }
+    if constexpr (FIXED) {
+        if (sp.line0 >= nlines) return;
+        const bool p2 = (Lp & (Lp - 1)) == 0;
+        const int lg = __ffs(Lp) - 1;
+        for (int bfly = sp.bfly0; bfly < nb; bfly += sp.bstep) {
+            const int blk = p2 ? (bfly >> lg) : bfly / Lp;
+            const int j = bfly - blk * Lp;
+            fft_butterfly<RAD, DIT, R>(buf, ld, sp.line0, blk * L + j, Lp, j, tstride, sign, tw);
         }
-        small_dft<RAD>(v, sign);
-        if (!DIT && j) {
-#pragma unroll
-            for (int q = 1; q < RAD; ++q) {
-                T w = tw[q * j * tstride];
-                if (sign > 0) w.y = -w.y;
-                v[q] = cmul(v[q], w);
-            }
+    } else {
+        const int total = nb * nlines;
+        for (int item = threadIdx.x; item < total; item += blockDim.x) {
+            const int bfly = item / nlines;
+            const int line = item - bfly * nlines;
+            const int blk = bfly / Lp;
+            const int j = bfly - blk * Lp;
+            fft_butterfly<RAD, DIT, R>(buf, ld, line, blk * L + j, Lp, j, tstride, sign, tw);
         }
-#pragma unroll
-        for (int q = 0; q < RAD; ++q) buf[(base + q * Lp) * ld + line] = v[q];
     }
 }
 
@@ -164,21 +194,25 @@ __device__ __forceinline__ void fft_stage(cpx<R>* buf, int ld, int nlines, const
 // synchronises the block before returning.  tw: the plan's twiddles staged
 // in shared memory (stage_plan).  MAXR is the largest radix instantiated:
 // kernels built with MAXR = 8 hold fewer registers and run more blocks per
-// SM, and only take plans without radix-16 stages.
-template <bool DIT, typename R, int MAXR = 16>
-__device__ void fft_batch(cpx<R>* buf, int ld, int nlines, const FFTPlan& P, int sign, const cpx<R>* tw) {
+// SM, and only take plans without radix-16 stages.  NSLOTS > 0 selects the
+// fixed-line split (NSLOTS must divide the block size, nlines <= NSLOTS is
+// passed at run time); 0 splits (butterfly, line) items.
+template <bool DIT, typename R, int MAXR = 16, bool FIXED = false>
+__device__ void fft_batch(cpx<R>* buf, int ld, int nlines, const FFTPlan& P, int sign, const cpx<R>* tw,
+                          int nslots = 0) {
     __syncthreads();
+    const StageSplit sp = stage_split(FIXED ? nslots : 1);
     for (int s0 = 0; s0 < P.nst; ++s0) {
         const int st = DIT ? s0 : P.nst - 1 - s0;
         const int Lp = P.lp[st];
         switch (P.r[st]) {
-            case 2: fft_stage<2, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
-            case 3: fft_stage<3, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
-            case 4: fft_stage<4, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
-            case 5: fft_stage<5, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
-            case 8: fft_stage<8, DIT, R>(buf, ld, nlines, P, Lp, sign, tw); break;
+            case 2: fft_stage<2, DIT, FIXED, R>(buf, ld, nlines, P, Lp, sign, tw, sp); break;
+            case 3: fft_stage<3, DIT, FIXED, R>(buf, ld, nlines, P, Lp, sign, tw, sp); break;
+            case 4: fft_stage<4, DIT, FIXED, R>(buf, ld, nlines, P, Lp, sign, tw, sp); break;
+            case 5: fft_stage<5, DIT, FIXED, R>(buf, ld, nlines, P, Lp, sign, tw, sp); break;
+            case 8: fft_stage<8, DIT, FIXED, R>(buf, ld, nlines, P, Lp, sign, tw, sp); break;
             case 16:
-                if constexpr (MAXR >= 16) fft_stage<16, DIT, R>(buf, ld, nlines, P, Lp, sign, tw);
+                if constexpr (MAXR >= 16) fft_stage<16, DIT, FIXED, R>(buf, ld, nlines, P, Lp, sign, tw, sp);
                 break;
             default: break;
         }

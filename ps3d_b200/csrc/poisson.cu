@@ -33,7 +33,7 @@ constexpr int kPlaneThreads = 256;
 // blocks per SM the plane kernels are built for: the radix-16 instantiation
 // needs ~128 FP64 registers, the radix-8 one fits in 80
 template <int MAXR> constexpr int plane_min_blocks() { return MAXR >= 16 ? 2 : 3; }
-template <int MAXR> constexpr int lines_min_blocks() { return MAXR >= 16 ? 2 : 4; }
+template <typename R, int MAXR> constexpr int lines_min_blocks() { return MAXR >= 16 ? 2 : 4; }
 
 // Divergence of the pair of points (2m, 2m+1) of row j in plane k, divided by
 // dt (pressure_solver.f90:16-24), or the pair of source values (mode 1).
@@ -308,7 +308,71 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
     const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
     const double ks = a.hkx[i] + a.hky[j];
     const double fxa = a.fxa;
-    if (ks > 0) {
+    if (ks > 0 && a.rtab) {
+        // factors from the table: the same values the recurrence below forms
+        const double* rt = a.rtab + c;
+        const double bend = -ks - fxa;
+        double dp = 0.0;
+        R nxt[KC];
+        double rn[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q)
+            if (q < nz) { nxt[q] = col[(long)q * ls]; rn[q] = __ldg(rt + (long)q * ncols); }
+        for (int kb = 0; kb < nz; kb += KC) {
+            R d[KC];
+            double r[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) { d[q] = nxt[q]; r[q] = rn[q]; }
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + KC + q < nz) {
+                    nxt[q] = col[(long)(kb + KC + q) * ls];
+                    rn[q] = __ldg(rt + (long)(kb + KC + q) * ncols);
+                }
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int k = kb + q;
+                if (k < nz) {
+                    if (k == 0) dp = (double)d[q] / bend;               // dp(1) = d(1)/b(1)
+                    else dp = ((double)d[q] - dp * fxa) * r[q];
+                    d[q] = (R)dp;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + q < nz) col[(long)(kb + q) * ls] = d[q];
+        }
+        double x = dp;   // x(nz) = dp(nz)
+        const int last = (nz - 1) / KC;
+#pragma unroll
+        for (int q = 0; q < KC; ++q)
+            if (last * KC + q < nz - 1) { nxt[q] = col[(long)(last * KC + q) * ls]; rn[q] = __ldg(rt + (long)(last * KC + q) * ncols); }
+        for (int sg = last; sg >= 0; --sg) {
+            const int kb = sg * KC;
+            R d[KC];
+            double r[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) { d[q] = nxt[q]; r[q] = rn[q]; }
+            if (sg > 0) {
+#pragma unroll
+                for (int q = 0; q < KC; ++q) {
+                    nxt[q] = col[(long)(kb - KC + q) * ls];
+                    rn[q] = __ldg(rt + (long)(kb - KC + q) * ncols);
+                }
+            }
+#pragma unroll
+            for (int q = KC - 1; q >= 0; --q) {
+                const int k = kb + q;
+                if (k >= nz - 1) continue;
+                const double cpk = k == 0 ? r[q] : fxa * r[q];          // c'(k)
+                x = (double)d[q] - cpk * x;
+                d[q] = (R)x;
+            }
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + q < nz - 1) col[(long)(kb + q) * ls] = d[q];
+        }
+    } else if (ks > 0) {
         const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
         double cp = 0.0, dp = 0.0;
         R nxt[KC];
@@ -397,6 +461,33 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
                 orig_km1 = ok;
             }
         }
+    }
+}
+
+// Thomas factors of every column with ks > 0, built once per grid with the
+// arithmetic of the recurrence in k_thomas: level 0 holds c'(1) = c/b(1),
+// level k >= 1 holds 1/(b(k) - c'(k-1) a) (c'(k) = a times it).
+__global__ void k_thomas_factor(const ColumnArgs a, double* __restrict__ rtab) {
+    const long ncols = (long)a.nxh * a.ny;
+    const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
+    const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
+    const double ks = a.hkx[i] + a.hky[j];
+    const double fxa = a.fxa;
+    const int nz = a.nz;
+    if (!(ks > 0)) {
+        for (int k = 0; k < nz; ++k) rtab[(long)k * ncols + c] = 0.0;
+        return;
+    }
+    const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+    double cp = fxa / bend;
+    rtab[c] = cp;
+    for (int k = 1; k < nz; ++k) {
+        const double bk = (k == nz - 1) ? bend : bmid;
+        const double r = __drcp_rn(bk - cp * fxa);
+        cp = fxa * r;
+        rtab[(long)k * ncols + c] = r;
     }
 }
 
@@ -508,7 +599,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
             }
         }
     }
-    fft_batch<false, R, MAXR>(buf, ld, tj, a.px, -1, tx.tw);   // its first barrier also orders the tables
+    fft_batch<false, R, MAXR, true>(buf, ld, tj, a.px, -1, tx.tw, tj);   // its first barrier also orders the tables
     T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
     for (int t = threadIdx.x; t < tj * (n2 + 1); t += blockDim.x) {
         const int kx = t / tj, rr = t - kx * tj;
@@ -520,7 +611,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
 
 // one y transform of every kx line of a plane, in place on [k][kx][ky]
 template <typename R, int MAXR>
-__global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<MAXR>()) k_ylines(const PlaneArgs a, int sign,
+__global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_ylines(const PlaneArgs a, int sign,
                                                                                   double scale) {
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -551,7 +642,7 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<MAXR>()) k_yli
             }
         }
     }
-    fft_batch<false, R, MAXR>(buf, ld, nl, a.py, sign, ty.tw);
+    fft_batch<false, R, MAXR, true>(buf, ld, nl, a.py, sign, ty.tw, ly);
     const R sc = (R)scale;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int line = t / ny, q = t - line * ny;   // q: position in shared memory
@@ -598,7 +689,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
             }
         }
     }
-    fft_batch<false, R, MAXR>(buf, ld, tj, a.px, +1, tx.tw);
+    fft_batch<false, R, MAXR, true>(buf, ld, tj, a.px, +1, tx.tw, tj);
     const double sc = a.scale;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int rr = t / n2, q = t - rr * n2;
@@ -746,6 +837,12 @@ cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s) {
     const size_t sm = (size_t)((a.nz + kThomasChunk - 1) / kThomasChunk + 1) * kThomasThreads * sizeof(double);
     if (fp32) k_thomas<float><<<blocks, kThomasThreads, sm, s>>>(a);
     else k_thomas<double><<<blocks, kThomasThreads, sm, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_thomas_factor(const ColumnArgs& a, double* rtab, cudaStream_t s) {
+    const long ncols = (long)a.nxh * a.ny;
+    k_thomas_factor<<<(int)((ncols + 127) / 128), 128, 0, s>>>(a, rtab);
     return cudaGetLastError();
 }
 

@@ -57,6 +57,7 @@ static size_t footprint_of(const ps3d_params& p) {
     b += N * 8;                            // p
     b += 9 * N * ts + 3 * N * 8;           // 3 tendency levels x 4 fields (w always FP64)
     b += M * (mixed ? 8 : 16);             // Poisson spectral array
+    if (p.enable_vertical_boundaries && mixed) b += M * 8;   // Thomas factors
     b += 6 * M * 16;                       // projection spectra, g0_base, scratch
     b += 4 * 4 * N * 8;                    // balanced, base, saved, zero-order field sets
     b += N * 8 + 9 * N * ts + 3 * N * 8;   // saved p and tendencies
