@@ -40,6 +40,15 @@ def set_grid(nx, ny, nz):
     NX, NY, NZ = nx, ny, nz
     WORKLOAD = f"jets {nx}x{ny}x{nz} rigid lid AB3 Laplacian friction"
 
+# DRAM bytes per grid point per launch of the step kernel, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) at 256x256x64, where its
+# traffic already streams far beyond L2, so it scales with the grid points;
+# commands and tables in profiles/hot_kernels_{fp64,mixed}_256x256x64.md.
+MEASURED_TRAFFIC_PER_POINT = {
+    "fp64": {"step": 167.9},
+    "mixed": {"step": 131.1},
+}
+
 # algorithmic HBM bytes per grid point per launch.  The step kernel reads
 # u,v,w,b, 2 AB history slots x 4 fields and the pending pressure (the
 # previous projection's gradient is applied while loading), and writes 4
@@ -211,7 +220,12 @@ def e2e_run(precision, steps, dev):
     m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
     m.run(3)                      # warm the kernels
     names = ("u", "v", "w", "b", "p")
-    host = {n: np.ascontiguousarray(f.get(n, np.zeros_like(f["u"]))) for n in names}
+    host = {}
+    for n in names:   # page-locked host arrays, as a host code would keep its state
+        a = torch.empty(f["u"].shape, dtype=torch.float64, pin_memory=True).numpy()
+        a[...] = f[n] if n in f else 0.0
+        host[n] = a
+    out = {n: torch.empty(f["u"].shape, dtype=torch.float64, pin_memory=True).numpy() for n in names}
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     m.upload(**host, itt=0, tau=3, taum1=2, taum2=1)
@@ -224,7 +238,7 @@ def e2e_run(precision, steps, dev):
             ndiag += 1
         tau, t1, t2 = tau % 3 + 1, t1 % 3 + 1, t2 % 3 + 1
         itt += 1
-    out = m.download(tendencies=False)
+    m.download_into(out)
     t = time.perf_counter() - t0
     m.close()
     field_bytes = host["u"].nbytes
@@ -356,12 +370,12 @@ def main():
     ap.add_argument("--serve", type=int, default=1, help="also run the serving workload")
     args = ap.parse_args()
     set_grid(args.nx, args.ny, args.nz)
-    world, rank, local, pg = dist_setup()
     unit = "grid-point-steps/s"
     metric = f"grid-point-steps/s of the ps3D time step, {NX}x{NY}x{NZ} jets, mixed FP32/FP64 path (FP64 path beside)"
 
     if args.impl == "reference":
-        if rank != 0:
+        # the CPU restatement on the host cores: rank 0 alone, no process group
+        if int(os.environ.get("RANK", "0")) != 0:
             return
         steps = max(1, args.steps)
         val, cores, n = cpu_baseline_run(steps, warmup_steps=min(max(args.warmup, 1), 2), budget_s=150.0)
@@ -377,6 +391,7 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
+    world, rank, local, pg = dist_setup()
     import torch
     from ps3d_b200 import build as b
     from ps3d_b200 import abi
@@ -424,7 +439,10 @@ def main():
                        "l2": "inputs larger than L2 (state > 1 GB)" if npts >= 2 ** 23 else "small case"},
             "kernels": head["roof"],
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_v["achieved_gbs"], "peak": peak,
-                         "unit": "GB/s", "frac": (dom_v["achieved_gbs"] or 0) / peak, "traffic": None,
+                         "unit": "GB/s", "frac": (dom_v["achieved_gbs"] or 0) / peak,
+                         "traffic": (MEASURED_TRAFFIC_PER_POINT[hname].get(dom_name, 0) * npts or None),
+                         "traffic_unit": "DRAM bytes per launch (ncu, scaled by grid points)",
+                         "algorithmic_bytes": BYTES_PER_POINT[hname].get(dom_name, 0) * npts,
                          "peak_kind": peak_kind},
             "gpu_launches": int(launches), "clocks": head["clk"]}
     if "fp64" in res:

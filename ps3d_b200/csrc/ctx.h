@@ -183,8 +183,8 @@ struct Ctx {
     cudaError_t copy_state_to(int set);
     cudaError_t copy_set_to_state(int set);
 
-    void gather(const double* h, double* dst) const;
-    void scatter(const double* src, double* h, int kind) const;
+    int upload_raw(void* dev, const double* h, bool f32);
+    int download_raw(const void* dev, double* h, bool pghost, bool f32);
     int upload_field(double* dev, const double* h);
     double* member_field(int f, int m) { return field(f) + (size_t)m * N; }
     int download_field(const double* dev, double* h, int kind);

@@ -1107,61 +1107,42 @@ cudaError_t Ctx::ensure_saved_tail() {
 // ---------------------------------------------------------------------------
 cudaError_t Ctx::ensure_staging() {
     if (staging.p) return cudaSuccess;
-    return staging.alloc_host(N * sizeof(double));
+    return staging.alloc((size_t)(nx + 4) * (ny + 4) * (nz + 4) * sizeof(double));
 }
-void Ctx::gather(const double* h, double* dst) const {
-    const long sy = nx + 4, sz = (long)(nx + 4) * (ny + 4);
-    for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < ny; ++j)
-            std::memcpy(dst + ((long)k * ny + j) * nx, h + 2 + sy * (j + 2) + sz * (k + 2), nx * sizeof(double));
+// One contiguous copy of the host array into device staging, then the
+// interior is extracted on the device.  The stream is synchronised before
+// returning, so the caller may reuse the host array at once.
+int Ctx::upload_raw(void* dev, const double* h, bool f32) {
+    CK(ensure_staging());
+    const size_t n3 = (size_t)(nx + 4) * (ny + 4) * (nz + 4);
+    CK(cudaMemcpyAsync(staging.p, h, n3 * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CK(launch_from_halo((const double*)staging.p, dev, nx, ny, nz, f32, stream));
+    CK(cudaStreamSynchronize(stream));
+    return PS3D_OK;
 }
-void Ctx::scatter(const double* src, double* h, int kind) const {
-    const long sy = nx + 4, sz = (long)(nx + 4) * (ny + 4);
-    for (int kk = -1; kk <= nz + 2; ++kk) {
-        int k = ((kk - 1) % nz + nz) % nz;   // periodic copy of every halo point
-        if (kind == 1 && rigid) k = kk < 1 ? 0 : (kk > nz ? nz - 1 : kk - 1);   // p ghost levels (:82-93)
-        for (int jj = -1; jj <= ny + 2; ++jj) {
-            const int j = ((jj - 1) % ny + ny) % ny;
-            const double* row = src + ((long)k * ny + j) * nx;
-            double* out = h + sy * (jj + 1) + sz * (kk + 1);
-            out[0] = row[nx - 2]; out[1] = row[nx - 1];
-            std::memcpy(out + 2, row, nx * sizeof(double));
-            out[nx + 2] = row[0]; out[nx + 3] = row[1];
-        }
-    }
+int Ctx::download_raw(const void* dev, double* h, bool pghost, bool f32) {
+    CK(ensure_staging());
+    const size_t n3 = (size_t)(nx + 4) * (ny + 4) * (nz + 4);
+    CK(launch_to_halo(dev, (double*)staging.p, nx, ny, nz, pghost, f32, stream));
+    CK(cudaMemcpyAsync(h, staging.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return PS3D_OK;
 }
 int Ctx::upload_field(double* dev, const double* h) {
     if (!h) return PS3D_OK;
-    CK(ensure_staging());
-    gather(h, (double*)staging.p);
-    CK(cudaMemcpyAsync(dev, staging.p, N * sizeof(double), cudaMemcpyHostToDevice, stream));
-    CK(cudaStreamSynchronize(stream));
-    return PS3D_OK;
+    return upload_raw(dev, h, false);
 }
 int Ctx::download_field(const double* dev, double* h, int kind) {
     if (!h) return PS3D_OK;
-    CK(ensure_staging());
-    CK(cudaMemcpyAsync(staging.p, dev, N * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-    scatter((const double*)staging.p, h, kind);
-    return PS3D_OK;
+    return download_raw(dev, h, kind == 1 && rigid, false);
 }
 int Ctx::upload_tend(int f, const double* h) {
     const long n3 = (long)(nx + 4) * (ny + 4) * (nz + 4);
     for (int s = 0; s < 3; ++s) {
         char* dev = (char*)tend[f].p + (size_t)s * N * tsz(f);
         if (!h) { CK(cudaMemsetAsync(dev, 0, N * tsz(f), stream)); continue; }
-        CK(ensure_staging());
-        gather(h + s * n3, (double*)staging.p);
-        if (tsz(f) == sizeof(float)) {
-            std::vector<float> tmp(N);
-            const double* d = (const double*)staging.p;
-            for (long t = 0; t < N; ++t) tmp[t] = (float)d[t];
-            CK(cudaMemcpy(dev, tmp.data(), N * sizeof(float), cudaMemcpyHostToDevice));
-        } else {
-            CK(cudaMemcpyAsync(dev, staging.p, N * sizeof(double), cudaMemcpyHostToDevice, stream));
-            CK(cudaStreamSynchronize(stream));
-        }
+        int rc = upload_raw(dev, h + s * n3, tsz(f) == sizeof(float));
+        if (rc) return rc;
     }
     CK(cudaStreamSynchronize(stream));
     return PS3D_OK;
@@ -1169,19 +1150,10 @@ int Ctx::upload_tend(int f, const double* h) {
 int Ctx::download_tend(int f, double* h) {
     if (!h) return PS3D_OK;
     const long n3 = (long)(nx + 4) * (ny + 4) * (nz + 4);
-    CK(ensure_staging());
     for (int s = 0; s < 3; ++s) {
         const char* dev = (const char*)tend[f].p + (size_t)s * N * tsz(f);
-        if (tsz(f) == sizeof(float)) {
-            std::vector<float> tmp(N);
-            CK(cudaMemcpy(tmp.data(), dev, N * sizeof(float), cudaMemcpyDeviceToHost));
-            double* d = (double*)staging.p;
-            for (long t = 0; t < N; ++t) d[t] = tmp[t];
-        } else {
-            CK(cudaMemcpyAsync(staging.p, dev, N * sizeof(double), cudaMemcpyDeviceToHost, stream));
-            CK(cudaStreamSynchronize(stream));
-        }
-        scatter((const double*)staging.p, h + s * n3, 0);
+        int rc = download_raw(dev, h + s * n3, false, tsz(f) == sizeof(float));
+        if (rc) return rc;
     }
     return PS3D_OK;
 }

@@ -132,6 +132,12 @@ cudaError_t launch_project(const ProjArgs& a, cudaStream_t s);
 cudaError_t launch_vert_mode(const double2* in, double2* out, const double* mode, int nz, long ncol,
                              double scale, int transpose, cudaStream_t s);
 
+// layout.cu: host halo layout <-> device interior layout (h_dev holds the
+// whole host array, (nx+4)*(ny+4)*(nz+4) doubles)
+cudaError_t launch_from_halo(const double* h_dev, void* dst, int nx, int ny, int nz, bool f32, cudaStream_t s);
+cudaError_t launch_to_halo(const void* src, double* h_dev, int nx, int ny, int nz, bool pghost, bool f32,
+                           cudaStream_t s);
+
 // reduce.cu
 struct DiagOut { double ke, pe, umax, wmax; unsigned flags; };
 cudaError_t launch_diagnose(const double* u, const double* v, const double* w, const double* b, const double* p,

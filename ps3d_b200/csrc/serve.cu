@@ -62,6 +62,7 @@ static size_t footprint_of(const ps3d_params& p) {
     b += 4 * 4 * N * 8;                    // balanced, base, saved, zero-order field sets
     b += N * 8 + 9 * N * ts + 3 * N * 8;   // saved p and tendencies
     if (p.nz > 0) b += 3 * (size_t)p.nz * p.nz * 8;
+    b += (size_t)(p.nx + 4) * (p.ny + 4) * (p.nz + 4) * 8;   // host-layout staging
     return b + (64u << 20);                // tables, plans, reductions, allocator slack
 }
 

@@ -128,6 +128,17 @@ class Model:
         out["itt"], out["tau"], out["taum1"], out["taum2"] = (t.value for t in tl)
         return out
 
+    def download_into(self, out):
+        """Like download(tendencies=False), into caller-owned C-contiguous
+        float64 arrays out["u"], ..., out["p"] of the halo shape (e.g. pinned)."""
+        for n in ("u", "v", "w", "b", "p"):
+            a = out[n]
+            if a.shape != self.shape or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"download_into: {n} must be C-contiguous float64 of shape {self.shape}")
+        _check(self.L.ps3d_download_state(self.h, *[dptr(out[n]) for n in ("u", "v", "w", "b", "p")],
+                                          None, None, None, None, None, None, None, None), "ps3d_download_state")
+        return out
+
     def get_fields(self, which=abi.PS3D_FIELDS_STATE):
         out = [np.zeros(self.shape) for _ in range(4)]
         _check(self.L.ps3d_get_fields(self.h, which, *[dptr(a) for a in out]), "ps3d_get_fields")
