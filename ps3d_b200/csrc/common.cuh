@@ -55,6 +55,27 @@ struct FFTPlan {
 };
 
 // ---------------------------------------------------------------------------
+// Division by a run-time invariant divisor 1 <= d < 2^31, for numerators
+// 0 <= n < 2^31, by one multiply-high, one add and one shift: the round-up
+// method of Granlund & Montgomery, "Division by invariant integers using
+// multiplication" (PLDI 1994).  With l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, n / d = (mulhi(m, n) + n) >> l.
+// ---------------------------------------------------------------------------
+struct FastDiv {
+    unsigned d, m;
+    int l;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d ? d : 1;
+    f.l = 0;
+    while ((1ull << f.l) < f.d) ++f.l;
+    f.m = (unsigned)((((1ull << 32) * ((1ull << f.l) - f.d)) / f.d) + 1);
+    return f;
+}
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) { return (__umulhi(n, f.m) + n) >> f.l; }
+
+// ---------------------------------------------------------------------------
 // periodic index helpers
 // ---------------------------------------------------------------------------
 PS3D_HD int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }

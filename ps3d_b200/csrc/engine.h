@@ -64,6 +64,7 @@ struct PlaneArgs {
     int impl;                      // 0: one cluster per plane (DSMEM), 1: rows pass + y-lines pass
     int tj;                        // impl 1: rows per CTA of the rows passes
     int ly;                        // impl 1: lines per CTA of the y-lines passes
+    FastDiv fd_n2, fd_ny, fd_tj;   // set by the launchers
 };
 
 struct ColumnArgs {
@@ -84,6 +85,7 @@ struct ColumnArgs {
     // (level 0: c'(1) = c/b(1); level k >= 1: 1/(b(k) - c'(k-1) a)), or NULL
     // to compute them on the fly
     const double* rtab;
+    FastDiv fd_ncols, fd_ny, fd_nxh;   // set by the launchers
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);

@@ -298,14 +298,15 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
     const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (gid >= 2 * ncols * a.batch) return;
     const int part = (int)(gid & 1);
-    const long cb = gid >> 1;
-    const long inst = cb / ncols;
-    const long c = cb - inst * ncols;
-    R* col = reinterpret_cast<R*>(a.spec) + 2 * (inst * a.sM + c) + part;
+    const unsigned cb = (unsigned)(gid >> 1);
+    const unsigned inst = fdiv(cb, a.fd_ncols);
+    const unsigned c = cb - inst * (unsigned)ncols;
+    R* col = reinterpret_cast<R*>(a.spec) + 2 * ((long)inst * a.sM + c) + part;
     const long ls = 2 * ncols;   // level stride in R
     const int nz = a.nz;
-    const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
-    const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
+    const unsigned q0 = fdiv(c, a.layout ? a.fd_ny : a.fd_nxh);
+    const int i = a.layout ? (int)q0 : (int)(c - q0 * (unsigned)a.nxh);
+    const int j = a.layout ? (int)(c - q0 * (unsigned)a.ny) : (int)q0;
     const double ks = a.hkx[i] + a.hky[j];
     const double fxa = a.fxa;
     if (ks > 0 && a.rtab) {
@@ -586,7 +587,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * blockDim.x;
             if (t < total) {
-                const int rr = t / n2, m = t - rr * n2;
+                const int rr = (int)fdiv(t, a.fd_n2), m = t - rr * n2;
                 d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + rr, m);
             }
         }
@@ -594,7 +595,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * blockDim.x;
             if (t < total) {
-                const int rr = t / n2, m = t - rr * n2;
+                const int rr = (int)fdiv(t, a.fd_n2), m = t - rr * n2;
                 buf[m * ld + rr] = mk<R>((R)d[q].x, (R)d[q].y);
             }
         }
@@ -602,7 +603,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     fft_batch<false, R, MAXR, true>(buf, ld, tj, a.px, -1, tx.tw, tj);   // its first barrier also orders the tables
     T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
     for (int t = threadIdx.x; t < tj * (n2 + 1); t += blockDim.x) {
-        const int kx = t / tj, rr = t - kx * tj;
+        const int kx = (int)fdiv(t, a.fd_tj), rr = t - kx * tj;
         const int k1 = (kx == n2) ? 0 : kx;
         const int k2 = (kx == 0) ? 0 : n2 - kx;
         spec[(long)kx * ny + jb + rr] = r2c_unpack<R>(buf[tx.pos[k1] * ld + rr], buf[tx.pos[k2] * ld + rr], twx[kx]);
@@ -637,7 +638,7 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * blockDim.x;
             if (t < total) {
-                const int line = t / ny, e = t - line * ny;
+                const int line = (int)fdiv(t, a.fd_ny), e = t - line * ny;
                 buf[e * ld + line] = v[q];
             }
         }
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_
     fft_batch<false, R, MAXR, true>(buf, ld, nl, a.py, sign, ty.tw, ly);
     const R sc = (R)scale;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        const int line = t / ny, q = t - line * ny;   // q: position in shared memory
+        const int line = (int)fdiv(t, a.fd_ny), q = t - line * ny;   // q: position in shared memory
         spec[(long)line * ny + ty.ipos[q]] = cscale(buf[q * ld + line], sc);
     }
 }
@@ -675,7 +676,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * blockDim.x;
             if (t < total) {
-                const int kk = t / tj, rr = t - kk * tj;
+                const int kk = (int)fdiv(t, a.fd_tj), rr = t - kk * tj;
                 xk[q] = spec[(long)kk * ny + jb + rr];
                 xc[q] = spec[(long)(n2 - kk) * ny + jb + rr];
             }
@@ -684,7 +685,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * blockDim.x;
             if (t < total) {
-                const int kk = t / tj, rr = t - kk * tj;
+                const int kk = (int)fdiv(t, a.fd_tj), rr = t - kk * tj;
                 buf[kk * ld + rr] = c2r_pack<R>(xk[q], xc[q], twx[kk], kk == 0);
             }
         }
@@ -692,7 +693,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     fft_batch<false, R, MAXR, true>(buf, ld, tj, a.px, +1, tx.tw, tj);
     const double sc = a.scale;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        const int rr = t / n2, q = t - rr * n2;
+        const int rr = (int)fdiv(t, a.fd_n2), q = t - rr * n2;
         const int m = tx.ipos[q];
         const T z = buf[q * ld + rr];
         const long g = (long)k * plane + (long)(jb + rr) * nx + 2 * m;
@@ -745,7 +746,11 @@ static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) 
     return cudaGetLastError();
 }
 template <typename R>
-static cudaError_t launch_split_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
+static cudaError_t launch_split_t(const PlaneArgs& a0, bool fwd, cudaStream_t s) {
+    PlaneArgs a = a0;
+    a.fd_n2 = make_fastdiv(a.nx / 2);
+    a.fd_ny = make_fastdiv(a.ny);
+    a.fd_tj = make_fastdiv(a.tj);
     const int mx = maxr_x(a), my = maxr_y(a);
     if (mx == 16 && my == 16) return launch_split_m<R, 16, 16>(a, fwd, s);
     if (mx == 16) return launch_split_m<R, 16, 8>(a, fwd, s);
@@ -831,7 +836,11 @@ cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
     return fp32 ? launch_plane_t<float, false>(a, s) : launch_plane_t<double, false>(a, s);
 }
 
-cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s) {
+cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
+    ColumnArgs a = a0;
+    a.fd_ncols = make_fastdiv((unsigned)((long)a.nxh * a.ny));
+    a.fd_ny = make_fastdiv(a.ny);
+    a.fd_nxh = make_fastdiv(a.nxh);
     const long nthreads = 2 * (long)a.nxh * a.ny * std::max(1, a.batch);
     const int blocks = (int)((nthreads + kThomasThreads - 1) / kThomasThreads);
     const size_t sm = (size_t)((a.nz + kThomasChunk - 1) / kThomasChunk + 1) * kThomasThreads * sizeof(double);
