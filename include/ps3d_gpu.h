@@ -176,11 +176,40 @@ PS3D_API int ps3d_project_geostrophic(ps3d_ctx* ctx, int mode);
 PS3D_API int ps3d_opt_balance(ps3d_ctx* ctx, const ps3d_optbal* opt,
                      double* final_norm, int* iters);
 
+/* diag_balance (diag_balance.f90:89-106) without its netCDF output: the
+ * Warn-et-al. normal-mode balance of the current state to `order` (0..3):
+ * diag_balance_zero_order (:109-132), _first_order (:135-176),
+ * _second_order (:180-272) and _third_order (:275-362), with model_nonlin
+ * (:500-535) and model_run (:465-497).  The components u0..b0, u1..b1,
+ * u2..b2, u3..b3 are read with ps3d_get_fields(PS3D_FIELDS_ZERO .. _THIRD);
+ * the balanced state is their sum (for_config/eddy1.f90:111-133).
+ * filter_width >= 0 turns on enable_diag_balance_filter with
+ * diag_balance_filter_width = filter_width (main_module.f90:22-23); < 0
+ * leaves it off.  The model state and time levels are unchanged.         */
+PS3D_API int ps3d_diag_balance(ps3d_ctx* ctx, int order, int filter_width);
+
+/* write_restart / read_restart (restart.f90:2-82) for one rank: the file
+ * the reference writes as restart_pe=000000000.dta, a Fortran unformatted
+ * sequential file with 4-byte record markers holding (nx, ny, nz, itt,
+ * time, taum2, taum1, tau), the rank bounds (1, nx, 1, ny, 1, nz) and
+ * u, v, w, b, p, du, dv, dw, db in the halo layout.  Records longer than
+ * 2147483639 bytes are split into subrecords with negative continuation
+ * markers (gfortran's layout for records beyond 2 GiB).  read_restart
+ * returns PS3D_ERR_BADPARAM where the reference aborts (grid or bounds
+ * mismatch, short or malformed file) and stores the file's time in *time
+ * (the reference adds it to runlen); itt, time and the time levels of the
+ * context are set from the file.                                            */
+PS3D_API int ps3d_write_restart(ps3d_ctx* ctx, const char* path);
+PS3D_API int ps3d_read_restart(ps3d_ctx* ctx, const char* path, double* time);
+
 /* Auxiliary field sets in halo layout (u,v,w,b; any may be NULL).          */
 #define PS3D_FIELDS_STATE    0   /* u, v, w, b                         */
 #define PS3D_FIELDS_BALANCED 1   /* u_bal..b_bal  (diag_opt_balance)   */
 #define PS3D_FIELDS_BASE     2   /* u_base..b_base                     */
 #define PS3D_FIELDS_ZERO     3   /* u0..b0 (diag_balance_zero_order)   */
+#define PS3D_FIELDS_FIRST    4   /* u1..b1 (diag_balance_first_order)  */
+#define PS3D_FIELDS_SECOND   5   /* u2..b2 (diag_balance_second_order) */
+#define PS3D_FIELDS_THIRD    6   /* u3..b3 (diag_balance_third_order)  */
 PS3D_API int ps3d_get_fields(ps3d_ctx* ctx, int which,
                     double* u, double* v, double* w, double* b);
 

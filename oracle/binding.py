@@ -21,7 +21,9 @@ FIELD_IDS = {"u": 0, "v": 1, "w": 2, "b": 3, "p": 4,
              "du": 5, "dv": 8, "dw": 11, "db": 14,
              "u_bal": 20, "v_bal": 21, "w_bal": 22, "b_bal": 23,
              "u_base": 24, "v_base": 25, "w_base": 26, "b_base": 27,
-             "u0": 28, "v0": 29, "w0": 30, "b0": 31}
+             "u0": 28, "v0": 29, "w0": 30, "b0": 31,
+             "u1": 32, "v1": 33, "w1": 34, "b1": 35, "u2": 36, "v2": 37, "w2": 38, "b2": 39,
+             "u3": 40, "v3": 41, "w3": 42, "b3": 43}
 
 
 def build():
@@ -50,6 +52,7 @@ def lib():
         L.ps3d_oracle_integrate.argtypes = [vp, C.c_int]
         L.ps3d_oracle_pressure_solver.argtypes = [vp]
         L.ps3d_oracle_project.argtypes = [vp, C.c_int]
+        L.ps3d_oracle_diag_balance.argtypes = [vp, C.c_int, C.c_int]
         L.ps3d_oracle_forward_transform.argtypes = [vp]
         L.ps3d_oracle_opt_balance.argtypes = [vp, C.POINTER(OptBal), dp, ip]
         L.ps3d_oracle_diagnose.restype = C.c_int
@@ -145,6 +148,11 @@ class Oracle:
 
     def project(self, mode):
         self.L.ps3d_oracle_project(self.h, mode)
+
+    def diag_balance(self, order, filter_width=-1):
+        """Warn-et-al. balance to `order` (diag_balance.f90:89-362); components
+        in fields u0..b0, u1..b1, u2..b2, u3..b3."""
+        self.L.ps3d_oracle_diag_balance(self.h, order, filter_width)
 
     def forward_transform(self):
         """forward_transform of the state; read the result with spectral(1..4)."""

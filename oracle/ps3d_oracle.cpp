@@ -171,6 +171,12 @@ struct Model {
     std::vector<double> u_bal, v_bal, w_bal, b_bal, u_base, v_base, w_base, b_base;
     std::vector<double> u0, v0, w0, b0;
     std::vector<double> u_save, v_save, w_save, b_save, u_ave, v_ave, w_ave, b_ave;
+    /* Warn-et-al. balance (module_diag_balance, diag_balance.f90:3-24) */
+    std::vector<double> u1, v1, w1, b1, u2, v2, w2, b2, u3, v3, w3, b3, pTu0, pTv0, pTw0, pTb0;
+    std::vector<cx> f1p, f1m, I_00, I_0p, I_0m, I_f1p, I_f1m, I_0f1p, I_0f1m, I_pT0p, I_pT0m;
+    std::vector<cx> f2p, f2m, I_f2p, I_f2m, I_0f2p, I_0f2m, pTf2p, pTf2m;
+    bool balance_filter = false;   /* enable_diag_balance_filter (main_module.f90:22) */
+    int balance_filter_width = 3;  /* diag_balance_filter_width  (main_module.f90:23) */
     /* forcing */
     int force_kind = 0;
     double omega = 0.0;
@@ -1024,6 +1030,278 @@ static void project(Model& M, int mode) {
     }
 }
 
+/* ---- diag_balance.f90:500-535: advective tendencies of a given state,
+ *      divided by Ro (w also by dsqr), forward transformed; optional kz filter */
+static void model_nonlin(Model& M, const double* ui, const double* vi, const double* wi, const double* bi,
+                         cx* US, cx* VS, cx* WS, cx* BS) {
+    const long n3 = M.n3;
+    std::vector<double> u_loc = M.u, v_loc = M.v, w_loc = M.w, b_loc = M.b;
+    std::vector<double> du_loc(n3, 0.0), dv_loc(n3, 0.0), dw_loc(n3, 0.0), db_loc(n3, 0.0);
+    std::copy(ui, ui + n3, M.u.begin());
+    std::copy(vi, vi + n3, M.v.begin());
+    std::copy(wi, wi + n3, M.w.begin());
+    std::copy(bi, bi + n3, M.b.begin());
+    buoyancy_advection_2nd(M, db_loc.data());
+    momentum_advection_2nd(M, du_loc.data(), dv_loc.data(), dw_loc.data());
+    const double Ro = M.P.Ro, dsqr = M.P.dsqr;
+    for (long t = 0; t < n3; ++t) {
+        db_loc[t] = db_loc[t] / Ro;
+        du_loc[t] = du_loc[t] / Ro;
+        dv_loc[t] = dv_loc[t] / Ro;
+        dw_loc[t] = dw_loc[t] / Ro / dsqr;
+    }
+    M.u = u_loc; M.v = v_loc; M.w = w_loc; M.b = b_loc;
+    forward_transform(M, du_loc.data(), dv_loc.data(), dw_loc.data(), db_loc.data(), US, VS, WS, BS);
+    if (M.balance_filter) {
+        const double fxa = std::fabs(M.kz[M.nz / 2 + M.balance_filter_width]);   /* kz(nz/2+1+width) */
+        for (int k = 1; k <= M.nz; ++k) {
+            if (M.kz[k - 1] * M.kz[k - 1] < fxa * fxa) continue;
+            for (int j = 1; j <= M.ny; ++j)
+                for (int i = 1; i <= M.nxh; ++i) {
+                    const long q = M.S(i, j, k);
+                    US[q] = C(0, 0); VS[q] = C(0, 0); WS[q] = C(0, 0); BS[q] = C(0, 0);
+                }
+        }
+    }
+}
+
+/* ---- diag_balance.f90:465-497: max_steps of integrate from a given state
+ *      (itt stays 0, so every step is a forward step), state saved/restored */
+static void model_run(Model& M, const double* ui, const double* vi, const double* wi, const double* bi,
+                      double* uo, double* vo, double* wo, double* bo, int max_steps) {
+    const long n3 = M.n3;
+    std::vector<double> u_loc = M.u, v_loc = M.v, w_loc = M.w, b_loc = M.b, p_loc = M.p;
+    std::vector<double> du_loc[3], dv_loc[3], dw_loc[3], db_loc[3];
+    for (int s = 0; s < 3; ++s) { du_loc[s] = M.du[s]; dv_loc[s] = M.dv[s]; dw_loc[s] = M.dw[s]; db_loc[s] = M.db[s]; }
+    const int tau_loc = M.tau, taum1_loc = M.taum1, taum2_loc = M.taum2, itt_loc = M.itt;
+    std::copy(ui, ui + n3, M.u.begin());
+    std::copy(vi, vi + n3, M.v.begin());
+    std::copy(wi, wi + n3, M.w.begin());
+    std::copy(bi, bi + n3, M.b.begin());
+    M.itt = 0; M.taum2 = 1; M.taum1 = 2; M.tau = 3;
+    for (int n = 1; n <= max_steps; ++n) {
+        integrate(M);
+        rotate(M);
+    }
+    std::copy(M.u.begin(), M.u.end(), uo);
+    std::copy(M.v.begin(), M.v.end(), vo);
+    std::copy(M.w.begin(), M.w.end(), wo);
+    std::copy(M.b.begin(), M.b.end(), bo);
+    M.u = u_loc; M.v = v_loc; M.w = w_loc; M.b = b_loc; M.p = p_loc;
+    for (int s = 0; s < 3; ++s) { M.du[s] = du_loc[s]; M.dv[s] = dv_loc[s]; M.dw[s] = dw_loc[s]; M.db[s] = db_loc[s]; }
+    M.tau = tau_loc; M.taum1 = taum1_loc; M.taum2 = taum2_loc; M.itt = itt_loc;
+}
+
+/* elementwise a + s*b (s*b alone when a is null) over full halo arrays */
+static std::vector<double> comb(const std::vector<double>* a, const std::vector<double>& b, double s, bool divide) {
+    std::vector<double> out(b.size());
+    for (size_t t = 0; t < b.size(); ++t) {
+        const double y = divide ? b[t] / s : b[t] * s;
+        out[t] = a ? (*a)[t] + y : y;
+    }
+    return out;
+}
+
+static void warn_alloc(Model& M) {
+    const long n = M.nspec();
+    for (auto* a : {&M.US, &M.VS, &M.WS, &M.BS, &M.f1p, &M.f1m, &M.I_00, &M.I_0p, &M.I_0m, &M.I_f1p, &M.I_f1m,
+                    &M.I_0f1p, &M.I_0f1m, &M.I_pT0p, &M.I_pT0m, &M.f2p, &M.f2m, &M.I_f2p, &M.I_f2m, &M.I_0f2p,
+                    &M.I_0f2m, &M.pTf2p, &M.pTf2m})
+        if ((long)a->size() != n) a->assign(n, C(0, 0));
+    for (auto* a : {&M.u0, &M.v0, &M.w0, &M.b0, &M.u1, &M.v1, &M.w1, &M.b1, &M.u2, &M.v2, &M.w2, &M.b2, &M.u3, &M.v3,
+                    &M.w3, &M.b3, &M.pTu0, &M.pTv0, &M.pTw0, &M.pTb0})
+        if ((long)a->size() != M.n3) a->assign(M.n3, 0.0);
+}
+
+#define WARN_LOOP(...)                                                                                    \
+    for (int k = 1; k <= M.nz; ++k)                                                                       \
+        for (int j = 1; j <= M.ny; ++j)                                                                   \
+            for (int i = 1; i <= M.nxh; ++i) {                                                            \
+                const long q = M.S(i, j, k);                                                              \
+                const double kxx = M.kx[i - 1], kyy = M.ky[j - 1], kzz = M.kz[k - 1];                     \
+                __VA_ARGS__                                                                               \
+            }
+static inline cx dotp(cx a, cx b, cx c, cx d, cx U, cx V, cx W, cx B) { return a * U + b * V + c * W + d * B; }
+
+/* ---- diag_balance.f90:135-176 -------------------------------------------- */
+static void diag_balance_first_order(Model& M) {
+    model_nonlin(M, M.u0.data(), M.v0.data(), M.w0.data(), M.b0.data(), M.US.data(), M.VS.data(), M.WS.data(),
+                 M.BS.data());
+    const double Ro = M.P.Ro;
+    #pragma omp parallel for collapse(2)
+    WARN_LOOP({
+        cx px0, py0, pz0, pb0, pxp, pyp, pzp, pbp, pxm, pym, pzm, pbm, qxp, qyp, qzp, qbp, qxm, qym, qzm, qbm;
+        vec_p(M, kxx, kyy, kzz, 0.0, px0, py0, pz0, pb0);
+        vec_p(M, kxx, kyy, kzz, +1.0, pxp, pyp, pzp, pbp);
+        vec_p(M, kxx, kyy, kzz, -1.0, pxm, pym, pzm, pbm);
+        vec_q(M, kxx, kyy, kzz, +1.0, qxp, qyp, qzp, qbp);
+        vec_q(M, kxx, kyy, kzz, -1.0, qxm, qym, qzm, qbm);
+        const double om = std::sqrt(omega2(M, kxx, kyy, kzz));
+        M.I_00[q] = IM * dotp(px0, py0, pz0, pb0, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        M.I_0p[q] = IM * dotp(pxp, pyp, pzp, pbp, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        M.I_0m[q] = IM * dotp(pxm, pym, pzm, pbm, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        if (om > 0.) { M.f1p[q] = M.I_0p[q] / om; M.f1m[q] = -(M.I_0m[q] / om); }
+        else { M.f1p[q] = C(0, 0); M.f1m[q] = C(0, 0); }
+        M.US[q] = Ro * (M.f1p[q] * qxp + M.f1m[q] * qxm);
+        M.VS[q] = Ro * (M.f1p[q] * qyp + M.f1m[q] * qym);
+        M.WS[q] = Ro * (M.f1p[q] * qzp + M.f1m[q] * qzm);
+        M.BS[q] = Ro * (M.f1p[q] * qbp + M.f1m[q] * qbm);
+    })
+    backward_transform(M, M.US.data(), M.VS.data(), M.WS.data(), M.BS.data(), M.u1.data(), M.v1.data(), M.w1.data(),
+                       M.b1.data());
+}
+
+/* I = im * p(s).S for s = +1 and -1 into (Ip, Im) */
+static void warn_pm(Model& M, std::vector<cx>& Ip, std::vector<cx>& Im) {
+    #pragma omp parallel for collapse(2)
+    WARN_LOOP({
+        cx pxp, pyp, pzp, pbp, pxm, pym, pzm, pbm;
+        vec_p(M, kxx, kyy, kzz, +1.0, pxp, pyp, pzp, pbp);
+        vec_p(M, kxx, kyy, kzz, -1.0, pxm, pym, pzm, pbm);
+        Ip[q] = IM * dotp(pxp, pyp, pzp, pbp, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        Im[q] = IM * dotp(pxm, pym, pzm, pbm, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+    })
+}
+
+/* ---- diag_balance.f90:180-272 -------------------------------------------- */
+static void diag_balance_second_order(Model& M) {
+    const double Ro = M.P.Ro;
+    {
+        auto a = comb(nullptr, M.u1, Ro, true), b = comb(nullptr, M.v1, Ro, true);
+        auto c = comb(nullptr, M.w1, Ro, true), d = comb(nullptr, M.b1, Ro, true);
+        model_nonlin(M, a.data(), b.data(), c.data(), d.data(), M.US.data(), M.VS.data(), M.WS.data(), M.BS.data());
+    }
+    warn_pm(M, M.I_f1p, M.I_f1m);
+    {
+        auto a = comb(&M.u0, M.u1, Ro, true), b = comb(&M.v0, M.v1, Ro, true);
+        auto c = comb(&M.w0, M.w1, Ro, true), d = comb(&M.b0, M.b1, Ro, true);
+        model_nonlin(M, a.data(), b.data(), c.data(), d.data(), M.US.data(), M.VS.data(), M.WS.data(), M.BS.data());
+    }
+    #pragma omp parallel for collapse(2)
+    WARN_LOOP({
+        cx pxp, pyp, pzp, pbp, pxm, pym, pzm, pbm, qx0, qy0, qz0, qb0;
+        vec_p(M, kxx, kyy, kzz, +1.0, pxp, pyp, pzp, pbp);
+        vec_p(M, kxx, kyy, kzz, -1.0, pxm, pym, pzm, pbm);
+        vec_q(M, kxx, kyy, kzz, 0.0, qx0, qy0, qz0, qb0);
+        M.I_0f1p[q] = IM * dotp(pxp, pyp, pzp, pbp, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        M.I_0f1m[q] = IM * dotp(pxm, pym, pzm, pbm, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        const cx pTg0 = -(IM * M.I_00[q]);
+        M.US[q] = pTg0 * qx0; M.VS[q] = pTg0 * qy0; M.WS[q] = pTg0 * qz0; M.BS[q] = pTg0 * qb0;
+    })
+    backward_transform(M, M.US.data(), M.VS.data(), M.WS.data(), M.BS.data(), M.pTu0.data(), M.pTv0.data(),
+                       M.pTw0.data(), M.pTb0.data());
+    model_nonlin(M, M.pTu0.data(), M.pTv0.data(), M.pTw0.data(), M.pTb0.data(), M.US.data(), M.VS.data(),
+                 M.WS.data(), M.BS.data());
+    warn_pm(M, M.I_pT0p, M.I_pT0m);
+    {
+        auto a = comb(&M.u0, M.pTu0, 1.0, false), b = comb(&M.v0, M.pTv0, 1.0, false);
+        auto c = comb(&M.w0, M.pTw0, 1.0, false), d = comb(&M.b0, M.pTb0, 1.0, false);
+        model_nonlin(M, a.data(), b.data(), c.data(), d.data(), M.US.data(), M.VS.data(), M.WS.data(), M.BS.data());
+    }
+    const double Ro2 = Ro * Ro;
+    #pragma omp parallel for collapse(2)
+    WARN_LOOP({
+        cx pxp, pyp, pzp, pbp, pxm, pym, pzm, pbm, qxp, qyp, qzp, qbp, qxm, qym, qzm, qbm;
+        vec_p(M, kxx, kyy, kzz, +1.0, pxp, pyp, pzp, pbp);
+        vec_p(M, kxx, kyy, kzz, -1.0, pxm, pym, pzm, pbm);
+        vec_q(M, kxx, kyy, kzz, +1.0, qxp, qyp, qzp, qbp);
+        vec_q(M, kxx, kyy, kzz, -1.0, qxm, qym, qzm, qbm);
+        const double om = std::sqrt(omega2(M, kxx, kyy, kzz));
+        const cx I_0pT0p = IM * dotp(pxp, pyp, pzp, pbp, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        const cx I_0pT0m = IM * dotp(pxm, pym, pzm, pbm, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        if (om > 0) {
+            const cx pTf1p = (I_0pT0p - M.I_0p[q] - M.I_pT0p[q]) / om;
+            const cx pTf1m = -((I_0pT0m - M.I_0m[q] - M.I_pT0m[q]) / om);
+            M.f2p[q] = (M.I_0f1p[q] - M.I_0p[q] - M.I_f1p[q] - IM * pTf1p) / om;
+            M.f2m[q] = -((M.I_0f1m[q] - M.I_0m[q] - M.I_f1m[q] - IM * pTf1m) / om);
+        } else {
+            M.f2p[q] = C(0, 0); M.f2m[q] = C(0, 0);
+        }
+        M.US[q] = Ro2 * (M.f2p[q] * qxp + M.f2m[q] * qxm);
+        M.VS[q] = Ro2 * (M.f2p[q] * qyp + M.f2m[q] * qym);
+        M.WS[q] = Ro2 * (M.f2p[q] * qzp + M.f2m[q] * qzm);
+        M.BS[q] = Ro2 * (M.f2p[q] * qbp + M.f2m[q] * qbm);
+    })
+    backward_transform(M, M.US.data(), M.VS.data(), M.WS.data(), M.BS.data(), M.u2.data(), M.v2.data(), M.w2.data(),
+                       M.b2.data());
+}
+
+/* ---- diag_balance.f90:275-362 -------------------------------------------- */
+static void diag_balance_third_order(Model& M) {
+    const double Ro = M.P.Ro, Ro2 = Ro * Ro, Ro3 = Ro * Ro * Ro;
+    {
+        auto a = comb(nullptr, M.u2, Ro2, true), b = comb(nullptr, M.v2, Ro2, true);
+        auto c = comb(nullptr, M.w2, Ro2, true), d = comb(nullptr, M.b2, Ro2, true);
+        model_nonlin(M, a.data(), b.data(), c.data(), d.data(), M.US.data(), M.VS.data(), M.WS.data(), M.BS.data());
+    }
+    warn_pm(M, M.I_f2p, M.I_f2m);
+    {
+        auto a = comb(&M.u0, M.u2, Ro2, true), b = comb(&M.v0, M.v2, Ro2, true);
+        auto c = comb(&M.w0, M.w2, Ro2, true), d = comb(&M.b0, M.b2, Ro2, true);
+        model_nonlin(M, a.data(), b.data(), c.data(), d.data(), M.US.data(), M.VS.data(), M.WS.data(), M.BS.data());
+    }
+    warn_pm(M, M.I_0f2p, M.I_0f2m);
+    {
+        auto a = comb(&M.u0, M.u1, 1.0, false), b = comb(&M.v0, M.v1, 1.0, false);
+        auto c = comb(&M.w0, M.w1, 1.0, false), d = comb(&M.b0, M.b1, 1.0, false);
+        a = comb(&a, M.u2, 1.0, false); b = comb(&b, M.v2, 1.0, false);
+        c = comb(&c, M.w2, 1.0, false); d = comb(&d, M.b2, 1.0, false);
+        model_run(M, a.data(), b.data(), c.data(), d.data(), M.u3.data(), M.v3.data(), M.w3.data(), M.b3.data(), 10);
+    }
+    forward_transform(M, M.u3.data(), M.v3.data(), M.w3.data(), M.b3.data(), M.US.data(), M.VS.data(), M.WS.data(),
+                      M.BS.data());
+    #pragma omp parallel for collapse(2)
+    WARN_LOOP({
+        cx qx0, qy0, qz0, qb0, px0, py0, pz0, pb0;
+        vec_q(M, kxx, kyy, kzz, 0.0, qx0, qy0, qz0, qb0);
+        vec_p(M, kxx, kyy, kzz, 0.0, px0, py0, pz0, pb0);
+        const cx g0 = dotp(px0, py0, pz0, pb0, M.US[q], M.VS[q], M.WS[q], M.BS[q]);
+        M.US[q] = g0 * qx0; M.VS[q] = g0 * qy0; M.WS[q] = g0 * qz0; M.BS[q] = g0 * qb0;
+    })
+    backward_transform(M, M.US.data(), M.VS.data(), M.WS.data(), M.BS.data(), M.u0.data(), M.v0.data(), M.w0.data(),
+                       M.b0.data());
+    M.pTf2p = M.f2p; M.pTf2m = M.f2m;
+    diag_balance_first_order(M);
+    diag_balance_second_order(M);
+    const long n = M.nspec();
+    for (long q = 0; q < n; ++q) {
+        M.pTf2p[q] = (M.f2p[q] - M.pTf2p[q]) / (10. * M.P.dt) / Ro;
+        M.pTf2m[q] = (M.f2m[q] - M.pTf2m[q]) / (10. * M.P.dt) / Ro;
+    }
+    project(M, 3);   /* diag_balance_zero_order */
+    diag_balance_first_order(M);
+    diag_balance_second_order(M);
+    #pragma omp parallel for collapse(2)
+    WARN_LOOP({
+        cx qxp, qyp, qzp, qbp, qxm, qym, qzm, qbm;
+        vec_q(M, kxx, kyy, kzz, +1.0, qxp, qyp, qzp, qbp);
+        vec_q(M, kxx, kyy, kzz, -1.0, qxm, qym, qzm, qbm);
+        const double om = std::sqrt(omega2(M, kxx, kyy, kzz));
+        cx f3p, f3m;
+        if (om > 0) {
+            f3p = (M.I_0f2p[q] + M.I_f1p[q] - M.I_f2p[q] - M.I_0p[q] - IM * M.pTf2p[q]) / om;
+            f3m = -((M.I_0f2m[q] + M.I_f1m[q] - M.I_f2m[q] - M.I_0m[q] - IM * M.pTf2m[q]) / om);
+        } else {
+            f3p = C(0, 0); f3m = C(0, 0);
+        }
+        M.US[q] = Ro3 * (f3p * qxp + f3m * qxm);
+        M.VS[q] = Ro3 * (f3p * qyp + f3m * qym);
+        M.WS[q] = Ro3 * (f3p * qzp + f3m * qzm);
+        M.BS[q] = Ro3 * (f3p * qbp + f3m * qbm);
+    })
+    backward_transform(M, M.US.data(), M.VS.data(), M.WS.data(), M.BS.data(), M.u3.data(), M.v3.data(), M.w3.data(),
+                       M.b3.data());
+}
+
+/* diag_balance (diag_balance.f90:89-106) up to `order`, without the output */
+static void diag_balance(Model& M, int order) {
+    warn_alloc(M);
+    project(M, 3);
+    if (order >= 1) diag_balance_first_order(M);
+    if (order >= 2) diag_balance_second_order(M);
+    if (order >= 3) diag_balance_third_order(M);
+}
+
 /* ---- diag_opt_balance.f90:367-378 ---------------------------------------- */
 static double ramp(double theta) {
     double t1 = 1. / std::max(1e-32, theta);
@@ -1179,6 +1457,9 @@ static std::vector<double>* field_ptr(Model& M, int id) {
         case 20: return &M.u_bal; case 21: return &M.v_bal; case 22: return &M.w_bal; case 23: return &M.b_bal;
         case 24: return &M.u_base; case 25: return &M.v_base; case 26: return &M.w_base; case 27: return &M.b_base;
         case 28: return &M.u0; case 29: return &M.v0; case 30: return &M.w0; case 31: return &M.b0;
+        case 32: return &M.u1; case 33: return &M.v1; case 34: return &M.w1; case 35: return &M.b1;
+        case 36: return &M.u2; case 37: return &M.v2; case 38: return &M.w2; case 39: return &M.b2;
+        case 40: return &M.u3; case 41: return &M.v3; case 42: return &M.w3; case 43: return &M.b3;
         default: return nullptr;
     }
 }
@@ -1254,6 +1535,14 @@ void ps3d_oracle_integrate(void* h, int nsteps) {
 }
 void ps3d_oracle_pressure_solver(void* h) { pressure_solver(*static_cast<Model*>(h)); }
 void ps3d_oracle_project(void* h, int mode) { project(*static_cast<Model*>(h), mode); }
+/* diag_balance_zero_order .. third_order up to `order`; filter_width < 0:
+ * no enable_diag_balance_filter.  Results in field ids 28-43 (u0..b3). */
+void ps3d_oracle_diag_balance(void* h, int order, int filter_width) {
+    Model& M = *static_cast<Model*>(h);
+    M.balance_filter = filter_width >= 0;
+    if (filter_width >= 0) M.balance_filter_width = filter_width;
+    diag_balance(M, order);
+}
 /* forward_transform of the current state into US..BS (diag_balance.f90:421-438) */
 void ps3d_oracle_forward_transform(void* h) {
     Model& M = *static_cast<Model*>(h);

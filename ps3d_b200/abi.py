@@ -32,6 +32,9 @@ PS3D_FIELDS_STATE = 0
 PS3D_FIELDS_BALANCED = 1
 PS3D_FIELDS_BASE = 2
 PS3D_FIELDS_ZERO = 3
+PS3D_FIELDS_FIRST = 4
+PS3D_FIELDS_SECOND = 5
+PS3D_FIELDS_THIRD = 6
 
 
 class Params(C.Structure):

@@ -57,7 +57,7 @@ struct DevPlan {
 
 bool fft_length_ok(int n);
 
-enum { kSetSave = 10, kSetAve = 11, kSetSave2 = 12 };
+enum { kSetSave = 10, kSetAve = 11, kSetSave2 = 12, kSetPT0 = 13, kSetComb = 14 };
 
 struct Ctx {
     ps3d_params P{};
@@ -95,6 +95,11 @@ struct Ctx {
     // projections
     DevBuf spec4[4], g0base, qtmp;
     DevBuf bal[4], base[4], zero[4], save[4], ave[4], save2[4];
+    // Warn-et-al. balance: components u1..b3, pTu0..pTb0, combinations,
+    // advective tendencies and the spectral work arrays (warn.cu)
+    DevBuf first[4], second[4], third[4], pt0[4], comb[4], nl_tend[4];
+    DevBuf warn_arr[19];
+    int warn_filter = -1;
     DevBuf saved_p, saved_tend[4];
     // tables
     DevPlan plx, ply, plz;      // radix-16/8 schedules
@@ -170,6 +175,22 @@ struct Ctx {
     int forward_transform(const double* const* in);
     int backward_transform(double* const* out);
     int project(int mode);
+    int project_spectral(int mode);
+    // restart.f90 record layout (restart.cu)
+    int write_restart(const char* path);
+    int read_restart(const char* path, double* time_out);
+    // Warn-et-al. balance (warn.cu)
+    int diag_balance(int order, int filter_width);
+    cudaError_t ensure_warn();
+    int warn_launch(int mode, double2* o1 = nullptr, double2* o2 = nullptr, double kzcut2 = 0.0);
+    int model_nonlin(const double* const* in);
+    int model_nonlin_set(int set);
+    int warn_comb(int set_a, int set_b, double s, bool divide);
+    int backward_to_set(int set);
+    int model_run(int in, int out, int max_steps);
+    int warn_first();
+    int warn_second();
+    int warn_third();
     int diagnose(double* ke, double* pe, double* umax, double* wmax);
     int opt_time_ave(int set, int n_end_ave);
     int opt_balance(const ps3d_optbal& O, double* final_norm, int* iters);

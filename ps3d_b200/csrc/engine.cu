@@ -393,6 +393,11 @@ DevBuf* Ctx::fieldset(int which) {
         case PS3D_FIELDS_BALANCED: return bal;
         case PS3D_FIELDS_BASE: return base;
         case PS3D_FIELDS_ZERO: return zero;
+        case PS3D_FIELDS_FIRST: return first;
+        case PS3D_FIELDS_SECOND: return second;
+        case PS3D_FIELDS_THIRD: return third;
+        case kSetPT0: return pt0;
+        case kSetComb: return comb;
         case kSetSave: return save;
         case kSetAve: return ave;
         case kSetSave2: return save2;
@@ -892,6 +897,22 @@ int Ctx::project(int mode) {
     const double* in[4] = {field(0), field(1), field(2), field(3)};
     int rc = forward_transform(in);
     if (rc) return rc;
+    rc = project_spectral(mode);
+    if (rc) return rc;
+    double* out[4];
+    if (mode == PS3D_PROJ_NORMAL_MODE || mode == PS3D_PROJ_EXCHANGE) {
+        for (int f = 0; f < 4; ++f) out[f] = field(f);
+    } else {
+        const int set = mode == PS3D_PROJ_BASE_POINT ? PS3D_FIELDS_BASE : PS3D_FIELDS_ZERO;
+        CK(ensure_fieldset(set));
+        DevBuf* s = fieldset(set);
+        for (int f = 0; f < 4; ++f) out[f] = (double*)s[f].p;
+    }
+    return backward_transform(out);
+}
+
+// the pointwise projection of one kind on the spectral fields spec4
+int Ctx::project_spectral(int mode) {
     ProjArgs a{};
     a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid; a.layout = pa64.impl;
     a.dx = P.dx; a.dy = P.dy; a.dz = P.dz; a.f0 = P.f0; a.N0 = P.N0; a.dsqr = P.dsqr;
@@ -904,16 +925,7 @@ int Ctx::project(int mode) {
     a.g0base = (double2*)g0base.p;
     a.mode = mode;
     LAUNCH(PS3D_K_OTHER, launch_project(a, stream));
-    double* out[4];
-    if (mode == PS3D_PROJ_NORMAL_MODE || mode == PS3D_PROJ_EXCHANGE) {
-        for (int f = 0; f < 4; ++f) out[f] = field(f);
-    } else {
-        const int set = mode == PS3D_PROJ_BASE_POINT ? PS3D_FIELDS_BASE : PS3D_FIELDS_ZERO;
-        CK(ensure_fieldset(set));
-        DevBuf* s = fieldset(set);
-        for (int f = 0; f < 4; ++f) out[f] = (double*)s[f].p;
-    }
-    return backward_transform(out);
+    return PS3D_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1344,6 +1356,27 @@ int ps3d_get_fields(ps3d_ctx* ctx, int which, double* u, double* v, double* w, d
         if (rc) return rc;
     }
     return PS3D_OK;
+    GUARD_END
+}
+
+int ps3d_write_restart(ps3d_ctx* ctx, const char* path) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.write_restart(path);
+    GUARD_END
+}
+
+int ps3d_read_restart(ps3d_ctx* ctx, const char* path, double* time) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.read_restart(path, time);
+    GUARD_END
+}
+
+int ps3d_diag_balance(ps3d_ctx* ctx, int order, int filter_width) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.diag_balance(order, filter_width);
     GUARD_END
 }
 

@@ -58,6 +58,9 @@ def load():
     L.ps3d_project_geostrophic.argtypes = [vp, C.c_int]
     L.ps3d_opt_balance.argtypes = [vp, C.POINTER(OptBal), dp, ip]
     L.ps3d_get_fields.argtypes = [vp, C.c_int, dp, dp, dp, dp]
+    L.ps3d_diag_balance.argtypes = [vp, C.c_int, C.c_int]
+    L.ps3d_write_restart.argtypes = [vp, C.c_char_p]
+    L.ps3d_read_restart.argtypes = [vp, C.c_char_p, dp]
     L.ps3d_diagnose.argtypes = [vp, dp, dp, dp, dp]
     L.ps3d_set_forcing.argtypes = [vp, C.POINTER(Forcing)]
     L.ps3d_get_stream.argtypes = [vp, C.POINTER(C.c_void_p)]
@@ -174,6 +177,25 @@ class Model:
     def diag_balance_zero_order(self):
         self.project(abi.PS3D_PROJ_ZERO_ORDER)
         return self.get_fields(abi.PS3D_FIELDS_ZERO)
+
+    def write_restart(self, path):
+        """write_restart (restart.f90:2-22): the reference's one-rank restart file."""
+        _check(self.L.ps3d_write_restart(self.h, os.fsencode(path)), "ps3d_write_restart")
+
+    def read_restart(self, path):
+        """read_restart (restart.f90:27-82); returns the file's time."""
+        t = C.c_double()
+        _check(self.L.ps3d_read_restart(self.h, os.fsencode(path), C.byref(t)), "ps3d_read_restart")
+        return t.value
+
+    def diag_balance(self, order=3, filter_width=-1):
+        """Warn-et-al. balance to `order` (diag_balance.f90:89-362): returns
+        [components of order 0, 1, ...], each {"u","v","w","b"} in halo
+        layout; the balanced state is their sum.  filter_width >= 0 turns on
+        enable_diag_balance_filter with that width."""
+        _check(self.L.ps3d_diag_balance(self.h, order, filter_width), "ps3d_diag_balance")
+        sets = (abi.PS3D_FIELDS_ZERO, abi.PS3D_FIELDS_FIRST, abi.PS3D_FIELDS_SECOND, abi.PS3D_FIELDS_THIRD)
+        return [self.get_fields(sets[n]) for n in range(order + 1)]
 
     def diag_opt_balance(self, opt: OptBal):
         norm, iters = C.c_double(), C.c_int()

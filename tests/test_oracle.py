@@ -209,3 +209,27 @@ def test_ramp_function():
     xs = np.linspace(0.01, 0.99, 50)
     r = [ob.ramp(x) for x in xs]
     assert all(np.diff(r) > 0)
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+def test_warn_balance_orders_scale_with_rossby_number(rigid):
+    """u_n of the Warn-et-al. balance is O(Ro^n) with u0 fixed: doubling Ro
+    doubles u1 and quadruples u2 (diag_balance.f90:168-171, 262-265), and the
+    components shrink order by order for a weakly nonlinear eddy."""
+    from ps3d_b200 import configs as cf
+    res = {}
+    for ro in (1.0, 2.0):
+        p = cf.eddy_params(32, 32, 16, rigid=rigid)
+        p.Ro = ro
+        f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=0)
+        o = Oracle(p)
+        for n in "uvwb":
+            o.field(n)[...] = f[n]
+        o.diag_balance(2)
+        res[ro] = {k: o.field(k).copy() for k in ("u0", "u1", "u2", "b1", "b2")}
+    assert np.array_equal(res[1.0]["u0"], res[2.0]["u0"])
+    for k, s in (("u1", 2.0), ("b1", 2.0), ("u2", 4.0), ("b2", 4.0)):
+        a, b = res[1.0][k], res[2.0][k]
+        assert np.linalg.norm(b - s * a) <= 1e-12 * np.linalg.norm(b), k
+    n0, n1, n2 = (np.abs(res[1.0][k]).max() for k in ("u0", "u1", "u2"))
+    assert n0 > n1 > n2 > 0
