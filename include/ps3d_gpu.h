@@ -202,6 +202,16 @@ PS3D_API int ps3d_diag_balance(ps3d_ctx* ctx, int order, int filter_width);
 PS3D_API int ps3d_write_restart(ps3d_ctx* ctx, const char* path);
 PS3D_API int ps3d_read_restart(ps3d_ctx* ctx, const char* path, double* time);
 
+/* Asynchronous snapshot, no counterpart in the reference (whose snapshots,
+ * main.f90:144-152, write netCDF synchronously): the state and p as they
+ * are at the call are copied on the device, then converted to the halo
+ * layout and copied into the host arrays on a second stream while the next
+ * steps run.  Any array may be NULL.  The host arrays (page-locked for the
+ * copies to overlap) must stay valid until ps3d_snapshot_wait returns; a
+ * new ps3d_snapshot_begin first waits for the previous one.                */
+PS3D_API int ps3d_snapshot_begin(ps3d_ctx* ctx, double* u, double* v, double* w, double* b, double* p);
+PS3D_API int ps3d_snapshot_wait(ps3d_ctx* ctx);
+
 /* Auxiliary field sets in halo layout (u,v,w,b; any may be NULL).          */
 #define PS3D_FIELDS_STATE    0   /* u, v, w, b                         */
 #define PS3D_FIELDS_BALANCED 1   /* u_bal..b_bal  (diag_opt_balance)   */

@@ -99,6 +99,10 @@ struct Ctx {
     // advective tendencies and the spectral work arrays (warn.cu)
     DevBuf first[4], second[4], third[4], pt0[4], comb[4], nl_tend[4];
     DevBuf warn_arr[19];
+    // asynchronous snapshots (restart.cu)
+    DevBuf snap[5], snap_staging;
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_event = nullptr;
     int warn_filter = -1;
     DevBuf saved_p, saved_tend[4];
     // tables
@@ -143,11 +147,18 @@ struct Ctx {
     // reductions / staging
     int nred = 0;
     DevBuf red_partials, red_out, staging;
+    // kernel error word in mapped page-locked memory: kernels whose bounded
+    // waits ran out store 1; read after every stream synchronisation
+    unsigned* kerr_h = nullptr;
+    unsigned* kerr_d = nullptr;
 
     ~Ctx() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (stream) { cudaStreamSynchronize(stream); if (own_stream) cudaStreamDestroy(stream); }
         for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
+        if (snap_stream) { cudaStreamSynchronize(snap_stream); cudaStreamDestroy(snap_stream); }
+        if (snap_event) cudaEventDestroy(snap_event);
+        if (kerr_h) cudaFreeHost(kerr_h);
     }
 
     double* field(int f) { return (double*)state[f][cur[f]].p; }
@@ -159,6 +170,10 @@ struct Ctx {
     int sync() {
         CK(cudaStreamSynchronize(stream));
         CK(cudaGetLastError());
+        if (kerr_h && *(volatile unsigned*)kerr_h) {
+            *(volatile unsigned*)kerr_h = 0;
+            return PS3D_ERR_TIMEOUT;
+        }
         return PS3D_OK;
     }
 
@@ -179,6 +194,8 @@ struct Ctx {
     // restart.f90 record layout (restart.cu)
     int write_restart(const char* path);
     int read_restart(const char* path, double* time_out);
+    int snapshot_begin(double* const* host);
+    int snapshot_wait();
     // Warn-et-al. balance (warn.cu)
     int diag_balance(int order, int filter_width);
     cudaError_t ensure_warn();

@@ -152,7 +152,7 @@ cudaError_t DevPlan::build(int len, int policy) {
     return cudaSuccess;
 }
 
-constexpr size_t kMaxSmem = 227 * 1024;   // dynamic shared memory a block may opt in to
+constexpr size_t kMaxSmem = 226 * 1024;   // dynamic shared memory a block may opt in to, less static headroom
 
 // Feasible shapes of the plane kernels for one element size.
 static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const PlaneArgs& base) {
@@ -174,15 +174,17 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
             out.push_back(a);
         }
     }
-    // rows pass + y-lines pass
-    for (int tj : {8, 16, 32}) {
-        if (ny % tj) continue;
-        for (int ly : {8, 16, 32}) {
-            PlaneArgs a = base;
-            a.impl = 1; a.tj = tj; a.ly = ly;
-            a.C = 1; a.rows_per_cta = ny; a.cols_per_cta = nxh; a.row_chunk = 8; a.ldr = 9; a.ldc = nxh | 1;
-            if (plane_smem(a, es == sizeof(float2)) > kMaxSmem) continue;
-            out.push_back(a);
+    // rows pass + y-lines pass, and its pipelined-rows variant
+    for (int im : {1, 2}) {
+        for (int tj : {4, 8, 16, 32}) {
+            if (ny % tj || (im == 1 && tj == 4) || (im == 2 && tj > 16)) continue;
+            for (int ly : {8, 16, 32}) {
+                PlaneArgs a = base;
+                a.impl = im; a.tj = tj; a.ly = ly;
+                a.C = 1; a.rows_per_cta = ny; a.cols_per_cta = nxh; a.row_chunk = 8; a.ldr = 9; a.ldc = nxh | 1;
+                if (plane_smem(a, es == sizeof(float2)) > kMaxSmem) continue;
+                out.push_back(a);
+            }
         }
     }
     return out;
@@ -211,11 +213,12 @@ static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
     return false;
 }
 
-// Default shape of the rows + y-lines plane kernels for one element size.
-static bool choose_split_config(int nx, int ny, size_t es, PlaneArgs& a) {
+// Default shape of the rows + y-lines plane kernels (implementation 1 or 2)
+// for one element size.
+static bool choose_split_config(int nx, int ny, size_t es, PlaneArgs& a, int impl) {
     for (const PlaneArgs& c : plane_candidates(nx, ny, es, a)) {
-        if (c.impl != 1 || c.ly != 16) continue;
-        if (c.tj == 16 || (c.tj == 8 && ny % 16)) {
+        if (c.impl != impl || c.ly != 16) continue;
+        if (c.tj == (impl == 2 ? 8 : 16) || (c.tj == (impl == 2 ? 4 : 8) && ny % (impl == 2 ? 8 : 16))) {
             const FFTPlan px = a.px, py = a.py;
             a = c;
             a.px = px; a.py = py;
@@ -341,11 +344,16 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     // PS3D_PLANE_IMPL=0|1 pins the plane implementation (cluster, or rows +
     // y-lines) for the defaults and the autotuner; grids the rows + y-lines
     // kernels cannot take keep the cluster kernels
-    if (const char* pi = std::getenv("PS3D_PLANE_IMPL")) plane_force = pi[0] == '1' ? 1 : pi[0] == '0' ? 0 : -1;
-    if (plane_force == 1) {
-        choose_split_config(nx, ny, sizeof(double2), pa64);
-        choose_split_config(nx, ny, sizeof(float2), pa32);
+    if (const char* pi = std::getenv("PS3D_PLANE_IMPL"))
+        plane_force = (pi[0] >= '0' && pi[0] <= '2') ? pi[0] - '0' : -1;
+    if (plane_force >= 1) {
+        choose_split_config(nx, ny, sizeof(double2), pa64, plane_force);
+        choose_split_config(nx, ny, sizeof(float2), pa32, plane_force);
     }
+    CK(cudaHostAlloc((void**)&kerr_h, 16, cudaHostAllocMapped));
+    *kerr_h = 0;
+    CK(cudaHostGetDevicePointer((void**)&kerr_d, kerr_h, 0));
+    pa64.err = kerr_d; pa32.err = kerr_d;
     kchunk = nz <= 16 ? nz : 8;
     // reductions
     nred = 148 * 4;
@@ -358,7 +366,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
         // the vertical solve's factors depend only on the grid: built once, in
         // the spectral column order of the plane kernels the tuner picked
         ColumnArgs c{};
-        c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.layout = (mixed ? pa32 : pa64).impl;
+        c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.layout = spectral_layout(mixed ? pa32 : pa64);
         c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p;
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         CK(thomas_r.alloc((size_t)M * sizeof(double)));
@@ -581,7 +589,7 @@ int Ctx::autotune() {
         for (const PlaneArgs& c : plane_candidates(nx, ny, f32 ? sizeof(float2) : sizeof(double2), pa)) {
             if (c.impl != im) continue;
             if (im == 0 && (c.C != C || c.row_chunk != rc)) continue;
-            if (im == 1 && (c.tj != tj || c.ly != ly)) continue;
+            if (im >= 1 && (c.tj != tj || c.ly != ly)) continue;
             pa = c;
             plans_of(pol, pa);
             kchunk = kc;
@@ -790,7 +798,7 @@ int Ctx::poisson_once(double* out, double beta, bool lazy, const double* pc) {
     LAUNCH(PS3D_K_FFT_FWD, launch_plane_fwd(a, f32, stream));
     ColumnArgs c{};
     c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = FS.p;
-    c.batch = batch; c.sM = M; c.layout = a.impl;
+    c.batch = batch; c.sM = M; c.layout = spectral_layout(a);
     c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p; c.hkz = (const double*)t_hkz_ds.p;
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
@@ -858,7 +866,7 @@ int Ctx::forward_transform(const double* const* in) {
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
-            c.batch = 1; c.sM = M; c.layout = pa64.impl;
+            c.batch = 1; c.sM = M; c.layout = spectral_layout(pa64);
             c.pz = plz.plan; c.scale = P.dz; c.op = 1;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -876,7 +884,7 @@ int Ctx::backward_transform(double* const* out) {
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
-            c.batch = 1; c.sM = M; c.layout = pa64.impl;
+            c.batch = 1; c.sM = M; c.layout = spectral_layout(pa64);
             c.pz = plz.plan; c.scale = 1.0; c.op = 2;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -914,7 +922,7 @@ int Ctx::project(int mode) {
 // the pointwise projection of one kind on the spectral fields spec4
 int Ctx::project_spectral(int mode) {
     ProjArgs a{};
-    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid; a.layout = pa64.impl;
+    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid; a.layout = spectral_layout(pa64);
     a.dx = P.dx; a.dy = P.dy; a.dz = P.dz; a.f0 = P.f0; a.N0 = P.N0; a.dsqr = P.dsqr;
     a.ax.kx = (const double*)t_kx.p; a.ax.ky = (const double*)t_ky.p; a.ax.kz = (const double*)t_kz.p;
     a.ax.hkx = (const double*)t_hkx.p; a.ax.hky = (const double*)t_hky.p; a.ax.hkz = (const double*)t_hkz.p;
@@ -1373,6 +1381,21 @@ int ps3d_read_restart(ps3d_ctx* ctx, const char* path, double* time) {
     GUARD_END
 }
 
+int ps3d_snapshot_begin(ps3d_ctx* ctx, double* u, double* v, double* w, double* b, double* p) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    double* h[5] = {u, v, w, b, p};
+    return ctx->impl.snapshot_begin(h);
+    GUARD_END
+}
+
+int ps3d_snapshot_wait(ps3d_ctx* ctx) {
+    GUARD_BEGIN
+    if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
+    return ctx->impl.snapshot_wait();
+    GUARD_END
+}
+
 int ps3d_diag_balance(ps3d_ctx* ctx, int order, int filter_width) {
     GUARD_BEGIN
     if (!ctx_ok(ctx)) return PS3D_ERR_BADPARAM;
@@ -1417,7 +1440,7 @@ int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
     const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
     std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_impl=%s plane_cluster=%d row_chunk=%d tj=%d ly=%d "
                   "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.mixed ? "mixed" : "fp64",
-                  C.batch, pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
+                  C.batch, pa.impl == 2 ? "pipe+lines" : pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
                   C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
     return PS3D_OK;
 }

@@ -61,11 +61,15 @@ struct PlaneArgs {
     const double2* twx;            // exp(-2 pi i t/nx), t = 0..nx/2
     int batch;                     // instances (>= 1): grid.y = nz*batch
     long sN, sM;                   // instance strides: real fields, spectral elements
-    int impl;                      // 0: one cluster per plane (DSMEM), 1: rows pass + y-lines pass
+    int impl;                      // 0: one cluster per plane (DSMEM), 1: rows pass + y-lines pass,
+                                   // 2: as 1 with the forward rows pass pipelined by bulk copies
     int tj;                        // impl 1: rows per CTA of the rows passes
     int ly;                        // impl 1: lines per CTA of the y-lines passes
     FastDiv fd_n2, fd_ny, fd_tj;   // set by the launchers
+    unsigned* err;                 // implementation 2: set to 1 when a bounded wait ran out
 };
+// spectral layout of a plane configuration: 0 [k][ky][kx], 1 [k][kx][ky]
+inline int spectral_layout(const PlaneArgs& a) { return a.impl != 0; }
 
 struct ColumnArgs {
     int nx, ny, nz, nxh;

@@ -22,6 +22,7 @@
 // The real FFTs pack even/odd samples into a half-length complex FFT.
 #include <cooperative_groups.h>
 #include "engine.h"
+#include "async.cuh"
 #include "fft.cuh"
 
 namespace cg = cooperative_groups;
@@ -610,6 +611,132 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rows pass, pipelined (implementation 2, divergence and source modes): a
+// persistent grid walks the (plane, row-block) tiles; the whole input rows
+// of a tile (u, v with the row below, w at k and k-1, or the source field)
+// arrive by bulk copies on the TMA engine into one of two shared-memory
+// stages while the previous tile is transformed, so the HBM stream never
+// waits on the FFT.  The arithmetic is that of k_rows_fwd.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int pipe_rows(const PlaneArgs& a) { return a.mode == 0 ? 4 * a.tj + 1 : a.tj; }
+__host__ __device__ inline size_t pipe_stage_bytes(const PlaneArgs& a) {
+    return (size_t)(4 * a.tj + 1) * a.nx * sizeof(double);
+}
+
+template <typename R, int MAXR>
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_rows_fwd_pipe(const PlaneArgs a, int ntiles) {
+    using T = cpx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = a.nxh, n2 = nx / 2;
+    const int tj = a.tj, ld = tj | 1;
+    const size_t sb = pipe_stage_bytes(a);
+    auto stage = [&](int s) { return reinterpret_cast<double*>(smem_raw + (size_t)s * sb); };
+    T* buf = reinterpret_cast<T*>(smem_raw + 2 * sb);
+    unsigned char* tail = smem_raw + 2 * sb + align16((size_t)n2 * ld * sizeof(T));
+    const PlanTables<R> tx = stage_plan<R>(a.px, tail);
+    const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(n2, sizeof(T)));
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(tail + tables_x_bytes(a, sizeof(T)));
+    __shared__ int abort_flag;
+    const int tpp = ny / tj;                 // tiles per plane
+    const long plane = (long)nx * ny;
+    const int nrows = pipe_rows(a);
+    const unsigned bytes = (unsigned)((size_t)nrows * nx * sizeof(double));
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async();
+    }
+    __syncthreads();
+    auto tile_of = [&](int t, int& inst, int& k, int& jb) {
+        inst = t / (tpp * nz);
+        const int r = t - inst * tpp * nz;
+        k = r / tpp;
+        jb = (r - k * tpp) * tj;
+    };
+    // warp 0 issues every row of tile t into stage s
+    auto issue = [&](int t, int s) {
+        if (threadIdx.x >= 32) return;
+        int inst, k, jb;
+        tile_of(t, inst, k, jb);
+        const long ioff = (long)inst * a.sN;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            mbar_expect(&bars[s], bytes);
+        }
+        __syncwarp();
+        const int km = wrap(k - 1, nz);
+        for (int r = threadIdx.x; r < nrows; r += 32) {
+            const double* row;
+            if (a.mode != 0) row = a.src + ioff + (long)k * plane + (long)(jb + r) * nx;
+            else if (r < tj) row = a.u + ioff + (long)k * plane + (long)(jb + r) * nx;
+            else if (r < 2 * tj + 1) row = a.v + ioff + (long)k * plane + (long)wrap(jb - 1 + (r - tj), ny) * nx;
+            else if (r < 3 * tj + 1) row = a.w + ioff + (long)k * plane + (long)(jb + (r - 2 * tj - 1)) * nx;
+            else row = a.w + ioff + (long)km * plane + (long)(jb + (r - 3 * tj - 1)) * nx;
+            bulk_copy_g2s(stage(s) + (size_t)r * nx, row, (unsigned)(nx * sizeof(double)), &bars[s]);
+        }
+    };
+    const int G = gridDim.x;
+    int n = 0, t = blockIdx.x;
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + G < ntiles) issue(blockIdx.x + G, 1);
+    for (; t < ntiles; t += G, ++n) {
+        const int s = n & 1;
+        if (!mbar_wait(&bars[s], (unsigned)(n >> 1) & 1u)) {
+            abort_flag = 1;
+            if (a.err) *(volatile unsigned*)a.err = 1u;
+        }
+        __syncthreads();
+        if (abort_flag) break;
+        int inst, k, jb;
+        tile_of(t, inst, k, jb);
+        const double* st = stage(s);
+        const int total = tj * n2;
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int rr = (int)fdiv(e, a.fd_n2), m = e - rr * n2;
+            double d0, d1;
+            if (a.mode == 0) {
+                const double* U = st + (size_t)rr * nx;
+                const double* Vm = st + (size_t)(tj + rr) * nx;
+                const double* Vc = Vm + nx;
+                const double* Wc = st + (size_t)(2 * tj + 1 + rr) * nx;
+                const double* Wm = st + (size_t)(3 * tj + 1 + rr) * nx;
+                const double2 uu = *reinterpret_cast<const double2*>(U + 2 * m);
+                const double um = U[wrap(2 * m - 1, nx)];
+                const double2 vv = *reinterpret_cast<const double2*>(Vc + 2 * m);
+                const double2 vm = *reinterpret_cast<const double2*>(Vm + 2 * m);
+                const double2 ww = *reinterpret_cast<const double2*>(Wc + 2 * m);
+                const double2 wm = *reinterpret_cast<const double2*>(Wm + 2 * m);
+                d0 = ((uu.x - um) * a.rdx + (vv.x - vm.x) * a.rdy + (ww.x - wm.x) * a.rdz) * a.rdt;
+                d1 = ((uu.y - uu.x) * a.rdx + (vv.y - vm.y) * a.rdy + (ww.y - wm.y) * a.rdz) * a.rdt;
+            } else {
+                const double2 sv = *reinterpret_cast<const double2*>(st + (size_t)rr * nx + 2 * m);
+                d0 = sv.x; d1 = sv.y;
+            }
+            buf[m * ld + rr] = mk<R>((R)d0, (R)d1);
+        }
+        __syncthreads();   // stage s consumed: refill it with tile t + 2G
+        if (t + 2 * G < ntiles) issue(t + 2 * G, s);
+        fft_batch<false, R, MAXR, true>(buf, ld, tj, a.px, -1, tx.tw, tj);
+        T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
+        for (int e = threadIdx.x; e < tj * (n2 + 1); e += blockDim.x) {
+            const int kx = (int)fdiv(e, a.fd_tj), rr = e - kx * tj;
+            const int k1 = (kx == n2) ? 0 : kx;
+            const int k2 = (kx == 0) ? 0 : n2 - kx;
+            spec[(long)kx * ny + jb + rr] = r2c_unpack<R>(buf[tx.pos[k1] * ld + rr], buf[tx.pos[k2] * ld + rr], twx[kx]);
+        }
+        __syncthreads();   // buf free for the next tile
+    }
+    if (abort_flag && threadIdx.x == 0) {
+        // let copies already in flight (tiles t and t + G) land before the
+        // block's shared memory is released
+        mbar_wait(&bars[n & 1], (unsigned)(n >> 1) & 1u);
+        if (t + G < ntiles) mbar_wait(&bars[(n + 1) & 1], (unsigned)((n + 1) >> 1) & 1u);
+    }
+}
+
 // one y transform of every kx line of a plane, in place on [k][kx][ky]
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_ylines(const PlaneArgs a, int sign,
@@ -723,7 +850,9 @@ size_t plane_fwd_smem(const PlaneArgs& a, bool fp32) {
            tables_y_bytes(a, es);
 }
 size_t plane_inv_smem(const PlaneArgs& a, bool fp32) { return plane_fwd_smem(a, fp32); }
+size_t pipe_smem(const PlaneArgs& a, bool fp32);
 size_t plane_smem(const PlaneArgs& a, bool fp32) {
+    if (a.impl == 2) return std::max(pipe_smem(a, fp32), std::max(rows_smem(a, fp32), ylines_smem(a, fp32)));
     if (a.impl == 1) return std::max(rows_smem(a, fp32), ylines_smem(a, fp32));
     return plane_fwd_smem(a, fp32);
 }
@@ -731,12 +860,41 @@ size_t plane_smem(const PlaneArgs& a, bool fp32) {
 static int maxr_x(const PlaneArgs& a) { return plan_max_radix(a.px) >= 16 ? 16 : 8; }
 static int maxr_y(const PlaneArgs& a) { return plan_max_radix(a.py) >= 16 ? 16 : 8; }
 
+size_t pipe_smem(const PlaneArgs& a, bool fp32) {
+    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
+    return 2 * pipe_stage_bytes(a) + align16((size_t)(a.nx / 2) * (a.tj | 1) * es) + tables_x_bytes(a, es) +
+           2 * sizeof(unsigned long long);
+}
+
+template <typename R, int MX>
+static cudaError_t launch_pipe(const PlaneArgs& a, cudaStream_t s) {
+    const size_t sm = pipe_smem(a, sizeof(R) == 4);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rows_fwd_pipe<R, MX>, kPlaneThreads, sm);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int ntiles = (a.ny / a.tj) * a.nz * std::max(1, a.batch);
+    const int grid = std::min(ntiles, per_sm * sms);
+    k_rows_fwd_pipe<R, MX><<<grid, kPlaneThreads, sm, s>>>(a, ntiles);
+    return cudaGetLastError();
+}
+
 template <typename R, int MX, int MY>
 static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) {
     const int nb = std::max(1, a.batch);
     const dim3 grows(a.ny / a.tj, a.nz * nb), glines((a.nxh + a.ly - 1) / a.ly, a.nz * nb);
     const size_t smr = rows_smem(a, sizeof(R) == 4), sml = ylines_smem(a, sizeof(R) == 4);
-    if (fwd) {
+    if (fwd && a.impl == 2 && a.mode != 2) {
+        cudaError_t e = launch_pipe<R, MX>(a, s);
+        if (e != cudaSuccess) return e;
+        k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
+    } else if (fwd) {
         k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
         k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
     } else {
@@ -758,6 +916,17 @@ static cudaError_t launch_split_t(const PlaneArgs& a0, bool fwd, cudaStream_t s)
     return launch_split_m<R, 8, 8>(a, fwd, s);
 }
 
+// opt a kernel in to the largest dynamic shared memory its static shared
+// memory leaves within the 227 KB a block may use
+template <typename K>
+static cudaError_t max_dynamic_smem(K kernel) {
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                227 * 1024 - (int)fa.sharedSizeBytes);
+}
+
 template <typename R, int MAXR>
 static cudaError_t setup_m() {
     cudaError_t e;
@@ -769,6 +938,7 @@ static cudaError_t setup_m() {
     if ((e = cudaFuncSetAttribute(k_rows_fwd<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
     if ((e = cudaFuncSetAttribute(k_rows_inv<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
     if ((e = cudaFuncSetAttribute(k_ylines<R, MAXR>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+    if ((e = max_dynamic_smem(k_rows_fwd_pipe<R, MAXR>))) return e;
     return cudaSuccess;
 }
 template <typename R>
@@ -828,11 +998,11 @@ int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd) {
 }
 
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s) {
-    if (a.impl == 1) return fp32 ? launch_split_t<float>(a, true, s) : launch_split_t<double>(a, true, s);
+    if (a.impl >= 1) return fp32 ? launch_split_t<float>(a, true, s) : launch_split_t<double>(a, true, s);
     return fp32 ? launch_plane_t<float, true>(a, s) : launch_plane_t<double, true>(a, s);
 }
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
-    if (a.impl == 1) return fp32 ? launch_split_t<float>(a, false, s) : launch_split_t<double>(a, false, s);
+    if (a.impl >= 1) return fp32 ? launch_split_t<float>(a, false, s) : launch_split_t<double>(a, false, s);
     return fp32 ? launch_plane_t<float, false>(a, s) : launch_plane_t<double, false>(a, s);
 }
 

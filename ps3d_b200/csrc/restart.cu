@@ -141,4 +141,42 @@ int Ctx::read_restart(const char* path, double* time_out) {
     return PS3D_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous snapshot (the snapshot cadence of main.f90:144-152 without the
+// netCDF writer): the state and p are copied on the device at the point of
+// the call, then converted to the halo layout and copied to the host on a
+// second stream while the main stream keeps stepping.
+// ---------------------------------------------------------------------------
+int Ctx::snapshot_begin(double* const* host) {
+    if (batch != 1) return PS3D_ERR_BADPARAM;
+    int rc = materialize();
+    if (rc) return rc;
+    if (!snap_stream) CK(cudaStreamCreateWithFlags(&snap_stream, cudaStreamNonBlocking));
+    if (!snap_event) CK(cudaEventCreateWithFlags(&snap_event, cudaEventDisableTiming));
+    CK(cudaStreamSynchronize(snap_stream));   // the previous snapshot's buffers are free
+    const size_t n3 = (size_t)(nx + 4) * (ny + 4) * (nz + 4);
+    if (!snap[0].p) {
+        for (int q = 0; q < 5; ++q) CK(snap[q].alloc(N * sizeof(double)));
+        CK(snap_staging.alloc(n3 * sizeof(double)));
+    }
+    const double* src[5] = {field(0), field(1), field(2), field(3), (const double*)p.p};
+    for (int q = 0; q < 5; ++q)
+        CK(cudaMemcpyAsync(snap[q].p, src[q], N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaEventRecord(snap_event, stream));
+    CK(cudaStreamWaitEvent(snap_stream, snap_event, 0));
+    for (int q = 0; q < 5; ++q) {
+        if (!host[q]) continue;
+        CK(launch_to_halo(snap[q].p, (double*)snap_staging.p, nx, ny, nz, q == 4 && rigid, false, snap_stream));
+        CK(cudaMemcpyAsync(host[q], snap_staging.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, snap_stream));
+    }
+    return PS3D_OK;
+}
+
+int Ctx::snapshot_wait() {
+    if (!snap_stream) return PS3D_OK;
+    CK(cudaStreamSynchronize(snap_stream));
+    CK(cudaGetLastError());
+    return PS3D_OK;
+}
+
 }  // namespace ps3d

@@ -229,7 +229,7 @@ cudaError_t Ctx::ensure_warn() {
 
 int Ctx::warn_launch(int mode, double2* o1, double2* o2, double kzcut2) {
     WarnArgs a{};
-    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid; a.layout = pa64.impl; a.mode = mode;
+    a.nxh = nxh; a.ny = ny; a.nz = nz; a.rigid = rigid; a.layout = spectral_layout(pa64); a.mode = mode;
     a.dx = P.dx; a.dy = P.dy; a.dz = P.dz; a.f0 = P.f0; a.N0 = P.N0; a.dsqr = P.dsqr; a.Ro = P.Ro; a.dt = P.dt;
     a.kzcut2 = kzcut2;
     a.ax.kx = (const double*)t_kx.p; a.ax.ky = (const double*)t_ky.p; a.ax.kz = (const double*)t_kz.p;

@@ -60,6 +60,8 @@ def load():
     L.ps3d_get_fields.argtypes = [vp, C.c_int, dp, dp, dp, dp]
     L.ps3d_diag_balance.argtypes = [vp, C.c_int, C.c_int]
     L.ps3d_write_restart.argtypes = [vp, C.c_char_p]
+    L.ps3d_snapshot_begin.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.ps3d_snapshot_wait.argtypes = [vp]
     L.ps3d_read_restart.argtypes = [vp, C.c_char_p, dp]
     L.ps3d_diagnose.argtypes = [vp, dp, dp, dp, dp]
     L.ps3d_set_forcing.argtypes = [vp, C.POINTER(Forcing)]
@@ -177,6 +179,22 @@ class Model:
     def diag_balance_zero_order(self):
         self.project(abi.PS3D_PROJ_ZERO_ORDER)
         return self.get_fields(abi.PS3D_FIELDS_ZERO)
+
+    def snapshot_begin(self, out):
+        """Queue an asynchronous snapshot of u, v, w, b, p into caller-owned
+        C-contiguous float64 arrays of the halo shape (page-locked to overlap);
+        keep them alive until snapshot_wait()."""
+        for n in ("u", "v", "w", "b", "p"):
+            a = out.get(n)
+            if a is not None and (a.shape != self.shape or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError(f"snapshot_begin: {n} must be C-contiguous float64 of shape {self.shape}")
+        self._snap_keep = out
+        _check(self.L.ps3d_snapshot_begin(self.h, *[dptr(out.get(n)) for n in ("u", "v", "w", "b", "p")]),
+               "ps3d_snapshot_begin")
+
+    def snapshot_wait(self):
+        _check(self.L.ps3d_snapshot_wait(self.h), "ps3d_snapshot_wait")
+        self._snap_keep = None
 
     def write_restart(self, path):
         """write_restart (restart.f90:2-22): the reference's one-rank restart file."""

@@ -17,7 +17,7 @@ def _member_fields(p, amp, seed):
     return cf.add_noise(p, f, "b", rel=1e-3, seed=seed)
 
 
-@pytest.mark.parametrize("impl", ["0", "1"])
+@pytest.mark.parametrize("impl", ["0", "1", "2"])
 @pytest.mark.parametrize("precision", [abi.PS3D_FP64, abi.PS3D_MIXED])
 def test_ensemble_members_match_single_runs(precision, impl, monkeypatch):
     monkeypatch.setenv("PS3D_PLANE_IMPL", impl)
@@ -67,7 +67,7 @@ def test_plane_implementations_agree():
     p = cf.eddy_params(64, 64, 32)
     f = _member_fields(p, 0.1, seed=4)
     out = []
-    for impl in ("0", "1"):
+    for impl in ("0", "1", "2"):
         os.environ["PS3D_PLANE_IMPL"] = impl
         try:
             m = Model(p)
@@ -77,5 +77,6 @@ def test_plane_implementations_agree():
         m.run(30)
         out.append(m.download(tendencies=False))
         m.close()
-    for n in ("u", "v", "w", "b", "p"):
-        assert rel(out[1][n], out[0][n]) < 1e-12, n
+    for q in (1, 2):
+        for n in ("u", "v", "w", "b", "p"):
+            assert rel(out[q][n], out[0][n]) < 1e-12, (q, n)

@@ -22,11 +22,12 @@ TOL_KERNEL = 1e-12
 TOL_MIXED = 1e-5
 
 
-@pytest.fixture(autouse=True, params=["cluster", "rows+lines"])
+@pytest.fixture(autouse=True, params=["cluster", "rows+lines", "pipe+lines"])
 def plane_impl(request, monkeypatch):
-    """Every parity case runs on both plane-transform implementations: the
-    one-cluster-per-plane kernels and the rows pass + y-lines pass."""
-    monkeypatch.setenv("PS3D_PLANE_IMPL", "0" if request.param == "cluster" else "1")
+    """Every parity case runs on the three plane-transform implementations:
+    the one-cluster-per-plane kernels, the rows pass + y-lines pass, and the
+    latter with the forward rows pass pipelined by bulk copies."""
+    monkeypatch.setenv("PS3D_PLANE_IMPL", {"cluster": "0", "rows+lines": "1", "pipe+lines": "2"}[request.param])
     return request.param
 
 

@@ -127,3 +127,20 @@ def test_read_restart_rejects_other_grid(tmp_path):
         other.read_restart(str(tmp_path / "missing.dta"))
     other.close()
     m.close()
+
+
+def test_async_snapshot_is_the_state_at_the_call():
+    import torch
+    p, a = _model(seed=3)
+    _, b = _model(seed=3)
+    a.run(5)
+    out = {n: torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for n in "uvwbp"}
+    a.snapshot_begin(out)
+    a.run(5)          # keeps stepping while the copies drain
+    a.snapshot_wait()
+    b.run(5)
+    ref = b.download(tendencies=False)
+    for n in "uvwbp":
+        assert np.array_equal(out[n], ref[n]), n
+    a.close()
+    b.close()
