@@ -446,22 +446,34 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
                 if (kb + q < nz - 1) col[(long)(kb + q) * ls] = d[q];
         }
     } else {
-        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
+        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr,
+        // in chunks with the next chunk's loads in flight like the sweeps above
         const double h = a.dz2dsqr;
-        const R prev_orig = col[0];
-        col[0] = (R)0;
-        if (nz > 1) {
-            double x0 = 0.0;
-            R orig_km1 = col[ls];
-            double x1 = (double)prev_orig * h;
-            col[ls] = (R)x1;
-            for (int k = 2; k < nz; ++k) {
-                const R ok = col[(long)k * ls];
-                const double xk = 2 * x1 - x0 + (double)orig_km1 * h;
-                col[(long)k * ls] = (R)xk;
-                x0 = x1; x1 = xk;
-                orig_km1 = ok;
+        double x0 = 0.0, x1 = 0.0, fprev = 0.0;   // p(k-2), p(k-1), f(k-1)
+        R nxt[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q)
+            if (q < nz) nxt[q] = col[(long)q * ls];
+        for (int kb = 0; kb < nz; kb += KC) {
+            R d[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + KC + q < nz) nxt[q] = col[(long)(kb + KC + q) * ls];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int k = kb + q;
+                if (k < nz) {
+                    const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
+                    fprev = (double)d[q];
+                    x0 = x1; x1 = xk;
+                    d[q] = (R)xk;
+                }
             }
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + q < nz) col[(long)(kb + q) * ls] = d[q];
         }
     }
 }

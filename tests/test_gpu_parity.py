@@ -51,6 +51,19 @@ def test_pressure_solver(rigid, shape, plane_impl):
     assert max(err.values()) < TOL_KERNEL, err
 
 
+@pytest.mark.parametrize("nz", [40, 64, 100, 129])
+def test_pressure_solver_tall_columns(nz):
+    """Rigid-lid solve on columns split into several segments: nz = 64 fills
+    every segment, 40 and 100 leave the last one short, 129 leaves trailing
+    segments empty."""
+    p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
+    o, m = _pair(p, random_state(p, seed=3))
+    o.pressure_solver()
+    m.pressure_solver()
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL_KERNEL, err
+
+
 def test_pressure_solver_divergence_free():
     p = small_params(64, 32, 16, rigid=True)
     _, m = _pair(p, random_state(p, seed=2))
