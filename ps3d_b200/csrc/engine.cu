@@ -179,6 +179,7 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
         for (int tj : {4, 8, 16, 32}) {
             if (ny % tj || (im == 1 && tj == 4) || (im == 2 && tj > 16)) continue;
             for (int ly : {8, 16, 32}) {
+                if (ylines_in_registers(ny) && ly != 16) continue;
                 PlaneArgs a = base;
                 a.impl = im; a.tj = tj; a.ly = ly;
                 a.C = 1; a.rows_per_cta = ny; a.cols_per_cta = nxh; a.row_chunk = 8; a.ldr = 9; a.ldc = nxh | 1;

@@ -108,6 +108,9 @@ cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int
 size_t plane_fwd_smem(const PlaneArgs& a, bool fp32);
 size_t plane_inv_smem(const PlaneArgs& a, bool fp32);
 size_t plane_smem(const PlaneArgs& a, bool fp32);   // largest dynamic shared memory of the configuration
+// ny with a register-resident y transform (k_ylines_reg): the y-lines pass
+// then has no lines-per-CTA parameter
+bool ylines_in_registers(int ny);
 cudaError_t plane_setup(bool fp32);
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);

@@ -790,6 +790,70 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_
     }
 }
 
+// ---------------------------------------------------------------------------
+// y transforms held in registers, for ny = N1 N2 (64, 128, 256): the
+// four-step split of one DFT of length N,
+//   X[k1 + N1 k2] = sum_n2 w_N2^(n2 k2) w_N^(n2 k1) sum_n1 x[N2 n1 + n2] w_N1^(n1 k1),
+// with w_M = exp(sign 2 pi i / M).  A line is N2 adjacent lanes of one warp:
+// lane n2 loads x[N2 n1 + n2] straight from HBM (consecutive lanes,
+// consecutive addresses), runs the length-N1 DFT in registers, applies
+// w_N^(n2 k1) and writes its N1 values to the line's shared-memory tile;
+// after a warp barrier lane t takes the N1/N2 rows k1 = t + N2 r, runs the
+// length-N2 DFTs and stores X in natural order, again consecutive lanes on
+// consecutive addresses.  One shared-memory round trip per element (the
+// staged radix stages of k_ylines make one per stage plus the staging), no
+// block barrier, no permutation.  Lines run over all planes and instances
+// of the [k][kx][ky] array, so partial blocks occur only at the very end.
+// ---------------------------------------------------------------------------
+template <int N1, int N2>
+struct YReg {
+    static constexpr int N = N1 * N2;
+    static constexpr int LPB = kPlaneThreads / N2;            // lines per block
+    static constexpr int LS = N1 * (N2 + 1) + 1;              // tile stride of a line (elements)
+};
+
+template <typename R, int N1, int N2>
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs a, long nlines, int sign,
+                                                                 double scale) {
+    using T = cpx<R>;
+    using Y = YReg<N1, N2>;
+    static_assert(N1 >= N2 && N1 % N2 == 0, "split");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tl = threadIdx.x % N2;
+    const int li = threadIdx.x / N2;
+    T* tile = reinterpret_cast<T*>(smem_raw) + li * Y::LS;
+    const long g = (long)blockIdx.x * Y::LPB + li;
+    const bool valid = g < nlines;
+    T* line = reinterpret_cast<T*>(a.spec) + (valid ? g : 0) * Y::N;
+    const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.py.tw : (const void*)a.py.twf);
+    T v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = valid ? line[N2 * n1 + tl] : mk<R>((R)0, (R)0);
+    small_dft<N1>(v, sign);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+        T w = __ldg(tw + tl * k1);
+        if (sign > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) tile[k1 * (N2 + 1) + tl] = v[k1];
+    __syncwarp();
+    const R sc = (R)scale;
+#pragma unroll
+    for (int r = 0; r < N1 / N2; ++r) {
+        const int k1 = tl + N2 * r;
+        T u[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = tile[k1 * (N2 + 1) + n2];
+        small_dft<N2>(u, sign);
+        if (valid) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) line[k1 + N1 * k2] = cscale(u[k2], sc);
+        }
+    }
+}
+
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_inv(const PlaneArgs a) {
     using T = cpx<R>;
@@ -897,22 +961,47 @@ static cudaError_t launch_pipe(const PlaneArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <typename R, int N1, int N2>
+static cudaError_t launch_ylines_reg_t(const PlaneArgs& a, int sign, double scale, cudaStream_t s) {
+    using Y = YReg<N1, N2>;
+    const long nlines = (long)a.nxh * a.nz * std::max(1, a.batch);
+    const size_t sm = (size_t)Y::LPB * Y::LS * sizeof(cpx<R>);
+    k_ylines_reg<R, N1, N2><<<(unsigned)((nlines + Y::LPB - 1) / Y::LPB), kPlaneThreads, sm, s>>>(a, nlines, sign,
+                                                                                                   scale);
+    return cudaGetLastError();
+}
+// the register y transform when ny has a two-factor split, else false
+bool ylines_in_registers(int ny) { return ny == 64 || ny == 128 || ny == 256; }
+
+template <typename R>
+static bool ylines_reg(const PlaneArgs& a, int sign, double scale, cudaStream_t s, cudaError_t* e) {
+    switch (a.ny) {
+        case 64: *e = launch_ylines_reg_t<R, 8, 8>(a, sign, scale, s); return true;
+        case 128: *e = launch_ylines_reg_t<R, 16, 8>(a, sign, scale, s); return true;
+        case 256: *e = launch_ylines_reg_t<R, 16, 16>(a, sign, scale, s); return true;
+        default: return false;
+    }
+}
+
 template <typename R, int MX, int MY>
 static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) {
     const int nb = std::max(1, a.batch);
     const dim3 grows(a.ny / a.tj, a.nz * nb), glines((a.nxh + a.ly - 1) / a.ly, a.nz * nb);
     const size_t smr = rows_smem(a, sizeof(R) == 4), sml = ylines_smem(a, sizeof(R) == 4);
+    cudaError_t e = cudaSuccess;
     if (fwd && a.impl == 2 && a.mode != 2) {
-        cudaError_t e = launch_pipe<R, MX>(a, s);
+        e = launch_pipe<R, MX>(a, s);
         if (e != cudaSuccess) return e;
-        k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
+        if (!ylines_reg<R>(a, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
     } else if (fwd) {
         k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
-        k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
+        if (!ylines_reg<R>(a, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
     } else {
-        k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, +1, 1.0);
+        if (!ylines_reg<R>(a, +1, 1.0, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, +1, 1.0);
+        if (e != cudaSuccess) return e;
         k_rows_inv<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
     }
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 template <typename R>
@@ -956,6 +1045,9 @@ static cudaError_t setup_m() {
 template <typename R>
 static cudaError_t setup_t() {
     cudaError_t e;
+    if ((e = max_dynamic_smem(k_ylines_reg<R, 8, 8>))) return e;
+    if ((e = max_dynamic_smem(k_ylines_reg<R, 16, 8>))) return e;
+    if ((e = max_dynamic_smem(k_ylines_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
     if ((e = setup_m<R, 16>())) return e;
     return setup_m<R, 8>();

@@ -40,7 +40,7 @@ def _pair(p, fields, pfield=None):
 
 
 @pytest.mark.parametrize("rigid", [True, False])
-@pytest.mark.parametrize("shape", [(32, 32, 16), (48, 40, 12), (256, 256, 8), (128, 64, 8), (64, 256, 4)])
+@pytest.mark.parametrize("shape", [(32, 32, 16), (48, 40, 12), (256, 256, 8), (128, 64, 8), (64, 128, 8), (64, 256, 4)])
 def test_pressure_solver(rigid, shape, plane_impl):
     p = small_params(*shape, rigid=rigid)
     o, m = _pair(p, random_state(p, seed=1))
