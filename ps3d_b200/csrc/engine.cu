@@ -178,6 +178,8 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
     for (int im : {1, 2}) {
         for (int tj : {4, 8, 16, 32}) {
             if (ny % tj || (im == 1 && tj == 4) || (im == 2 && tj > 16)) continue;
+            // FP32 runs both rows passes in registers (no rows-per-CTA parameter)
+            if (im == 1 && es == sizeof(float2) && rows_in_registers(nx, ny) && tj != 16) continue;
             for (int ly : {8, 16, 32}) {
                 if (ylines_in_registers(ny) && ly != 16) continue;
                 PlaneArgs a = base;

@@ -111,6 +111,9 @@ size_t plane_smem(const PlaneArgs& a, bool fp32);   // largest dynamic shared me
 // ny with a register-resident y transform (k_ylines_reg): the y-lines pass
 // then has no lines-per-CTA parameter
 bool ylines_in_registers(int ny);
+// grid with register-resident rows passes (k_rows_fwd_reg / k_rows_inv_reg):
+// the rows pass then has no rows-per-CTA parameter
+bool rows_in_registers(int nx, int ny);
 cudaError_t plane_setup(bool fp32);
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);

@@ -854,6 +854,184 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rows passes held in registers, for nx/2 = N1 N2 (64, 128, 256): the
+// half-length complex transform of each row (z_m = s(2m) + i s(2m+1)) by
+// the same four-step split as k_ylines_reg.  A block takes kRowsRegTJ
+// consecutive rows of one plane, N2 lanes per row.
+//   forward: all lanes form z from u, v, w (or the source field) with m
+//            fastest into the rows' tiles; lane n2 of a row takes
+//            m = N2 n1 + n2, DFT N1, twiddle, warp-local transpose, DFT N2;
+//            Z goes to a block tile [m][row] (a barrier, aliasing the row
+//            tiles) from which the r2c unpack reads Z_kx and Z_{N-kx} and
+//            writes each kx as a run of kRowsRegTJ rows.
+//   inverse: the c2r pack reads X_kx and X_{N-kx} in runs of rows into the
+//            block tile, lanes take their stride-N2 elements from it, DFT
+//            N1, twiddle, transpose, DFT N2, and each lane stores its pairs
+//            (2m, 2m+1) straight to p.
+// Three (forward) and two (inverse) shared-memory round trips per element
+// against the staged kernels' one per radix stage plus staging and the
+// unpack gather.
+// ---------------------------------------------------------------------------
+constexpr int kRowsRegTJ = 16;
+
+template <int N1, int N2>
+struct RowReg {
+    static constexpr int N = N1 * N2;
+    static constexpr int TJ = kRowsRegTJ;
+    static constexpr int NT = TJ * N2;                    // threads per block
+    static constexpr int LS = N1 * (N2 + 1) + 1;          // transpose tile stride of a row
+    static constexpr int LD = TJ + 1;                     // block tile [m][row] pitch
+    static constexpr size_t T1 = (size_t)TJ * LS, T2 = (size_t)N * LD;
+    static constexpr size_t elems = T1 > T2 ? T1 : T2;
+};
+
+template <typename R, int N1, int N2>
+__global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const PlaneArgs a) {
+    using T = cpx<R>;
+    using G = RowReg<N1, N2>;
+    constexpr int N = G::N, TJ = G::TJ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* tb = reinterpret_cast<T*>(smem_raw);
+    const int nz = a.nz, ny = a.ny;
+    const int tl = threadIdx.x % N2;
+    const int row = threadIdx.x / N2;
+    const int jb = blockIdx.x * TJ;
+    const int inst = blockIdx.y / nz;
+    const int k = blockIdx.y - inst * nz;
+    const long ioff = (long)inst * a.sN;
+    const double* asrc = a.src ? a.src + ioff : nullptr;
+    const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.px.tw : (const void*)a.px.twf);
+    // z = s(2m) + i s(2m+1) of the block's rows, formed by all lanes with m
+    // fastest (coalesced, LB points in flight per lane) into each row's tile
+    constexpr int LB = 4;
+    static_assert((N * TJ) % (LB * G::NT) == 0, "source batches");
+    for (int t0 = threadIdx.x; t0 < N * TJ; t0 += LB * G::NT) {
+        double2 d[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * G::NT;
+            d[q] = plane_source_pair(a, a.u + ioff, a.v + ioff, a.w + ioff, asrc, k, jb + t / N, t % N);
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * G::NT;
+            tb[(t / N) * G::LS + t % N] = mk<R>((R)d[q].x, (R)d[q].y);
+        }
+    }
+    __syncthreads();
+    T* t1 = tb + row * G::LS;   // this row's tile: the source, then the transpose
+    T v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = t1[N2 * n1 + tl];
+    __syncwarp();
+    small_dft<N1>(v, -1);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], __ldg(tw + tl * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) t1[k1 * (N2 + 1) + tl] = v[k1];
+    __syncwarp();
+    T z[N1];   // z[r N2 + k2] = Z[k1 + N1 k2], k1 = tl + N2 r
+#pragma unroll
+    for (int r = 0; r < N1 / N2; ++r) {
+        const int k1 = tl + N2 * r;
+        T u[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = t1[k1 * (N2 + 1) + n2];
+        small_dft<N2>(u, -1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) z[r * N2 + k2] = u[k2];
+    }
+    __syncthreads();   // the transpose tiles are read; the block tile reuses them
+#pragma unroll
+    for (int r = 0; r < N1 / N2; ++r)
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) tb[(tl + N2 * r + N1 * k2) * G::LD + row] = z[r * N2 + k2];
+    __syncthreads();
+    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * a.nxh * ny + jb;
+    for (int t = threadIdx.x; t < (N + 1) * TJ; t += G::NT) {
+        const int kx = t / TJ, rr = t - kx * TJ;
+        const int k1 = (kx == N) ? 0 : kx;
+        const int k2 = (kx == 0) ? 0 : N - kx;
+        const double2 w = __ldg(a.twx + kx);
+        spec[(long)kx * ny + rr] = r2c_unpack<R>(tb[k1 * G::LD + rr], tb[k2 * G::LD + rr], mk<R>((R)w.x, (R)w.y));
+    }
+}
+
+template <typename R, int N1, int N2>
+__global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const PlaneArgs a) {
+    using T = cpx<R>;
+    using G = RowReg<N1, N2>;
+    constexpr int N = G::N, TJ = G::TJ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* tb = reinterpret_cast<T*>(smem_raw);
+    const int nz = a.nz, ny = a.ny, nx = a.nx;
+    const int tl = threadIdx.x % N2;
+    const int row = threadIdx.x / N2;
+    const int jb = blockIdx.x * TJ;
+    const int inst = blockIdx.y / nz;
+    const int k = blockIdx.y - inst * nz;
+    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)k * a.nxh * ny + jb;
+    const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.px.tw : (const void*)a.px.twf);
+    // c2r pack into the block tile [m][row], loads batched per thread
+    constexpr int LB = 4;
+    static_assert((N * TJ) % (LB * G::NT) == 0, "pack batches");
+    for (int t0 = threadIdx.x; t0 < N * TJ; t0 += LB * G::NT) {
+        T xk[LB], xc[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * G::NT;
+            const int kk = t / TJ, rr = t - kk * TJ;
+            xk[q] = spec[(long)kk * ny + rr];
+            xc[q] = spec[(long)(N - kk) * ny + rr];
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int t = t0 + q * G::NT;
+            const int kk = t / TJ, rr = t - kk * TJ;
+            const double2 w = __ldg(a.twx + kk);
+            tb[kk * G::LD + rr] = c2r_pack<R>(xk[q], xc[q], mk<R>((R)w.x, (R)w.y), kk == 0);
+        }
+    }
+    __syncthreads();
+    T v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = tb[(N2 * n1 + tl) * G::LD + row];
+    __syncthreads();   // the block tile is read; the transpose tiles reuse it
+    small_dft<N1>(v, +1);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+        T w = __ldg(tw + tl * k1);
+        w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    T* t1 = tb + row * G::LS;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) t1[k1 * (N2 + 1) + tl] = v[k1];
+    __syncwarp();
+    const double sc = a.scale;
+    double* out = a.out + (long)inst * a.sN + (long)k * nx * ny + (long)(jb + row) * nx;
+#pragma unroll
+    for (int r = 0; r < N1 / N2; ++r) {
+        const int k1 = tl + N2 * r;
+        T u[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = t1[k1 * (N2 + 1) + n2];
+        small_dft<N2>(u, +1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            const int m = k1 + N1 * k2;
+            double2 o = make_double2((double)u[k2].x * sc, (double)u[k2].y * sc);
+            double2* g = reinterpret_cast<double2*>(out + 2 * m);
+            if (a.beta != 0.0) {
+                const double2 prev = *g;
+                o.x = o.x + a.beta * prev.x; o.y = o.y + a.beta * prev.y;
+            }
+            *g = o;
+        }
+    }
+}
+
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_inv(const PlaneArgs a) {
     using T = cpx<R>;
@@ -983,6 +1161,35 @@ static bool ylines_reg(const PlaneArgs& a, int sign, double scale, cudaStream_t 
     }
 }
 
+bool rows_in_registers(int nx, int ny) {
+    return (nx == 128 || nx == 256 || nx == 512) && ny % kRowsRegTJ == 0;
+}
+template <typename R, int N1, int N2>
+static cudaError_t launch_rows_reg_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
+    using G = RowReg<N1, N2>;
+    const dim3 g(a.ny / G::TJ, a.nz * std::max(1, a.batch));
+    const size_t sm = G::elems * sizeof(cpx<R>);
+    if (fwd) k_rows_fwd_reg<R, N1, N2><<<g, G::NT, sm, s>>>(a);
+    else k_rows_inv_reg<R, N1, N2><<<g, G::NT, sm, s>>>(a);
+    return cudaGetLastError();
+}
+// The register rows pass when nx/2 has a two-factor split, else false.  The
+// FP64 forward pass keeps the staged kernel: its register form needs ~92
+// registers for the 16 source points of a lane and runs 5 blocks per SM,
+// too few to cover the six loads per point (112.8 vs 105.4 us for the
+// forward transform at 256x256x128); in FP32 it runs 7 (87 vs 100 us).
+template <typename R>
+static bool rows_reg(const PlaneArgs& a, bool fwd, cudaStream_t s, cudaError_t* e) {
+    if (fwd && sizeof(R) == 8) return false;
+    if (!rows_in_registers(a.nx, a.ny)) return false;
+    switch (a.nx) {
+        case 128: *e = launch_rows_reg_t<R, 8, 8>(a, fwd, s); return true;
+        case 256: *e = launch_rows_reg_t<R, 16, 8>(a, fwd, s); return true;
+        case 512: *e = launch_rows_reg_t<R, 16, 16>(a, fwd, s); return true;
+        default: return false;
+    }
+}
+
 template <typename R, int MX, int MY>
 static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) {
     const int nb = std::max(1, a.batch);
@@ -994,12 +1201,13 @@ static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) 
         if (e != cudaSuccess) return e;
         if (!ylines_reg<R>(a, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
     } else if (fwd) {
-        k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
+        if (!rows_reg<R>(a, true, s, &e)) k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
+        if (e != cudaSuccess) return e;
         if (!ylines_reg<R>(a, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
     } else {
         if (!ylines_reg<R>(a, +1, 1.0, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, +1, 1.0);
         if (e != cudaSuccess) return e;
-        k_rows_inv<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
+        if (!rows_reg<R>(a, false, s, &e)) k_rows_inv<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
     }
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
@@ -1048,6 +1256,12 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_ylines_reg<R, 8, 8>))) return e;
     if ((e = max_dynamic_smem(k_ylines_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_ylines_reg<R, 16, 16>))) return e;
+    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 8, 8>))) return e;
+    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 16, 8>))) return e;
+    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 16, 16>))) return e;
+    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 8, 8>))) return e;
+    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
+    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
     if ((e = setup_m<R, 16>())) return e;
     return setup_m<R, 8>();
