@@ -24,9 +24,15 @@ namespace ps3d {
 
 constexpr int kTX = 32;
 
-template <int BY, int NF>
+// The ring of state planes, and this level's Adams-Bashforth history of the
+// block's points (t1, t2), staged through shared memory so that its loads
+// go out with the next plane's before the barrier without holding
+// registers through the tendency arithmetic.
+template <typename TT, int BY, int NF>
 struct StepSmem {
     double pl[NF][3][(BY + 2) * (kTX + 2)];
+    TT hu[2][kTX * BY], hv[2][kTX * BY], hb[2][kTX * BY];
+    double hw[2][kTX * BY];
 };
 
 // read field f at offsets (di, dj) in ring slot s
@@ -36,7 +42,8 @@ template <typename TT, int BY, bool HARM, bool WM, bool BG>
 __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) {
     using TW = double;   // stored w tendencies stay FP64 in both paths
     constexpr int NF = BG ? 6 : 4;
-    __shared__ StepSmem<BY, NF> sm;
+    extern __shared__ __align__(16) unsigned char step_smem_raw[];
+    StepSmem<TT, BY, NF>& sm = *reinterpret_cast<StepSmem<TT, BY, NF>*>(step_smem_raw);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
@@ -98,8 +105,23 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
     load_plane(kb, kb % 3);
     const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
     const bool rigid = a.rigid;
+    const bool h1 = a.do_ab && a.ab1 != 0.0, h2 = a.do_ab && a.ab2 != 0.0;
     for (int k = kb; k < ke; ++k) {
+        // history loads first, so they are in flight with the plane's
+        TT hu1 = 0, hv1 = 0, hb1 = 0, hu2 = 0, hv2 = 0, hb2 = 0;
+        double hw1 = 0.0, hw2 = 0.0;
+        const long gh = (long)k * plane + (long)j * nx + i + ioff;
+        if (active && h1) {
+            const TT* const* h = (const TT* const*)a.t1;
+            hu1 = h[0][gh]; hv1 = h[1][gh]; hw1 = ((const TW*)a.t1[2])[gh]; hb1 = h[3][gh];
+        }
+        if (active && h2) {
+            const TT* const* h = (const TT* const*)a.t2;
+            hu2 = h[0][gh]; hv2 = h[1][gh]; hw2 = ((const TW*)a.t2[2])[gh]; hb2 = h[3][gh];
+        }
         load_plane(k + 1, (k + 1) % 3);
+        sm.hu[0][tid] = hu1; sm.hv[0][tid] = hv1; sm.hw[0][tid] = hw1; sm.hb[0][tid] = hb1;
+        sm.hu[1][tid] = hu2; sm.hv[1][tid] = hv2; sm.hw[1][tid] = hw2; sm.hb[1][tid] = hb2;
         __syncthreads();
         if (active) {
             const int sm1 = (k + 2) % 3, s0 = k % 3, sp1 = (k + 1) % 3;
@@ -245,15 +267,13 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
                 // the current tendency enters at full precision; only the
                 // stored history (FP32 in the mixed path) is rounded
                 double tu = c0 * du_, tv = c0 * dv_, tw = c0 * dw_, tb = c0 * db_;
-                if (c1 != 0.0) {
-                    const TT* const* h = (const TT* const*)a.t1;
-                    tu = tu + c1 * (double)h[0][g]; tv = tv + c1 * (double)h[1][g];
-                    tw = tw + c1 * (double)((const TW*)a.t1[2])[g]; tb = tb + c1 * (double)h[3][g];
+                if (h1) {
+                    tu = tu + c1 * (double)sm.hu[0][tid]; tv = tv + c1 * (double)sm.hv[0][tid];
+                    tw = tw + c1 * sm.hw[0][tid]; tb = tb + c1 * (double)sm.hb[0][tid];
                 }
-                if (c2 != 0.0) {
-                    const TT* const* h = (const TT* const*)a.t2;
-                    tu = tu + c2 * (double)h[0][g]; tv = tv + c2 * (double)h[1][g];
-                    tw = tw + c2 * (double)((const TW*)a.t2[2])[g]; tb = tb + c2 * (double)h[3][g];
+                if (h2) {
+                    tu = tu + c2 * (double)sm.hu[1][tid]; tv = tv + c2 * (double)sm.hv[1][tid];
+                    tw = tw + c2 * sm.hw[1][tid]; tb = tb + c2 * (double)sm.hb[1][tid];
                 }
                 u1 = u1 + dt * tu; v1 = v1 + dt * tv; w1 = w1 + dtw * tw; b1 = b1 + dt * tb;
             }
@@ -433,7 +453,7 @@ template <typename TT, int BY, bool HARM, bool WM, bool BG>
 static cudaError_t launch_step_t(const StepArgs& a, cudaStream_t s) {
     const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, a.nz) : (a.nz <= 16 ? a.nz : 8);
     dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((a.nz + kchunk - 1) / kchunk) * std::max(1, a.batch));
-    k_step<TT, BY, HARM, WM, BG><<<grid, dim3(kTX, BY), 0, s>>>(a, kchunk);
+    k_step<TT, BY, HARM, WM, BG><<<grid, dim3(kTX, BY), sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s>>>(a, kchunk);
     return cudaGetLastError();
 }
 
@@ -448,7 +468,24 @@ static cudaError_t launch_step_tt(const StepArgs& a, cudaStream_t s) {
 #undef L
 }
 
-cudaError_t step_setup() { return cudaSuccess; }   // static shared memory: nothing to opt in to
+template <typename TT>
+static cudaError_t step_setup_tt() {
+    cudaError_t e;
+#define S(H, W, G)                                                                                        \
+    if ((e = cudaFuncSetAttribute(k_step<TT, 8, H, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                  (int)sizeof(StepSmem<TT, 8, G ? 6 : 4>))))                              \
+        return e;
+    S(true, true, true) S(true, true, false) S(true, false, true) S(true, false, false)
+    S(false, true, true) S(false, true, false) S(false, false, true) S(false, false, false)
+#undef S
+    return cudaSuccess;
+}
+// opts the step kernels in to their dynamic shared memory (above 48 KB with
+// the background fields)
+cudaError_t step_setup() {
+    cudaError_t e = step_setup_tt<double>();
+    return e != cudaSuccess ? e : step_setup_tt<float>();
+}
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s) {
     return fp32_tendencies ? launch_step_tt<float>(a, s) : launch_step_tt<double>(a, s);
