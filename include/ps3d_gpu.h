@@ -294,6 +294,52 @@ PS3D_API int ps3d_ensemble_integrate(ps3d_ensemble* e, int nsteps);   /* waits f
 PS3D_API int ps3d_ensemble_enqueue(ps3d_ensemble* e, int nsteps);     /* queues only         */
 PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launches, void** stream);
 
+/* ---- one grid over several GPUs: z-slabs -----------------------------------
+ * Replaces the reference's MPI decomposition inside P3DFFT (my_fft.f90,
+ * p3dfft_setup; pressure_solver.f90 on its pencils) for the time step: rank r
+ * of nranks owns global levels k0 = r*nzl .. k0+nzl-1 (nzl = nz/nranks >= 2).
+ * A step is the phases below, in this order, each queued on the slab's
+ * stream (ps3d_slab_info); between them the caller moves data between ranks:
+ *   TENDENCY, PACK_STATE, [halo exchange], UNPACK_STATE, FORWARD,
+ *   [all-to-all: xbuf -> colbuf], VSOLVE, [all-to-all: colbuf -> xbuf],
+ *   INVERSE, PACK_P, [halo exchange], UNPACK_P, END_STEP.
+ * Halo exchange: hsend holds [planes for the rank below][planes for the rank
+ * above] (state: 4 and 4 planes of nx*ny doubles; p: 2 and 1); hrecv receives
+ * [what the rank below sent up][what the rank above sent down]; z is
+ * periodic over the ranks.  All-to-all: xbuf is [r][nzl][ccnt[r]] complex
+ * (blocks for rank r in rank order), colbuf is [nranks][nzl][ccnt[rank]].
+ * Before the first step after an upload the state halos are exchanged once
+ * (PACK_STATE, exchange, UNPACK_STATE).  ps3d_slab_group_step does all of it
+ * for the ranks of one process (device copies; one GPU or several).
+ * Upload/download take the rank's interior levels, [nzl][ny][nx] doubles,
+ * x fastest (no halos).  Rigid lid, FP64 and the fused step only
+ * (PS3D_ERR_UNSUPPORTED otherwise).                                        */
+#define PS3D_SLAB_TENDENCY     0
+#define PS3D_SLAB_PACK_STATE   1
+#define PS3D_SLAB_UNPACK_STATE 2
+#define PS3D_SLAB_FORWARD      3
+#define PS3D_SLAB_VSOLVE       4
+#define PS3D_SLAB_INVERSE      5
+#define PS3D_SLAB_PACK_P       6
+#define PS3D_SLAB_UNPACK_P     7
+#define PS3D_SLAB_END_STEP     8
+typedef struct ps3d_slab ps3d_slab;
+PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, int device, ps3d_slab** out);
+PS3D_API int ps3d_slab_destroy(ps3d_slab* s);
+PS3D_API int ps3d_slab_info(ps3d_slab* s, int* k0, int* nzl, long long* col0, long long* ncl, void** stream);
+/* sizes of the exchange buffers and every rank's column count (nranks entries) */
+PS3D_API int ps3d_slab_buffers(ps3d_slab* s, size_t* xbytes, size_t* colbytes, size_t* hbytes,
+                               long long* col_counts);
+/* use caller-owned device buffers (e.g. the tensors a collective library
+ * sends from and receives into) instead of the slab's own                 */
+PS3D_API int ps3d_slab_bind(ps3d_slab* s, void* xbuf, void* colbuf, void* hsend, void* hrecv);
+PS3D_API int ps3d_slab_upload(ps3d_slab* s, const double* u, const double* v, const double* w, const double* b);
+/* applies the pending pressure correction first; waits for the stream      */
+PS3D_API int ps3d_slab_download(ps3d_slab* s, double* u, double* v, double* w, double* b, double* p);
+PS3D_API int ps3d_slab_phase(ps3d_slab* s, int phase);
+PS3D_API int ps3d_slab_sync(ps3d_slab* s);
+PS3D_API int ps3d_slab_group_step(ps3d_slab* const* ranks, int n, int nsteps);
+
 /* ---- serving loop for optimal-balance requests (no counterpart in the
  * reference) ---------------------------------------------------------------
  * Requests (one diag_opt_balance each, on their own grid and state) are

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libps3d_gpu.so")
-SOURCES = ["stencil.cu", "poisson.cu", "modes.cu", "reduce.cu", "engine.cu", "ensemble.cu", "serve.cu", "noalloc.cu", "layout.cu", "warn.cu", "restart.cu"]
+SOURCES = ["stencil.cu", "poisson.cu", "modes.cu", "reduce.cu", "engine.cu", "ensemble.cu", "serve.cu", "noalloc.cu", "layout.cu", "warn.cu", "restart.cu", "slab.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]

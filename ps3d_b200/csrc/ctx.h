@@ -111,6 +111,12 @@ struct Ctx {
     DevPlan plx8, ply8;         // radix-8 schedules (autotuner alternative)
     DevBuf thomas_r;            // rigid lid: Thomas factors [k][column] (constant for the grid)
     int plane_force = -1;       // PS3D_PLANE_IMPL: -1 free, 0 cluster, 1 rows + y-lines
+    int force_impl = -1;        // set before init: pins the plane implementation (z-slabs: 1)
+    // z-slab of a larger grid (slab.cu): the step kernel advances levels
+    // win_kbeg .. win_kbeg+win_kcount-1 whose global level is k + win_kofs of
+    // win_nzg, and step() stops after it (the slab driver runs the solve)
+    int win_kbeg = 0, win_kcount = 0, win_kofs = 0, win_nzg = 0;
+    bool split_solve = false;
     int kchunk = 8;             // z levels per block of the step kernel
     std::string tuned;          // description of the autotuned choice
     DevBuf twx;

@@ -349,6 +349,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     // kernels cannot take keep the cluster kernels
     if (const char* pi = std::getenv("PS3D_PLANE_IMPL"))
         plane_force = (pi[0] >= '0' && pi[0] <= '2') ? pi[0] - '0' : -1;
+    if (force_impl >= 0) plane_force = force_impl;
     if (plane_force >= 1) {
         choose_split_config(nx, ny, sizeof(double2), pa64, plane_force);
         choose_split_config(nx, ny, sizeof(float2), pa32, plane_force);
@@ -423,6 +424,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
     StepArgs a{};
     a.nx = nx; a.ny = ny; a.nz = nz;
     a.batch = batch; a.sN = N; a.kchunk = kchunk;
+    a.kbeg = win_kbeg; a.kcount = win_kcount; a.kofs = win_kofs; a.nzg = win_nzg;
     a.rigid = rigid; a.nonlinear = P.enable_nonlinear != 0;
     a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz;
     a.dt = P.dt; a.dtw = P.dt / P.dsqr;
@@ -450,6 +452,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         for (int f = 0; f < 4; ++f) { a.wr[f] = (const double*)wr[f].p; a.wi[f] = (const double*)wi[f].p; }
     }
     const bool fused = !bih && !cb && !(bg && harm);
+    if (split_solve && (!fused || wm || bg)) return PS3D_ERR_UNSUPPORTED;   // z-slabs: the fused step, no forcing
     if (!fused) {
         int rc = materialize();
         if (rc) return rc;
@@ -469,6 +472,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         LAUNCH(PS3D_K_STEP, launch_step(a, mixed, stream));
         for (int f = 0; f < 4; ++f) cur[f] = nxt[f];
         pending = false;   // consumed by the step kernel
+        if (split_solve) return PS3D_OK;
     } else {
         if (mixed || batch > 1) return PS3D_ERR_UNSUPPORTED;   // generic path: FP64 tendencies, one grid
         int old[4], B[4], Cb[4];

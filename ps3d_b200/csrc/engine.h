@@ -36,6 +36,10 @@ struct StepArgs {
     // the state arrays hold u'' and the true velocity is u'' - dtp*grad(pc)
     const double* pc;
     double dtp, dtwp;
+    // level window of a z-slab (0: the whole local grid): levels
+    // kbeg .. kbeg+kcount-1 are stepped; the rigid-lid masks see the global
+    // level k + kofs of a grid of nzg levels
+    int kbeg, kcount, kofs, nzg;
 };
 
 // Plane-FFT kernels (divergence + forward 2D FFT, inverse 2D FFT) for one grid.
@@ -67,6 +71,10 @@ struct PlaneArgs {
     int ly;                        // impl 1: lines per CTA of the y-lines passes
     FastDiv fd_n2, fd_ny, fd_tj;   // set by the launchers
     unsigned* err;                 // implementation 2: set to 1 when a bounded wait ran out
+    // level window of a z-slab (0: the whole local grid; implementation 1
+    // only): real-field levels kbeg .. kbeg+kcount-1 map to spectral levels
+    // 0 .. kcount-1; the rigid-lid masks see the global level k + kofs of nzg
+    int kbeg, kcount, kofs, nzg;
 };
 // spectral layout of a plane configuration: 0 [k][ky][kx], 1 [k][kx][ky]
 inline int spectral_layout(const PlaneArgs& a) { return a.impl != 0; }
@@ -89,6 +97,9 @@ struct ColumnArgs {
     // (level 0: c'(1) = c/b(1); level k >= 1: 1/(b(k) - c'(k-1) a)), or NULL
     // to compute them on the fly
     const double* rtab;
+    // column slab (ncl 0: all nxh*ny columns): the array holds ncl columns per
+    // level, global columns col0 .. col0+ncl-1 (one instance)
+    long col0, ncl;
     FastDiv fd_ncols, fd_ny, fd_nxh;   // set by the launchers
 };
 
@@ -102,7 +113,7 @@ cudaError_t launch_forcing_background(const StepArgs& a, cudaStream_t s);
 cudaError_t launch_wavemaker_ab(const StepArgs& a, int do_wm, cudaStream_t s);
 cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int nx, int ny, int nz, int rigid,
                            double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s,
-                           int batch = 1);
+                           int batch = 1, int kbeg = 0, int kcount = 0, int kofs = 0, int nzg = 0);
 
 // poisson.cu
 size_t plane_fwd_smem(const PlaneArgs& a, bool fp32);

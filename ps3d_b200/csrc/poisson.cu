@@ -73,13 +73,14 @@ __device__ __forceinline__ double2 plane_source_pair(const PlaneArgs& a, const d
         vv.y = vv.y - dt * (pn.y - p0.y) * a.rdy;
         vm.x = vm.x - dt * (p0.x - ps.x) * a.rdy;
         vm.y = vm.y - dt * (p0.y - ps.y) * a.rdy;
-        if (a.rigid && k == nz - 1) {
+        const int kg = k + a.kofs, nzg = a.nzg ? a.nzg : nz;   // global level (z-slabs)
+        if (a.rigid && kg == nzg - 1) {
             ww.x = 0.0; ww.y = 0.0;
         } else {
             ww.x = ww.x - dtw * (pu.x - p0.x) * a.rdz;
             ww.y = ww.y - dtw * (pu.y - p0.y) * a.rdz;
         }
-        if (a.rigid && wrap(k - 1, nz) == nz - 1) {
+        if (a.rigid && kg == 0) {   // the level below is the (global) top
             wm.x = 0.0; wm.y = 0.0;
         } else {
             wm.x = wm.x - dtw * (p0.x - pd.x) * a.rdz;
@@ -295,7 +296,7 @@ template <typename R>
 __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a) {
     constexpr int KC = kThomasChunk;
     extern __shared__ double cps[];   // [nz/KC + 1][blockDim.x] checkpoints of c'
-    const long ncols = (long)a.nxh * a.ny;
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
     const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (gid >= 2 * ncols * a.batch) return;
     const int part = (int)(gid & 1);
@@ -305,9 +306,10 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
     R* col = reinterpret_cast<R*>(a.spec) + 2 * ((long)inst * a.sM + c) + part;
     const long ls = 2 * ncols;   // level stride in R
     const int nz = a.nz;
-    const unsigned q0 = fdiv(c, a.layout ? a.fd_ny : a.fd_nxh);
-    const int i = a.layout ? (int)q0 : (int)(c - q0 * (unsigned)a.nxh);
-    const int j = a.layout ? (int)(c - q0 * (unsigned)a.ny) : (int)q0;
+    const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
+    const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
+    const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
+    const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
     const double ks = a.hkx[i] + a.hky[j];
     const double fxa = a.fxa;
     if (ks > 0 && a.rtab) {
@@ -585,8 +587,10 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     const PlanTables<R> tx = stage_plan<R>(a.px, tail);
     const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(n2, sizeof(T)));
     const int jb = blockIdx.x * tj;
-    const int inst = blockIdx.y / nz;
-    const int k = blockIdx.y - inst * nz;
+    const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
+    const int inst = blockIdx.y / kcnt;
+    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    const int k = a.kbeg + kl;                    // real-field level
     const long ioff = (long)inst * a.sN;
     const double* au = a.u + ioff;
     const double* av = a.v + ioff;
@@ -614,7 +618,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
         }
     }
     fft_batch<false, R, MAXR, true>(buf, ld, tj, a.px, -1, tx.tw, tj);   // its first barrier also orders the tables
-    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
+    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kl * nxh * ny;
     for (int t = threadIdx.x; t < tj * (n2 + 1); t += blockDim.x) {
         const int kx = (int)fdiv(t, a.fd_tj), rr = t - kx * tj;
         const int k1 = (kx == n2) ? 0 : kx;
@@ -897,8 +901,10 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
     const int tl = threadIdx.x % N2;
     const int row = threadIdx.x / N2;
     const int jb = blockIdx.x * TJ;
-    const int inst = blockIdx.y / nz;
-    const int k = blockIdx.y - inst * nz;
+    const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
+    const int inst = blockIdx.y / kcnt;
+    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    const int k = a.kbeg + kl;                    // real-field level
     const long ioff = (long)inst * a.sN;
     const double* asrc = a.src ? a.src + ioff : nullptr;
     const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.px.tw : (const void*)a.px.twf);
@@ -948,7 +954,7 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) tb[(tl + N2 * r + N1 * k2) * G::LD + row] = z[r * N2 + k2];
     __syncthreads();
-    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)k * a.nxh * ny + jb;
+    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + jb;
     for (int t = threadIdx.x; t < (N + 1) * TJ; t += G::NT) {
         const int kx = t / TJ, rr = t - kx * TJ;
         const int k1 = (kx == N) ? 0 : kx;
@@ -969,9 +975,11 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
     const int tl = threadIdx.x % N2;
     const int row = threadIdx.x / N2;
     const int jb = blockIdx.x * TJ;
-    const int inst = blockIdx.y / nz;
-    const int k = blockIdx.y - inst * nz;
-    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)k * a.nxh * ny + jb;
+    const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
+    const int inst = blockIdx.y / kcnt;
+    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    const int k = a.kbeg + kl;                    // real-field level
+    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + jb;
     const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.px.tw : (const void*)a.px.twf);
     // c2r pack into the block tile [m][row], loads batched per thread
     constexpr int LB = 4;
@@ -1043,10 +1051,12 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     const PlanTables<R> tx = stage_plan<R>(a.px, tail);
     const T* twx = stage_twx<R>(a, tail + plan_tables_bytes(n2, sizeof(T)));
     const int jb = blockIdx.x * tj;
-    const int inst = blockIdx.y / nz;
-    const int k = blockIdx.y - inst * nz;
+    const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
+    const int inst = blockIdx.y / kcnt;
+    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    const int k = a.kbeg + kl;                    // real-field level
     const long plane = (long)nx * ny;
-    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)k * nxh * ny;
+    const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)kl * nxh * ny;
     double* out = a.out + (long)inst * a.sN;
     __syncthreads();   // twx staged
     constexpr int LB = sizeof(R) == 8 ? 2 : 4;
@@ -1167,7 +1177,7 @@ bool rows_in_registers(int nx, int ny) {
 template <typename R, int N1, int N2>
 static cudaError_t launch_rows_reg_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
     using G = RowReg<N1, N2>;
-    const dim3 g(a.ny / G::TJ, a.nz * std::max(1, a.batch));
+    const dim3 g(a.ny / G::TJ, (a.kcount ? a.kcount : a.nz) * std::max(1, a.batch));
     const size_t sm = G::elems * sizeof(cpx<R>);
     if (fwd) k_rows_fwd_reg<R, N1, N2><<<g, G::NT, sm, s>>>(a);
     else k_rows_inv_reg<R, N1, N2><<<g, G::NT, sm, s>>>(a);
@@ -1193,19 +1203,23 @@ static bool rows_reg(const PlaneArgs& a, bool fwd, cudaStream_t s, cudaError_t* 
 template <typename R, int MX, int MY>
 static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) {
     const int nb = std::max(1, a.batch);
-    const dim3 grows(a.ny / a.tj, a.nz * nb), glines((a.nxh + a.ly - 1) / a.ly, a.nz * nb);
+    const int kcnt = a.kcount ? a.kcount : a.nz;
+    const dim3 grows(a.ny / a.tj, kcnt * nb), glines((a.nxh + a.ly - 1) / a.ly, kcnt * nb);
+    // the y-lines passes see only the spectral array: kcnt levels
+    PlaneArgs ay = a;
+    ay.nz = kcnt; ay.kbeg = 0; ay.kcount = 0;
     const size_t smr = rows_smem(a, sizeof(R) == 4), sml = ylines_smem(a, sizeof(R) == 4);
     cudaError_t e = cudaSuccess;
     if (fwd && a.impl == 2 && a.mode != 2) {
         e = launch_pipe<R, MX>(a, s);
         if (e != cudaSuccess) return e;
-        if (!ylines_reg<R>(a, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
+        if (!ylines_reg<R>(ay, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(ay, -1, a.scale);
     } else if (fwd) {
         if (!rows_reg<R>(a, true, s, &e)) k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
         if (e != cudaSuccess) return e;
-        if (!ylines_reg<R>(a, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, -1, a.scale);
+        if (!ylines_reg<R>(ay, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(ay, -1, a.scale);
     } else {
-        if (!ylines_reg<R>(a, +1, 1.0, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(a, +1, 1.0);
+        if (!ylines_reg<R>(ay, +1, 1.0, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(ay, +1, 1.0);
         if (e != cudaSuccess) return e;
         if (!rows_reg<R>(a, false, s, &e)) k_rows_inv<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
     }
@@ -1316,20 +1330,24 @@ int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd) {
 }
 
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s) {
+    if ((a.kcount || a.kbeg) && a.impl != 1) return cudaErrorInvalidValue;   // level windows: implementation 1 only
     if (a.impl >= 1) return fp32 ? launch_split_t<float>(a, true, s) : launch_split_t<double>(a, true, s);
     return fp32 ? launch_plane_t<float, true>(a, s) : launch_plane_t<double, true>(a, s);
 }
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
+    if ((a.kcount || a.kbeg) && a.impl != 1) return cudaErrorInvalidValue;
     if (a.impl >= 1) return fp32 ? launch_split_t<float>(a, false, s) : launch_split_t<double>(a, false, s);
     return fp32 ? launch_plane_t<float, false>(a, s) : launch_plane_t<double, false>(a, s);
 }
 
 cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     ColumnArgs a = a0;
-    a.fd_ncols = make_fastdiv((unsigned)((long)a.nxh * a.ny));
+    if (a.ncl && (a.rtab || a.batch > 1)) return cudaErrorInvalidValue;   // column slabs: one grid, no table
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;
+    a.fd_ncols = make_fastdiv((unsigned)ncols);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_nxh = make_fastdiv(a.nxh);
-    const long nthreads = 2 * (long)a.nxh * a.ny * std::max(1, a.batch);
+    const long nthreads = 2 * ncols * std::max(1, a.batch);
     const int blocks = (int)((nthreads + kThomasThreads - 1) / kThomasThreads);
     const size_t sm = (size_t)((a.nz + kThomasChunk - 1) / kThomasChunk + 1) * kThomasThreads * sizeof(double);
     if (fp32) k_thomas<float><<<blocks, kThomasThreads, sm, s>>>(a);

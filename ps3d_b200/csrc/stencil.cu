@@ -47,10 +47,12 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
-    const int nzc = (nz + kchunk - 1) / kchunk;
+    const int kcnt = a.kcount ? a.kcount : nz;           // levels stepped (a z-slab's interior)
+    const int kofs = a.kofs, nzg = a.nzg ? a.nzg : nz;   // global level k + kofs of nzg (rigid-lid masks)
+    const int nzc = (kcnt + kchunk - 1) / kchunk;
     const int inst = blockIdx.z / nzc;
-    const int kb = (blockIdx.z - inst * nzc) * kchunk;
-    const int ke = min(nz, kb + kchunk);
+    const int kb = a.kbeg + (blockIdx.z - inst * nzc) * kchunk;
+    const int ke = min(a.kbeg + kcnt, kb + kchunk);
     const long ioff = (long)inst * a.sN;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = (i < nx) && (j < ny);
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
                     const double pt = __ldg(pc + pu + eo[e]);
                     v[0] = v[0] - a.dtp * (pe - p0) * a.rdx;
                     v[1] = v[1] - a.dtp * (pn - p0) * a.rdy;
-                    v[2] = (a.rigid && kw == nz - 1) ? 0.0 : v[2] - a.dtwp * (pt - p0) * a.rdz;
+                    v[2] = (a.rigid && wrap(kw + kofs, nzg) == nzg - 1) ? 0.0 : v[2] - a.dtwp * (pt - p0) * a.rdz;
                 }
 #pragma unroll
                 for (int f = 0; f < NF; ++f) sm.pl[f][slot][t] = v[f];
@@ -131,8 +133,9 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
 #define B(di, dj, dk) SM(3, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
 #define UB(di, dj, dk) SM(4, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
 #define BB(di, dj, dk) SM(5, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-            const bool top = rigid && (k == nz - 1);   // flux_top(nz) = 0
-            const bool bot = rigid && (k == 0);        // flux_top(0)  = 0
+            const int kg = k + kofs;                     // global level
+            const bool top = rigid && (kg == nzg - 1);   // flux_top(nz) = 0
+            const bool bot = rigid && (kg == 0);         // flux_top(0)  = 0
             const long g0 = (long)k * plane + (long)j * nx + i;   // point within the instance
             const long g = g0 + ioff;                              // point within the batch
             double db_, du_, dv_, dw_;
@@ -168,8 +171,8 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
                 // ---- vertical momentum (advection.f90:145-181); rigid lid zeroes
                 //      flux_top(nz-1:nz+2) for w (:167-170)
                 {
-                    const bool wtop = rigid && (k >= nz - 2);
-                    const bool wbot = rigid && (k == 0 || k >= nz - 1);
+                    const bool wtop = rigid && (kg >= nzg - 2);
+                    const bool wbot = rigid && (kg == 0 || kg >= nzg - 1);
                     const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
                     const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
                     const double n = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
@@ -426,18 +429,23 @@ __global__ void k_wavemaker_ab(StepArgs a, int do_wm) {
 // pressure gradient correction, pressure_solver.f90:98-110 (and the rigid-lid
 // ghost levels :82-93, which make the w correction vanish at level nz)
 // ---------------------------------------------------------------------------
+// levels kbeg .. kbeg+kcnt-1 of each instance; the rigid lid is global level
+// nzg-1 with global level k + kofs
 __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                           const double* __restrict__ p, int nx, int ny, int nz, int rigid,
-                          double dt, double dtw, double rdx, double rdy, double rdz, int batch) {
-    const long plane = (long)nx * ny, N = plane * nz, NB = N * batch;
-    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < NB; g += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(g % nx), j = (int)((g / nx) % ny), k = (int)((g / plane) % nz);
+                          double dt, double dtw, double rdx, double rdy, double rdz, int batch,
+                          int kbeg, int kcnt, int kofs, int nzg) {
+    const long plane = (long)nx * ny, N = plane * nz, NW = plane * kcnt, NB = NW * batch;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < NB; q += (long)gridDim.x * blockDim.x) {
+        const long inst = q / NW, r = q - inst * NW;
+        const long g = inst * N + (long)kbeg * plane + r;
+        const int i = (int)(r % nx), j = (int)((r / nx) % ny), k = kbeg + (int)(r / plane);
         const double p0 = p[g];
         const double pe = p[g - i + wrap(i + 1, nx)];
         const double pn = p[g + (long)(wrap(j + 1, ny) - j) * nx];
         u[g] = u[g] - dt * (pe - p0) * rdx;
         v[g] = v[g] - dt * (pn - p0) * rdy;
-        if (rigid && k == nz - 1) {
+        if (rigid && wrap(k + kofs, nzg) == nzg - 1) {
             w[g] = 0.0;
         } else {
             const double pt = p[g + (long)(wrap(k + 1, nz) - k) * plane];
@@ -451,8 +459,9 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double
 // ---------------------------------------------------------------------------
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
 static cudaError_t launch_step_t(const StepArgs& a, cudaStream_t s) {
-    const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, a.nz) : (a.nz <= 16 ? a.nz : 8);
-    dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((a.nz + kchunk - 1) / kchunk) * std::max(1, a.batch));
+    const int kcnt = a.kcount ? a.kcount : a.nz;
+    const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
+    dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((kcnt + kchunk - 1) / kchunk) * std::max(1, a.batch));
     k_step<TT, BY, HARM, WM, BG><<<grid, dim3(kTX, BY), sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s>>>(a, kchunk);
     return cudaGetLastError();
 }
@@ -519,9 +528,12 @@ cudaError_t launch_wavemaker_ab(const StepArgs& a, int do_wm, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_correct(double* u, double* v, double* w, const double* p, int nx, int ny, int nz, int rigid,
-                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s, int batch) {
-    const long N = (long)nx * ny * nz * batch;
-    k_correct<<<grid_for(N, 256), 256, 0, s>>>(u, v, w, p, nx, ny, nz, rigid, dt, dtw, rdx, rdy, rdz, batch);
+                           double dt, double dtw, double rdx, double rdy, double rdz, cudaStream_t s, int batch,
+                           int kbeg, int kcount, int kofs, int nzg) {
+    const int kcnt = kcount ? kcount : nz;
+    const long N = (long)nx * ny * kcnt * batch;
+    k_correct<<<grid_for(N, 256), 256, 0, s>>>(u, v, w, p, nx, ny, nz, rigid, dt, dtw, rdx, rdy, rdz, batch, kbeg, kcnt,
+                                              kofs, nzg ? nzg : nz);
     return cudaGetLastError();
 }
 
