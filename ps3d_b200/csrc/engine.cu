@@ -350,9 +350,13 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     if (const char* pi = std::getenv("PS3D_PLANE_IMPL"))
         plane_force = (pi[0] >= '0' && pi[0] <= '2') ? pi[0] - '0' : -1;
     if (force_impl >= 0) plane_force = force_impl;
-    if (plane_force >= 1) {
-        choose_split_config(nx, ny, sizeof(double2), pa64, plane_force);
-        choose_split_config(nx, ny, sizeof(float2), pa32, plane_force);
+    // default (and untuned) shape: the rows + y-lines passes where the grid
+    // allows them (their register forms beat the cluster kernels at every
+    // size measured), else the cluster kernels
+    const int def_impl = plane_force >= 1 ? plane_force : (plane_force == 0 ? 0 : 1);
+    if (def_impl >= 1) {
+        choose_split_config(nx, ny, sizeof(double2), pa64, def_impl);
+        choose_split_config(nx, ny, sizeof(float2), pa32, def_impl);
     }
     CK(cudaHostAlloc((void**)&kerr_h, 16, cudaHostAllocMapped));
     *kerr_h = 0;
@@ -577,7 +581,7 @@ int Ctx::autotune() {
     const char* env = std::getenv("PS3D_AUTOTUNE");
     const bool pinned = std::getenv("PS3D_TUNE") != nullptr;
     if (env && env[0] == '0' && !pinned) return PS3D_OK;
-    if ((long)N * batch < (1L << 18) && !(env && env[0] == '2') && !pinned) return PS3D_OK;   // small grids: defaults
+    if ((long)N * batch < (1L << 15) && !(env && env[0] == '2') && !pinned) return PS3D_OK;   // tiny grids: defaults
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceProp prop;
