@@ -217,6 +217,8 @@ struct Ctx {
     int diagnose(double* ke, double* pe, double* umax, double* wmax);
     int opt_time_ave(int set, int n_end_ave);
     int opt_balance(const ps3d_optbal& O, double* final_norm, int* iters);
+    int reset_request();      // back to the just-created state (the serving pool reuses contexts)
+    int ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double period, void* graphs);
     int set_forcing(const ps3d_forcing* f);
 
     cudaError_t ensure_spectral4();

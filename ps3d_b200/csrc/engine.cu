@@ -635,7 +635,7 @@ int Ctx::autotune() {
         float best = 1e30f;
         if (fn() != PS3D_OK) return best;
         if (cudaStreamSynchronize(stream) != cudaSuccess) { cudaGetLastError(); return best; }
-        for (int r = 0; r < 3; ++r) {
+        for (int r = 0; r < 5; ++r) {
             cudaEventRecord(e0, stream);
             if (fn() != PS3D_OK) return 1e30f;
             cudaEventRecord(e1, stream);
@@ -688,6 +688,8 @@ int Ctx::autotune() {
             a.harm_uvw = (P.Ah > 0. || P.Av > 0.); a.harm_b = (P.Kh > 0. || P.Kv > 0.);
             a.ab0 = 23.0 / 12.0; a.ab1 = -16.0 / 12.0; a.ab2 = 5.0 / 12.0; a.do_ab = 1;
             a.u = field(0); a.v = field(1); a.w = field(2); a.b = field(3);
+            // every production step loads with the previous step's pending correction
+            a.pc = (const double*)p.p; a.dtp = P.dt; a.dtwp = P.dt / P.dsqr;
             for (int f = 0; f < 4; ++f) {
                 a.t0[f] = (char*)tend[f].p + (size_t)2 * batch * N * tsz(f);
                 a.t1[f] = (const char*)tend[f].p + (size_t)1 * batch * N * tsz(f);
@@ -1015,6 +1017,100 @@ int Ctx::opt_time_ave(int set, int n_end_ave) {
     return PS3D_OK;
 }
 
+// One ramped integration, opt_backward_integration / opt_forward_integration
+// (diag_opt_balance.f90:183-231): n_end steps at itt = 0 with Ro ramped per
+// step.  Every ramp of a balance call repeats the same steps from the same
+// time levels, so the steps are captured once per starting state (buffer
+// phase, pending correction) into a CUDA graph, with each step's Ro in its
+// kernel arguments, and replayed: one launch per ramp instead of several per
+// step, which keeps concurrent serving requests off the launch path.
+struct RampGraph {
+    cudaGraphExec_t exec = nullptr;
+    bool backward = false;
+    int cur_in[4] = {0, 0, 0, 0}, cur_out[4] = {0, 0, 0, 0};
+    bool pend_in = false, pend_out = false;
+    const double* pcor_in = nullptr;
+    const double* pcor_out = nullptr;
+    double dtp_in = 0.0, dtp_out = 0.0;
+    int tau_out = 3, taum1_out = 2, taum2_out = 1;
+    double Ro_out = 0.0;
+    long long nlaunch = 0;
+};
+
+int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double period, void* cache_v) {
+    std::vector<RampGraph>& cache = *static_cast<std::vector<RampGraph>*>(cache_v);
+    auto ro = [&](int s) {
+        const double r = ramp(s * dt_loc / period);
+        return (backward ? 1. - r : r) * Ro_loc;
+    };
+    if (!graphable() || n_end < 3) {
+        int rc = PS3D_OK;
+        for (int s = 0; s <= n_end - 1 && !rc; ++s) {
+            if (cancelled()) return PS3D_ERR_CANCELLED;
+            P.Ro = ro(s);
+            rc = step(itt, tau, taum1, taum2);
+            rotate();
+        }
+        return rc;
+    }
+    RampGraph* g = nullptr;
+    for (RampGraph& c : cache)
+        if (c.backward == backward && std::equal(c.cur_in, c.cur_in + 4, cur) && c.pend_in == pending &&
+            c.pcor_in == pcor && c.dtp_in == dtp)
+            g = &c;
+    if (!g) {
+        RampGraph n;
+        n.backward = backward;
+        std::copy(cur, cur + 4, n.cur_in);
+        n.pend_in = pending; n.pcor_in = pcor; n.dtp_in = dtp;
+        const int itt0 = itt, tau0 = tau, t10 = taum1, t20 = taum2;
+        const long long l0 = launches;
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int rc = PS3D_OK;
+        for (int s = 0; s <= n_end - 1 && !rc; ++s) {
+            P.Ro = ro(s);
+            rc = step(itt, tau, taum1, taum2);
+            rotate();
+        }
+        const cudaError_t e = cudaStreamEndCapture(stream, &graph);
+        std::copy(cur, cur + 4, n.cur_out);
+        n.pend_out = pending; n.pcor_out = pcor; n.dtp_out = dtp;
+        n.tau_out = tau; n.taum1_out = taum1; n.taum2_out = taum2;
+        n.Ro_out = P.Ro;
+        n.nlaunch = launches - l0;
+        // back to the starting state: the replay below performs the steps
+        itt = itt0; tau = tau0; taum1 = t10; taum2 = t20;
+        std::copy(n.cur_in, n.cur_in + 4, cur);
+        pending = n.pend_in; pcor = n.pcor_in; dtp = n.dtp_in;
+        launches = l0;
+        if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+        CK(e);
+        const cudaError_t ie = cudaGraphInstantiate(&n.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(ie);
+        cache.push_back(n);
+        g = &cache.back();
+    }
+    if (cancelled()) return PS3D_ERR_CANCELLED;
+    CK(cudaGraphLaunch(g->exec, stream));
+    std::copy(g->cur_out, g->cur_out + 4, cur);
+    pending = g->pend_out; pcor = g->pcor_out; dtp = g->dtp_out;
+    tau = g->tau_out; taum1 = g->taum1_out; taum2 = g->taum2_out;
+    P.Ro = g->Ro_out;
+    launches += g->nlaunch;
+    return PS3D_OK;
+}
+
+int Ctx::reset_request() {
+    itt = 0; tau = 3; taum1 = 2; taum2 = 1; time = 0.0;
+    pending = false; pcor = nullptr; dtp = 0.0;
+    for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(tend[f].p, 0, tend[f].bytes, stream));
+    CK(cudaMemsetAsync(p.p, 0, p.bytes, stream));
+    invalidate_graph();
+    return PS3D_OK;
+}
+
 int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     if (!(O.period > 0) || O.max_itts < 1 || (O.enable_time_ave && (!(O.average > 0) || O.average_times < 1)))
         return PS3D_ERR_BADPARAM;
@@ -1032,6 +1128,11 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     const int n_end_ave = (int)(O.average / P.dt) + 1;
     double norm_diff = 1.0;
     int rc = PS3D_OK, n_done = 0;
+    std::vector<RampGraph> graphs;   // ramp graphs of this call (ramp_run)
+    struct Release {
+        std::vector<RampGraph>& g;
+        ~Release() { for (RampGraph& r : g) if (r.exec) cudaGraphExecDestroy(r.exec); }
+    } release{graphs};
     if (O.enable_time_ave) {
         for (int m = 1; m <= O.average_times && !rc; ++m) {
             rc = opt_time_ave(PS3D_FIELDS_BASE, n_end_ave);
@@ -1047,12 +1148,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
         P.Ahbi = 0; P.Avbi = 0; P.Khbi = 0; P.Kvbi = 0;
         itt = 0; taum2 = 1; taum1 = 2; tau = 3;
         P.dt = -std::fabs(P.dt);
-        for (int s = 0; s <= n_end - 1 && !rc; ++s) {
-            if (cancelled()) { rc = PS3D_ERR_CANCELLED; break; }
-            P.Ro = (1. - ramp(s * dt_loc / O.period)) * Ro_loc;
-            rc = step(itt, tau, taum1, taum2);
-            rotate();
-        }
+        rc = ramp_run(true, n_end, Ro_loc, dt_loc, O.period, &graphs);
         P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
         if (rc) break;
         if (O.enable_time_ave) {
@@ -1067,12 +1163,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
         // opt_forward_integration (:213-231)
         itt = 0; taum2 = 1; taum1 = 2; tau = 3;
         P.dt = std::fabs(P.dt);
-        for (int s = 0; s <= n_end - 1 && !rc; ++s) {
-            if (cancelled()) { rc = PS3D_ERR_CANCELLED; break; }
-            P.Ro = ramp(s * dt_loc / O.period) * Ro_loc;
-            rc = step(itt, tau, taum1, taum2);
-            rotate();
-        }
+        rc = ramp_run(false, n_end, Ro_loc, dt_loc, O.period, &graphs);
         if (rc) break;
         if (O.enable_time_ave) {
             CK(copy_state_to(kSetSave2));

@@ -9,6 +9,13 @@
 // requests overlap on the GPU while each request's arithmetic stays exactly
 // what it would be alone (no data is shared, reductions are deterministic).
 // Every wait is bounded; nothing here blocks without a limit.
+//
+// A finished request's context is kept idle, still counted in the budget,
+// and handed to the next request with the same parameters after a reset to
+// its just-created state (the request mix repeats grid sizes, and creating
+// and destroying a context per request costs allocations, table uploads and
+// device-synchronising frees that stall the other requests); idle contexts
+// are destroyed, oldest first, when an admission needs their memory.
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -66,8 +73,15 @@ static size_t footprint_of(const ps3d_params& p) {
     return b + (64u << 20);                // tables, plans, reductions, allocator slack
 }
 
+struct IdleCtx {
+    ps3d_params prm;
+    std::unique_ptr<Ctx> ctx;
+    size_t footprint;
+};
+
 struct ps3d_server {
     int device = 0;
+    std::deque<IdleCtx> idle;   // finished requests' contexts, oldest first (counted in `used`)
     size_t budget = 0, used = 0, peak_used = 0;
     int max_active = 1, active = 0, peak_active = 0;
     long long next_id = 1;
@@ -79,13 +93,25 @@ struct ps3d_server {
     std::vector<std::thread> workers;
 
     void worker_loop();
-    void run(Request& r);
+    std::unique_ptr<Ctx> run(Request& r, std::unique_ptr<Ctx> reuse);
 };
 
-void ps3d_server::run(Request& r) {
+static bool same_params(const ps3d_params& a, const ps3d_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+
+// Runs request r on `reuse` (an idle context of the same parameters) or on a
+// new context; returns the context for the idle pool when the request
+// succeeded.
+std::unique_ptr<Ctx> ps3d_server::run(Request& r, std::unique_ptr<Ctx> reuse) {
     cudaSetDevice(device);
-    Ctx c;
-    int rc = c.init(r.prm, device);
+    std::unique_ptr<Ctx> cp = std::move(reuse);
+    int rc = PS3D_OK;
+    if (cp) {
+        rc = cp->reset_request();
+    } else {
+        cp.reset(new Ctx());
+        rc = cp->init(r.prm, device);
+    }
+    Ctx& c = *cp;
     if (!rc) {
         c.cancel_flag = &r.cancel;
         for (int f = 0; f < 4 && !rc; ++f) rc = c.upload_field(c.field(f), r.in[f].data());
@@ -107,39 +133,81 @@ void ps3d_server::run(Request& r) {
             rc = c.download_field(c.field(f), r.out[f].data(), 0);
         }
     }
+    c.cancel_flag = nullptr;
     r.status = rc;
+    if (rc) cp.reset();
+    return cp;
 }
 
 void ps3d_server::worker_loop() {
     for (;;) {
         std::shared_ptr<Request> r;
+        std::unique_ptr<Ctx> reuse;
+        std::vector<std::unique_ptr<Ctx>> evicted;   // destroyed after the lock is released
         {
             std::unique_lock<std::mutex> lk(mu);
             for (;;) {
                 if (stopping) return;
-                // admit the oldest request if a slot and its HBM footprint are free
-                if (!queue.empty() && active < max_active && used + queue.front()->footprint <= budget) {
-                    r = queue.front();
-                    queue.pop_front();
-                    ++active;
-                    used += r->footprint;
-                    peak_used = std::max(peak_used, used);
-                    peak_active = std::max(peak_active, active);
-                    r->state = kRunning;
-                    r->t_start = Clock::now();
-                    break;
+                // admit the oldest request if a slot and its HBM footprint are free:
+                // on an idle context of the same parameters, or after freeing idle ones
+                if (!queue.empty() && active < max_active) {
+                    const std::shared_ptr<Request>& q = queue.front();
+                    long hit = -1;
+                    for (size_t i = 0; i < idle.size() && hit < 0; ++i)
+                        if (same_params(idle[i].prm, q->prm)) hit = (long)i;
+                    bool fits = hit >= 0;
+                    while (!fits && !idle.empty() && used + q->footprint > budget) {   // no hit: free idle ones
+                        evicted.push_back(std::move(idle.front().ctx));
+                        used -= idle.front().footprint;
+                        idle.pop_front();
+                    }
+                    if (!fits) fits = used + q->footprint <= budget;
+                    if (fits) {
+                        r = q;
+                        queue.pop_front();
+                        if (hit >= 0) {
+                            reuse = std::move(idle[hit].ctx);   // its footprint is already counted
+                            idle.erase(idle.begin() + hit);
+                        } else {
+                            used += r->footprint;
+                        }
+                        ++active;
+                        peak_used = std::max(peak_used, used);
+                        peak_active = std::max(peak_active, active);
+                        r->state = kRunning;
+                        r->t_start = Clock::now();
+                        break;
+                    }
                 }
+                if (!evicted.empty()) break;   // free them, then look again
                 cv_work.wait_for(lk, std::chrono::milliseconds(50));
             }
         }
-        run(*r);
+        if (!evicted.empty()) {
+            cudaSetDevice(device);
+            evicted.clear();
+            if (!r) continue;
+        }
+        std::unique_ptr<Ctx> done = run(*r, std::move(reuse));
         {
             std::lock_guard<std::mutex> lk(mu);
             r->t_end = Clock::now();
             r->state = r->status == PS3D_OK ? kDone : (r->status == PS3D_ERR_CANCELLED ? kCancelled : kFailed);
             for (int f = 0; f < 4; ++f) { r->in[f].clear(); r->in[f].shrink_to_fit(); }
             --active;
-            used -= r->footprint;
+            if (done && !stopping) idle.push_back({r->prm, std::move(done), r->footprint});
+            else used -= r->footprint;
+            // keep at most max_active idle contexts
+            while ((int)idle.size() > max_active) {
+                evicted.push_back(std::move(idle.front().ctx));
+                used -= idle.front().footprint;
+                idle.pop_front();
+            }
+        }
+        if (!evicted.empty() || done) {
+            cudaSetDevice(device);
+            evicted.clear();
+            done.reset();   // not kept (server stopping)
         }
         cv_work.notify_all();
         cv_done.notify_all();
@@ -183,6 +251,7 @@ PS3D_API int ps3d_server_destroy(ps3d_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
+    cudaSetDevice(s->device);
     delete s;
     return PS3D_OK;
     SGUARD_END

@@ -39,6 +39,22 @@ def test_result_same_alone_and_in_mix():
     assert st["peak_active"] >= 2
 
 
+def test_reused_context_gives_the_same_result():
+    """A finished request's context serves the next request with the same
+    parameters; the result is bit for bit what a new context gives."""
+    p, opt, f = _req((32, 32, 16))
+    s = Server(max_active=1)
+    first = s.wait(s.submit(p, opt, f))
+    g = {k: v * 1.01 for k, v in f.items()}   # another state on the same grid in between
+    other = s.wait(s.submit(p, opt, g))
+    again = s.wait(s.submit(p, opt, f))
+    s.close()
+    assert first.status == other.status == again.status == 0
+    assert again.norm == first.norm and again.iters == first.iters
+    for n in ("u", "v", "w", "b"):
+        assert np.array_equal(again.fields[n], first.fields[n]), n
+
+
 def test_admission_respects_budget():
     reqs = [_req((64, 64, 16)) for _ in range(4)]
     fp = Server.footprint(reqs[0][0])
