@@ -300,19 +300,22 @@ PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launc
  * of nranks owns global levels k0 = r*nzl .. k0+nzl-1 (nzl = nz/nranks >= 2).
  * A step is the phases below, in this order, each queued on the slab's
  * stream (ps3d_slab_info); between them the caller moves data between ranks:
- *   TENDENCY, PACK_STATE, [halo exchange], UNPACK_STATE, FORWARD,
- *   [all-to-all: xbuf -> colbuf], VSOLVE, [all-to-all: colbuf -> xbuf],
- *   INVERSE, PACK_P, [halo exchange], UNPACK_P, END_STEP.
+ *   TENDENCY, PACK_STATE, [halo exchange], UNPACK_STATE, then `passes` times
+ *   (1 for FP64; 2 for the mixed path, whose second pass is the FP64-residual
+ *   refinement) FORWARD, [all-to-all: xbuf -> colbuf], VSOLVE,
+ *   [all-to-all: colbuf -> xbuf], INVERSE, PACK_P, [halo exchange], UNPACK_P;
+ *   then END_STEP.
  * Halo exchange: hsend holds [planes for the rank below][planes for the rank
  * above] (state: 4 and 4 planes of nx*ny doubles; p: 2 and 1); hrecv receives
  * [what the rank below sent up][what the rank above sent down]; z is
  * periodic over the ranks.  All-to-all: xbuf is [r][nzl][ccnt[r]] complex
- * (blocks for rank r in rank order), colbuf is [nranks][nzl][ccnt[rank]].
+ * (blocks for rank r in rank order), colbuf is [nranks][nzl][ccnt[rank]]
+ * (complex double, or complex float in the mixed path).
  * Before the first step after an upload the state halos are exchanged once
  * (PACK_STATE, exchange, UNPACK_STATE).  ps3d_slab_group_step does all of it
  * for the ranks of one process (device copies; one GPU or several).
  * Upload/download take the rank's interior levels, [nzl][ny][nx] doubles,
- * x fastest (no halos).  Rigid lid, FP64 and the fused step only
+ * x fastest (no halos).  Rigid lid and the fused step only
  * (PS3D_ERR_UNSUPPORTED otherwise).                                        */
 #define PS3D_SLAB_TENDENCY     0
 #define PS3D_SLAB_PACK_STATE   1
@@ -326,7 +329,8 @@ PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launc
 typedef struct ps3d_slab ps3d_slab;
 PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, int device, ps3d_slab** out);
 PS3D_API int ps3d_slab_destroy(ps3d_slab* s);
-PS3D_API int ps3d_slab_info(ps3d_slab* s, int* k0, int* nzl, long long* col0, long long* ncl, void** stream);
+PS3D_API int ps3d_slab_info(ps3d_slab* s, int* k0, int* nzl, long long* col0, long long* ncl, void** stream,
+                             int* passes);
 /* sizes of the exchange buffers and every rank's column count (nranks entries) */
 PS3D_API int ps3d_slab_buffers(ps3d_slab* s, size_t* xbytes, size_t* colbytes, size_t* hbytes,
                                long long* col_counts);

@@ -22,12 +22,17 @@
 //   p halo      p one level below and two above (the step kernel's lazy
 //               correction reads p at the plane it loads and the one above)
 //
+// The mixed path (FP32 transforms) runs forward .. p halo twice per step:
+// the second pass solves for the divergence of u - dt grad p in FP64 (the
+// FP64-residual refinement, pressure_solve in engine.cu) and adds its
+// pressure to p.
+//
 // Local arrays hold nzl + 3 levels: halo 0, interior 1 .. nzl, halos nzl+1
 // and nzl+2 (the second only for p).  The transport between ranks is the
 // caller's: NCCL all-to-all and send/receive between processes (the Python
 // driver, ps3d_b200/slab.py), or ps3d_slab_group_step for contexts in one
-// process, which copies device to device.  Supported: rigid lid, FP64, the
-// fused step (Laplacian friction, no biharmonic, no forcing).
+// process, which copies device to device.  Supported: rigid lid, FP64 and
+// mixed, the fused step (Laplacian friction, no biharmonic, no forcing).
 #include <cstring>
 #include <memory>
 #include <new>
@@ -48,9 +53,13 @@ struct ps3d_slab {
     void* hsend = nullptr;          // halo planes to send: [down][up]
     void* hrecv = nullptr;          // halo planes received: [from below][from above]
     bool need_halo = true;          // state halos not yet exchanged (after an upload)
+    bool mixed = false;             // FP32 spectra, two solve passes per step
+    int pass = 0;                   // solve pass of the current step (0, then 1 in the mixed path)
 
-    size_t xbytes() const { return (size_t)nzl * ncols * sizeof(double2); }
-    size_t colbytes() const { return (size_t)nzg * ccnt[rank] * sizeof(double2); }
+    int passes() const { return mixed ? 2 : 1; }
+    size_t es() const { return mixed ? sizeof(float2) : sizeof(double2); }
+    size_t xbytes() const { return (size_t)nzl * ncols * es(); }
+    size_t colbytes() const { return (size_t)nzg * ccnt[rank] * es(); }
     size_t hbytes() const { return (size_t)8 * plane * sizeof(double); }
     double* lvl(double* f, int L) const { return f + (size_t)L * plane; }
 };
@@ -62,6 +71,7 @@ constexpr int kDown[2] = {4, 2}, kUp[2] = {4, 1};
 
 int slab_tendency(ps3d_slab* s) {
     Ctx& c = *s->ctx;
+    s->pass = 0;
     return c.step(c.itt, c.tau, c.taum1, c.taum2);
 }
 
@@ -112,15 +122,18 @@ ps3d::PlaneArgs window(ps3d_slab* s, const ps3d::PlaneArgs& base) {
 
 int slab_forward(ps3d_slab* s) {
     Ctx& c = *s->ctx;
-    ps3d::PlaneArgs a = window(s, c.pa64);
-    a.mode = 0;
+    ps3d::PlaneArgs a = window(s, s->mixed ? c.pa32 : c.pa64);
+    // pass 1 (mixed): the divergence of u - dt grad p, p from pass 0 with its halos
+    a.mode = s->pass ? 2 : 0;
     a.u = c.field(0); a.v = c.field(1); a.w = c.field(2);
-    a.pc = nullptr; a.rigid = 1;
+    a.pc = s->pass ? (const double*)c.p.p : nullptr;
+    a.dtp = c.P.dt; a.dtwp = c.P.dt / c.P.dsqr;
+    a.rigid = 1;
     a.rdt = 1.0 / c.P.dt;
     a.scale = c.P.dx * c.P.dy;
     a.spec = c.FS.p;
-    CK(ps3d::launch_plane_fwd(a, false, c.stream));
-    const size_t es = sizeof(double2);
+    CK(ps3d::launch_plane_fwd(a, s->mixed, c.stream));
+    const size_t es = s->es();
     for (int r = 0; r < s->nranks; ++r)
         CK(cudaMemcpy2DAsync((char*)s->xbuf + (size_t)s->nzl * s->cbeg[r] * es, s->ccnt[r] * es,
                              (const char*)c.FS.p + s->cbeg[r] * es, s->ncols * es, s->ccnt[r] * es, s->nzl,
@@ -134,32 +147,34 @@ int slab_vsolve(ps3d_slab* s) {
     a.nx = c.nx; a.ny = c.ny; a.nz = s->nzg; a.nxh = c.nxh;
     a.spec = s->colbuf;
     a.batch = 1; a.sM = (long)s->nzg * s->ccnt[s->rank];
-    a.layout = ps3d::spectral_layout(c.pa64);
+    a.layout = ps3d::spectral_layout(s->mixed ? c.pa32 : c.pa64);
     a.hkx = (const double*)c.t_hkx.p; a.hky = (const double*)c.t_hky.p;
     a.fxa = 1.0 / (c.P.dz * c.P.dz) / c.P.dsqr;
     a.dz2dsqr = c.P.dz * c.P.dz * c.P.dsqr;
-    a.rtab = nullptr;
+    a.rtab = nullptr;   // factors formed on the fly (FP64) for both storage precisions
     a.col0 = s->cbeg[s->rank]; a.ncl = s->ccnt[s->rank];
-    CK(ps3d::launch_thomas(a, false, c.stream));
+    CK(ps3d::launch_thomas(a, s->mixed, c.stream));
     return PS3D_OK;
 }
 
 int slab_inverse(ps3d_slab* s) {
     Ctx& c = *s->ctx;
-    const size_t es = sizeof(double2);
+    const size_t es = s->es();
     for (int r = 0; r < s->nranks; ++r)
         CK(cudaMemcpy2DAsync((char*)c.FS.p + s->cbeg[r] * es, s->ncols * es,
                              (const char*)s->xbuf + (size_t)s->nzl * s->cbeg[r] * es, s->ccnt[r] * es,
                              s->ccnt[r] * es, s->nzl, cudaMemcpyDeviceToDevice, c.stream));
-    ps3d::PlaneArgs b = window(s, c.pa64);
+    ps3d::PlaneArgs b = window(s, s->mixed ? c.pa32 : c.pa64);
     b.spec = c.FS.p;
     b.out = (double*)c.p.p;
-    b.beta = 0.0;
+    b.beta = s->pass ? 1.0 : 0.0;   // the refinement pass adds its pressure
     b.scale = 1.0 / (c.P.Lx * c.P.Ly);
-    CK(ps3d::launch_plane_inv(b, false, c.stream));
-    c.pending = true;
-    c.pcor = (const double*)c.p.p;
-    c.dtp = c.P.dt;
+    CK(ps3d::launch_plane_inv(b, s->mixed, c.stream));
+    if (++s->pass >= s->passes()) {
+        c.pending = true;
+        c.pcor = (const double*)c.p.p;
+        c.dtp = c.P.dt;
+    }
     return PS3D_OK;
 }
 
@@ -201,7 +216,7 @@ int transport_halo(ps3d_slab* const* r, int n, int which) {
 int transport_columns(ps3d_slab* const* r, int n, bool forward) {
     int rc = sync_all(r, n);
     if (rc) return rc;
-    const size_t es = sizeof(double2);
+    const size_t es = r[0]->es();
     for (int d = 0; d < n; ++d) {
         cudaSetDevice(r[d]->ctx->device);
         for (int q = 0; q < n; ++q) {
@@ -248,12 +263,14 @@ int group_step(ps3d_slab* const* r, int n) {
     if (r[0]->need_halo && (rc = group_halo(r, n, 0))) return rc;
     FOR_RANKS(slab_tendency(r[q]))
     if ((rc = group_halo(r, n, 0))) return rc;
-    FOR_RANKS(slab_forward(r[q]))
-    if ((rc = transport_columns(r, n, true))) return rc;
-    FOR_RANKS(slab_vsolve(r[q]))
-    if ((rc = transport_columns(r, n, false))) return rc;
-    FOR_RANKS(slab_inverse(r[q]))
-    if ((rc = group_halo(r, n, 1))) return rc;
+    for (int pass = 0; pass < r[0]->passes(); ++pass) {
+        FOR_RANKS(slab_forward(r[q]))
+        if ((rc = transport_columns(r, n, true))) return rc;
+        FOR_RANKS(slab_vsolve(r[q]))
+        if ((rc = transport_columns(r, n, false))) return rc;
+        FOR_RANKS(slab_inverse(r[q]))
+        if ((rc = group_halo(r, n, 1))) return rc;
+    }
     FOR_RANKS(slab_end_step(r[q]))
     return PS3D_OK;
 }
@@ -272,10 +289,11 @@ PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, i
     SGUARD_BEGIN
     if (!global || !out || nranks < 1 || rank < 0 || rank >= nranks) return PS3D_ERR_BADPARAM;
     *out = nullptr;
-    if (!global->enable_vertical_boundaries || global->precision != PS3D_FP64) return PS3D_ERR_UNSUPPORTED;
+    if (!global->enable_vertical_boundaries) return PS3D_ERR_UNSUPPORTED;
     if (global->nz % nranks || global->nz / nranks < 2) return PS3D_ERR_BADPARAM;
     std::unique_ptr<ps3d_slab> s(new ps3d_slab());
     s->nranks = nranks; s->rank = rank;
+    s->mixed = global->precision == PS3D_MIXED;
     s->nzg = global->nz; s->nzl = global->nz / nranks; s->k0 = rank * s->nzl;
     ps3d_params lp = *global;
     lp.nz = s->nzl + 3;
@@ -287,7 +305,7 @@ PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, i
     c.win_kbeg = 1; c.win_kcount = s->nzl; c.win_kofs = s->k0 - 1; c.win_nzg = s->nzg;
     int rc = c.init(lp, device);
     if (rc) return rc;
-    if (c.pa64.impl != 1) return PS3D_ERR_UNSUPPORTED;   // grid the rows + y-lines kernels cannot take
+    if ((s->mixed ? c.pa32 : c.pa64).impl != 1) return PS3D_ERR_UNSUPPORTED;   // grid the rows + y-lines kernels cannot take
     c.use_graphs = false;
     s->ncols = (long)c.nxh * c.ny;
     s->plane = (long)c.nx * c.ny;
@@ -315,8 +333,10 @@ PS3D_API int ps3d_slab_destroy(ps3d_slab* s) {
     SGUARD_END
 }
 
-PS3D_API int ps3d_slab_info(ps3d_slab* s, int* k0, int* nzl, long long* col0, long long* ncl, void** stream) {
+PS3D_API int ps3d_slab_info(ps3d_slab* s, int* k0, int* nzl, long long* col0, long long* ncl, void** stream,
+                             int* passes) {
     if (!s) return PS3D_ERR_BADPARAM;
+    if (passes) *passes = s->passes();
     if (k0) *k0 = s->k0;
     if (nzl) *nzl = s->nzl;
     if (col0) *col0 = s->cbeg[s->rank];

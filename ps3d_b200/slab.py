@@ -39,7 +39,7 @@ def _lib():
     L.ps3d_slab_create.argtypes = [C.POINTER(Params), C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
     L.ps3d_slab_destroy.argtypes = [vp]
     L.ps3d_slab_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong),
-                                 C.POINTER(C.c_longlong), C.POINTER(vp)]
+                                 C.POINTER(C.c_longlong), C.POINTER(vp), C.POINTER(C.c_int)]
     L.ps3d_slab_buffers.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                     C.POINTER(C.c_longlong)]
     L.ps3d_slab_bind.argtypes = [vp, vp, vp, vp, vp]
@@ -66,10 +66,11 @@ class Slab:
         h = C.c_void_p()
         _check(self.L.ps3d_slab_create(C.byref(self.params), nranks, rank, device, C.byref(h)), "ps3d_slab_create")
         self.h = h
-        k0, nzl, col0, ncl, st = C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong(), C.c_void_p()
-        _check(self.L.ps3d_slab_info(h, C.byref(k0), C.byref(nzl), C.byref(col0), C.byref(ncl), C.byref(st)),
-               "ps3d_slab_info")
+        k0, nzl, col0, ncl, st, ps = C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong(), C.c_void_p(), C.c_int()
+        _check(self.L.ps3d_slab_info(h, C.byref(k0), C.byref(nzl), C.byref(col0), C.byref(ncl), C.byref(st),
+                                     C.byref(ps)), "ps3d_slab_info")
         self.k0, self.nzl, self.col0, self.ncl, self.stream = k0.value, nzl.value, col0.value, ncl.value, st.value
+        self.passes = ps.value   # solve passes per step: 2 in the mixed path (refinement)
         xb, cb, hb = C.c_size_t(), C.c_size_t(), C.c_size_t()
         counts = (C.c_longlong * nranks)()
         _check(self.L.ps3d_slab_buffers(h, C.byref(xb), C.byref(cb), C.byref(hb), counts), "ps3d_slab_buffers")
@@ -193,8 +194,11 @@ class DistSlab:
         self.slab = Slab(params, self.nranks, self.rank, device)
         dev = torch.device("cuda", device)
         f8 = torch.float64
-        self.xbuf = torch.empty(self.slab.xbytes // 8, dtype=f8, device=dev)
-        self.colbuf = torch.empty(self.slab.colbytes // 8, dtype=f8, device=dev)
+        # spectra: complex double, or complex float in the mixed path
+        fs = torch.float32 if self.slab.passes == 2 else torch.float64
+        esz = 4 if fs == torch.float32 else 8
+        self.xbuf = torch.empty(self.slab.xbytes // esz, dtype=fs, device=dev)
+        self.colbuf = torch.empty(self.slab.colbytes // esz, dtype=fs, device=dev)
         self.hsend = torch.empty(self.slab.hbytes // 8, dtype=f8, device=dev)
         self.hrecv = torch.empty(self.slab.hbytes // 8, dtype=f8, device=dev)
         torch.cuda.synchronize(dev)
@@ -222,14 +226,15 @@ class DistSlab:
                 self.need_halo = False
             s.phase("tendency")
             self._halo(0)
-            s.phase("forward")
-            with self.torch.cuda.stream(self.stream):
-                columns_forward(self.xbuf, self.colbuf, counts, nzl, self.rank, self.group)
-            s.phase("vsolve")
-            with self.torch.cuda.stream(self.stream):
-                columns_backward(self.xbuf, self.colbuf, counts, nzl, self.rank, self.group)
-            s.phase("inverse")
-            self._halo(1)
+            for _ in range(s.passes):
+                s.phase("forward")
+                with self.torch.cuda.stream(self.stream):
+                    columns_forward(self.xbuf, self.colbuf, counts, nzl, self.rank, self.group)
+                s.phase("vsolve")
+                with self.torch.cuda.stream(self.stream):
+                    columns_backward(self.xbuf, self.colbuf, counts, nzl, self.rank, self.group)
+                s.phase("inverse")
+                self._halo(1)
             s.phase("end_step")
 
     def download(self):
