@@ -292,9 +292,11 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
 constexpr int kThomasChunk = 8;
 constexpr int kThomasThreads = 128;
 
-template <typename R>
+template <typename R, bool FULL>
 __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a) {
     constexpr int KC = kThomasChunk;
+    // FULL: nz is a multiple of KC, so only the chunk ends need tests
+#define IN(cond) (FULL || (cond))
     extern __shared__ double cps[];   // [nz/KC + 1][blockDim.x] checkpoints of c'
     const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
     const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -321,7 +323,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
         double rn[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (q < nz) { nxt[q] = col[(long)q * ls]; rn[q] = __ldg(rt + (long)q * ncols); }
+            if (IN(q < nz)) { nxt[q] = col[(long)q * ls]; rn[q] = __ldg(rt + (long)q * ncols); }
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
             double r[KC];
@@ -329,14 +331,14 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             for (int q = 0; q < KC; ++q) { d[q] = nxt[q]; r[q] = rn[q]; }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + KC + q < nz) {
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) {
                     nxt[q] = col[(long)(kb + KC + q) * ls];
                     rn[q] = __ldg(rt + (long)(kb + KC + q) * ncols);
                 }
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
-                if (k < nz) {
+                if (IN(k < nz)) {
                     if (k == 0) dp = (double)d[q] / bend;               // dp(1) = d(1)/b(1)
                     else dp = ((double)d[q] - dp * fxa) * r[q];
                     d[q] = (R)dp;
@@ -344,13 +346,13 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + q < nz) col[(long)(kb + q) * ls] = d[q];
+                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
         }
         double x = dp;   // x(nz) = dp(nz)
         const int last = (nz - 1) / KC;
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (last * KC + q < nz - 1) { nxt[q] = col[(long)(last * KC + q) * ls]; rn[q] = __ldg(rt + (long)(last * KC + q) * ncols); }
+            if (FULL ? (q < KC - 1) : (last * KC + q < nz - 1)) { nxt[q] = col[(long)(last * KC + q) * ls]; rn[q] = __ldg(rt + (long)(last * KC + q) * ncols); }
         for (int sg = last; sg >= 0; --sg) {
             const int kb = sg * KC;
             R d[KC];
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + q < nz - 1) col[(long)(kb + q) * ls] = d[q];
+                if (FULL ? !(sg == last && q == KC - 1) : (kb + q < nz - 1)) col[(long)(kb + q) * ls] = d[q];
         }
     } else if (ks > 0) {
         const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
@@ -382,18 +384,18 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
         R nxt[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (q < nz) nxt[q] = col[(long)q * ls];
+            if (IN(q < nz)) nxt[q] = col[(long)q * ls];
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
 #pragma unroll
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + KC + q < nz) nxt[q] = col[(long)(kb + KC + q) * ls];
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = col[(long)(kb + KC + q) * ls];
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
-                if (k < nz) {
+                if (IN(k < nz)) {
                     const double bk = (k == 0 || k == nz - 1) ? bend : bmid;
                     if (k == 0) {
                         cp = fxa / bk;                   // cp(1) = c(1)/b(1)
@@ -409,13 +411,13 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + q < nz) col[(long)(kb + q) * ls] = d[q];
+                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
         }
         double x = dp;   // x(nz) = dp(nz)
         const int last = (nz - 1) / KC;
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (last * KC + q < nz - 1) nxt[q] = col[(long)(last * KC + q) * ls];
+            if (FULL ? (q < KC - 1) : (last * KC + q < nz - 1)) nxt[q] = col[(long)(last * KC + q) * ls];
         for (int sg = last; sg >= 0; --sg) {
             const int kb = sg * KC;
             R d[KC];
@@ -430,7 +432,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
 #pragma unroll
             for (int q = 1; q < KC; ++q) {
                 const int k = kb + q;
-                if (k < nz) {
+                if (IN(k < nz)) {
                     const double bk = (k == nz - 1) ? bend : bmid;
                     cpl[q] = fxa * __drcp_rn(bk - cpl[q - 1] * fxa);
                 } else {
@@ -439,13 +441,13 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = KC - 1; q >= 0; --q) {
-                if (kb + q >= nz - 1) continue;
+                if (FULL ? (sg == last && q == KC - 1) : (kb + q >= nz - 1)) continue;
                 x = (double)d[q] - cpl[q] * x;
                 d[q] = (R)x;
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + q < nz - 1) col[(long)(kb + q) * ls] = d[q];
+                if (FULL ? !(sg == last && q == KC - 1) : (kb + q < nz - 1)) col[(long)(kb + q) * ls] = d[q];
         }
     } else {
         // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr,
@@ -455,18 +457,18 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
         R nxt[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (q < nz) nxt[q] = col[(long)q * ls];
+            if (IN(q < nz)) nxt[q] = col[(long)q * ls];
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
 #pragma unroll
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + KC + q < nz) nxt[q] = col[(long)(kb + KC + q) * ls];
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = col[(long)(kb + KC + q) * ls];
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
-                if (k < nz) {
+                if (IN(k < nz)) {
                     const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
                     fprev = (double)d[q];
                     x0 = x1; x1 = xk;
@@ -475,10 +477,11 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + q < nz) col[(long)(kb + q) * ls] = d[q];
+                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
         }
     }
 }
+#undef IN
 
 // Thomas factors of every column with ks > 0, built once per grid with the
 // arithmetic of the recurrence in k_thomas: level 0 holds c'(1) = c/b(1),
@@ -1350,8 +1353,13 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     const long nthreads = 2 * ncols * std::max(1, a.batch);
     const int blocks = (int)((nthreads + kThomasThreads - 1) / kThomasThreads);
     const size_t sm = (size_t)((a.nz + kThomasChunk - 1) / kThomasChunk + 1) * kThomasThreads * sizeof(double);
-    if (fp32) k_thomas<float><<<blocks, kThomasThreads, sm, s>>>(a);
-    else k_thomas<double><<<blocks, kThomasThreads, sm, s>>>(a);
+    if (a.nz % kThomasChunk == 0) {
+        if (fp32) k_thomas<float, true><<<blocks, kThomasThreads, sm, s>>>(a);
+        else k_thomas<double, true><<<blocks, kThomasThreads, sm, s>>>(a);
+    } else {
+        if (fp32) k_thomas<float, false><<<blocks, kThomasThreads, sm, s>>>(a);
+        else k_thomas<double, false><<<blocks, kThomasThreads, sm, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
