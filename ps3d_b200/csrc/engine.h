@@ -40,6 +40,8 @@ struct StepArgs {
     // kbeg .. kbeg+kcount-1 are stepped; the rigid-lid masks see the global
     // level k + kofs of a grid of nzg levels
     int kbeg, kcount, kofs, nzg;
+    // 0.5/dx, 0.5/dy, 0.5/dz, 0.25/dx, 0.25/dy, 0.25/dz, 0.25 f0, 0.5 N0^2 (set by launch_step)
+    double hdx, hdy, hdz, qdx, qdy, qdz, qf0, hN0sq;
 };
 
 // Plane-FFT kernels (divergence + forward 2D FFT, inverse 2D FFT) for one grid.

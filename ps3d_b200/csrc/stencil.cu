@@ -140,54 +140,60 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
             const long g = g0 + ioff;                              // point within the batch
             double db_, du_, dv_, dw_;
             // ---- buoyancy advection + N^2 (advection.f90:12-47, integrate.f90:21-23)
+            // The reference's 0.5 and 0.25 flux factors are powers of two: they
+            // are carried in the per-axis factors a.hd* = 0.5/d*, a.qd* = 0.25/d*
+            // (and 0.25 f0, 0.5 N0^2, set by the launcher), a multiply saved per
+            // flux.  Scaling by a power of two rounds exactly; the results move
+            // at round-off level only where the compiler now contracts a flux
+            // product into the difference that follows (FMA).
             if (a.nonlinear) {
-                const double fe = 0.5 * (B(0, 0, 0) + B(1, 0, 0)) * U(0, 0, 0);
-                const double fem = 0.5 * (B(-1, 0, 0) + B(0, 0, 0)) * U(-1, 0, 0);
-                const double fn = 0.5 * (B(0, 0, 0) + B(0, 1, 0)) * V(0, 0, 0);
-                const double fnm = 0.5 * (B(0, -1, 0) + B(0, 0, 0)) * V(0, -1, 0);
-                const double ft = top ? 0.0 : 0.5 * (B(0, 0, 0) + B(0, 0, 1)) * W(0, 0, 0);
-                const double ftm = bot ? 0.0 : 0.5 * (B(0, 0, -1) + B(0, 0, 0)) * W(0, 0, -1);
-                db_ = -Ro * ((fe - fem) * rdx + (fn - fnm) * rdy + (ft - ftm) * rdz);
+                const double fe = (B(0, 0, 0) + B(1, 0, 0)) * U(0, 0, 0);
+                const double fem = (B(-1, 0, 0) + B(0, 0, 0)) * U(-1, 0, 0);
+                const double fn = (B(0, 0, 0) + B(0, 1, 0)) * V(0, 0, 0);
+                const double fnm = (B(0, -1, 0) + B(0, 0, 0)) * V(0, -1, 0);
+                const double ft = top ? 0.0 : (B(0, 0, 0) + B(0, 0, 1)) * W(0, 0, 0);
+                const double ftm = bot ? 0.0 : (B(0, 0, -1) + B(0, 0, 0)) * W(0, 0, -1);
+                db_ = -Ro * ((fe - fem) * a.hdx + (fn - fnm) * a.hdy + (ft - ftm) * a.hdz);
                 // ---- zonal momentum (advection.f90:65-100)
                 {
-                    const double e = 0.25 * (U(0, 0, 0) + U(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
-                    const double em = 0.25 * (U(-1, 0, 0) + U(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
-                    const double n = 0.25 * (U(0, 0, 0) + U(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
-                    const double nm = 0.25 * (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : 0.25 * (U(0, 0, 1) + U(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
-                    const double tm = bot ? 0.0 : 0.25 * (U(0, 0, 0) + U(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
-                    du_ = -Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                    const double e = (U(0, 0, 0) + U(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+                    const double em = (U(-1, 0, 0) + U(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
+                    const double n = (U(0, 0, 0) + U(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+                    const double nm = (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+                    const double t = top ? 0.0 : (U(0, 0, 1) + U(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
+                    const double tm = bot ? 0.0 : (U(0, 0, 0) + U(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
+                    du_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
                 }
                 // ---- meridional momentum (advection.f90:104-140)
                 {
-                    const double e = 0.25 * (V(0, 0, 0) + V(1, 0, 0)) * (U(0, 1, 0) + U(0, 0, 0));
-                    const double em = 0.25 * (V(-1, 0, 0) + V(0, 0, 0)) * (U(-1, 1, 0) + U(-1, 0, 0));
-                    const double n = 0.25 * (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 1, 0) + V(0, 0, 0));
-                    const double nm = 0.25 * (V(0, -1, 0) + V(0, 0, 0)) * (V(0, 0, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : 0.25 * (V(0, 0, 1) + V(0, 0, 0)) * (W(0, 0, 0) + W(0, 1, 0));
-                    const double tm = bot ? 0.0 : 0.25 * (V(0, 0, 0) + V(0, 0, -1)) * (W(0, 0, -1) + W(0, 1, -1));
-                    dv_ = -Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                    const double e = (V(0, 0, 0) + V(1, 0, 0)) * (U(0, 1, 0) + U(0, 0, 0));
+                    const double em = (V(-1, 0, 0) + V(0, 0, 0)) * (U(-1, 1, 0) + U(-1, 0, 0));
+                    const double n = (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 1, 0) + V(0, 0, 0));
+                    const double nm = (V(0, -1, 0) + V(0, 0, 0)) * (V(0, 0, 0) + V(0, -1, 0));
+                    const double t = top ? 0.0 : (V(0, 0, 1) + V(0, 0, 0)) * (W(0, 0, 0) + W(0, 1, 0));
+                    const double tm = bot ? 0.0 : (V(0, 0, 0) + V(0, 0, -1)) * (W(0, 0, -1) + W(0, 1, -1));
+                    dv_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
                 }
                 // ---- vertical momentum (advection.f90:145-181); rigid lid zeroes
                 //      flux_top(nz-1:nz+2) for w (:167-170)
                 {
                     const bool wtop = rigid && (kg >= nzg - 2);
                     const bool wbot = rigid && (kg == 0 || kg >= nzg - 1);
-                    const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
-                    const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
-                    const double n = 0.25 * (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
-                    const double nm = 0.25 * (W(0, -1, 0) + W(0, 0, 0)) * (V(0, -1, 0) + V(0, -1, 1));
-                    const double t = wtop ? 0.0 : 0.25 * (W(0, 0, 1) + W(0, 0, 0)) * (W(0, 0, 0) + W(0, 0, 1));
-                    const double tm = wbot ? 0.0 : 0.25 * (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, -1) + W(0, 0, 0));
-                    dw_ = -a.dsqr * Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+                    const double e = (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
+                    const double em = (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
+                    const double n = (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
+                    const double nm = (W(0, -1, 0) + W(0, 0, 0)) * (V(0, -1, 0) + V(0, -1, 1));
+                    const double t = wtop ? 0.0 : (W(0, 0, 1) + W(0, 0, 0)) * (W(0, 0, 0) + W(0, 0, 1));
+                    const double tm = wbot ? 0.0 : (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, -1) + W(0, 0, 0));
+                    dw_ = -a.dsqr * Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
                 }
             } else {
                 db_ = du_ = dv_ = dw_ = 0.0;
             }
-            db_ = db_ - 0.5 * (W(0, 0, 0) + W(0, 0, -1)) * a.N0sq;
+            db_ = db_ - (W(0, 0, 0) + W(0, 0, -1)) * a.hN0sq;
             // ---- Coriolis, buoyancy force, rigid-lid mask (integrate.f90:37-54)
-            du_ = du_ + (V(0, 0, 0) + V(0, -1, 0) + V(1, 0, 0) + V(1, -1, 0)) * 0.25 * a.f0;
-            dv_ = dv_ - (U(-1, 0, 0) + U(0, 0, 0) + U(-1, 1, 0) + U(0, 1, 0)) * 0.25 * a.f0;
+            du_ = du_ + (V(0, 0, 0) + V(0, -1, 0) + V(1, 0, 0) + V(1, -1, 0)) * a.qf0;
+            dv_ = dv_ - (U(-1, 0, 0) + U(0, 0, 0) + U(-1, 1, 0) + U(0, 1, 0)) * a.qf0;
             dw_ = dw_ + 0.5 * (B(0, 0, 0) + B(0, 0, 1));
             if (top) dw_ = 0.0;
             // ---- friction, in place before AB (integrate.f90:59-66)
@@ -458,7 +464,11 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double
 // launchers
 // ---------------------------------------------------------------------------
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
-static cudaError_t launch_step_t(const StepArgs& a, cudaStream_t s) {
+static cudaError_t launch_step_t(const StepArgs& a0, cudaStream_t s) {
+    StepArgs a = a0;
+    a.hdx = 0.5 * a.rdx; a.hdy = 0.5 * a.rdy; a.hdz = 0.5 * a.rdz;
+    a.qdx = 0.25 * a.rdx; a.qdy = 0.25 * a.rdy; a.qdz = 0.25 * a.rdz;
+    a.qf0 = 0.25 * a.f0; a.hN0sq = 0.5 * a.N0sq;
     const int kcnt = a.kcount ? a.kcount : a.nz;
     const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
     dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((kcnt + kchunk - 1) / kchunk) * std::max(1, a.batch));
