@@ -45,8 +45,8 @@ def set_grid(nx, ny, nz):
 # traffic already streams far beyond L2, so it scales with the grid points;
 # commands and tables in profiles/hot_kernels_{fp64,mixed}_256x256x64.md.
 MEASURED_TRAFFIC_PER_POINT = {
-    "fp64": {"step": 166.9},
-    "mixed": {"step": 127.6},
+    "fp64": {"step": 165.8},
+    "mixed": {"step": 128.4},
 }
 
 # algorithmic HBM bytes per grid point per launch.  The step kernel reads
