@@ -80,6 +80,17 @@ __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) { return 
 // ---------------------------------------------------------------------------
 PS3D_HD int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch (sm_90+): a kernel launched with
+// launch_pdl lets the next kernel of the stream be scheduled once all of its
+// own blocks are resident (pdl_trigger at block start), so the successor's
+// launch and prologue overlap this kernel's tail; every such kernel calls
+// pdl_wait before it reads anything an earlier kernel wrote (it returns when
+// the preceding grids have completed and their memory is visible).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // status flags written by kernels (bit mask, OR-ed)
 enum : unsigned {
     kFlagNonFinite = 1u,

@@ -7,6 +7,24 @@
 
 namespace ps3d {
 
+// Launch with programmatic stream serialization (see pdl_trigger/pdl_wait):
+// only for kernels that call pdl_wait before reading their inputs.
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<A&&>(args)...);
+}
+
 // Arguments of one time step for one grid (K1 and the generic-path kernels).
 // Tendency slots are untyped: FP64 in the plain path, FP32 in the mixed path.
 struct StepArgs {

@@ -294,6 +294,8 @@ constexpr int kThomasThreads = 128;
 
 template <typename R, bool FULL>
 __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     constexpr int KC = kThomasChunk;
     // FULL: nz is a multiple of KC, so only the chunk ends need tests
 #define IN(cond) (FULL || (cond))
@@ -581,6 +583,8 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
 // ---------------------------------------------------------------------------
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_fwd(const PlaneArgs a) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
@@ -760,6 +764,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_rows_fwd_pipe(const PlaneA
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_ylines(const PlaneArgs a, int sign,
                                                                                   double scale) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
@@ -822,6 +828,8 @@ struct YReg {
 template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs a, long nlines, int sign,
                                                                  double scale) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     using T = cpx<R>;
     using Y = YReg<N1, N2>;
     static_assert(N1 >= N2 && N1 % N2 == 0, "split");
@@ -895,6 +903,8 @@ struct RowReg {
 
 template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const PlaneArgs a) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     using T = cpx<R>;
     using G = RowReg<N1, N2>;
     constexpr int N = G::N, TJ = G::TJ;
@@ -969,6 +979,8 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
 
 template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const PlaneArgs a) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     using T = cpx<R>;
     using G = RowReg<N1, N2>;
     constexpr int N = G::N, TJ = G::TJ;
@@ -1045,6 +1057,8 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
 
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_inv(const PlaneArgs a) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
@@ -1157,9 +1171,8 @@ static cudaError_t launch_ylines_reg_t(const PlaneArgs& a, int sign, double scal
     using Y = YReg<N1, N2>;
     const long nlines = (long)a.nxh * a.nz * std::max(1, a.batch);
     const size_t sm = (size_t)Y::LPB * Y::LS * sizeof(cpx<R>);
-    k_ylines_reg<R, N1, N2><<<(unsigned)((nlines + Y::LPB - 1) / Y::LPB), kPlaneThreads, sm, s>>>(a, nlines, sign,
-                                                                                                   scale);
-    return cudaGetLastError();
+    return launch_pdl(k_ylines_reg<R, N1, N2>, dim3((unsigned)((nlines + Y::LPB - 1) / Y::LPB)), dim3(kPlaneThreads), sm, s,
+                      a, nlines, sign, scale);
 }
 // the register y transform when ny has a two-factor split, else false
 bool ylines_in_registers(int ny) { return ny == 64 || ny == 128 || ny == 256; }
@@ -1182,8 +1195,8 @@ static cudaError_t launch_rows_reg_t(const PlaneArgs& a, bool fwd, cudaStream_t 
     using G = RowReg<N1, N2>;
     const dim3 g(a.ny / G::TJ, (a.kcount ? a.kcount : a.nz) * std::max(1, a.batch));
     const size_t sm = G::elems * sizeof(cpx<R>);
-    if (fwd) k_rows_fwd_reg<R, N1, N2><<<g, G::NT, sm, s>>>(a);
-    else k_rows_inv_reg<R, N1, N2><<<g, G::NT, sm, s>>>(a);
+    if (fwd) return launch_pdl(k_rows_fwd_reg<R, N1, N2>, g, dim3(G::NT), sm, s, a);
+    return launch_pdl(k_rows_inv_reg<R, N1, N2>, g, dim3(G::NT), sm, s, a);
     return cudaGetLastError();
 }
 // The register rows pass when nx/2 has a two-factor split, else false.  The
@@ -1216,15 +1229,18 @@ static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) 
     if (fwd && a.impl == 2 && a.mode != 2) {
         e = launch_pipe<R, MX>(a, s);
         if (e != cudaSuccess) return e;
-        if (!ylines_reg<R>(ay, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(ay, -1, a.scale);
+        if (!ylines_reg<R>(ay, -1, a.scale, s, &e))
+            e = launch_pdl(k_ylines<R, MY>, glines, dim3(kPlaneThreads), sml, s, ay, -1, a.scale);
     } else if (fwd) {
-        if (!rows_reg<R>(a, true, s, &e)) k_rows_fwd<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
+        if (!rows_reg<R>(a, true, s, &e)) e = launch_pdl(k_rows_fwd<R, MX>, grows, dim3(kPlaneThreads), smr, s, a);
         if (e != cudaSuccess) return e;
-        if (!ylines_reg<R>(ay, -1, a.scale, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(ay, -1, a.scale);
+        if (!ylines_reg<R>(ay, -1, a.scale, s, &e))
+            e = launch_pdl(k_ylines<R, MY>, glines, dim3(kPlaneThreads), sml, s, ay, -1, a.scale);
     } else {
-        if (!ylines_reg<R>(ay, +1, 1.0, s, &e)) k_ylines<R, MY><<<glines, kPlaneThreads, sml, s>>>(ay, +1, 1.0);
+        if (!ylines_reg<R>(ay, +1, 1.0, s, &e))
+            e = launch_pdl(k_ylines<R, MY>, glines, dim3(kPlaneThreads), sml, s, ay, +1, 1.0);
         if (e != cudaSuccess) return e;
-        if (!rows_reg<R>(a, false, s, &e)) k_rows_inv<R, MX><<<grows, kPlaneThreads, smr, s>>>(a);
+        if (!rows_reg<R>(a, false, s, &e)) e = launch_pdl(k_rows_inv<R, MX>, grows, dim3(kPlaneThreads), smr, s, a);
     }
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
@@ -1353,14 +1369,13 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     const long nthreads = 2 * ncols * std::max(1, a.batch);
     const int blocks = (int)((nthreads + kThomasThreads - 1) / kThomasThreads);
     const size_t sm = (size_t)((a.nz + kThomasChunk - 1) / kThomasChunk + 1) * kThomasThreads * sizeof(double);
+    const dim3 g(blocks), b(kThomasThreads);
     if (a.nz % kThomasChunk == 0) {
-        if (fp32) k_thomas<float, true><<<blocks, kThomasThreads, sm, s>>>(a);
-        else k_thomas<double, true><<<blocks, kThomasThreads, sm, s>>>(a);
-    } else {
-        if (fp32) k_thomas<float, false><<<blocks, kThomasThreads, sm, s>>>(a);
-        else k_thomas<double, false><<<blocks, kThomasThreads, sm, s>>>(a);
+        if (fp32) return launch_pdl(k_thomas<float, true>, g, b, sm, s, a);
+        return launch_pdl(k_thomas<double, true>, g, b, sm, s, a);
     }
-    return cudaGetLastError();
+    if (fp32) return launch_pdl(k_thomas<float, false>, g, b, sm, s, a);
+    return launch_pdl(k_thomas<double, false>, g, b, sm, s, a);
 }
 
 cudaError_t launch_thomas_factor(const ColumnArgs& a, double* rtab, cudaStream_t s) {

@@ -44,6 +44,8 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
     constexpr int NF = BG ? 6 : 4;
     extern __shared__ __align__(16) unsigned char step_smem_raw[];
     StepSmem<TT, BY, NF>& sm = *reinterpret_cast<StepSmem<TT, BY, NF>*>(step_smem_raw);
+    pdl_trigger();
+    pdl_wait();   // the state, p and history were written by the preceding kernels
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
@@ -472,8 +474,8 @@ static cudaError_t launch_step_t(const StepArgs& a0, cudaStream_t s) {
     const int kcnt = a.kcount ? a.kcount : a.nz;
     const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
     dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((kcnt + kchunk - 1) / kchunk) * std::max(1, a.batch));
-    k_step<TT, BY, HARM, WM, BG><<<grid, dim3(kTX, BY), sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s>>>(a, kchunk);
-    return cudaGetLastError();
+    return launch_pdl(k_step<TT, BY, HARM, WM, BG>, grid, dim3(kTX, BY), sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s, a,
+                      kchunk);
 }
 
 template <typename TT>
