@@ -47,6 +47,7 @@ def set_grid(nx, ny, nz):
 MEASURED_TRAFFIC_PER_POINT = {
     "fp64": {"step": 165.8},
     "mixed": {"step": 128.4},
+    "mixed_refined": {"step": 128.4},   # the same step kernel
 }
 
 # algorithmic HBM bytes per grid point per launch.  The step kernel reads
@@ -54,13 +55,16 @@ MEASURED_TRAFFIC_PER_POINT = {
 # previous projection's gradient is applied while loading), and writes 4
 # tendencies + 4 state fields.  FP64: 32 + 64 + 8 + 32 + 32 = 168.  Mixed
 # (u,v,b history FP32, w history FP64): 32 + 40 + 8 + 20 + 32 = 132.
-# The mixed step runs two forward transforms: the divergence of u (24 B read,
-# 4 B complex64 written) and the refinement residual, which also reads p
-# (36 B): 32 B per launch on average.  Its inverse transforms write p
-# (4 + 8 B) and, for the refinement, read it back (+8 B): 16 on average.
+# A warm mixed step (every step after the first) solves once, for the
+# residual against the previous step's p: its forward transform reads u, v,
+# w and p (32 B) and writes complex64 (4 B); its inverse reads the spectra
+# (4 B) and reads and writes p (16 B).
+# PS3D_MIXED_REFINED runs a full solve (24 B read, 4 B written; 4 + 8 B)
+# and the residual one (36 B; 20 B) every step: 32 and 16 B on average.
 BYTES_PER_POINT = {
     "fp64": {"step": 168, "fft_fwd": 32, "vsolve": 16, "fft_inv": 16, "correct": 56, "other": 16},
-    "mixed": {"step": 132, "fft_fwd": 32, "vsolve": 8, "fft_inv": 16, "correct": 56, "other": 24},
+    "mixed": {"step": 132, "fft_fwd": 36, "vsolve": 8, "fft_inv": 20, "correct": 56, "other": 24},
+    "mixed_refined": {"step": 132, "fft_fwd": 32, "vsolve": 8, "fft_inv": 16, "correct": 56, "other": 24},
 }
 
 
@@ -361,7 +365,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--case", default="both", choices=["both", "fp64", "mixed"],
+    ap.add_argument("--case", default="both", choices=["both", "fp64", "mixed", "mixed_refined"],
                     help="which time-step paths to time (profiling runs use one)")
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--ny", type=int, default=256)
@@ -417,7 +421,8 @@ def main():
         return out
 
     res = {}
-    for case, prec, name in ((("both", "fp64"), abi.PS3D_FP64, "fp64"), (("both", "mixed"), abi.PS3D_MIXED, "mixed")):
+    for case, prec, name in ((("both", "fp64"), abi.PS3D_FP64, "fp64"), (("both", "mixed"), abi.PS3D_MIXED, "mixed"),
+                             (("both", "mixed_refined"), abi.PS3D_MIXED_REFINED, "mixed_refined")):
         if args.case not in case:
             continue
         m_, p_, ms_, msmax_, k_, clk_, st_, desc_ = time_path(prec, args.steps, args.warmup, dev, pg)
@@ -425,14 +430,14 @@ def main():
         res[name] = {"p": p_, "ms_max": msmax_, "kern": k_, "clk": clk_, "state": st_, "desc": desc_,
                      "value": world * npts * args.steps / (msmax_ * 1e-3),
                      "roof": roof(k_, name)}
-    head = res.get("mixed") or res["fp64"]
-    hname = "mixed" if "mixed" in res else "fp64"
+    hname = "mixed" if "mixed" in res else "fp64" if "fp64" in res else "mixed_refined"
+    head = res[hname]
     dom_name, dom_v = max(head["roof"].items(), key=lambda kv: kv[1]["ms_total"])
     launches = sum(n for _, n in head["kern"].values())
     line = {"metric": metric, "value": head["value"], "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_max"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64 (FP64 state/AB/tridiagonal)" if hname == "mixed" else "f64",
+            "dtype": "f64" if hname == "fp64" else "f32+f64 (FP64 state/AB/tridiagonal)",
             "data": "synthetic (seeded jets + 1e-3 b noise)",
             "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "parallelism": f"replicas x{world}",
                        "path": hname, "kernel_config": head["desc"],
@@ -449,17 +454,32 @@ def main():
         r64 = res["fp64"]
         line["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms_max"] / args.steps, "kernels": r64["roof"],
                         "kernel_config": r64["desc"], "clocks": r64["clk"]}
+    def max_div(st, pp):
+        u, v, w = st["u"], st["v"], st["w"]
+        div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / pp.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / pp.dy
+               + (w[2:-2, 2:-2, 2:-2] - w[1:-3, 2:-2, 2:-2]) / pp.dz)
+        return float(np.abs(div).max())
+
+    if "fp64" in res:
+        line["fp64"]["max_div"] = max_div(res["fp64"]["state"], res["fp64"]["p"])
     if "fp64" in res and "mixed" in res:
         s64, smx, pmx = res["fp64"]["state"], res["mixed"]["state"], res["mixed"]["p"]
         line["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
         line["rel_l2_mixed_vs_fp64"] = {n: cf.rel_l2(cf.interior(smx[n]), cf.interior(s64[n]))
                                         for n in ("u", "v", "w", "b", "p")}
-        u, v, w = smx["u"], smx["v"], smx["w"]
-        div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / pmx.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / pmx.dy
-               + (w[2:-2, 2:-2, 2:-2] - w[1:-3, 2:-2, 2:-2]) / pmx.dz)
-        line["max_div_mixed"] = float(np.abs(div).max())
+        line["max_div_mixed"] = max_div(smx, pmx)
+    if "mixed_refined" in res and hname != "mixed_refined":
+        rr = res["mixed_refined"]
+        line["mixed_refined"] = {"value": rr["value"], "ms_per_step": rr["ms_max"] / args.steps, "kernels": rr["roof"],
+                                 "max_div": max_div(rr["state"], rr["p"]),
+                                 "note": "PS3D_MIXED_REFINED: full FP32 solve + FP64-residual refinement every step"}
+        if "fp64" in res:
+            line["mixed_refined"]["rel_l2_vs_fp64"] = {
+                n: cf.rel_l2(cf.interior(rr["state"][n]), cf.interior(res["fp64"]["state"][n]))
+                for n in ("u", "v", "w", "b", "p")}
     if not args.no_e2e:
-        t, h2d, d2h, _ = e2e_run(abi.PS3D_MIXED if hname == "mixed" else abi.PS3D_FP64, args.steps, dev)
+        eprec = {"fp64": abi.PS3D_FP64, "mixed": abi.PS3D_MIXED, "mixed_refined": abi.PS3D_MIXED_REFINED}[hname]
+        t, h2d, d2h, _ = e2e_run(eprec, args.steps, dev)
         t = max_over_ranks(t, pg, dev)
         line["e2e"] = {"value": world * npts * args.steps / t, "unit": unit, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h,

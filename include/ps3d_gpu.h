@@ -60,12 +60,19 @@ typedef struct ps3d_params {
     int enable_nonlinear;                 /* main_module.f90:16                */
     int enable_vertical_boundaries;       /* rigid lid (1) or periodic z (0)   */
     int enable_AB_3_order;                /* AB3 (1) or AB2 (0)                */
-    int precision;                        /* PS3D_FP64 or PS3D_MIXED           */
+    int precision;                        /* PS3D_FP64, PS3D_MIXED(_REFINED)   */
 } ps3d_params;
 
 #define PS3D_FP64  0   /* every kernel in FP64                                  */
 #define PS3D_MIXED 1   /* FP32 stencils/FFTs, FP64 state, tridiagonal, AB and
-                          eigen-projection, one FP64-residual Poisson refinement */
+                          eigen-projection; the Poisson solve is one FP64-residual
+                          refinement step per time step, started from the previous
+                          step's pressure (a full FP32 solve first after create or
+                          an upload): one solve per step, divergence left at the
+                          FP32 rounding of the step's change of p              */
+#define PS3D_MIXED_REFINED 2   /* as PS3D_MIXED with a full FP32 solve and one
+                          FP64-residual refinement at every step: two solves per
+                          step, divergence left at FP64 roundoff              */
 
 /* ---- optimal balance knobs (for_src/main_module.f90:24-30) ------------- */
 typedef struct ps3d_optbal {
@@ -301,8 +308,10 @@ PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launc
  * A step is the phases below, in this order, each queued on the slab's
  * stream (ps3d_slab_info); between them the caller moves data between ranks:
  *   TENDENCY, PACK_STATE, [halo exchange], UNPACK_STATE, then `passes` times
- *   (1 for FP64; 2 for the mixed path, whose second pass is the FP64-residual
- *   refinement) FORWARD, [all-to-all: xbuf -> colbuf], VSOLVE,
+ *   (ps3d_slab_info, read before each step: 1 for FP64; for the mixed path 2
+ *   on the first step after create or upload, a full solve and its
+ *   FP64-residual refinement, then 1, the residual solve against the
+ *   previous step's pressure) FORWARD, [all-to-all: xbuf -> colbuf], VSOLVE,
  *   [all-to-all: colbuf -> xbuf], INVERSE, PACK_P, [halo exchange], UNPACK_P;
  *   then END_STEP.
  * Halo exchange: hsend holds [planes for the rank below][planes for the rank

@@ -17,6 +17,7 @@ PS3D_ERR_TOOLARGE = -8
 
 PS3D_FP64 = 0
 PS3D_MIXED = 1
+PS3D_MIXED_REFINED = 2
 
 PS3D_FORCE_NONE = 0
 PS3D_FORCE_WAVEMAKER = 1

@@ -65,6 +65,7 @@ struct Ctx {
     int nx = 0, ny = 0, nz = 0, nxh = 0;
     long N = 0, M2 = 0, M = 0;
     bool rigid = true, mixed = false;
+    bool refine_full = false;   // PS3D_MIXED_REFINED: a full solve + refinement every step
     cudaStream_t stream = nullptr;
     bool own_stream = true;
     // bytes per stored tendency of field f: FP32 history in the mixed path,
@@ -83,6 +84,7 @@ struct Ctx {
     const double* g_pcor_in = nullptr;
     const double* g_pcor_out = nullptr;
     double g_dtp_in = 0.0, g_dtp_out = 0.0;
+    bool g_warm_in = false, g_warm_out = false;
     bool use_graphs = true;
     std::atomic<int>* cancel_flag = nullptr;   // serving: set to abandon a running request
     bool cancelled() const { return cancel_flag && cancel_flag->load(std::memory_order_relaxed) != 0; }
@@ -139,6 +141,12 @@ struct Ctx {
     const double* pcor = nullptr;
     double dtp = 0.0;
     bool lazy_correction = true;
+    // p holds the pressure of the previous step's projection of this
+    // trajectory (set by the time step's solve, cleared whenever the state
+    // or p is replaced from outside the time loop): the mixed path then
+    // solves only for the FP64 residual against it
+    bool p_warm = false;
+    bool warm_solve() const { return mixed && !refine_full && p_warm; }
     // per-kernel event timing (ps3d_profile)
     bool prof = false;
     struct ProfRec { int kid; cudaEvent_t e0, e1; };
@@ -188,10 +196,11 @@ struct Ctx {
     int advance(int nsteps, bool allow_graph);
     bool graphable() const;
     int capture_graph();
-    void invalidate_graph() { ++version; }
+    // the state, p or the parameters changed outside the time loop
+    void invalidate_graph() { ++version; p_warm = false; }
     int step(int itt, int tau, int taum1, int taum2);
     int poisson_once(double* out, double beta, bool lazy = false, const double* pc = nullptr);
-    int pressure_solve(bool lazy = false);
+    int pressure_solve(bool lazy = false, bool warm = false);
     int materialize();        // apply a pending correction so the state arrays hold the true state
     int forward_transform(const double* const* in);
     int backward_transform(double* const* out);

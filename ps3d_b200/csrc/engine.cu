@@ -246,10 +246,11 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     M2 = (long)nxh * ny;
     M = M2 * nz;
     rigid = P.enable_vertical_boundaries != 0;
-    mixed = P.precision == PS3D_MIXED;
+    mixed = P.precision == PS3D_MIXED || P.precision == PS3D_MIXED_REFINED;
+    refine_full = P.precision == PS3D_MIXED_REFINED;
     if (nx < 2 || ny < 2 || nz < 2 || nx % 2 || ny % 2 || (!rigid && nz % 2)) return PS3D_ERR_BADPARAM;
     if (!fft_length_ok(nx / 2) || !fft_length_ok(ny) || (!rigid && !fft_length_ok(nz))) return PS3D_ERR_BADPARAM;
-    if (P.precision != PS3D_FP64 && P.precision != PS3D_MIXED) return PS3D_ERR_BADPARAM;
+    if (P.precision != PS3D_FP64 && !mixed) return PS3D_ERR_BADPARAM;
     if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0)) return PS3D_ERR_BADPARAM;
     if (cudaSetDevice(dev) != cudaSuccess) return PS3D_ERR_CUDA;
     if (use_stream) { stream = use_stream; own_stream = false; }
@@ -370,6 +371,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     CK(cudaStreamSynchronize(stream));
     int rc = autotune();
     if (rc) return rc;
+    CK(cudaMemsetAsync(p.p, 0, p.bytes, stream));   // the tuner's timing runs wrote p
     if (rigid && mixed) {
         // the vertical solve's factors depend only on the grid: built once, in
         // the spectral column order of the plane kernels the tuner picked
@@ -539,7 +541,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         for (int f = 0; f < 4; ++f) cur[f] = fin[f];
         return pressure_solve(false);
     }
-    return pressure_solve(lazy_correction);
+    return pressure_solve(lazy_correction, true);
 }
 
 // ---------------------------------------------------------------------------
@@ -740,6 +742,7 @@ int Ctx::capture_graph() {
     const bool pend0 = pending;
     const double* pcor0 = pcor;
     const double dtp0 = dtp;
+    const bool warm0 = p_warm;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     int rc = PS3D_OK;
@@ -749,10 +752,10 @@ int Ctx::capture_graph() {
         ++itt;
     }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
-    g_pend_out = pending; g_pcor_out = pcor; g_dtp_out = dtp;
+    g_pend_out = pending; g_pcor_out = pcor; g_dtp_out = dtp; g_warm_out = p_warm;
     itt = itt0; tau = tau0; taum1 = t10; taum2 = t20;
     for (int f = 0; f < 4; ++f) cur[f] = cur0[f];
-    pending = pend0; pcor = pcor0; dtp = dtp0;
+    pending = pend0; pcor = pcor0; dtp = dtp0; p_warm = warm0;
     g_launches = launches - l0;
     launches = l0;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -761,7 +764,7 @@ int Ctx::capture_graph() {
     cudaGraphDestroy(g);
     CK(e);
     g_tau = tau; g_cur = cur[0]; g_version = version;
-    g_pend_in = pending; g_pcor_in = pcor; g_dtp_in = dtp;
+    g_pend_in = pending; g_pcor_in = pcor; g_dtp_in = dtp; g_warm_in = p_warm;
     return PS3D_OK;
 }
 
@@ -769,7 +772,7 @@ int Ctx::advance(int nsteps, bool allow_graph) {
     while (nsteps > 0) {
         if (allow_graph && nsteps >= 3 && itt >= 2 && graphable()) {
             if (!gexec || g_tau != tau || g_cur != cur[0] || g_version != version || g_pend_in != pending ||
-                g_pcor_in != pcor || g_dtp_in != dtp) {
+                g_pcor_in != pcor || g_dtp_in != dtp || g_warm_in != p_warm) {
                 int rc = capture_graph();
                 if (rc) return rc;
             }
@@ -780,7 +783,7 @@ int Ctx::advance(int nsteps, bool allow_graph) {
                 time = time + P.dt;
                 ++itt;
             }
-            pending = g_pend_out; pcor = g_pcor_out; dtp = g_dtp_out;
+            pending = g_pend_out; pcor = g_pcor_out; dtp = g_dtp_out; p_warm = g_warm_out;
             launches += g_launches;
             nsteps -= 3;
             continue;
@@ -848,18 +851,32 @@ int Ctx::materialize() {
     return PS3D_OK;
 }
 
-int Ctx::pressure_solve(bool lazy) {
+int Ctx::pressure_solve(bool lazy, bool warm) {
     int rc = materialize();
     if (rc) return rc;
-    if (!mixed) return poisson_once((double*)p.p, 0.0, lazy);
-    // one FP64-residual refinement: the divergence of u - dt grad p1 (formed
-    // on the fly from u and p1, in FP64) is solved again and the inverse
-    // transform adds its pressure to p, so p = p1 + p2 and one correction
-    // with p (lazy or not) projects the velocity
-    rc = poisson_once((double*)p.p, 0.0, true);
+    if (!mixed) {
+        rc = poisson_once((double*)p.p, 0.0, lazy);
+    } else if (warm && warm_solve()) {
+        // warm start: p holds p0, the previous step's pressure, so one solve of
+        // the FP64 residual div(u - dt grad p0)/dt (formed on the fly from u and
+        // p0), added to p by the inverse transform, gives the projection's
+        // pressure exactly in exact arithmetic (p0 is in the solver's gauge: a
+        // solver output, or zero); its FP32 rounding scales with the step's
+        // change of p, and the next step's residual is formed against this p
+        rc = poisson_once((double*)p.p, 1.0, lazy, (const double*)p.p);
+    } else {
+        // cold start: a full solve for p1, then one FP64-residual refinement,
+        // the divergence of u - dt grad p1 solved again and its pressure added,
+        // so p = p1 + p2 and one correction with p (lazy or not) projects
+        rc = poisson_once((double*)p.p, 0.0, true);
+        if (rc) return rc;
+        pending = false;
+        rc = poisson_once((double*)p.p, 1.0, lazy, (const double*)p.p);
+    }
     if (rc) return rc;
-    pending = false;
-    return poisson_once((double*)p.p, 1.0, lazy, (const double*)p.p);
+    // only the time step's solve leaves p as the next step's starting point
+    p_warm = warm;
+    return PS3D_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -922,6 +939,7 @@ int Ctx::project(int mode) {
     if (rc) return rc;
     double* out[4];
     if (mode == PS3D_PROJ_NORMAL_MODE || mode == PS3D_PROJ_EXCHANGE) {
+        p_warm = false;   // the projection replaces the state
         for (int f = 0; f < 4; ++f) out[f] = field(f);
     } else {
         const int set = mode == PS3D_PROJ_BASE_POINT ? PS3D_FIELDS_BASE : PS3D_FIELDS_ZERO;
@@ -984,6 +1002,7 @@ cudaError_t Ctx::copy_state_to(int set) {
 }
 cudaError_t Ctx::copy_set_to_state(int set) {
     pending = false;   // the state arrays now hold a true state
+    p_warm = false;    // ... unrelated to the last projection's pressure
     DevBuf* s = fieldset(set);
     cudaError_t e;
     for (int f = 0; f < 4; ++f)
@@ -1029,6 +1048,7 @@ struct RampGraph {
     bool backward = false;
     int cur_in[4] = {0, 0, 0, 0}, cur_out[4] = {0, 0, 0, 0};
     bool pend_in = false, pend_out = false;
+    bool warm_in = false, warm_out = false;
     const double* pcor_in = nullptr;
     const double* pcor_out = nullptr;
     double dtp_in = 0.0, dtp_out = 0.0;
@@ -1056,13 +1076,13 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
     RampGraph* g = nullptr;
     for (RampGraph& c : cache)
         if (c.backward == backward && std::equal(c.cur_in, c.cur_in + 4, cur) && c.pend_in == pending &&
-            c.pcor_in == pcor && c.dtp_in == dtp)
+            c.pcor_in == pcor && c.dtp_in == dtp && c.warm_in == p_warm)
             g = &c;
     if (!g) {
         RampGraph n;
         n.backward = backward;
         std::copy(cur, cur + 4, n.cur_in);
-        n.pend_in = pending; n.pcor_in = pcor; n.dtp_in = dtp;
+        n.pend_in = pending; n.pcor_in = pcor; n.dtp_in = dtp; n.warm_in = p_warm;
         const int itt0 = itt, tau0 = tau, t10 = taum1, t20 = taum2;
         const long long l0 = launches;
         cudaGraph_t graph = nullptr;
@@ -1075,14 +1095,14 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
         }
         const cudaError_t e = cudaStreamEndCapture(stream, &graph);
         std::copy(cur, cur + 4, n.cur_out);
-        n.pend_out = pending; n.pcor_out = pcor; n.dtp_out = dtp;
+        n.pend_out = pending; n.pcor_out = pcor; n.dtp_out = dtp; n.warm_out = p_warm;
         n.tau_out = tau; n.taum1_out = taum1; n.taum2_out = taum2;
         n.Ro_out = P.Ro;
         n.nlaunch = launches - l0;
         // back to the starting state: the replay below performs the steps
         itt = itt0; tau = tau0; taum1 = t10; taum2 = t20;
         std::copy(n.cur_in, n.cur_in + 4, cur);
-        pending = n.pend_in; pcor = n.pcor_in; dtp = n.dtp_in;
+        pending = n.pend_in; pcor = n.pcor_in; dtp = n.dtp_in; p_warm = n.warm_in;
         launches = l0;
         if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
         CK(e);
@@ -1095,7 +1115,7 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
     if (cancelled()) return PS3D_ERR_CANCELLED;
     CK(cudaGraphLaunch(g->exec, stream));
     std::copy(g->cur_out, g->cur_out + 4, cur);
-    pending = g->pend_out; pcor = g->pcor_out; dtp = g->dtp_out;
+    pending = g->pend_out; pcor = g->pcor_out; dtp = g->dtp_out; p_warm = g->warm_out;
     tau = g->tau_out; taum1 = g->taum1_out; taum2 = g->taum2_out;
     P.Ro = g->Ro_out;
     launches += g->nlaunch;
@@ -1173,6 +1193,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
             }
             if (rc) break;
             DevBuf *sv = fieldset(kSetSave2), *av = fieldset(kSetAve), *bs = fieldset(PS3D_FIELDS_BASE);
+            p_warm = false;
             for (int f = 0; f < 4; ++f) {
                 CK(cudaMemcpyAsync(field(f), sv[f].p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
                 LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)av[f].p, N, 1.0, -1.0, stream));
@@ -1357,6 +1378,7 @@ int ps3d_upload_state(ps3d_ctx* ctx, const double* u, const double* v, const dou
     Ctx& C = ctx->impl;
     if (tau < 1 || tau > 3 || taum1 < 1 || taum1 > 3 || taum2 < 1 || taum2 > 3 || itt < 0) return PS3D_ERR_BADPARAM;
     int rc = C.materialize(); if (rc) return rc;   // fields not uploaded keep their true values
+    C.p_warm = false;
     const double* f[4] = {u, v, w, b};
     for (int q = 0; q < 4; ++q) { rc = C.upload_field(C.field(q), f[q]); if (rc) return rc; }
     rc = C.upload_field((double*)C.p.p, p); if (rc) return rc;
@@ -1541,7 +1563,7 @@ int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
     const Ctx& C = ctx->impl;
     const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
     std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_impl=%s plane_cluster=%d row_chunk=%d tj=%d ly=%d "
-                  "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.mixed ? "mixed" : "fp64",
+                  "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.refine_full ? "mixed_refined" : C.mixed ? "mixed" : "fp64",
                   C.batch, pa.impl == 2 ? "pipe+lines" : pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
                   C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
     return PS3D_OK;

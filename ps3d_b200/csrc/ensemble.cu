@@ -54,11 +54,11 @@ bool all_graphable(ps3d_ensemble* e) {
 
 int capture(ps3d_ensemble* e) {
     if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
-    struct Book { int itt, tau, t1, t2, cur[4]; double time; long long launches; bool pend; const double* pcor; double dtp; };
+    struct Book { int itt, tau, t1, t2, cur[4]; double time; long long launches; bool pend; const double* pcor; double dtp; bool warm; };
     std::vector<Book> saved;
     for (auto& g : e->groups)
         saved.push_back({g->itt, g->tau, g->taum1, g->taum2, {g->cur[0], g->cur[1], g->cur[2], g->cur[3]}, g->time,
-                         g->launches, g->pending, g->pcor, g->dtp});
+                         g->launches, g->pending, g->pcor, g->dtp, g->p_warm});
     const int itt0 = e->itt;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PS3D_ERR_CUDA;
@@ -72,9 +72,9 @@ int capture(ps3d_ensemble* e) {
         for (int f = 0; f < 4; ++f) g.cur[f] = saved[q].cur[f];
         g.time = saved[q].time;
         g.launches = saved[q].launches;
-        g.g_pend_out = g.pending; g.g_pcor_out = g.pcor; g.g_dtp_out = g.dtp;
-        g.pending = saved[q].pend; g.pcor = saved[q].pcor; g.dtp = saved[q].dtp;
-        g.g_pend_in = g.pending; g.g_pcor_in = g.pcor; g.g_dtp_in = g.dtp;
+        g.g_pend_out = g.pending; g.g_pcor_out = g.pcor; g.g_dtp_out = g.dtp; g.g_warm_out = g.p_warm;
+        g.pending = saved[q].pend; g.pcor = saved[q].pcor; g.dtp = saved[q].dtp; g.p_warm = saved[q].warm;
+        g.g_pend_in = g.pending; g.g_pcor_in = g.pcor; g.g_dtp_in = g.dtp; g.g_warm_in = g.p_warm;
     }
     e->itt = itt0;
     if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -91,7 +91,8 @@ int advance(ps3d_ensemble* e, int nsteps) {
         if (nsteps >= 3 && e->itt >= 2 && all_graphable(e)) {
             bool same = true;
             for (auto& g : e->groups)
-                same = same && g->g_pend_in == g->pending && g->g_pcor_in == g->pcor && g->g_dtp_in == g->dtp;
+                same = same && g->g_pend_in == g->pending && g->g_pcor_in == g->pcor && g->g_dtp_in == g->dtp &&
+                       g->g_warm_in == g->p_warm;
             if (!e->graph_valid || !same) {
                 int rc = capture(e);
                 if (rc) return rc;
@@ -106,7 +107,7 @@ int advance(ps3d_ensemble* e, int nsteps) {
                 }
             for (auto& g : e->groups) {
                 g->launches += g->g_launches;
-                g->pending = g->g_pend_out; g->pcor = g->g_pcor_out; g->dtp = g->g_dtp_out;
+                g->pending = g->g_pend_out; g->pcor = g->g_pcor_out; g->dtp = g->g_dtp_out; g->p_warm = g->g_warm_out;
             }
             e->itt += 3;
             nsteps -= 3;
@@ -175,6 +176,7 @@ PS3D_API int ps3d_ensemble_upload(ps3d_ensemble* e, int member, const double* u,
     const int m = e->where[member].second;
     { int rc = g.materialize(); if (rc) return rc; }
     e->graph_valid = false;
+    g.p_warm = false;   // the group's next step starts cold (every member)
     const double* f[4] = {u, v, w, b};
     for (int q = 0; q < 4; ++q) {
         int rc = g.upload_field(g.member_field(q, m), f[q]);

@@ -57,7 +57,7 @@ struct Request {
 static size_t footprint_of(const ps3d_params& p) {
     const size_t N = (size_t)p.nx * p.ny * p.nz;
     const size_t M = (size_t)(p.nx / 2 + 1) * p.ny * p.nz;
-    const bool mixed = p.precision == PS3D_MIXED;
+    const bool mixed = p.precision == PS3D_MIXED || p.precision == PS3D_MIXED_REFINED;
     const size_t ts = mixed ? 4 : 8;
     size_t b = 0;
     b += 12 * N * 8;                       // 3 state buffers x 4 fields
@@ -268,7 +268,7 @@ PS3D_API int ps3d_server_submit(ps3d_server* s, const ps3d_params* prm, const ps
     if (!ps3d::fft_length_ok(p.nx / 2) || !ps3d::fft_length_ok(p.ny) || (!rigid && !ps3d::fft_length_ok(p.nz)))
         return PS3D_ERR_BADPARAM;
     if (!(p.dt > 0) || !(opt->period > 0) || opt->max_itts < 1) return PS3D_ERR_BADPARAM;
-    if (p.precision == PS3D_MIXED && (p.Ahbi > 0 || p.Avbi > 0 || p.Khbi > 0 || p.Kvbi > 0)) return PS3D_ERR_UNSUPPORTED;
+    if (p.precision != PS3D_FP64 && (p.Ahbi > 0 || p.Avbi > 0 || p.Khbi > 0 || p.Kvbi > 0)) return PS3D_ERR_UNSUPPORTED;
     auto r = std::make_shared<Request>();
     r->prm = p;
     r->opt = *opt;

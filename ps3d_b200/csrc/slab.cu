@@ -22,10 +22,11 @@
 //   p halo      p one level below and two above (the step kernel's lazy
 //               correction reads p at the plane it loads and the one above)
 //
-// The mixed path (FP32 transforms) runs forward .. p halo twice per step:
-// the second pass solves for the divergence of u - dt grad p in FP64 (the
-// FP64-residual refinement, pressure_solve in engine.cu) and adds its
-// pressure to p.
+// The mixed path (FP32 transforms) solves for the divergence of
+// u - dt grad p in FP64 and adds that pressure to p (pressure_solve in
+// engine.cu): once per step from the previous step's p (warm), and on a cold
+// start (after create or upload) after a first full solve, so forward ..
+// p halo run twice on that step.
 //
 // Local arrays hold nzl + 3 levels: halo 0, interior 1 .. nzl, halos nzl+1
 // and nzl+2 (the second only for p).  The transport between ranks is the
@@ -53,10 +54,13 @@ struct ps3d_slab {
     void* hsend = nullptr;          // halo planes to send: [down][up]
     void* hrecv = nullptr;          // halo planes received: [from below][from above]
     bool need_halo = true;          // state halos not yet exchanged (after an upload)
-    bool mixed = false;             // FP32 spectra, two solve passes per step
-    int pass = 0;                   // solve pass of the current step (0, then 1 in the mixed path)
+    bool mixed = false;             // FP32 spectra, residual solves
+    int pass = 0;                   // solve pass: 0 full solve, 1 residual solve (mixed path)
 
-    int passes() const { return mixed ? 2 : 1; }
+    // solve passes of the next step: 1 in FP64; in the mixed path 2 on a cold
+    // start (full solve, then the residual one), else 1 (the residual solve
+    // against the previous step's p)
+    int passes() const { return mixed && !ctx->warm_solve() ? 2 : 1; }
     size_t es() const { return mixed ? sizeof(float2) : sizeof(double2); }
     size_t xbytes() const { return (size_t)nzl * ncols * es(); }
     size_t colbytes() const { return (size_t)nzg * ccnt[rank] * es(); }
@@ -71,7 +75,7 @@ constexpr int kDown[2] = {4, 2}, kUp[2] = {4, 1};
 
 int slab_tendency(ps3d_slab* s) {
     Ctx& c = *s->ctx;
-    s->pass = 0;
+    s->pass = c.warm_solve() ? 1 : 0;
     return c.step(c.itt, c.tau, c.taum1, c.taum2);
 }
 
@@ -123,7 +127,8 @@ ps3d::PlaneArgs window(ps3d_slab* s, const ps3d::PlaneArgs& base) {
 int slab_forward(ps3d_slab* s) {
     Ctx& c = *s->ctx;
     ps3d::PlaneArgs a = window(s, s->mixed ? c.pa32 : c.pa64);
-    // pass 1 (mixed): the divergence of u - dt grad p, p from pass 0 with its halos
+    // pass 1 (mixed): the divergence of u - dt grad p, p from pass 0 or from the
+    // previous step, with its halos
     a.mode = s->pass ? 2 : 0;
     a.u = c.field(0); a.v = c.field(1); a.w = c.field(2);
     a.pc = s->pass ? (const double*)c.p.p : nullptr;
@@ -167,13 +172,14 @@ int slab_inverse(ps3d_slab* s) {
     ps3d::PlaneArgs b = window(s, s->mixed ? c.pa32 : c.pa64);
     b.spec = c.FS.p;
     b.out = (double*)c.p.p;
-    b.beta = s->pass ? 1.0 : 0.0;   // the refinement pass adds its pressure
+    b.beta = s->pass ? 1.0 : 0.0;   // the residual pass adds its pressure
     b.scale = 1.0 / (c.P.Lx * c.P.Ly);
     CK(ps3d::launch_plane_inv(b, s->mixed, c.stream));
-    if (++s->pass >= s->passes()) {
+    if (++s->pass >= (s->mixed ? 2 : 1)) {
         c.pending = true;
         c.pcor = (const double*)c.p.p;
         c.dtp = c.P.dt;
+        c.p_warm = true;
     }
     return PS3D_OK;
 }
@@ -263,7 +269,8 @@ int group_step(ps3d_slab* const* r, int n) {
     if (r[0]->need_halo && (rc = group_halo(r, n, 0))) return rc;
     FOR_RANKS(slab_tendency(r[q]))
     if ((rc = group_halo(r, n, 0))) return rc;
-    for (int pass = 0; pass < r[0]->passes(); ++pass) {
+    const int np = r[0]->passes();
+    for (int pass = 0; pass < np; ++pass) {
         FOR_RANKS(slab_forward(r[q]))
         if ((rc = transport_columns(r, n, true))) return rc;
         FOR_RANKS(slab_vsolve(r[q]))
@@ -293,7 +300,7 @@ PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, i
     if (global->nz % nranks || global->nz / nranks < 2) return PS3D_ERR_BADPARAM;
     std::unique_ptr<ps3d_slab> s(new ps3d_slab());
     s->nranks = nranks; s->rank = rank;
-    s->mixed = global->precision == PS3D_MIXED;
+    s->mixed = global->precision == PS3D_MIXED || global->precision == PS3D_MIXED_REFINED;
     s->nzg = global->nz; s->nzl = global->nz / nranks; s->k0 = rank * s->nzl;
     ps3d_params lp = *global;
     lp.nz = s->nzl + 3;
@@ -377,6 +384,7 @@ PS3D_API int ps3d_slab_upload(ps3d_slab* s, const double* u, const double* v, co
     const size_t bytes = (size_t)s->nzl * s->plane * sizeof(double);
     for (int q = 0; q < 4; ++q) CK(cudaMemcpy(s->lvl(c.field(q), 1), f[q], bytes, cudaMemcpyHostToDevice));
     c.pending = false;
+    c.p_warm = false;
     c.itt = 0; c.tau = 3; c.taum1 = 2; c.taum2 = 1; c.time = 0.0;
     for (int q = 0; q < 4; ++q) CK(cudaMemset(c.tend[q].p, 0, c.tend[q].bytes));
     s->need_halo = true;

@@ -386,6 +386,7 @@ int Ctx::diag_balance(int order, int filter_width) {
     if (order < 0 || order > 3) return PS3D_ERR_BADPARAM;
     if (filter_width >= 0 && nz / 2 + filter_width >= nz) return PS3D_ERR_BADPARAM;
     WCHK(materialize());
+    p_warm = false;   // the balanced state replaces the model state
     CK(ensure_warn());
     warn_filter = filter_width;
     WCHK(project(PS3D_PROJ_ZERO_ORDER));   // diag_balance_zero_order

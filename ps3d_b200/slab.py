@@ -20,7 +20,7 @@ import ctypes as C
 
 import numpy as np
 
-from .abi import Params
+from .abi import PS3D_FP64, Params
 from .model import _check, load
 
 PHASE = {"tendency": 0, "pack_state": 1, "unpack_state": 2, "forward": 3, "vsolve": 4, "inverse": 5,
@@ -70,13 +70,22 @@ class Slab:
         _check(self.L.ps3d_slab_info(h, C.byref(k0), C.byref(nzl), C.byref(col0), C.byref(ncl), C.byref(st),
                                      C.byref(ps)), "ps3d_slab_info")
         self.k0, self.nzl, self.col0, self.ncl, self.stream = k0.value, nzl.value, col0.value, ncl.value, st.value
-        self.passes = ps.value   # solve passes per step: 2 in the mixed path (refinement)
+        self.passes = ps.value   # solve passes of the first step (step_passes: of the next one)
+        self.mixed = self.params.precision != PS3D_FP64
         xb, cb, hb = C.c_size_t(), C.c_size_t(), C.c_size_t()
         counts = (C.c_longlong * nranks)()
         _check(self.L.ps3d_slab_buffers(h, C.byref(xb), C.byref(cb), C.byref(hb), counts), "ps3d_slab_buffers")
         self.xbytes, self.colbytes, self.hbytes = xb.value, cb.value, hb.value
         self.col_counts = [int(c) for c in counts]
         self.plane = self.params.nx * self.params.ny
+
+    def step_passes(self):
+        """Solve passes of the next step: 1 in FP64; in the mixed path 2 after
+        create or upload (full solve and FP64-residual refinement), then 1
+        (the residual solve against the previous step's pressure)."""
+        ps = C.c_int()
+        _check(self.L.ps3d_slab_info(self.h, None, None, None, None, None, C.byref(ps)), "ps3d_slab_info")
+        return ps.value
 
     def bind(self, xbuf, colbuf, hsend, hrecv):
         """Use caller-owned device buffers (addresses) for the exchanges."""
@@ -195,7 +204,7 @@ class DistSlab:
         dev = torch.device("cuda", device)
         f8 = torch.float64
         # spectra: complex double, or complex float in the mixed path
-        fs = torch.float32 if self.slab.passes == 2 else torch.float64
+        fs = torch.float32 if self.slab.mixed else torch.float64
         esz = 4 if fs == torch.float32 else 8
         self.xbuf = torch.empty(self.slab.xbytes // esz, dtype=fs, device=dev)
         self.colbuf = torch.empty(self.slab.colbytes // esz, dtype=fs, device=dev)
@@ -224,9 +233,10 @@ class DistSlab:
             if self.need_halo:
                 self._halo(0)
                 self.need_halo = False
+            npass = s.step_passes()
             s.phase("tendency")
             self._halo(0)
-            for _ in range(s.passes):
+            for _ in range(npass):
                 s.phase("forward")
                 with self.torch.cuda.stream(self.stream):
                     columns_forward(self.xbuf, self.colbuf, counts, nzl, self.rank, self.group)

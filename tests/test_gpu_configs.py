@@ -5,7 +5,8 @@ the oracle finishes in seconds; at full size the oracle is too slow for a
 test, so the mixed path is held to its 1e-5 relative-L2 bound against the
 FP64 path on the same seeded inputs:
   * jets 256x256x128, rigid lid, 500 steps: u, v, w, b, p, and the
-    divergence left by the projection;
+    divergence left by the projection (PS3D_MIXED, one warm-started residual
+    solve per step, and PS3D_MIXED_REFINED, a full solve and its refinement);
   * lee-wave-like 512x256x128, triply periodic, background flow U = 0.1 m/s
     and a bottom wavemaker with seeded phases, 300 steps: w and p.
 """
@@ -46,19 +47,23 @@ def _div(p, s):
 
 def test_jets_mixed_vs_fp64_500_steps():
     out = {}
-    for prec in (abi.PS3D_FP64, abi.PS3D_MIXED):
+    for prec in (abi.PS3D_FP64, abi.PS3D_MIXED, abi.PS3D_MIXED_REFINED):
         p = cf.jets_params(256, 256, 128, precision=prec)
         f = cf.add_noise(p, cf.jets_fields(p), "b", rel=1e-3, seed=1)
         out[prec] = (p, _run(p, f, 500))
-    (p64, s64), (_, smx) = out[abi.PS3D_FP64], out[abi.PS3D_MIXED]
-    for n in ("u", "v", "w", "b", "p"):
-        e = rel(smx[n][2:-2, 2:-2, 2:-2], s64[n][2:-2, 2:-2, 2:-2])
-        assert e < TOL_MIXED, (n, e)
-    # the refined projection leaves the mixed velocity about as divergence-free
-    # as the FP64 one (both at roundoff of |u|/dx)
+    p64, s64 = out[abi.PS3D_FP64]
     scale = np.abs(s64["u"]).max() / p64.dx
-    d64, dmx = np.abs(_div(p64, s64)).max(), np.abs(_div(p64, smx)).max()
-    assert dmx < max(10 * d64, 1e-7 * scale), (dmx, d64, scale)
+    d64 = np.abs(_div(p64, s64)).max()
+    # the refined projection leaves the mixed velocity about as divergence-free
+    # as the FP64 one (both at roundoff of |u|/dx); the warm-started one at
+    # the FP32 rounding of the step's change of p (6.6e-7 |u|/dx measured)
+    for prec, dtol in ((abi.PS3D_MIXED, 4e-6 * scale), (abi.PS3D_MIXED_REFINED, max(10 * d64, 1e-7 * scale))):
+        smx = out[prec][1]
+        for n in ("u", "v", "w", "b", "p"):
+            e = rel(smx[n][2:-2, 2:-2, 2:-2], s64[n][2:-2, 2:-2, 2:-2])
+            assert e < TOL_MIXED, (prec, n, e)
+        dmx = np.abs(_div(p64, smx)).max()
+        assert dmx < dtol, (prec, dmx, d64, scale)
 
 
 def test_lee_wave_mixed_vs_fp64_300_steps():

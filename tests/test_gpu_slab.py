@@ -86,20 +86,24 @@ def test_slab_download_per_rank(monkeypatch):
     g.close()
 
 
+@pytest.mark.parametrize("precision", [abi.PS3D_MIXED, abi.PS3D_MIXED_REFINED])
 @pytest.mark.parametrize("nranks", [2, 4])
-def test_mixed_slabs_match_single_grid(nranks, monkeypatch):
-    """The mixed path: FP32 transforms, two solve passes per step (the FP64
-    residual refinement, with a p-halo exchange between them).  The single
-    grid reads its Thomas factors from a table; the column slabs form the
-    same FP64 values on the fly."""
+def test_mixed_slabs_match_single_grid(nranks, precision, monkeypatch):
+    """The mixed path: FP32 transforms; the first step solves twice (a full
+    solve and the FP64-residual refinement, with a p-halo exchange between
+    them), every later one once (the residual against the previous step's
+    p).  The single grid reads its Thomas factors from a table; the column
+    slabs form the same FP64 values on the fly."""
     monkeypatch.setenv("PS3D_TUNE", "im1,C1,rc8,tj16,ly16,pol0,kc8")
-    p = small_params(64, 32, 32, rigid=True, precision=abi.PS3D_MIXED)
+    p = small_params(64, 32, 32, rigid=True, precision=precision)
     f = random_state(p, seed=11, amp=0.05)
     ref = _single(p, f, 6, monkeypatch)
     g = SlabGroup(p, nranks)
     assert g.ranks[0].passes == 2
     g.upload(*[_interior(f[n]) for n in "uvwb"])
     g.step(6)
+    # warm: the residual solve only; refined: both solves at every step
+    assert all(s.step_passes() == (1 if precision == abi.PS3D_MIXED else 2) for s in g.ranks)
     got = g.download()
     g.close()
     err = {n: rel(got[n], ref[n]) for n in NAMES}
