@@ -1,0 +1,138 @@
+"""The C++ host driver (ps3d_b200/ps3d_main, main.f90 over the C ABI) on the
+GPU, against the CPU oracle.
+
+A 32x32x16 eddy runs 12 steps with diagnose every 4 and a snapshot every 6
+steps.  The restart file the driver writes at the end (restart.f90 layout)
+and the snapshot at itt = 6 (the state after the integrate of itt = 6, i.e.
+7 steps) must match the oracle's state after the same steps, and the KE it
+prints at itt = 4 the oracle's diagnose.  A second run in the same directory
+reads that restart file, extends runlen by its time (restart.f90:51-53) and
+continues to 24 steps."""
+import os
+import re
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.binding import Oracle
+from ps3d_b200 import build
+from ps3d_b200 import configs as cf
+from tests.helpers import load_oracle, rel
+from tests.test_gpu_restart import _records
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-11
+NAMES = ("u", "v", "w", "b", "p")
+
+
+def _setup(tmp_path):
+    p = cf.eddy_params(32, 32, 16)
+    f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=4)
+    init = tmp_path / "init.bin"
+    np.concatenate([np.ascontiguousarray(f[n], dtype="<f8").ravel() for n in "uvwb"]).tofile(init)
+    par = tmp_path / "eddy.par"
+    par.write_text(f"""! 32x32x16 eddy (for_config/eddy1.f90 template)
+nx = {p.nx}
+ny = {p.ny}
+nz = {p.nz}
+Lx = {p.Lx!r}
+Ly = {p.Ly!r}
+Lz = {p.Lz!r}
+dt = {p.dt!r}
+f0 = {p.f0!r}
+N0 = {p.N0!r}
+Ah = {p.Ah!r}
+Av = {p.Av!r}
+enable_vertical_boundaries = .true.
+enable_AB_3_order = .true.
+runlen = {12 * p.dt!r}
+tsmonint = {4 * p.dt!r}
+snapint = {6 * p.dt!r}
+enable_diag_snap = .true.
+init = {init}
+outdir = {tmp_path}
+""")
+    return p, f, par
+
+
+def _oracle_after(p, f, nsteps):
+    o = Oracle(p)
+    load_oracle(o, f)
+    o.integrate(nsteps)
+    return o
+
+
+def _restart_fields(path, p):
+    r1, r2, r3 = _records(path)
+    nx, ny, nz, itt = struct.unpack_from("<4i", r1, 0)
+    a = np.frombuffer(r3, dtype="<f8")
+    n = (p.nz + 4) * (p.ny + 4) * (p.nx + 4)
+    return itt, {nm: a[q * n:(q + 1) * n].reshape(p.nz + 4, p.ny + 4, p.nx + 4) for q, nm in enumerate(NAMES)}
+
+
+def _snapshot(path, p):
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"PS3DSNAP"
+    nx, ny, nz, nf, itt = struct.unpack_from("<5i", raw, 8)
+    (time,) = struct.unpack_from("<d", raw, 32)
+    assert (nx, ny, nz, nf) == (p.nx, p.ny, p.nz, 5)
+    a = np.frombuffer(raw[64:], dtype="<f8")
+    n = (p.nz + 4) * (p.ny + 4) * (p.nx + 4)
+    return itt, time, {nm: a[q * n:(q + 1) * n].reshape(p.nz + 4, p.ny + 4, p.nx + 4) for q, nm in enumerate(NAMES)}
+
+
+def test_driver_run_and_restart(tmp_path):
+    build.build()
+    p, f, par = _setup(tmp_path)
+    r = subprocess.run([build.DRIVER, str(par)], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = r.stdout
+    assert "found no restart file" in out
+    assert [int(x) for x in re.findall(r"diagnosing at t=\s*\S+ itt=\s*(\d+)", out)] == [0, 4, 8]
+    assert (tmp_path / "ritt").read_text().split() == ["12"]
+
+    # the restart file after 12 steps
+    itt, got = _restart_fields(tmp_path / "restart_pe=000000000.dta", p)
+    assert itt == 12
+    o12 = _oracle_after(p, f, 12)
+    err = {n: rel(got[n], o12.field(n)) for n in NAMES}
+    assert max(err.values()) < TOL64, err
+
+    # the snapshot of itt = 6: 7 steps done, time = 6 dt
+    itt, time, snap = _snapshot(tmp_path / "snap_000000006.bin", p)
+    assert itt == 6 and time == pytest.approx(6 * p.dt)
+    o7 = _oracle_after(p, f, 7)
+    err = {n: rel(snap[n], o7.field(n)) for n in NAMES}
+    assert max(err.values()) < TOL64, err
+    assert (tmp_path / "snap_000000000.bin").exists()
+
+    # diagnose at itt = 4 reports the state after 5 steps
+    ke = float(re.findall(r"KE = (\S+) m\^2/s\^2", out)[1])
+    _, ke_ref, _, _, _ = _oracle_after(p, f, 5).diagnose()
+    assert ke == pytest.approx(ke_ref, rel=1e-3)
+
+    # second run: reads the restart, runs to 24 steps
+    r = subprocess.run([build.DRIVER, str(par)], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "reading restart file" in r.stdout and "adjusting run length" in r.stdout
+    assert (tmp_path / "ritt").read_text().split() == ["24"]
+    itt, got = _restart_fields(tmp_path / "restart_pe=000000000.dta", p)
+    assert itt == 24
+    o24 = _oracle_after(p, f, 24)
+    err = {n: rel(got[n], o24.field(n)) for n in NAMES}
+    assert max(err.values()) < TOL64, err
+
+
+def test_driver_reports_library_errors(tmp_path):
+    """A grid the engine cannot take (nz = 1 under a rigid lid) passes the
+    reference's own checks but not ps3d_create: the driver prints the
+    library's message and stops with 99."""
+    build.build()
+    r = subprocess.run([build.DRIVER, "nx=32", "ny=32", "nz=1", "Lx=1", "Ly=1", "Lz=1", "dt=1",
+                        "enable_vertical_boundaries=1", f"outdir={tmp_path}"],
+                       capture_output=True, text=True, timeout=120, cwd=tmp_path)
+    assert r.returncode == 99
+    assert "ps3d_create" in r.stderr
