@@ -12,18 +12,23 @@ from ps3d_b200.model import PS3DError
 pytestmark = pytest.mark.gpu
 
 
-def _req(n=(32, 32, 16), ramp=6, iters=2):
-    return request(*n, ramp_steps=ramp, iters=iters)
+def _req(n=(32, 32, 16), ramp=6, iters=2, precision=abi.PS3D_FP64):
+    return request(*n, precision=precision, ramp_steps=ramp, iters=iters)
 
 
-def test_result_same_alone_and_in_mix():
-    p, opt, f = _req((32, 32, 16))
+PRECISIONS = [abi.PS3D_FP64, abi.PS3D_MIXED]
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_result_same_alone_and_in_mix(precision):
+    p, opt, f = _req((32, 32, 16), precision=precision)
     s = Server(max_active=1)
     alone = s.wait(s.submit(p, opt, f))
     s.close()
     assert alone.status == 0
     s = Server(max_active=4)
-    others = [_req((64, 32, 16)), _req((32, 32, 8)), _req((64, 64, 16))]
+    # neighbours of the other precision too: contexts of both kinds share the GPU
+    others = [_req((64, 32, 16)), _req((32, 32, 8), precision=abi.PS3D_MIXED), _req((64, 64, 16))]
     tks = [s.submit(*o) for o in others[:2]]
     mine = s.submit(p, opt, f)
     tks += [s.submit(*others[2])]
@@ -39,10 +44,12 @@ def test_result_same_alone_and_in_mix():
     assert st["peak_active"] >= 2
 
 
-def test_reused_context_gives_the_same_result():
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_reused_context_gives_the_same_result(precision):
     """A finished request's context serves the next request with the same
-    parameters; the result is bit for bit what a new context gives."""
-    p, opt, f = _req((32, 32, 16))
+    parameters; the result is bit for bit what a new context gives (the
+    mixed path's warm start included: a reset context starts cold)."""
+    p, opt, f = _req((32, 32, 16), precision=precision)
     s = Server(max_active=1)
     first = s.wait(s.submit(p, opt, f))
     g = {k: v * 1.01 for k, v in f.items()}   # another state on the same grid in between
@@ -53,6 +60,26 @@ def test_reused_context_gives_the_same_result():
     assert again.norm == first.norm and again.iters == first.iters
     for n in ("u", "v", "w", "b"):
         assert np.array_equal(again.fields[n], first.fields[n]), n
+
+
+def test_mixed_request_matches_fp64():
+    """The same optimal-balance request on the mixed path (FP32 transforms,
+    warm-started residual projection) and on the FP64 path."""
+    s = Server(max_active=2)
+    res = {}
+    for prec in (abi.PS3D_FP64, abi.PS3D_MIXED):
+        p, opt, f = _req((64, 64, 16), ramp=10, iters=3, precision=prec)
+        res[prec] = s.wait(s.submit(p, opt, f))
+    s.close()
+    r64, rmx = res[abi.PS3D_FP64], res[abi.PS3D_MIXED]
+    assert r64.status == rmx.status == 0 and r64.iters == rmx.iters == 3
+    err = {}
+    for n in ("u", "v", "w", "b"):
+        a, b = rmx.fields[n][2:-2, 2:-2, 2:-2], r64.fields[n][2:-2, 2:-2, 2:-2]
+        err[n] = np.linalg.norm(a - b) / np.linalg.norm(b)
+    # w is the balanced state's small ageostrophic part, the field the FP32
+    # tendency history perturbs most relative to its size
+    assert max(err["u"], err["v"], err["b"]) < 1e-5 and err["w"] < 1e-3, err
 
 
 def test_admission_respects_budget():
