@@ -7,7 +7,8 @@ and the snapshot at itt = 6 (the state after the integrate of itt = 6, i.e.
 7 steps) must match the oracle's state after the same steps, and the KE it
 prints at itt = 4 the oracle's diagnose.  A second run in the same directory
 reads that restart file, extends runlen by its time (restart.f90:51-53) and
-continues to 24 steps."""
+continues to 24 steps.  A third run writes diag_balance and diag_opt_balance
+outputs, checked against the same library calls through the Python binding."""
 import os
 import re
 import struct
@@ -136,3 +137,53 @@ def test_driver_reports_library_errors(tmp_path):
                        capture_output=True, text=True, timeout=120, cwd=tmp_path)
     assert r.returncode == 99
     assert "ps3d_create" in r.stderr
+
+
+def _fields_file(path, p, nf):
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"PS3DSNAP"
+    assert struct.unpack_from("<4i", raw, 8) == (p.nx, p.ny, p.nz, nf)
+    a = np.frombuffer(raw[64:], dtype="<f8")
+    n = (p.nz + 4) * (p.ny + 4) * (p.nx + 4)
+    assert a.size == nf * n
+    return {nm: a[q * n:(q + 1) * n].reshape(p.nz + 4, p.ny + 4, p.nx + 4) for q, nm in enumerate("uvwb"[:nf])}
+
+
+def test_driver_balance_outputs(tmp_path):
+    """diag_balance and diag_opt_balance at the snapshot interval (itt = 0
+    and 3): the driver's output files hold what the same library calls give
+    through the Python binding after the same steps."""
+    from ps3d_b200.abi import OptBal, PS3D_FIELDS_BALANCED
+    from ps3d_b200.model import Model
+    build.build()
+    p = cf.eddy_params(32, 32, 16)
+    p.Ah = p.Av = 0.0   # the backward ramp keeps harmonic friction (diag_opt_balance.f90:190-192)
+    f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=5)
+    init = tmp_path / "init.bin"
+    np.concatenate([np.ascontiguousarray(f[n], dtype="<f8").ravel() for n in "uvwb"]).tofile(init)
+    args = [f"nx={p.nx}", f"ny={p.ny}", f"nz={p.nz}", f"Lx={p.Lx!r}", f"Ly={p.Ly!r}", f"Lz={p.Lz!r}",
+            f"dt={p.dt!r}", f"f0={p.f0!r}", f"N0={p.N0!r}", "enable_vertical_boundaries=.true.",
+            "enable_AB_3_order=.true.", f"runlen={4 * p.dt!r}", f"tsmonint={100 * p.dt!r}",
+            f"snapint={3.5 * p.dt!r}", "enable_diag_balance=.true.", "enable_diag_opt_balance=.true.",
+            f"opt_balance_period={5.5 * p.dt!r}", "opt_balance_max_Itts=2", "opt_balance_tol=0",
+            f"init={init}", f"outdir={tmp_path}", "write_restart=.false."]
+    r = subprocess.run([build.DRIVER, *args], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert len(re.findall(r"optimal balance: 2 iterations", r.stdout)) == 2
+    assert not (tmp_path / "restart_pe=000000000.dta").exists()
+
+    m = Model(p)
+    m.upload(**{n: f[n] for n in "uvwb"})
+    opt = OptBal(period=5.5 * p.dt, average=1.0, max_itts=2, average_times=1, tol=0.0, enable_time_ave=0, adopt=0)
+    for itt, nrun in ((0, 1), (3, 3)):
+        m.run(nrun)
+        comps = m.diag_balance(3)
+        bal = {n: sum(c[n] for c in comps) for n in "uvwb"}
+        m.diag_opt_balance(opt)
+        obal = m.get_fields(PS3D_FIELDS_BALANCED)
+        got_b = _fields_file(tmp_path / f"balance_{itt:09d}.bin", p, 4)
+        got_o = _fields_file(tmp_path / f"opt_balance_{itt:09d}.bin", p, 4)
+        for n in "uvwb":
+            assert rel(got_b[n], bal[n]) < 1e-13, (itt, "balance", n)
+            assert rel(got_o[n], obal[n]) < 1e-13, (itt, "opt_balance", n)
+    m.close()
