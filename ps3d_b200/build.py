@@ -42,7 +42,7 @@ def build_driver(force=False):
         return DRIVER
     tmp = DRIVER + ".tmp"
     subprocess.run(["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I" + os.path.join(ROOT, "include"),
-                    DRIVER_SRC, "-o", tmp, "-L" + HERE, "-lps3d_gpu", "-Wl,-rpath,$ORIGIN"], check=True)
+                    DRIVER_SRC, "-o", tmp, "-L" + HERE, "-lps3d_gpu", "-ldl", "-Wl,-rpath,$ORIGIN"], check=True)
     os.replace(tmp, DRIVER)
     return DRIVER
 

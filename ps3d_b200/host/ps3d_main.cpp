@@ -13,6 +13,13 @@
 //                      u, v, w, b (optionally p) in the halo layout, float64
 //                      little-endian, x fastest; w is then zeroed on the
 //                      rigid-lid levels as main.f90:119-122
+// set_forcing          the hook integrate.f90:82 calls, through ps3d_set_forcing:
+//                      forcing_wavemaker = path of u_r, v_r, w_r, b_r, u_i, v_i,
+//                      w_i, b_i (halo layout) with omega_forc (config.f90:224-237);
+//                      forcing_background = path of u_back, b_back
+//                      (lee_wave1.f90:245-312); forcing_plugin = lib.so:symbol,
+//                      a ps3d_forcing_fn for any other forcing, loaded with
+//                      dlopen in place of a compiled-in set_forcing
 // read_restart         restart = path (default restart_pe=000000000.dta, the
 //                      reference's one-rank file name): read when it exists,
 //                      runlen += its time (restart.f90:27-82)
@@ -39,6 +46,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <dlfcn.h>
 #include <functional>
 #include <map>
 #include <string>
@@ -58,6 +66,8 @@ struct Run {
     bool diag_opt_balance = false;
     ps3d_optbal opt{1.0, 1.0, 100, 1, 1e-9, 0, 0};         // main_module.f90:23-29
     std::string init = "rest";
+    std::string forcing_wavemaker, forcing_background, forcing_plugin;
+    double omega_forc = 0.0;
     std::string restart = "restart_pe=000000000.dta";
     bool write_restart = true;
     std::string outdir = ".";
@@ -171,6 +181,10 @@ const std::map<std::string, Setter>& setters() {
         };
         s["opt_balance_tol"] = [](Run& r, const std::string& k, const std::string& v) { r.opt.tol = to_double(k, v); };
         s["init"] = [](Run& r, const std::string&, const std::string& v) { r.init = v; };
+        s["forcing_wavemaker"] = [](Run& r, const std::string&, const std::string& v) { r.forcing_wavemaker = v; };
+        s["forcing_background"] = [](Run& r, const std::string&, const std::string& v) { r.forcing_background = v; };
+        s["forcing_plugin"] = [](Run& r, const std::string&, const std::string& v) { r.forcing_plugin = v; };
+        s["omega_forc"] = [](Run& r, const std::string& k, const std::string& v) { r.omega_forc = to_double(k, v); };
         s["restart"] = [](Run& r, const std::string&, const std::string& v) { r.restart = v; };
         s["write_restart"] = [](Run& r, const std::string& k, const std::string& v) { r.write_restart = to_bool(k, v); };
         s["outdir"] = [](Run& r, const std::string&, const std::string& v) { r.outdir = v; };
@@ -291,27 +305,69 @@ void write_fields(const Run& r, const char* stem, int itt, double time, const st
     if (std::fclose(f) != 0 || !ok) halt("error writing " + path);
 }
 
+// fields in the halo layout from a raw file holding one of `counts` fields;
+// returns how many it held
+int read_fields(const Run& r, const std::string& path, const char* what, std::initializer_list<int> counts,
+                std::vector<std::vector<double>>& f) {
+    const size_t n = halo_points(r.p);
+    FILE* fh = std::fopen(path.c_str(), "rb");
+    if (!fh) halt(std::string("cannot open ") + what + " " + path);
+    std::fseek(fh, 0, SEEK_END);
+    const long bytes = std::ftell(fh);
+    std::fseek(fh, 0, SEEK_SET);
+    int nf = 0;
+    std::string want;
+    for (int c : counts) {
+        if (bytes == (long)(c * n * sizeof(double))) nf = c;
+        want += (want.empty() ? "" : " or ") + std::to_string(c * n * sizeof(double));
+    }
+    if (!nf) halt(std::string(what) + " " + path + ": " + std::to_string(bytes) + " bytes, expected " + want);
+    if ((int)f.size() < nf) f.resize(nf, std::vector<double>(n, 0.0));
+    for (int q = 0; q < nf; ++q)
+        if (std::fread(f[q].data(), sizeof(double), n, fh) != n) halt("short read of " + path);
+    std::fclose(fh);
+    return nf;
+}
+
+// set_forcing (integrate.f90:82) through ps3d_set_forcing; the host arrays
+// are copied to the device during the call
+void set_forcing(const Run& r, ps3d_ctx* ctx) {
+    ps3d_forcing fc{};
+    std::vector<std::vector<double>> wm, bg;
+    if (!r.forcing_wavemaker.empty()) {
+        read_fields(r, r.forcing_wavemaker, "wavemaker forcing (u_r, v_r, w_r, b_r, u_i, v_i, w_i, b_i)", {8}, wm);
+        fc.kind |= PS3D_FORCE_WAVEMAKER;
+        fc.omega = r.omega_forc;
+        fc.u_r = wm[0].data(); fc.v_r = wm[1].data(); fc.w_r = wm[2].data(); fc.b_r = wm[3].data();
+        fc.u_i = wm[4].data(); fc.v_i = wm[5].data(); fc.w_i = wm[6].data(); fc.b_i = wm[7].data();
+    }
+    if (!r.forcing_background.empty()) {
+        read_fields(r, r.forcing_background, "background flow (u_back, b_back)", {2}, bg);
+        fc.kind |= PS3D_FORCE_BACKGROUND;
+        fc.u_back = bg[0].data(); fc.b_back = bg[1].data();
+    }
+    if (!r.forcing_plugin.empty()) {
+        const size_t c = r.forcing_plugin.rfind(':');
+        if (c == std::string::npos || c == 0 || c + 1 == r.forcing_plugin.size())
+            halt("forcing_plugin wants library:symbol, got " + r.forcing_plugin);
+        const std::string lib = r.forcing_plugin.substr(0, c), sym = r.forcing_plugin.substr(c + 1);
+        void* h = dlopen(lib.c_str(), RTLD_NOW | RTLD_LOCAL);   // kept open for the run
+        if (!h) halt("cannot load forcing plugin " + lib + ": " + dlerror());
+        void* fn = dlsym(h, sym.c_str());
+        if (!fn) halt("forcing plugin " + lib + " has no symbol " + sym);
+        fc.kind |= PS3D_FORCE_CALLBACK;
+        fc.fn = reinterpret_cast<ps3d_forcing_fn>(fn);
+        fc.user = nullptr;
+    }
+    if (fc.kind) check(ps3d_set_forcing(ctx, &fc), "ps3d_set_forcing");
+}
+
 // set_initial_conditions: a rest state or the fields of a file
 void initial_conditions(const Run& r, std::vector<std::vector<double>>& f, bool& have_p) {
     const size_t n = halo_points(r.p);
     f.assign(5, std::vector<double>(n, 0.0));
     have_p = false;
-    if (lower(r.init) != "rest") {
-        FILE* fh = std::fopen(r.init.c_str(), "rb");
-        if (!fh) halt("cannot open initial conditions " + r.init);
-        std::fseek(fh, 0, SEEK_END);
-        const long bytes = std::ftell(fh);
-        std::fseek(fh, 0, SEEK_SET);
-        const long want4 = (long)(4 * n * sizeof(double)), want5 = (long)(5 * n * sizeof(double));
-        if (bytes != want4 && bytes != want5)
-            halt("initial conditions " + r.init + ": " + std::to_string(bytes) + " bytes, expected " +
-                 std::to_string(want4) + " (u, v, w, b) or " + std::to_string(want5) + " (and p)");
-        const int nf = bytes == want5 ? 5 : 4;
-        for (int q = 0; q < nf; ++q)
-            if (std::fread(f[q].data(), sizeof(double), n, fh) != n) halt("short read of " + r.init);
-        std::fclose(fh);
-        have_p = nf == 5;
-    }
+    if (lower(r.init) != "rest") have_p = read_fields(r, r.init, "initial conditions (u, v, w, b[, p])", {4, 5}, f) == 5;
     if (r.p.enable_vertical_boundaries) {   // main.f90:119-122: w(:,:,1-onx:0) = 0, w(:,:,nz:nz+onx) = 0
         const size_t plane = (size_t)(r.p.nx + 4) * (r.p.ny + 4);
         std::vector<double>& w = f[2];
@@ -385,6 +441,7 @@ int main(int argc, char** argv) {
     ps3d_ctx* ctx = nullptr;
     if (!r.dry_run) {
         check(ps3d_create(&p, r.device, &ctx), "ps3d_create");   // allocate_main_module, wavenumber_initialisation
+        set_forcing(r, ctx);
         std::printf(" setting initial conditions \n");
         std::vector<std::vector<double>> f;
         bool have_p = false;

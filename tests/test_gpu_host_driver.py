@@ -8,7 +8,9 @@ and the snapshot at itt = 6 (the state after the integrate of itt = 6, i.e.
 prints at itt = 4 the oracle's diagnose.  A second run in the same directory
 reads that restart file, extends runlen by its time (restart.f90:51-53) and
 continues to 24 steps.  A third run writes diag_balance and diag_opt_balance
-outputs, checked against the same library calls through the Python binding."""
+outputs, checked against the same library calls through the Python binding.
+The forcing options: wavemaker and background-flow files against the same
+forcing through the Python binding, and a user plugin loaded with dlopen."""
 import os
 import re
 import struct
@@ -187,3 +189,96 @@ def test_driver_balance_outputs(tmp_path):
             assert rel(got_b[n], bal[n]) < 1e-13, (itt, "balance", n)
             assert rel(got_o[n], obal[n]) < 1e-13, (itt, "opt_balance", n)
     m.close()
+
+
+def _par_args(p, runlen_steps, tmp_path, init, extra=()):
+    return [f"nx={p.nx}", f"ny={p.ny}", f"nz={p.nz}", f"Lx={p.Lx!r}", f"Ly={p.Ly!r}", f"Lz={p.Lz!r}",
+            f"dt={p.dt!r}", f"f0={p.f0!r}", f"N0={p.N0!r}", f"Ah={p.Ah!r}", f"Av={p.Av!r}",
+            f"enable_vertical_boundaries={p.enable_vertical_boundaries}",
+            f"enable_AB_3_order={p.enable_AB_3_order}", f"runlen={runlen_steps * p.dt!r}",
+            f"tsmonint={1000 * p.dt!r}", f"init={init}", f"outdir={tmp_path}", *extra]
+
+
+def test_driver_wavemaker_and_background_forcing(tmp_path):
+    """set_forcing of the lee-wave case (config.f90:224-237 wavemaker,
+    lee_wave1.f90:245-312 background flow) from files, against the same
+    forcing installed through the Python binding."""
+    from ps3d_b200.model import Model
+    build.build()
+    p = cf.lee_wave_params(32, 16, 16)
+    fr = cf.lee_wave_forcing(p, seed=2)
+    zero = cf.empty_field(p)
+    init = tmp_path / "init.bin"
+    np.concatenate([zero.ravel()] * 4).astype("<f8").tofile(init)
+    wm = tmp_path / "wavemaker.bin"
+    names = ("u_r", "v_r", "w_r", "b_r", "u_i", "v_i", "w_i", "b_i")
+    np.concatenate([np.ascontiguousarray(fr.get(n, zero), dtype="<f8").ravel() for n in names]).tofile(wm)
+    bg = tmp_path / "background.bin"
+    np.concatenate([np.ascontiguousarray(fr[n], dtype="<f8").ravel() for n in ("u_back", "b_back")]).tofile(bg)
+    args = _par_args(p, 10, tmp_path, init, [f"forcing_wavemaker={wm}", f"omega_forc={fr['omega']!r}",
+                                             f"forcing_background={bg}"])
+    r = subprocess.run([build.DRIVER, *args], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    itt, got = _restart_fields(tmp_path / "restart_pe=000000000.dta", p)
+    assert itt == 10
+
+    from ps3d_b200 import abi
+    m = Model(p)
+    m.set_forcing(abi.PS3D_FORCE_WAVEMAKER | abi.PS3D_FORCE_BACKGROUND, omega=fr["omega"], w_r=fr["w_r"],
+                  w_i=fr["w_i"], u_back=fr["u_back"], b_back=fr["b_back"])
+    m.upload(**{n: zero for n in "uvwb"})
+    m.run(10)
+    ref = m.download(tendencies=False)
+    m.close()
+    assert np.abs(ref["w"]).max() > 0.0
+    err = {n: rel(got[n], ref[n]) for n in NAMES}
+    assert max(err.values()) < 1e-13, err
+
+
+PLUGIN = r"""
+#include "ps3d_gpu.h"
+/* a set_forcing that adds nothing; fails at itt = 3 when built with FAIL */
+int my_forcing(void* user, const ps3d_device_view* v) {
+    (void)user;
+    if (v->nx != 32 || v->ny != 32 || v->nz != 16 || !(v->dt > 0) || !v->u || !v->du || !v->stream) return -2;
+#ifdef FAIL
+    if (v->itt == 3) return -2;
+#endif
+    return 0;
+}
+"""
+
+
+def test_driver_forcing_plugin(tmp_path):
+    """forcing_plugin = lib.so:symbol: the callback runs inside every step (a
+    no-op callback leaves the oracle's trajectory), and its error status
+    stops the run with 99."""
+    build.build()
+    p, f, _ = _setup(tmp_path)
+    init = tmp_path / "init.bin"
+    src = tmp_path / "plugin.c"
+    src.write_text(PLUGIN)
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    libs = {}
+    for tag, flags in (("ok", []), ("fail", ["-DFAIL"])):
+        libs[tag] = tmp_path / f"libforce_{tag}.so"
+        subprocess.run(["gcc", "-shared", "-fPIC", "-O2", "-I" + inc, *flags, str(src), "-o", str(libs[tag])],
+                       check=True)
+    r = subprocess.run([build.DRIVER, *_par_args(p, 8, tmp_path, init, [f"forcing_plugin={libs['ok']}:my_forcing"])],
+                       capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    itt, got = _restart_fields(tmp_path / "restart_pe=000000000.dta", p)
+    assert itt == 8
+    o8 = _oracle_after(p, f, 8)
+    err = {n: rel(got[n], o8.field(n)) for n in NAMES}
+    assert max(err.values()) < TOL64, err
+
+    os.remove(tmp_path / "restart_pe=000000000.dta")
+    r = subprocess.run([build.DRIVER, *_par_args(p, 8, tmp_path, init,
+                                                 [f"forcing_plugin={libs['fail']}:my_forcing"])],
+                       capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 99
+    assert "ps3d_integrate" in r.stderr
+    r = subprocess.run([build.DRIVER, *_par_args(p, 8, tmp_path, init, [f"forcing_plugin={libs['ok']}:nothing"])],
+                       capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 99 and "has no symbol nothing" in r.stderr
