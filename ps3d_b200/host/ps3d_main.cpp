@@ -3,6 +3,7 @@
 // compiler.  It uses nothing but that header: no CUDA headers, no torch.
 //
 //   ps3d_main [--dry-run] [parameter file] [key=value ...]
+//   ps3d_main --help        the accepted keys
 //
 // set_parameter        a parameter file of `key = value` lines ('!' and '#'
 //                      start comments; Fortran 1d-3 exponents and .true. /
@@ -231,6 +232,17 @@ Run set_parameter(int argc, char** argv) {
     r.p.precision = PS3D_FP64;
     for (int a = 1; a < argc; ++a) {
         const std::string s = argv[a];
+        if (s == "--help" || s == "-h") {
+            std::printf("usage: %s [--dry-run] [parameter file] [key=value ...]\nkeys:", argv[0]);
+            int col = 0;
+            for (const auto& kv : setters()) {
+                if (col % 4 == 0) std::printf("\n ");
+                std::printf(" %-28s", kv.first.c_str());
+                ++col;
+            }
+            std::printf("\n");
+            std::exit(0);
+        }
         if (s == "--dry-run") r.dry_run = true;
         else if (s.find('=') != std::string::npos) set_one(r, s, "argument " + std::to_string(a));
         else read_parameter_file(r, argv[a]);

@@ -113,3 +113,12 @@ def test_driver_uses_only_the_c_abi(driver):
     assert not [i for i in includes if "cuda" in i or "torch" in i]
     out = subprocess.run(["ldd", driver], capture_output=True, text=True).stdout
     assert "libps3d_gpu.so" in out
+
+
+def test_help_lists_every_key(driver):
+    out = _run(driver, ["--help"]).stdout
+    for key in ("nx", "lx", "dt", "n0", "ah", "enable_vertical_boundaries", "enable_ab_3_order", "precision",
+                "runlen", "tsmonint", "snapint", "enable_diag_snap", "enable_diag_balance",
+                "enable_diag_opt_balance", "opt_balance_period", "opt_balance_max_itts", "init", "restart",
+                "forcing_wavemaker", "forcing_background", "forcing_plugin", "omega_forc", "outdir", "profile"):
+        assert re.search(r"\b" + key + r"\b", out), key
