@@ -433,7 +433,11 @@ def main():
     hname = "mixed" if "mixed" in res else "fp64" if "fp64" in res else "mixed_refined"
     head = res[hname]
     dom_name, dom_v = max(head["roof"].items(), key=lambda kv: kv[1]["ms_total"])
-    launches = sum(n for _, n in head["kern"].values())
+    # kernels per library call of each class: the split transforms (rows +
+    # y-lines passes) launch two kernels per call, the cluster ones one
+    split = "plane_impl=cluster" not in head["desc"]
+    per_call = {"fft_fwd": 2 if split else 1, "fft_inv": 2 if split else 1}
+    launches = sum(n * per_call.get(k, 1) for k, (_, n) in head["kern"].items())
     line = {"metric": metric, "value": head["value"], "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_max"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
