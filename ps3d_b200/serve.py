@@ -7,7 +7,6 @@ their own CUDA streams.  `replay_poisson` drives a seeded Poisson arrival
 process against a server and reports latency percentiles and throughput.
 """
 import ctypes as C
-import threading
 import time
 
 import numpy as np

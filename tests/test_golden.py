@@ -8,7 +8,6 @@ import os
 import numpy as np
 import pytest
 
-from ps3d_b200 import abi
 from ps3d_b200 import configs as cf
 from tests.golden.make_golden import CASES, make
 from tests.helpers import FIELDS, rel, small_params

@@ -7,7 +7,6 @@ arithmetic per level and per column is the same, so the tolerance is the
 single-kernel one.  Ranks run as contexts of one process on one GPU, moved
 between by device copies (ps3d_slab_group_step); no kernel waits on another.
 """
-import os
 
 import numpy as np
 import pytest
