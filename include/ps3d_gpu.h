@@ -161,7 +161,10 @@ PS3D_API int ps3d_integrate(ps3d_ctx* ctx, int nsteps);
 PS3D_API int ps3d_set_step_params(ps3d_ctx* ctx, double dt, double Ro,
                          double Ahbi, double Avbi, double Khbi, double Kvbi);
 
-/* pressure_solver (pressure_solver.f90:2-120) on the current device state.  */
+/* pressure_solver (pressure_solver.f90:2-120) on the current device state.
+ * The mixed paths solve from scratch here (a full FP32 solve and one
+ * FP64-residual refinement): only the time step's solve starts from the
+ * previous step's pressure.                                                 */
 PS3D_API int ps3d_pressure_solve(ps3d_ctx* ctx);
 
 /* Normal-mode projections on the device state:
