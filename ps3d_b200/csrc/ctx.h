@@ -196,8 +196,11 @@ struct Ctx {
     int advance(int nsteps, bool allow_graph);
     bool graphable() const;
     int capture_graph();
-    // the state, p or the parameters changed outside the time loop
-    void invalidate_graph() { ++version; p_warm = false; }
+    // parameters changed outside the time loop: captured graphs are stale
+    void invalidate_graph() { ++version; }
+    // the state or p replaced outside the time loop: graphs are stale, and p
+    // no longer holds the previous step's pressure of this trajectory
+    void state_replaced() { ++version; p_warm = false; }
     int step(int itt, int tau, int taum1, int taum2);
     int poisson_once(double* out, double beta, bool lazy = false, const double* pc = nullptr);
     int pressure_solve(bool lazy = false, bool warm = false);

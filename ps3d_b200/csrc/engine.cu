@@ -1127,7 +1127,7 @@ int Ctx::reset_request() {
     pending = false; pcor = nullptr; dtp = 0.0;
     for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(tend[f].p, 0, tend[f].bytes, stream));
     CK(cudaMemsetAsync(p.p, 0, p.bytes, stream));
-    invalidate_graph();
+    state_replaced();
     return PS3D_OK;
 }
 
@@ -1228,7 +1228,7 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     P.Ro = Ro_loc; P.dt = dt_loc;
     P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
     tau = tau_loc; taum1 = taum1_loc; taum2 = taum2_loc; itt = itt_loc;
-    invalidate_graph();
+    state_replaced();
     if (rc) return rc;
     if (O.adopt) CK(copy_set_to_state(PS3D_FIELDS_BALANCED));
     CK(cudaStreamSynchronize(stream));

@@ -129,7 +129,7 @@ int Ctx::read_restart(const char* path, double* time_out) {
     if (!read_record(F.f, {{h.data(), h.size() * sizeof(double)}})) return PS3D_ERR_BADPARAM;
     int rc = materialize();
     if (rc) return rc;
-    invalidate_graph();
+    state_replaced();
     pending = false;
     for (int q = 0; q < 4; ++q) if ((rc = upload_field(field(q), h.data() + q * n3))) return rc;
     if ((rc = upload_field((double*)p.p, h.data() + 4 * n3))) return rc;

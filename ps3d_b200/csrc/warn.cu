@@ -312,7 +312,7 @@ int Ctx::model_run(int in, int out, int max_steps) {
     for (int f = 0; f < 4; ++f)
         CK(cudaMemcpyAsync(tend[f].p, saved_tend[f].p, 3 * N * tsz(f), cudaMemcpyDeviceToDevice, stream));
     tau = tau_loc; taum1 = taum1_loc; taum2 = taum2_loc; itt = itt_loc;
-    invalidate_graph();
+    state_replaced();
     return rc;
 }
 

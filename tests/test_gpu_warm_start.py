@@ -61,41 +61,51 @@ def test_solves_per_step(precision, first, later):
     m.close()
 
 
-def _run(p, f, nsteps, cold_every_step=False):
+def _run(p, f, nsteps):
     m = Model(p)
     m.upload(**{n: f[n] for n in "uvwb"})
-    if cold_every_step:
-        for _ in range(nsteps):
-            m.set_step_params(p.dt, p.Ro)   # unchanged values; resets the warm start
-            m.run(1)
-    else:
-        m.run(nsteps)
+    m.run(nsteps)
     s = m.download(tendencies=False)
     m.close()
     return s
 
 
 def test_warm_start_matches_refined_solves():
-    """60 steps warm (graphs included) against PS3D_MIXED_REFINED and against
-    PS3D_MIXED started cold at every step: the step's change of p rounded to
-    FP32 moves the fields by < 1e-6 (w, whose buoyancy and pressure terms
-    nearly cancel, the most); the refined projection leaves the divergence at
-    FP64 roundoff, the warm one at the FP32 rounding of the change of p."""
+    """60 steps warm (graphs included) against PS3D_MIXED_REFINED: the step's
+    change of p rounded to FP32 moves the fields by < 1e-6 (w, whose
+    buoyancy and pressure terms nearly cancel, the most); the refined
+    projection leaves the divergence at FP64 roundoff, the warm one at the
+    FP32 rounding of the change of p."""
     p, f = _eddy()
     pr = p.copy()
     pr.precision = abi.PS3D_MIXED_REFINED
     sw = _run(p, f, 60)
     sr = _run(pr, f, 60)
-    sc = _run(p, f, 60, cold_every_step=True)
-    for other in (sr, sc):
-        err = {n: rel(_interior(sw[n]), _interior(other[n])) for n in NAMES}
-        assert max(err.values()) < 1e-6, err
-    # a cold PS3D_MIXED step is a PS3D_MIXED_REFINED step
-    err = {n: rel(_interior(sc[n]), _interior(sr[n])) for n in NAMES}
-    assert max(err.values()) < 1e-13, err
+    err = {n: rel(_interior(sw[n]), _interior(sr[n])) for n in NAMES}
+    assert max(err.values()) < 1e-6, err
     scale = np.abs(_interior(sr["u"])).max() / p.dx
     assert np.abs(_div(p, sr)).max() < 1e-9 * scale
     assert np.abs(_div(p, sw)).max() < 4e-6 * scale
+
+
+def test_step_parameters_keep_the_warm_start():
+    """The drop-in integrate sets the step parameters before every ps3d_step
+    (the balance drivers ramp them); new parameters do not replace the state,
+    so the mixed path stays warm: one forward transform per step after the
+    first, and the trajectory of ps3d_integrate."""
+    p, f = _eddy()
+    m = Model(p)
+    m.upload(**{n: f[n] for n in "uvwb"})
+    m.profile(True)
+    for _ in range(6):
+        m.set_step_params(p.dt, p.Ro)
+        m.run(1)
+    assert m.profile_read()["fft_fwd"][1] == 2 + 5
+    s1 = m.download(tendencies=False)
+    m.close()
+    s2 = _run(p, f, 6)
+    err = {n: rel(_interior(s1[n]), _interior(s2[n])) for n in NAMES}
+    assert max(err.values()) < 1e-13, err
 
 
 def test_uploaded_pressure_does_not_leak():
