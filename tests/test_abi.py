@@ -82,3 +82,18 @@ def test_model_fails_loudly_without_gpu(lib_path):
     from tests.helpers import small_params
     with pytest.raises(PS3DError):
         Model(small_params())
+
+
+def test_constants_match_header():
+    """Every numeric #define PS3D_* of the header that the Python mirror
+    (ps3d_b200/abi.py) also names has the same value there."""
+    text = open(HEADER).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(PS3D_\w+)\s+(-?\d+)\b", text)}
+    assert "PS3D_MIXED_REFINED" in defs and "PS3D_ERR_TOOLARGE" in defs
+    shared = [k for k in defs if hasattr(abi, k)]
+    assert len(shared) >= 20, shared
+    bad = {k: (defs[k], getattr(abi, k)) for k in shared if getattr(abi, k) != defs[k]}
+    assert not bad, bad
+    for k in ("PS3D_FP64", "PS3D_MIXED", "PS3D_MIXED_REFINED", "PS3D_OK", "PS3D_ERR_NONFINITE",
+              "PS3D_PROJ_NORMAL_MODE", "PS3D_FIELDS_BALANCED", "PS3D_FORCE_CALLBACK"):
+        assert k in shared, k
