@@ -97,3 +97,20 @@ def test_constants_match_header():
     for k in ("PS3D_FP64", "PS3D_MIXED", "PS3D_MIXED_REFINED", "PS3D_OK", "PS3D_ERR_NONFINITE",
               "PS3D_PROJ_NORMAL_MODE", "PS3D_FIELDS_BALANCED", "PS3D_FORCE_CALLBACK"):
         assert k in shared, k
+
+
+def test_phase_and_kernel_class_mirrors():
+    """The slab phases (ps3d_b200/slab.py PHASE) and the profile's kernel
+    classes (Model.KERNELS, indexed by PS3D_K_*) match the header."""
+    from ps3d_b200.model import Model
+    from ps3d_b200.slab import PHASE
+    text = open(HEADER).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(PS3D_\w+)\s+(-?\d+)\b", text)}
+    for name, v in PHASE.items():
+        assert defs["PS3D_SLAB_" + name.upper()] == v, name
+    assert len(PHASE) == len([k for k in defs if k.startswith("PS3D_SLAB_")])
+    names = {"step": "STEP", "fft_fwd": "FFT_FWD", "vsolve": "VSOLVE", "fft_inv": "FFT_INV",
+             "correct": "CORRECT", "other": "OTHER"}
+    for i, k in enumerate(Model.KERNELS):
+        assert defs["PS3D_K_" + names[k]] == i, k
+    assert defs["PS3D_K_COUNT"] == len(Model.KERNELS)
