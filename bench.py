@@ -14,8 +14,14 @@ oracle restatement timed on this host's cores.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 (torchrun): every rank runs an independent replica on its own GPU
-(a single grid does not shard here); value = all ranks' grid-point-steps over
-the slowest rank's time.
+(weak scaling; the z-slab decomposition of one grid is exercised by its own
+tests, not here); value = all ranks' grid-point-steps over the slowest
+rank's time.
+
+`value` is the median of five windows of exactly K steps each, replayed as
+CUDA graphs with per-kernel profiling off (what a user's ps3d_integrate
+runs); the per-kernel breakdown and the roofline come from a separate pass
+of K steps with an event pair around every launch.
 """
 import argparse
 import json
@@ -43,7 +49,7 @@ def set_grid(nx, ny, nz):
 # DRAM bytes per grid point per launch of the step kernel, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) at 256x256x64, where its
 # traffic already streams far beyond L2, so it scales with the grid points;
-# commands and tables in profiles/hot_kernels_{fp64,mixed}_256x256x64.md.
+# the ncu commands that produced these figures are kept with the profiles.
 MEASURED_TRAFFIC_PER_POINT = {
     "fp64": {"step": 165.8},
     "mixed": {"step": 128.4},
@@ -167,8 +173,10 @@ def barrier(pg, dev):
     torch.cuda.synchronize(dev)
 
 
-def time_path(precision, steps, warmup, dev, pg):
-    """Warm up, then time exactly `steps` steps with CUDA events on the engine's stream."""
+def time_path(precision, steps, warmup, dev, pg, windows=5):
+    """Warm up, then time `windows` windows of exactly `steps` steps with CUDA
+    events on the engine's stream (graph replay, no profiling; median), then
+    one profiled pass of `steps` steps for the per-kernel breakdown."""
     import torch
     from ps3d_b200 import configs as cf
     from ps3d_b200.model import Model
@@ -187,20 +195,26 @@ def time_path(precision, steps, warmup, dev, pg):
     stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    m.profile(True)
+    times = []
+    for _ in range(windows):
+        barrier(pg, dev)
+        ev0.record(stream)
+        m.enqueue(steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1))
     barrier(pg, dev)
-    ev0.record(stream)
+    ms = float(np.median(times))
+    # per-kernel breakdown: eager launches, an event pair around each
+    m.profile(True)
     m.enqueue(steps)
-    ev1.record(stream)
-    ev1.synchronize()
     kern = m.profile_read()
     m.profile(False)
-    ms = ev0.elapsed_time(ev1)
     try:
         diag = list(m.diagnose())
     except Exception as e:   # non-finite state: reported, not hidden
         diag = str(e)
-    state = m.download(tendencies=False)   # after warmup + exactly `steps` steps
+    state = m.download(tendencies=False)   # after warmup + (windows + 1) x `steps` steps
     t_s = time.perf_counter()
     while time.perf_counter() - t_s < 0.5:   # keep the GPU loaded while the sampler catches up
         m.run(3)
@@ -208,7 +222,7 @@ def time_path(precision, steps, warmup, dev, pg):
     clk["diagnose_after_timed"] = diag
     barrier(pg, dev)
     ms_max = max_over_ranks(ms, pg, dev)
-    return m, p, ms, ms_max, kern, clk, state, m.describe()
+    return m, p, ms, ms_max, kern, clk, state, m.describe(), times
 
 
 def e2e_run(precision, steps, dev):
@@ -277,11 +291,13 @@ ENS_SIZES = [(32, 32, 16), (64, 64, 32), (128, 64, 32), (128, 128, 64)]
 
 def ensemble_run(dev, pg, world, n_members=256, steps=200, seed=3):
     """Batched ensemble: 256 eddies, sizes drawn by seed from ENS_SIZES,
-    amplitudes U(0.05, 0.2) m/s, mixed precision, `steps` steps, all members
-    in batched launches replayed as CUDA graphs.  Compared with the same
-    members stepped one at a time on the plain FP64 path (timed on one member
-    per size class and summed over the members).  With N ranks each rank runs
-    its own ensemble (weak scaling)."""
+    amplitudes U(0.05, 0.2) m/s, `steps` steps, all members in batched
+    launches replayed as CUDA graphs, in mixed precision and in FP64.
+    Compared with the same members stepped one at a time on the plain FP64
+    path: every member measured, one context per size class, the member's
+    state uploaded and 3 steps run untimed (graph capture), then `steps`
+    steps replayed as CUDA graphs and timed with events.  With N ranks each
+    rank runs its own ensemble (weak scaling)."""
     import torch
     from ps3d_b200 import abi
     from ps3d_b200 import configs as cf
@@ -290,53 +306,113 @@ def ensemble_run(dev, pg, world, n_members=256, steps=200, seed=3):
     rng = np.random.default_rng(seed)
     picks = rng.integers(0, len(ENS_SIZES), n_members)
     amps = rng.uniform(0.05, 0.2, n_members)
-    members = [cf.eddy_params(*ENS_SIZES[k], precision=abi.PS3D_MIXED) for k in picks]
     fields = {}
-    ens = Ensemble(members, device=dev)
-    for i, (k, a) in enumerate(zip(picks, amps)):
-        key = int(k)
-        if key not in fields:
-            p = members[i]
-            fields[key] = cf.add_noise(p, cf.eddy_fields(p, amp=1.0), "b", rel=1e-3, seed=0)
-        f = fields[key]
-        ens.upload(i, f["u"] * a, f["v"] * a, f["w"] * a, f["b"] * a)
-    ens.integrate(3)
-    info0 = ens.info()
-    stream = torch.cuda.ExternalStream(info0["stream"], device=f"cuda:{dev}")
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(pg, dev)
-    e0.record(stream)
-    ens.enqueue(steps)
-    e1.record(stream)
-    e1.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1), pg, dev)
-    launches = ens.info()["launches"] - info0["launches"]
-    pts = sum(int(np.prod(ENS_SIZES[k])) for k in picks)
-    ens.close()
-    # serial plain FP64: one member per size class, same number of steps
-    rate = {}
     for k in sorted(set(int(x) for x in picks)):
         p = cf.eddy_params(*ENS_SIZES[k])
-        f = fields[k]
+        fields[k] = cf.add_noise(p, cf.eddy_fields(p, amp=1.0), "b", rel=1e-3, seed=0)
+    pts = sum(int(np.prod(ENS_SIZES[k])) for k in picks)
+
+    def batched(prec):
+        members = [cf.eddy_params(*ENS_SIZES[k], precision=prec) for k in picks]
+        ens = Ensemble(members, device=dev)
+        for i, (k, a) in enumerate(zip(picks, amps)):
+            f = fields[int(k)]
+            ens.upload(i, f["u"] * a, f["v"] * a, f["w"] * a, f["b"] * a)
+        ens.integrate(3)
+        info0 = ens.info()
+        stream = torch.cuda.ExternalStream(info0["stream"], device=f"cuda:{dev}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(pg, dev)
+        e0.record(stream)
+        ens.enqueue(steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), pg, dev)
+        launches = ens.info()["launches"] - info0["launches"]
+        ens.close()
+        return ms, int(launches)
+
+    ms_mx, l_mx = batched(abi.PS3D_MIXED)
+    ms_64, l_64 = batched(abi.PS3D_FP64)
+    # serial plain FP64, every member
+    serial_ms = 0.0
+    per_size_ms = {}
+    for k in sorted(set(int(x) for x in picks)):
+        p = cf.eddy_params(*ENS_SIZES[k])
         m = Model(p, device=dev)
-        m.upload(**{n: f[n] * 0.1 for n in ("u", "v", "w", "b")})
-        m.run(3)
         st = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(st)
-        for _ in range(steps):
-            m.enqueue(1)
-        a1.record(st)
-        a1.synchronize()
-        rate[k] = a0.elapsed_time(a1) / steps   # ms per step, one member
+        f = fields[k]
+        tot = 0.0
+        for i in np.nonzero(picks == k)[0]:
+            a = amps[i]
+            m.upload(**{n: f[n] * a for n in ("u", "v", "w", "b")})
+            m.run(3)
+            a0.record(st)
+            m.enqueue(steps)
+            a1.record(st)
+            a1.synchronize()
+            tot += a0.elapsed_time(a1)
         m.close()
-    serial_ms = sum(rate[int(k)] * steps for k in picks)
+        per_size_ms[f"{ENS_SIZES[k][0]}x{ENS_SIZES[k][1]}x{ENS_SIZES[k][2]}"] = tot
+        serial_ms += tot
+    serial_ms = max_over_ranks(serial_ms, pg, dev)
     return {"members": n_members, "steps": steps, "sizes": [list(s) for s in ENS_SIZES],
             "members_per_size": [int((picks == k).sum()) for k in range(len(ENS_SIZES))],
-            "batched_value": world * pts * steps / (ms * 1e-3), "batched_ms": ms, "batched_launches": int(launches),
-            "serial_fp64_value": pts * steps / (serial_ms * 1e-3), "serial_fp64_ms_estimated": serial_ms,
-            "batched_over_serial_fp64": serial_ms / ms,
-            "note": "mixed precision batched (CUDA graphs) vs members stepped one at a time on the FP64 path"}
+            "batched_mixed_value": world * pts * steps / (ms_mx * 1e-3), "batched_mixed_ms": ms_mx,
+            "batched_mixed_launches": l_mx,
+            "batched_fp64_value": world * pts * steps / (ms_64 * 1e-3), "batched_fp64_ms": ms_64,
+            "batched_fp64_launches": l_64,
+            "serial_fp64_value": world * pts * steps / (serial_ms * 1e-3), "serial_fp64_ms": serial_ms,
+            "serial_fp64_ms_per_size": per_size_ms,
+            "batched_mixed_over_serial_fp64": serial_ms / ms_mx,
+            "batched_fp64_over_serial_fp64": serial_ms / ms_64,
+            "batched_mixed_over_batched_fp64": ms_64 / ms_mx,
+            "note": "all three arms measured over every member with CUDA graphs; the serial arm steps one member "
+                    "at a time (one context per size, state uploaded per member, 3 untimed steps first)"}
+
+
+def projection_run(dev, nx=256, ny=256, nz=64):
+    """normal_mode_projection (diag_opt_balance.f90:288-310) on a rigid-lid
+    eddy of the largest serving size: forward transform (4 plane FFTs + 4
+    vertical-mode transforms), eigen projection, backward transform.  Median
+    of 5 timed calls; the vertical-mode transform's FP64 roofline from a
+    profiled call (2 nz^2 flop per complex multiply-add, i.e. 4 nz^2 per
+    complex column, against the nominal 40 TFLOP/s FP64 of a B200)."""
+    import torch
+    from ps3d_b200 import configs as cf
+    from ps3d_b200.model import Model
+    p = cf.eddy_params(nx, ny, nz)
+    f = cf.eddy_fields(p)
+    m = Model(p, device=dev)
+    m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+    m.normal_mode_projection()
+    st = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t = []
+    for _ in range(5):
+        e0.record(st)
+        m.normal_mode_projection()
+        e1.record(st)
+        e1.synchronize()
+        t.append(e0.elapsed_time(e1))
+    m.profile(True)
+    m.normal_mode_projection()
+    kern = m.profile_read()
+    m.profile(False)
+    m.close()
+    ms_v, n_v = kern["vmode"]
+    ncol = (nx // 2 + 1) * ny
+    flop = 4.0 * nz * nz * ncol            # per launch
+    per = ms_v / max(n_v, 1)
+    peak_fp64 = 40.0
+    return {"grid": [nx, ny, nz], "ms_median": float(np.median(t)), "ms_windows": t,
+            "vmode": {"launches": int(n_v), "ms_per_launch": per, "flop_per_launch": flop,
+                      "achieved_tflops": flop / (per * 1e-3) / 1e12 if n_v else None,
+                      "peak_tflops": peak_fp64, "peak_kind": "nominal FP64 (no measured FP64 peak)",
+                      "frac": (flop / (per * 1e-3) / 1e12) / peak_fp64 if n_v else None,
+                      "bytes_per_launch": 2 * 16 * ncol * nz},
+            "kernels_ms": {k: v[0] for k, v in kern.items() if v[1]}}
 
 
 def serve_run(dev, n_requests=40, rate_hz=50.0, max_active=8):
@@ -372,6 +448,7 @@ def main():
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--ensemble", type=int, default=1, help="also run the batched-ensemble workload")
     ap.add_argument("--serve", type=int, default=1, help="also run the serving workload")
+    ap.add_argument("--projection", type=int, default=1, help="also time the normal-mode projection")
     args = ap.parse_args()
     set_grid(args.nx, args.ny, args.nz)
     unit = "grid-point-steps/s"
@@ -425,10 +502,10 @@ def main():
                              (("both", "mixed_refined"), abi.PS3D_MIXED_REFINED, "mixed_refined")):
         if args.case not in case:
             continue
-        m_, p_, ms_, msmax_, k_, clk_, st_, desc_ = time_path(prec, args.steps, args.warmup, dev, pg)
+        m_, p_, ms_, msmax_, k_, clk_, st_, desc_, win_ = time_path(prec, args.steps, args.warmup, dev, pg)
         m_.close()
         res[name] = {"p": p_, "ms_max": msmax_, "kern": k_, "clk": clk_, "state": st_, "desc": desc_,
-                     "value": world * npts * args.steps / (msmax_ * 1e-3),
+                     "value": world * npts * args.steps / (msmax_ * 1e-3), "windows_ms": win_,
                      "roof": roof(k_, name)}
     hname = "mixed" if "mixed" in res else "fp64" if "fp64" in res else "mixed_refined"
     head = res[hname]
@@ -453,11 +530,15 @@ def main():
                          "traffic_unit": "DRAM bytes per launch (ncu, scaled by grid points)",
                          "algorithmic_bytes": BYTES_PER_POINT[hname].get(dom_name, 0) * npts,
                          "peak_kind": peak_kind},
-            "gpu_launches": int(launches), "clocks": head["clk"]}
+            "gpu_launches": int(launches), "clocks": head["clk"],
+            "timing": {"value": "median of 5 windows of exactly `steps` steps, CUDA-graph replay, profiling off",
+                       "windows_ms": head["windows_ms"],
+                       "kernels": "separate pass of `steps` steps, eager launches with an event pair each",
+                       "profiled_ms_per_step": sum(v[0] for v in head["kern"].values()) / args.steps}}
     if "fp64" in res:
         r64 = res["fp64"]
         line["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms_max"] / args.steps, "kernels": r64["roof"],
-                        "kernel_config": r64["desc"], "clocks": r64["clk"]}
+                        "kernel_config": r64["desc"], "clocks": r64["clk"], "windows_ms": r64["windows_ms"]}
     def max_div(st, pp):
         u, v, w = st["u"], st["v"], st["w"]
         div = ((u[2:-2, 2:-2, 2:-2] - u[2:-2, 2:-2, 1:-3]) / pp.dx + (v[2:-2, 2:-2, 2:-2] - v[2:-2, 1:-3, 2:-2]) / pp.dy
@@ -490,6 +571,8 @@ def main():
                        "path": "public C ABI: upload, ps3d_step per step, diagnose every 10 steps, download"}
     if args.ensemble:
         line["ensemble"] = ensemble_run(dev, pg, world)
+    if args.projection:
+        line["projection"] = projection_run(dev)
     if args.serve:
         line["serving"] = serve_run(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

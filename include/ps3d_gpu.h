@@ -11,7 +11,8 @@
  * on an opaque context that owns the device-resident state.  Every entry point
  * takes plain pointers and sizes, returns an int status (0 = success, negative
  * = error) and never aborts or traps; a Fortran host binds them through
- * ISO_C_BINDING (interfaces are listed in INTEGRATION.md).
+ * ISO_C_BINDING: each entry point is a bind(C) interface with value and
+ * reference arguments matching the C types below.
  *
  * Host arrays use the reference's layout: real(8) fields are column-major,
  * x fastest, with two halo points on every side, i.e. Fortran bounds
@@ -44,7 +45,8 @@ extern "C" {
 #define PS3D_ERR_BADPARAM     -5  /* invalid argument, size or configuration        */
 #define PS3D_ERR_UNSUPPORTED  -6  /* valid in the reference, not built here         */
 #define PS3D_ERR_CANCELLED    -7  /* a serving request was cancelled                */
-#define PS3D_ERR_TOOLARGE     -8  /* grid exceeds ps3d_pressure_solve_noalloc's static scratch */
+#define PS3D_ERR_TOOLARGE     -8  /* grid exceeds a fixed limit: columns too tall for a block's
+                                       shared memory, or ps3d_pressure_solve_noalloc's static scratch */
 
 /* ---- parameters (for_src/main_module.f90:16-57) -------------------------- */
 typedef struct ps3d_params {
@@ -262,7 +264,8 @@ PS3D_API int ps3d_enqueue(ps3d_ctx* ctx, int nsteps);
 #define PS3D_K_FFT_INV  3   /* inverse plane FFT                            */
 #define PS3D_K_CORRECT  4   /* pressure-gradient correction                 */
 #define PS3D_K_OTHER    5   /* friction stages, forcing, projections, ...   */
-#define PS3D_K_COUNT    6
+#define PS3D_K_VMODE    6   /* vertical-mode transforms (rigid-lid projections) */
+#define PS3D_K_COUNT    7
 PS3D_API int ps3d_profile(ps3d_ctx* ctx, int enable);
 /* One-line description of the context's kernel configuration (grid,
  * precision, plane cluster shape, FFT stages, autotuner choice).          */
@@ -272,18 +275,22 @@ PS3D_API int ps3d_profile_read(ps3d_ctx* ctx, double* ms, long long* launches);
 /* ---- pressure projection without device allocation -----------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * when they need the projection (they own their device arrays through CUDA
- * Fortran, OpenACC or their own pool, must not allocate inside a locked or
- * captured region, or must keep a fixed device footprint): the same
- * computation as ps3d_pressure_solve (pressure_solver.f90:2-120, FP64) on the
- * caller's device arrays u, v, w (updated in place) and p (written), each
- * nx*ny*nz doubles, x fastest, interior points only, queued on `stream`
- * (a cudaStream_t, NULL for the default stream) and waited for.  The
- * spectral work array and the FFT tables are file-scope static device arrays
- * (about 16.1 MiB, held on every GPU that loads the library until exit):
- * (nx/2+1)*ny*nz must not exceed 1048576 and nx/2, ny, nz not 1024, else
- * PS3D_ERR_TOOLARGE.  The first call on a device looks up those arrays with
- * that device current; make it before any stream capture.  Every call
- * shares the arrays: calls that overlap on the GPU race.                    */
+ * Fortran, OpenACC or their own pool, hold a lock their allocator also
+ * takes, or must keep a fixed device footprint): the same computation as
+ * ps3d_pressure_solve (pressure_solver.f90:2-120, FP64) on the caller's
+ * device arrays u, v, w (updated in place) and p (written), each nx*ny*nz
+ * doubles, x fastest, interior points only, queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) and waited for: the call is
+ * synchronous, and cannot be captured in a CUDA graph.  It allocates no
+ * device memory: the spectral work array, the FFT tables and an error word
+ * are file-scope static device arrays (about 16.1 MiB, held on every GPU
+ * that loads the library until exit), and the host image of the tables is
+ * a static buffer.  (nx/2+1)*ny*nz must not exceed 1048576 and nx/2, ny, nz
+ * not 1024, and periodic grids nz not about 420 (the z transform's shared
+ * memory), else PS3D_ERR_TOOLARGE.  The first call on a device looks up the
+ * static arrays with that device current.  Calls from threads of one
+ * process are serialised by the library; calls from several processes that
+ * overlap on one GPU race on the arrays.                                   */
 PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, double* v, double* w, double* p,
                                          void* stream);
 

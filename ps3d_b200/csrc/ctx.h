@@ -111,7 +111,6 @@ struct Ctx {
     DevPlan plx, ply, plz;      // radix-16/8 schedules
     DevPlan plx4, ply4;         // radix-4 schedules (autotuner alternative)
     DevPlan plx8, ply8;         // radix-8 schedules (autotuner alternative)
-    DevBuf thomas_r;            // rigid lid: Thomas factors [k][column] (constant for the grid)
     int plane_force = -1;       // PS3D_PLANE_IMPL: -1 free, 0 cluster, 1 rows + y-lines
     int force_impl = -1;        // set before init: pins the plane implementation (z-slabs: 1)
     // z-slab of a larger grid (slab.cu): the step kernel advances levels

@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <new>
 #include <string>
@@ -193,8 +194,9 @@ static std::vector<PlaneArgs> plane_candidates(int nx, int ny, size_t es, const 
     return out;
 }
 
-// Default cluster shape of the plane kernels for one element size.
-static bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
+// Default cluster shape of the plane kernels for one element size (also the
+// shape of ps3d_pressure_solve_noalloc's plane kernels).
+bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a) {
     const int nxh = nx / 2 + 1;
     for (int pass = 0; pass < 2; ++pass) {
         const size_t limit = pass == 0 ? 110 * 1024 : kMaxSmem;
@@ -252,6 +254,10 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     if (!fft_length_ok(nx / 2) || !fft_length_ok(ny) || (!rigid && !fft_length_ok(nz))) return PS3D_ERR_BADPARAM;
     if (P.precision != PS3D_FP64 && !mixed) return PS3D_ERR_BADPARAM;
     if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0)) return PS3D_ERR_BADPARAM;
+    // columns too tall for the vertical solve's (or the projections' periodic
+    // z transform's) shared memory
+    if (rigid ? vsolve_tile_width(nz, mixed) == 0 || vsolve_tile_width(nz, false) == 0 : !zsolve_fits(nz, false))
+        return PS3D_ERR_TOOLARGE;
     if (cudaSetDevice(dev) != cudaSuccess) return PS3D_ERR_CUDA;
     if (use_stream) { stream = use_stream; own_stream = false; }
     else CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -259,6 +265,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     CK(plane_setup(false));
     CK(plane_setup(true));
     CK(step_setup());
+    CK(modes_setup());
     // state: 3 buffers per field (fused path ping-pongs two, the generic path needs three)
     for (int f = 0; f < 4; ++f)
         for (int q = 0; q < 3; ++q) { CK(state[f][q].alloc(NB * sizeof(double))); CK(cudaMemset(state[f][q].p, 0, NB * sizeof(double))); }
@@ -333,8 +340,18 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
                 A(psib, k, k2) = (A(psi, k, k2) + A(psi, k - 1, k2)) / cd;
             }
         }
-        CK(up(m_phi, phi.data(), phi.size() * 8)); CK(up(m_psi, psi.data(), psi.size() * 8));
-        CK(up(m_psib, psib.data(), psib.size() * 8));
+        // each buffer holds the matrix, then its transpose (the forward
+        // transform's operand order, see launch_vert_mode)
+        auto with_t = [&](const std::vector<double>& m) {
+            std::vector<double> o(2 * (size_t)nz * nz);
+            for (size_t e = 0; e < (size_t)nz * nz; ++e) o[e] = m[e];
+            for (int a = 0; a < nz; ++a)
+                for (int b = 0; b < nz; ++b) o[(size_t)nz * nz + a + (size_t)nz * b] = m[b + (size_t)nz * a];
+            return o;
+        };
+        const std::vector<double> phi2 = with_t(phi), psi2 = with_t(psi), psib2 = with_t(psib);
+        CK(up(m_phi, phi2.data(), phi2.size() * 8)); CK(up(m_psi, psi2.data(), psi2.size() * 8));
+        CK(up(m_psib, psib2.data(), psib2.size() * 8));
     }
     // plane kernel shapes
     PlaneArgs base{};
@@ -372,17 +389,6 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     int rc = autotune();
     if (rc) return rc;
     CK(cudaMemsetAsync(p.p, 0, p.bytes, stream));   // the tuner's timing runs wrote p
-    if (rigid && mixed) {
-        // the vertical solve's factors depend only on the grid: built once, in
-        // the spectral column order of the plane kernels the tuner picked
-        ColumnArgs c{};
-        c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.layout = spectral_layout(mixed ? pa32 : pa64);
-        c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p;
-        c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
-        CK(thomas_r.alloc((size_t)M * sizeof(double)));
-        CK(launch_thomas_factor(c, (double*)thomas_r.p, stream));
-        CK(cudaStreamSynchronize(stream));
-    }
     return PS3D_OK;
 }
 
@@ -550,8 +556,11 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
 // events, and keep the fastest.  Runs at creation on the zero state (every
 // output is zero, nothing observable changes); results are cached per
 // (grid, precision, batch, device) for the process and in a text file
-// ($PS3D_TUNE_CACHE, default ~/.cache/ps3d_b200_tune.txt).
+// ($PS3D_TUNE_CACHE, default ~/.cache/ps3d_b200_tune.txt).  Contexts created
+// concurrently (the serving loop's workers) tune one at a time: g_tune_mu is
+// held for the whole of autotune(), which is the only user of the cache.
 // ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
 static std::map<std::string, std::string>& tune_cache() {
     static std::map<std::string, std::string> m;
     static bool loaded = false;
@@ -580,6 +589,7 @@ static void tune_cache_store(const std::string& k, const std::string& v) {
 }
 
 int Ctx::autotune() {
+    std::lock_guard<std::mutex> tune_lock(g_tune_mu);
     const char* env = std::getenv("PS3D_AUTOTUNE");
     const bool pinned = std::getenv("PS3D_TUNE") != nullptr;
     if (env && env[0] == '0' && !pinned) return PS3D_OK;
@@ -819,7 +829,7 @@ int Ctx::poisson_once(double* out, double beta, bool lazy, const double* pc) {
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         c.dz2dsqr = P.dz * P.dz * P.dsqr;
-        c.rtab = f32 ? (const double*)thomas_r.p : nullptr;   // FP64: the recurrence is cheaper than the table traffic
+        c.err = kerr_d;
         LAUNCH(PS3D_K_VSOLVE, launch_thomas(c, f32, stream));
     } else {
         c.pz = plz.plan; c.scale = P.dz; c.op = 0;
@@ -891,8 +901,9 @@ int Ctx::forward_transform(const double* const* in) {
         a.spec = rigid ? qtmp.p : spec4[f].p;
         LAUNCH(PS3D_K_OTHER, launch_plane_fwd(a, false, stream));
         if (rigid) {
-            LAUNCH(PS3D_K_OTHER, launch_vert_mode((const double2*)qtmp.p, (double2*)spec4[f].p, (const double*)modes[f]->p,
-                                nz, M2, P.dz, 0, stream));
+            // A = the transposed matrix, the second half of the mode buffer
+            LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)qtmp.p, (double2*)spec4[f].p,
+                                                  (const double*)modes[f]->p + (size_t)nz * nz, nz, M2, P.dz, stream));
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
@@ -908,8 +919,8 @@ int Ctx::backward_transform(double* const* out) {
     for (int f = 0; f < 4; ++f) {
         void* src = spec4[f].p;
         if (rigid) {
-            LAUNCH(PS3D_K_OTHER, launch_vert_mode((const double2*)spec4[f].p, (double2*)qtmp.p, (const double*)modes[f]->p,
-                                nz, M2, 1.0, 1, stream));
+            LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)spec4[f].p, (double2*)qtmp.p, (const double*)modes[f]->p,
+                                                  nz, M2, 1.0, stream));
             src = qtmp.p;
         } else {
             ColumnArgs c{};
@@ -1598,7 +1609,7 @@ const char* ps3d_strerror(int status) {
         case PS3D_ERR_BADPARAM: return "invalid argument";
         case PS3D_ERR_UNSUPPORTED: return "configuration not supported by this engine";
         case PS3D_ERR_CANCELLED: return "request cancelled";
-        case PS3D_ERR_TOOLARGE: return "grid exceeds the static scratch of ps3d_pressure_solve_noalloc";
+        case PS3D_ERR_TOOLARGE: return "grid exceeds a fixed limit (columns too tall for a block's shared memory, or the static scratch of ps3d_pressure_solve_noalloc)";
         default: return "unknown status";
     }
 }

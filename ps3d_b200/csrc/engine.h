@@ -113,14 +113,11 @@ struct ColumnArgs {
     int batch;                     // instances (>= 1), spectral stride sM elements
     long sM;
     int layout;                    // spectral layout: 0 [k][ky][kx], 1 [k][kx][ky]
-    // rigid lid: Thomas factors [k][column] built once by launch_thomas_factor
-    // (level 0: c'(1) = c/b(1); level k >= 1: 1/(b(k) - c'(k-1) a)), or NULL
-    // to compute them on the fly
-    const double* rtab;
     // column slab (ncl 0: all nxh*ny columns): the array holds ncl columns per
     // level, global columns col0 .. col0+ncl-1 (one instance)
     long col0, ncl;
     FastDiv fd_ncols, fd_ny, fd_nxh;   // set by the launchers
+    unsigned* err;                 // rigid lid: set to 1 when a bounded wait for a tile ran out (or NULL)
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
@@ -146,12 +143,19 @@ bool ylines_in_registers(int ny);
 // the rows pass then has no rows-per-CTA parameter
 bool rows_in_registers(int nx, int ny);
 cudaError_t plane_setup(bool fp32);
+// default one-cluster-per-plane shape for element size es (false: no shape
+// fits the shared memory of a block)
+bool choose_plane_config(int nx, int ny, size_t es, PlaneArgs& a);
 cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);
 int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd);
+// rigid-lid vertical solve; cudaErrorInvalidValue when nz is too tall for
+// the shared memory of a block (vsolve_tile_width(nz) == 0)
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s);
-cudaError_t launch_thomas_factor(const ColumnArgs& a, double* rtab, cudaStream_t s);
+int vsolve_tile_width(int nz, bool fp32);
+// periodic z solve; zsolve_fits(nz, fp32) false: too tall for a block's shared memory
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
+bool zsolve_fits(int nz, bool fp32);
 
 // modes.cu: eigen tables for one grid and the projections
 struct EigenAxes {
@@ -172,8 +176,12 @@ struct ProjArgs {
     int mode;                      // PS3D_PROJ_*
 };
 cudaError_t launch_project(const ProjArgs& a, cudaStream_t s);
-cudaError_t launch_vert_mode(const double2* in, double2* out, const double* mode, int nz, long ncol,
-                             double scale, int transpose, cudaStream_t s);
+// A: nz x nz, read as A[ko + nz*ki] (the forward transform passes the
+// transposed mode matrix); cudaErrorInvalidValue when !vert_mode_fits(nz)
+cudaError_t launch_vert_mode(const double2* in, double2* out, const double* A, int nz, long ncol, double scale,
+                             cudaStream_t s);
+bool vert_mode_fits(int nz);
+cudaError_t modes_setup();   // per device, before the first launch_vert_mode
 
 // layout.cu: host halo layout <-> device interior layout (h_dev holds the
 // whole host array, (nx+4)*(ny+4)*(nz+4) doubles)

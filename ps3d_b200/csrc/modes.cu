@@ -52,13 +52,30 @@ __global__ void k_project(const ProjArgs a) {
     }
 }
 
-// out[ko][c] = sum_ki in[ki][c] * mode(ki, ko) * scale   (forward, transpose = 0)
-// out[ko][c] = sum_ki in[ki][c] * mode(ko, ki) * scale   (inverse, transpose = 1)
-// mode is the Fortran column-major nz x nz matrix, mode(a,b) = mode[a + nz*b].
+// Vertical-mode transforms (my_fft_vert_mode, my_fft.f90:234-252;
+// my_ifft_vert_mode, my_fft.f90:211-229) over the columns of a plane-FFT'd
+// field:
+//   out[ko][c] = scale * sum_ki in[ki][c] * A[ko + nz*ki]
+// with A = mode(ki, ko) (forward: the transpose of the Fortran column-major
+// mode matrix) or A = mode(ko, ki) (inverse: the matrix itself); the forward
+// scale dz multiplies the sum instead of every term.  A dense FP64 product,
+// nz^2 multiply-adds per complex column: bound by the FP64 pipe, not HBM.
+// A block stages 32 columns (one per lane) x nz levels in shared memory;
+// each warp accumulates kVmKo output levels of its lane's column per pass in
+// FP64 registers, reading each 16-byte pair of matrix entries once per warp
+// (a warp-uniform load, broadcast from L1), so a shared-memory load of one
+// complex input feeds 2*kVmKo fused multiply-adds.
 constexpr int kVmCols = 32;
-__global__ void __launch_bounds__(256) k_vert_mode(const double2* __restrict__ in, double2* __restrict__ out,
-                                                   const double* __restrict__ mode, int nz, long ncol,
-                                                   double scale, int transpose) {
+constexpr int kVmKo = 8;
+constexpr int kVmThreads = 256;
+
+size_t vert_mode_smem(int nz) { return (size_t)nz * kVmCols * sizeof(double2); }
+bool vert_mode_fits(int nz) { return vert_mode_smem(nz) <= 227 * 1024; }
+
+template <bool VEC>
+__global__ void __launch_bounds__(kVmThreads) k_vert_mode(const double2* __restrict__ in, double2* __restrict__ out,
+                                                          const double* __restrict__ A, int nz, long ncol,
+                                                          double scale) {
     extern __shared__ double2 tile[];   // [nz][kVmCols]
     const long c0 = blockIdx.x * (long)kVmCols;
     const int nl = (int)min((long)kVmCols, ncol - c0);
@@ -68,17 +85,45 @@ __global__ void __launch_bounds__(256) k_vert_mode(const double2* __restrict__ i
     }
     __syncthreads();
     const int l = threadIdx.x % kVmCols;
-    const int grp = threadIdx.x / kVmCols, ngrp = blockDim.x / kVmCols;
-    if (l >= nl) return;
-    for (int ko = grp; ko < nz; ko += ngrp) {
-        double sr = 0.0, si = 0.0;
-        for (int ki = 0; ki < nz; ++ki) {
-            const double m = transpose ? __ldg(mode + ko + (long)nz * ki) : __ldg(mode + ki + (long)nz * ko);
-            const double2 v = tile[ki * kVmCols + l];
-            sr = sr + v.x * m * scale;
-            si = si + v.y * m * scale;
+    const int wid = threadIdx.x / kVmCols, nw = blockDim.x / kVmCols;
+    if (l >= nl) return;   // no block barrier below
+    const int nch = (nz + kVmKo - 1) / kVmKo;
+    for (int ch = wid; ch < nch; ch += nw) {
+        const int ko0 = ch * kVmKo;
+        double ar[kVmKo], ai[kVmKo];
+#pragma unroll
+        for (int q = 0; q < kVmKo; ++q) { ar[q] = 0.0; ai[q] = 0.0; }
+        if (VEC && ko0 + kVmKo <= nz) {
+            // nz even and ko0 a multiple of kVmKo: the pairs are 16-byte aligned
+#pragma unroll 2
+            for (int ki = 0; ki < nz; ++ki) {
+                const double2 v = tile[ki * kVmCols + l];
+                const double2* row = reinterpret_cast<const double2*>(A + ko0 + (long)nz * ki);
+#pragma unroll
+                for (int q = 0; q < kVmKo / 2; ++q) {
+                    const double2 m = __ldg(row + q);
+                    ar[2 * q] = fma(v.x, m.x, ar[2 * q]);
+                    ai[2 * q] = fma(v.y, m.x, ai[2 * q]);
+                    ar[2 * q + 1] = fma(v.x, m.y, ar[2 * q + 1]);
+                    ai[2 * q + 1] = fma(v.y, m.y, ai[2 * q + 1]);
+                }
+            }
+        } else {
+            for (int ki = 0; ki < nz; ++ki) {
+                const double2 v = tile[ki * kVmCols + l];
+#pragma unroll
+                for (int q = 0; q < kVmKo; ++q) {
+                    if (ko0 + q < nz) {
+                        const double m = __ldg(A + ko0 + q + (long)nz * ki);
+                        ar[q] = fma(v.x, m, ar[q]);
+                        ai[q] = fma(v.y, m, ai[q]);
+                    }
+                }
+            }
         }
-        out[(long)ko * ncol + c0 + l] = make_double2(sr, si);
+#pragma unroll
+        for (int q = 0; q < kVmKo; ++q)
+            if (ko0 + q < nz) out[(long)(ko0 + q) * ncol + c0 + l] = make_double2(ar[q] * scale, ai[q] * scale);
     }
 }
 
@@ -89,16 +134,20 @@ cudaError_t launch_project(const ProjArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_vert_mode(const double2* in, double2* out, const double* mode, int nz, long ncol,
-                             double scale, int transpose, cudaStream_t s) {
-    const size_t sm = (size_t)nz * kVmCols * sizeof(double2);
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(k_vert_mode, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr_done = true;
-    }
+// opts the transform in to its dynamic shared memory on the current device
+cudaError_t modes_setup() {
+    cudaError_t e = cudaFuncSetAttribute(k_vert_mode<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_vert_mode<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+cudaError_t launch_vert_mode(const double2* in, double2* out, const double* A, int nz, long ncol, double scale,
+                             cudaStream_t s) {
+    if (!vert_mode_fits(nz)) return cudaErrorInvalidValue;
+    const size_t sm = vert_mode_smem(nz);
     const int blocks = (int)((ncol + kVmCols - 1) / kVmCols);
-    k_vert_mode<<<blocks, 256, sm, s>>>(in, out, mode, nz, ncol, scale, transpose);
+    if (nz % 2 == 0) k_vert_mode<true><<<blocks, kVmThreads, sm, s>>>(in, out, A, nz, ncol, scale);
+    else k_vert_mode<false><<<blocks, kVmThreads, sm, s>>>(in, out, A, nz, ncol, scale);
     return cudaGetLastError();
 }
 

@@ -16,12 +16,16 @@
 // Every GPU that loads the library holds both arrays (about 16.1 MiB) until
 // the process exits.  Nothing in them has to start at zero: each call
 // rewrites the tables and every spectral element it later reads.  All calls
-// share the arrays, so calls that overlap on the GPU (different streams or
-// host threads) race and must be serialised by the caller.
+// share the arrays, so calls that overlap on the GPU race: calls from host
+// threads of one process are serialised here (one lock around the call),
+// calls from other processes must be serialised by the caller.  A third
+// static word, g_err, records a bounded wait of the vertical solve that ran
+// out; it is read and cleared after every call.  The call is synchronous (it
+// waits for its stream) and cannot be captured in a CUDA graph; it allocates
+// no device memory, and its host staging image is a static per-device buffer.
 #include <cmath>
 #include <cstring>
 #include <mutex>
-#include <vector>
 #include "ctx.h"
 
 namespace ps3d {
@@ -42,43 +46,56 @@ constexpr long kTableDoubles = kPos + 3L * kMaxLen;
 
 static __device__ __align__(256) double2 g_spectral[kMaxSpectral];
 static __device__ __align__(256) double g_tables[kTableDoubles];
+static __device__ __align__(256) unsigned g_err;
 
-// device addresses of the two arrays, looked up once per device
-struct StaticArrays { double2* spectral = nullptr; double* tables = nullptr; bool ready = false; };
-static std::mutex g_mu;
-static StaticArrays g_dev[64];
+// device addresses of the static arrays, looked up once per device, and the
+// host image of the tables (static, so a call allocates no host memory either)
+struct StaticArrays {
+    double2* spectral = nullptr;
+    double* tables = nullptr;
+    unsigned* err = nullptr;
+    bool ready = false;
+    double img[kTableDoubles];
+};
+static std::mutex g_mu;   // held for a whole call
+static StaticArrays g_dev[16];
 
-static int static_arrays(int dev, StaticArrays& out) {
-    if (dev < 0 || dev >= 64) return PS3D_ERR_BADPARAM;
-    std::lock_guard<std::mutex> lk(g_mu);
+// with g_mu held
+static int static_arrays(int dev, StaticArrays*& out) {
+    if (dev < 0 || dev >= 16) return PS3D_ERR_BADPARAM;
     StaticArrays& s = g_dev[dev];
     if (!s.ready) {
         void* a = nullptr;
         void* b = nullptr;
+        void* e = nullptr;
         if (cudaGetSymbolAddress(&a, g_spectral) != cudaSuccess) return PS3D_ERR_CUDA;
         if (cudaGetSymbolAddress(&b, g_tables) != cudaSuccess) return PS3D_ERR_CUDA;
+        if (cudaGetSymbolAddress(&e, g_err) != cudaSuccess) return PS3D_ERR_CUDA;
         s.spectral = (double2*)a;
         s.tables = (double*)b;
+        s.err = (unsigned*)e;
         if (plane_setup(false) != cudaSuccess) return PS3D_ERR_CUDA;
+        if (cudaMemset(s.err, 0, sizeof(unsigned)) != cudaSuccess) return PS3D_ERR_CUDA;
         s.ready = true;
     }
-    out = s;
+    out = &s;
     return PS3D_OK;
 }
 
 // host construction of one FFT plan's tables into the staging image
-static bool plan_into(int n, std::vector<double>& img, long tw_off, long pos_off, long ipos_off, FFTPlan& P,
+static bool plan_into(int n, double* img, long tw_off, long pos_off, long ipos_off, FFTPlan& P,
                       const double* dev_tables) {
-    std::vector<int> r;
+    int r[64];
+    int nr = 0;
     int m = n;
-    while (m % 16 == 0) { r.push_back(16); m /= 16; }
-    if (m % 8 == 0) { r.push_back(8); m /= 8; }
-    while (m % 4 == 0) { r.push_back(4); m /= 4; }
-    while (m % 2 == 0) { r.push_back(2); m /= 2; }
-    while (m % 3 == 0) { r.push_back(3); m /= 3; }
-    while (m % 5 == 0) { r.push_back(5); m /= 5; }
-    if (m != 1 || n > kMaxLen || (int)r.size() > kMaxStages) return false;
-    int* ip = reinterpret_cast<int*>(img.data() + kPos);
+    while (m % 16 == 0) { r[nr++] = 16; m /= 16; }
+    if (m % 8 == 0) { r[nr++] = 8; m /= 8; }
+    while (m % 4 == 0) { r[nr++] = 4; m /= 4; }
+    while (m % 2 == 0) { r[nr++] = 2; m /= 2; }
+    while (m % 3 == 0) { r[nr++] = 3; m /= 3; }
+    while (m % 5 == 0) { r[nr++] = 5; m /= 5; }
+    if (m != 1 || n > kMaxLen || nr > kMaxStages) return false;
+    int* ip = reinterpret_cast<int*>(img + kPos);
     for (int t = 0; t < n; ++t) {
         long tt = t;
         double c, s;
@@ -94,10 +111,11 @@ static bool plan_into(int n, std::vector<double>& img, long tw_off, long pos_off
         img[tw_off + 2 * t] = c;
         img[tw_off + 2 * t + 1] = -s;
     }
-    std::vector<int> pos(n);
+    int* pos = ip + ipos_off;   // scratch: overwritten by the inverse table below
+    int* ipos = ip + ipos_off;
     for (int t = 0; t < n; ++t) {
         int v = t, len = n, p = 0;
-        for (int st = (int)r.size() - 1; st >= 0; --st) {
+        for (int st = nr - 1; st >= 0; --st) {
             const int R = r[st];
             p += (v % R) * (len / R);
             v /= R;
@@ -105,12 +123,13 @@ static bool plan_into(int n, std::vector<double>& img, long tw_off, long pos_off
         }
         pos[t] = p;
     }
-    for (int t = 0; t < n; ++t) { ip[pos_off + t] = pos[t]; ip[ipos_off + pos[t]] = t; }
+    for (int t = 0; t < n; ++t) ip[pos_off + t] = pos[t];
+    for (int t = 0; t < n; ++t) ipos[ip[pos_off + t]] = t;
     P.n = n;
-    P.nst = (int)r.size();
+    P.nst = nr;
     int acc = 1;
     for (int st = 0; st < kMaxStages; ++st) {
-        P.r[st] = st < (int)r.size() ? r[st] : 1;
+        P.r[st] = st < nr ? r[st] : 1;
         P.lp[st] = acc;
         acc *= P.r[st];
     }
@@ -130,7 +149,7 @@ extern "C" {
 // arrays, FP64, allocating nothing.  u, v, w, p: nx*ny*nz doubles each, x
 // fastest, interior points only.  The first call on a device looks up the
 // static arrays' device addresses (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture.
+// current; make that first call before any stream capture.  Synchronous.
 PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, double* v, double* w, double* p,
                                          void* stream) {
     using namespace ps3d;
@@ -139,25 +158,36 @@ PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, doub
     const bool rigid = P.enable_vertical_boundaries != 0;
     const int nx = P.nx, ny = P.ny, nz = P.nz, nxh = nx / 2 + 1;
     if (nx < 2 || ny < 2 || nz < 2 || nx % 2 || ny % 2 || (!rigid && nz % 2)) return PS3D_ERR_BADPARAM;
-    // the static arrays bound the grid; checked before the field pointers so
-    // that a caller can probe a size with null pointers
+    // the static arrays and the column kernels' shared memory bound the grid;
+    // checked before the field pointers so that a caller can probe a size
+    // with null pointers
     if ((long)nxh * ny * nz > kMaxSpectral || nx / 2 > kMaxLen || ny > kMaxLen || nz > kMaxLen)
         return PS3D_ERR_TOOLARGE;
+    if (rigid ? vsolve_tile_width(nz, false) == 0 : !zsolve_fits(nz, false)) return PS3D_ERR_TOOLARGE;
     if (!u || !v || !w || !p) return PS3D_ERR_BADPARAM;
     if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0 && P.dt != 0))
         return PS3D_ERR_BADPARAM;
+    // a failing CUDA call: its error is taken off the thread's error state so
+    // that it is not reported again by a later call
+    auto fail = [](cudaError_t e) {
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? PS3D_ERR_OOM : PS3D_ERR_CUDA;
+    };
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return PS3D_ERR_CUDA;
-    StaticArrays sa;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(e);
+    std::lock_guard<std::mutex> lk(g_mu);
+    StaticArrays* sa = nullptr;
     int rc = static_arrays(dev, sa);
-    if (rc) return rc;
+    if (rc) { cudaGetLastError(); return rc; }
     cudaStream_t s = (cudaStream_t)stream;
-    // tables: built on the host, copied into g_tables
-    std::vector<double> img(kTableDoubles, 0.0);
+    // tables: built on the host into the static image, copied into g_tables
+    double* img = sa->img;
+    std::memset(img, 0, sizeof(sa->img));
     FFTPlan px{}, py{}, pz{};
-    if (!plan_into(nx / 2, img, kTwX, 0, kMaxLen, px, sa.tables)) return PS3D_ERR_BADPARAM;
-    if (!plan_into(ny, img, kTwY, 2 * kMaxLen, 3 * kMaxLen, py, sa.tables)) return PS3D_ERR_BADPARAM;
-    if (!rigid && !plan_into(nz, img, kTwZ, 4 * kMaxLen, 5 * kMaxLen, pz, sa.tables)) return PS3D_ERR_BADPARAM;
+    if (!plan_into(nx / 2, img, kTwX, 0, kMaxLen, px, sa->tables)) return PS3D_ERR_BADPARAM;
+    if (!plan_into(ny, img, kTwY, 2 * kMaxLen, 3 * kMaxLen, py, sa->tables)) return PS3D_ERR_BADPARAM;
+    if (!rigid && !plan_into(nz, img, kTwZ, 4 * kMaxLen, 5 * kMaxLen, pz, sa->tables)) return PS3D_ERR_BADPARAM;
     const double pi = std::acos(0.0) * 2.0;
     for (int t = 0; t < nxh; ++t) {
         long tt = t;
@@ -185,63 +215,54 @@ PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, doub
             const double kz = k <= (nz + 1) / 2 ? 2 * (k - 1) * pi / P.Lz : -(2 * (nz - k + 1) * pi / P.Lz);
             img[kHkz + k - 1] = hat(kz, P.dz) / P.dsqr;
         }
-    if (cudaMemcpyAsync(sa.tables, img.data(), kTableDoubles * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return PS3D_ERR_CUDA;
-    // plane-kernel shape: the default choice of the engine
+    // plane-kernel shape: the engine's default one-cluster-per-plane shape
     PlaneArgs a{};
     a.nx = nx; a.ny = ny; a.nz = nz; a.nxh = nxh;
     a.px = px; a.py = py;
-    a.twx = reinterpret_cast<const double2*>(sa.tables + kTwR);
+    a.twx = reinterpret_cast<const double2*>(sa->tables + kTwR);
     a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz;
     a.batch = 1; a.sN = (long)nx * ny * nz; a.sM = (long)nxh * ny * nz;
-    {
-        const int n2 = nx / 2;
-        bool found = false;
-        for (int pass = 0; pass < 2 && !found; ++pass) {
-            const size_t limit = pass == 0 ? 110 * 1024 : 225 * 1024;
-            for (int C : {1, 2, 4, 8, 16}) {
-                if (ny % C) continue;
-                const int R = ny / C, cpc = (nxh + C - 1) / C;
-                if ((C - 1) * cpc >= nxh) continue;
-                const int rcc = std::min(8, R);
-                const int ldr = rcc | 1, ldc = cpc | 1;
-                if (((size_t)ny * ldc + (size_t)n2 * ldr) * sizeof(double2) > limit) continue;
-                a.C = C; a.rows_per_cta = R; a.cols_per_cta = cpc; a.row_chunk = rcc; a.ldr = ldr; a.ldc = ldc;
-                found = true;
-                break;
-            }
-        }
-        if (!found) return PS3D_ERR_BADPARAM;
-    }
+    if (!choose_plane_config(nx, ny, sizeof(double2), a)) return PS3D_ERR_TOOLARGE;
+    a.impl = 0;
+    if ((e = cudaMemcpyAsync(sa->tables, img, sizeof(sa->img), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail(e);
     PlaneArgs f = a;
     f.mode = 0; f.u = u; f.v = v; f.w = w;
     f.rdt = 1.0 / P.dt;
     f.scale = P.dx * P.dy;
-    f.spec = sa.spectral;
-    if (launch_plane_fwd(f, false, s) != cudaSuccess) return PS3D_ERR_CUDA;
+    f.spec = sa->spectral;
+    if ((e = launch_plane_fwd(f, false, s)) != cudaSuccess) return fail(e);
     ColumnArgs c{};
-    c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = sa.spectral;
+    c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = sa->spectral;
     c.batch = 1; c.sM = a.sM;
-    c.hkx = sa.tables + kHkx; c.hky = sa.tables + kHky; c.hkz = sa.tables + kHkz;
+    c.hkx = sa->tables + kHkx; c.hky = sa->tables + kHky; c.hkz = sa->tables + kHkz;
+    c.layout = spectral_layout(a);
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         c.dz2dsqr = P.dz * P.dz * P.dsqr;
-        if (launch_thomas(c, false, s) != cudaSuccess) return PS3D_ERR_CUDA;
+        c.err = sa->err;
+        if ((e = launch_thomas(c, false, s)) != cudaSuccess) return fail(e);
     } else {
         c.pz = pz; c.scale = P.dz; c.op = 0;
-        if (launch_zsolve(c, false, s) != cudaSuccess) return PS3D_ERR_CUDA;
+        if ((e = launch_zsolve(c, false, s)) != cudaSuccess) return fail(e);
     }
     PlaneArgs b = a;
-    b.spec = sa.spectral;
+    b.spec = sa->spectral;
     b.out = p;
     b.beta = 0.0;
     b.scale = rigid ? 1.0 / (P.Lx * P.Ly) : 1.0 / (P.Lx * P.Ly * P.Lz);
-    if (launch_plane_inv(b, false, s) != cudaSuccess) return PS3D_ERR_CUDA;
-    if (launch_correct(u, v, w, p, nx, ny, nz, rigid, P.dt, P.dt / P.dsqr, 1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz, s) !=
-        cudaSuccess)
-        return PS3D_ERR_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return PS3D_ERR_CUDA;
-    return cudaGetLastError() == cudaSuccess ? PS3D_OK : PS3D_ERR_CUDA;
+    if ((e = launch_plane_inv(b, false, s)) != cudaSuccess) return fail(e);
+    if ((e = launch_correct(u, v, w, p, nx, ny, nz, rigid, P.dt, P.dt / P.dsqr, 1.0 / P.dx, 1.0 / P.dy, 1.0 / P.dz,
+                            s)) != cudaSuccess)
+        return fail(e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
+    // the vertical solve's bounded waits: read and clear the error word
+    unsigned timed_out = 0;
+    if ((e = cudaMemcpy(&timed_out, sa->err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess) return fail(e);
+    if (timed_out) {
+        if ((e = cudaMemset(sa->err, 0, sizeof(unsigned))) != cudaSuccess) return fail(e);
+        return PS3D_ERR_TIMEOUT;
+    }
+    return PS3D_OK;
 }
 
 }  // extern "C"

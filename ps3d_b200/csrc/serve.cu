@@ -64,11 +64,10 @@ static size_t footprint_of(const ps3d_params& p) {
     b += N * 8;                            // p
     b += 9 * N * ts + 3 * N * 8;           // 3 tendency levels x 4 fields (w always FP64)
     b += M * (mixed ? 8 : 16);             // Poisson spectral array
-    if (p.enable_vertical_boundaries && mixed) b += M * 8;   // Thomas factors
     b += 6 * M * 16;                       // projection spectra, g0_base, scratch
     b += 4 * 4 * N * 8;                    // balanced, base, saved, zero-order field sets
     b += N * 8 + 9 * N * ts + 3 * N * 8;   // saved p and tendencies
-    if (p.nz > 0) b += 3 * (size_t)p.nz * p.nz * 8;
+    if (p.nz > 0) b += 6 * (size_t)p.nz * p.nz * 8;   // mode matrices and their transposes
     b += (size_t)(p.nx + 4) * (p.ny + 4) * (p.nz + 4) * 8;   // host-layout staging
     return b + (64u << 20);                // tables, plans, reductions, allocator slack
 }

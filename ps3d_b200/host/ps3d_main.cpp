@@ -581,8 +581,8 @@ int main(int argc, char** argv) {
     std::printf(" loop                     = %15.2f s\n", loop_s);
     std::printf(" integrate                = %15.2f s\n", integrate_s);
     if (r.profile) {
-        double ms[6] = {0};
-        long long n[6] = {0};
+        double ms[PS3D_K_COUNT] = {0};
+        long long n[PS3D_K_COUNT] = {0};
         check(ps3d_profile_read(ctx, ms, n), "ps3d_profile_read");
         std::printf(" stencils (device)        = %15.4f s\n", ms[PS3D_K_STEP] * 1e-3);
         std::printf(" pressure (device)        = %15.4f s\n",

@@ -245,12 +245,12 @@ class Model:
         _check(self.L.ps3d_describe(self.h, buf, 512), "ps3d_describe")
         return buf.value.decode()
 
-    KERNELS = ("step", "fft_fwd", "vsolve", "fft_inv", "correct", "other")
+    KERNELS = ("step", "fft_fwd", "vsolve", "fft_inv", "correct", "other", "vmode")
 
     def profile_read(self):
         """{kernel class: (device ms summed over launches, launches)} since ps3d_profile."""
-        ms = (C.c_double * 6)()
-        n = (C.c_longlong * 6)()
+        ms = (C.c_double * len(self.KERNELS))()
+        n = (C.c_longlong * len(self.KERNELS))()
         _check(self.L.ps3d_profile_read(self.h, ms, n), "ps3d_profile_read")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
 

@@ -110,7 +110,7 @@ def test_phase_and_kernel_class_mirrors():
         assert defs["PS3D_SLAB_" + name.upper()] == v, name
     assert len(PHASE) == len([k for k in defs if k.startswith("PS3D_SLAB_")])
     names = {"step": "STEP", "fft_fwd": "FFT_FWD", "vsolve": "VSOLVE", "fft_inv": "FFT_INV",
-             "correct": "CORRECT", "other": "OTHER"}
+             "correct": "CORRECT", "other": "OTHER", "vmode": "VMODE"}
     for i, k in enumerate(Model.KERNELS):
         assert defs["PS3D_K_" + names[k]] == i, k
     assert defs["PS3D_K_COUNT"] == len(Model.KERNELS)

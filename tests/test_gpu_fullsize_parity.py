@@ -1,0 +1,123 @@
+"""Parity with the CPU oracle at the benchmarked sizes.
+
+The jets case at 256x256x128 (rigid lid, AB3, Laplacian friction; the size
+bench.py times) after 200 steps, and the forced lee-wave-like case at
+512x256x128 (triply periodic: the 3-D FFT branch of pressure_solver.f90:
+58-70, background-flow advection and a bottom wavemaker, lee_wave1.f90:
+232-332) after 50 steps.  The oracle runs on every host core (OpenMP); the
+same oracle trajectory checks the FP64 path (relative L2 <= 1e-11 in u, v,
+w, b, p) and the mixed path (<= 1e-5).  The measured errors and the maximum
+divergence are printed (pytest -s shows them).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.binding import Oracle, set_threads
+from ps3d_b200 import abi
+from ps3d_b200 import configs as cf
+from ps3d_b200.model import Model
+from tests.helpers import rel
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-11
+TOL_MIXED = 1e-5
+NAMES = ("u", "v", "w", "b", "p")
+
+
+def _max_div(p, s):
+    u, v, w = (s[n][2:-2, 2:-2, 2:-2] for n in ("u", "v", "w"))
+    du = (u - np.roll(u, 1, axis=2)) / p.dx
+    dv = (v - np.roll(v, 1, axis=1)) / p.dy
+    wm = np.roll(w, 1, axis=0)
+    if p.enable_vertical_boundaries:
+        wm[0] = 0.0
+    return float(np.abs(du + dv + (w - wm) / p.dz).max())
+
+
+def _gpu(p, fields, nsteps, forcing=None):
+    m = Model(p)
+    if forcing:
+        m.set_forcing(abi.PS3D_FORCE_WAVEMAKER | abi.PS3D_FORCE_BACKGROUND, omega=forcing["omega"],
+                      w_r=forcing["w_r"], w_i=forcing["w_i"], u_back=forcing["u_back"], b_back=forcing["b_back"])
+    m.upload(**{n: fields[n] for n in ("u", "v", "w", "b")})
+    m.run(nsteps)
+    st = m.download(tendencies=False)
+    m.close()
+    return st
+
+
+def _oracle(p, fields, nsteps, forcing=None):
+    set_threads(os.cpu_count() or 1)
+    o = Oracle(p)
+    for n in ("u", "v", "w", "b"):
+        o.field(n)[...] = fields[n]
+    if forcing:
+        from ps3d_b200.abi import Forcing, dptr
+        f = Forcing()
+        f.kind = abi.PS3D_FORCE_BACKGROUND | abi.PS3D_FORCE_WAVEMAKER
+        f.omega = forcing["omega"]
+        f.w_r, f.w_i = dptr(forcing["w_r"]), dptr(forcing["w_i"])
+        f.u_back, f.b_back = dptr(forcing["u_back"]), dptr(forcing["b_back"])
+        o.set_forcing(f, keep=forcing)
+    o.integrate(nsteps)
+    out = {n: o.field(n).copy() for n in NAMES}
+    del o
+    return out
+
+
+def _report(tag, p, got, ref):
+    err = {n: rel(got[n], ref[n]) for n in NAMES}
+    print(f"\n[parity] {tag}: " + " ".join(f"{n}={err[n]:.3e}" for n in NAMES) +
+          f" max_div={_max_div(p, got):.3e} oracle_max_div={_max_div(p, ref):.3e}"
+          f" |u|max/dx={np.abs(ref['u']).max() / p.dx:.3e}")
+    return err
+
+
+@pytest.fixture(scope="module")
+def jets():
+    p = cf.jets_params(256, 256, 128)
+    f = cf.add_noise(p, cf.jets_fields(p), "b", rel=1e-3, seed=1)
+    return p, f, _oracle(p, f, 200)
+
+
+def test_jets_256x256x128_fp64_vs_oracle_200_steps(jets):
+    p, f, ref = jets
+    got = _gpu(p, f, 200)
+    err = _report("jets 256x256x128 FP64, 200 steps", p, got, ref)
+    assert max(err.values()) < TOL64, err
+
+
+@pytest.mark.parametrize("prec", [abi.PS3D_MIXED, abi.PS3D_MIXED_REFINED])
+def test_jets_256x256x128_mixed_vs_oracle_200_steps(jets, prec):
+    p, f, ref = jets
+    pm = cf.jets_params(256, 256, 128, precision=prec)
+    got = _gpu(pm, f, 200)
+    err = _report(f"jets 256x256x128 precision {prec}, 200 steps", p, got, ref)
+    assert max(err.values()) < TOL_MIXED, err
+
+
+@pytest.fixture(scope="module")
+def lee_wave():
+    p = cf.lee_wave_params(512, 256, 128)
+    fr = cf.lee_wave_forcing(p, seed=2)
+    zero = {n: cf.empty_field(p) for n in ("u", "v", "w", "b")}
+    return p, fr, zero, _oracle(p, zero, 50, forcing=fr)
+
+
+def test_lee_wave_512x256x128_fp64_vs_oracle_50_steps(lee_wave):
+    p, fr, zero, ref = lee_wave
+    assert np.abs(ref["w"]).max() > 0.0
+    got = _gpu(p, zero, 50, forcing=fr)
+    err = _report("lee wave 512x256x128 FP64, 50 steps", p, got, ref)
+    assert max(err.values()) < TOL64, err
+
+
+def test_lee_wave_512x256x128_mixed_vs_oracle_50_steps(lee_wave):
+    p, fr, zero, ref = lee_wave
+    pm = cf.lee_wave_params(512, 256, 128, precision=abi.PS3D_MIXED)
+    got = _gpu(pm, zero, 50, forcing=fr)
+    err = _report("lee wave 512x256x128 mixed, 50 steps", p, got, ref)
+    assert max(err.values()) < TOL_MIXED, err

@@ -214,6 +214,18 @@ def test_projection(rigid, mode):
     assert max(err.values()) < TOL_KERNEL, err
 
 
+@pytest.mark.parametrize("nz", [33, 64, 128])
+def test_normal_mode_projection_tall_rigid(nz):
+    """Rigid-lid projection through the vertical-mode transforms at nz = 128
+    (the tiled FP64 product), 64 and an odd 33 (the unpaired-load path)."""
+    p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
+    o, m = _pair(p, smooth_state(p, seed=15))
+    o.project(abi.PS3D_PROJ_NORMAL_MODE)
+    m.project(abi.PS3D_PROJ_NORMAL_MODE)
+    err = compare_state(m, o, names=FIELDS)
+    assert max(err.values()) < TOL_KERNEL, err
+
+
 @pytest.mark.parametrize("time_ave", [False, True])
 def test_opt_balance(time_ave):
     p = small_params(32, 32, 8, rigid=True, dt=600.0)

@@ -77,9 +77,52 @@ def test_mixed_request_matches_fp64():
     for n in ("u", "v", "w", "b"):
         a, b = rmx.fields[n][2:-2, 2:-2, 2:-2], r64.fields[n][2:-2, 2:-2, 2:-2]
         err[n] = np.linalg.norm(a - b) / np.linalg.norm(b)
-    # w is the balanced state's small ageostrophic part, the field the FP32
-    # tendency history perturbs most relative to its size
-    assert max(err["u"], err["v"], err["b"]) < 1e-5 and err["w"] < 1e-3, err
+    # w is the balanced state's small ageostrophic part: its own norm is
+    # ~1e-3 of the horizontal velocity's, so its error is also held against
+    # the velocity scale ||(u, v, w)||
+    uvw = np.sqrt(sum(np.linalg.norm(r64.fields[n][2:-2, 2:-2, 2:-2]) ** 2 for n in ("u", "v", "w")))
+    w_abs = np.linalg.norm(rmx.fields["w"][2:-2, 2:-2, 2:-2] - r64.fields["w"][2:-2, 2:-2, 2:-2])
+    print(f"\n[serve mixed vs fp64] rel L2 {err}; w error / ||(u,v,w)|| = {w_abs / uvw:.3e}; "
+          f"||w||/||(u,v,w)|| = {np.linalg.norm(r64.fields['w'][2:-2, 2:-2, 2:-2]) / uvw:.3e}")
+    assert max(err["u"], err["v"], err["b"]) < 1e-5 and w_abs / uvw < 1e-5 and err["w"] < 1e-3, err
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_concurrent_submissions_from_threads_match_alone(precision):
+    """Requests of several sizes submitted at the same moment from several
+    host threads (their contexts created, and grids of >= 2^15 points
+    autotuned, concurrently by the server's workers) give the same bits as
+    each request run alone afterwards in the same process."""
+    import threading
+    sizes = [(64, 64, 16), (32, 64, 16), (64, 32, 32), (32, 32, 32), (64, 64, 16), (32, 32, 16)]
+    reqs = []
+    for i, n in enumerate(sizes):
+        p, opt, f = _req(n, ramp=6, iters=2, precision=precision)
+        f = {k: v * (1.0 + 0.05 * i) for k, v in f.items()}
+        reqs.append((p, opt, f))
+    s = Server(max_active=4)
+    tickets = [None] * len(reqs)
+    go = threading.Barrier(len(reqs))
+
+    def submit(i):
+        go.wait(timeout=60)
+        tickets[i] = s.submit(*reqs[i])
+
+    th = [threading.Thread(target=submit, args=(i,)) for i in range(len(reqs))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=120)
+    mix = [s.wait(t) for t in tickets]
+    s.close()
+    for i, r in enumerate(reqs):
+        s1 = Server(max_active=1)
+        alone = s1.wait(s1.submit(*r))
+        s1.close()
+        assert mix[i].status == alone.status == 0, (i, mix[i].status, alone.status)
+        assert mix[i].norm == alone.norm, i
+        for n in ("u", "v", "w", "b"):
+            assert np.array_equal(mix[i].fields[n], alone.fields[n]), (i, n)
 
 
 def test_admission_respects_budget():
