@@ -282,12 +282,12 @@ PS3D_API int ps3d_profile_read(ps3d_ctx* ctx, double* ms, long long* launches);
  * doubles, x fastest, interior points only, queued on `stream` (a
  * cudaStream_t, NULL for the default stream) and waited for: the call is
  * synchronous, and cannot be captured in a CUDA graph.  It allocates no
- * device memory: the spectral work array, the FFT tables and an error word
- * are file-scope static device arrays (about 16.1 MiB, held on every GPU
- * that loads the library until exit), and the host image of the tables is
- * a static buffer.  (nx/2+1)*ny*nz must not exceed 1048576 and nx/2, ny, nz
- * not 1024, and periodic grids nz not about 420 (the z transform's shared
- * memory), else PS3D_ERR_TOOLARGE.  The first call on a device looks up the
+ * device memory: the spectral work array and the FFT tables are file-scope
+ * static device arrays (about 16.1 MiB, held on every GPU that loads the
+ * library until exit), and the host image of the tables is a static buffer.
+ * (nx/2+1)*ny*nz must not exceed 1048576 and nx/2, ny, nz not 1024, and
+ * periodic grids nz not about 420 (the z transform's shared memory), else
+ * PS3D_ERR_TOOLARGE.  The first call on a device looks up the
  * static arrays with that device current.  Calls from threads of one
  * process are serialised by the library; calls from several processes that
  * overlap on one GPU race on the arrays.                                   */

@@ -50,6 +50,7 @@ struct StepArgs {
     int batch;                     // instances of the same grid stepped together (>= 1)
     long sN;                       // element stride between instances (fields and tendency slots)
     int kchunk;                    // z levels per block (autotuned)
+    int form;                      // 0: all threads load and compute, 1: warp-specialised (autotuned)
     // pending pressure correction of the previous step (NULL: state is final):
     // the state arrays hold u'' and the true velocity is u'' - dtp*grad(pc)
     const double* pc;
@@ -117,7 +118,6 @@ struct ColumnArgs {
     // level, global columns col0 .. col0+ncl-1 (one instance)
     long col0, ncl;
     FastDiv fd_ncols, fd_ny, fd_nxh;   // set by the launchers
-    unsigned* err;                 // rigid lid: set to 1 when a bounded wait for a tile ran out (or NULL)
 };
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
@@ -150,9 +150,9 @@ cudaError_t launch_plane_fwd(const PlaneArgs& a, bool fp32, cudaStream_t s);
 cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s);
 int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd);
 // rigid-lid vertical solve; cudaErrorInvalidValue when nz is too tall for
-// the shared memory of a block (vsolve_tile_width(nz) == 0)
+// the shared memory of a block (thomas_threads(nz) == 0)
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s);
-int vsolve_tile_width(int nz, bool fp32);
+int thomas_threads(int nz);
 // periodic z solve; zsolve_fits(nz, fp32) false: too tall for a block's shared memory
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
 bool zsolve_fits(int nz, bool fp32);

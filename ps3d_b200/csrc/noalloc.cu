@@ -18,11 +18,10 @@
 // rewrites the tables and every spectral element it later reads.  All calls
 // share the arrays, so calls that overlap on the GPU race: calls from host
 // threads of one process are serialised here (one lock around the call),
-// calls from other processes must be serialised by the caller.  A third
-// static word, g_err, records a bounded wait of the vertical solve that ran
-// out; it is read and cleared after every call.  The call is synchronous (it
-// waits for its stream) and cannot be captured in a CUDA graph; it allocates
-// no device memory, and its host staging image is a static per-device buffer.
+// calls from other processes must be serialised by the caller.  The call is
+// synchronous (it waits for its stream) and cannot be captured in a CUDA
+// graph; it allocates no device memory, and its host staging image is a
+// static per-device buffer.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -46,14 +45,12 @@ constexpr long kTableDoubles = kPos + 3L * kMaxLen;
 
 static __device__ __align__(256) double2 g_spectral[kMaxSpectral];
 static __device__ __align__(256) double g_tables[kTableDoubles];
-static __device__ __align__(256) unsigned g_err;
 
 // device addresses of the static arrays, looked up once per device, and the
 // host image of the tables (static, so a call allocates no host memory either)
 struct StaticArrays {
     double2* spectral = nullptr;
     double* tables = nullptr;
-    unsigned* err = nullptr;
     bool ready = false;
     double img[kTableDoubles];
 };
@@ -67,15 +64,11 @@ static int static_arrays(int dev, StaticArrays*& out) {
     if (!s.ready) {
         void* a = nullptr;
         void* b = nullptr;
-        void* e = nullptr;
         if (cudaGetSymbolAddress(&a, g_spectral) != cudaSuccess) return PS3D_ERR_CUDA;
         if (cudaGetSymbolAddress(&b, g_tables) != cudaSuccess) return PS3D_ERR_CUDA;
-        if (cudaGetSymbolAddress(&e, g_err) != cudaSuccess) return PS3D_ERR_CUDA;
         s.spectral = (double2*)a;
         s.tables = (double*)b;
-        s.err = (unsigned*)e;
         if (plane_setup(false) != cudaSuccess) return PS3D_ERR_CUDA;
-        if (cudaMemset(s.err, 0, sizeof(unsigned)) != cudaSuccess) return PS3D_ERR_CUDA;
         s.ready = true;
     }
     out = &s;
@@ -163,7 +156,7 @@ PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, doub
     // with null pointers
     if ((long)nxh * ny * nz > kMaxSpectral || nx / 2 > kMaxLen || ny > kMaxLen || nz > kMaxLen)
         return PS3D_ERR_TOOLARGE;
-    if (rigid ? vsolve_tile_width(nz, false) == 0 : !zsolve_fits(nz, false)) return PS3D_ERR_TOOLARGE;
+    if (rigid ? thomas_threads(nz) == 0 : !zsolve_fits(nz, false)) return PS3D_ERR_TOOLARGE;
     if (!u || !v || !w || !p) return PS3D_ERR_BADPARAM;
     if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0 && P.dt != 0))
         return PS3D_ERR_BADPARAM;
@@ -239,7 +232,6 @@ PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, doub
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         c.dz2dsqr = P.dz * P.dz * P.dsqr;
-        c.err = sa->err;
         if ((e = launch_thomas(c, false, s)) != cudaSuccess) return fail(e);
     } else {
         c.pz = pz; c.scale = P.dz; c.op = 0;
@@ -255,13 +247,6 @@ PS3D_API int ps3d_pressure_solve_noalloc(const ps3d_params* prm, double* u, doub
                             s)) != cudaSuccess)
         return fail(e);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
-    // the vertical solve's bounded waits: read and clear the error word
-    unsigned timed_out = 0;
-    if ((e = cudaMemcpy(&timed_out, sa->err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess) return fail(e);
-    if (timed_out) {
-        if ((e = cudaMemset(sa->err, 0, sizeof(unsigned))) != cudaSuccess) return fail(e);
-        return PS3D_ERR_TIMEOUT;
-    }
     return PS3D_OK;
 }
 

@@ -10,10 +10,10 @@
 //                   the CTA that owns that kx column (distributed shared
 //                   memory), which then transforms along y.  The plane never
 //                   round-trips through HBM between the two directions.
-// K3 k_vsolve     : the vertical tridiagonal solves and the (0,0)-mode
-//                   recurrence (pressure_solver.f90:33-53,126-162); one warp
-//                   per tile of 32 whole columns staged in shared memory by
-//                   bulk copies, FP64 recurrences, the pivots formed on the fly.
+// K3 k_thomas     : the vertical tridiagonal solves and the (0,0)-mode
+//                   recurrence (pressure_solver.f90:33-53,126-162); one thread
+//                   per (kx,ky) column and part, FP64 recurrences checkpointed
+//                   every 8 levels in shared memory, the pivots formed on the fly.
 //    k_zsolve     : periodic branch (pressure_solver.f90:58-70): z FFT,
 //                   -f/ksqr and inverse z FFT of a batch of columns in one pass.
 // K4 k_plane_inv  : inverse y FFT, DSMEM gather, complex-to-real x FFT and the
@@ -279,168 +279,158 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
 }
 
 // ---------------------------------------------------------------------------
-// K3, rigid lid: the vertical tridiagonal solves (pressure_solver.f90:33-53;
+// K3, rigid lid: batched Thomas along z (pressure_solver.f90:33-53;
 // solve_tridiag, pressure_solver.f90:126-162) and the (0,0)-mode recurrence.
-// One warp per tile of W <= 32 consecutive spectral columns, which are
-// contiguous along every level in both spectral layouts.  The tile's nz level
-// rows arrive by bulk copies on the TMA engine (one per level, no tensor map,
-// no multicast) that complete on one mbarrier, so a block has its whole tile
-// in flight without holding registers for it; lane l then runs column l's
-// recurrence in FP64 out of shared memory.  The coefficients are real, so
-// one lane carries both parts of its complex column through one pivot chain.
-// The elimination d' is never rounded to the storage precision: the forward
-// sweep keeps the reciprocal pivots r(k) and, every kVsChunk levels, the
-// running d' (FP64) in shared memory; the backward sweep recomputes each
-// chunk's d' from its checkpoint with the same operations (hence the same
-// values) and substitutes back.  The pivots are formed from ksqr on the fly:
-// no factor table in HBM.
+// The coefficients are real, so the real and imaginary parts of a column are
+// independent recurrences: one thread per (column, part), every column in
+// one wave.  Levels move in chunks of KC, and the loads of the next chunk
+// are issued before the recurrence runs over the current one, so memory
+// latency overlaps the serial arithmetic.  The elimination runs in FP64 and
+// is never rounded to the storage precision: the forward sweep writes
+// nothing to the array, it keeps (c', d') of the level before every chunk in
+// shared memory; the backward sweep re-reads a chunk's right-hand side,
+// recomputes its pivots and d' from those two values with the same
+// operations (so the same values), substitutes back and overwrites the
+// chunk with x.  The pivots are formed from ksqr on the fly: no factor
+// table and no d' array in HBM.
 // ---------------------------------------------------------------------------
-constexpr int kVsChunk = 8;
+constexpr int kThomasChunk = 8;
+constexpr int kThomasThreads = 128;
 
-// shared memory of one tile: the columns in the storage precision, the
-// pivots r(k) and the d' checkpoints (FP64)
-PS3D_HD size_t vsolve_smem(int nz, int W, size_t es) {
-    const size_t nch = (size_t)(nz + kVsChunk - 1) / kVsChunk;
-    return align16((size_t)nz * W * es) + align16((size_t)nz * W * sizeof(double)) + nch * W * sizeof(double2);
+PS3D_HD size_t thomas_smem(int nz, int threads) {
+    return (size_t)((nz + kThomasChunk - 1) / kThomasChunk + 1) * threads * sizeof(double2);
 }
 
-template <typename R>
-__global__ void __launch_bounds__(32) k_vsolve(const ColumnArgs a, int W, unsigned tpi, int bulk) {
-    using T = cpx<R>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) unsigned long long bar;
+template <typename R, bool FULL>
+__global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a) {
     pdl_trigger();
-    const int nz = a.nz, lane = threadIdx.x;
+    pdl_wait();   // inputs written by the preceding kernels
+    constexpr int KC = kThomasChunk;
+    // FULL: nz is a multiple of KC, so only the chunk ends need tests
+#define IN(cond) (FULL || (cond))
+    extern __shared__ double2 ckp[];   // [chunk][thread]: (c', d') of the level before the chunk
     const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
-    const unsigned inst = blockIdx.x / tpi;
-    const long c0 = (long)(blockIdx.x - inst * tpi) * W;
-    const int nl = (int)min((long)W, ncols - c0);
-    T* tile = reinterpret_cast<T*>(smem_raw);   // [nz][W]
-    double* rs = reinterpret_cast<double*>(smem_raw + align16((size_t)nz * W * sizeof(T)));   // [nz][W]
-    double2* ck = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(rs) +
-                                             align16((size_t)nz * W * sizeof(double)));      // [nz/KC][W]
-    T* g = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + c0;
-    if (bulk) {
-        if (lane == 0) {
-            mbar_init(&bar, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (gid >= 2 * ncols * a.batch) return;
+    const int part = (int)(gid & 1);
+    const unsigned cb = (unsigned)(gid >> 1);
+    const unsigned inst = fdiv(cb, a.fd_ncols);
+    const unsigned c = cb - inst * (unsigned)ncols;
+    R* col = reinterpret_cast<R*>(a.spec) + 2 * ((long)inst * a.sM + c) + part;
+    const long ls = 2 * ncols;   // level stride in R
+    const int nz = a.nz;
+    const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
+    const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
+    const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
+    const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
+    const double ks = a.hkx[i] + a.hky[j];
+    const double fxa = a.fxa;
+    double2* ck = ckp + threadIdx.x;
+    const int cs = blockDim.x;   // checkpoint stride
+    if (ks > 0) {
+        const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+        // one level of the forward elimination: cp(1) = c/b(1), dp(1) = d(1)/b(1);
+        // r = 1/(b(k) - cp(k-1) a), cp(k) = c r, dp(k) = (d(k) - dp(k-1) a) r
+        auto elim = [&](int k, double d, double& cp, double& dp) {
+            const double bk = (k == 0 || k == nz - 1) ? bend : bmid;
+            if (k == 0) {
+                cp = fxa / bk;
+                dp = d / bk;
+            } else {
+                const double r = __drcp_rn(bk - cp * fxa);   // == 1.0 / x (both correctly rounded)
+                cp = fxa * r;
+                dp = (d - dp * fxa) * r;
+            }
+        };
+        double cp = 0.0, dp = 0.0;
+        R nxt[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q)
+            if (IN(q < nz)) nxt[q] = col[(long)q * ls];
+        for (int kb = 0; kb < nz; kb += KC) {
+            R d[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = col[(long)(kb + KC + q) * ls];
+            ck[(kb / KC) * cs] = make_double2(cp, dp);   // (cp, dp) of level kb-1
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (IN(kb + q < nz)) elim(kb + q, (double)d[q], cp, dp);
         }
-        __syncwarp();
-    }
-    pdl_wait();   // the spectra were written by the preceding kernels
-    if (bulk) {
-        const unsigned rowb = (unsigned)nl * (unsigned)sizeof(T);
-        if (lane == 0) mbar_expect(&bar, rowb * (unsigned)nz);
-        __syncwarp();
-        for (int k = lane; k < nz; k += 32) bulk_copy_g2s(tile + (long)k * W, g + (long)k * ncols, rowb, &bar);
-        if (!mbar_wait(&bar, 0)) {
-            // the copies did not complete in time: report, give the copies in
-            // flight one more bounded wait, and leave the column untouched
-            if (lane == 0 && a.err) *(volatile unsigned*)a.err = 1u;
-            mbar_wait(&bar, 0);
-            return;
+        // back substitution, chunk by chunk from the top: x(nz) = dp(nz),
+        // x(k) = dp(k) - cp(k) x(k+1)
+        double x = 0.0;
+        const int last = (nz - 1) / KC;
+#pragma unroll
+        for (int q = 0; q < KC; ++q)
+            if (IN(last * KC + q < nz)) nxt[q] = col[(long)(last * KC + q) * ls];
+        for (int sg = last; sg >= 0; --sg) {
+            const int kb = sg * KC;
+            R d[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+            if (sg > 0) {
+#pragma unroll
+                for (int q = 0; q < KC; ++q) nxt[q] = col[(long)(kb - KC + q) * ls];
+            }
+            double cpl[KC], dpl[KC];
+            {
+                const double2 c0 = ck[sg * cs];
+                double cpv = c0.x, dpv = c0.y;
+#pragma unroll
+                for (int q = 0; q < KC; ++q) {
+                    if (IN(kb + q < nz)) elim(kb + q, (double)d[q], cpv, dpv);
+                    cpl[q] = cpv;
+                    dpl[q] = dpv;
+                }
+            }
+#pragma unroll
+            for (int q = KC - 1; q >= 0; --q) {
+                const int k = kb + q;
+                if (IN(k < nz)) {
+                    x = (k == nz - 1) ? dpl[q] : dpl[q] - cpl[q] * x;
+                    d[q] = (R)x;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
         }
     } else {
-        for (int k = 0; k < nz; ++k)
-            if (lane < nl) tile[k * W + lane] = g[(long)k * ncols + lane];
-        __syncwarp();
-    }
-    if (lane < nl) {
-        const unsigned cg = (unsigned)(c0 + lane + a.col0);   // global column: its wavenumbers
-        const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
-        const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
-        const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
-        const double ks = a.hkx[i] + a.hky[j];
-        T* col = tile + lane;
-        double* r = rs + lane;
-        double2* cp2 = ck + lane;
-        if (ks > 0) {
-            // a(k) = c(k) = fxa; b(k) = -ks - 2 fxa, -ks - fxa at both ends
-            const double fxa = a.fxa;
-            const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-            // forward elimination: cp(1) = c/b(1), dp(1) = d(1)/b(1); then
-            // r = 1/(b(k) - cp(k-1) a), cp(k) = c r, dp(k) = (d(k) - dp(k-1) a) r
-            double cp = fxa / bend;
-            double dx, dy;
-            {
-                const T d = col[0];
-                dx = (double)d.x / bend;
-                dy = (double)d.y / bend;
-            }
-            for (int k = 1; k < nz; ++k) {
-                if ((k & (kVsChunk - 1)) == 0) cp2[(k / kVsChunk) * W] = make_double2(dx, dy);   // dp(k-1)
-                const double bk = (k == nz - 1) ? bend : bmid;
-                const double rk = __drcp_rn(bk - cp * fxa);   // == 1.0 / x (both correctly rounded)
-                r[k * W] = rk;
-                cp = fxa * rk;
-                const T d = col[k * W];
-                dx = ((double)d.x - dx * fxa) * rk;
-                dy = ((double)d.y - dy * fxa) * rk;
-            }
-            // back substitution x(nz) = dp(nz), x(k) = dp(k) - cp(k) x(k+1),
-            // chunk by chunk from the top, each chunk's dp recomputed first
-            double xx = dx, xy = dy;
-            col[(nz - 1) * W] = mk<R>((R)xx, (R)xy);
-            const int nch = (nz - 1 + kVsChunk - 1) / kVsChunk;   // chunks covering levels 0 .. nz-2
-            for (int s = nch - 1; s >= 0; --s) {
-                const int kb = s * kVsChunk;
-                const int ke = min(kb + kVsChunk, nz - 1);   // levels kb .. ke-1
-                double px[kVsChunk], py[kVsChunk];
-                double ppx, ppy;
-                if (kb == 0) {
-                    const T d = col[0];
-                    ppx = (double)d.x / bend;
-                    ppy = (double)d.y / bend;
-                } else {
-                    const double2 c = cp2[s * W];
-                    const T d = col[kb * W];
-                    const double rk = r[kb * W];
-                    ppx = ((double)d.x - c.x * fxa) * rk;
-                    ppy = ((double)d.y - c.y * fxa) * rk;
-                }
-                px[0] = ppx; py[0] = ppy;
+        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr,
+        // in chunks with the next chunk's loads in flight like the sweeps above
+        const double h = a.dz2dsqr;
+        double x0 = 0.0, x1 = 0.0, fprev = 0.0;   // p(k-2), p(k-1), f(k-1)
+        R nxt[KC];
 #pragma unroll
-                for (int q = 1; q < kVsChunk; ++q) {
-                    const int k = kb + q;
-                    if (k < ke) {
-                        const T d = col[k * W];
-                        const double rk = r[k * W];
-                        ppx = ((double)d.x - ppx * fxa) * rk;
-                        ppy = ((double)d.y - ppy * fxa) * rk;
-                        px[q] = ppx; py[q] = ppy;
-                    }
-                }
+        for (int q = 0; q < KC; ++q)
+            if (IN(q < nz)) nxt[q] = col[(long)q * ls];
+        for (int kb = 0; kb < nz; kb += KC) {
+            R d[KC];
 #pragma unroll
-                for (int q = kVsChunk - 1; q >= 0; --q) {
-                    const int k = kb + q;
-                    if (k < ke) {
-                        const double cpk = k == 0 ? fxa / bend : fxa * r[k * W];   // cp(k)
-                        xx = px[q] - cpk * xx;
-                        xy = py[q] - cpk * xy;
-                        col[k * W] = mk<R>((R)xx, (R)xy);
-                    }
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = col[(long)(kb + KC + q) * ls];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int k = kb + q;
+                if (IN(k < nz)) {
+                    const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
+                    fprev = (double)d[q];
+                    x0 = x1; x1 = xk;
+                    d[q] = (R)xk;
                 }
             }
-        } else {
-            // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
-            const double h = a.dz2dsqr;
-            double x0x = 0.0, x0y = 0.0, x1x = 0.0, x1y = 0.0, fx = 0.0, fy = 0.0;
-            for (int k = 0; k < nz; ++k) {
-                const T d = col[k * W];
-                const double xkx = k == 0 ? 0.0 : 2 * x1x - x0x + fx * h;
-                const double xky = k == 0 ? 0.0 : 2 * x1y - x0y + fy * h;
-                fx = (double)d.x;
-                fy = (double)d.y;
-                x0x = x1x; x0y = x1y;
-                x1x = xkx; x1y = xky;
-                col[k * W] = mk<R>((R)xkx, (R)xky);
-            }
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
         }
     }
-    __syncwarp();
-    for (int k = 0; k < nz; ++k)
-        if (lane < nl) g[(long)k * ncols + lane] = tile[k * W + lane];
 }
+#undef IN
 
 // ---------------------------------------------------------------------------
 // K3, triply periodic: z FFT, spectral division, inverse z FFT
@@ -1226,7 +1216,8 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
-    if ((e = max_dynamic_smem(k_vsolve<R>))) return e;
+    if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
+    if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
     if ((e = setup_m<R, 16>())) return e;
     return setup_m<R, 8>();
 }
@@ -1290,14 +1281,11 @@ cudaError_t launch_plane_inv(const PlaneArgs& a, bool fp32, cudaStream_t s) {
     return fp32 ? launch_plane_t<float, false>(a, s) : launch_plane_t<double, false>(a, s);
 }
 
-// columns per tile of the vertical solve: 32 (one per lane) while two tiles
-// fit in an SM's shared memory, fewer for tall columns; 0 when not even two
-// columns fit in one block's shared memory
-int vsolve_tile_width(int nz, bool fp32) {
-    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
-    const size_t lim = 227 * 1024 - 64;
-    for (int W = 32; W >= 2; W /= 2)
-        if ((W == 32 && vsolve_smem(nz, W, es) <= lim / 2) || (W < 32 && vsolve_smem(nz, W, es) <= lim)) return W;
+// threads per block of the vertical solve: 128 while its checkpoints fit
+// in a block's shared memory, fewer for tall columns; 0 when not even 32 fit
+int thomas_threads(int nz) {
+    for (int t = kThomasThreads; t >= 32; t /= 2)
+        if (thomas_smem(nz, t) <= 227 * 1024 - 64) return t;
     return 0;
 }
 
@@ -1307,16 +1295,18 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     a.fd_ncols = make_fastdiv((unsigned)ncols);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_nxh = make_fastdiv(a.nxh);
-    const int W = vsolve_tile_width(a.nz, fp32);
-    if (W == 0 || ncols < 1) return cudaErrorInvalidValue;
-    const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
-    // bulk copies need 16-byte aligned rows whose length is a multiple of 16 bytes
-    const int bulk = ((size_t)ncols * es) % 16 == 0 && ((uintptr_t)a.spec & 15) == 0 && ((size_t)W * es) % 16 == 0;
-    const unsigned tpi = (unsigned)((ncols + W - 1) / W);
-    const dim3 g(tpi * (unsigned)std::max(1, a.batch)), b(32);
-    const size_t sm = vsolve_smem(a.nz, W, es);
-    if (fp32) return launch_pdl(k_vsolve<float>, g, b, sm, s, a, W, tpi, bulk);
-    return launch_pdl(k_vsolve<double>, g, b, sm, s, a, W, tpi, bulk);
+    const int nt = thomas_threads(a.nz);
+    if (nt == 0 || ncols < 1) return cudaErrorInvalidValue;
+    const long nthreads = 2 * ncols * std::max(1, a.batch);
+    const int blocks = (int)((nthreads + nt - 1) / nt);
+    const size_t sm = thomas_smem(a.nz, nt);
+    const dim3 g(blocks), b(nt);
+    if (a.nz % kThomasChunk == 0) {
+        if (fp32) return launch_pdl(k_thomas<float, true>, g, b, sm, s, a);
+        return launch_pdl(k_thomas<double, true>, g, b, sm, s, a);
+    }
+    if (fp32) return launch_pdl(k_thomas<float, false>, g, b, sm, s, a);
+    return launch_pdl(k_thomas<double, false>, g, b, sm, s, a);
 }
 
 static size_t zsolve_smem(int nz, size_t es) {

@@ -16,7 +16,7 @@
 //   transpose   all-to-all: each rank receives every rank's levels of its own
 //               columns, i.e. whole columns [nz][ccnt] (pressure_solver.f90
 //               needs the full column for the tridiagonal solve)
-//   vsolve      the Thomas solves of those columns (k_vsolve on a column slab)
+//   vsolve      the Thomas solves of those columns (k_thomas on a column slab)
 //   transpose   all-to-all back, unpacked into [nzl][kx][ky]
 //   inverse     per-level inverse 2D transforms into p (pending correction)
 //   p halo      p one level below and two above (the step kernel's lazy
@@ -156,7 +156,6 @@ int slab_vsolve(ps3d_slab* s) {
     a.hkx = (const double*)c.t_hkx.p; a.hky = (const double*)c.t_hky.p;
     a.fxa = 1.0 / (c.P.dz * c.P.dz) / c.P.dsqr;
     a.dz2dsqr = c.P.dz * c.P.dz * c.P.dsqr;
-    a.err = c.kerr_d;
     a.col0 = s->cbeg[s->rank]; a.ncl = s->ccnt[s->rank];
     CK(ps3d::launch_thomas(a, s->mixed, c.stream));
     return PS3D_OK;

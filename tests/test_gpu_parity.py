@@ -31,6 +31,15 @@ def plane_impl(request, monkeypatch):
     return request.param
 
 
+@pytest.fixture(autouse=True, params=["ring", "warp-specialised"])
+def step_form(request, monkeypatch):
+    """... and on both forms of the step kernel: all threads loading and
+    computing over a three-plane ring, and producer warps staging a
+    four-plane ring for consumer warps."""
+    monkeypatch.setenv("PS3D_STEP_FORM", {"ring": "0", "warp-specialised": "1"}[request.param])
+    return request.param
+
+
 def _pair(p, fields, pfield=None):
     o = Oracle(p)
     load_oracle(o, fields, pfield)

@@ -77,14 +77,10 @@ def test_mixed_request_matches_fp64():
     for n in ("u", "v", "w", "b"):
         a, b = rmx.fields[n][2:-2, 2:-2, 2:-2], r64.fields[n][2:-2, 2:-2, 2:-2]
         err[n] = np.linalg.norm(a - b) / np.linalg.norm(b)
-    # w is the balanced state's small ageostrophic part: its own norm is
-    # ~1e-3 of the horizontal velocity's, so its error is also held against
-    # the velocity scale ||(u, v, w)||
-    uvw = np.sqrt(sum(np.linalg.norm(r64.fields[n][2:-2, 2:-2, 2:-2]) ** 2 for n in ("u", "v", "w")))
-    w_abs = np.linalg.norm(rmx.fields["w"][2:-2, 2:-2, 2:-2] - r64.fields["w"][2:-2, 2:-2, 2:-2])
-    print(f"\n[serve mixed vs fp64] rel L2 {err}; w error / ||(u,v,w)|| = {w_abs / uvw:.3e}; "
-          f"||w||/||(u,v,w)|| = {np.linalg.norm(r64.fields['w'][2:-2, 2:-2, 2:-2]) / uvw:.3e}")
-    assert max(err["u"], err["v"], err["b"]) < 1e-5 and w_abs / uvw < 1e-5 and err["w"] < 1e-3, err
+    # the mixed path's 1e-5 bound in every field, w (the balanced state's
+    # small ageostrophic part, ~6e-4 of the velocity's norm) included
+    print(f"\n[serve mixed vs fp64] rel L2 {err}")
+    assert max(err.values()) < 1e-5, err
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
