@@ -363,10 +363,11 @@ PS3D_API int ps3d_slab_phase(ps3d_slab* s, int phase);
 PS3D_API int ps3d_slab_sync(ps3d_slab* s);
 PS3D_API int ps3d_slab_group_step(ps3d_slab* const* ranks, int n, int nsteps);
 
-/* ---- serving loop for optimal-balance requests (no counterpart in the
- * reference) ---------------------------------------------------------------
- * Requests (one diag_opt_balance each, on their own grid and state) are
- * admitted in arrival order as execution slots and device memory free up:
+/* ---- serving loop for optimal-balance and ensemble requests (no
+ * counterpart in the reference) -------------------------------------------
+ * Requests (one diag_opt_balance each, on their own grid and state, or one
+ * ensemble run) are admitted in arrival order as execution slots and device
+ * memory free up:
  * the sum of the admitted requests' footprints (ps3d_server_footprint) stays
  * within hbm_budget_bytes (0: 80% of free memory).  Each admitted request
  * runs on its own CUDA stream, so concurrent requests overlap on the GPU;
@@ -384,6 +385,17 @@ PS3D_API int ps3d_server_submit(ps3d_server* s, const ps3d_params* prm, const ps
  * is handed out once.                                                      */
 PS3D_API int ps3d_server_wait(ps3d_server* s, long long ticket, int timeout_ms,
                               double* u_bal, double* v_bal, double* w_bal, double* b_bal, double* res);
+/* An ensemble run as a request: members[0..n-1] (any grid sizes), each
+ * advanced nsteps main-loop steps from its halo-layout u[m], v[m], w[m],
+ * b[m] in batched launches (ps3d_ensemble_*); its footprint is the sum of the
+ * members'.  ps3d_server_wait_ensemble copies member m's final state to
+ * u[m] .. b[m] (any array or entry NULL to skip) and fills res[6] as
+ * ps3d_server_wait does (norm 0, iterations = nsteps).                     */
+PS3D_API int ps3d_server_submit_ensemble(ps3d_server* s, const ps3d_params* members, int n, int nsteps,
+                                         const double* const* u, const double* const* v, const double* const* w,
+                                         const double* const* b, long long* ticket);
+PS3D_API int ps3d_server_wait_ensemble(ps3d_server* s, long long ticket, int timeout_ms, double* const* u,
+                                       double* const* v, double* const* w, double* const* b, double* res);
 PS3D_API int ps3d_server_cancel(ps3d_server* s, long long ticket);
 /* stats[6] = {active, queued, bytes in use, peak bytes, peak active, budget} */
 PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats);

@@ -1,7 +1,9 @@
 // serve.cu — a request loop for optimal-balance integrations.
 //
-// Each request is one diag_opt_balance (for_src/diag_opt_balance.f90:55-179)
-// on its own grid and initial state.  Requests are admitted in arrival order
+// A request is one diag_opt_balance (for_src/diag_opt_balance.f90:55-179)
+// on its own grid and initial state, or one ensemble run: n members of any
+// grid sizes advanced nsteps main-loop steps together in batched launches
+// (ps3d_ensemble_*), their final states returned.  Requests are admitted in arrival order
 // as execution slots and HBM free up: a request's device footprint is
 // computed from its grid before admission and the sum over running requests
 // never exceeds the budget.  Every admitted request owns a context with its
@@ -38,8 +40,12 @@ enum State { kQueued, kRunning, kDone, kFailed, kCancelled };
 
 struct Request {
     long long id = 0;
+    int kind = 0;                   // 0: optimal balance, 1: ensemble run
     ps3d_params prm{};
     ps3d_optbal opt{};
+    std::vector<ps3d_params> members;   // ensemble run: the members, nsteps each
+    int nsteps = 0;
+    std::vector<std::vector<double>> ein, eout;   // ensemble run: [member * 4 + field], halo layout
     std::vector<double> in[4];      // halo-layout input fields
     std::vector<double> out[4];     // balanced fields (u_bal..b_bal)
     size_t footprint = 0;
@@ -97,11 +103,46 @@ struct ps3d_server {
 
 static bool same_params(const ps3d_params& a, const ps3d_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
 
+// An ensemble run: batched contexts of its own (not pooled), advanced in
+// chunks of 30 steps (a multiple of the graph period 3) with the cancel flag
+// checked between chunks.
+static int run_ensemble(Request& r, int device) {
+    const int n = (int)r.members.size();
+    ps3d_ensemble* e = nullptr;
+    int rc = ps3d_ensemble_create(r.members.data(), n, device, &e);
+    for (int m = 0; m < n && !rc; ++m)
+        rc = ps3d_ensemble_upload(e, m, r.ein[4 * m].data(), r.ein[4 * m + 1].data(), r.ein[4 * m + 2].data(),
+                                  r.ein[4 * m + 3].data());
+    for (int left = r.nsteps; left > 0 && !rc;) {
+        if (r.cancel.load(std::memory_order_relaxed)) { rc = PS3D_ERR_CANCELLED; break; }
+        const int c = left < 30 ? left : 30;
+        rc = ps3d_ensemble_integrate(e, c);
+        left -= c;
+    }
+    if (!rc) {
+        r.eout.assign(4 * (size_t)n, std::vector<double>());
+        for (int m = 0; m < n && !rc; ++m) {
+            const ps3d_params& q = r.members[m];
+            const size_t n3 = (size_t)(q.nx + 4) * (q.ny + 4) * (q.nz + 4);
+            for (int f = 0; f < 4; ++f) r.eout[4 * m + f].assign(n3, 0.0);
+            std::vector<double> pbuf(n3);
+            rc = ps3d_ensemble_download(e, m, r.eout[4 * m].data(), r.eout[4 * m + 1].data(), r.eout[4 * m + 2].data(),
+                                        r.eout[4 * m + 3].data(), pbuf.data());
+        }
+    }
+    if (e) ps3d_ensemble_destroy(e);
+    return rc;
+}
+
 // Runs request r on `reuse` (an idle context of the same parameters) or on a
 // new context; returns the context for the idle pool when the request
 // succeeded.
 std::unique_ptr<Ctx> ps3d_server::run(Request& r, std::unique_ptr<Ctx> reuse) {
     cudaSetDevice(device);
+    if (r.kind == 1) {
+        r.status = run_ensemble(r, device);
+        return nullptr;
+    }
     std::unique_ptr<Ctx> cp = std::move(reuse);
     int rc = PS3D_OK;
     if (cp) {
@@ -152,7 +193,7 @@ void ps3d_server::worker_loop() {
                 if (!queue.empty() && active < max_active) {
                     const std::shared_ptr<Request>& q = queue.front();
                     long hit = -1;
-                    for (size_t i = 0; i < idle.size() && hit < 0; ++i)
+                    for (size_t i = 0; i < idle.size() && hit < 0 && q->kind == 0; ++i)
                         if (same_params(idle[i].prm, q->prm)) hit = (long)i;
                     bool fits = hit >= 0;
                     while (!fits && !idle.empty() && used + q->footprint > budget) {   // no hit: free idle ones
@@ -193,6 +234,8 @@ void ps3d_server::worker_loop() {
             r->t_end = Clock::now();
             r->state = r->status == PS3D_OK ? kDone : (r->status == PS3D_ERR_CANCELLED ? kCancelled : kFailed);
             for (int f = 0; f < 4; ++f) { r->in[f].clear(); r->in[f].shrink_to_fit(); }
+            r->ein.clear();
+            r->ein.shrink_to_fit();
             --active;
             if (done && !stopping) idle.push_back({r->prm, std::move(done), r->footprint});
             else used -= r->footprint;
@@ -291,6 +334,51 @@ PS3D_API int ps3d_server_submit(ps3d_server* s, const ps3d_params* prm, const ps
     SGUARD_END
 }
 
+// An ensemble run as a request: n members (any grid sizes; members with
+// identical parameters share launches), each advanced nsteps main-loop steps
+// from the given halo-layout state.  Admitted by the sum of the members'
+// footprints like any request.
+PS3D_API int ps3d_server_submit_ensemble(ps3d_server* s, const ps3d_params* members, int n, int nsteps,
+                                         const double* const* u, const double* const* v, const double* const* w,
+                                         const double* const* b, long long* ticket) {
+    SGUARD_BEGIN
+    if (!s || !members || n < 1 || nsteps < 0 || !u || !v || !w || !b || !ticket) return PS3D_ERR_BADPARAM;
+    auto r = std::make_shared<Request>();
+    r->kind = 1;
+    r->nsteps = nsteps;
+    r->members.assign(members, members + n);
+    r->footprint = 0;
+    for (int m = 0; m < n; ++m) {
+        const ps3d_params& p = members[m];
+        const bool rigid = p.enable_vertical_boundaries != 0;
+        if (p.nx < 2 || p.ny < 2 || p.nz < 2 || p.nx % 2 || p.ny % 2 || (!rigid && p.nz % 2)) return PS3D_ERR_BADPARAM;
+        if (!ps3d::fft_length_ok(p.nx / 2) || !ps3d::fft_length_ok(p.ny) || (!rigid && !ps3d::fft_length_ok(p.nz)))
+            return PS3D_ERR_BADPARAM;
+        if (!u[m] || !v[m] || !w[m] || !b[m]) return PS3D_ERR_BADPARAM;
+        r->footprint += footprint_of(p);
+    }
+    if (r->footprint > s->budget) return PS3D_ERR_OOM;   // can never be admitted
+    r->ein.resize(4 * (size_t)n);
+    for (int m = 0; m < n; ++m) {
+        const ps3d_params& p = members[m];
+        const size_t n3 = (size_t)(p.nx + 4) * (p.ny + 4) * (p.nz + 4);
+        const double* f[4] = {u[m], v[m], w[m], b[m]};
+        for (int q = 0; q < 4; ++q) r->ein[4 * m + q].assign(f[q], f[q] + n3);
+    }
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stopping) return PS3D_ERR_CANCELLED;
+        r->id = s->next_id++;
+        s->all[r->id] = r;
+        s->queue.push_back(r);
+    }
+    s->cv_work.notify_all();
+    *ticket = r->id;
+    return PS3D_OK;
+    SGUARD_END
+}
+
 // Wait up to timeout_ms for a request.  On success the balanced fields are
 // copied out (any pointer may be NULL) and res receives
 // {status, final norm, iterations, latency ms, queue ms, run ms}.
@@ -310,7 +398,7 @@ PS3D_API int ps3d_server_wait(ps3d_server* s, long long ticket, int timeout_ms,
             return PS3D_ERR_TIMEOUT;
     }
     double* out[4] = {u_bal, v_bal, w_bal, b_bal};
-    if (r->state == kDone)
+    if (r->state == kDone && r->kind == 0)
         for (int q = 0; q < 4; ++q)
             if (out[q] && !r->out[q].empty()) std::memcpy(out[q], r->out[q].data(), r->out[q].size() * sizeof(double));
     if (res) {
@@ -327,6 +415,47 @@ PS3D_API int ps3d_server_wait(ps3d_server* s, long long ticket, int timeout_ms,
     }
     const int st = r->status;
     s->all.erase(ticket);   // results are handed out once
+    return st;
+    SGUARD_END
+}
+
+// Wait for an ensemble run; on success member m's final u, v, w, b (halo
+// layout) are copied to u[m] .. b[m] (an array, or one of its entries, may
+// be NULL); res as for ps3d_server_wait (norm 0, iterations = nsteps).
+PS3D_API int ps3d_server_wait_ensemble(ps3d_server* s, long long ticket, int timeout_ms, double* const* u,
+                                       double* const* v, double* const* w, double* const* b, double* res) {
+    SGUARD_BEGIN
+    if (!s) return PS3D_ERR_BADPARAM;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end() || it->second->kind != 1) return PS3D_ERR_BADPARAM;
+    std::shared_ptr<Request> r = it->second;
+    const auto deadline = Clock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
+    while (r->state == kQueued || r->state == kRunning) {
+        if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout &&
+            (r->state == kQueued || r->state == kRunning))
+            return PS3D_ERR_TIMEOUT;
+    }
+    double* const* out[4] = {u, v, w, b};
+    if (r->state == kDone)
+        for (size_t m = 0; m < r->members.size(); ++m)
+            for (int q = 0; q < 4; ++q)
+                if (out[q] && out[q][m] && !r->eout[4 * m + q].empty())
+                    std::memcpy(out[q][m], r->eout[4 * m + q].data(), r->eout[4 * m + q].size() * sizeof(double));
+    if (res) {
+        auto ms = [](Clock::time_point a, Clock::time_point c) {
+            return std::chrono::duration<double, std::milli>(c - a).count();
+        };
+        res[0] = r->status;
+        res[1] = 0.0;
+        res[2] = r->nsteps;
+        const bool ran = r->state != kCancelled || r->t_start.time_since_epoch().count() != 0;
+        res[3] = ms(r->t_submit, r->t_end);
+        res[4] = ran ? ms(r->t_submit, r->t_start) : res[3];
+        res[5] = ran ? ms(r->t_start, r->t_end) : 0.0;
+    }
+    const int st = r->status;
+    s->all.erase(ticket);
     return st;
     SGUARD_END
 }

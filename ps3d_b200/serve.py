@@ -1,7 +1,10 @@
-"""Serving loop for optimal-balance requests over the C ABI (ps3d_server_*).
+"""Serving loop for optimal-balance and ensemble requests over the C ABI
+(ps3d_server_*).
 
 `Server.submit` copies one request (grid parameters, opt-balance knobs, the
-initial state in the halo layout) into the engine's queue; requests are
+initial state in the halo layout) into the engine's queue;
+`Server.submit_ensemble` queues an ensemble run (members of any sizes,
+nsteps steps each, in batched launches); requests are
 admitted in arrival order as slots and HBM free up and run concurrently on
 their own CUDA streams.  `replay_poisson` drives a seeded Poisson arrival
 process against a server and reports latency percentiles and throughput.
@@ -26,6 +29,10 @@ def _lib():
         L.ps3d_server_submit.argtypes = [vp, C.POINTER(Params), C.POINTER(OptBal), dp, dp, dp, dp,
                                          C.POINTER(C.c_longlong)]
         L.ps3d_server_wait.argtypes = [vp, C.c_longlong, C.c_int, dp, dp, dp, dp, dp]
+        pp = C.POINTER(dp)
+        L.ps3d_server_submit_ensemble.argtypes = [vp, C.POINTER(Params), C.c_int, C.c_int, pp, pp, pp, pp,
+                                                  C.POINTER(C.c_longlong)]
+        L.ps3d_server_wait_ensemble.argtypes = [vp, C.c_longlong, C.c_int, pp, pp, pp, pp, dp]
         L.ps3d_server_cancel.argtypes = [vp, C.c_longlong]
         L.ps3d_server_stats.argtypes = [vp, dp]
         L.ps3d_server_footprint.restype = C.c_longlong
@@ -88,6 +95,36 @@ class Server:
             raise PS3DError(rc, "ps3d_server_wait")
         self._params.pop(ticket, None)
         return Result(res, dict(zip(("u", "v", "w", "b"), out)) if out[0] is not None else None)
+
+    def submit_ensemble(self, members, states, nsteps):
+        """An ensemble run: members (Params list), states[m] = {u, v, w, b}
+        in the halo layout, nsteps steps each.  Returns a ticket for
+        wait_ensemble."""
+        n = len(members)
+        arr = (Params * n)(*members)
+        keep = [[np.ascontiguousarray(st[f], dtype=np.float64) for f in ("u", "v", "w", "b")] for st in states]
+        ptrs = [(C.POINTER(C.c_double) * n)(*[dptr(keep[m][f]) for m in range(n)]) for f in range(4)]
+        t = C.c_longlong()
+        rc = self.L.ps3d_server_submit_ensemble(self.h, arr, n, nsteps, *ptrs, C.byref(t))
+        if rc:
+            raise PS3DError(rc, "ps3d_server_submit_ensemble")
+        self._params[t.value] = [m.copy() for m in members]
+        return t.value
+
+    def wait_ensemble(self, ticket, timeout_ms=600000):
+        """Result of an ensemble run: fields = [{u, v, w, b} per member]."""
+        members = self._params.get(ticket)
+        if members is None:
+            raise PS3DError(abi.PS3D_ERR_BADPARAM, "ps3d_server_wait_ensemble")
+        n = len(members)
+        outs = [{f: np.zeros(halo_shape(m)) for f in ("u", "v", "w", "b")} for m in members]
+        ptrs = [(C.POINTER(C.c_double) * n)(*[dptr(outs[m][f]) for m in range(n)]) for f in ("u", "v", "w", "b")]
+        res = (C.c_double * 6)()
+        rc = self.L.ps3d_server_wait_ensemble(self.h, ticket, timeout_ms, *ptrs, res)
+        if rc == abi.PS3D_ERR_TIMEOUT and res[3] == 0.0:
+            raise PS3DError(rc, "ps3d_server_wait_ensemble")
+        self._params.pop(ticket, None)
+        return Result(res, outs)
 
     def cancel(self, ticket):
         rc = self.L.ps3d_server_cancel(self.h, ticket)

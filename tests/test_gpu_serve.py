@@ -186,3 +186,46 @@ def test_malformed_params_refused():
         s.submit(q, opt, f)
     assert ei.value.status == abi.PS3D_ERR_BADPARAM
     s.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_ensemble_request_matches_standalone_ensemble(precision):
+    """An ensemble run submitted as a request, admitted beside optimal-balance
+    requests, ends bit for bit where the same ensemble run directly ends."""
+    from ps3d_b200 import configs as cf
+    from ps3d_b200.ensemble import Ensemble
+    sizes = [(32, 32, 16), (64, 32, 16), (32, 32, 16), (64, 64, 16)]
+    members = [cf.eddy_params(*sz, precision=precision) for sz in sizes]
+    states = [cf.add_noise(p, cf.eddy_fields(p, amp=0.05 + 0.03 * i), "b", rel=1e-3, seed=i)
+              for i, p in enumerate(members)]
+    nsteps = 23
+    s = Server(max_active=3)
+    others = [s.submit(*_req((64, 32, 16), precision=precision)), s.submit(*_req((32, 32, 16)))]
+    t = s.submit_ensemble(members, states, nsteps)
+    res = s.wait_ensemble(t)
+    for o in others:
+        assert s.wait(o).status == 0
+    st = s.stats()
+    s.close()
+    assert res.status == 0 and res.iters == nsteps
+    assert st["peak_active"] >= 2
+    ens = Ensemble(members)
+    for i, f in enumerate(states):
+        ens.upload(i, f["u"], f["v"], f["w"], f["b"])
+    ens.integrate(nsteps)
+    for i in range(len(members)):
+        ref = ens.download(i)
+        for n in ("u", "v", "w", "b"):
+            assert np.array_equal(res.fields[i][n], ref[n]), (i, n)
+    ens.close()
+
+
+def test_ensemble_request_refused_when_it_can_never_fit():
+    from ps3d_b200 import configs as cf
+    members = [cf.eddy_params(64, 64, 32) for _ in range(3)]
+    states = [cf.eddy_fields(p) for p in members]
+    s = Server(hbm_budget_bytes=Server.footprint(members[0]) * 2, max_active=2)
+    with pytest.raises(PS3DError) as ei:
+        s.submit_ensemble(members, states, 5)
+    assert ei.value.status == abi.PS3D_ERR_OOM
+    s.close()
