@@ -134,9 +134,80 @@ cudaError_t launch_project(const ProjArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The same product with the matrix staged in shared memory as well (nz^2
+// doubles beside the tile; nz <= 104 keeps two blocks per SM): the matrix
+// pairs are then warp-uniform shared-memory loads instead of L1 loads.  A
+// block copies the matrix once and runs kVmTiles column tiles in turn, so
+// the copy is amortised.
+constexpr int kVmTiles = 4;
+size_t vert_mode_smem_staged(int nz) { return (size_t)nz * kVmCols * sizeof(double2) + (size_t)nz * nz * sizeof(double); }
+
+__global__ void __launch_bounds__(kVmThreads) k_vert_mode_staged(const double2* __restrict__ in,
+                                                                 double2* __restrict__ out,
+                                                                 const double* __restrict__ A, int nz, long ncol,
+                                                                 double scale) {
+    extern __shared__ double2 tile[];   // [nz][kVmCols], then the matrix [ki][ko]
+    double* Am = reinterpret_cast<double*>(tile + (size_t)nz * kVmCols);
+    for (int t = threadIdx.x; t < nz * nz; t += blockDim.x) Am[t] = __ldg(A + t);
+    const int l = threadIdx.x % kVmCols;
+    const int wid = threadIdx.x / kVmCols, nw = blockDim.x / kVmCols;
+    const int nch = (nz + kVmKo - 1) / kVmKo;
+    for (int tt = 0; tt < kVmTiles; ++tt) {
+        const long c0 = ((long)blockIdx.x * kVmTiles + tt) * kVmCols;
+        if (c0 >= ncol) break;
+        const int nl = (int)min((long)kVmCols, ncol - c0);
+        __syncthreads();   // the previous tile is read (and, the first time, nothing)
+        for (int t = threadIdx.x; t < nz * kVmCols; t += blockDim.x) {
+            const int k = t / kVmCols, ll = t - k * kVmCols;
+            tile[t] = (ll < nl) ? in[(long)k * ncol + c0 + ll] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        if (l < nl) {
+            for (int ch = wid; ch < nch; ch += nw) {
+                const int ko0 = ch * kVmKo;
+                double ar[kVmKo], ai[kVmKo];
+#pragma unroll
+                for (int q = 0; q < kVmKo; ++q) { ar[q] = 0.0; ai[q] = 0.0; }
+                if (ko0 + kVmKo <= nz) {
+#pragma unroll 2
+                    for (int ki = 0; ki < nz; ++ki) {
+                        const double2 v = tile[ki * kVmCols + l];
+                        const double2* row = reinterpret_cast<const double2*>(Am + ko0 + nz * ki);
+#pragma unroll
+                        for (int q = 0; q < kVmKo / 2; ++q) {
+                            const double2 m = row[q];
+                            ar[2 * q] = fma(v.x, m.x, ar[2 * q]);
+                            ai[2 * q] = fma(v.y, m.x, ai[2 * q]);
+                            ar[2 * q + 1] = fma(v.x, m.y, ar[2 * q + 1]);
+                            ai[2 * q + 1] = fma(v.y, m.y, ai[2 * q + 1]);
+                        }
+                    }
+                } else {
+                    for (int ki = 0; ki < nz; ++ki) {
+                        const double2 v = tile[ki * kVmCols + l];
+#pragma unroll
+                        for (int q = 0; q < kVmKo; ++q) {
+                            if (ko0 + q < nz) {
+                                const double m = Am[ko0 + q + nz * ki];
+                                ar[q] = fma(v.x, m, ar[q]);
+                                ai[q] = fma(v.y, m, ai[q]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kVmKo; ++q)
+                    if (ko0 + q < nz) out[(long)(ko0 + q) * ncol + c0 + l] = make_double2(ar[q] * scale, ai[q] * scale);
+            }
+        }
+    }
+}
+
 // opts the transform in to its dynamic shared memory on the current device
 cudaError_t modes_setup() {
     cudaError_t e = cudaFuncSetAttribute(k_vert_mode<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_vert_mode_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_vert_mode<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
@@ -144,6 +215,17 @@ cudaError_t modes_setup() {
 cudaError_t launch_vert_mode(const double2* in, double2* out, const double* A, int nz, long ncol, double scale,
                              cudaStream_t s) {
     if (!vert_mode_fits(nz)) return cudaErrorInvalidValue;
+    // the staged form where two blocks fit an SM and nz is even (16-byte
+    // matrix pairs); PS3D_VMODE_FORM=0|1 pins the form
+    int form = (nz % 2 == 0 && vert_mode_smem_staged(nz) <= 113 * 1024) ? 1 : 0;
+    if (const char* f = std::getenv("PS3D_VMODE_FORM"))
+        if ((f[0] == '0' || f[0] == '1') && (f[0] == '0' || (nz % 2 == 0 && vert_mode_smem_staged(nz) <= 227 * 1024)))
+            form = f[0] - '0';
+    if (form == 1) {
+        const int blocks = (int)((ncol + (long)kVmCols * kVmTiles - 1) / ((long)kVmCols * kVmTiles));
+        k_vert_mode_staged<<<blocks, kVmThreads, vert_mode_smem_staged(nz), s>>>(in, out, A, nz, ncol, scale);
+        return cudaGetLastError();
+    }
     const size_t sm = vert_mode_smem(nz);
     const int blocks = (int)((ncol + kVmCols - 1) / kVmCols);
     if (nz % 2 == 0) k_vert_mode<true><<<blocks, kVmThreads, sm, s>>>(in, out, A, nz, ncol, scale);
