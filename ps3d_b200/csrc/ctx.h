@@ -119,7 +119,6 @@ struct Ctx {
     int win_kbeg = 0, win_kcount = 0, win_kofs = 0, win_nzg = 0;
     bool split_solve = false;
     int kchunk = 8;             // z levels per block of the step kernel
-    int kform = 0;              // step kernel form: 0 all threads load and compute, 1 warp-specialised
     std::string tuned;          // description of the autotuned choice
     DevBuf twx;
     DevBuf t_kx, t_ky, t_kz, t_hkx, t_hky, t_hkz, t_ex, t_ey, t_ez, t_px, t_py, t_pz, t_sz, t_cz, t_hkz_ds;

@@ -388,10 +388,9 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     CK(cudaStreamSynchronize(stream));
     int rc = autotune();
     if (rc) return rc;
-    // PS3D_STEP_FORM=0|1 pins the step kernel's form over the default or the
-    // tuner's choice (the parity suite runs both)
-    if (const char* sf = std::getenv("PS3D_STEP_FORM"))
-        if (sf[0] == '0' || sf[0] == '1') kform = sf[0] - '0';
+    // PS3D_GRAPHS=0: no CUDA-graph replay of the main loop (eager launches)
+    if (const char* g = std::getenv("PS3D_GRAPHS"))
+        if (g[0] == '0') use_graphs = false;
     CK(cudaMemsetAsync(p.p, 0, p.bytes, stream));   // the tuner's timing runs wrote p
     return PS3D_OK;
 }
@@ -439,7 +438,7 @@ DevBuf* Ctx::fieldset(int which) {
 int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
     StepArgs a{};
     a.nx = nx; a.ny = ny; a.nz = nz;
-    a.batch = batch; a.sN = N; a.kchunk = kchunk; a.form = kform;
+    a.batch = batch; a.sN = N; a.kchunk = kchunk;
     a.kbeg = win_kbeg; a.kcount = win_kcount; a.kofs = win_kofs; a.nzg = win_nzg;
     a.rigid = rigid; a.nonlinear = P.enable_nonlinear != 0;
     a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz;
@@ -612,7 +611,7 @@ int Ctx::autotune() {
         a.px = pol == 0 ? plx.plan : pol == 1 ? plx4.plan : plx8.plan;
         a.py = pol == 0 ? ply.plan : pol == 1 ? ply4.plan : ply8.plan;
     };
-    auto apply = [&](int im, int C, int rc, int tj, int ly, int pol, int kc, int sf) -> bool {
+    auto apply = [&](int im, int C, int rc, int tj, int ly, int pol, int kc) -> bool {
         for (const PlaneArgs& c : plane_candidates(nx, ny, f32 ? sizeof(float2) : sizeof(double2), pa)) {
             if (c.impl != im) continue;
             if (im == 0 && (c.C != C || c.row_chunk != rc)) continue;
@@ -620,23 +619,19 @@ int Ctx::autotune() {
             pa = c;
             plans_of(pol, pa);
             kchunk = kc;
-            kform = sf;
             return true;
         }
         return false;
     };
     // PS3D_TUNE pins a configuration in the cache's format, e.g.
-    // "im1,C1,rc8,tj16,ly8,pol2,kc8,sf1" (reproducible profiling, no timing
-    // runs; sf, the step kernel's form, defaults to 0 when absent)
+    // "im1,C1,rc8,tj16,ly8,pol2,kc8" (reproducible profiling, no timing runs)
     auto parse = [](const char* str, int* v) {
-        const int n = std::sscanf(str, "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d,sf%d", &v[0], &v[1], &v[2], &v[3], &v[4],
-                                  &v[5], &v[6], &v[7]);
-        if (n == 7) v[7] = 0;
-        return n >= 7;
+        return std::sscanf(str, "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5],
+                           &v[6]) == 7;
     };
     if (const char* pin = std::getenv("PS3D_TUNE")) {
         int v[8];
-        if (parse(pin, v) && apply(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7])) {
+        if (parse(pin, v) && apply(v[0], v[1], v[2], v[3], v[4], v[5], v[6])) {
             tuned = std::string("pinned:") + pin;
             return PS3D_OK;
         }
@@ -645,7 +640,7 @@ int Ctx::autotune() {
     auto it = tune_cache().find(key);
     if (it != tune_cache().end()) {
         int v[8];
-        if (parse(it->second.c_str(), v) && apply(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7])) {
+        if (parse(it->second.c_str(), v) && apply(v[0], v[1], v[2], v[3], v[4], v[5], v[6])) {
             tuned = std::string("cached:") + it->second;
             return PS3D_OK;
         }
@@ -694,17 +689,15 @@ int Ctx::autotune() {
     }
     bestpa.batch = 1;
     pa = bestpa;
-    // step kernel form and z chunk
+    // step kernel z chunk
     float bestk = 1e30f;
-    int bestkc = kchunk, bestsf = kform;
-    for (int sf : {0, 1})
+    int bestkc = kchunk;
     for (int kc : {4, 8, 16, 32}) {
         if (kc > nz) continue;
         kchunk = kc;
-        kform = sf;
         const float t = timeit([&]() -> int {
             StepArgs a{};
-            a.nx = nx; a.ny = ny; a.nz = nz; a.batch = batch; a.sN = N; a.kchunk = kc; a.form = sf;
+            a.nx = nx; a.ny = ny; a.nz = nz; a.batch = batch; a.sN = N; a.kchunk = kc;
             a.rigid = rigid; a.nonlinear = 1;
             a.rdx = 1.0 / P.dx; a.rdy = 1.0 / P.dy; a.rdz = 1.0 / P.dz; a.dt = P.dt; a.dtw = P.dt / P.dsqr;
             a.Ro = P.Ro; a.dsqr = P.dsqr; a.N0sq = P.N0 * P.N0; a.f0 = P.f0;
@@ -724,16 +717,15 @@ int Ctx::autotune() {
             CK(launch_step(a, mixed, stream));
             return PS3D_OK;
         });
-        if (t < bestk) { bestk = t; bestkc = kc; bestsf = sf; }
+        if (t < bestk) { bestk = t; bestkc = kc; }
     }
     kchunk = bestkc;
-    kform = bestsf;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CK(cudaStreamSynchronize(stream));
     char val[128];
-    std::snprintf(val, sizeof val, "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d,sf%d", pa.impl, pa.C, pa.row_chunk, pa.tj, pa.ly,
-                  bestpol, kchunk, kform);
+    std::snprintf(val, sizeof val, "im%d,C%d,rc%d,tj%d,ly%d,pol%d,kc%d", pa.impl, pa.C, pa.row_chunk, pa.tj, pa.ly,
+                  bestpol, kchunk);
     tuned = val;
     tune_cache_store(key, val);
     return PS3D_OK;
@@ -1586,9 +1578,9 @@ int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
     const Ctx& C = ctx->impl;
     const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
     std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_impl=%s plane_cluster=%d row_chunk=%d tj=%d ly=%d "
-                  "fft_x=%d stages fft_y=%d stages kchunk=%d step_form=%d tuned=%s", C.nx, C.ny, C.nz, C.refine_full ? "mixed_refined" : C.mixed ? "mixed" : "fp64",
+                  "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.refine_full ? "mixed_refined" : C.mixed ? "mixed" : "fp64",
                   C.batch, pa.impl == 2 ? "pipe+lines" : pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
-                  C.kchunk, C.kform, C.tuned.empty() ? "default" : C.tuned.c_str());
+                  C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
     return PS3D_OK;
 }
 
@@ -1629,6 +1621,14 @@ const char* ps3d_strerror(int status) {
 }  // extern "C"
 
 namespace ps3d {
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("PS3D_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // Records the last failing CUDA call; printed to stderr when PS3D_VERBOSE is set.
 void note_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
     static const bool verbose = std::getenv("PS3D_VERBOSE") != nullptr;

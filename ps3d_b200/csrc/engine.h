@@ -9,6 +9,9 @@ namespace ps3d {
 
 // Launch with programmatic stream serialization (see pdl_trigger/pdl_wait):
 // only for kernels that call pdl_wait before reading their inputs.
+// PS3D_PDL=0 launches them with ordinary full dependencies instead
+// (griddepcontrol.wait then returns at once).
+bool pdl_enabled();
 template <typename... P, typename... A>
 inline cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                               A&&... args) {
@@ -21,7 +24,7 @@ inline cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kernel, static_cast<A&&>(args)...);
 }
 
@@ -50,7 +53,6 @@ struct StepArgs {
     int batch;                     // instances of the same grid stepped together (>= 1)
     long sN;                       // element stride between instances (fields and tendency slots)
     int kchunk;                    // z levels per block (autotuned)
-    int form;                      // 0: all threads load and compute, 1: warp-specialised (autotuned)
     // pending pressure correction of the previous step (NULL: state is final):
     // the state arrays hold u'' and the true velocity is u'' - dtp*grad(pc)
     const double* pc;

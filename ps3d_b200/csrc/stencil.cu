@@ -23,48 +23,27 @@
 namespace ps3d {
 
 constexpr int kTX = 32;
-// K1 is warp-specialised: kStepProdWarps producer warps stage the planes of
-// the ring (global loads, the pending pressure correction, the periodic
-// wrap) and the level's summed Adams-Bashforth history into shared memory,
-// kStepRing planes deep, while the 32 x BY consumer threads compute.  The two
-// roles hand slots over through named barriers (FULL: a slot holds its plane,
-// EMPTY: the consumers are done with it), so the consumers never wait on
-// HBM latency except when the producers fall behind.
-constexpr int kStepRing = 4;
-constexpr int kStepProdWarps = 4;
 
-// The ring of state planes, and the summed history c1 h1 + c2 h2 (FP64) of
-// each level's points, one history slot per plane slot.
-template <int BY, int NF>
-struct StepSmem {
-    double pl[NF][kStepRing][(BY + 2) * (kTX + 2)];
-    double hs[kStepRing][4][kTX * BY];
-};
-
-// read field f at offsets (di, dj) in ring slot s
-#define SM(fi, s, dj, di) sm.pl[fi][s][(ty + 1 + (dj)) * (kTX + 2) + (tx + 1 + (di))]
-
-// ---------------------------------------------------------------------------
-// K1, first form (all threads load and compute): the three planes k-1, k,
-// k+1 in a ring; each level's next plane and Adams-Bashforth history (t1,
-// t2) are loaded by all threads before the level's barrier, the history
-// parked in shared memory so that its loads go out with the plane's without
-// holding registers through the tendency arithmetic.  The autotuner times
-// it against the warp-specialised form below and keeps the faster.
-// ---------------------------------------------------------------------------
+// The ring of state planes, and this level's Adams-Bashforth history of the
+// block's points (t1, t2), staged through shared memory so that its loads
+// go out with the next plane's before the barrier without holding
+// registers through the tendency arithmetic.
 template <typename TT, int BY, int NF>
-struct RingSmem {
+struct StepSmem {
     double pl[NF][3][(BY + 2) * (kTX + 2)];
     TT hu[2][kTX * BY], hv[2][kTX * BY], hb[2][kTX * BY];
     double hw[2][kTX * BY];
 };
 
+// read field f at offsets (di, dj) in ring slot s
+#define SM(fi, s, dj, di) sm.pl[fi][s][(ty + 1 + (dj)) * (kTX + 2) + (tx + 1 + (di))]
+
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
-__global__ void __launch_bounds__(kTX* BY) k_step_ring(const StepArgs a, int kchunk) {
+__global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) {
     using TW = double;   // stored w tendencies stay FP64 in both paths
     constexpr int NF = BG ? 6 : 4;
     extern __shared__ __align__(16) unsigned char step_smem_raw[];
-    RingSmem<TT, BY, NF>& sm = *reinterpret_cast<RingSmem<TT, BY, NF>*>(step_smem_raw);
+    StepSmem<TT, BY, NF>& sm = *reinterpret_cast<StepSmem<TT, BY, NF>*>(step_smem_raw);
     pdl_trigger();
     pdl_wait();   // the state, p and history were written by the preceding kernels
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -316,305 +295,6 @@ __global__ void __launch_bounds__(kTX* BY) k_step_ring(const StepArgs a, int kch
 }
 
 // ---------------------------------------------------------------------------
-// K1, second form: warp-specialised (producers and consumers, above).
-// ---------------------------------------------------------------------------
-// named barriers 1..2*kStepRing: FULL(slot) = 1 + slot, EMPTY(slot) = 1 + kStepRing + slot
-__device__ __forceinline__ void nb_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-__device__ __forceinline__ void nb_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-
-template <typename TT, int BY, bool HARM, bool WM, bool BG>
-__global__ void __launch_bounds__(kTX*(BY + kStepProdWarps), 2) k_step(const StepArgs a, int kchunk) {
-    using TW = double;   // stored w tendencies stay FP64 in both paths
-    constexpr int NF = BG ? 6 : 4;
-    constexpr int S = kStepRing;
-    constexpr int NC = kTX * BY;                     // consumer threads (the tile)
-    constexpr int NP = 32 * kStepProdWarps;          // producer threads
-    constexpr int NALL = NC + NP;
-    constexpr int TP = (kTX + 2) * (BY + 2);         // ring plane elements (tile + halo)
-    extern __shared__ __align__(16) unsigned char step_smem_raw[];
-    StepSmem<BY, NF>& sm = *reinterpret_cast<StepSmem<BY, NF>*>(step_smem_raw);
-    pdl_trigger();
-    pdl_wait();   // the state, p and history were written by the preceding kernels
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
-    const int kcnt = a.kcount ? a.kcount : nz;           // levels stepped (a z-slab's interior)
-    const int kofs = a.kofs, nzg = a.nzg ? a.nzg : nz;   // global level k + kofs of nzg (rigid-lid masks)
-    const int nzc = (kcnt + kchunk - 1) / kchunk;
-    const int inst = blockIdx.z / nzc;
-    const int kb = a.kbeg + (blockIdx.z - inst * nzc) * kchunk;
-    const int ke = min(a.kbeg + kcnt, kb + kchunk);
-    const long ioff = (long)inst * a.sN;
-    const long plane = (long)nx * ny;
-    const bool h1 = a.do_ab && a.ab1 != 0.0, h2 = a.do_ab && a.ab2 != 0.0;
-    auto slot = [](int q) { return (q + S) % S; };   // q >= -1
-    if (threadIdx.y >= BY) {
-        // ------------------------------------------------------------ producers
-        const int pid = (threadIdx.y - BY) * kTX + threadIdx.x;
-        const double* src[6] = {a.u + ioff, a.v + ioff, a.w + ioff, a.b + ioff, a.ub, a.bb};
-        const double* pc = a.pc ? a.pc + ioff : nullptr;
-        // this thread's ring elements: plane offsets of the point and of its
-        // east and north neighbours (full modulo: tiles may be wider than the grid)
-        constexpr int EPT = (TP + NP - 1) / NP;
-        int eo[EPT], eoE[EPT], eoN[EPT];
-#pragma unroll
-        for (int e = 0; e < EPT; ++e) {
-            const int t = min(pid + e * NP, TP - 1);
-            const int ti = t % (kTX + 2), tj = t / (kTX + 2);
-            const int gi = ((i0 - 1 + ti) % nx + nx) % nx, gj = ((j0 - 1 + tj) % ny + ny) % ny;
-            eo[e] = gj * nx + gi;
-            eoE[e] = gj * nx + wrap(gi + 1, nx);
-            eoN[e] = wrap(gj + 1, ny) * nx + gi;
-        }
-        // this thread's history points
-        constexpr int HPT = (NC + NP - 1) / NP;
-        const double c1 = a.ab1, c2 = a.ab2;
-        for (int q = kb - 1; q <= ke; ++q) {
-            const int s = slot(q);
-            if (q - (kb - 1) >= S) nb_sync(1 + S + s, NALL);   // the consumers released plane q - S
-            const int kw = wrap(q, nz);
-            const long po = (long)kw * plane, pu = (long)wrap(kw + 1, nz) * plane;
-            double v[EPT][NF];
-#pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-                if (pid + e * NP < TP) {
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) v[e][f] = __ldg(src[f] + po + eo[e]);
-                    if (pc) {
-                        // the previous step's pressure-gradient correction
-                        // (pressure_solver.f90:98-110), applied where the state is read
-                        const double p0 = __ldg(pc + po + eo[e]);
-                        const double pe = __ldg(pc + po + eoE[e]);
-                        const double pn = __ldg(pc + po + eoN[e]);
-                        const double pt = __ldg(pc + pu + eo[e]);
-                        v[e][0] = v[e][0] - a.dtp * (pe - p0) * a.rdx;
-                        v[e][1] = v[e][1] - a.dtp * (pn - p0) * a.rdy;
-                        v[e][2] = (a.rigid && wrap(kw + kofs, nzg) == nzg - 1) ? 0.0
-                                                                               : v[e][2] - a.dtwp * (pt - p0) * a.rdz;
-                    }
-                }
-            }
-            // history of level q - 1, computed by the consumers with plane q
-            double hsum[HPT][4];
-            const bool hist = q >= kb + 1 && (h1 || h2);
-            if (hist) {
-#pragma unroll
-                for (int e = 0; e < HPT; ++e) {
-                    const int t = pid + e * NP;
-                    const int ii = i0 + (t % kTX), jj = j0 + (t / kTX);
-                    double s1[4] = {0.0, 0.0, 0.0, 0.0}, s2[4] = {0.0, 0.0, 0.0, 0.0};
-                    if (t < NC && ii < nx && jj < ny) {
-                        const long gh = (long)(q - 1) * plane + (long)jj * nx + ii + ioff;
-                        if (h1) {
-                            s1[0] = (double)((const TT*)a.t1[0])[gh]; s1[1] = (double)((const TT*)a.t1[1])[gh];
-                            s1[2] = ((const TW*)a.t1[2])[gh];        s1[3] = (double)((const TT*)a.t1[3])[gh];
-                        }
-                        if (h2) {
-                            s2[0] = (double)((const TT*)a.t2[0])[gh]; s2[1] = (double)((const TT*)a.t2[1])[gh];
-                            s2[2] = ((const TW*)a.t2[2])[gh];        s2[3] = (double)((const TT*)a.t2[3])[gh];
-                        }
-                    }
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) hsum[e][f] = c1 * s1[f] + c2 * s2[f];
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-                const int t = pid + e * NP;
-                if (t < TP) {
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) sm.pl[f][s][t] = v[e][f];
-                }
-            }
-            if (hist) {
-                const int hsl = slot(q - 1);
-#pragma unroll
-                for (int e = 0; e < HPT; ++e) {
-                    const int t = pid + e * NP;
-                    if (t < NC) {
-#pragma unroll
-                        for (int f = 0; f < 4; ++f) sm.hs[hsl][f][t] = hsum[e][f];
-                    }
-                }
-            }
-            nb_arrive(1 + s, NALL);   // plane q (and the history of level q - 1) is in slot s
-        }
-        return;
-    }
-    // ---------------------------------------------------------------- consumers
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i = i0 + tx, j = j0 + ty;
-    const bool active = (i < nx) && (j < ny);
-    const int tid = ty * kTX + tx;
-    const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
-    const bool rigid = a.rigid;
-    nb_sync(1 + slot(kb - 1), NALL);
-    nb_sync(1 + slot(kb), NALL);
-    for (int k = kb; k < ke; ++k) {
-        nb_sync(1 + slot(k + 1), NALL);
-        if (active) {
-            const int sm1 = slot(k - 1), s0 = slot(k), sp1 = slot(k + 1);
-#define U(di, dj, dk) SM(0, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define V(di, dj, dk) SM(1, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define W(di, dj, dk) SM(2, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define B(di, dj, dk) SM(3, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define UB(di, dj, dk) SM(4, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define BB(di, dj, dk) SM(5, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-            const int kg = k + kofs;                     // global level
-            const bool top = rigid && (kg == nzg - 1);   // flux_top(nz) = 0
-            const bool bot = rigid && (kg == 0);         // flux_top(0)  = 0
-            const long g0 = (long)k * plane + (long)j * nx + i;   // point within the instance
-            const long g = g0 + ioff;                              // point within the batch
-            double db_, du_, dv_, dw_;
-            // ---- buoyancy advection + N^2 (advection.f90:12-47, integrate.f90:21-23)
-            // The reference's 0.5 and 0.25 flux factors are powers of two: they
-            // are carried in the per-axis factors a.hd* = 0.5/d*, a.qd* = 0.25/d*
-            // (and 0.25 f0, 0.5 N0^2, set by the launcher), a multiply saved per
-            // flux.  Scaling by a power of two rounds exactly; the results move
-            // at round-off level only where the compiler now contracts a flux
-            // product into the difference that follows (FMA).
-            if (a.nonlinear) {
-                const double fe = (B(0, 0, 0) + B(1, 0, 0)) * U(0, 0, 0);
-                const double fem = (B(-1, 0, 0) + B(0, 0, 0)) * U(-1, 0, 0);
-                const double fn = (B(0, 0, 0) + B(0, 1, 0)) * V(0, 0, 0);
-                const double fnm = (B(0, -1, 0) + B(0, 0, 0)) * V(0, -1, 0);
-                const double ft = top ? 0.0 : (B(0, 0, 0) + B(0, 0, 1)) * W(0, 0, 0);
-                const double ftm = bot ? 0.0 : (B(0, 0, -1) + B(0, 0, 0)) * W(0, 0, -1);
-                db_ = -Ro * ((fe - fem) * a.hdx + (fn - fnm) * a.hdy + (ft - ftm) * a.hdz);
-                // ---- zonal momentum (advection.f90:65-100)
-                {
-                    const double e = (U(0, 0, 0) + U(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
-                    const double em = (U(-1, 0, 0) + U(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
-                    const double n = (U(0, 0, 0) + U(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
-                    const double nm = (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : (U(0, 0, 1) + U(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
-                    const double tm = bot ? 0.0 : (U(0, 0, 0) + U(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
-                    du_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
-                }
-                // ---- meridional momentum (advection.f90:104-140)
-                {
-                    const double e = (V(0, 0, 0) + V(1, 0, 0)) * (U(0, 1, 0) + U(0, 0, 0));
-                    const double em = (V(-1, 0, 0) + V(0, 0, 0)) * (U(-1, 1, 0) + U(-1, 0, 0));
-                    const double n = (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 1, 0) + V(0, 0, 0));
-                    const double nm = (V(0, -1, 0) + V(0, 0, 0)) * (V(0, 0, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : (V(0, 0, 1) + V(0, 0, 0)) * (W(0, 0, 0) + W(0, 1, 0));
-                    const double tm = bot ? 0.0 : (V(0, 0, 0) + V(0, 0, -1)) * (W(0, 0, -1) + W(0, 1, -1));
-                    dv_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
-                }
-                // ---- vertical momentum (advection.f90:145-181); rigid lid zeroes
-                //      flux_top(nz-1:nz+2) for w (:167-170)
-                {
-                    const bool wtop = rigid && (kg >= nzg - 2);
-                    const bool wbot = rigid && (kg == 0 || kg >= nzg - 1);
-                    const double e = (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
-                    const double em = (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
-                    const double n = (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
-                    const double nm = (W(0, -1, 0) + W(0, 0, 0)) * (V(0, -1, 0) + V(0, -1, 1));
-                    const double t = wtop ? 0.0 : (W(0, 0, 1) + W(0, 0, 0)) * (W(0, 0, 0) + W(0, 0, 1));
-                    const double tm = wbot ? 0.0 : (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, -1) + W(0, 0, 0));
-                    dw_ = -a.dsqr * Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
-                }
-            } else {
-                db_ = du_ = dv_ = dw_ = 0.0;
-            }
-            db_ = db_ - (W(0, 0, 0) + W(0, 0, -1)) * a.hN0sq;
-            // ---- Coriolis, buoyancy force, rigid-lid mask (integrate.f90:37-54)
-            du_ = du_ + (V(0, 0, 0) + V(0, -1, 0) + V(1, 0, 0) + V(1, -1, 0)) * a.qf0;
-            dv_ = dv_ - (U(-1, 0, 0) + U(0, 0, 0) + U(-1, 1, 0) + U(0, 1, 0)) * a.qf0;
-            dw_ = dw_ + 0.5 * (B(0, 0, 0) + B(0, 0, 1));
-            if (top) dw_ = 0.0;
-            // ---- friction, in place before AB (integrate.f90:59-66)
-            double u1 = U(0, 0, 0), v1 = V(0, 0, 0), w1 = W(0, 0, 0), b1 = B(0, 0, 0);
-            if constexpr (HARM) {
-                const double dt = a.dt;
-#define HARMONIC(F, Hm, Vm, out)                                                                   \
-    {                                                                                            \
-        const double e = Hm * (F(1, 0, 0) - F(0, 0, 0)) * rdx;                                   \
-        const double em = Hm * (F(0, 0, 0) - F(-1, 0, 0)) * rdx;                                 \
-        const double n = Hm * (F(0, 1, 0) - F(0, 0, 0)) * rdy;                                   \
-        const double nm = Hm * (F(0, 0, 0) - F(0, -1, 0)) * rdy;                                 \
-        const double t = top ? 0.0 : Vm * (F(0, 0, 1) - F(0, 0, 0)) * rdz;                       \
-        const double tm = bot ? 0.0 : Vm * (F(0, 0, 0) - F(0, 0, -1)) * rdz;                     \
-        out = F(0, 0, 0) + dt * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);              \
-    }
-                if (a.harm_uvw) {
-                    HARMONIC(U, a.Ah, a.Av, u1)
-                    HARMONIC(V, a.Ah, a.Av, v1)
-                    HARMONIC(W, a.Ah, a.Av, w1)
-                    if (top) w1 = 0.0;
-                }
-                if (a.harm_b) HARMONIC(B, a.Kh, a.Kv, b1)
-#undef HARMONIC
-            }
-            // ---- set_forcing: background-flow advection (lee_wave1.f90:245-312)
-            if constexpr (BG) {
-                {
-                    const double e = 2 * 0.25 * (UB(0, 0, 0) + UB(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
-                    const double em = 2 * 0.25 * (UB(-1, 0, 0) + UB(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
-                    const double n = 0.25 * (UB(0, 0, 0) + UB(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
-                    const double nm = 0.25 * (UB(0, -1, 0) + UB(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : 0.25 * (UB(0, 0, 1) + UB(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
-                    const double tm = bot ? 0.0 : 0.25 * (UB(0, 0, 0) + UB(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
-                    du_ = du_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
-                }
-                {
-                    const double e = 0.25 * (V(0, 0, 0) + V(1, 0, 0)) * (UB(0, 1, 0) + UB(0, 0, 0));
-                    const double em = 0.25 * (V(-1, 0, 0) + V(0, 0, 0)) * (UB(-1, 1, 0) + UB(-1, 0, 0));
-                    dv_ = dv_ - Ro * (e - em) * rdx;
-                }
-                {
-                    const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (UB(0, 0, 0) + UB(0, 0, 1));
-                    const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (UB(-1, 0, 0) + UB(-1, 0, 1));
-                    dw_ = dw_ - a.dsqr * Ro * (e - em) * rdx;
-                }
-                {
-                    const double e = 0.5 * (B(0, 0, 0) + B(1, 0, 0)) * UB(0, 0, 0) + 0.5 * (BB(0, 0, 0) + BB(1, 0, 0)) * U(0, 0, 0);
-                    const double em = 0.5 * (B(-1, 0, 0) + B(0, 0, 0)) * UB(-1, 0, 0) + 0.5 * (BB(-1, 0, 0) + BB(0, 0, 0)) * U(-1, 0, 0);
-                    const double n = 0.5 * (BB(0, 0, 0) + BB(0, 1, 0)) * V(0, 0, 0);
-                    const double nm = 0.5 * (BB(0, -1, 0) + BB(0, 0, 0)) * V(0, -1, 0);
-                    const double t = top ? 0.0 : 0.5 * (BB(0, 0, 0) + BB(0, 0, 1)) * W(0, 0, 0);
-                    const double tm = bot ? 0.0 : 0.5 * (BB(0, 0, -1) + BB(0, 0, 0)) * W(0, 0, -1);
-                    db_ = db_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
-                }
-            }
-#undef U
-#undef V
-#undef W
-#undef B
-#undef UB
-#undef BB
-            // ---- set_forcing: wavemaker (config.f90:224-237)
-            if constexpr (WM) {
-                const double dt = a.dt, c = a.wm_c, s = a.wm_s;
-                if (a.wr[0] || a.wi[0]) u1 = u1 + dt * (c * (a.wr[0] ? a.wr[0][g0] : 0.0) + s * (a.wi[0] ? a.wi[0][g0] : 0.0));
-                if (a.wr[1] || a.wi[1]) v1 = v1 + dt * (c * (a.wr[1] ? a.wr[1][g0] : 0.0) + s * (a.wi[1] ? a.wi[1][g0] : 0.0));
-                if (a.wr[2] || a.wi[2]) w1 = w1 + dt * (c * (a.wr[2] ? a.wr[2][g0] : 0.0) + s * (a.wi[2] ? a.wi[2][g0] : 0.0));
-                if (a.wr[3] || a.wi[3]) b1 = b1 + dt * (c * (a.wr[3] ? a.wr[3][g0] : 0.0) + s * (a.wi[3] ? a.wi[3][g0] : 0.0));
-            }
-            // ---- store tendency of time level tau
-            ((TT*)a.t0[0])[g] = (TT)du_;
-            ((TT*)a.t0[1])[g] = (TT)dv_;
-            ((TW*)a.t0[2])[g] = (TW)dw_;
-            ((TT*)a.t0[3])[g] = (TT)db_;
-            // ---- Adams-Bashforth (integrate.f90:87-102)
-            if (a.do_ab) {
-                const double dt = a.dt, dtw = a.dtw;
-                // the current tendency enters at full precision; the stored
-                // history (FP32 in the mixed path) arrives summed, c1 h1 + c2 h2
-                double tu = a.ab0 * du_, tv = a.ab0 * dv_, tw = a.ab0 * dw_, tb = a.ab0 * db_;
-                if (h1 || h2) {
-                    tu = tu + sm.hs[s0][0][tid]; tv = tv + sm.hs[s0][1][tid];
-                    tw = tw + sm.hs[s0][2][tid]; tb = tb + sm.hs[s0][3][tid];
-                }
-                u1 = u1 + dt * tu; v1 = v1 + dt * tv; w1 = w1 + dtw * tw; b1 = b1 + dt * tb;
-            }
-            a.uo[g] = u1; a.vo[g] = v1; a.wo[g] = w1; a.bo[g] = b1;
-        }
-        // plane k - 1 is done with; release its slot if the producers refill it
-        if (k - 1 + S <= ke) nb_arrive(1 + S + slot(k - 1), NALL);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Generic friction stages with the reference's stale-halo semantics: the
 // biharmonic operators of mixing.f90:96-217 run after harmonic() without a
 // halo exchange, so any neighbour outside the interior still holds the
@@ -788,18 +468,14 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
 static cudaError_t launch_step_t(const StepArgs& a0, cudaStream_t s) {
     StepArgs a = a0;
-    const int form = a.form;
     a.hdx = 0.5 * a.rdx; a.hdy = 0.5 * a.rdy; a.hdz = 0.5 * a.rdz;
     a.qdx = 0.25 * a.rdx; a.qdy = 0.25 * a.rdy; a.qdz = 0.25 * a.rdz;
     a.qf0 = 0.25 * a.f0; a.hN0sq = 0.5 * a.N0sq;
     const int kcnt = a.kcount ? a.kcount : a.nz;
     const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
     dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((kcnt + kchunk - 1) / kchunk) * std::max(1, a.batch));
-    if (form == 0)
-        return launch_pdl(k_step_ring<TT, BY, HARM, WM, BG>, grid, dim3(kTX, BY),
-                          sizeof(RingSmem<TT, BY, BG ? 6 : 4>), s, a, kchunk);
-    return launch_pdl(k_step<TT, BY, HARM, WM, BG>, grid, dim3(kTX, BY + kStepProdWarps),
-                      sizeof(StepSmem<BY, BG ? 6 : 4>), s, a, kchunk);
+    return launch_pdl(k_step<TT, BY, HARM, WM, BG>, grid, dim3(kTX, BY), sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s, a,
+                      kchunk);
 }
 
 template <typename TT>
@@ -818,10 +494,7 @@ static cudaError_t step_setup_tt() {
     cudaError_t e;
 #define S(H, W, G)                                                                                        \
     if ((e = cudaFuncSetAttribute(k_step<TT, 8, H, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                  (int)sizeof(StepSmem<8, G ? 6 : 4>))))                                  \
-        return e;                                                                                         \
-    if ((e = cudaFuncSetAttribute(k_step_ring<TT, 8, H, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)sizeof(RingSmem<TT, 8, G ? 6 : 4>))))                               \
+                                  (int)sizeof(StepSmem<TT, 8, G ? 6 : 4>))))                              \
         return e;
     S(true, true, true) S(true, true, false) S(true, false, true) S(true, false, false)
     S(false, true, true) S(false, true, false) S(false, false, true) S(false, false, false)

@@ -31,14 +31,6 @@ def plane_impl(request, monkeypatch):
     return request.param
 
 
-@pytest.fixture(autouse=True, params=["ring", "warp-specialised"])
-def step_form(request, monkeypatch):
-    """... and on both forms of the step kernel: all threads loading and
-    computing over a three-plane ring, and producer warps staging a
-    four-plane ring for consumer warps."""
-    monkeypatch.setenv("PS3D_STEP_FORM", {"ring": "0", "warp-specialised": "1"}[request.param])
-    return request.param
-
 
 def _pair(p, fields, pfield=None):
     o = Oracle(p)
@@ -60,11 +52,14 @@ def test_pressure_solver(rigid, shape, plane_impl):
     assert max(err.values()) < TOL_KERNEL, err
 
 
+@pytest.mark.parametrize("thomas_form", ["0", "1"])
 @pytest.mark.parametrize("nz", [40, 64, 100, 129])
-def test_pressure_solver_tall_columns(nz):
+def test_pressure_solver_tall_columns(nz, thomas_form, monkeypatch):
     """Rigid-lid solve on columns split into several segments: nz = 64 fills
     every segment, 40 and 100 leave the last one short, 129 leaves trailing
-    segments empty."""
+    segments empty; both forms of the vertical solve (right-hand side loaded
+    by the threads, or streamed through a cp.async ring)."""
+    monkeypatch.setenv("PS3D_THOMAS_FORM", thomas_form)
     p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
     o, m = _pair(p, random_state(p, seed=3))
     o.pressure_solver()
