@@ -582,6 +582,165 @@ __global__ void __launch_bounds__(64) k_thomas_async(const ColumnArgs a) {
 }
 #undef IN
 
+// The same solve eliminated from both ends at once (a twisted
+// factorisation): the matrix is persymmetric (constant a = c = fxa, the same
+// end coefficient at the top and the bottom level), so the elimination from
+// the bottom up runs through exactly the pivots of the elimination from the
+// top down, cp(j) for level j from the top and level nz-1-j from the bottom.
+// One pivot chain of ceil(nz/2) levels therefore serves two d' chains, the
+// two halves meet in a 2x2 solve at the middle,
+//   x(m) = (dp(m) - cp(m) dq(jb)) / (1 - cp(m) cp(jb)),  x(m+1) = dq(jb) - cp(jb) x(m),
+// and two back substitutions run outward.  The serial FP64 chain (divide,
+// then multiply-add, per level) is half as long as a one-ended sweep, where
+// it bounds the kernel.  Checkpoints (cp, dp, dq) before every chunk of 8
+// pivot levels in shared memory; each chunk's values recomputed on the way
+// back as in k_thomas.
+PS3D_HD size_t thomas2_smem(int nz, int threads) {
+    const int h = (nz + 1) / 2;
+    return (size_t)((h + kThomasChunk - 1) / kThomasChunk + 1) * threads * (sizeof(double2) + sizeof(double));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs a) {
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
+    constexpr int KC = kThomasChunk;
+    extern __shared__ double2 ck2[];   // [chunk][thread] (cp, dp), then [chunk][thread] dq
+    const int nz = a.nz;
+    const int H = (nz + 1) / 2;   // pivot levels: top 0 .. H-1, bottom nz-1 .. nz-Bc
+    const int Bc = nz - H;
+    const int m = H - 1, jb = Bc - 1;
+    const int nch = (H + KC - 1) / KC;
+    const int T = blockDim.x, tid = threadIdx.x;
+    double* ckq = reinterpret_cast<double*>(ck2 + (size_t)(nch + 1) * T);
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
+    const long gid = blockIdx.x * (long)T + tid;
+    if (gid >= 2 * ncols * a.batch) return;
+    const int part = (int)(gid & 1);
+    const unsigned cb = (unsigned)(gid >> 1);
+    const unsigned inst = fdiv(cb, a.fd_ncols);
+    const unsigned c = cb - inst * (unsigned)ncols;
+    R* col = reinterpret_cast<R*>(a.spec) + 2 * ((long)inst * a.sM + c) + part;
+    const long ls = 2 * ncols;   // level stride in R
+    const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
+    const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
+    const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
+    const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
+    const double ks = a.hkx[i] + a.hky[j];
+    const double fxa = a.fxa;
+    if (!(ks > 0)) {
+        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
+        const double h = a.dz2dsqr;
+        double x0 = 0.0, x1 = 0.0, fprev = 0.0;   // p(k-2), p(k-1), f(k-1)
+        R nxt[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q)
+            if (q < nz) nxt[q] = col[(long)q * ls];
+        for (int kb = 0; kb < nz; kb += KC) {
+            R d[KC];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) d[q] = nxt[q];
+#pragma unroll
+            for (int q = 0; q < KC; ++q)
+                if (kb + KC + q < nz) nxt[q] = col[(long)(kb + KC + q) * ls];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int k = kb + q;
+                if (k < nz) {
+                    const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
+                    fprev = (double)d[q];
+                    x0 = x1; x1 = xk;
+                    col[(long)k * ls] = (R)xk;
+                }
+            }
+        }
+        return;
+    }
+    const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+    // pivot level jj (from either end) with the top value dt and the bottom
+    // value db: cp(1) = c/b(1), dp(1) = d(1)/b(1); r = 1/(b - cp a),
+    // cp = c r, dp = (d - dp a) r (the bottom chain the same with its own d)
+    auto elim = [&](int jj, double dt, double db, double& cp, double& dp, double& dq) {
+        if (jj == 0) {
+            cp = fxa / bend;
+            dp = dt / bend;
+            dq = db / bend;
+        } else {
+            const double r = __drcp_rn(bmid - cp * fxa);   // == 1.0 / x (both correctly rounded)
+            cp = fxa * r;
+            dp = (dt - dp * fxa) * r;
+            if (jj < Bc) dq = (db - dq * fxa) * r;
+        }
+    };
+    // the chunk of pivot levels jc .. jc+KC-1: top levels jc.., bottom levels nz-1-jc..
+    auto load = [&](int jc, R* top, R* bot) {
+#pragma unroll
+        for (int q = 0; q < KC; ++q) {
+            const int jj = jc + q;
+            if (jj < H) top[q] = col[(long)jj * ls];
+            if (jj < Bc) bot[q] = col[(long)(nz - 1 - jj) * ls];
+        }
+    };
+    double cp = 0.0, dp = 0.0, dq = 0.0, cp_jb = 0.0, dq_jb = 0.0;
+    R nt[KC], nb[KC];
+#pragma unroll
+    for (int q = 0; q < KC; ++q) { nt[q] = (R)0; nb[q] = (R)0; }
+    load(0, nt, nb);
+    for (int ch = 0; ch < nch; ++ch) {
+        const int jc = ch * KC;
+        R dt[KC], db[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
+        if (ch + 1 < nch) load(jc + KC, nt, nb);
+        ck2[ch * T + tid] = make_double2(cp, dp);   // before pivot level jc
+        ckq[ch * T + tid] = dq;
+#pragma unroll
+        for (int q = 0; q < KC; ++q) {
+            const int jj = jc + q;
+            if (jj < H) {
+                elim(jj, (double)dt[q], (double)db[q], cp, dp, dq);
+                if (jj == jb) { cp_jb = cp; dq_jb = dq; }
+            }
+        }
+    }
+    // the two halves meet: x(m) and x(m+1)
+    double xt = (dp - cp * dq_jb) / (1.0 - cp * cp_jb);
+    double xb = dq_jb - cp_jb * xt;
+    // back substitution outward, chunk by chunk from the middle
+    load((nch - 1) * KC, nt, nb);
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        const int jc = ch * KC;
+        R dt[KC], db[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
+        if (ch > 0) load(jc - KC, nt, nb);
+        double cpl[KC], dpl[KC], dql[KC];
+        {
+            const double2 c0 = ck2[ch * T + tid];
+            double cpv = c0.x, dpv = c0.y, dqv = ckq[ch * T + tid];
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                if (jc + q < H) elim(jc + q, (double)dt[q], (double)db[q], cpv, dpv, dqv);
+                cpl[q] = cpv;
+                dpl[q] = dpv;
+                dql[q] = dqv;
+            }
+        }
+#pragma unroll
+        for (int q = KC - 1; q >= 0; --q) {
+            const int jj = jc + q;
+            if (jj < H) {
+                if (jj < m) xt = dpl[q] - cpl[q] * xt;
+                col[(long)jj * ls] = (R)xt;
+                if (jj <= jb) {
+                    if (jj < jb) xb = dql[q] - cpl[q] * xb;
+                    col[(long)(nz - 1 - jj) * ls] = (R)xb;
+                }
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // K3, triply periodic: z FFT, spectral division, inverse z FFT
 // (pressure_solver.f90:58-70; my_fft_3D/my_ifft_3D z leg)
@@ -1366,6 +1525,7 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
     if ((e = max_dynamic_smem(k_thomas_async<R, true, sizeof(R) == 4 ? 4 : 3>))) return e;
@@ -1447,16 +1607,25 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     a.fd_ncols = make_fastdiv((unsigned)ncols);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_nxh = make_fastdiv(a.nxh);
-    // the streamed form (64-thread blocks, a ring 4 chunks deep in FP32, 3 in
-    // FP64) where its shared memory leaves room for 4 blocks per SM;
-    // PS3D_THOMAS_FORM=0|1 pins the form
+    // the two-ended form where its checkpoints leave room for 4 blocks of 128
+    // per SM; else the streamed form (64-thread blocks, a ring 4 chunks deep
+    // in FP32, 3 in FP64) where it fits, else the one-ended form with fewer
+    // threads per block; PS3D_THOMAS_FORM=0|1|2 pins one
+    const char* pin = std::getenv("PS3D_THOMAS_FORM");
+    if ((!pin && thomas2_smem(a.nz, kThomasThreads) <= 56 * 1024) ||
+        (pin && pin[0] == '2' && thomas2_smem(a.nz, kThomasThreads) <= 227 * 1024 - 64)) {
+        const long nthreads = 2 * ncols * std::max(1, a.batch);
+        const dim3 g((unsigned)((nthreads + kThomasThreads - 1) / kThomasThreads)), b(kThomasThreads);
+        const size_t sm2 = thomas2_smem(a.nz, kThomasThreads);
+        if (fp32) return launch_pdl(k_thomas2<float>, g, b, sm2, s, a);
+        return launch_pdl(k_thomas2<double>, g, b, sm2, s, a);
+    }
     {
         const size_t rs = fp32 ? sizeof(float) : sizeof(double);
         const int depth = fp32 ? 4 : 3;
         const size_t sma = thomas_async_smem(a.nz, 64, depth, rs);
         int form = sma <= 56 * 1024 ? 1 : 0;
-        if (const char* f = std::getenv("PS3D_THOMAS_FORM"))
-            if (f[0] == '0' || (f[0] == '1' && sma <= 227 * 1024 - 64)) form = f[0] - '0';
+        if (pin && (pin[0] == '0' || (pin[0] == '1' && sma <= 227 * 1024 - 64))) form = pin[0] - '0';
         if (form == 1) {
             const long nthreads = 2 * ncols * std::max(1, a.batch);
             const dim3 g((unsigned)((nthreads + 63) / 64)), b(64);
