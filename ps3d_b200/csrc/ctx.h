@@ -74,11 +74,26 @@ struct Ctx {
     // relative in w within 100 steps)
     size_t tsz(int f) const { return (mixed && f != 2) ? sizeof(float) : sizeof(double); }
     int batch = 1;            // instances of this grid stepped together (ensembles)
-    // CUDA graph of three consecutive steps (tau and the state buffers both
-    // cycle with period 3), replayed by advance() for constant parameters
-    cudaGraphExec_t gexec = nullptr;
+    // CUDA graphs of three consecutive steps (tau and the state buffers both
+    // cycle with period 3), replayed by advance() for constant parameters: one
+    // per phase of the cycle (slot tau - 1), so that calls of any length keep
+    // replaying without a new capture
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        int tau = -1, cur = -1;
+        long version = -1;
+        long long launches = 0;
+        bool pend_in = false, pend_out = false;
+        const double* pcor_in = nullptr;
+        const double* pcor_out = nullptr;
+        double dtp_in = 0.0, dtp_out = 0.0;
+        bool warm_in = false, warm_out = false;
+    };
+    GraphSlot gslot[3];
+    // the ensemble's capture bookkeeping (ensemble.cu): outputs of its last
+    // capture and the inputs it was captured with
     int g_tau = -1, g_cur = -1;
-    long g_version = -1, version = 0;
+    long version = 0;
     long long g_launches = 0;
     bool g_pend_in = false, g_pend_out = false;
     const double* g_pcor_in = nullptr;
@@ -166,7 +181,8 @@ struct Ctx {
     unsigned* kerr_d = nullptr;
 
     ~Ctx() {
-        if (gexec) cudaGraphExecDestroy(gexec);
+        for (GraphSlot& s : gslot)
+            if (s.exec) cudaGraphExecDestroy(s.exec);
         if (stream) { cudaStreamSynchronize(stream); if (own_stream) cudaStreamDestroy(stream); }
         for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
         if (snap_stream) { cudaStreamSynchronize(snap_stream); cudaStreamDestroy(snap_stream); }
@@ -194,7 +210,7 @@ struct Ctx {
     int autotune();
     int advance(int nsteps, bool allow_graph);
     bool graphable() const;
-    int capture_graph();
+    int capture_graph(GraphSlot& slot);
     // parameters changed outside the time loop: captured graphs are stale
     void invalidate_graph() { ++version; }
     // the state or p replaced outside the time loop: graphs are stale, and p

@@ -748,8 +748,8 @@ bool Ctx::graphable() const {
     return cur[0] == cur[1] && cur[1] == cur[2] && cur[2] == cur[3];
 }
 
-int Ctx::capture_graph() {
-    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+int Ctx::capture_graph(GraphSlot& gs) {
+    if (gs.exec) { cudaGraphExecDestroy(gs.exec); gs.exec = nullptr; }
     const int itt0 = itt, tau0 = tau, t10 = taum1, t20 = taum2;
     int cur0[4];
     for (int f = 0; f < 4; ++f) cur0[f] = cur[f];
@@ -767,39 +767,40 @@ int Ctx::capture_graph() {
         ++itt;
     }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
-    g_pend_out = pending; g_pcor_out = pcor; g_dtp_out = dtp; g_warm_out = p_warm;
+    gs.pend_out = pending; gs.pcor_out = pcor; gs.dtp_out = dtp; gs.warm_out = p_warm;
     itt = itt0; tau = tau0; taum1 = t10; taum2 = t20;
     for (int f = 0; f < 4; ++f) cur[f] = cur0[f];
     pending = pend0; pcor = pcor0; dtp = dtp0; p_warm = warm0;
-    g_launches = launches - l0;
+    gs.launches = launches - l0;
     launches = l0;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     CK(e);
-    e = cudaGraphInstantiate(&gexec, g, 0);
+    e = cudaGraphInstantiate(&gs.exec, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    g_tau = tau; g_cur = cur[0]; g_version = version;
-    g_pend_in = pending; g_pcor_in = pcor; g_dtp_in = dtp; g_warm_in = p_warm;
+    gs.tau = tau; gs.cur = cur[0]; gs.version = version;
+    gs.pend_in = pending; gs.pcor_in = pcor; gs.dtp_in = dtp; gs.warm_in = p_warm;
     return PS3D_OK;
 }
 
 int Ctx::advance(int nsteps, bool allow_graph) {
     while (nsteps > 0) {
         if (allow_graph && nsteps >= 3 && itt >= 2 && graphable()) {
-            if (!gexec || g_tau != tau || g_cur != cur[0] || g_version != version || g_pend_in != pending ||
-                g_pcor_in != pcor || g_dtp_in != dtp || g_warm_in != p_warm) {
-                int rc = capture_graph();
+            GraphSlot& gs = gslot[(tau + 2) % 3];
+            if (!gs.exec || gs.tau != tau || gs.cur != cur[0] || gs.version != version || gs.pend_in != pending ||
+                gs.pcor_in != pcor || gs.dtp_in != dtp || gs.warm_in != p_warm) {
+                int rc = capture_graph(gs);
                 if (rc) return rc;
             }
-            CK(cudaGraphLaunch(gexec, stream));
+            CK(cudaGraphLaunch(gs.exec, stream));
             for (int s = 0; s < 3; ++s) {
                 rotate();
                 for (int f = 0; f < 4; ++f) cur[f] = (cur[f] + 1) % 3;
                 time = time + P.dt;
                 ++itt;
             }
-            pending = g_pend_out; pcor = g_pcor_out; dtp = g_dtp_out; p_warm = g_warm_out;
-            launches += g_launches;
+            pending = gs.pend_out; pcor = gs.pcor_out; dtp = gs.dtp_out; p_warm = gs.warm_out;
+            launches += gs.launches;
             nsteps -= 3;
             continue;
         }

@@ -75,6 +75,7 @@ int capture(ps3d_ensemble* e) {
         g.g_pend_out = g.pending; g.g_pcor_out = g.pcor; g.g_dtp_out = g.dtp; g.g_warm_out = g.p_warm;
         g.pending = saved[q].pend; g.pcor = saved[q].pcor; g.dtp = saved[q].dtp; g.p_warm = saved[q].warm;
         g.g_pend_in = g.pending; g.g_pcor_in = g.pcor; g.g_dtp_in = g.dtp; g.g_warm_in = g.p_warm;
+        g.g_tau = g.tau; g.g_cur = g.cur[0];   // the phase of the cycle the graph starts at
     }
     e->itt = itt0;
     if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -90,9 +91,11 @@ int advance(ps3d_ensemble* e, int nsteps) {
     while (nsteps > 0) {
         if (nsteps >= 3 && e->itt >= 2 && all_graphable(e)) {
             bool same = true;
+            // the same phase of the (tau, state buffer) cycle and the same
+            // pending correction and warm start as at the capture
             for (auto& g : e->groups)
                 same = same && g->g_pend_in == g->pending && g->g_pcor_in == g->pcor && g->g_dtp_in == g->dtp &&
-                       g->g_warm_in == g->p_warm;
+                       g->g_warm_in == g->p_warm && g->g_tau == g->tau && g->g_cur == g->cur[0];
             if (!e->graph_valid || !same) {
                 int rc = capture(e);
                 if (rc) return rc;

@@ -64,6 +64,54 @@ def test_graph_replay_matches_eager():
         assert np.array_equal(ra[n], rb[n]), n
 
 
+@pytest.mark.parametrize("precision", [abi.PS3D_FP64, abi.PS3D_MIXED])
+def test_graph_replay_across_calls_of_any_length(precision):
+    """Calls whose step counts are not multiples of the graph period (3)
+    leave the (tau, state buffer) cycle at another phase: each phase replays
+    its own graph, and the result equals one call of the summed length and
+    stepping one step per call."""
+    p = cf.eddy_params(64, 64, 32, precision=precision)
+    f = _member_fields(p, 0.1, seed=5)
+    ms = [Model(p) for _ in range(3)]
+    for m in ms:
+        m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+    for n in (7, 8, 5, 11, 4):
+        ms[0].run(n)
+    ms[1].run(35)
+    for _ in range(35):
+        ms[2].run(1)
+    r = [m.download(tendencies=False) for m in ms]
+    for m in ms:
+        m.close()
+    for q in (1, 2):
+        for n in ("u", "v", "w", "b", "p"):
+            assert np.array_equal(r[0][n], r[q][n]), (q, n)
+
+
+@pytest.mark.parametrize("precision", [abi.PS3D_FP64, abi.PS3D_MIXED])
+def test_ensemble_calls_of_any_length(precision, monkeypatch):
+    """An ensemble advanced by calls of 7, 8, 5 and 11 steps ends where one
+    call of 31 steps ends: a call that starts at another phase of the cycle
+    captures a graph for that phase instead of replaying the old one."""
+    monkeypatch.setenv("PS3D_AUTOTUNE", "0")
+    sizes = [(32, 32, 16), (64, 32, 16), (32, 32, 16)]
+    members = [cf.eddy_params(*s, precision=precision) for s in sizes]
+    fields = [_member_fields(p, 0.05 + 0.05 * i, seed=i) for i, p in enumerate(members)]
+    ens = [Ensemble(members) for _ in range(2)]
+    for e in ens:
+        for i, f in enumerate(fields):
+            e.upload(i, f["u"], f["v"], f["w"], f["b"])
+    for n in (7, 8, 5, 11):
+        ens[0].integrate(n)
+    ens[1].integrate(31)
+    for i in range(len(members)):
+        a, b = ens[0].download(i), ens[1].download(i)
+        for n in ("u", "v", "w", "b", "p"):
+            assert np.array_equal(a[n], b[n]), (i, n)
+    for e in ens:
+        e.close()
+
+
 def test_plane_implementations_agree():
     """The cluster kernels and the rows + y-lines kernels compute the same
     transforms with the same radix schedules: 30 steps agree to 1e-12."""
