@@ -1625,7 +1625,7 @@ namespace ps3d {
 bool pdl_enabled() {
     static const bool on = [] {
         const char* e = std::getenv("PS3D_PDL");
-        return !(e && e[0] == '0');
+        return e && e[0] == '1';
     }();
     return on;
 }

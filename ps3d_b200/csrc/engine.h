@@ -8,9 +8,11 @@
 namespace ps3d {
 
 // Launch with programmatic stream serialization (see pdl_trigger/pdl_wait):
-// only for kernels that call pdl_wait before reading their inputs.
-// PS3D_PDL=0 launches them with ordinary full dependencies instead
-// (griddepcontrol.wait then returns at once).
+// only for kernels that call pdl_wait before reading their inputs.  Off by
+// default (ordinary full dependencies; griddepcontrol.wait then returns at
+// once): measured on a B200 at 256x256x128, the programmatic overlap made
+// the step 95 us slower in both precisions, eager or in CUDA graphs.
+// PS3D_PDL=1 turns it on.
 bool pdl_enabled();
 template <typename... P, typename... A>
 inline cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
