@@ -18,6 +18,7 @@
 // my_ifft_vert_mode, my_fft.f90:211-252) are dense nz x nz real matrices
 // applied to every (kx,ky) column; k_vert_mode stages a block of columns in
 // shared memory and sums in the reference's order.
+#include <cstdlib>
 #include "eigen.cuh"
 
 namespace ps3d {
@@ -136,10 +137,10 @@ cudaError_t launch_project(const ProjArgs& a, cudaStream_t s) {
 
 // The same product with the matrix staged in shared memory as well (nz^2
 // doubles beside the tile; nz <= 104 keeps two blocks per SM): the matrix
-// pairs are then warp-uniform shared-memory loads instead of L1 loads.  A
-// block copies the matrix once and runs kVmTiles column tiles in turn, so
-// the copy is amortised.
-constexpr int kVmTiles = 4;
+// pairs are then warp-uniform shared-memory loads instead of L1 loads.  The
+// grid is as many blocks as are resident at once, each copying the matrix
+// once and walking the column tiles with the grid's stride, so the copy is
+// amortised and no SM idles in a partial last wave.
 size_t vert_mode_smem_staged(int nz) { return (size_t)nz * kVmCols * sizeof(double2) + (size_t)nz * nz * sizeof(double); }
 
 __global__ void __launch_bounds__(kVmThreads) k_vert_mode_staged(const double2* __restrict__ in,
@@ -152,9 +153,9 @@ __global__ void __launch_bounds__(kVmThreads) k_vert_mode_staged(const double2* 
     const int l = threadIdx.x % kVmCols;
     const int wid = threadIdx.x / kVmCols, nw = blockDim.x / kVmCols;
     const int nch = (nz + kVmKo - 1) / kVmKo;
-    for (int tt = 0; tt < kVmTiles; ++tt) {
-        const long c0 = ((long)blockIdx.x * kVmTiles + tt) * kVmCols;
-        if (c0 >= ncol) break;
+    const long ntiles = (ncol + kVmCols - 1) / kVmCols;
+    for (long tile_i = blockIdx.x; tile_i < ntiles; tile_i += gridDim.x) {
+        const long c0 = tile_i * kVmCols;
         const int nl = (int)min((long)kVmCols, ncol - c0);
         __syncthreads();   // the previous tile is read (and, the first time, nothing)
         for (int t = threadIdx.x; t < nz * kVmCols; t += blockDim.x) {
@@ -222,8 +223,17 @@ cudaError_t launch_vert_mode(const double2* in, double2* out, const double* A, i
         if ((f[0] == '0' || f[0] == '1') && (f[0] == '0' || (nz % 2 == 0 && vert_mode_smem_staged(nz) <= 227 * 1024)))
             form = f[0] - '0';
     if (form == 1) {
-        const int blocks = (int)((ncol + (long)kVmCols * kVmTiles - 1) / ((long)kVmCols * kVmTiles));
-        k_vert_mode_staged<<<blocks, kVmThreads, vert_mode_smem_staged(nz), s>>>(in, out, A, nz, ncol, scale);
+        const size_t sm = vert_mode_smem_staged(nz);
+        int dev = 0, nsm = 148, per = 1;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_vert_mode_staged, kVmThreads, sm) != cudaSuccess ||
+            per < 1) {
+            cudaGetLastError();
+            per = 1;
+        }
+        const long ntiles = (ncol + kVmCols - 1) / kVmCols;
+        const int blocks = (int)std::min<long>(ntiles, (long)nsm * per);
+        k_vert_mode_staged<<<blocks, kVmThreads, sm, s>>>(in, out, A, nz, ncol, scale);
         return cudaGetLastError();
     }
     const size_t sm = vert_mode_smem(nz);
