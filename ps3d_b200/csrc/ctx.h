@@ -134,6 +134,7 @@ struct Ctx {
     int win_kbeg = 0, win_kcount = 0, win_kofs = 0, win_nzg = 0;
     bool split_solve = false;
     int kchunk = 8;             // z levels per block of the step kernel
+    bool tune_timing = true;    // false: the autotuner takes cached choices or the defaults, no timing runs
     std::string tuned;          // description of the autotuned choice
     DevBuf twx;
     DevBuf t_kx, t_ky, t_kz, t_hkx, t_hky, t_hkz, t_ex, t_ey, t_ez, t_px, t_py, t_pz, t_sz, t_cz, t_hkz_ds;

@@ -645,6 +645,7 @@ int Ctx::autotune() {
             return PS3D_OK;
         }
     }
+    if (!tune_timing) return PS3D_OK;   // the defaults chosen at init
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

@@ -433,154 +433,6 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
 }
 #undef IN
 
-// The same solve with its right-hand side streamed through a per-thread
-// ring of DEPTH chunks in shared memory, filled by asynchronous copies
-// (cp.async, 4 or 8 bytes per thread and level, a warp's copies of one level
-// coalesced): DEPTH - 1 chunks are in flight while the recurrence runs over
-// the current one, without registers held for them.  Each thread reads only
-// the ring slots it filled itself, so no block barrier is involved.
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-template <typename R>
-__device__ __forceinline__ void cp_async_elem(R* dst, const R* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_u32(dst)), "l"(src), "n"((int)sizeof(R))
-                 : "memory");
-}
-
-PS3D_HD size_t thomas_async_smem(int nz, int threads, int depth, size_t rs) {
-    return thomas_smem(nz, threads) + (size_t)depth * kThomasChunk * threads * rs;
-}
-
-template <typename R, bool FULL, int DEPTH>
-__global__ void __launch_bounds__(64) k_thomas_async(const ColumnArgs a) {
-    pdl_trigger();
-    pdl_wait();   // inputs written by the preceding kernels
-    constexpr int KC = kThomasChunk;
-#define IN(cond) (FULL || (cond))
-    extern __shared__ double2 ckp[];   // [chunk][thread] (c', d'), then the ring [DEPTH][KC][thread]
-    const int nz = a.nz;
-    const int nchk = (nz + KC - 1) / KC;
-    const int T = blockDim.x, tid = threadIdx.x;
-    R* ring = reinterpret_cast<R*>(ckp + (size_t)(nchk + 1) * T);
-    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
-    const long gid = blockIdx.x * (long)T + tid;
-    if (gid >= 2 * ncols * a.batch) return;
-    const int part = (int)(gid & 1);
-    const unsigned cb = (unsigned)(gid >> 1);
-    const unsigned inst = fdiv(cb, a.fd_ncols);
-    const unsigned c = cb - inst * (unsigned)ncols;
-    R* col = reinterpret_cast<R*>(a.spec) + 2 * ((long)inst * a.sM + c) + part;
-    const long ls = 2 * ncols;   // level stride in R
-    const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
-    const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
-    const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
-    const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
-    const double ks = a.hkx[i] + a.hky[j];
-    const double fxa = a.fxa;
-    double2* ck = ckp + tid;
-    // chunk s of the column into its ring slot (levels past nz are not copied)
-    auto issue = [&](int s) {
-        if (s >= 0 && s < nchk) {
-            R* slot = ring + (size_t)(s % DEPTH) * KC * T + tid;
-#pragma unroll
-            for (int q = 0; q < KC; ++q)
-                if (IN(s * KC + q < nz)) cp_async_elem(slot + q * T, col + (long)(s * KC + q) * ls);
-        }
-        cp_async_commit();   // an empty group keeps the count uniform
-    };
-    auto take = [&](int s, R* d) {
-        const R* slot = ring + (size_t)(s % DEPTH) * KC * T + tid;
-#pragma unroll
-        for (int q = 0; q < KC; ++q) d[q] = slot[q * T];
-    };
-    if (ks > 0) {
-        const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-        // forward elimination (as k_thomas): cp(1) = c/b(1), dp(1) = d(1)/b(1);
-        // r = 1/(b(k) - cp(k-1) a), cp(k) = c r, dp(k) = (d(k) - dp(k-1) a) r
-        auto elim = [&](int k, double d, double& cp, double& dp) {
-            const double bk = (k == 0 || k == nz - 1) ? bend : bmid;
-            if (k == 0) {
-                cp = fxa / bk;
-                dp = d / bk;
-            } else {
-                const double r = __drcp_rn(bk - cp * fxa);   // == 1.0 / x (both correctly rounded)
-                cp = fxa * r;
-                dp = (d - dp * fxa) * r;
-            }
-        };
-        double cp = 0.0, dp = 0.0;
-#pragma unroll
-        for (int s = 0; s < DEPTH - 1; ++s) issue(s);
-        for (int s = 0; s < nchk; ++s) {
-            issue(s + DEPTH - 1);
-            cp_async_wait<DEPTH - 1>();   // chunk s has landed
-            R d[KC];
-            take(s, d);
-            ck[s * T] = make_double2(cp, dp);   // (cp, dp) of level s*KC - 1
-#pragma unroll
-            for (int q = 0; q < KC; ++q)
-                if (IN(s * KC + q < nz)) elim(s * KC + q, (double)d[q], cp, dp);
-        }
-        cp_async_wait<0>();
-        // back substitution from the top chunk down: x(nz) = dp(nz),
-        // x(k) = dp(k) - cp(k) x(k+1); each chunk's dp recomputed first
-        double x = 0.0;
-#pragma unroll
-        for (int u = 0; u < DEPTH - 1; ++u) issue(nchk - 1 - u);
-        for (int s = nchk - 1; s >= 0; --s) {
-            issue(s - (DEPTH - 1));
-            cp_async_wait<DEPTH - 1>();
-            R d[KC];
-            take(s, d);
-            const int kb = s * KC;
-            double cpl[KC], dpl[KC];
-            {
-                const double2 c0 = ck[s * T];
-                double cpv = c0.x, dpv = c0.y;
-#pragma unroll
-                for (int q = 0; q < KC; ++q) {
-                    if (IN(kb + q < nz)) elim(kb + q, (double)d[q], cpv, dpv);
-                    cpl[q] = cpv;
-                    dpl[q] = dpv;
-                }
-            }
-#pragma unroll
-            for (int q = KC - 1; q >= 0; --q) {
-                const int k = kb + q;
-                if (IN(k < nz)) {
-                    x = (k == nz - 1) ? dpl[q] : dpl[q] - cpl[q] * x;
-                    col[(long)k * ls] = (R)x;
-                }
-            }
-        }
-        cp_async_wait<0>();
-    } else {
-        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
-        const double h = a.dz2dsqr;
-        double x0 = 0.0, x1 = 0.0, fprev = 0.0;   // p(k-2), p(k-1), f(k-1)
-#pragma unroll
-        for (int s = 0; s < DEPTH - 1; ++s) issue(s);
-        for (int s = 0; s < nchk; ++s) {
-            issue(s + DEPTH - 1);
-            cp_async_wait<DEPTH - 1>();
-            R d[KC];
-            take(s, d);
-#pragma unroll
-            for (int q = 0; q < KC; ++q) {
-                const int k = s * KC + q;
-                if (IN(k < nz)) {
-                    const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
-                    fprev = (double)d[q];
-                    x0 = x1; x1 = xk;
-                    col[(long)k * ls] = (R)xk;
-                }
-            }
-        }
-        cp_async_wait<0>();
-    }
-}
-#undef IN
 
 // The same solve eliminated from both ends at once (a twisted
 // factorisation): the matrix is persymmetric (constant a = c = fxa, the same
@@ -1528,8 +1380,6 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
-    if ((e = max_dynamic_smem(k_thomas_async<R, true, sizeof(R) == 4 ? 4 : 3>))) return e;
-    if ((e = max_dynamic_smem(k_thomas_async<R, false, sizeof(R) == 4 ? 4 : 3>))) return e;
     if ((e = setup_m<R, 16>())) return e;
     return setup_m<R, 8>();
 }
@@ -1608,9 +1458,8 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_nxh = make_fastdiv(a.nxh);
     // the two-ended form where its checkpoints leave room for 4 blocks of 128
-    // per SM; else the streamed form (64-thread blocks, a ring 4 chunks deep
-    // in FP32, 3 in FP64) where it fits, else the one-ended form with fewer
-    // threads per block; PS3D_THOMAS_FORM=0|1|2 pins one
+    // per SM, else the one-ended form with as many threads per block as its
+    // checkpoints allow; PS3D_THOMAS_FORM=0|2 pins one
     const char* pin = std::getenv("PS3D_THOMAS_FORM");
     if ((!pin && thomas2_smem(a.nz, kThomasThreads) <= 56 * 1024) ||
         (pin && pin[0] == '2' && thomas2_smem(a.nz, kThomasThreads) <= 227 * 1024 - 64)) {
@@ -1619,24 +1468,6 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
         const size_t sm2 = thomas2_smem(a.nz, kThomasThreads);
         if (fp32) return launch_pdl(k_thomas2<float>, g, b, sm2, s, a);
         return launch_pdl(k_thomas2<double>, g, b, sm2, s, a);
-    }
-    {
-        const size_t rs = fp32 ? sizeof(float) : sizeof(double);
-        const int depth = fp32 ? 4 : 3;
-        const size_t sma = thomas_async_smem(a.nz, 64, depth, rs);
-        int form = sma <= 56 * 1024 ? 1 : 0;
-        if (pin && (pin[0] == '0' || (pin[0] == '1' && sma <= 227 * 1024 - 64))) form = pin[0] - '0';
-        if (form == 1) {
-            const long nthreads = 2 * ncols * std::max(1, a.batch);
-            const dim3 g((unsigned)((nthreads + 63) / 64)), b(64);
-            const bool full = a.nz % kThomasChunk == 0;
-            if (fp32) {
-                if (full) return launch_pdl(k_thomas_async<float, true, 4>, g, b, sma, s, a);
-                return launch_pdl(k_thomas_async<float, false, 4>, g, b, sma, s, a);
-            }
-            if (full) return launch_pdl(k_thomas_async<double, true, 3>, g, b, sma, s, a);
-            return launch_pdl(k_thomas_async<double, false, 3>, g, b, sma, s, a);
-        }
     }
     const int nt = thomas_threads(a.nz);
     if (nt == 0 || ncols < 1) return cudaErrorInvalidValue;

@@ -149,6 +149,10 @@ std::unique_ptr<Ctx> ps3d_server::run(Request& r, std::unique_ptr<Ctx> reuse) {
         rc = cp->reset_request();
     } else {
         cp.reset(new Ctx());
+        // no autotuning runs here: they would time their candidates while
+        // other requests share the GPU, and one context at a time (the
+        // tuner's lock); cached choices or the defaults are taken instead
+        cp->tune_timing = false;
         rc = cp->init(r.prm, device);
     }
     Ctx& c = *cp;
