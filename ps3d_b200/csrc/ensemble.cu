@@ -125,6 +125,12 @@ int advance(ps3d_ensemble* e, int nsteps) {
 
 }  // namespace
 
+namespace ps3d {
+// ps3d_ensemble_create with the autotuner's timing runs optional (the
+// serving loop creates ensembles while other requests run)
+int ensemble_create(const ps3d_params* members, int n, int device, bool tune, ps3d_ensemble** out);
+}
+
 #define EGUARD_BEGIN try {
 #define EGUARD_END                                         \
     }                                                      \
@@ -134,6 +140,12 @@ int advance(ps3d_ensemble* e, int nsteps) {
 extern "C" {
 
 PS3D_API int ps3d_ensemble_create(const ps3d_params* members, int n, int device, ps3d_ensemble** out) {
+    return ps3d::ensemble_create(members, n, device, true, out);
+}
+
+}  // extern "C"
+
+int ps3d::ensemble_create(const ps3d_params* members, int n, int device, bool tune, ps3d_ensemble** out) {
     EGUARD_BEGIN
     if (!members || n < 1 || !out) return PS3D_ERR_BADPARAM;
     *out = nullptr;
@@ -152,6 +164,7 @@ PS3D_API int ps3d_ensemble_create(const ps3d_params* members, int n, int device,
     }
     for (size_t q = 0; q < leader.size(); ++q) {
         std::unique_ptr<Ctx> c(new Ctx());
+        c->tune_timing = tune;
         int rc = c->init(members[leader[q]], device, count[q], e->stream);
         if (rc) return rc;
         e->groups.push_back(std::move(c));
@@ -160,6 +173,8 @@ PS3D_API int ps3d_ensemble_create(const ps3d_params* members, int n, int device,
     return PS3D_OK;
     EGUARD_END
 }
+
+extern "C" {
 
 PS3D_API int ps3d_ensemble_destroy(ps3d_ensemble* e) {
     EGUARD_BEGIN

@@ -34,6 +34,10 @@
 using ps3d::Ctx;
 using Clock = std::chrono::steady_clock;
 
+namespace ps3d {
+int ensemble_create(const ps3d_params* members, int n, int device, bool tune, ps3d_ensemble** out);
+}
+
 namespace {
 
 enum State { kQueued, kRunning, kDone, kFailed, kCancelled };
@@ -109,7 +113,7 @@ static bool same_params(const ps3d_params& a, const ps3d_params& b) { return std
 static int run_ensemble(Request& r, int device) {
     const int n = (int)r.members.size();
     ps3d_ensemble* e = nullptr;
-    int rc = ps3d_ensemble_create(r.members.data(), n, device, &e);
+    int rc = ps3d::ensemble_create(r.members.data(), n, device, false, &e);
     for (int m = 0; m < n && !rc; ++m)
         rc = ps3d_ensemble_upload(e, m, r.ein[4 * m].data(), r.ein[4 * m + 1].data(), r.ein[4 * m + 2].data(),
                                   r.ein[4 * m + 3].data());
