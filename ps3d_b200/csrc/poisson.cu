@@ -593,6 +593,164 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
     }
 }
 
+// The two-ended solve with one thread per complex column: a pivot's
+// reciprocal serves both parts, and the ceil(nz/2) reciprocals are kept in
+// shared memory for the back substitution instead of being formed again, so
+// a column costs about a quarter of the instructions of two threads that
+// each form every pivot twice (the bound of the forms above, which issue
+// ~5,000 instructions per thread at ~14 warps per SM).  d' and d'' (the
+// two ends) are still never stored: their values before every KC-level
+// chunk are kept in shared memory and each chunk's are recomputed, from
+// the untouched right-hand side and the stored reciprocals, on the way back.
+template <int KC>
+PS3D_HD size_t thomas3_smem(int nz, int threads) {
+    const int h = (nz + 1) / 2;
+    return (size_t)h * threads * sizeof(double) + (size_t)((h + KC - 1) / KC) * threads * 2 * sizeof(double2);
+}
+
+template <typename R, int KC>
+__global__ void __launch_bounds__(64) k_thomas3(const ColumnArgs a) {
+    using T = cpx<R>;
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
+    extern __shared__ double2 sm3[];
+    const int nz = a.nz;
+    const int H = (nz + 1) / 2;   // pivot levels: top 0 .. H-1, bottom nz-1 .. nz-Bc
+    const int Bc = nz - H;
+    const int m = H - 1, jb = Bc - 1;
+    const int nch = (H + KC - 1) / KC;
+    const int NT = blockDim.x, tid = threadIdx.x;
+    double* rs = reinterpret_cast<double*>(sm3) + tid;                          // [H][NT] reciprocal pivots
+    double2* ck = reinterpret_cast<double2*>(reinterpret_cast<double*>(sm3) + (size_t)H * NT) + tid;   // [nch][2][NT]
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
+    const long gid = blockIdx.x * (long)NT + tid;
+    if (gid >= ncols * a.batch) return;
+    const unsigned inst = fdiv((unsigned)gid, a.fd_ncols);
+    const unsigned c = (unsigned)gid - inst * (unsigned)ncols;
+    T* col = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + c;
+    const long ls = ncols;   // level stride in complex elements
+    const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
+    const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
+    const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
+    const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
+    const double ks = a.hkx[i] + a.hky[j];
+    const double fxa = a.fxa;
+    if (!(ks > 0)) {
+        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
+        const double h = a.dz2dsqr;
+        double x0x = 0.0, x0y = 0.0, x1x = 0.0, x1y = 0.0, fx = 0.0, fy = 0.0;
+        for (int k = 0; k < nz; ++k) {
+            const T d = col[(long)k * ls];
+            const double xkx = k == 0 ? 0.0 : 2 * x1x - x0x + fx * h;
+            const double xky = k == 0 ? 0.0 : 2 * x1y - x0y + fy * h;
+            fx = (double)d.x; fy = (double)d.y;
+            x0x = x1x; x0y = x1y; x1x = xkx; x1y = xky;
+            col[(long)k * ls] = mk<R>((R)xkx, (R)xky);
+        }
+        return;
+    }
+    const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+    const double cp0 = fxa / bend;   // cp(1) = c/b(1)
+    // one pivot level jj from both ends: dp(1) = d(1)/b(1), dp = (d - dp a) r;
+    // the bottom chain the same with its own right-hand side
+    auto load = [&](int jc, T* top, T* bot) {
+#pragma unroll
+        for (int q = 0; q < KC; ++q) {
+            const int jj = jc + q;
+            if (jj < H) top[q] = col[(long)jj * ls];
+            if (jj < Bc) bot[q] = col[(long)(nz - 1 - jj) * ls];
+        }
+    };
+    double cp = 0.0, dpx = 0.0, dpy = 0.0, dqx = 0.0, dqy = 0.0;
+    double cp_jb = 0.0, dqx_jb = 0.0, dqy_jb = 0.0;
+    T nt[KC], nb[KC];
+#pragma unroll
+    for (int q = 0; q < KC; ++q) { nt[q] = mk<R>((R)0, (R)0); nb[q] = nt[q]; }
+    load(0, nt, nb);
+    for (int ch = 0; ch < nch; ++ch) {
+        const int jc = ch * KC;
+        T dt[KC], db[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
+        if (ch + 1 < nch) load(jc + KC, nt, nb);
+        ck[(2 * ch) * NT] = make_double2(dpx, dpy);   // before pivot level jc
+        ck[(2 * ch + 1) * NT] = make_double2(dqx, dqy);
+#pragma unroll
+        for (int q = 0; q < KC; ++q) {
+            const int jj = jc + q;
+            if (jj < H) {
+                if (jj == 0) {
+                    cp = cp0;
+                    dpx = (double)dt[q].x / bend; dpy = (double)dt[q].y / bend;
+                    dqx = (double)db[q].x / bend; dqy = (double)db[q].y / bend;
+                } else {
+                    const double r = __drcp_rn(bmid - cp * fxa);   // == 1.0 / x (both correctly rounded)
+                    rs[jj * NT] = r;
+                    cp = fxa * r;
+                    dpx = ((double)dt[q].x - dpx * fxa) * r;
+                    dpy = ((double)dt[q].y - dpy * fxa) * r;
+                    if (jj < Bc) {
+                        dqx = ((double)db[q].x - dqx * fxa) * r;
+                        dqy = ((double)db[q].y - dqy * fxa) * r;
+                    }
+                }
+                if (jj == jb) { cp_jb = cp; dqx_jb = dqx; dqy_jb = dqy; }
+            }
+        }
+    }
+    // the two halves meet: x(m) = (dp(m) - cp(m) dq(jb)) / (1 - cp(m) cp(jb)),
+    // x(m+1) = dq(jb) - cp(jb) x(m)
+    const double den = 1.0 - cp * cp_jb;
+    double xtx = (dpx - cp * dqx_jb) / den, xty = (dpy - cp * dqy_jb) / den;
+    double xbx = dqx_jb - cp_jb * xtx, xby = dqy_jb - cp_jb * xty;
+    load((nch - 1) * KC, nt, nb);
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        const int jc = ch * KC;
+        T dt[KC], db[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
+        if (ch > 0) load(jc - KC, nt, nb);
+        double px[KC], py[KC], qx[KC], qy[KC], cpl[KC];
+        {
+            const double2 p0 = ck[(2 * ch) * NT], b0 = ck[(2 * ch + 1) * NT];
+            double vx = p0.x, vy = p0.y, wx = b0.x, wy = b0.y;
+#pragma unroll
+            for (int q = 0; q < KC; ++q) {
+                const int jj = jc + q;
+                if (jj < H) {
+                    if (jj == 0) {
+                        cpl[q] = cp0;
+                        vx = (double)dt[q].x / bend; vy = (double)dt[q].y / bend;
+                        wx = (double)db[q].x / bend; wy = (double)db[q].y / bend;
+                    } else {
+                        const double r = rs[jj * NT];
+                        cpl[q] = fxa * r;
+                        vx = ((double)dt[q].x - vx * fxa) * r;
+                        vy = ((double)dt[q].y - vy * fxa) * r;
+                        if (jj < Bc) {
+                            wx = ((double)db[q].x - wx * fxa) * r;
+                            wy = ((double)db[q].y - wy * fxa) * r;
+                        }
+                    }
+                }
+                px[q] = vx; py[q] = vy; qx[q] = wx; qy[q] = wy;
+            }
+        }
+#pragma unroll
+        for (int q = KC - 1; q >= 0; --q) {
+            const int jj = jc + q;
+            if (jj < H) {
+                if (jj < m) { xtx = px[q] - cpl[q] * xtx; xty = py[q] - cpl[q] * xty; }
+                col[(long)jj * ls] = mk<R>((R)xtx, (R)xty);
+                if (jj <= jb) {
+                    if (jj < jb) { xbx = qx[q] - cpl[q] * xbx; xby = qy[q] - cpl[q] * xby; }
+                    col[(long)(nz - 1 - jj) * ls] = mk<R>((R)xbx, (R)xby);
+                }
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // K3, triply periodic: z FFT, spectral division, inverse z FFT
 // (pressure_solver.f90:58-70; my_fft_3D/my_ifft_3D z leg)
@@ -1377,6 +1535,7 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
+    if ((e = max_dynamic_smem(k_thomas3<R, 4>))) return e;
     if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
@@ -1457,10 +1616,30 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     a.fd_ncols = make_fastdiv((unsigned)ncols);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_nxh = make_fastdiv(a.nxh);
-    // the two-ended form where its checkpoints leave room for 4 blocks of 128
-    // per SM, else the one-ended form with as many threads per block as its
-    // checkpoints allow; PS3D_THOMAS_FORM=0|2 pins one
+    // the one-thread-per-column form where its reciprocals and checkpoints
+    // leave room for 4 blocks of 64 per SM, else the two-ended form with two
+    // threads per column where 4 blocks of 128 fit, else the one-ended form
+    // with as many threads per block as its checkpoints allow;
+    // PS3D_THOMAS_FORM=0|2|3 pins one
     const char* pin = std::getenv("PS3D_THOMAS_FORM");
+    {
+        // 64 or 32 threads per block, whichever keeps more columns resident
+        // (the shared memory per column is fixed)
+        int nt3 = 0, best = 0;
+        for (int nt : {64, 32}) {
+            const size_t sm = thomas3_smem<4>(a.nz, nt);
+            if (sm > 227 * 1024 - 64) continue;
+            const int res = std::min(32, (int)((228 * 1024) / (sm + 1024))) * nt;
+            if (res > best) { best = res; nt3 = nt; }
+        }
+        if (nt3 && ((!pin && best >= 128) || (pin && pin[0] == '3'))) {
+            const size_t sm3 = thomas3_smem<4>(a.nz, nt3);
+            const long nthreads = ncols * std::max(1, a.batch);
+            const dim3 g((unsigned)((nthreads + nt3 - 1) / nt3)), b(nt3);
+            if (fp32) return launch_pdl(k_thomas3<float, 4>, g, b, sm3, s, a);
+            return launch_pdl(k_thomas3<double, 4>, g, b, sm3, s, a);
+        }
+    }
     if ((!pin && thomas2_smem(a.nz, kThomasThreads) <= 56 * 1024) ||
         (pin && pin[0] == '2' && thomas2_smem(a.nz, kThomasThreads) <= 227 * 1024 - 64)) {
         const long nthreads = 2 * ncols * std::max(1, a.batch);
