@@ -91,6 +91,72 @@ PS3D_HD int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// ---------------------------------------------------------------------------
+// L2 eviction priorities (createpolicy + .L2::cache_hint).  A pressure solve
+// writes its spectral array in the forward rows pass and every later pass
+// reads it (y lines, vertical solve, y lines, inverse rows), while the real
+// fields stream through L2 at several times its bytes: the spectra are
+// accessed with evict_last and the streamed fields with evict_first, so the
+// spectra stay resident in the 126 MB L2 between the kernels of a solve
+// instead of being pushed out by the fields.  kL2Normal gives the default
+// priority (the hints off).
+// ---------------------------------------------------------------------------
+enum : int { kL2Normal = 0, kL2Keep = 1, kL2Stream = 2 };
+__device__ __forceinline__ unsigned long long l2_policy(int kind) {
+    unsigned long long p;
+    if (kind == kL2Keep)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else if (kind == kL2Stream)
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// coherent loads and stores with a policy (data the kernel may also write)
+__device__ __forceinline__ float2 ld_l2(const float2* a, unsigned long long pol) {
+    float2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ double2 ld_l2(const double2* a, unsigned long long pol) {
+    double2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_l2(float2* a, float2 v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(a), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_l2(double2* a, double2 v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ float ld_l2(const float* a, unsigned long long pol) {
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ double ld_l2(const double* a, unsigned long long pol) {
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_l2(float* a, float v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_l2(double* a, double v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+// read-only (non-coherent) loads with a policy: fields the kernel does not write
+__device__ __forceinline__ double ldg_l2(const double* a, unsigned long long pol) {
+    double v;
+    asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double2 ldg_l2(const double2* a, unsigned long long pol) {
+    double2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+    return v;
+}
+
 // status flags written by kernels (bit mask, OR-ed)
 enum : unsigned {
     kFlagNonFinite = 1u,

@@ -833,6 +833,7 @@ int Ctx::poisson_once(double* out, double beta, bool lazy, const double* pc) {
     c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = FS.p;
     c.batch = batch; c.sM = M; c.layout = spectral_layout(a);
     c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p; c.hkz = (const double*)t_hkz_ds.p;
+    c.err = kerr_d;
     if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         c.dz2dsqr = P.dz * P.dz * P.dsqr;

@@ -100,6 +100,7 @@ struct PlaneArgs {
     // only): real-field levels kbeg .. kbeg+kcount-1 map to spectral levels
     // 0 .. kcount-1; the rigid-lid masks see the global level k + kofs of nzg
     int kbeg, kcount, kofs, nzg;
+    int l2hint;                    // L2 eviction priorities on (set by the launchers; PS3D_L2HINT=0: off)
 };
 // spectral layout of a plane configuration: 0 [k][ky][kx], 1 [k][kx][ky]
 inline int spectral_layout(const PlaneArgs& a) { return a.impl != 0; }
@@ -122,7 +123,13 @@ struct ColumnArgs {
     // level, global columns col0 .. col0+ncl-1 (one instance)
     long col0, ncl;
     FastDiv fd_ncols, fd_ny, fd_nxh;   // set by the launchers
+    int l2hint;                        // L2 eviction priorities on (set by the launchers)
+    unsigned* err;                     // set to 1 when a bounded wait ran out (NULL: not reported)
 };
+// the L2 eviction priorities the launchers set: 1 (default) spectra kept in
+// L2 across the passes of a solve, 0 off (PS3D_L2HINT=0), 2 also the real
+// fields evict_first (PS3D_L2HINT=2)
+int l2hint_mode();
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
 cudaError_t step_setup();   // opts the step kernels in to their dynamic shared memory

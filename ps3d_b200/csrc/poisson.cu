@@ -36,35 +36,43 @@ constexpr int kPlaneThreads = 256;
 template <int MAXR> constexpr int plane_min_blocks() { return MAXR >= 16 ? 2 : 3; }
 template <typename R, int MAXR> constexpr int lines_min_blocks() { return MAXR >= 16 ? 2 : 4; }
 
+// the L2 policies of a kernel (PlaneArgs/ColumnArgs::l2hint): the spectra
+// evict_last while later passes read them, evict_first at their last read;
+// the real fields default priority (evict_first with l2hint == 2)
+__device__ __forceinline__ unsigned long long pol_keep(int h) { return l2_policy(h ? kL2Keep : kL2Normal); }
+__device__ __forceinline__ unsigned long long pol_last(int h) { return l2_policy(h ? kL2Stream : kL2Normal); }
+__device__ __forceinline__ unsigned long long pol_field(int h) { return l2_policy(h == 2 ? kL2Stream : kL2Normal); }
+
 // Divergence of the pair of points (2m, 2m+1) of row j in plane k, divided by
 // dt (pressure_solver.f90:16-24), or the pair of source values (mode 1).
 __device__ __forceinline__ double2 plane_source_pair(const PlaneArgs& a, const double* au, const double* av,
-                                                     const double* aw, const double* asrc, int k, int j, int m) {
+                                                     const double* aw, const double* asrc, int k, int j, int m,
+                                                     unsigned long long pol) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const long plane = (long)nx * ny;
     const long g = (long)k * plane + (long)j * nx + 2 * m;
-    if (a.mode == 1) return __ldg(reinterpret_cast<const double2*>(asrc + g));
+    if (a.mode == 1) return ldg_l2(reinterpret_cast<const double2*>(asrc + g), pol);
     const long gum = g - 2 * m + wrap(2 * m - 1, nx);
     const long gv = g + (long)(wrap(j - 1, ny) - j) * nx;
     const long gw = g + (long)(wrap(k - 1, nz) - k) * plane;
-    double2 uu = __ldg(reinterpret_cast<const double2*>(au + g));
-    double um = __ldg(au + gum);
-    double2 vv = __ldg(reinterpret_cast<const double2*>(av + g));
-    double2 vm = __ldg(reinterpret_cast<const double2*>(av + gv));
-    double2 ww = __ldg(reinterpret_cast<const double2*>(aw + g));
-    double2 wm = __ldg(reinterpret_cast<const double2*>(aw + gw));
+    double2 uu = ldg_l2(reinterpret_cast<const double2*>(au + g), pol);
+    double um = ldg_l2(au + gum, pol);
+    double2 vv = ldg_l2(reinterpret_cast<const double2*>(av + g), pol);
+    double2 vm = ldg_l2(reinterpret_cast<const double2*>(av + gv), pol);
+    double2 ww = ldg_l2(reinterpret_cast<const double2*>(aw + g), pol);
+    double2 wm = ldg_l2(reinterpret_cast<const double2*>(aw + gw), pol);
     if (a.mode == 2) {
         // u - dt grad p at the points the divergence reads (pressure_solver.f90:98-110)
         const double* pc = a.pc + (au - a.u);   // same instance offset as the fields
         const long gpe = g - 2 * m + wrap(2 * m + 2, nx);
         const long gpn = g + (long)(wrap(j + 1, ny) - j) * nx;
         const long gpu = g + (long)(wrap(k + 1, nz) - k) * plane;
-        const double2 p0 = __ldg(reinterpret_cast<const double2*>(pc + g));
-        const double pw = __ldg(pc + gum), pe = __ldg(pc + gpe);
-        const double2 ps = __ldg(reinterpret_cast<const double2*>(pc + gv));
-        const double2 pn = __ldg(reinterpret_cast<const double2*>(pc + gpn));
-        const double2 pd = __ldg(reinterpret_cast<const double2*>(pc + gw));
-        const double2 pu = __ldg(reinterpret_cast<const double2*>(pc + gpu));
+        const double2 p0 = ldg_l2(reinterpret_cast<const double2*>(pc + g), pol);
+        const double pw = ldg_l2(pc + gum, pol), pe = ldg_l2(pc + gpe, pol);
+        const double2 ps = ldg_l2(reinterpret_cast<const double2*>(pc + gv), pol);
+        const double2 pn = ldg_l2(reinterpret_cast<const double2*>(pc + gpn), pol);
+        const double2 pd = ldg_l2(reinterpret_cast<const double2*>(pc + gw), pol);
+        const double2 pu = ldg_l2(reinterpret_cast<const double2*>(pc + gpu), pol);
         const double dt = a.dtp, dtw = a.dtwp;
         um = um - dt * (p0.x - pw) * a.rdx;
         uu.x = uu.x - dt * (p0.y - p0.x) * a.rdx;
@@ -135,6 +143,7 @@ __device__ __forceinline__ cpx<R> c2r_pack(cpx<R> Xk, cpx<R> Xc, cpx<R> w, bool 
 // ---------------------------------------------------------------------------
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_plane_fwd(const PlaneArgs a) {
+    const unsigned long long pfield = pol_field(a.l2hint), pkeep = pol_keep(a.l2hint);
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
@@ -167,7 +176,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
                 const int t = t0 + q * blockDim.x;
                 if (t < total) {
                     const int rr = t / n2, m = t - rr * n2;
-                    d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + jc + rr, m);
+                    d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + jc + rr, m, pfield);
                 }
             }
 #pragma unroll
@@ -199,12 +208,13 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
     const R sc = (R)a.scale;
     for (int t = threadIdx.x; t < ny * ncol; t += blockDim.x) {
         const int ky = t / ncol, c = t - ky * ncol;
-        spec[((long)k * ny + ky) * nxh + c0 + c] = cscale(colbuf[ty.pos[ky] * ldc + c], sc);
+        st_l2(&spec[((long)k * ny + ky) * nxh + c0 + c], cscale(colbuf[ty.pos[ky] * ldc + c], sc), pkeep);
     }
 }
 
 template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_plane_inv(const PlaneArgs a) {
+    const unsigned long long plast = pol_last(a.l2hint);
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
@@ -233,7 +243,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
             const int t = t0 + q * blockDim.x;
             if (t < total) {
                 const int ky = t / ncol, c = t - ky * ncol;
-                v[q] = spec[((long)k * ny + ky) * nxh + c0 + c];
+                v[q] = ld_l2(&spec[((long)k * ny + ky) * nxh + c0 + c], plast);
             }
         }
 #pragma unroll
@@ -295,6 +305,25 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
 // chunk with x.  The pivots are formed from ksqr on the fly: no factor
 // table and no d' array in HBM.
 // ---------------------------------------------------------------------------
+// The FP64 reciprocal of a pivot by Newton-Raphson from the hardware
+// approximation (PTX rcp.approx.ftz.f64): two iterations y += y (1 - x y)
+// take its ~2^-20 relative error below 2^-80, and a third, with the
+// residual 1 - x y formed exactly by an FMA, rounds the result correctly
+// (Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  The pivots are
+// normal numbers bounded away from zero (the matrix is strictly diagonally
+// dominant), so the flush-to-zero approximation never sees a subnormal.
+__device__ __forceinline__ double rcp_newton(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
 constexpr int kThomasChunk = 8;
 constexpr int kThomasThreads = 128;
 
@@ -306,6 +335,7 @@ template <typename R, bool FULL>
 __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
     constexpr int KC = kThomasChunk;
     // FULL: nz is a multiple of KC, so only the chunk ends need tests
 #define IN(cond) (FULL || (cond))
@@ -347,14 +377,14 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
         R nxt[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (IN(q < nz)) nxt[q] = col[(long)q * ls];
+            if (IN(q < nz)) nxt[q] = ld_l2(&col[(long)q * ls], pk);
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
 #pragma unroll
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = col[(long)(kb + KC + q) * ls];
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = ld_l2(&col[(long)(kb + KC + q) * ls], pk);
             ck[(kb / KC) * cs] = make_double2(cp, dp);   // (cp, dp) of level kb-1
 #pragma unroll
             for (int q = 0; q < KC; ++q)
@@ -366,7 +396,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
         const int last = (nz - 1) / KC;
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (IN(last * KC + q < nz)) nxt[q] = col[(long)(last * KC + q) * ls];
+            if (IN(last * KC + q < nz)) nxt[q] = ld_l2(&col[(long)(last * KC + q) * ls], pk);
         for (int sg = last; sg >= 0; --sg) {
             const int kb = sg * KC;
             R d[KC];
@@ -374,7 +404,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
             if (sg > 0) {
 #pragma unroll
-                for (int q = 0; q < KC; ++q) nxt[q] = col[(long)(kb - KC + q) * ls];
+                for (int q = 0; q < KC; ++q) nxt[q] = ld_l2(&col[(long)(kb - KC + q) * ls], pk);
             }
             double cpl[KC], dpl[KC];
             {
@@ -397,7 +427,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
+                if (IN(kb + q < nz)) st_l2(&col[(long)(kb + q) * ls], d[q], pk);
         }
     } else {
         // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr,
@@ -407,14 +437,14 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
         R nxt[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (IN(q < nz)) nxt[q] = col[(long)q * ls];
+            if (IN(q < nz)) nxt[q] = ld_l2(&col[(long)q * ls], pk);
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
 #pragma unroll
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = col[(long)(kb + KC + q) * ls];
+                if (FULL ? (kb + KC < nz) : (kb + KC + q < nz)) nxt[q] = ld_l2(&col[(long)(kb + KC + q) * ls], pk);
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
@@ -427,7 +457,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
             }
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (IN(kb + q < nz)) col[(long)(kb + q) * ls] = d[q];
+                if (IN(kb + q < nz)) st_l2(&col[(long)(kb + q) * ls], d[q], pk);
         }
     }
 }
@@ -452,10 +482,11 @@ PS3D_HD size_t thomas2_smem(int nz, int threads) {
     return (size_t)((h + kThomasChunk - 1) / kThomasChunk + 1) * threads * (sizeof(double2) + sizeof(double));
 }
 
-template <typename R>
+template <typename R, bool NR>
 __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
     constexpr int KC = kThomasChunk;
     extern __shared__ double2 ck2[];   // [chunk][thread] (cp, dp), then [chunk][thread] dq
     const int nz = a.nz;
@@ -487,14 +518,14 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
         R nxt[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (q < nz) nxt[q] = col[(long)q * ls];
+            if (q < nz) nxt[q] = ld_l2(&col[(long)q * ls], pk);
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
 #pragma unroll
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + KC + q < nz) nxt[q] = col[(long)(kb + KC + q) * ls];
+                if (kb + KC + q < nz) nxt[q] = ld_l2(&col[(long)(kb + KC + q) * ls], pk);
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
@@ -502,7 +533,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
                     const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
                     fprev = (double)d[q];
                     x0 = x1; x1 = xk;
-                    col[(long)k * ls] = (R)xk;
+                    st_l2(&col[(long)k * ls], (R)xk, pk);
                 }
             }
         }
@@ -518,7 +549,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
             dp = dt / bend;
             dq = db / bend;
         } else {
-            const double r = __drcp_rn(bmid - cp * fxa);   // == 1.0 / x (both correctly rounded)
+            const double r = NR ? rcp_newton(bmid - cp * fxa) : __drcp_rn(bmid - cp * fxa);
             cp = fxa * r;
             dp = (dt - dp * fxa) * r;
             if (jj < Bc) dq = (db - dq * fxa) * r;
@@ -529,8 +560,8 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
 #pragma unroll
         for (int q = 0; q < KC; ++q) {
             const int jj = jc + q;
-            if (jj < H) top[q] = col[(long)jj * ls];
-            if (jj < Bc) bot[q] = col[(long)(nz - 1 - jj) * ls];
+            if (jj < H) top[q] = ld_l2(&col[(long)jj * ls], pk);
+            if (jj < Bc) bot[q] = ld_l2(&col[(long)(nz - 1 - jj) * ls], pk);
         }
     };
     double cp = 0.0, dp = 0.0, dq = 0.0, cp_jb = 0.0, dq_jb = 0.0;
@@ -583,10 +614,10 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
             const int jj = jc + q;
             if (jj < H) {
                 if (jj < m) xt = dpl[q] - cpl[q] * xt;
-                col[(long)jj * ls] = (R)xt;
+                st_l2(&col[(long)jj * ls], (R)xt, pk);
                 if (jj <= jb) {
                     if (jj < jb) xb = dql[q] - cpl[q] * xb;
-                    col[(long)(nz - 1 - jj) * ls] = (R)xb;
+                    st_l2(&col[(long)(nz - 1 - jj) * ls], (R)xb, pk);
                 }
             }
         }
@@ -613,6 +644,7 @@ __global__ void __launch_bounds__(64) k_thomas3(const ColumnArgs a) {
     using T = cpx<R>;
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
     extern __shared__ double2 sm3[];
     const int nz = a.nz;
     const int H = (nz + 1) / 2;   // pivot levels: top 0 .. H-1, bottom nz-1 .. nz-Bc
@@ -640,12 +672,12 @@ __global__ void __launch_bounds__(64) k_thomas3(const ColumnArgs a) {
         const double h = a.dz2dsqr;
         double x0x = 0.0, x0y = 0.0, x1x = 0.0, x1y = 0.0, fx = 0.0, fy = 0.0;
         for (int k = 0; k < nz; ++k) {
-            const T d = col[(long)k * ls];
+            const T d = ld_l2(&col[(long)k * ls], pk);
             const double xkx = k == 0 ? 0.0 : 2 * x1x - x0x + fx * h;
             const double xky = k == 0 ? 0.0 : 2 * x1y - x0y + fy * h;
             fx = (double)d.x; fy = (double)d.y;
             x0x = x1x; x0y = x1y; x1x = xkx; x1y = xky;
-            col[(long)k * ls] = mk<R>((R)xkx, (R)xky);
+            st_l2(&col[(long)k * ls], mk<R>((R)xkx, (R)xky), pk);
         }
         return;
     }
@@ -657,8 +689,8 @@ __global__ void __launch_bounds__(64) k_thomas3(const ColumnArgs a) {
 #pragma unroll
         for (int q = 0; q < KC; ++q) {
             const int jj = jc + q;
-            if (jj < H) top[q] = col[(long)jj * ls];
-            if (jj < Bc) bot[q] = col[(long)(nz - 1 - jj) * ls];
+            if (jj < H) top[q] = ld_l2(&col[(long)jj * ls], pk);
+            if (jj < Bc) bot[q] = ld_l2(&col[(long)(nz - 1 - jj) * ls], pk);
         }
     };
     double cp = 0.0, dpx = 0.0, dpy = 0.0, dqx = 0.0, dqy = 0.0;
@@ -741,13 +773,230 @@ __global__ void __launch_bounds__(64) k_thomas3(const ColumnArgs a) {
             const int jj = jc + q;
             if (jj < H) {
                 if (jj < m) { xtx = px[q] - cpl[q] * xtx; xty = py[q] - cpl[q] * xty; }
-                col[(long)jj * ls] = mk<R>((R)xtx, (R)xty);
+                st_l2(&col[(long)jj * ls], mk<R>((R)xtx, (R)xty), pk);
                 if (jj <= jb) {
                     if (jj < jb) { xbx = qx[q] - cpl[q] * xbx; xby = qy[q] - cpl[q] * xby; }
-                    col[(long)(nz - 1 - jj) * ls] = mk<R>((R)xbx, (R)xby);
+                    st_l2(&col[(long)(nz - 1 - jj) * ls], mk<R>((R)xbx, (R)xby), pk);
                 }
             }
         }
+    }
+}
+
+// The two-ended solve fed by bulk copies: one thread per complex column,
+// kT4Cols columns per block.  Pivot step j needs level j (from the top) and
+// level nz-1-j (from the bottom) of the block's columns, two contiguous rows
+// of the spectral array.  One thread issues both rows of a step as bulk
+// copies (TMA engine, no tensor map, no multicast) into a ring of D steps in
+// shared memory, completing on the step's mbarrier, so the copies of the
+// next D steps are in flight while the serial FP64 recurrence runs: the
+// recurrence never waits on a load, and a block holds no registers for the
+// loads in flight.  The forward sweep keeps (c', d', d'') before every
+// kT4KC-step chunk in shared memory; the backward sweep streams the steps
+// again, chunk by chunk from the middle outward (the steps of a chunk in
+// ascending order), forms the chunk's pivots and d' again from its checkpoint
+// with the same operations (so the same values), substitutes back and
+// stores x.  The (0,0) column runs its recurrence over the top half in the
+// forward sweep, parks the bottom half's right-hand side in shared memory and
+// finishes from there.  Waits are bounded: a wait that runs out sets the
+// error word and the block stops issuing, drains its copies and returns.
+// ---------------------------------------------------------------------------
+constexpr int kT4Cols = 64;   // columns (threads) per block
+constexpr int kT4KC = 8;      // pivot steps per checkpoint chunk
+template <typename R> constexpr int t4_depth() { return sizeof(R) == 4 ? 32 : 16; }   // ring steps
+
+struct T4Layout {
+    size_t ck, stash, bars, total;
+};
+template <typename R>
+PS3D_HD T4Layout t4_layout(int nz) {
+    const int H = (nz + 1) / 2, nch = (H + kT4KC - 1) / kT4KC;
+    T4Layout L;
+    L.ck = (size_t)t4_depth<R>() * 2 * kT4Cols * sizeof(cpx<R>);
+    L.stash = L.ck + (size_t)nch * 5 * kT4Cols * sizeof(double);
+    L.bars = L.stash + align16((size_t)(nz - H) * sizeof(cpx<R>));
+    L.total = L.bars + (size_t)t4_depth<R>() * sizeof(unsigned long long);
+    return L;
+}
+
+template <typename R, bool NR>
+__global__ void __launch_bounds__(kT4Cols) k_thomas4(const ColumnArgs a) {
+    using T = cpx<R>;
+    constexpr int D = t4_depth<R>(), KC = kT4KC, NT = kT4Cols;
+    static_assert(D % KC == 0, "ring of whole chunks");
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
+    extern __shared__ __align__(16) unsigned char t4_raw[];
+    __shared__ int t4_abort;
+    const int nz = a.nz, H = (nz + 1) / 2, Bc = nz - H;
+    const int m = H - 1, jb = Bc - 1;
+    const int nch = (H + KC - 1) / KC, HP = nch * KC, nsteps = 2 * HP;
+    const T4Layout L = t4_layout<R>(nz);
+    T* ring = reinterpret_cast<T*>(t4_raw);                        // [D][top, bottom][NT]
+    double* ck = reinterpret_cast<double*>(t4_raw + L.ck);         // [nch][5][NT]
+    T* stash = reinterpret_cast<T*>(t4_raw + L.stash);             // (0,0) column, levels H..nz-1
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(t4_raw + L.bars);
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
+    const int bpi = (int)((ncols + NT - 1) / NT);             // blocks per instance
+    const int inst = blockIdx.x / bpi;
+    const long c0 = (long)(blockIdx.x - inst * bpi) * NT;
+    const int ncb = (int)min((long)NT, ncols - c0);
+    const int tid = threadIdx.x;
+    const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
+    T* base = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + c0;
+    const long ls = ncols;   // level stride in complex elements
+    const unsigned bytes = (unsigned)(ncb * sizeof(T));
+    // step s: s < HP the forward sweep's pivot step s; then the backward
+    // sweep, chunks from the last, the steps of a chunk ascending
+    auto step_j = [&](int st) { return st < HP ? st : (nch - 1 - (st - HP) / KC) * KC + (st - HP) % KC; };
+    // (a slot is refilled after a block barrier that follows every thread's
+    // reads of it; the copy's write needs no proxy fence after reads)
+    auto issue = [&](int st) {   // thread 0
+        const int slot = st % D, j = step_j(st);
+        mbar_expect(&bar[slot], (j < H ? bytes : 0u) + (j < Bc ? bytes : 0u));
+        if (j < H) bulk_copy_g2s(ring + (size_t)(2 * slot) * NT, base + (long)j * ls, bytes, &bar[slot]);
+        if (j < Bc) bulk_copy_g2s(ring + (size_t)(2 * slot + 1) * NT, base + (long)(nz - 1 - j) * ls, bytes, &bar[slot]);
+    };
+    if (tid == 0) {
+        for (int i = 0; i < D; ++i) mbar_init(&bar[i], 1);
+        t4_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async();
+        for (int st = 0; st < D && st < nsteps; ++st) issue(st);
+    }
+    __syncthreads();
+    int issued = min(D, nsteps);   // thread 0's count of steps issued
+    // a chunk's D-ahead refill, after every thread has read the chunk's slots
+    auto refill = [&](int first) {
+        if (tid == 0 && !t4_abort)
+            for (int st = first + D; st < first + D + KC && st < nsteps; ++st) { issue(st); issued = st + 1; }
+    };
+    auto wait_step = [&](int st) {
+        if (!mbar_wait(&bar[st % D], (unsigned)(st / D) & 1u)) {
+            t4_abort = 1;
+            if (a.err) *(volatile unsigned*)a.err = 1u;
+        }
+    };
+
+    const bool have = tid < ncb;
+    const unsigned cg = (unsigned)(c0 + tid) + (unsigned)a.col0;   // global column: its wavenumbers
+    double ks = 1.0;
+    if (have) {
+        const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
+        const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
+        const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
+        ks = a.hkx[i] + a.hky[j];
+    }
+    const bool zero = have && !(ks > 0);   // the (0,0) column
+    const double fxa = a.fxa, h0 = a.dz2dsqr;
+    const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+    const double cp0 = fxa / bend;   // cp(1) = c/b(1)
+    double cp = 0.0, dpx = 0.0, dpy = 0.0, dqx = 0.0, dqy = 0.0;
+    double cp_jb = 0.0, dqx_jb = 0.0, dqy_jb = 0.0;
+    // (0,0): p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
+    double z0x = 0.0, z0y = 0.0, z1x = 0.0, z1y = 0.0, zfx = 0.0, zfy = 0.0;
+    auto zstep = [&](int k, T d) {
+        const double xkx = k == 0 ? 0.0 : 2 * z1x - z0x + zfx * h0;
+        const double xky = k == 0 ? 0.0 : 2 * z1y - z0y + zfy * h0;
+        zfx = (double)d.x; zfy = (double)d.y;
+        z0x = z1x; z0y = z1y; z1x = xkx; z1y = xky;
+        st_l2(&base[(long)k * ls + tid], mk<R>((R)xkx, (R)xky), pk);
+    };
+    // ---- forward sweep
+    for (int ch = 0; ch < nch && !t4_abort; ++ch) {
+        double* c = ck + (size_t)ch * 5 * NT + tid;
+        c[0] = cp; c[NT] = dpx; c[2 * NT] = dpy; c[3 * NT] = dqx; c[4 * NT] = dqy;
+        for (int q = 0; q < KC; ++q) {
+            const int jj = ch * KC + q, slot = jj % D;
+            wait_step(jj);
+            if (!have || jj >= H) continue;
+            const T dt = ring[(size_t)(2 * slot) * NT + tid];
+            const T db = jj < Bc ? ring[(size_t)(2 * slot + 1) * NT + tid] : mk<R>((R)0, (R)0);
+            if (zero) {
+                zstep(jj, dt);
+                if (jj < Bc) stash[nz - 1 - jj - H] = db;
+                continue;
+            }
+            if (jj == 0) {
+                cp = cp0;
+                dpx = (double)dt.x / bend; dpy = (double)dt.y / bend;
+                dqx = (double)db.x / bend; dqy = (double)db.y / bend;
+            } else {
+                const double r = NR ? rcp_newton(bmid - cp * fxa) : __drcp_rn(bmid - cp * fxa);
+                cp = fxa * r;
+                dpx = ((double)dt.x - dpx * fxa) * r;
+                dpy = ((double)dt.y - dpy * fxa) * r;
+                if (jj < Bc) {
+                    dqx = ((double)db.x - dqx * fxa) * r;
+                    dqy = ((double)db.y - dqy * fxa) * r;
+                }
+            }
+            if (jj == jb) { cp_jb = cp; dqx_jb = dqx; dqy_jb = dqy; }
+        }
+        __syncthreads();
+        refill(ch * KC);
+    }
+    if (zero && !t4_abort)
+        for (int k = H; k < nz; ++k) zstep(k, stash[k - H]);
+    // ---- the halves meet: x(m) = (dp(m) - cp(m) dq(jb)) / (1 - cp(m) cp(jb)), x(m+1) = dq(jb) - cp(jb) x(m)
+    const double den = 1.0 - cp * cp_jb;
+    double xtx = 0.0, xty = 0.0, xbx = 0.0, xby = 0.0;
+    if (have && !zero) {
+        xtx = (dpx - cp * dqx_jb) / den; xty = (dpy - cp * dqy_jb) / den;
+        xbx = dqx_jb - cp_jb * xtx; xby = dqy_jb - cp_jb * xty;
+    }
+    // ---- backward sweep
+    for (int t = 0; t < nch && !t4_abort; ++t) {
+        const int ch = nch - 1 - t, jc = ch * KC;
+        const double* c = ck + (size_t)ch * 5 * NT + tid;
+        double cpv = c[0], vx = c[NT], vy = c[2 * NT], wx = c[3 * NT], wy = c[4 * NT];
+        double px[KC], py[KC], qx[KC], qy[KC], cpl[KC];
+#pragma unroll
+        for (int q = 0; q < KC; ++q) {
+            const int st = HP + t * KC + q, slot = st % D, jj = jc + q;
+            wait_step(st);
+            if (have && !zero && jj < H) {
+                const T dt = ring[(size_t)(2 * slot) * NT + tid];
+                const T db = jj < Bc ? ring[(size_t)(2 * slot + 1) * NT + tid] : mk<R>((R)0, (R)0);
+                if (jj == 0) {
+                    cpv = cp0;
+                    vx = (double)dt.x / bend; vy = (double)dt.y / bend;
+                    wx = (double)db.x / bend; wy = (double)db.y / bend;
+                } else {
+                    const double r = NR ? rcp_newton(bmid - cpv * fxa) : __drcp_rn(bmid - cpv * fxa);
+                    cpv = fxa * r;
+                    vx = ((double)dt.x - vx * fxa) * r;
+                    vy = ((double)dt.y - vy * fxa) * r;
+                    if (jj < Bc) {
+                        wx = ((double)db.x - wx * fxa) * r;
+                        wy = ((double)db.y - wy * fxa) * r;
+                    }
+                }
+            }
+            cpl[q] = cpv; px[q] = vx; py[q] = vy; qx[q] = wx; qy[q] = wy;
+        }
+        if (have && !zero) {
+#pragma unroll
+            for (int q = KC - 1; q >= 0; --q) {
+                const int jj = jc + q;
+                if (jj < H) {
+                    if (jj < m) { xtx = px[q] - cpl[q] * xtx; xty = py[q] - cpl[q] * xty; }
+                    st_l2(&base[(long)jj * ls + tid], mk<R>((R)xtx, (R)xty), pk);
+                    if (jj <= jb) {
+                        if (jj < jb) { xbx = qx[q] - cpl[q] * xbx; xby = qy[q] - cpl[q] * xby; }
+                        st_l2(&base[(long)(nz - 1 - jj) * ls + tid], mk<R>((R)xbx, (R)xby), pk);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        refill(HP + t * KC);
+    }
+    if (t4_abort && tid == 0) {
+        // drain: every step issued completes (or its bounded wait runs out)
+        // before the block's shared memory is released
+        for (int st = max(0, issued - D); st < issued; ++st)
+            if (!mbar_try(&bar[st % D], (unsigned)(st / D) & 1u)) mbar_wait(&bar[st % D], (unsigned)(st / D) & 1u);
     }
 }
 
@@ -824,6 +1073,7 @@ template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_fwd(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pfield = pol_field(a.l2hint), pkeep = pol_keep(a.l2hint);
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
@@ -851,7 +1101,7 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
             const int t = t0 + q * blockDim.x;
             if (t < total) {
                 const int rr = (int)fdiv(t, a.fd_n2), m = t - rr * n2;
-                d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + rr, m);
+                d[q] = plane_source_pair(a, au, av, aw, asrc, k, jb + rr, m, pfield);
             }
         }
 #pragma unroll
@@ -869,7 +1119,8 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
         const int kx = (int)fdiv(t, a.fd_tj), rr = t - kx * tj;
         const int k1 = (kx == n2) ? 0 : kx;
         const int k2 = (kx == 0) ? 0 : n2 - kx;
-        spec[(long)kx * ny + jb + rr] = r2c_unpack<R>(buf[tx.pos[k1] * ld + rr], buf[tx.pos[k2] * ld + rr], twx[kx]);
+        st_l2(&spec[(long)kx * ny + jb + rr], r2c_unpack<R>(buf[tx.pos[k1] * ld + rr], buf[tx.pos[k2] * ld + rr], twx[kx]),
+              pkeep);
     }
 }
 
@@ -1005,6 +1256,7 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_
                                                                                   double scale) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pkeep = pol_keep(a.l2hint);
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
@@ -1023,7 +1275,7 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * blockDim.x;
-            if (t < total) v[q] = spec[t];
+            if (t < total) v[q] = ld_l2(&spec[t], pkeep);
         }
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
@@ -1038,7 +1290,7 @@ __global__ void __launch_bounds__(kPlaneThreads, lines_min_blocks<R, MAXR>()) k_
     const R sc = (R)scale;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int line = (int)fdiv(t, a.fd_ny), q = t - line * ny;   // q: position in shared memory
-        spec[(long)line * ny + ty.ipos[q]] = cscale(buf[q * ld + line], sc);
+        st_l2(&spec[(long)line * ny + ty.ipos[q]], cscale(buf[q * ld + line], sc), pkeep);
     }
 }
 
@@ -1069,6 +1321,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs
                                                                  double scale) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pkeep = pol_keep(a.l2hint);
     using T = cpx<R>;
     using Y = YReg<N1, N2>;
     static_assert(N1 >= N2 && N1 % N2 == 0, "split");
@@ -1082,7 +1335,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs
     const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.py.tw : (const void*)a.py.twf);
     T v[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[n1] = valid ? line[N2 * n1 + tl] : mk<R>((R)0, (R)0);
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = valid ? ld_l2(&line[N2 * n1 + tl], pkeep) : mk<R>((R)0, (R)0);
     small_dft<N1>(v, sign);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) {
@@ -1103,7 +1356,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs
         small_dft<N2>(u, sign);
         if (valid) {
 #pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) line[k1 + N1 * k2] = cscale(u[k2], sc);
+            for (int k2 = 0; k2 < N2; ++k2) st_l2(&line[k1 + N1 * k2], cscale(u[k2], sc), pkeep);
         }
     }
 }
@@ -1134,8 +1387,15 @@ struct RowReg {
     static constexpr int N = N1 * N2;
     static constexpr int TJ = kRowsRegTJ;
     static constexpr int NT = TJ * N2;                    // threads per block
-    static constexpr int LS = N1 * (N2 + 1) + 1;          // transpose tile stride of a row
-    static constexpr int LD = TJ + 1;                     // block tile [m][row] pitch
+    // Tile pitches chosen against shared-memory bank conflicts (8-byte
+    // complex FP32 elements take two 4-byte banks; a half-warp's 16 lanes
+    // are served together).  With N2 = 8 a half-warp spans two rows, so the
+    // rows' transpose tiles start 16 banks apart (LS = 8 mod 16 elements);
+    // in the block tile [m][row] the lanes of a row step through m, so its
+    // pitch is TJ + 2 (4 banks per step of m, the two rows 2 banks apart).
+    static constexpr int LS0 = N1 * (N2 + 1);
+    static constexpr int LS = N2 == 8 ? LS0 + (24 - LS0 % 16) % 16 : LS0 + 1;   // transpose tile stride of a row
+    static constexpr int LD = TJ + 2;                     // block tile [m][row] pitch
     static constexpr size_t T1 = (size_t)TJ * LS, T2 = (size_t)N * LD;
     static constexpr size_t elems = T1 > T2 ? T1 : T2;
 };
@@ -1144,6 +1404,7 @@ template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long pfield = pol_field(a.l2hint), pkeep = pol_keep(a.l2hint);
     using T = cpx<R>;
     using G = RowReg<N1, N2>;
     constexpr int N = G::N, TJ = G::TJ;
@@ -1169,7 +1430,7 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * G::NT;
-            d[q] = plane_source_pair(a, a.u + ioff, a.v + ioff, a.w + ioff, asrc, k, jb + t / N, t % N);
+            d[q] = plane_source_pair(a, a.u + ioff, a.v + ioff, a.w + ioff, asrc, k, jb + t / N, t % N, pfield);
         }
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
@@ -1212,7 +1473,8 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
         const int k1 = (kx == N) ? 0 : kx;
         const int k2 = (kx == 0) ? 0 : N - kx;
         const double2 w = __ldg(a.twx + kx);
-        spec[(long)kx * ny + rr] = r2c_unpack<R>(tb[k1 * G::LD + rr], tb[k2 * G::LD + rr], mk<R>((R)w.x, (R)w.y));
+        st_l2(&spec[(long)kx * ny + rr], r2c_unpack<R>(tb[k1 * G::LD + rr], tb[k2 * G::LD + rr], mk<R>((R)w.x, (R)w.y)),
+              pkeep);
     }
 }
 
@@ -1220,6 +1482,7 @@ template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long plast = pol_last(a.l2hint);
     using T = cpx<R>;
     using G = RowReg<N1, N2>;
     constexpr int N = G::N, TJ = G::TJ;
@@ -1244,8 +1507,8 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * G::NT;
             const int kk = t / TJ, rr = t - kk * TJ;
-            xk[q] = spec[(long)kk * ny + rr];
-            xc[q] = spec[(long)(N - kk) * ny + rr];
+            xk[q] = ld_l2(&spec[(long)kk * ny + rr], plast);
+            xc[q] = ld_l2(&spec[(long)(N - kk) * ny + rr], plast);
         }
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
@@ -1298,6 +1561,7 @@ template <typename R, int MAXR>
 __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_rows_inv(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
+    const unsigned long long plast = pol_last(a.l2hint);
     using T = cpx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
@@ -1324,8 +1588,8 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
             const int t = t0 + q * blockDim.x;
             if (t < total) {
                 const int kk = (int)fdiv(t, a.fd_tj), rr = t - kk * tj;
-                xk[q] = spec[(long)kk * ny + jb + rr];
-                xc[q] = spec[(long)(n2 - kk) * ny + jb + rr];
+                xk[q] = ld_l2(&spec[(long)kk * ny + jb + rr], plast);
+                xc[q] = ld_l2(&spec[(long)(n2 - kk) * ny + jb + rr], plast);
             }
         }
 #pragma unroll
@@ -1484,9 +1748,18 @@ static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) 
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
+int l2hint_mode() {
+    static const int m = [] {
+        const char* e = std::getenv("PS3D_L2HINT");
+        return e ? std::atoi(e) : 1;
+    }();
+    return m;
+}
+
 template <typename R>
 static cudaError_t launch_split_t(const PlaneArgs& a0, bool fwd, cudaStream_t s) {
     PlaneArgs a = a0;
+    a.l2hint = l2hint_mode();
     a.fd_n2 = make_fastdiv(a.nx / 2);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_tj = make_fastdiv(a.tj);
@@ -1535,8 +1808,11 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
+    if ((e = max_dynamic_smem(k_thomas4<R, false>))) return e;
+    if ((e = max_dynamic_smem(k_thomas4<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas3<R, 4>))) return e;
-    if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R, false>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
     if ((e = setup_m<R, 16>())) return e;
@@ -1567,7 +1843,9 @@ static cudaError_t launch_plane_m(const PlaneArgs& a, cudaStream_t s) {
     return cudaLaunchKernelEx(&cfg, k_plane_inv<R, MAXR>, a);
 }
 template <typename R, bool FWD>
-static cudaError_t launch_plane_t(const PlaneArgs& a, cudaStream_t s) {
+static cudaError_t launch_plane_t(const PlaneArgs& a0, cudaStream_t s) {
+    PlaneArgs a = a0;
+    a.l2hint = l2hint_mode();
     if (std::max(maxr_x(a), maxr_y(a)) >= 16) return launch_plane_m<R, FWD, 16>(a, s);
     return launch_plane_m<R, FWD, 8>(a, s);
 }
@@ -1612,16 +1890,38 @@ int thomas_threads(int nz) {
 
 cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     ColumnArgs a = a0;
+    a.l2hint = l2hint_mode();
     const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;
     a.fd_ncols = make_fastdiv((unsigned)ncols);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_nxh = make_fastdiv(a.nxh);
-    // the one-thread-per-column form where its reciprocals and checkpoints
-    // leave room for 4 blocks of 64 per SM, else the two-ended form with two
-    // threads per column where 4 blocks of 128 fit, else the one-ended form
-    // with as many threads per block as its checkpoints allow;
-    // PS3D_THOMAS_FORM=0|2|3 pins one
+    // the two-ended form with two threads per column where 4 blocks of 128
+    // fit an SM, else the one-ended form with as many threads per block as
+    // its checkpoints allow.  PS3D_THOMAS_FORM=0|2|3|4 pins one: 3 and 4 (one
+    // thread per complex column, loads from HBM or fed by bulk copies) are
+    // parity-tested forms that measured slower at 256x256x128 (52 and 66 us
+    // against 41 us)
     const char* pin = std::getenv("PS3D_THOMAS_FORM");
+    // PS3D_THOMAS_RCP=nr: the pivots' reciprocals by Newton-Raphson (rcp_newton)
+    const char* rcpv = std::getenv("PS3D_THOMAS_RCP");
+    const bool nr = rcpv && rcpv[0] == 'n';
+    {
+        // the bulk-copy-fed form: every copied row starts and ends on a
+        // 16-byte boundary
+        const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
+        const size_t sm4 = fp32 ? t4_layout<float>(a.nz).total : t4_layout<double>(a.nz).total;
+        const bool al = (ncols * es) % 16 == 0 && (a.sM * es) % 16 == 0 && (reinterpret_cast<uintptr_t>(a.spec) % 16) == 0;
+        if (al && sm4 <= 227 * 1024 - 64 && pin && pin[0] == '4') {
+            const long bpi = (ncols + kT4Cols - 1) / kT4Cols;
+            const dim3 g((unsigned)(bpi * std::max(1, a.batch))), b(kT4Cols);
+            if (nr) {
+                if (fp32) return launch_pdl(k_thomas4<float, true>, g, b, sm4, s, a);
+                return launch_pdl(k_thomas4<double, true>, g, b, sm4, s, a);
+            }
+            if (fp32) return launch_pdl(k_thomas4<float, false>, g, b, sm4, s, a);
+            return launch_pdl(k_thomas4<double, false>, g, b, sm4, s, a);
+        }
+    }
     {
         // 64 or 32 threads per block, whichever keeps more columns resident
         // (the shared memory per column is fixed)
@@ -1632,7 +1932,7 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
             const int res = std::min(32, (int)((228 * 1024) / (sm + 1024))) * nt;
             if (res > best) { best = res; nt3 = nt; }
         }
-        if (nt3 && ((!pin && best >= 128) || (pin && pin[0] == '3'))) {
+        if (nt3 && pin && pin[0] == '3') {
             const size_t sm3 = thomas3_smem<4>(a.nz, nt3);
             const long nthreads = ncols * std::max(1, a.batch);
             const dim3 g((unsigned)((nthreads + nt3 - 1) / nt3)), b(nt3);
@@ -1645,8 +1945,12 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
         const long nthreads = 2 * ncols * std::max(1, a.batch);
         const dim3 g((unsigned)((nthreads + kThomasThreads - 1) / kThomasThreads)), b(kThomasThreads);
         const size_t sm2 = thomas2_smem(a.nz, kThomasThreads);
-        if (fp32) return launch_pdl(k_thomas2<float>, g, b, sm2, s, a);
-        return launch_pdl(k_thomas2<double>, g, b, sm2, s, a);
+        if (nr) {
+            if (fp32) return launch_pdl(k_thomas2<float, true>, g, b, sm2, s, a);
+            return launch_pdl(k_thomas2<double, true>, g, b, sm2, s, a);
+        }
+        if (fp32) return launch_pdl(k_thomas2<float, false>, g, b, sm2, s, a);
+        return launch_pdl(k_thomas2<double, false>, g, b, sm2, s, a);
     }
     const int nt = thomas_threads(a.nz);
     if (nt == 0 || ncols < 1) return cudaErrorInvalidValue;

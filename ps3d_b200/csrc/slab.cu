@@ -157,6 +157,7 @@ int slab_vsolve(ps3d_slab* s) {
     a.fxa = 1.0 / (c.P.dz * c.P.dz) / c.P.dsqr;
     a.dz2dsqr = c.P.dz * c.P.dz * c.P.dsqr;
     a.col0 = s->cbeg[s->rank]; a.ncl = s->ccnt[s->rank];
+    a.err = c.kerr_d;
     CK(ps3d::launch_thomas(a, s->mixed, c.stream));
     return PS3D_OK;
 }

@@ -47,6 +47,32 @@ def test_ensemble_members_match_single_runs(precision, impl, monkeypatch):
     ens.close()
 
 
+@pytest.mark.parametrize("precision,tol", [(abi.PS3D_FP64, 1e-11), (abi.PS3D_MIXED, 1e-5)])
+def test_ensemble_members_match_oracle(precision, tol):
+    """Every member of an ensemble of two sizes, stepped in batched launches
+    replayed as CUDA graphs, against the CPU oracle run on that member alone
+    (FP64 at the parity tolerance of many steps, mixed at 1e-5)."""
+    from oracle.binding import Oracle
+    sizes = [(32, 32, 16), (64, 32, 16), (32, 32, 16)]
+    members = [cf.eddy_params(*s, precision=precision) for s in sizes]
+    amps = [0.08, 0.15, 0.2]
+    fields = [_member_fields(p, a, seed=10 + i) for i, (p, a) in enumerate(zip(members, amps))]
+    ens = Ensemble(members)
+    for i, f in enumerate(fields):
+        ens.upload(i, f["u"], f["v"], f["w"], f["b"])
+    nsteps = 20
+    ens.integrate(nsteps)
+    for i, (p, f) in enumerate(zip(members, fields)):
+        o = Oracle(cf.eddy_params(*sizes[i]))
+        for n in ("u", "v", "w", "b"):
+            o.field(n)[...] = f[n]
+        o.integrate(nsteps)
+        got = ens.download(i)
+        for n in ("u", "v", "w", "b", "p"):
+            assert rel(got[n], o.field(n)) < tol, (i, n, rel(got[n], o.field(n)))
+    ens.close()
+
+
 def test_graph_replay_matches_eager():
     """ps3d_integrate replays 3-step CUDA graphs; the result equals stepping
     one call at a time."""
