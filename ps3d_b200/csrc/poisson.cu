@@ -302,15 +302,17 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_pla
 // shared memory; the backward sweep re-reads a chunk's right-hand side,
 // recomputes its pivots and d' from those two values with the same
 // operations (so the same values), substitutes back and overwrites the
-// chunk with x.  The pivots are formed from ksqr on the fly: no factor
-// table and no d' array in HBM.
+// chunk with x.  The pivots are formed from ksqr on the fly (rcp_newton):
+// no factor table and no d' array in HBM.
 // ---------------------------------------------------------------------------
 // The FP64 reciprocal of a pivot by Newton-Raphson from the hardware
-// approximation (PTX rcp.approx.ftz.f64): two iterations y += y (1 - x y)
-// take its ~2^-20 relative error below 2^-80, and a third, with the
-// residual 1 - x y formed exactly by an FMA, rounds the result correctly
-// (Markstein, "Computation of elementary functions on the IBM RISC
-// System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  The pivots are
+// approximation (PTX rcp.approx.ftz.f64): each iteration y += y (1 - x y)
+// squares the relative error, two take it far below the FP64 rounding unit,
+// and a third, with the residual 1 - x y formed exactly by an FMA, rounds
+// the result correctly (Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990); on a
+// B200 it agreed bit for bit with the correctly rounded 1.0 / x on 2^30
+// random inputs over 81 binades, in fewer instructions.  The pivots are
 // normal numbers bounded away from zero (the matrix is strictly diagonally
 // dominant), so the flush-to-zero approximation never sees a subnormal.
 __device__ __forceinline__ double rcp_newton(double x) {
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
                 cp = fxa / bk;
                 dp = d / bk;
             } else {
-                const double r = __drcp_rn(bk - cp * fxa);   // == 1.0 / x (both correctly rounded)
+                const double r = rcp_newton(bk - cp * fxa);
                 cp = fxa * r;
                 dp = (d - dp * fxa) * r;
             }
@@ -482,7 +484,7 @@ PS3D_HD size_t thomas2_smem(int nz, int threads) {
     return (size_t)((h + kThomasChunk - 1) / kThomasChunk + 1) * threads * (sizeof(double2) + sizeof(double));
 }
 
-template <typename R, bool NR>
+template <typename R>
 __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
@@ -549,7 +551,7 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
             dp = dt / bend;
             dq = db / bend;
         } else {
-            const double r = NR ? rcp_newton(bmid - cp * fxa) : __drcp_rn(bmid - cp * fxa);
+            const double r = rcp_newton(bmid - cp * fxa);
             cp = fxa * r;
             dp = (dt - dp * fxa) * r;
             if (jj < Bc) dq = (db - dq * fxa) * r;
@@ -621,382 +623,6 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
                 }
             }
         }
-    }
-}
-
-// The two-ended solve with one thread per complex column: a pivot's
-// reciprocal serves both parts, and the ceil(nz/2) reciprocals are kept in
-// shared memory for the back substitution instead of being formed again, so
-// a column costs about a quarter of the instructions of two threads that
-// each form every pivot twice (the bound of the forms above, which issue
-// ~5,000 instructions per thread at ~14 warps per SM).  d' and d'' (the
-// two ends) are still never stored: their values before every KC-level
-// chunk are kept in shared memory and each chunk's are recomputed, from
-// the untouched right-hand side and the stored reciprocals, on the way back.
-template <int KC>
-PS3D_HD size_t thomas3_smem(int nz, int threads) {
-    const int h = (nz + 1) / 2;
-    return (size_t)h * threads * sizeof(double) + (size_t)((h + KC - 1) / KC) * threads * 2 * sizeof(double2);
-}
-
-template <typename R, int KC>
-__global__ void __launch_bounds__(64) k_thomas3(const ColumnArgs a) {
-    using T = cpx<R>;
-    pdl_trigger();
-    pdl_wait();   // inputs written by the preceding kernels
-    const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
-    extern __shared__ double2 sm3[];
-    const int nz = a.nz;
-    const int H = (nz + 1) / 2;   // pivot levels: top 0 .. H-1, bottom nz-1 .. nz-Bc
-    const int Bc = nz - H;
-    const int m = H - 1, jb = Bc - 1;
-    const int nch = (H + KC - 1) / KC;
-    const int NT = blockDim.x, tid = threadIdx.x;
-    double* rs = reinterpret_cast<double*>(sm3) + tid;                          // [H][NT] reciprocal pivots
-    double2* ck = reinterpret_cast<double2*>(reinterpret_cast<double*>(sm3) + (size_t)H * NT) + tid;   // [nch][2][NT]
-    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
-    const long gid = blockIdx.x * (long)NT + tid;
-    if (gid >= ncols * a.batch) return;
-    const unsigned inst = fdiv((unsigned)gid, a.fd_ncols);
-    const unsigned c = (unsigned)gid - inst * (unsigned)ncols;
-    T* col = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + c;
-    const long ls = ncols;   // level stride in complex elements
-    const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
-    const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
-    const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
-    const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
-    const double ks = a.hkx[i] + a.hky[j];
-    const double fxa = a.fxa;
-    if (!(ks > 0)) {
-        // (0,0) mode: p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
-        const double h = a.dz2dsqr;
-        double x0x = 0.0, x0y = 0.0, x1x = 0.0, x1y = 0.0, fx = 0.0, fy = 0.0;
-        for (int k = 0; k < nz; ++k) {
-            const T d = ld_l2(&col[(long)k * ls], pk);
-            const double xkx = k == 0 ? 0.0 : 2 * x1x - x0x + fx * h;
-            const double xky = k == 0 ? 0.0 : 2 * x1y - x0y + fy * h;
-            fx = (double)d.x; fy = (double)d.y;
-            x0x = x1x; x0y = x1y; x1x = xkx; x1y = xky;
-            st_l2(&col[(long)k * ls], mk<R>((R)xkx, (R)xky), pk);
-        }
-        return;
-    }
-    const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-    const double cp0 = fxa / bend;   // cp(1) = c/b(1)
-    // one pivot level jj from both ends: dp(1) = d(1)/b(1), dp = (d - dp a) r;
-    // the bottom chain the same with its own right-hand side
-    auto load = [&](int jc, T* top, T* bot) {
-#pragma unroll
-        for (int q = 0; q < KC; ++q) {
-            const int jj = jc + q;
-            if (jj < H) top[q] = ld_l2(&col[(long)jj * ls], pk);
-            if (jj < Bc) bot[q] = ld_l2(&col[(long)(nz - 1 - jj) * ls], pk);
-        }
-    };
-    double cp = 0.0, dpx = 0.0, dpy = 0.0, dqx = 0.0, dqy = 0.0;
-    double cp_jb = 0.0, dqx_jb = 0.0, dqy_jb = 0.0;
-    T nt[KC], nb[KC];
-#pragma unroll
-    for (int q = 0; q < KC; ++q) { nt[q] = mk<R>((R)0, (R)0); nb[q] = nt[q]; }
-    load(0, nt, nb);
-    for (int ch = 0; ch < nch; ++ch) {
-        const int jc = ch * KC;
-        T dt[KC], db[KC];
-#pragma unroll
-        for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
-        if (ch + 1 < nch) load(jc + KC, nt, nb);
-        ck[(2 * ch) * NT] = make_double2(dpx, dpy);   // before pivot level jc
-        ck[(2 * ch + 1) * NT] = make_double2(dqx, dqy);
-#pragma unroll
-        for (int q = 0; q < KC; ++q) {
-            const int jj = jc + q;
-            if (jj < H) {
-                if (jj == 0) {
-                    cp = cp0;
-                    dpx = (double)dt[q].x / bend; dpy = (double)dt[q].y / bend;
-                    dqx = (double)db[q].x / bend; dqy = (double)db[q].y / bend;
-                } else {
-                    const double r = __drcp_rn(bmid - cp * fxa);   // == 1.0 / x (both correctly rounded)
-                    rs[jj * NT] = r;
-                    cp = fxa * r;
-                    dpx = ((double)dt[q].x - dpx * fxa) * r;
-                    dpy = ((double)dt[q].y - dpy * fxa) * r;
-                    if (jj < Bc) {
-                        dqx = ((double)db[q].x - dqx * fxa) * r;
-                        dqy = ((double)db[q].y - dqy * fxa) * r;
-                    }
-                }
-                if (jj == jb) { cp_jb = cp; dqx_jb = dqx; dqy_jb = dqy; }
-            }
-        }
-    }
-    // the two halves meet: x(m) = (dp(m) - cp(m) dq(jb)) / (1 - cp(m) cp(jb)),
-    // x(m+1) = dq(jb) - cp(jb) x(m)
-    const double den = 1.0 - cp * cp_jb;
-    double xtx = (dpx - cp * dqx_jb) / den, xty = (dpy - cp * dqy_jb) / den;
-    double xbx = dqx_jb - cp_jb * xtx, xby = dqy_jb - cp_jb * xty;
-    load((nch - 1) * KC, nt, nb);
-    for (int ch = nch - 1; ch >= 0; --ch) {
-        const int jc = ch * KC;
-        T dt[KC], db[KC];
-#pragma unroll
-        for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
-        if (ch > 0) load(jc - KC, nt, nb);
-        double px[KC], py[KC], qx[KC], qy[KC], cpl[KC];
-        {
-            const double2 p0 = ck[(2 * ch) * NT], b0 = ck[(2 * ch + 1) * NT];
-            double vx = p0.x, vy = p0.y, wx = b0.x, wy = b0.y;
-#pragma unroll
-            for (int q = 0; q < KC; ++q) {
-                const int jj = jc + q;
-                if (jj < H) {
-                    if (jj == 0) {
-                        cpl[q] = cp0;
-                        vx = (double)dt[q].x / bend; vy = (double)dt[q].y / bend;
-                        wx = (double)db[q].x / bend; wy = (double)db[q].y / bend;
-                    } else {
-                        const double r = rs[jj * NT];
-                        cpl[q] = fxa * r;
-                        vx = ((double)dt[q].x - vx * fxa) * r;
-                        vy = ((double)dt[q].y - vy * fxa) * r;
-                        if (jj < Bc) {
-                            wx = ((double)db[q].x - wx * fxa) * r;
-                            wy = ((double)db[q].y - wy * fxa) * r;
-                        }
-                    }
-                }
-                px[q] = vx; py[q] = vy; qx[q] = wx; qy[q] = wy;
-            }
-        }
-#pragma unroll
-        for (int q = KC - 1; q >= 0; --q) {
-            const int jj = jc + q;
-            if (jj < H) {
-                if (jj < m) { xtx = px[q] - cpl[q] * xtx; xty = py[q] - cpl[q] * xty; }
-                st_l2(&col[(long)jj * ls], mk<R>((R)xtx, (R)xty), pk);
-                if (jj <= jb) {
-                    if (jj < jb) { xbx = qx[q] - cpl[q] * xbx; xby = qy[q] - cpl[q] * xby; }
-                    st_l2(&col[(long)(nz - 1 - jj) * ls], mk<R>((R)xbx, (R)xby), pk);
-                }
-            }
-        }
-    }
-}
-
-// The two-ended solve fed by bulk copies: one thread per complex column,
-// kT4Cols columns per block.  Pivot step j needs level j (from the top) and
-// level nz-1-j (from the bottom) of the block's columns, two contiguous rows
-// of the spectral array.  One thread issues both rows of a step as bulk
-// copies (TMA engine, no tensor map, no multicast) into a ring of D steps in
-// shared memory, completing on the step's mbarrier, so the copies of the
-// next D steps are in flight while the serial FP64 recurrence runs: the
-// recurrence never waits on a load, and a block holds no registers for the
-// loads in flight.  The forward sweep keeps (c', d', d'') before every
-// kT4KC-step chunk in shared memory; the backward sweep streams the steps
-// again, chunk by chunk from the middle outward (the steps of a chunk in
-// ascending order), forms the chunk's pivots and d' again from its checkpoint
-// with the same operations (so the same values), substitutes back and
-// stores x.  The (0,0) column runs its recurrence over the top half in the
-// forward sweep, parks the bottom half's right-hand side in shared memory and
-// finishes from there.  Waits are bounded: a wait that runs out sets the
-// error word and the block stops issuing, drains its copies and returns.
-// ---------------------------------------------------------------------------
-constexpr int kT4Cols = 64;   // columns (threads) per block
-constexpr int kT4KC = 8;      // pivot steps per checkpoint chunk
-template <typename R> constexpr int t4_depth() { return sizeof(R) == 4 ? 32 : 16; }   // ring steps
-
-struct T4Layout {
-    size_t ck, stash, bars, total;
-};
-template <typename R>
-PS3D_HD T4Layout t4_layout(int nz) {
-    const int H = (nz + 1) / 2, nch = (H + kT4KC - 1) / kT4KC;
-    T4Layout L;
-    L.ck = (size_t)t4_depth<R>() * 2 * kT4Cols * sizeof(cpx<R>);
-    L.stash = L.ck + (size_t)nch * 5 * kT4Cols * sizeof(double);
-    L.bars = L.stash + align16((size_t)(nz - H) * sizeof(cpx<R>));
-    L.total = L.bars + (size_t)t4_depth<R>() * sizeof(unsigned long long);
-    return L;
-}
-
-template <typename R, bool NR>
-__global__ void __launch_bounds__(kT4Cols) k_thomas4(const ColumnArgs a) {
-    using T = cpx<R>;
-    constexpr int D = t4_depth<R>(), KC = kT4KC, NT = kT4Cols;
-    static_assert(D % KC == 0, "ring of whole chunks");
-    pdl_trigger();
-    pdl_wait();   // inputs written by the preceding kernels
-    extern __shared__ __align__(16) unsigned char t4_raw[];
-    __shared__ int t4_abort;
-    const int nz = a.nz, H = (nz + 1) / 2, Bc = nz - H;
-    const int m = H - 1, jb = Bc - 1;
-    const int nch = (H + KC - 1) / KC, HP = nch * KC, nsteps = 2 * HP;
-    const T4Layout L = t4_layout<R>(nz);
-    T* ring = reinterpret_cast<T*>(t4_raw);                        // [D][top, bottom][NT]
-    double* ck = reinterpret_cast<double*>(t4_raw + L.ck);         // [nch][5][NT]
-    T* stash = reinterpret_cast<T*>(t4_raw + L.stash);             // (0,0) column, levels H..nz-1
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(t4_raw + L.bars);
-    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
-    const int bpi = (int)((ncols + NT - 1) / NT);             // blocks per instance
-    const int inst = blockIdx.x / bpi;
-    const long c0 = (long)(blockIdx.x - inst * bpi) * NT;
-    const int ncb = (int)min((long)NT, ncols - c0);
-    const int tid = threadIdx.x;
-    const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
-    T* base = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + c0;
-    const long ls = ncols;   // level stride in complex elements
-    const unsigned bytes = (unsigned)(ncb * sizeof(T));
-    // step s: s < HP the forward sweep's pivot step s; then the backward
-    // sweep, chunks from the last, the steps of a chunk ascending
-    auto step_j = [&](int st) { return st < HP ? st : (nch - 1 - (st - HP) / KC) * KC + (st - HP) % KC; };
-    // (a slot is refilled after a block barrier that follows every thread's
-    // reads of it; the copy's write needs no proxy fence after reads)
-    auto issue = [&](int st) {   // thread 0
-        const int slot = st % D, j = step_j(st);
-        mbar_expect(&bar[slot], (j < H ? bytes : 0u) + (j < Bc ? bytes : 0u));
-        if (j < H) bulk_copy_g2s(ring + (size_t)(2 * slot) * NT, base + (long)j * ls, bytes, &bar[slot]);
-        if (j < Bc) bulk_copy_g2s(ring + (size_t)(2 * slot + 1) * NT, base + (long)(nz - 1 - j) * ls, bytes, &bar[slot]);
-    };
-    if (tid == 0) {
-        for (int i = 0; i < D; ++i) mbar_init(&bar[i], 1);
-        t4_abort = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        fence_proxy_async();
-        for (int st = 0; st < D && st < nsteps; ++st) issue(st);
-    }
-    __syncthreads();
-    int issued = min(D, nsteps);   // thread 0's count of steps issued
-    // a chunk's D-ahead refill, after every thread has read the chunk's slots
-    auto refill = [&](int first) {
-        if (tid == 0 && !t4_abort)
-            for (int st = first + D; st < first + D + KC && st < nsteps; ++st) { issue(st); issued = st + 1; }
-    };
-    auto wait_step = [&](int st) {
-        if (!mbar_wait(&bar[st % D], (unsigned)(st / D) & 1u)) {
-            t4_abort = 1;
-            if (a.err) *(volatile unsigned*)a.err = 1u;
-        }
-    };
-
-    const bool have = tid < ncb;
-    const unsigned cg = (unsigned)(c0 + tid) + (unsigned)a.col0;   // global column: its wavenumbers
-    double ks = 1.0;
-    if (have) {
-        const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
-        const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
-        const int j = a.layout ? (int)(cg - q0 * (unsigned)a.ny) : (int)q0;
-        ks = a.hkx[i] + a.hky[j];
-    }
-    const bool zero = have && !(ks > 0);   // the (0,0) column
-    const double fxa = a.fxa, h0 = a.dz2dsqr;
-    const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-    const double cp0 = fxa / bend;   // cp(1) = c/b(1)
-    double cp = 0.0, dpx = 0.0, dpy = 0.0, dqx = 0.0, dqy = 0.0;
-    double cp_jb = 0.0, dqx_jb = 0.0, dqy_jb = 0.0;
-    // (0,0): p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
-    double z0x = 0.0, z0y = 0.0, z1x = 0.0, z1y = 0.0, zfx = 0.0, zfy = 0.0;
-    auto zstep = [&](int k, T d) {
-        const double xkx = k == 0 ? 0.0 : 2 * z1x - z0x + zfx * h0;
-        const double xky = k == 0 ? 0.0 : 2 * z1y - z0y + zfy * h0;
-        zfx = (double)d.x; zfy = (double)d.y;
-        z0x = z1x; z0y = z1y; z1x = xkx; z1y = xky;
-        st_l2(&base[(long)k * ls + tid], mk<R>((R)xkx, (R)xky), pk);
-    };
-    // ---- forward sweep
-    for (int ch = 0; ch < nch && !t4_abort; ++ch) {
-        double* c = ck + (size_t)ch * 5 * NT + tid;
-        c[0] = cp; c[NT] = dpx; c[2 * NT] = dpy; c[3 * NT] = dqx; c[4 * NT] = dqy;
-        for (int q = 0; q < KC; ++q) {
-            const int jj = ch * KC + q, slot = jj % D;
-            wait_step(jj);
-            if (!have || jj >= H) continue;
-            const T dt = ring[(size_t)(2 * slot) * NT + tid];
-            const T db = jj < Bc ? ring[(size_t)(2 * slot + 1) * NT + tid] : mk<R>((R)0, (R)0);
-            if (zero) {
-                zstep(jj, dt);
-                if (jj < Bc) stash[nz - 1 - jj - H] = db;
-                continue;
-            }
-            if (jj == 0) {
-                cp = cp0;
-                dpx = (double)dt.x / bend; dpy = (double)dt.y / bend;
-                dqx = (double)db.x / bend; dqy = (double)db.y / bend;
-            } else {
-                const double r = NR ? rcp_newton(bmid - cp * fxa) : __drcp_rn(bmid - cp * fxa);
-                cp = fxa * r;
-                dpx = ((double)dt.x - dpx * fxa) * r;
-                dpy = ((double)dt.y - dpy * fxa) * r;
-                if (jj < Bc) {
-                    dqx = ((double)db.x - dqx * fxa) * r;
-                    dqy = ((double)db.y - dqy * fxa) * r;
-                }
-            }
-            if (jj == jb) { cp_jb = cp; dqx_jb = dqx; dqy_jb = dqy; }
-        }
-        __syncthreads();
-        refill(ch * KC);
-    }
-    if (zero && !t4_abort)
-        for (int k = H; k < nz; ++k) zstep(k, stash[k - H]);
-    // ---- the halves meet: x(m) = (dp(m) - cp(m) dq(jb)) / (1 - cp(m) cp(jb)), x(m+1) = dq(jb) - cp(jb) x(m)
-    const double den = 1.0 - cp * cp_jb;
-    double xtx = 0.0, xty = 0.0, xbx = 0.0, xby = 0.0;
-    if (have && !zero) {
-        xtx = (dpx - cp * dqx_jb) / den; xty = (dpy - cp * dqy_jb) / den;
-        xbx = dqx_jb - cp_jb * xtx; xby = dqy_jb - cp_jb * xty;
-    }
-    // ---- backward sweep
-    for (int t = 0; t < nch && !t4_abort; ++t) {
-        const int ch = nch - 1 - t, jc = ch * KC;
-        const double* c = ck + (size_t)ch * 5 * NT + tid;
-        double cpv = c[0], vx = c[NT], vy = c[2 * NT], wx = c[3 * NT], wy = c[4 * NT];
-        double px[KC], py[KC], qx[KC], qy[KC], cpl[KC];
-#pragma unroll
-        for (int q = 0; q < KC; ++q) {
-            const int st = HP + t * KC + q, slot = st % D, jj = jc + q;
-            wait_step(st);
-            if (have && !zero && jj < H) {
-                const T dt = ring[(size_t)(2 * slot) * NT + tid];
-                const T db = jj < Bc ? ring[(size_t)(2 * slot + 1) * NT + tid] : mk<R>((R)0, (R)0);
-                if (jj == 0) {
-                    cpv = cp0;
-                    vx = (double)dt.x / bend; vy = (double)dt.y / bend;
-                    wx = (double)db.x / bend; wy = (double)db.y / bend;
-                } else {
-                    const double r = NR ? rcp_newton(bmid - cpv * fxa) : __drcp_rn(bmid - cpv * fxa);
-                    cpv = fxa * r;
-                    vx = ((double)dt.x - vx * fxa) * r;
-                    vy = ((double)dt.y - vy * fxa) * r;
-                    if (jj < Bc) {
-                        wx = ((double)db.x - wx * fxa) * r;
-                        wy = ((double)db.y - wy * fxa) * r;
-                    }
-                }
-            }
-            cpl[q] = cpv; px[q] = vx; py[q] = vy; qx[q] = wx; qy[q] = wy;
-        }
-        if (have && !zero) {
-#pragma unroll
-            for (int q = KC - 1; q >= 0; --q) {
-                const int jj = jc + q;
-                if (jj < H) {
-                    if (jj < m) { xtx = px[q] - cpl[q] * xtx; xty = py[q] - cpl[q] * xty; }
-                    st_l2(&base[(long)jj * ls + tid], mk<R>((R)xtx, (R)xty), pk);
-                    if (jj <= jb) {
-                        if (jj < jb) { xbx = qx[q] - cpl[q] * xbx; xby = qy[q] - cpl[q] * xby; }
-                        st_l2(&base[(long)(nz - 1 - jj) * ls + tid], mk<R>((R)xbx, (R)xby), pk);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        refill(HP + t * KC);
-    }
-    if (t4_abort && tid == 0) {
-        // drain: every step issued completes (or its bounded wait runs out)
-        // before the block's shared memory is released
-        for (int st = max(0, issued - D); st < issued; ++st)
-            if (!mbar_try(&bar[st % D], (unsigned)(st / D) & 1u)) mbar_wait(&bar[st % D], (unsigned)(st / D) & 1u);
     }
 }
 
@@ -1808,11 +1434,7 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
-    if ((e = max_dynamic_smem(k_thomas4<R, false>))) return e;
-    if ((e = max_dynamic_smem(k_thomas4<R, true>))) return e;
-    if ((e = max_dynamic_smem(k_thomas3<R, 4>))) return e;
-    if ((e = max_dynamic_smem(k_thomas2<R, false>))) return e;
-    if ((e = max_dynamic_smem(k_thomas2<R, true>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
     if ((e = setup_m<R, 16>())) return e;
@@ -1897,60 +1519,15 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     a.fd_nxh = make_fastdiv(a.nxh);
     // the two-ended form with two threads per column where 4 blocks of 128
     // fit an SM, else the one-ended form with as many threads per block as
-    // its checkpoints allow.  PS3D_THOMAS_FORM=0|2|3|4 pins one: 3 and 4 (one
-    // thread per complex column, loads from HBM or fed by bulk copies) are
-    // parity-tested forms that measured slower at 256x256x128 (52 and 66 us
-    // against 41 us)
+    // its checkpoints allow; PS3D_THOMAS_FORM=0|2 pins one
     const char* pin = std::getenv("PS3D_THOMAS_FORM");
-    // PS3D_THOMAS_RCP=nr: the pivots' reciprocals by Newton-Raphson (rcp_newton)
-    const char* rcpv = std::getenv("PS3D_THOMAS_RCP");
-    const bool nr = rcpv && rcpv[0] == 'n';
-    {
-        // the bulk-copy-fed form: every copied row starts and ends on a
-        // 16-byte boundary
-        const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
-        const size_t sm4 = fp32 ? t4_layout<float>(a.nz).total : t4_layout<double>(a.nz).total;
-        const bool al = (ncols * es) % 16 == 0 && (a.sM * es) % 16 == 0 && (reinterpret_cast<uintptr_t>(a.spec) % 16) == 0;
-        if (al && sm4 <= 227 * 1024 - 64 && pin && pin[0] == '4') {
-            const long bpi = (ncols + kT4Cols - 1) / kT4Cols;
-            const dim3 g((unsigned)(bpi * std::max(1, a.batch))), b(kT4Cols);
-            if (nr) {
-                if (fp32) return launch_pdl(k_thomas4<float, true>, g, b, sm4, s, a);
-                return launch_pdl(k_thomas4<double, true>, g, b, sm4, s, a);
-            }
-            if (fp32) return launch_pdl(k_thomas4<float, false>, g, b, sm4, s, a);
-            return launch_pdl(k_thomas4<double, false>, g, b, sm4, s, a);
-        }
-    }
-    {
-        // 64 or 32 threads per block, whichever keeps more columns resident
-        // (the shared memory per column is fixed)
-        int nt3 = 0, best = 0;
-        for (int nt : {64, 32}) {
-            const size_t sm = thomas3_smem<4>(a.nz, nt);
-            if (sm > 227 * 1024 - 64) continue;
-            const int res = std::min(32, (int)((228 * 1024) / (sm + 1024))) * nt;
-            if (res > best) { best = res; nt3 = nt; }
-        }
-        if (nt3 && pin && pin[0] == '3') {
-            const size_t sm3 = thomas3_smem<4>(a.nz, nt3);
-            const long nthreads = ncols * std::max(1, a.batch);
-            const dim3 g((unsigned)((nthreads + nt3 - 1) / nt3)), b(nt3);
-            if (fp32) return launch_pdl(k_thomas3<float, 4>, g, b, sm3, s, a);
-            return launch_pdl(k_thomas3<double, 4>, g, b, sm3, s, a);
-        }
-    }
     if ((!pin && thomas2_smem(a.nz, kThomasThreads) <= 56 * 1024) ||
         (pin && pin[0] == '2' && thomas2_smem(a.nz, kThomasThreads) <= 227 * 1024 - 64)) {
         const long nthreads = 2 * ncols * std::max(1, a.batch);
         const dim3 g((unsigned)((nthreads + kThomasThreads - 1) / kThomasThreads)), b(kThomasThreads);
         const size_t sm2 = thomas2_smem(a.nz, kThomasThreads);
-        if (nr) {
-            if (fp32) return launch_pdl(k_thomas2<float, true>, g, b, sm2, s, a);
-            return launch_pdl(k_thomas2<double, true>, g, b, sm2, s, a);
-        }
-        if (fp32) return launch_pdl(k_thomas2<float, false>, g, b, sm2, s, a);
-        return launch_pdl(k_thomas2<double, false>, g, b, sm2, s, a);
+        if (fp32) return launch_pdl(k_thomas2<float>, g, b, sm2, s, a);
+        return launch_pdl(k_thomas2<double>, g, b, sm2, s, a);
     }
     const int nt = thomas_threads(a.nz);
     if (nt == 0 || ncols < 1) return cudaErrorInvalidValue;

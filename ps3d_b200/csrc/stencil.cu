@@ -35,6 +35,183 @@ struct StepSmem {
     double hw[2][kTX * BY];
 };
 
+// The tendency, friction, forcing and Adams-Bashforth update of the point
+// (i, j, k) of instance `ioff`: F(f, di, dj, dk) reads field f (0 u, 1 v,
+// 2 w, 3 b, 4 U_back, 5 B_back) of the corrected state at the offsets,
+// Hh(f, l) the point's stored tendency of field f at history level l
+// (0: taum1, 1: taum2).  Shared by the step kernels, which differ only in
+// how they stage the state.
+template <typename TT, bool HARM, bool WM, bool BG, class FV, class HV>
+__device__ __forceinline__ void step_point(const StepArgs& a, const FV& F, const HV& Hh, int i, int j, int k,
+                                           long ioff, bool h1, bool h2) {
+    using TW = double;   // stored w tendencies stay FP64 in both paths
+    const int nx = a.nx, ny = a.ny;
+    const long plane = (long)nx * ny;
+    const int kofs = a.kofs, nzg = a.nzg ? a.nzg : a.nz;
+    const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
+    const bool rigid = a.rigid;
+#define U(di, dj, dk) F(0, di, dj, dk)
+#define V(di, dj, dk) F(1, di, dj, dk)
+#define W(di, dj, dk) F(2, di, dj, dk)
+#define B(di, dj, dk) F(3, di, dj, dk)
+#define UB(di, dj, dk) F(4, di, dj, dk)
+#define BB(di, dj, dk) F(5, di, dj, dk)
+    const int kg = k + kofs;                     // global level
+    const bool top = rigid && (kg == nzg - 1);   // flux_top(nz) = 0
+    const bool bot = rigid && (kg == 0);         // flux_top(0)  = 0
+    const long g0 = (long)k * plane + (long)j * nx + i;   // point within the instance
+    const long g = g0 + ioff;                              // point within the batch
+    double db_, du_, dv_, dw_;
+    // ---- buoyancy advection + N^2 (advection.f90:12-47, integrate.f90:21-23)
+    // The reference's 0.5 and 0.25 flux factors are powers of two: they
+    // are carried in the per-axis factors a.hd* = 0.5/d*, a.qd* = 0.25/d*
+    // (and 0.25 f0, 0.5 N0^2, set by the launcher), a multiply saved per
+    // flux.  Scaling by a power of two rounds exactly; the results move
+    // at round-off level only where the compiler now contracts a flux
+    // product into the difference that follows (FMA).
+    if (a.nonlinear) {
+        const double fe = (B(0, 0, 0) + B(1, 0, 0)) * U(0, 0, 0);
+        const double fem = (B(-1, 0, 0) + B(0, 0, 0)) * U(-1, 0, 0);
+        const double fn = (B(0, 0, 0) + B(0, 1, 0)) * V(0, 0, 0);
+        const double fnm = (B(0, -1, 0) + B(0, 0, 0)) * V(0, -1, 0);
+        const double ft = top ? 0.0 : (B(0, 0, 0) + B(0, 0, 1)) * W(0, 0, 0);
+        const double ftm = bot ? 0.0 : (B(0, 0, -1) + B(0, 0, 0)) * W(0, 0, -1);
+        db_ = -Ro * ((fe - fem) * a.hdx + (fn - fnm) * a.hdy + (ft - ftm) * a.hdz);
+        // ---- zonal momentum (advection.f90:65-100)
+        {
+            const double e = (U(0, 0, 0) + U(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+            const double em = (U(-1, 0, 0) + U(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
+            const double n = (U(0, 0, 0) + U(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+            const double nm = (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+            const double t = top ? 0.0 : (U(0, 0, 1) + U(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
+            const double tm = bot ? 0.0 : (U(0, 0, 0) + U(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
+            du_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
+        }
+        // ---- meridional momentum (advection.f90:104-140)
+        {
+            const double e = (V(0, 0, 0) + V(1, 0, 0)) * (U(0, 1, 0) + U(0, 0, 0));
+            const double em = (V(-1, 0, 0) + V(0, 0, 0)) * (U(-1, 1, 0) + U(-1, 0, 0));
+            const double n = (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 1, 0) + V(0, 0, 0));
+            const double nm = (V(0, -1, 0) + V(0, 0, 0)) * (V(0, 0, 0) + V(0, -1, 0));
+            const double t = top ? 0.0 : (V(0, 0, 1) + V(0, 0, 0)) * (W(0, 0, 0) + W(0, 1, 0));
+            const double tm = bot ? 0.0 : (V(0, 0, 0) + V(0, 0, -1)) * (W(0, 0, -1) + W(0, 1, -1));
+            dv_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
+        }
+        // ---- vertical momentum (advection.f90:145-181); rigid lid zeroes
+        //      flux_top(nz-1:nz+2) for w (:167-170)
+        {
+            const bool wtop = rigid && (kg >= nzg - 2);
+            const bool wbot = rigid && (kg == 0 || kg >= nzg - 1);
+            const double e = (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
+            const double em = (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
+            const double n = (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
+            const double nm = (W(0, -1, 0) + W(0, 0, 0)) * (V(0, -1, 0) + V(0, -1, 1));
+            const double t = wtop ? 0.0 : (W(0, 0, 1) + W(0, 0, 0)) * (W(0, 0, 0) + W(0, 0, 1));
+            const double tm = wbot ? 0.0 : (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, -1) + W(0, 0, 0));
+            dw_ = -a.dsqr * Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
+        }
+    } else {
+        db_ = du_ = dv_ = dw_ = 0.0;
+    }
+    db_ = db_ - (W(0, 0, 0) + W(0, 0, -1)) * a.hN0sq;
+    // ---- Coriolis, buoyancy force, rigid-lid mask (integrate.f90:37-54)
+    du_ = du_ + (V(0, 0, 0) + V(0, -1, 0) + V(1, 0, 0) + V(1, -1, 0)) * a.qf0;
+    dv_ = dv_ - (U(-1, 0, 0) + U(0, 0, 0) + U(-1, 1, 0) + U(0, 1, 0)) * a.qf0;
+    dw_ = dw_ + 0.5 * (B(0, 0, 0) + B(0, 0, 1));
+    if (top) dw_ = 0.0;
+    // ---- friction, in place before AB (integrate.f90:59-66)
+    double u1 = U(0, 0, 0), v1 = V(0, 0, 0), w1 = W(0, 0, 0), b1 = B(0, 0, 0);
+    if constexpr (HARM) {
+        const double dt = a.dt;
+#define HARMONIC(F, Hm, Vm, out)                                                                   \
+    {                                                                                            \
+const double e = Hm * (F(1, 0, 0) - F(0, 0, 0)) * rdx;                                   \
+const double em = Hm * (F(0, 0, 0) - F(-1, 0, 0)) * rdx;                                 \
+const double n = Hm * (F(0, 1, 0) - F(0, 0, 0)) * rdy;                                   \
+const double nm = Hm * (F(0, 0, 0) - F(0, -1, 0)) * rdy;                                 \
+const double t = top ? 0.0 : Vm * (F(0, 0, 1) - F(0, 0, 0)) * rdz;                       \
+const double tm = bot ? 0.0 : Vm * (F(0, 0, 0) - F(0, 0, -1)) * rdz;                     \
+out = F(0, 0, 0) + dt * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);              \
+    }
+        if (a.harm_uvw) {
+            HARMONIC(U, a.Ah, a.Av, u1)
+            HARMONIC(V, a.Ah, a.Av, v1)
+            HARMONIC(W, a.Ah, a.Av, w1)
+            if (top) w1 = 0.0;
+        }
+        if (a.harm_b) HARMONIC(B, a.Kh, a.Kv, b1)
+#undef HARMONIC
+    }
+    // ---- set_forcing: background-flow advection (lee_wave1.f90:245-312)
+    if constexpr (BG) {
+        {
+            const double e = 2 * 0.25 * (UB(0, 0, 0) + UB(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
+            const double em = 2 * 0.25 * (UB(-1, 0, 0) + UB(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
+            const double n = 0.25 * (UB(0, 0, 0) + UB(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
+            const double nm = 0.25 * (UB(0, -1, 0) + UB(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
+            const double t = top ? 0.0 : 0.25 * (UB(0, 0, 1) + UB(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
+            const double tm = bot ? 0.0 : 0.25 * (UB(0, 0, 0) + UB(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
+            du_ = du_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+        }
+        {
+            const double e = 0.25 * (V(0, 0, 0) + V(1, 0, 0)) * (UB(0, 1, 0) + UB(0, 0, 0));
+            const double em = 0.25 * (V(-1, 0, 0) + V(0, 0, 0)) * (UB(-1, 1, 0) + UB(-1, 0, 0));
+            dv_ = dv_ - Ro * (e - em) * rdx;
+        }
+        {
+            const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (UB(0, 0, 0) + UB(0, 0, 1));
+            const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (UB(-1, 0, 0) + UB(-1, 0, 1));
+            dw_ = dw_ - a.dsqr * Ro * (e - em) * rdx;
+        }
+        {
+            const double e = 0.5 * (B(0, 0, 0) + B(1, 0, 0)) * UB(0, 0, 0) + 0.5 * (BB(0, 0, 0) + BB(1, 0, 0)) * U(0, 0, 0);
+            const double em = 0.5 * (B(-1, 0, 0) + B(0, 0, 0)) * UB(-1, 0, 0) + 0.5 * (BB(-1, 0, 0) + BB(0, 0, 0)) * U(-1, 0, 0);
+            const double n = 0.5 * (BB(0, 0, 0) + BB(0, 1, 0)) * V(0, 0, 0);
+            const double nm = 0.5 * (BB(0, -1, 0) + BB(0, 0, 0)) * V(0, -1, 0);
+            const double t = top ? 0.0 : 0.5 * (BB(0, 0, 0) + BB(0, 0, 1)) * W(0, 0, 0);
+            const double tm = bot ? 0.0 : 0.5 * (BB(0, 0, -1) + BB(0, 0, 0)) * W(0, 0, -1);
+            db_ = db_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
+        }
+    }
+#undef U
+#undef V
+#undef W
+#undef B
+#undef UB
+#undef BB
+    // ---- set_forcing: wavemaker (config.f90:224-237)
+    if constexpr (WM) {
+        const double dt = a.dt, c = a.wm_c, s = a.wm_s;
+        if (a.wr[0] || a.wi[0]) u1 = u1 + dt * (c * (a.wr[0] ? a.wr[0][g0] : 0.0) + s * (a.wi[0] ? a.wi[0][g0] : 0.0));
+        if (a.wr[1] || a.wi[1]) v1 = v1 + dt * (c * (a.wr[1] ? a.wr[1][g0] : 0.0) + s * (a.wi[1] ? a.wi[1][g0] : 0.0));
+        if (a.wr[2] || a.wi[2]) w1 = w1 + dt * (c * (a.wr[2] ? a.wr[2][g0] : 0.0) + s * (a.wi[2] ? a.wi[2][g0] : 0.0));
+        if (a.wr[3] || a.wi[3]) b1 = b1 + dt * (c * (a.wr[3] ? a.wr[3][g0] : 0.0) + s * (a.wi[3] ? a.wi[3][g0] : 0.0));
+    }
+    // ---- store tendency of time level tau
+    ((TT*)a.t0[0])[g] = (TT)du_;
+    ((TT*)a.t0[1])[g] = (TT)dv_;
+    ((TW*)a.t0[2])[g] = (TW)dw_;
+    ((TT*)a.t0[3])[g] = (TT)db_;
+    // ---- Adams-Bashforth (integrate.f90:87-102)
+    if (a.do_ab) {
+        const double dt = a.dt, dtw = a.dtw;
+        const double c0 = a.ab0, c1 = a.ab1, c2 = a.ab2;
+        // the current tendency enters at full precision; only the
+        // stored history (FP32 in the mixed path) is rounded
+        double tu = c0 * du_, tv = c0 * dv_, tw = c0 * dw_, tb = c0 * db_;
+        if (h1) {
+            tu = tu + c1 * Hh(0, 0); tv = tv + c1 * Hh(1, 0);
+            tw = tw + c1 * Hh(2, 0); tb = tb + c1 * Hh(3, 0);
+        }
+        if (h2) {
+            tu = tu + c2 * Hh(0, 1); tv = tv + c2 * Hh(1, 1);
+            tw = tw + c2 * Hh(2, 1); tb = tb + c2 * Hh(3, 1);
+        }
+        u1 = u1 + dt * tu; v1 = v1 + dt * tv; w1 = w1 + dtw * tw; b1 = b1 + dt * tb;
+    }
+    a.uo[g] = u1; a.vo[g] = v1; a.wo[g] = w1; a.bo[g] = b1;
+}
+
 // read field f at offsets (di, dj) in ring slot s
 #define SM(fi, s, dj, di) sm.pl[fi][s][(ty + 1 + (dj)) * (kTX + 2) + (tx + 1 + (di))]
 
@@ -107,8 +284,6 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
 
     load_plane(kb - 1, (kb + 2) % 3);
     load_plane(kb, kb % 3);
-    const double Ro = a.Ro, rdx = a.rdx, rdy = a.rdy, rdz = a.rdz;
-    const bool rigid = a.rigid;
     const bool h1 = a.do_ab && a.ab1 != 0.0, h2 = a.do_ab && a.ab2 != 0.0;
     for (int k = kb; k < ke; ++k) {
         // history loads first, so they are in flight with the plane's
@@ -129,166 +304,14 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
         __syncthreads();
         if (active) {
             const int sm1 = (k + 2) % 3, s0 = k % 3, sp1 = (k + 1) % 3;
-#define U(di, dj, dk) SM(0, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define V(di, dj, dk) SM(1, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define W(di, dj, dk) SM(2, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define B(di, dj, dk) SM(3, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define UB(di, dj, dk) SM(4, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-#define BB(di, dj, dk) SM(5, (dk) < 0 ? sm1 : ((dk) > 0 ? sp1 : s0), dj, di)
-            const int kg = k + kofs;                     // global level
-            const bool top = rigid && (kg == nzg - 1);   // flux_top(nz) = 0
-            const bool bot = rigid && (kg == 0);         // flux_top(0)  = 0
-            const long g0 = (long)k * plane + (long)j * nx + i;   // point within the instance
-            const long g = g0 + ioff;                              // point within the batch
-            double db_, du_, dv_, dw_;
-            // ---- buoyancy advection + N^2 (advection.f90:12-47, integrate.f90:21-23)
-            // The reference's 0.5 and 0.25 flux factors are powers of two: they
-            // are carried in the per-axis factors a.hd* = 0.5/d*, a.qd* = 0.25/d*
-            // (and 0.25 f0, 0.5 N0^2, set by the launcher), a multiply saved per
-            // flux.  Scaling by a power of two rounds exactly; the results move
-            // at round-off level only where the compiler now contracts a flux
-            // product into the difference that follows (FMA).
-            if (a.nonlinear) {
-                const double fe = (B(0, 0, 0) + B(1, 0, 0)) * U(0, 0, 0);
-                const double fem = (B(-1, 0, 0) + B(0, 0, 0)) * U(-1, 0, 0);
-                const double fn = (B(0, 0, 0) + B(0, 1, 0)) * V(0, 0, 0);
-                const double fnm = (B(0, -1, 0) + B(0, 0, 0)) * V(0, -1, 0);
-                const double ft = top ? 0.0 : (B(0, 0, 0) + B(0, 0, 1)) * W(0, 0, 0);
-                const double ftm = bot ? 0.0 : (B(0, 0, -1) + B(0, 0, 0)) * W(0, 0, -1);
-                db_ = -Ro * ((fe - fem) * a.hdx + (fn - fnm) * a.hdy + (ft - ftm) * a.hdz);
-                // ---- zonal momentum (advection.f90:65-100)
-                {
-                    const double e = (U(0, 0, 0) + U(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
-                    const double em = (U(-1, 0, 0) + U(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
-                    const double n = (U(0, 0, 0) + U(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
-                    const double nm = (U(0, -1, 0) + U(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : (U(0, 0, 1) + U(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
-                    const double tm = bot ? 0.0 : (U(0, 0, 0) + U(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
-                    du_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
-                }
-                // ---- meridional momentum (advection.f90:104-140)
-                {
-                    const double e = (V(0, 0, 0) + V(1, 0, 0)) * (U(0, 1, 0) + U(0, 0, 0));
-                    const double em = (V(-1, 0, 0) + V(0, 0, 0)) * (U(-1, 1, 0) + U(-1, 0, 0));
-                    const double n = (V(0, 0, 0) + V(0, 1, 0)) * (V(0, 1, 0) + V(0, 0, 0));
-                    const double nm = (V(0, -1, 0) + V(0, 0, 0)) * (V(0, 0, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : (V(0, 0, 1) + V(0, 0, 0)) * (W(0, 0, 0) + W(0, 1, 0));
-                    const double tm = bot ? 0.0 : (V(0, 0, 0) + V(0, 0, -1)) * (W(0, 0, -1) + W(0, 1, -1));
-                    dv_ = -Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
-                }
-                // ---- vertical momentum (advection.f90:145-181); rigid lid zeroes
-                //      flux_top(nz-1:nz+2) for w (:167-170)
-                {
-                    const bool wtop = rigid && (kg >= nzg - 2);
-                    const bool wbot = rigid && (kg == 0 || kg >= nzg - 1);
-                    const double e = (W(0, 0, 0) + W(1, 0, 0)) * (U(0, 0, 0) + U(0, 0, 1));
-                    const double em = (W(-1, 0, 0) + W(0, 0, 0)) * (U(-1, 0, 0) + U(-1, 0, 1));
-                    const double n = (W(0, 0, 0) + W(0, 1, 0)) * (V(0, 0, 0) + V(0, 0, 1));
-                    const double nm = (W(0, -1, 0) + W(0, 0, 0)) * (V(0, -1, 0) + V(0, -1, 1));
-                    const double t = wtop ? 0.0 : (W(0, 0, 1) + W(0, 0, 0)) * (W(0, 0, 0) + W(0, 0, 1));
-                    const double tm = wbot ? 0.0 : (W(0, 0, 0) + W(0, 0, -1)) * (W(0, 0, -1) + W(0, 0, 0));
-                    dw_ = -a.dsqr * Ro * ((e - em) * a.qdx + (n - nm) * a.qdy + (t - tm) * a.qdz);
-                }
-            } else {
-                db_ = du_ = dv_ = dw_ = 0.0;
-            }
-            db_ = db_ - (W(0, 0, 0) + W(0, 0, -1)) * a.hN0sq;
-            // ---- Coriolis, buoyancy force, rigid-lid mask (integrate.f90:37-54)
-            du_ = du_ + (V(0, 0, 0) + V(0, -1, 0) + V(1, 0, 0) + V(1, -1, 0)) * a.qf0;
-            dv_ = dv_ - (U(-1, 0, 0) + U(0, 0, 0) + U(-1, 1, 0) + U(0, 1, 0)) * a.qf0;
-            dw_ = dw_ + 0.5 * (B(0, 0, 0) + B(0, 0, 1));
-            if (top) dw_ = 0.0;
-            // ---- friction, in place before AB (integrate.f90:59-66)
-            double u1 = U(0, 0, 0), v1 = V(0, 0, 0), w1 = W(0, 0, 0), b1 = B(0, 0, 0);
-            if constexpr (HARM) {
-                const double dt = a.dt;
-#define HARMONIC(F, Hm, Vm, out)                                                                   \
-    {                                                                                            \
-        const double e = Hm * (F(1, 0, 0) - F(0, 0, 0)) * rdx;                                   \
-        const double em = Hm * (F(0, 0, 0) - F(-1, 0, 0)) * rdx;                                 \
-        const double n = Hm * (F(0, 1, 0) - F(0, 0, 0)) * rdy;                                   \
-        const double nm = Hm * (F(0, 0, 0) - F(0, -1, 0)) * rdy;                                 \
-        const double t = top ? 0.0 : Vm * (F(0, 0, 1) - F(0, 0, 0)) * rdz;                       \
-        const double tm = bot ? 0.0 : Vm * (F(0, 0, 0) - F(0, 0, -1)) * rdz;                     \
-        out = F(0, 0, 0) + dt * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);              \
-    }
-                if (a.harm_uvw) {
-                    HARMONIC(U, a.Ah, a.Av, u1)
-                    HARMONIC(V, a.Ah, a.Av, v1)
-                    HARMONIC(W, a.Ah, a.Av, w1)
-                    if (top) w1 = 0.0;
-                }
-                if (a.harm_b) HARMONIC(B, a.Kh, a.Kv, b1)
-#undef HARMONIC
-            }
-            // ---- set_forcing: background-flow advection (lee_wave1.f90:245-312)
-            if constexpr (BG) {
-                {
-                    const double e = 2 * 0.25 * (UB(0, 0, 0) + UB(1, 0, 0)) * (U(1, 0, 0) + U(0, 0, 0));
-                    const double em = 2 * 0.25 * (UB(-1, 0, 0) + UB(0, 0, 0)) * (U(0, 0, 0) + U(-1, 0, 0));
-                    const double n = 0.25 * (UB(0, 0, 0) + UB(0, 1, 0)) * (V(1, 0, 0) + V(0, 0, 0));
-                    const double nm = 0.25 * (UB(0, -1, 0) + UB(0, 0, 0)) * (V(1, -1, 0) + V(0, -1, 0));
-                    const double t = top ? 0.0 : 0.25 * (UB(0, 0, 1) + UB(0, 0, 0)) * (W(0, 0, 0) + W(1, 0, 0));
-                    const double tm = bot ? 0.0 : 0.25 * (UB(0, 0, 0) + UB(0, 0, -1)) * (W(0, 0, -1) + W(1, 0, -1));
-                    du_ = du_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
-                }
-                {
-                    const double e = 0.25 * (V(0, 0, 0) + V(1, 0, 0)) * (UB(0, 1, 0) + UB(0, 0, 0));
-                    const double em = 0.25 * (V(-1, 0, 0) + V(0, 0, 0)) * (UB(-1, 1, 0) + UB(-1, 0, 0));
-                    dv_ = dv_ - Ro * (e - em) * rdx;
-                }
-                {
-                    const double e = 0.25 * (W(0, 0, 0) + W(1, 0, 0)) * (UB(0, 0, 0) + UB(0, 0, 1));
-                    const double em = 0.25 * (W(-1, 0, 0) + W(0, 0, 0)) * (UB(-1, 0, 0) + UB(-1, 0, 1));
-                    dw_ = dw_ - a.dsqr * Ro * (e - em) * rdx;
-                }
-                {
-                    const double e = 0.5 * (B(0, 0, 0) + B(1, 0, 0)) * UB(0, 0, 0) + 0.5 * (BB(0, 0, 0) + BB(1, 0, 0)) * U(0, 0, 0);
-                    const double em = 0.5 * (B(-1, 0, 0) + B(0, 0, 0)) * UB(-1, 0, 0) + 0.5 * (BB(-1, 0, 0) + BB(0, 0, 0)) * U(-1, 0, 0);
-                    const double n = 0.5 * (BB(0, 0, 0) + BB(0, 1, 0)) * V(0, 0, 0);
-                    const double nm = 0.5 * (BB(0, -1, 0) + BB(0, 0, 0)) * V(0, -1, 0);
-                    const double t = top ? 0.0 : 0.5 * (BB(0, 0, 0) + BB(0, 0, 1)) * W(0, 0, 0);
-                    const double tm = bot ? 0.0 : 0.5 * (BB(0, 0, -1) + BB(0, 0, 0)) * W(0, 0, -1);
-                    db_ = db_ - Ro * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);
-                }
-            }
-#undef U
-#undef V
-#undef W
-#undef B
-#undef UB
-#undef BB
-            // ---- set_forcing: wavemaker (config.f90:224-237)
-            if constexpr (WM) {
-                const double dt = a.dt, c = a.wm_c, s = a.wm_s;
-                if (a.wr[0] || a.wi[0]) u1 = u1 + dt * (c * (a.wr[0] ? a.wr[0][g0] : 0.0) + s * (a.wi[0] ? a.wi[0][g0] : 0.0));
-                if (a.wr[1] || a.wi[1]) v1 = v1 + dt * (c * (a.wr[1] ? a.wr[1][g0] : 0.0) + s * (a.wi[1] ? a.wi[1][g0] : 0.0));
-                if (a.wr[2] || a.wi[2]) w1 = w1 + dt * (c * (a.wr[2] ? a.wr[2][g0] : 0.0) + s * (a.wi[2] ? a.wi[2][g0] : 0.0));
-                if (a.wr[3] || a.wi[3]) b1 = b1 + dt * (c * (a.wr[3] ? a.wr[3][g0] : 0.0) + s * (a.wi[3] ? a.wi[3][g0] : 0.0));
-            }
-            // ---- store tendency of time level tau
-            ((TT*)a.t0[0])[g] = (TT)du_;
-            ((TT*)a.t0[1])[g] = (TT)dv_;
-            ((TW*)a.t0[2])[g] = (TW)dw_;
-            ((TT*)a.t0[3])[g] = (TT)db_;
-            // ---- Adams-Bashforth (integrate.f90:87-102)
-            if (a.do_ab) {
-                const double dt = a.dt, dtw = a.dtw;
-                const double c0 = a.ab0, c1 = a.ab1, c2 = a.ab2;
-                // the current tendency enters at full precision; only the
-                // stored history (FP32 in the mixed path) is rounded
-                double tu = c0 * du_, tv = c0 * dv_, tw = c0 * dw_, tb = c0 * db_;
-                if (h1) {
-                    tu = tu + c1 * (double)sm.hu[0][tid]; tv = tv + c1 * (double)sm.hv[0][tid];
-                    tw = tw + c1 * sm.hw[0][tid]; tb = tb + c1 * (double)sm.hb[0][tid];
-                }
-                if (h2) {
-                    tu = tu + c2 * (double)sm.hu[1][tid]; tv = tv + c2 * (double)sm.hv[1][tid];
-                    tw = tw + c2 * sm.hw[1][tid]; tb = tb + c2 * (double)sm.hb[1][tid];
-                }
-                u1 = u1 + dt * tu; v1 = v1 + dt * tv; w1 = w1 + dtw * tw; b1 = b1 + dt * tb;
-            }
-            a.uo[g] = u1; a.vo[g] = v1; a.wo[g] = w1; a.bo[g] = b1;
+            auto F = [&](int f, int di, int dj, int dk) -> double {
+                return SM(f, dk < 0 ? sm1 : (dk > 0 ? sp1 : s0), dj, di);
+            };
+            auto Hh = [&](int f, int l) -> double {
+                return f == 0 ? (double)sm.hu[l][tid] : f == 1 ? (double)sm.hv[l][tid]
+                     : f == 2 ? sm.hw[l][tid] : (double)sm.hb[l][tid];
+            };
+            step_point<TT, HARM, WM, BG>(a, F, Hh, i, j, k, ioff, h1, h2);
         }
         __syncthreads();
     }
