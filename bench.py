@@ -442,17 +442,20 @@ def projection_run(dev, nx=256, ny=256, nz=64):
             "kernels_ms": {k: v[0] for k, v in kern.items() if v[1]}}
 
 
-def serve_run(dev, n_requests=40, rate_hz=50.0, max_active=8):
+def serve_run(dev, n_requests=40, rate_hz=50.0, max_active=8, max_batch=8):
     """Optimal-balance requests: Poisson arrivals at rate_hz (seed 4), sizes
     drawn from 64x64x32 .. 256x256x64, 5 iterations of 100-step ramps each,
-    admitted by HBM footprint, FP64 and mixed."""
+    admitted by HBM footprint, FP64 and mixed; each request on its own
+    context, and with up to max_batch queued same-size requests sharing the
+    launches of one batched context."""
     from ps3d_b200 import abi
     from ps3d_b200.serve import Server, poisson_schedule, replay_poisson
     sched = poisson_schedule(n_requests, rate_hz, seed=4)
-    out = {"requests": n_requests, "rate_hz": rate_hz, "max_active": max_active,
+    out = {"requests": n_requests, "rate_hz": rate_hz, "max_active": max_active, "max_batch": max_batch,
            "request": "diag_opt_balance, 5 iterations x (100 back + 100 forward steps) + projections"}
-    for name, prec in (("fp64", abi.PS3D_FP64), ("mixed", abi.PS3D_MIXED)):
-        srv = Server(device=dev, max_active=max_active)
+    for name, prec, mb in (("fp64", abi.PS3D_FP64, 1), ("mixed", abi.PS3D_MIXED, 1),
+                           ("fp64_batched", abi.PS3D_FP64, max_batch), ("mixed_batched", abi.PS3D_MIXED, max_batch)):
+        srv = Server(device=dev, max_active=max_active, max_batch=mb)
         r = replay_poisson(srv, sched, precision=prec)
         r["peak_active"] = srv.stats()["peak_active"]
         srv.close()

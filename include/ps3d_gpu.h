@@ -397,6 +397,15 @@ PS3D_API int ps3d_server_submit_ensemble(ps3d_server* s, const ps3d_params* memb
 PS3D_API int ps3d_server_wait_ensemble(ps3d_server* s, long long ticket, int timeout_ms, double* const* u,
                                        double* const* v, double* const* w, double* const* b, double* res);
 PS3D_API int ps3d_server_cancel(ps3d_server* s, long long ticket);
+/* Shared launches for same-size requests: up to max_batch queued
+ * optimal-balance requests whose grid, physics and balance parameters are
+ * identical are admitted together and run as instances of one batched
+ * context (every kernel launch advances all of them; each keeps its own
+ * norm, iteration count and result, bit for bit what it gets alone with the
+ * same kernel shapes).  Their footprint is the sum of theirs.  1 (the
+ * default) runs every request on its own context.  Requests with
+ * biharmonic friction always run alone.                                    */
+PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch);
 /* stats[6] = {active, queued, bytes in use, peak bytes, peak active, budget} */
 PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats);
 PS3D_API long long ps3d_server_footprint(const ps3d_params* prm);

@@ -176,6 +176,7 @@ struct Ctx {
     // reductions / staging
     int nred = 0;
     DevBuf red_partials, red_out, staging;
+    DevBuf norms;             // a batched optimal balance's per-instance norms (4 doubles each)
     // kernel error word in mapped page-locked memory: kernels whose bounded
     // waits ran out store 1; read after every stream synchronisation
     unsigned* kerr_h = nullptr;
@@ -242,7 +243,7 @@ struct Ctx {
     int warn_first();
     int warn_second();
     int warn_third();
-    int diagnose(double* ke, double* pe, double* umax, double* wmax);
+    int diagnose(double* ke, double* pe, double* umax, double* wmax, int member = 0);
     int opt_time_ave(int set, int n_end_ave);
     int opt_balance(const ps3d_optbal& O, double* final_norm, int* iters);
     int reset_request();      // back to the just-created state (the serving pool reuses contexts)

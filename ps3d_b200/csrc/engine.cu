@@ -250,13 +250,16 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     rigid = P.enable_vertical_boundaries != 0;
     mixed = P.precision == PS3D_MIXED || P.precision == PS3D_MIXED_REFINED;
     refine_full = P.precision == PS3D_MIXED_REFINED;
-    if (nx < 2 || ny < 2 || nz < 2 || nx % 2 || ny % 2 || (!rigid && nz % 2)) return PS3D_ERR_BADPARAM;
-    if (!fft_length_ok(nx / 2) || !fft_length_ok(ny) || (!rigid && !fft_length_ok(nz))) return PS3D_ERR_BADPARAM;
+    // a z-slab's local grid (split_solve) never transforms along its own z:
+    // the slab driver solves whole columns of the global grid
+    const bool zfft = !rigid && !split_solve;
+    if (nx < 2 || ny < 2 || nz < 2 || nx % 2 || ny % 2 || (zfft && nz % 2)) return PS3D_ERR_BADPARAM;
+    if (!fft_length_ok(nx / 2) || !fft_length_ok(ny) || (zfft && !fft_length_ok(nz))) return PS3D_ERR_BADPARAM;
     if (P.precision != PS3D_FP64 && !mixed) return PS3D_ERR_BADPARAM;
     if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.Lx > 0 && P.Ly > 0 && P.Lz > 0 && P.dsqr > 0)) return PS3D_ERR_BADPARAM;
     // columns too tall for the vertical solve's (or the projections' periodic
     // z transform's) shared memory
-    if (rigid ? thomas_threads(nz) == 0 : !zsolve_fits(nz, false))
+    if (rigid ? thomas_threads(nz) == 0 : (zfft && !zsolve_fits(nz, false)))
         return PS3D_ERR_TOOLARGE;
     if (cudaSetDevice(dev) != cudaSuccess) return PS3D_ERR_CUDA;
     if (use_stream) { stream = use_stream; own_stream = false; }
@@ -274,7 +277,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     for (int f = 0; f < 4; ++f) { CK(tend[f].alloc(3 * NB * tsz(f))); CK(cudaMemset(tend[f].p, 0, 3 * NB * tsz(f))); }
     CK(FS.alloc(M * batch * (mixed ? sizeof(float2) : sizeof(double2))));
     // plans and tables
-    CK(plx.build(nx / 2, 0)); CK(ply.build(ny, 0)); CK(plz.build(rigid ? 1 : nz, 0));
+    CK(plx.build(nx / 2, 0)); CK(ply.build(ny, 0)); CK(plz.build(zfft ? nz : 1, 0));
     CK(plx4.build(nx / 2, 1)); CK(ply4.build(ny, 1));
     CK(plx8.build(nx / 2, 2)); CK(ply8.build(ny, 2));
     {
@@ -398,10 +401,11 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
 cudaError_t Ctx::ensure_spectral4() {
     if (spec4[0].p) return cudaSuccess;
     cudaError_t e;
-    for (int f = 0; f < 4; ++f) if ((e = spec4[f].alloc(M * sizeof(double2)))) return e;
-    if ((e = g0base.alloc(M * sizeof(double2)))) return e;
-    if ((e = cudaMemset(g0base.p, 0, M * sizeof(double2)))) return e;
-    if ((e = qtmp.alloc(M * sizeof(double2)))) return e;
+    const long MB = M * batch;   // projections of a batched context cover every instance
+    for (int f = 0; f < 4; ++f) if ((e = spec4[f].alloc(MB * sizeof(double2)))) return e;
+    if ((e = g0base.alloc(MB * sizeof(double2)))) return e;
+    if ((e = cudaMemset(g0base.p, 0, MB * sizeof(double2)))) return e;
+    if ((e = qtmp.alloc(MB * sizeof(double2)))) return e;
     return cudaSuccess;
 }
 cudaError_t Ctx::ensure_fieldset(int which) {
@@ -409,9 +413,9 @@ cudaError_t Ctx::ensure_fieldset(int which) {
     if (!s) return cudaErrorInvalidValue;
     if (s[0].p) return cudaSuccess;
     for (int f = 0; f < 4; ++f) {
-        cudaError_t e = s[f].alloc(N * sizeof(double));
+        cudaError_t e = s[f].alloc(N * batch * sizeof(double));
         if (e) return e;
-        if ((e = cudaMemsetAsync(s[f].p, 0, N * sizeof(double), stream))) return e;
+        if ((e = cudaMemsetAsync(s[f].p, 0, N * batch * sizeof(double), stream))) return e;
     }
     return cudaSuccess;
 }
@@ -905,16 +909,18 @@ int Ctx::forward_transform(const double* const* in) {
     for (int f = 0; f < 4; ++f) {
         PlaneArgs a = pa64;
         a.mode = 1; a.src = in[f]; a.scale = P.dx * P.dy;
+        a.batch = batch;
         a.spec = rigid ? qtmp.p : spec4[f].p;
         LAUNCH(PS3D_K_OTHER, launch_plane_fwd(a, false, stream));
         if (rigid) {
             // A = the transposed matrix, the second half of the mode buffer
-            LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)qtmp.p, (double2*)spec4[f].p,
-                                                  (const double*)modes[f]->p + (size_t)nz * nz, nz, M2, P.dz, stream));
+            for (int m = 0; m < batch; ++m)
+                LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)qtmp.p + m * M, (double2*)spec4[f].p + m * M,
+                                                      (const double*)modes[f]->p + (size_t)nz * nz, nz, M2, P.dz, stream));
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
-            c.batch = 1; c.sM = M; c.layout = spectral_layout(pa64);
+            c.batch = batch; c.sM = M; c.layout = spectral_layout(pa64);
             c.pz = plz.plan; c.scale = P.dz; c.op = 1;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
@@ -926,17 +932,19 @@ int Ctx::backward_transform(double* const* out) {
     for (int f = 0; f < 4; ++f) {
         void* src = spec4[f].p;
         if (rigid) {
-            LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)spec4[f].p, (double2*)qtmp.p, (const double*)modes[f]->p,
-                                                  nz, M2, 1.0, stream));
+            for (int m = 0; m < batch; ++m)
+                LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)spec4[f].p + m * M, (double2*)qtmp.p + m * M,
+                                                      (const double*)modes[f]->p, nz, M2, 1.0, stream));
             src = qtmp.p;
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
-            c.batch = 1; c.sM = M; c.layout = spectral_layout(pa64);
+            c.batch = batch; c.sM = M; c.layout = spectral_layout(pa64);
             c.pz = plz.plan; c.scale = 1.0; c.op = 2;
             LAUNCH(PS3D_K_OTHER, launch_zsolve(c, false, stream));
         }
         PlaneArgs b = pa64;
+        b.batch = batch;
         b.spec = src; b.out = out[f]; b.beta = 0.0;
         b.scale = rigid ? 1.0 / (P.Lx * P.Ly) : 1.0 / (P.Lx * P.Ly * P.Lz);
         LAUNCH(PS3D_K_OTHER, launch_plane_inv(b, false, stream));
@@ -978,24 +986,29 @@ int Ctx::project_spectral(int mode) {
     a.ax.ex = (const double*)t_ex.p; a.ax.ey = (const double*)t_ey.p; a.ax.ez = (const double*)t_ez.p;
     a.ax.px = (const double2*)t_px.p; a.ax.py = (const double2*)t_py.p; a.ax.pz = (const double2*)t_pz.p;
     a.ax.sz = (const double*)t_sz.p; a.ax.cz = (const double*)t_cz.p;
-    a.US = (double2*)spec4[0].p; a.VS = (double2*)spec4[1].p; a.WS = (double2*)spec4[2].p; a.BS = (double2*)spec4[3].p;
-    a.g0base = (double2*)g0base.p;
     a.mode = mode;
-    LAUNCH(PS3D_K_OTHER, launch_project(a, stream));
+    for (int m = 0; m < batch; ++m) {   // every instance of a batched context
+        a.US = (double2*)spec4[0].p + m * M; a.VS = (double2*)spec4[1].p + m * M;
+        a.WS = (double2*)spec4[2].p + m * M; a.BS = (double2*)spec4[3].p + m * M;
+        a.g0base = (double2*)g0base.p + m * M;
+        LAUNCH(PS3D_K_OTHER, launch_project(a, stream));
+    }
     return PS3D_OK;
 }
 
 // ---------------------------------------------------------------------------
 // diagnose (diagnose.F90:2-61)
 // ---------------------------------------------------------------------------
-int Ctx::diagnose(double* ke, double* pe, double* umax, double* wmax) {
+int Ctx::diagnose(double* ke, double* pe, double* umax, double* wmax, int m) {
     {
         int rc = materialize();
         if (rc) return rc;
     }
+    if (m < 0 || m >= batch) return PS3D_ERR_BADPARAM;
     DiagOut* d = (DiagOut*)red_out.p;
-    LAUNCH(PS3D_K_OTHER, launch_diagnose(field(0), field(1), field(2), field(3), (const double*)p.p, nx, ny, nz, P.dsqr, P.N0, P.dz,
-                       (double*)red_partials.p, nred, d, stream));
+    LAUNCH(PS3D_K_OTHER, launch_diagnose(member_field(0, m), member_field(1, m), member_field(2, m), member_field(3, m),
+                                         (const double*)p.p + (size_t)m * N, nx, ny, nz, P.dsqr, P.N0, P.dz,
+                                         (double*)red_partials.p, nred, d, stream));
     DiagOut h;
     CK(cudaMemcpyAsync(&h, d, sizeof(DiagOut), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
@@ -1015,7 +1028,8 @@ cudaError_t Ctx::copy_state_to(int set) {
     if (e) return e;
     DevBuf* s = fieldset(set);
     for (int f = 0; f < 4; ++f)
-        if ((e = cudaMemcpyAsync(s[f].p, field(f), N * sizeof(double), cudaMemcpyDeviceToDevice, stream))) return e;
+        if ((e = cudaMemcpyAsync(s[f].p, field(f), N * batch * sizeof(double), cudaMemcpyDeviceToDevice, stream)))
+            return e;
     return cudaSuccess;
 }
 cudaError_t Ctx::copy_set_to_state(int set) {
@@ -1024,7 +1038,8 @@ cudaError_t Ctx::copy_set_to_state(int set) {
     DevBuf* s = fieldset(set);
     cudaError_t e;
     for (int f = 0; f < 4; ++f)
-        if ((e = cudaMemcpyAsync(field(f), s[f].p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream))) return e;
+        if ((e = cudaMemcpyAsync(field(f), s[f].p, N * batch * sizeof(double), cudaMemcpyDeviceToDevice, stream)))
+            return e;
     return cudaSuccess;
 }
 
@@ -1041,16 +1056,17 @@ int Ctx::opt_time_ave(int set, int n_end_ave) {
     P.Ro = 0.;
     CK(ensure_fieldset(set));
     DevBuf* s = fieldset(set);
-    for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(s[f].p, 0, N * sizeof(double), stream));
+    const long NB = N * batch;
+    for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(s[f].p, 0, NB * sizeof(double), stream));
     for (int n = 0; n <= n_end_ave - 1; ++n) {
         int rc = step(itt, tau, taum1, taum2);
         if (rc) return rc;
         rotate();
         rc = materialize();
         if (rc) return rc;
-        for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, field(f), N, 1.0, 1.0, stream));
+        for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, field(f), NB, 1.0, 1.0, stream));
     }
-    for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, nullptr, N, 1.0 / n_end_ave, 0.0, stream));
+    for (int f = 0; f < 4; ++f) LAUNCH(PS3D_K_OTHER, launch_axpby((double*)s[f].p, nullptr, NB, 1.0 / n_end_ave, 0.0, stream));
     return PS3D_OK;
 }
 
@@ -1149,23 +1165,34 @@ int Ctx::reset_request() {
     return PS3D_OK;
 }
 
+// With batch > 1 every instance runs its own optimal balance with the same
+// parameters in the same launches: each instance's norm is reduced on its
+// own, and an instance whose loop would end (n > 1, norm < tol) keeps the
+// balanced state and norm of that iteration while the others go on; the
+// later iterations still advance its state, which nothing reads.
+// final_norm and iters then hold one value per instance.
 int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     if (!(O.period > 0) || O.max_itts < 1 || (O.enable_time_ave && (!(O.average > 0) || O.average_times < 1)))
         return PS3D_ERR_BADPARAM;
+    const long NB = N * batch;
     // save model state (:78-83)
     CK(copy_state_to(kSetSave));
     CK(ensure_saved_tail());
-    CK(cudaMemcpyAsync(saved_p.p, p.p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(saved_p.p, p.p, NB * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     for (int f = 0; f < 4; ++f)
-        CK(cudaMemcpyAsync(saved_tend[f].p, tend[f].p, 3 * N * tsz(f), cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(saved_tend[f].p, tend[f].p, 3 * NB * tsz(f), cudaMemcpyDeviceToDevice, stream));
     const double Ro_loc = P.Ro, dt_loc = P.dt;
     const double Ahbi_loc = P.Ahbi, Avbi_loc = P.Avbi, Khbi_loc = P.Khbi, Kvbi_loc = P.Kvbi;
     const int tau_loc = tau, taum1_loc = taum1, taum2_loc = taum2, itt_loc = itt;
     CK(copy_state_to(PS3D_FIELDS_BALANCED));
     const int n_end = (int)(O.period / P.dt) + 1;
     const int n_end_ave = (int)(O.average / P.dt) + 1;
-    double norm_diff = 1.0;
-    int rc = PS3D_OK, n_done = 0;
+    std::vector<double> norm_diff(batch, 1.0);
+    std::vector<int> n_done(batch, 0);
+    std::vector<char> running(batch, 1);
+    int nrun = batch;
+    if (batch > 1 && norms.bytes < (size_t)batch * 4 * sizeof(double)) CK(norms.alloc((size_t)batch * 4 * sizeof(double)));
+    int rc = PS3D_OK;
     std::vector<RampGraph> graphs;   // ramp graphs of this call (ramp_run)
     struct Release {
         std::vector<RampGraph>& g;
@@ -1180,8 +1207,9 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     } else {
         rc = project(PS3D_PROJ_BASE_POINT);
     }
-    for (int n = 1; n <= O.max_itts && !rc; ++n) {
-        n_done = n;
+    for (int n = 1; n <= O.max_itts && !rc && nrun > 0; ++n) {
+        for (int m = 0; m < batch; ++m)
+            if (running[m]) n_done[m] = n;
         // opt_backward_integration (:183-209)
         P.Ahbi = 0; P.Avbi = 0; P.Khbi = 0; P.Kvbi = 0;
         itt = 0; taum2 = 1; taum1 = 2; tau = 3;
@@ -1213,36 +1241,52 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
             DevBuf *sv = fieldset(kSetSave2), *av = fieldset(kSetAve), *bs = fieldset(PS3D_FIELDS_BASE);
             p_warm = false;
             for (int f = 0; f < 4; ++f) {
-                CK(cudaMemcpyAsync(field(f), sv[f].p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-                LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)av[f].p, N, 1.0, -1.0, stream));
-                LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)bs[f].p, N, 1.0, 1.0, stream));
+                CK(cudaMemcpyAsync(field(f), sv[f].p, NB * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+                LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)av[f].p, NB, 1.0, -1.0, stream));
+                LAUNCH(PS3D_K_OTHER, launch_axpby(field(f), (const double*)bs[f].p, NB, 1.0, 1.0, stream));
             }
         } else {
             rc = project(PS3D_PROJ_EXCHANGE);
             if (rc) break;
         }
-        // opt_balance_norm (:339-362)
+        // opt_balance_norm (:339-362), per instance
         {
             rc = materialize();
             if (rc) break;
             DevBuf* bl = fieldset(PS3D_FIELDS_BALANCED);
-            const double* x[4] = {field(0), field(1), field(2), field(3)};
-            const double* y[4] = {(const double*)bl[0].p, (const double*)bl[1].p, (const double*)bl[2].p, (const double*)bl[3].p};
-            double* out = (double*)red_out.p + 8;
-            LAUNCH(PS3D_K_OTHER, launch_norm(x, y, N, P.dsqr, P.N0 * P.N0, (double*)red_partials.p, nred, out, stream));
-            double h[4];
-            CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, stream));
+            double* out = batch > 1 ? (double*)norms.p : (double*)red_out.p + 8;
+            for (int m = 0; m < batch; ++m) {
+                if (!running[m]) continue;
+                const double* x[4] = {member_field(0, m), member_field(1, m), member_field(2, m), member_field(3, m)};
+                const double* y[4];
+                for (int f = 0; f < 4; ++f) y[f] = (const double*)bl[f].p + (size_t)m * N;
+                LAUNCH(PS3D_K_OTHER, launch_norm(x, y, N, P.dsqr, P.N0 * P.N0, (double*)red_partials.p, nred,
+                                                 out + 4 * m, stream));
+            }
+            std::vector<double> h(4 * (size_t)batch);
+            CK(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
             CK(cudaStreamSynchronize(stream));
-            norm_diff = h[3];
+            for (int m = 0; m < batch; ++m)
+                if (running[m]) norm_diff[m] = h[4 * m + 3];
         }
-        CK(copy_state_to(PS3D_FIELDS_BALANCED));
-        if (n > 1 && norm_diff < O.tol) break;
+        if (nrun == batch) {
+            CK(copy_state_to(PS3D_FIELDS_BALANCED));
+        } else {   // the instances still running only
+            DevBuf* bl = fieldset(PS3D_FIELDS_BALANCED);
+            for (int m = 0; m < batch; ++m)
+                if (running[m])
+                    for (int f = 0; f < 4; ++f)
+                        CK(cudaMemcpyAsync((double*)bl[f].p + (size_t)m * N, member_field(f, m), N * sizeof(double),
+                                           cudaMemcpyDeviceToDevice, stream));
+        }
+        for (int m = 0; m < batch; ++m)
+            if (running[m] && n > 1 && norm_diff[m] < O.tol) { running[m] = 0; --nrun; }
     }
     // restore model state (:172-176)
     CK(copy_set_to_state(kSetSave));
-    CK(cudaMemcpyAsync(p.p, saved_p.p, N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(p.p, saved_p.p, NB * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     for (int f = 0; f < 4; ++f)
-        CK(cudaMemcpyAsync(tend[f].p, saved_tend[f].p, 3 * N * tsz(f), cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(tend[f].p, saved_tend[f].p, 3 * NB * tsz(f), cudaMemcpyDeviceToDevice, stream));
     P.Ro = Ro_loc; P.dt = dt_loc;
     P.Ahbi = Ahbi_loc; P.Avbi = Avbi_loc; P.Khbi = Khbi_loc; P.Kvbi = Kvbi_loc;
     tau = tau_loc; taum1 = taum1_loc; taum2 = taum2_loc; itt = itt_loc;
@@ -1250,16 +1294,18 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     if (rc) return rc;
     if (O.adopt) CK(copy_set_to_state(PS3D_FIELDS_BALANCED));
     CK(cudaStreamSynchronize(stream));
-    if (final_norm) *final_norm = norm_diff;
-    if (iters) *iters = n_done;
+    for (int m = 0; m < batch; ++m) {
+        if (final_norm) final_norm[m] = norm_diff[m];
+        if (iters) iters[m] = n_done[m];
+    }
     return PS3D_OK;
 }
 
 cudaError_t Ctx::ensure_saved_tail() {
     if (saved_p.p) return cudaSuccess;
     cudaError_t e;
-    if ((e = saved_p.alloc(N * sizeof(double)))) return e;
-    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * tsz(f)))) return e;
+    if ((e = saved_p.alloc(N * batch * sizeof(double)))) return e;
+    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * batch * tsz(f)))) return e;
     return cudaSuccess;
 }
 

@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
     const int ld = kZLines + 1;
     const int nz = a.nz;
     const PlanTables<R> tz = stage_plan<R>(a.pz, smem_raw + align16((size_t)nz * ld * sizeof(T)));
-    const long ncols = (long)a.nxh * a.ny;
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
     const long bpi = (ncols + kZLines - 1) / kZLines;   // blocks per instance
     const long inst = blockIdx.x / bpi;
     const long c0 = (blockIdx.x - inst * bpi) * (long)kZLines;
@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(256) k_zsolve(const ColumnArgs a) {
             const int p = t / nl, l = t - p * nl;
             T v = cscale(buf[p * ld + l], sc);
             if (a.op == 0) {
-                const long c = c0 + l;
+                const long c = c0 + l + a.col0;   // global column: its wavenumbers
                 const int i = a.layout ? (int)(c / a.ny) : (int)(c % a.nxh);
                 const int j = a.layout ? (int)(c % a.ny) : (int)(c / a.nxh);
                 const int k = tz.ipos[p];
@@ -1551,7 +1551,7 @@ bool zsolve_fits(int nz, bool fp32) {
 }
 
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s) {
-    const long ncols = (long)a.nxh * a.ny;
+    const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;
     const int blocks = (int)(((ncols + kZLines - 1) / kZLines) * std::max(1, a.batch));
     const size_t es = fp32 ? sizeof(float2) : sizeof(double2);
     const size_t sm = zsolve_smem(a.nz, es);

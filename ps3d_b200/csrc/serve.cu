@@ -42,6 +42,13 @@ namespace {
 
 enum State { kQueued, kRunning, kDone, kFailed, kCancelled };
 
+struct Request;
+// requests admitted together as the instances of one batched context
+struct Group {
+    std::vector<Request*> members;
+    std::atomic<int> cancel{0};   // set once every member is cancelled
+};
+
 struct Request {
     long long id = 0;
     int kind = 0;                   // 0: optimal balance, 1: ensemble run
@@ -59,6 +66,7 @@ struct Request {
     int iters = 0;
     Clock::time_point t_submit, t_start, t_end;
     std::atomic<int> cancel{0};
+    std::shared_ptr<Group> group;   // batched with other requests (null: alone)
 };
 
 }  // namespace
@@ -84,6 +92,7 @@ static size_t footprint_of(const ps3d_params& p) {
 
 struct IdleCtx {
     ps3d_params prm;
+    int batch;
     std::unique_ptr<Ctx> ctx;
     size_t footprint;
 };
@@ -93,6 +102,7 @@ struct ps3d_server {
     std::deque<IdleCtx> idle;   // finished requests' contexts, oldest first (counted in `used`)
     size_t budget = 0, used = 0, peak_used = 0;
     int max_active = 1, active = 0, peak_active = 0;
+    int max_batch = 1;          // same-parameter requests run together (ps3d_server_set_batching)
     long long next_id = 1;
     bool stopping = false;
     std::mutex mu;
@@ -102,10 +112,17 @@ struct ps3d_server {
     std::vector<std::thread> workers;
 
     void worker_loop();
-    std::unique_ptr<Ctx> run(Request& r, std::unique_ptr<Ctx> reuse);
+    std::unique_ptr<Ctx> run(std::vector<std::shared_ptr<Request>>& g, std::unique_ptr<Ctx> reuse);
 };
 
 static bool same_params(const ps3d_params& a, const ps3d_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+static bool same_opt(const ps3d_optbal& a, const ps3d_optbal& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+// requests that may share a batched context: no biharmonic friction (its
+// generic-path kernels take one grid)
+static bool batchable(const Request& r) {
+    const ps3d_params& p = r.prm;
+    return r.kind == 0 && !(p.Ahbi > 0 || p.Avbi > 0 || p.Khbi > 0 || p.Kvbi > 0);
+}
 
 // An ensemble run: batched contexts of its own (not pooled), advanced in
 // chunks of 30 steps (a multiple of the graph period 3) with the cancel flag
@@ -138,15 +155,18 @@ static int run_ensemble(Request& r, int device) {
     return rc;
 }
 
-// Runs request r on `reuse` (an idle context of the same parameters) or on a
-// new context; returns the context for the idle pool when the request
-// succeeded.
-std::unique_ptr<Ctx> ps3d_server::run(Request& r, std::unique_ptr<Ctx> reuse) {
+// Runs the group g (one request, or several same-parameter optimal balances
+// as the instances of one batched context) on `reuse` (an idle context of
+// the same parameters and batch) or on a new context; returns the context
+// for the idle pool when every request of the group succeeded.
+std::unique_ptr<Ctx> ps3d_server::run(std::vector<std::shared_ptr<Request>>& g, std::unique_ptr<Ctx> reuse) {
     cudaSetDevice(device);
-    if (r.kind == 1) {
-        r.status = run_ensemble(r, device);
+    Request& r0 = *g[0];
+    if (r0.kind == 1) {
+        r0.status = run_ensemble(r0, device);
         return nullptr;
     }
+    const int nb = (int)g.size();
     std::unique_ptr<Ctx> cp = std::move(reuse);
     int rc = PS3D_OK;
     if (cp) {
@@ -157,73 +177,112 @@ std::unique_ptr<Ctx> ps3d_server::run(Request& r, std::unique_ptr<Ctx> reuse) {
         // other requests share the GPU, and one context at a time (the
         // tuner's lock); cached choices or the defaults are taken instead
         cp->tune_timing = false;
-        rc = cp->init(r.prm, device);
+        rc = cp->init(r0.prm, device, nb);
     }
     Ctx& c = *cp;
+    std::atomic<int> one{0};
     if (!rc) {
-        c.cancel_flag = &r.cancel;
-        for (int f = 0; f < 4 && !rc; ++f) rc = c.upload_field(c.field(f), r.in[f].data());
+        c.cancel_flag = nb > 1 ? &r0.group->cancel : &r0.cancel;
+        for (int m = 0; m < nb && !rc; ++m)
+            for (int f = 0; f < 4 && !rc; ++f) rc = c.upload_field(c.member_field(f, m), g[m]->in[f].data());
     }
-    if (!rc) rc = c.opt_balance(r.opt, &r.norm, &r.iters);
+    std::vector<double> norms(nb, 0.0);
+    std::vector<int> iters(nb, 0);
+    if (!rc) rc = c.opt_balance(r0.opt, norms.data(), iters.data());
+    std::vector<int> st(nb, rc);
     if (!rc) {
-        // a non-finite balanced state fails this request only
-        double ke, pe, um, wm;
         ps3d::DevBuf* bal = c.fieldset(PS3D_FIELDS_BALANCED);
         for (int f = 0; f < 4 && !rc; ++f)
-            if (cudaMemcpyAsync(c.field(f), bal[f].p, c.N * sizeof(double), cudaMemcpyDeviceToDevice, c.stream))
+            if (cudaMemcpyAsync(c.field(f), bal[f].p, c.N * nb * sizeof(double), cudaMemcpyDeviceToDevice, c.stream))
                 rc = PS3D_ERR_CUDA;
-        if (!rc) rc = c.diagnose(&ke, &pe, &um, &wm);
-    }
-    if (!rc) {
-        const size_t n3 = (size_t)(r.prm.nx + 4) * (r.prm.ny + 4) * (r.prm.nz + 4);
-        for (int f = 0; f < 4 && !rc; ++f) {
-            r.out[f].assign(n3, 0.0);
-            rc = c.download_field(c.field(f), r.out[f].data(), 0);
+        for (int m = 0; m < nb; ++m) {
+            st[m] = rc;
+            double ke, pe, um, wm;
+            // a non-finite balanced state fails this request only
+            if (!st[m]) st[m] = c.diagnose(&ke, &pe, &um, &wm, m);
+            if (!st[m]) {
+                const size_t n3 = (size_t)(r0.prm.nx + 4) * (r0.prm.ny + 4) * (r0.prm.nz + 4);
+                for (int f = 0; f < 4 && !st[m]; ++f) {
+                    g[m]->out[f].assign(n3, 0.0);
+                    st[m] = c.download_field(c.member_field(f, m), g[m]->out[f].data(), 0);
+                }
+            }
         }
     }
     c.cancel_flag = nullptr;
-    r.status = rc;
-    if (rc) cp.reset();
+    bool all_ok = true;
+    for (int m = 0; m < nb; ++m) {
+        Request& r = *g[m];
+        r.norm = norms[m];
+        r.iters = iters[m];
+        r.status = st[m];
+        if (!st[m] && r.cancel.load()) r.status = PS3D_ERR_CANCELLED;   // cancelled while its group ran on
+        if (r.status) all_ok = false;
+    }
+    if (rc || !all_ok) cp.reset();
     return cp;
 }
 
 void ps3d_server::worker_loop() {
     for (;;) {
-        std::shared_ptr<Request> r;
+        std::vector<std::shared_ptr<Request>> g;   // the request(s) admitted together
+        size_t gfoot = 0;
         std::unique_ptr<Ctx> reuse;
         std::vector<std::unique_ptr<Ctx>> evicted;   // destroyed after the lock is released
         {
             std::unique_lock<std::mutex> lk(mu);
             for (;;) {
                 if (stopping) return;
-                // admit the oldest request if a slot and its HBM footprint are free:
-                // on an idle context of the same parameters, or after freeing idle ones
+                // admit the oldest request if a slot and its HBM footprint are free,
+                // with the queued requests that share its parameters (up to
+                // max_batch): on an idle context of the same parameters and
+                // batch, or after freeing idle ones
                 if (!queue.empty() && active < max_active) {
                     const std::shared_ptr<Request>& q = queue.front();
+                    std::vector<std::shared_ptr<Request>> cand{q};
+                    if (max_batch > 1 && batchable(*q))
+                        for (size_t k = 1; k < queue.size() && (int)cand.size() < max_batch; ++k)
+                            if (batchable(*queue[k]) && same_params(queue[k]->prm, q->prm) &&
+                                same_opt(queue[k]->opt, q->opt))
+                                cand.push_back(queue[k]);
+                    // the largest group whose footprint fits, given what idle contexts could free
+                    size_t idle_bytes = 0;
+                    for (const IdleCtx& ic : idle) idle_bytes += ic.footprint;
+                    while (cand.size() > 1 && used - idle_bytes + cand.size() * q->footprint > budget) cand.pop_back();
+                    const int nb = (int)cand.size();
+                    const size_t foot = nb * q->footprint;
                     long hit = -1;
                     for (size_t i = 0; i < idle.size() && hit < 0 && q->kind == 0; ++i)
-                        if (same_params(idle[i].prm, q->prm)) hit = (long)i;
+                        if (idle[i].batch == nb && same_params(idle[i].prm, q->prm)) hit = (long)i;
                     bool fits = hit >= 0;
-                    while (!fits && !idle.empty() && used + q->footprint > budget) {   // no hit: free idle ones
+                    while (!fits && !idle.empty() && used + foot > budget) {   // no hit: free idle ones
                         evicted.push_back(std::move(idle.front().ctx));
                         used -= idle.front().footprint;
                         idle.pop_front();
                     }
-                    if (!fits) fits = used + q->footprint <= budget;
+                    if (!fits) fits = used + foot <= budget;
                     if (fits) {
-                        r = q;
-                        queue.pop_front();
+                        g = cand;
+                        for (const auto& r : g)
+                            for (auto it = queue.begin(); it != queue.end(); ++it)
+                                if (*it == r) { queue.erase(it); break; }
                         if (hit >= 0) {
                             reuse = std::move(idle[hit].ctx);   // its footprint is already counted
+                            gfoot = idle[hit].footprint;
                             idle.erase(idle.begin() + hit);
                         } else {
-                            used += r->footprint;
+                            used += foot;
+                            gfoot = foot;
+                        }
+                        if (nb > 1) {
+                            auto grp = std::make_shared<Group>();
+                            for (const auto& r : g) { grp->members.push_back(r.get()); r->group = grp; }
                         }
                         ++active;
                         peak_used = std::max(peak_used, used);
                         peak_active = std::max(peak_active, active);
-                        r->state = kRunning;
-                        r->t_start = Clock::now();
+                        const auto now = Clock::now();
+                        for (const auto& r : g) { r->state = kRunning; r->t_start = now; }
                         break;
                     }
                 }
@@ -234,19 +293,23 @@ void ps3d_server::worker_loop() {
         if (!evicted.empty()) {
             cudaSetDevice(device);
             evicted.clear();
-            if (!r) continue;
+            if (g.empty()) continue;
         }
-        std::unique_ptr<Ctx> done = run(*r, std::move(reuse));
+        std::unique_ptr<Ctx> done = run(g, std::move(reuse));
         {
             std::lock_guard<std::mutex> lk(mu);
-            r->t_end = Clock::now();
-            r->state = r->status == PS3D_OK ? kDone : (r->status == PS3D_ERR_CANCELLED ? kCancelled : kFailed);
-            for (int f = 0; f < 4; ++f) { r->in[f].clear(); r->in[f].shrink_to_fit(); }
-            r->ein.clear();
-            r->ein.shrink_to_fit();
+            const auto now = Clock::now();
+            for (const auto& r : g) {
+                r->t_end = now;
+                r->state = r->status == PS3D_OK ? kDone : (r->status == PS3D_ERR_CANCELLED ? kCancelled : kFailed);
+                for (int f = 0; f < 4; ++f) { r->in[f].clear(); r->in[f].shrink_to_fit(); }
+                r->ein.clear();
+                r->ein.shrink_to_fit();
+                r->group.reset();
+            }
             --active;
-            if (done && !stopping) idle.push_back({r->prm, std::move(done), r->footprint});
-            else used -= r->footprint;
+            if (done && !stopping) idle.push_back({g[0]->prm, (int)g.size(), std::move(done), gfoot});
+            else used -= gfoot;
             // keep at most max_active idle contexts
             while ((int)idle.size() > max_active) {
                 evicted.push_back(std::move(idle.front().ctx));
@@ -484,6 +547,11 @@ PS3D_API int ps3d_server_cancel(ps3d_server* s, long long ticket) {
             r.t_end = Clock::now();
         } else if (r.state == kRunning) {
             r.cancel.store(1);
+            if (r.group) {   // a batched group stops once every member is cancelled
+                bool all = true;
+                for (Request* m : r.group->members) all = all && m->cancel.load() != 0;
+                if (all) r.group->cancel.store(1);
+            }
         }
     }
     s->cv_done.notify_all();
@@ -505,5 +573,15 @@ PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats) {
 }
 
 PS3D_API long long ps3d_server_footprint(const ps3d_params* prm) { return prm ? (long long)footprint_of(*prm) : -1; }
+
+PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch) {
+    if (!s || max_batch < 1) return PS3D_ERR_BADPARAM;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->max_batch = max_batch;
+    }
+    s->cv_work.notify_all();
+    return PS3D_OK;
+}
 
 }  // extern "C"

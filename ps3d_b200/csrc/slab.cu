@@ -16,7 +16,10 @@
 //   transpose   all-to-all: each rank receives every rank's levels of its own
 //               columns, i.e. whole columns [nz][ccnt] (pressure_solver.f90
 //               needs the full column for the tridiagonal solve)
-//   vsolve      the Thomas solves of those columns (k_thomas on a column slab)
+//   vsolve      the vertical solves of those columns: the Thomas solves
+//               (rigid lid) or the z transform, division and inverse z
+//               transform (triply periodic, pressure_solver.f90:58-70) on a
+//               column slab
 //   transpose   all-to-all back, unpacked into [nzl][kx][ky]
 //   inverse     per-level inverse 2D transforms into p (pending correction)
 //   p halo      p one level below and two above (the step kernel's lazy
@@ -32,8 +35,10 @@
 // and nzl+2 (the second only for p).  The transport between ranks is the
 // caller's: NCCL all-to-all and send/receive between processes (the Python
 // driver, ps3d_b200/slab.py), or ps3d_slab_group_step for contexts in one
-// process, which copies device to device.  Supported: rigid lid, FP64 and
-// mixed, the fused step (Laplacian friction, no biharmonic, no forcing).
+// process, which copies device to device.  Supported: rigid lid or triply
+// periodic, FP64 and mixed, the fused step (Laplacian friction, no
+// biharmonic, no forcing).
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -55,6 +60,10 @@ struct ps3d_slab {
     void* hrecv = nullptr;          // halo planes received: [from below][from above]
     bool need_halo = true;          // state halos not yet exchanged (after an upload)
     bool mixed = false;             // FP32 spectra, residual solves
+    bool rigid = true;
+    double Lz = 0.0;                // the global grid's depth
+    ps3d::DevPlan plz;              // triply periodic: the global z transform
+    DevBuf hkz;                     // ... and hat_ksqr(kz)/dsqr of the global levels
     int pass = 0;                   // solve pass: 0 full solve, 1 residual solve (mixed path)
 
     // solve passes of the next step: 1 in FP64; in the mixed path 2 on a cold
@@ -133,7 +142,7 @@ int slab_forward(ps3d_slab* s) {
     a.u = c.field(0); a.v = c.field(1); a.w = c.field(2);
     a.pc = s->pass ? (const double*)c.p.p : nullptr;
     a.dtp = c.P.dt; a.dtwp = c.P.dt / c.P.dsqr;
-    a.rigid = 1;
+    a.rigid = s->rigid;
     a.rdt = 1.0 / c.P.dt;
     a.scale = c.P.dx * c.P.dy;
     a.spec = c.FS.p;
@@ -154,10 +163,16 @@ int slab_vsolve(ps3d_slab* s) {
     a.batch = 1; a.sM = (long)s->nzg * s->ccnt[s->rank];
     a.layout = ps3d::spectral_layout(s->mixed ? c.pa32 : c.pa64);
     a.hkx = (const double*)c.t_hkx.p; a.hky = (const double*)c.t_hky.p;
-    a.fxa = 1.0 / (c.P.dz * c.P.dz) / c.P.dsqr;
-    a.dz2dsqr = c.P.dz * c.P.dz * c.P.dsqr;
     a.col0 = s->cbeg[s->rank]; a.ncl = s->ccnt[s->rank];
     a.err = c.kerr_d;
+    if (!s->rigid) {
+        a.hkz = (const double*)s->hkz.p;
+        a.pz = s->plz.plan; a.scale = c.P.dz; a.op = 0;
+        CK(ps3d::launch_zsolve(a, s->mixed, c.stream));
+        return PS3D_OK;
+    }
+    a.fxa = 1.0 / (c.P.dz * c.P.dz) / c.P.dsqr;
+    a.dz2dsqr = c.P.dz * c.P.dz * c.P.dsqr;
     CK(ps3d::launch_thomas(a, s->mixed, c.stream));
     return PS3D_OK;
 }
@@ -173,7 +188,7 @@ int slab_inverse(ps3d_slab* s) {
     b.spec = c.FS.p;
     b.out = (double*)c.p.p;
     b.beta = s->pass ? 1.0 : 0.0;   // the residual pass adds its pressure
-    b.scale = 1.0 / (c.P.Lx * c.P.Ly);
+    b.scale = s->rigid ? 1.0 / (c.P.Lx * c.P.Ly) : 1.0 / (c.P.Lx * c.P.Ly * s->Lz);
     CK(ps3d::launch_plane_inv(b, s->mixed, c.stream));
     if (++s->pass >= (s->mixed ? 2 : 1)) {
         c.pending = true;
@@ -296,12 +311,16 @@ PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, i
     SGUARD_BEGIN
     if (!global || !out || nranks < 1 || rank < 0 || rank >= nranks) return PS3D_ERR_BADPARAM;
     *out = nullptr;
-    if (!global->enable_vertical_boundaries) return PS3D_ERR_UNSUPPORTED;
     if (global->nz % nranks || global->nz / nranks < 2) return PS3D_ERR_BADPARAM;
+    const bool rigid = global->enable_vertical_boundaries != 0;
+    if (!rigid && (global->nz % 2 || !ps3d::fft_length_ok(global->nz) || !ps3d::zsolve_fits(global->nz, false)))
+        return PS3D_ERR_BADPARAM;
     std::unique_ptr<ps3d_slab> s(new ps3d_slab());
     s->nranks = nranks; s->rank = rank;
     s->mixed = global->precision == PS3D_MIXED || global->precision == PS3D_MIXED_REFINED;
     s->nzg = global->nz; s->nzl = global->nz / nranks; s->k0 = rank * s->nzl;
+    s->rigid = rigid;
+    s->Lz = global->Lz;
     ps3d_params lp = *global;
     lp.nz = s->nzl + 3;
     lp.Lz = global->dz * lp.nz;   // keeps dz; the local grid's own Lz is not used by the slab phases
@@ -314,6 +333,18 @@ PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, i
     if (rc) return rc;
     if ((s->mixed ? c.pa32 : c.pa64).impl != 1) return PS3D_ERR_UNSUPPORTED;   // grid the rows + y-lines kernels cannot take
     c.use_graphs = false;
+    if (!rigid) {
+        // the global z transform and its wavenumbers (my_fft.f90:87-156)
+        CK(s->plz.build(s->nzg, 0));
+        const double pi = std::acos(0.0) * 2.0, dz = global->dz, Lz = global->Lz;
+        std::vector<double> hk(s->nzg);
+        for (int k = 1; k <= s->nzg; ++k) {
+            const double kz = k <= (s->nzg + 1) / 2 ? 2 * (k - 1) * pi / Lz : -(2 * (s->nzg - k + 1) * pi / Lz);
+            hk[k - 1] = 2.0 * (1.0 - std::cos(kz * dz)) / (dz * dz) / global->dsqr;
+        }
+        CK(s->hkz.alloc(hk.size() * sizeof(double)));
+        CK(cudaMemcpy(s->hkz.p, hk.data(), hk.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     s->ncols = (long)c.nxh * c.ny;
     s->plane = (long)c.nx * c.ny;
     for (int r = 0; r < nranks; ++r) {

@@ -37,6 +37,7 @@ def _lib():
         L.ps3d_server_stats.argtypes = [vp, dp]
         L.ps3d_server_footprint.restype = C.c_longlong
         L.ps3d_server_footprint.argtypes = [C.POINTER(Params)]
+        L.ps3d_server_set_batching.argtypes = [vp, C.c_int]
         L._srv_ready = True
     return L
 
@@ -52,7 +53,7 @@ class Result:
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget_bytes=0, max_active=4):
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=4, max_batch=1):
         self.L = _lib()
         h = C.c_void_p()
         rc = self.L.ps3d_server_create(device, hbm_budget_bytes, max_active, C.byref(h))
@@ -60,6 +61,15 @@ class Server:
             raise PS3DError(rc, "ps3d_server_create")
         self.h = h
         self._params = {}
+        if max_batch > 1:
+            self.set_batching(max_batch)
+
+    def set_batching(self, max_batch):
+        """Run up to max_batch queued same-parameter optimal balances as the
+        instances of one batched context (shared launches)."""
+        rc = self.L.ps3d_server_set_batching(self.h, int(max_batch))
+        if rc:
+            raise PS3DError(rc, "ps3d_server_set_batching")
 
     def close(self):
         if getattr(self, "h", None):

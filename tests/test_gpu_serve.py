@@ -232,3 +232,62 @@ def test_ensemble_request_refused_when_it_can_never_fit():
         s.submit_ensemble(members, states, 5)
     assert ei.value.status == abi.PS3D_ERR_OOM
     s.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_batched_requests_match_alone(precision, monkeypatch):
+    """Same-parameter requests admitted together run as the instances of one
+    batched context (shared launches).  Each gets bit for bit its result
+    alone: iterations, norm and balanced fields, including a request whose
+    loop ends at an earlier iteration than its neighbours' (per-instance
+    convergence), and a request cancelled while its group runs on."""
+    monkeypatch.setenv("PS3D_AUTOTUNE", "0")   # the same (default) kernel shapes for every batch size
+    p, opt, f = _req((32, 32, 16), ramp=6, iters=4, precision=precision)
+    states = [f] + [{k: v * a for k, v in f.items()} for a in (1.7, 0.6, 2.5)]
+    # a tolerance met at iteration 2 by the first state alone
+    o2 = abi.OptBal(period=opt.period, average=0.0, max_itts=2, average_times=1, tol=0.0, enable_time_ave=0,
+                    adopt=0)
+    s = Server(max_active=1)
+    first2 = s.wait(s.submit(p, o2, states[0]))
+    opt.tol = first2.norm * (1 + 1e-9)
+    alone = [s.wait(s.submit(p, opt, st)) for st in states]
+    s.close()
+    assert alone[0].iters == 2 and all(r.status == 0 for r in alone)
+    s = Server(max_active=1, max_batch=4)
+    blocker = s.submit(*_req((64, 32, 16)))   # holds the slot while the four queue up
+    tks = [s.submit(p, opt, st) for st in states]
+    assert s.wait(blocker).status == 0
+    got = [s.wait(t) for t in tks]
+    s.close()
+    for a, g in zip(alone, got):
+        assert g.status == 0 and g.iters == a.iters and g.norm == a.norm, (g.status, g.iters, a.iters)
+        for n in ("u", "v", "w", "b"):
+            assert np.array_equal(g.fields[n], a.fields[n]), n
+    # they shared one context: the queue time of the last equals that of the first
+    assert abs(got[-1].queue_ms - got[0].queue_ms) < 50.0
+
+
+def test_batched_group_member_cancelled_and_nonfinite(monkeypatch):
+    """In a batched group a cancelled member reports PS3D_ERR_CANCELLED and
+    a member whose state turns non-finite fails alone; the others finish
+    with their results alone."""
+    monkeypatch.setenv("PS3D_AUTOTUNE", "0")
+    p, opt, f = _req((32, 32, 16), ramp=30, iters=3)
+    bad = {k: v.copy() for k, v in f.items()}
+    bad["u"][5, 5, 5] = np.nan
+    s = Server(max_active=1)
+    ref = s.wait(s.submit(p, opt, f))
+    s.close()
+    s = Server(max_active=1, max_batch=3)
+    blocker = s.submit(*_req((64, 32, 16)))
+    t_ok, t_bad, t_cancel = s.submit(p, opt, f), s.submit(p, opt, bad), s.submit(p, opt, f)
+    import time
+    while s.stats()["queued"] > 0:   # the group is admitted once the blocker ends
+        time.sleep(0.005)
+    s.cancel(t_cancel)
+    assert s.wait(blocker).status == 0
+    ok, nf, cn = s.wait(t_ok), s.wait(t_bad), s.wait(t_cancel)
+    s.close()
+    assert ok.status == 0 and ok.norm == ref.norm
+    assert nf.status == abi.PS3D_ERR_NONFINITE
+    assert cn.status == abi.PS3D_ERR_CANCELLED

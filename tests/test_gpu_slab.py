@@ -2,7 +2,7 @@
 
 The slab phases (the step kernel on a level window, the per-level 2D
 transforms, the all-to-all transposes to column slabs, the column-slab
-Thomas solves, the halo planes) must reproduce the single-grid engine: the
+vertical solves, the halo planes) must reproduce the single-grid engine: the
 arithmetic per level and per column is the same, so the tolerance is the
 single-kernel one.  Ranks run as contexts of one process on one GPU, moved
 between by device copies (ps3d_slab_group_step); no kernel waits on another.
@@ -109,11 +109,50 @@ def test_mixed_slabs_match_single_grid(nranks, precision, monkeypatch):
     assert max(err.values()) < 1e-10, err
 
 
-def test_slab_rejects_periodic():
-    p = small_params(32, 32, 16, rigid=False)
+@pytest.mark.parametrize("precision,tol", [(abi.PS3D_FP64, TOL), (abi.PS3D_MIXED, 1e-10)])
+@pytest.mark.parametrize("nranks", [1, 2, 4])
+def test_periodic_slabs_match_single_grid(nranks, precision, tol, monkeypatch):
+    """Triply periodic grids: the halo planes wrap from the top rank to the
+    bottom one, and the column slabs run the z transform, the spectral
+    division and the inverse z transform (pressure_solver.f90:58-70) on
+    whole columns of the global grid."""
+    monkeypatch.setenv("PS3D_TUNE", "im1,C1,rc8,tj16,ly16,pol0,kc8")
+    p = small_params(64, 32, 32, rigid=False, precision=precision)
+    f = random_state(p, seed=13, amp=0.05)
+    ref = _single(p, f, 6, monkeypatch)
+    g = SlabGroup(p, nranks)
+    g.upload(*[_interior(f[n]) for n in "uvwb"])
+    g.step(6)
+    got = g.download()
+    g.close()
+    err = {n: rel(got[n], ref[n]) for n in NAMES}
+    assert max(err.values()) < tol, err
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+def test_slabs_match_oracle(rigid):
+    """Four slabs of one grid against the CPU oracle, 10 AB3 steps."""
+    from oracle.binding import Oracle
+    p = small_params(32, 32, 16, rigid=rigid)
+    f = random_state(p, seed=17, amp=0.05)
+    o = Oracle(p)
+    for n in "uvwb":
+        o.field(n)[...] = f[n]
+    o.integrate(10)
+    g = SlabGroup(p, 4)
+    g.upload(*[_interior(f[n]) for n in "uvwb"])
+    g.step(10)
+    got = g.download()
+    g.close()
+    err = {n: rel(got[n], _interior(o.field(n))) for n in NAMES}
+    assert max(err.values()) < 1e-11, err
+
+
+def test_slab_rejects_periodic_depth_without_fft():
+    p = small_params(32, 32, 22, rigid=False)   # 22 = 2 x 11: no FFT plan of that length
     with pytest.raises(PS3DError) as e:
         Slab(p, 2, 0)
-    assert e.value.status == abi.PS3D_ERR_UNSUPPORTED
+    assert e.value.status == abi.PS3D_ERR_BADPARAM
 
 
 def test_slab_rejects_uneven_levels():
