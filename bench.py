@@ -460,6 +460,15 @@ def serve_run(dev, n_requests=40, rate_hz=50.0, max_active=8, max_batch=8):
         r["peak_active"] = srv.stats()["peak_active"]
         srv.close()
         out[name] = r
+    # small requests only (64x64x32), where a request alone leaves the GPU idle
+    small = poisson_schedule(n_requests, rate_hz, seed=5, sizes=[(64, 64, 32)])
+    out["small_64x64x32"] = {}
+    for name, mb in (("mixed", 1), ("mixed_batched", max_batch)):
+        srv = Server(device=dev, max_active=max_active, max_batch=mb)
+        r = replay_poisson(srv, small, precision=abi.PS3D_MIXED)
+        r["peak_active"] = srv.stats()["peak_active"]
+        srv.close()
+        out["small_64x64x32"][name] = r
     return out
 
 

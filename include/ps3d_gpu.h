@@ -402,10 +402,12 @@ PS3D_API int ps3d_server_cancel(ps3d_server* s, long long ticket);
  * identical are admitted together and run as instances of one batched
  * context (every kernel launch advances all of them; each keeps its own
  * norm, iteration count and result, bit for bit what it gets alone with the
- * same kernel shapes).  Their footprint is the sum of theirs.  1 (the
- * default) runs every request on its own context.  Requests with
- * biharmonic friction always run alone.                                    */
-PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch);
+ * same kernel shapes), as long as their grid points together stay within
+ * max_points (0: 2^22; larger grids already fill the GPU alone and run
+ * side by side on their own streams instead).  Their footprint is the sum
+ * of theirs.  max_batch 1 (the default) runs every request on its own
+ * context.  Requests with biharmonic friction always run alone.           */
+PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch, long long max_points);
 /* stats[6] = {active, queued, bytes in use, peak bytes, peak active, budget} */
 PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats);
 PS3D_API long long ps3d_server_footprint(const ps3d_params* prm);

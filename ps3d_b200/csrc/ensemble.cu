@@ -4,9 +4,12 @@
 // Members with identical parameters (same grid, physics and time step) form
 // one group; a group is a batched context whose kernels carry the member
 // index in their grid, so one launch of each kernel advances every member of
-// the group.  All groups share one stream, and for constant parameters three
-// consecutive steps of every group are captured into a single CUDA graph that
-// is replayed (tau and the state buffers cycle with period 3).
+// the group.  Each group runs on its own stream, forked from the ensemble's
+// stream and joined back at every step, so the groups' kernels (which share
+// no data) run side by side on the GPU; for constant parameters three
+// consecutive steps of every group are captured into a single CUDA graph —
+// one branch per group — that is replayed (tau and the state buffers cycle
+// with period 3).
 #include <cstring>
 #include <memory>
 #include <new>
@@ -19,6 +22,8 @@ struct ps3d_ensemble {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::vector<std::unique_ptr<Ctx>> groups;
+    cudaEvent_t fork = nullptr;              // the ensemble stream's point the groups start from
+    std::vector<cudaEvent_t> joins;          // each group's end of a step
     std::vector<std::pair<int, int>> where;   // member -> (group, index in group)
     cudaGraphExec_t gexec = nullptr;
     bool graph_valid = false;
@@ -26,6 +31,8 @@ struct ps3d_ensemble {
     ~ps3d_ensemble() {
         if (gexec) cudaGraphExecDestroy(gexec);
         groups.clear();
+        if (fork) cudaEventDestroy(fork);
+        for (cudaEvent_t j : joins) cudaEventDestroy(j);
         if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
     }
 };
@@ -34,13 +41,20 @@ namespace {
 
 bool same_params(const ps3d_params& a, const ps3d_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
 
+// one step of every group: each group's stream waits for the ensemble
+// stream, runs its step, and the ensemble stream waits for every group
 int step_all(ps3d_ensemble* e) {
-    for (auto& g : e->groups) {
-        int rc = g->step(g->itt, g->tau, g->taum1, g->taum2);
+    if (cudaEventRecord(e->fork, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+    for (size_t q = 0; q < e->groups.size(); ++q) {
+        Ctx& g = *e->groups[q];
+        if (cudaStreamWaitEvent(g.stream, e->fork, 0) != cudaSuccess) return PS3D_ERR_CUDA;
+        int rc = g.step(g.itt, g.tau, g.taum1, g.taum2);
         if (rc) return rc;
-        g->rotate();
-        g->time = g->time + g->P.dt;
-        ++g->itt;
+        g.rotate();
+        g.time = g.time + g.P.dt;
+        ++g.itt;
+        if (cudaEventRecord(e->joins[q], g.stream) != cudaSuccess) return PS3D_ERR_CUDA;
+        if (cudaStreamWaitEvent(e->stream, e->joins[q], 0) != cudaSuccess) return PS3D_ERR_CUDA;
     }
     ++e->itt;
     return PS3D_OK;
@@ -120,6 +134,11 @@ int advance(ps3d_ensemble* e, int nsteps) {
         if (rc) return rc;
         --nsteps;
     }
+    // what a group's stream runs next (an upload, a download) waits for
+    // everything queued so far, graph replays included
+    if (cudaEventRecord(e->fork, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+    for (auto& g : e->groups)
+        if (cudaStreamWaitEvent(g->stream, e->fork, 0) != cudaSuccess) return PS3D_ERR_CUDA;
     return PS3D_OK;
 }
 
@@ -162,12 +181,16 @@ int ps3d::ensemble_create(const ps3d_params* members, int n, int device, bool tu
         if (gid[m] < 0) { gid[m] = (int)leader.size(); leader.push_back(m); count.push_back(0); }
         e->where.push_back({gid[m], count[gid[m]]++});
     }
+    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) return PS3D_ERR_CUDA;
     for (size_t q = 0; q < leader.size(); ++q) {
         std::unique_ptr<Ctx> c(new Ctx());
         c->tune_timing = tune;
-        int rc = c->init(members[leader[q]], device, count[q], e->stream);
+        int rc = c->init(members[leader[q]], device, count[q]);   // on a stream of its own
         if (rc) return rc;
         e->groups.push_back(std::move(c));
+        cudaEvent_t j = nullptr;
+        if (cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess) return PS3D_ERR_CUDA;
+        e->joins.push_back(j);
     }
     *out = e.release();
     return PS3D_OK;

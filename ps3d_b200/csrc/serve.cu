@@ -103,6 +103,7 @@ struct ps3d_server {
     size_t budget = 0, used = 0, peak_used = 0;
     int max_active = 1, active = 0, peak_active = 0;
     int max_batch = 1;          // same-parameter requests run together (ps3d_server_set_batching)
+    long batch_points = 1L << 22;   // ... while the group's grid points stay within this
     long long next_id = 1;
     bool stopping = false;
     std::mutex mu;
@@ -240,15 +241,21 @@ void ps3d_server::worker_loop() {
                 if (!queue.empty() && active < max_active) {
                     const std::shared_ptr<Request>& q = queue.front();
                     std::vector<std::shared_ptr<Request>> cand{q};
+                    const long qpts = (long)q->prm.nx * q->prm.ny * q->prm.nz;
                     if (max_batch > 1 && batchable(*q))
-                        for (size_t k = 1; k < queue.size() && (int)cand.size() < max_batch; ++k)
+                        for (size_t k = 1; k < queue.size() && (int)cand.size() < max_batch &&
+                                           (long)(cand.size() + 1) * qpts <= batch_points;
+                             ++k)
                             if (batchable(*queue[k]) && same_params(queue[k]->prm, q->prm) &&
                                 same_opt(queue[k]->opt, q->opt))
                                 cand.push_back(queue[k]);
-                    // the largest group whose footprint fits, given what idle contexts could free
+                    // the largest group whose footprint fits, given what idle contexts could
+                    // free, of a power-of-two size: a finished group's context then serves
+                    // later groups of the same parameters (the pool matches the batch)
                     size_t idle_bytes = 0;
                     for (const IdleCtx& ic : idle) idle_bytes += ic.footprint;
                     while (cand.size() > 1 && used - idle_bytes + cand.size() * q->footprint > budget) cand.pop_back();
+                    while (cand.size() & (cand.size() - 1)) cand.pop_back();
                     const int nb = (int)cand.size();
                     const size_t foot = nb * q->footprint;
                     long hit = -1;
@@ -574,11 +581,12 @@ PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats) {
 
 PS3D_API long long ps3d_server_footprint(const ps3d_params* prm) { return prm ? (long long)footprint_of(*prm) : -1; }
 
-PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch) {
-    if (!s || max_batch < 1) return PS3D_ERR_BADPARAM;
+PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch, long long max_points) {
+    if (!s || max_batch < 1 || max_points < 0) return PS3D_ERR_BADPARAM;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->max_batch = max_batch;
+        s->batch_points = max_points ? (long)max_points : (1L << 22);
     }
     s->cv_work.notify_all();
     return PS3D_OK;

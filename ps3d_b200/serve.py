@@ -37,7 +37,7 @@ def _lib():
         L.ps3d_server_stats.argtypes = [vp, dp]
         L.ps3d_server_footprint.restype = C.c_longlong
         L.ps3d_server_footprint.argtypes = [C.POINTER(Params)]
-        L.ps3d_server_set_batching.argtypes = [vp, C.c_int]
+        L.ps3d_server_set_batching.argtypes = [vp, C.c_int, C.c_longlong]
         L._srv_ready = True
     return L
 
@@ -64,10 +64,11 @@ class Server:
         if max_batch > 1:
             self.set_batching(max_batch)
 
-    def set_batching(self, max_batch):
+    def set_batching(self, max_batch, max_points=0):
         """Run up to max_batch queued same-parameter optimal balances as the
-        instances of one batched context (shared launches)."""
-        rc = self.L.ps3d_server_set_batching(self.h, int(max_batch))
+        instances of one batched context (shared launches), while their grid
+        points together stay within max_points (0: the engine's default)."""
+        rc = self.L.ps3d_server_set_batching(self.h, int(max_batch), int(max_points))
         if rc:
             raise PS3DError(rc, "ps3d_server_set_batching")
 

@@ -278,16 +278,18 @@ def test_batched_group_member_cancelled_and_nonfinite(monkeypatch):
     s = Server(max_active=1)
     ref = s.wait(s.submit(p, opt, f))
     s.close()
-    s = Server(max_active=1, max_batch=3)
+    s = Server(max_active=1, max_batch=4)
     blocker = s.submit(*_req((64, 32, 16)))
     t_ok, t_bad, t_cancel = s.submit(p, opt, f), s.submit(p, opt, bad), s.submit(p, opt, f)
+    t_ok2 = s.submit(p, opt, f)   # a group of four
     import time
     while s.stats()["queued"] > 0:   # the group is admitted once the blocker ends
         time.sleep(0.005)
     s.cancel(t_cancel)
     assert s.wait(blocker).status == 0
-    ok, nf, cn = s.wait(t_ok), s.wait(t_bad), s.wait(t_cancel)
+    ok, nf, cn, ok2 = s.wait(t_ok), s.wait(t_bad), s.wait(t_cancel), s.wait(t_ok2)
     s.close()
     assert ok.status == 0 and ok.norm == ref.norm
+    assert ok2.status == 0 and ok2.norm == ref.norm
     assert nf.status == abi.PS3D_ERR_NONFINITE
     assert cn.status == abi.PS3D_ERR_CANCELLED
