@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <atomic>
+#include <memory>
 #include <string>
 #include <vector>
 #include "engine.h"
@@ -58,6 +59,8 @@ struct DevPlan {
 bool fft_length_ok(int n);
 
 enum { kSetSave = 10, kSetAve = 11, kSetSave2 = 12, kSetPT0 = 13, kSetComb = 14 };
+
+struct RampGraph;   // a captured ramped integration (engine.cu)
 
 struct Ctx {
     ps3d_params P{};
@@ -121,11 +124,14 @@ struct Ctx {
     cudaStream_t snap_stream = nullptr;
     cudaEvent_t snap_event = nullptr;
     int warn_filter = -1;
+    // ramp graphs of the optimal balance (engine.cu), kept across calls
+    std::shared_ptr<std::vector<RampGraph>> ramp_graphs;
     DevBuf saved_p, saved_tend[4];
     // tables
     DevPlan plx, ply, plz;      // radix-16/8 schedules
     DevPlan plx4, ply4;         // radix-4 schedules (autotuner alternative)
     DevPlan plx8, ply8;         // radix-8 schedules (autotuner alternative)
+    DevPlan plyh;               // length ny/2 (the y-split solve, k_colsolve)
     int plane_force = -1;       // PS3D_PLANE_IMPL: -1 free, 0 cluster, 1 rows + y-lines
     int force_impl = -1;        // set before init: pins the plane implementation (z-slabs: 1)
     // z-slab of a larger grid (slab.cu): the step kernel advances levels
@@ -142,6 +148,7 @@ struct Ctx {
     PlaneArgs pa64{}, pa32{};
     // forcing
     int fkind = 0;
+    long forcing_gen = 0;     // counts set_forcing calls (keys of the ramp graphs)
     double omega = 0.0;
     DevBuf wr[4], wi[4], ub, bb;
     ps3d_forcing_fn fn = nullptr;

@@ -391,6 +391,26 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     CK(cudaStreamSynchronize(stream));
     int rc = autotune();
     if (rc) return rc;
+    // the y-split solve (k_colsolve) for the mixed rigid-lid path, with
+    // PS3D_YSPLIT=1, where the register rows passes and its shared memory
+    // take the grid (not for z-slabs, whose column slabs take the natural
+    // layout).  Off by default: at 256x256x128 it measured 486 us per step
+    // against 468 us for the y-lines passes and k_thomas2 (one 183 KB block
+    // per SM leaves its vertical solves eight warps to hide the FP64 chain)
+    {
+        const char* ys = std::getenv("PS3D_YSPLIT");
+        const bool want = ys && ys[0] == '1';
+        if (want && mixed && rigid && !split_solve && pa32.impl == 1 && rows_in_registers(nx, ny) &&
+            colsolve_fits(nz, ny) && fft_length_ok(ny / 2)) {
+            CK(plyh.build(ny / 2, 0));
+            int mr = 1;
+            for (int q = 0; q < plyh.plan.nst; ++q) mr = std::max(mr, plyh.plan.r[q]);
+            if (mr <= 16) {
+                pa32.ysplit = 1;
+                pa32.pyh = plyh.plan;
+            }
+        }
+    }
     // PS3D_GRAPHS=0: no CUDA-graph replay of the main loop (eager launches)
     if (const char* g = std::getenv("PS3D_GRAPHS"))
         if (g[0] == '0') use_graphs = false;
@@ -838,7 +858,11 @@ int Ctx::poisson_once(double* out, double beta, bool lazy, const double* pc) {
     c.batch = batch; c.sM = M; c.layout = spectral_layout(a);
     c.hkx = (const double*)t_hkx.p; c.hky = (const double*)t_hky.p; c.hkz = (const double*)t_hkz_ds.p;
     c.err = kerr_d;
-    if (rigid) {
+    if (rigid && a.ysplit) {
+        c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
+        c.dz2dsqr = P.dz * P.dz * P.dsqr;
+        LAUNCH(PS3D_K_VSOLVE, launch_colsolve(a, c, stream));
+    } else if (rigid) {
         c.fxa = 1.0 / (P.dz * P.dz) / P.dsqr;
         c.dz2dsqr = P.dz * P.dz * P.dsqr;
         LAUNCH(PS3D_K_VSOLVE, launch_thomas(c, f32, stream));
@@ -1076,8 +1100,16 @@ int Ctx::opt_time_ave(int set, int n_end_ave) {
 // time levels, so the steps are captured once per starting state (buffer
 // phase, pending correction) into a CUDA graph, with each step's Ro in its
 // kernel arguments, and replayed: one launch per ramp instead of several per
-// step, which keeps concurrent serving requests off the launch path.
+// step, which keeps concurrent serving requests off the launch path.  The
+// graphs stay with the context (Ctx::ramp_graphs), keyed by everything they
+// bake in — the parameters, the ramp and the starting state — so a context
+// that serves request after request with the same parameters (the serving
+// pool) replays them without capturing again.
 struct RampGraph {
+    ps3d_params P_at{};   // the step parameters at capture (Ro excepted: ramped)
+    long forcing_gen = 0;
+    int n_end = 0;
+    double Ro_loc = 0.0, dt_loc = 0.0, period = 0.0;
     cudaGraphExec_t exec = nullptr;
     bool backward = false;
     int cur_in[4] = {0, 0, 0, 0}, cur_out[4] = {0, 0, 0, 0};
@@ -1107,14 +1139,20 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
         }
         return rc;
     }
+    ps3d_params Pk = P;
+    Pk.Ro = 0.0;
     RampGraph* g = nullptr;
     for (RampGraph& c : cache)
         if (c.backward == backward && std::equal(c.cur_in, c.cur_in + 4, cur) && c.pend_in == pending &&
-            c.pcor_in == pcor && c.dtp_in == dtp && c.warm_in == p_warm)
+            c.pcor_in == pcor && c.dtp_in == dtp && c.warm_in == p_warm && c.n_end == n_end && c.Ro_loc == Ro_loc &&
+            c.dt_loc == dt_loc && c.period == period && c.forcing_gen == forcing_gen &&
+            std::memcmp(&c.P_at, &Pk, sizeof(Pk)) == 0)
             g = &c;
     if (!g) {
         RampGraph n;
         n.backward = backward;
+        n.P_at = Pk; n.n_end = n_end; n.Ro_loc = Ro_loc; n.dt_loc = dt_loc; n.period = period;
+        n.forcing_gen = forcing_gen;
         std::copy(cur, cur + 4, n.cur_in);
         n.pend_in = pending; n.pcor_in = pcor; n.dtp_in = dtp; n.warm_in = p_warm;
         const int itt0 = itt, tau0 = tau, t10 = taum1, t20 = taum2;
@@ -1156,6 +1194,13 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
     return PS3D_OK;
 }
 
+void release_ramp_graphs(std::vector<RampGraph>* g) {
+    if (!g) return;
+    for (RampGraph& r : *g)
+        if (r.exec) cudaGraphExecDestroy(r.exec);
+    delete g;
+}
+
 int Ctx::reset_request() {
     itt = 0; tau = 3; taum1 = 2; taum2 = 1; time = 0.0;
     pending = false; pcor = nullptr; dtp = 0.0;
@@ -1193,11 +1238,8 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
     int nrun = batch;
     if (batch > 1 && norms.bytes < (size_t)batch * 4 * sizeof(double)) CK(norms.alloc((size_t)batch * 4 * sizeof(double)));
     int rc = PS3D_OK;
-    std::vector<RampGraph> graphs;   // ramp graphs of this call (ramp_run)
-    struct Release {
-        std::vector<RampGraph>& g;
-        ~Release() { for (RampGraph& r : g) if (r.exec) cudaGraphExecDestroy(r.exec); }
-    } release{graphs};
+    if (!ramp_graphs) ramp_graphs = std::shared_ptr<std::vector<RampGraph>>(new std::vector<RampGraph>(), release_ramp_graphs);
+    std::vector<RampGraph>& graphs = *ramp_graphs;   // ramp graphs of this context (ramp_run)
     if (O.enable_time_ave) {
         for (int m = 1; m <= O.average_times && !rc; ++m) {
             rc = opt_time_ave(PS3D_FIELDS_BASE, n_end_ave);
@@ -1367,6 +1409,7 @@ int Ctx::download_tend(int f, double* h) {
 
 int Ctx::set_forcing(const ps3d_forcing* f) {
     invalidate_graph();
+    ++forcing_gen;   // ramp graphs captured with the old forcing no longer apply
     fkind = 0; fn = nullptr; user = nullptr;
     if (!f || f->kind == PS3D_FORCE_NONE) return PS3D_OK;
     if (f->kind & ~(PS3D_FORCE_WAVEMAKER | PS3D_FORCE_BACKGROUND | PS3D_FORCE_CALLBACK)) return PS3D_ERR_BADPARAM;
@@ -1628,7 +1671,7 @@ int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
     const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
     std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_impl=%s plane_cluster=%d row_chunk=%d tj=%d ly=%d "
                   "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.refine_full ? "mixed_refined" : C.mixed ? "mixed" : "fp64",
-                  C.batch, pa.impl == 2 ? "pipe+lines" : pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
+                  C.batch, pa.impl == 2 ? "pipe+lines" : pa.ysplit ? "rows+colsolve" : pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
                   C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
     return PS3D_OK;
 }

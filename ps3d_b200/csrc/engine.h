@@ -101,6 +101,12 @@ struct PlaneArgs {
     // 0 .. kcount-1; the rigid-lid masks see the global level k + kofs of nzg
     int kbeg, kcount, kofs, nzg;
     int l2hint;                    // L2 eviction priorities on (set by the launchers; PS3D_L2HINT=0: off)
+    // implementation 1 with the register rows passes only: the rows passes
+    // apply the first radix-2 stage of the y transform and the spectra are
+    // [k][kx][half][ny/2] (even ky, then odd); the y-lines passes and the
+    // vertical solve are then one kernel, k_colsolve (launch_colsolve)
+    int ysplit;
+    FFTPlan pyh;                   // ysplit: the half-length y plan (length ny/2)
 };
 // spectral layout of a plane configuration: 0 [k][ky][kx], 1 [k][kx][ky]
 inline int spectral_layout(const PlaneArgs& a) { return a.impl != 0; }
@@ -164,6 +170,10 @@ int plane_max_clusters(const PlaneArgs& a, bool fp32, bool fwd);
 // the shared memory of a block (thomas_threads(nz) == 0)
 cudaError_t launch_thomas(const ColumnArgs& a, bool fp32, cudaStream_t s);
 int thomas_threads(int nz);
+// the y transforms and the rigid-lid vertical solve on the y-split layout
+// (FP32 spectra); p: the forward plane arguments (scale, half-length plan)
+cudaError_t launch_colsolve(const PlaneArgs& p, const ColumnArgs& c, cudaStream_t s);
+bool colsolve_fits(int nz, int ny);
 // periodic z solve; zsolve_fits(nz, fp32) false: too tall for a block's shared memory
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
 bool zsolve_fits(int nz, bool fp32);

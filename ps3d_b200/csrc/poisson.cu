@@ -627,6 +627,169 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
 }
 
 // ---------------------------------------------------------------------------
+// K3 with the y transforms, on the y-split layout (PlaneArgs::ysplit): one
+// block per (instance, kx, half) holds that half-line's nz x ny/2 spectra
+// in shared memory, as [j][k] with an odd pitch, and runs
+//   the forward half-length y transforms of its nz levels (DIF, staying in
+//     digit-reversed order, scaled by dx dy as the y-lines pass scales),
+//   the rigid-lid vertical solves of its ny/2 columns — the two-ended FP64
+//     elimination of k_thomas2, one thread per (column, part), (c', d', d'')
+//     checkpointed every kT2KC levels, each chunk re-formed on the way back —
+//     and the (0,0) recurrence,
+//   the inverse half-length y transforms (DIT, back to natural order),
+// so the spectral array crosses memory once in and once out instead of six
+// times, and three kernels become one.  Column j of a half sits at ky =
+// 2 j + half.
+// ---------------------------------------------------------------------------
+constexpr int kCsThreads = 256;
+constexpr int kCsKC = 8;
+
+struct ColSolveArgs {
+    int nz, ny, nxh;
+    void* spec;                    // [inst][k][kx][half][ny/2], float2
+    long sM;                       // instance stride (elements)
+    int batch;
+    FFTPlan ph;                    // length ny/2
+    double scale;                  // forward y-transform scale (dx dy)
+    const double* hkx;             // hat_ksqr(kx)
+    const double* hky;             // hat_ksqr(ky)
+    double fxa, dz2dsqr;           // 1/dz^2/dsqr, dz^2 dsqr
+    int l2hint;
+};
+
+PS3D_HD size_t colsolve_smem(int nz, int ny) {
+    const int ny2 = ny / 2, H = (nz + 1) / 2, nch = (H + kCsKC - 1) / kCsKC;
+    return align16((size_t)ny2 * (nz | 1) * sizeof(float2)) +
+           align16((size_t)nch * 3 * kCsThreads * sizeof(double)) + plan_tables_bytes(ny2, sizeof(float2));
+}
+
+__global__ void __launch_bounds__(kCsThreads) k_colsolve(const ColSolveArgs a) {
+    using T = float2;
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
+    extern __shared__ __align__(16) unsigned char cs_raw[];
+    const int nz = a.nz, ny = a.ny, ny2 = ny / 2, nxh = a.nxh;
+    const int ld = nz | 1;
+    const int H = (nz + 1) / 2, Bc = nz - H, m = H - 1, jb = Bc - 1;
+    const int nch = (H + kCsKC - 1) / kCsKC;
+    T* buf = reinterpret_cast<T*>(cs_raw);                                        // [j][k], pitch ld
+    double* ck = reinterpret_cast<double*>(cs_raw + align16((size_t)ny2 * ld * sizeof(T)));   // [chunk][3][thread]
+    const PlanTables<float> ty = stage_plan<float>(
+        a.ph, cs_raw + align16((size_t)ny2 * ld * sizeof(T)) + align16((size_t)nch * 3 * kCsThreads * sizeof(double)));
+    const int units = nxh * 2;
+    const int inst = blockIdx.x / units, u = blockIdx.x - inst * units;
+    const int kx = u >> 1, half = u & 1;
+    T* g = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kx * ny + half * ny2;
+    const long ls = (long)nxh * ny;   // level stride
+    const unsigned long long pk = pol_keep(a.l2hint), pl = pol_last(a.l2hint);
+    const float sc = (float)a.scale;
+    for (int t = threadIdx.x; t < nz * ny2; t += kCsThreads) {
+        const int k = t / ny2, j = t - k * ny2;
+        buf[j * ld + k] = cscale(ld_l2(&g[(long)k * ls + j], pl), sc);
+    }
+    fft_batch<false, float, 16>(buf, ld, nz, a.ph, -1, ty.tw);   // synchronises before and after
+    // ---- vertical solves: thread (column p, part)
+    const int tid = threadIdx.x;
+    float* bf = reinterpret_cast<float*>(buf);
+    for (int p0 = 0; p0 < ny2; p0 += kCsThreads / 2) {
+        const int p = p0 + (tid >> 1), part = tid & 1;
+        if (p < ny2) {
+            float* col = bf + (size_t)p * ld * 2 + part;   // level k at col[2 k]
+            const int ky = 2 * ty.ipos[p] + half;
+            const double ks = a.hkx[kx] + a.hky[ky];
+            const double fxa = a.fxa;
+            if (!(ks > 0)) {
+                // (0,0): p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
+                double x0 = 0.0, x1 = 0.0, fprev = 0.0;
+                for (int k = 0; k < nz; ++k) {
+                    const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * a.dz2dsqr;
+                    fprev = (double)col[2 * k];
+                    x0 = x1; x1 = xk;
+                    col[2 * k] = (float)xk;
+                }
+            } else {
+                const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+                auto elim = [&](int jj, double dt, double db, double& cp, double& dp, double& dq) {
+                    if (jj == 0) {
+                        cp = fxa / bend;
+                        dp = dt / bend;
+                        dq = db / bend;
+                    } else {
+                        const double r = rcp_newton(bmid - cp * fxa);
+                        cp = fxa * r;
+                        dp = (dt - dp * fxa) * r;
+                        if (jj < Bc) dq = (db - dq * fxa) * r;
+                    }
+                };
+                double cp = 0.0, dp = 0.0, dq = 0.0, cp_jb = 0.0, dq_jb = 0.0;
+                for (int ch = 0; ch < nch; ++ch) {
+                    double* c = ck + (size_t)ch * 3 * kCsThreads + tid;
+                    c[0] = cp; c[kCsThreads] = dp; c[2 * kCsThreads] = dq;
+#pragma unroll
+                    for (int q = 0; q < kCsKC; ++q) {
+                        const int jj = ch * kCsKC + q;
+                        if (jj < H) {
+                            elim(jj, (double)col[2 * jj], jj < Bc ? (double)col[2 * (nz - 1 - jj)] : 0.0, cp, dp, dq);
+                            if (jj == jb) { cp_jb = cp; dq_jb = dq; }
+                        }
+                    }
+                }
+                double xt = (dp - cp * dq_jb) / (1.0 - cp * cp_jb);
+                double xb = dq_jb - cp_jb * xt;
+                for (int ch = nch - 1; ch >= 0; --ch) {
+                    const int jc = ch * kCsKC;
+                    const double* c = ck + (size_t)ch * 3 * kCsThreads + tid;
+                    double cpv = c[0], dpv = c[kCsThreads], dqv = c[2 * kCsThreads];
+                    double cpl[kCsKC], dpl[kCsKC], dql[kCsKC];
+#pragma unroll
+                    for (int q = 0; q < kCsKC; ++q) {
+                        const int jj = jc + q;
+                        if (jj < H)
+                            elim(jj, (double)col[2 * jj], jj < Bc ? (double)col[2 * (nz - 1 - jj)] : 0.0, cpv, dpv, dqv);
+                        cpl[q] = cpv; dpl[q] = dpv; dql[q] = dqv;
+                    }
+#pragma unroll
+                    for (int q = kCsKC - 1; q >= 0; --q) {
+                        const int jj = jc + q;
+                        if (jj < H) {
+                            if (jj < m) xt = dpl[q] - cpl[q] * xt;
+                            col[2 * jj] = (float)xt;
+                            if (jj <= jb) {
+                                if (jj < jb) xb = dql[q] - cpl[q] * xb;
+                                col[2 * (nz - 1 - jj)] = (float)xb;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    fft_batch<true, float, 16>(buf, ld, nz, a.ph, +1, ty.tw);
+    for (int t = threadIdx.x; t < nz * ny2; t += kCsThreads) {
+        const int k = t / ny2, j = t - k * ny2;
+        st_l2(&g[(long)k * ls + j], buf[j * ld + k], pk);
+    }
+}
+
+bool colsolve_fits(int nz, int ny) {
+    return ny % 16 == 0 && colsolve_smem(nz, ny) <= 227 * 1024 - 64;
+}
+
+cudaError_t launch_colsolve(const PlaneArgs& p, const ColumnArgs& c, cudaStream_t s) {
+    if (!colsolve_fits(c.nz, c.ny) || plan_max_radix(p.py) > 16) return cudaErrorInvalidValue;
+    ColSolveArgs a{};
+    a.nz = c.nz; a.ny = c.ny; a.nxh = c.nxh;
+    a.spec = c.spec; a.sM = c.sM; a.batch = std::max(1, c.batch);
+    a.ph = p.pyh;
+    a.scale = p.scale;
+    a.hkx = c.hkx; a.hky = c.hky;
+    a.fxa = c.fxa; a.dz2dsqr = c.dz2dsqr;
+    a.l2hint = l2hint_mode();
+    const dim3 g((unsigned)(c.nxh * 2 * a.batch)), b(kCsThreads);
+    return launch_pdl(k_colsolve, g, b, colsolve_smem(c.nz, c.ny), s, a);
+}
+
+// ---------------------------------------------------------------------------
 // K3, triply periodic: z FFT, spectral division, inverse z FFT
 // (pressure_solver.f90:58-70; my_fft_3D/my_ifft_3D z leg)
 // ---------------------------------------------------------------------------
@@ -1026,7 +1189,20 @@ struct RowReg {
     static constexpr size_t elems = T1 > T2 ? T1 : T2;
 };
 
-template <typename R, int N1, int N2>
+// YS (the y-split layout, PlaneArgs::ysplit): a block takes rows jb .. jb+7
+// and jb+ny/2 .. jb+ny/2+7 (jb = 8 blockIdx.x) and applies the first radix-2
+// stage of the forward y transform to each row pair before the store:
+//   E_j = X_j + X_{j+ny/2},  O_j = (X_j - X_{j+ny/2}) w_ny^j   (j < ny/2),
+// so that the y transform of every kx line splits into two independent
+// half-length transforms, E to the even and O to the odd ky, written as
+// [k][kx][half][j] (k_colsolve runs them with the vertical solve).
+template <int TJ, bool YS>
+__device__ __forceinline__ int rowreg_row(int jb_block, int r, int ny) {
+    if constexpr (!YS) return jb_block * TJ + r;
+    return jb_block * (TJ / 2) + (r < TJ / 2 ? r : ny / 2 + r - TJ / 2);
+}
+
+template <typename R, int N1, int N2, bool YS>
 __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
@@ -1056,7 +1232,8 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
             const int t = t0 + q * G::NT;
-            d[q] = plane_source_pair(a, a.u + ioff, a.v + ioff, a.w + ioff, asrc, k, jb + t / N, t % N, pfield);
+            d[q] = plane_source_pair(a, a.u + ioff, a.v + ioff, a.w + ioff, asrc, k,
+                                     rowreg_row<TJ, YS>(blockIdx.x, t / N, ny), t % N, pfield);
         }
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
@@ -1093,18 +1270,41 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) tb[(tl + N2 * r + N1 * k2) * G::LD + row] = z[r * N2 + k2];
     __syncthreads();
-    T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + jb;
-    for (int t = threadIdx.x; t < (N + 1) * TJ; t += G::NT) {
-        const int kx = t / TJ, rr = t - kx * TJ;
-        const int k1 = (kx == N) ? 0 : kx;
-        const int k2 = (kx == 0) ? 0 : N - kx;
-        const double2 w = __ldg(a.twx + kx);
-        st_l2(&spec[(long)kx * ny + rr], r2c_unpack<R>(tb[k1 * G::LD + rr], tb[k2 * G::LD + rr], mk<R>((R)w.x, (R)w.y)),
-              pkeep);
+    if constexpr (YS) {
+        constexpr int TH = TJ / 2;
+        const int ny2 = ny / 2, j0 = blockIdx.x * TH;
+        T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + j0;
+        const T* twy = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.py.tw : (const void*)a.py.twf);
+        for (int t = threadIdx.x; t < (N + 1) * TH; t += G::NT) {
+            const int kx = t / TH, rr = t - kx * TH;
+            const int k1 = (kx == N) ? 0 : kx;
+            const int k2 = (kx == 0) ? 0 : N - kx;
+            const double2 w = __ldg(a.twx + kx);
+            const T wx = mk<R>((R)w.x, (R)w.y);
+            const T xa = r2c_unpack<R>(tb[k1 * G::LD + rr], tb[k2 * G::LD + rr], wx);
+            const T xb = r2c_unpack<R>(tb[k1 * G::LD + rr + TH], tb[k2 * G::LD + rr + TH], wx);
+            const T wy = __ldg(twy + j0 + rr);   // w_ny^j
+            st_l2(&spec[(long)kx * ny + rr], cadd(xa, xb), pkeep);
+            st_l2(&spec[(long)kx * ny + ny2 + rr], cmul(csub(xa, xb), wy), pkeep);
+        }
+    } else {
+        T* spec = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + jb;
+        for (int t = threadIdx.x; t < (N + 1) * TJ; t += G::NT) {
+            const int kx = t / TJ, rr = t - kx * TJ;
+            const int k1 = (kx == N) ? 0 : kx;
+            const int k2 = (kx == 0) ? 0 : N - kx;
+            const double2 w = __ldg(a.twx + kx);
+            st_l2(&spec[(long)kx * ny + rr], r2c_unpack<R>(tb[k1 * G::LD + rr], tb[k2 * G::LD + rr], mk<R>((R)w.x, (R)w.y)),
+                  pkeep);
+        }
     }
 }
 
-template <typename R, int N1, int N2>
+// YS: the inverse of the split above: from the half-length inverse
+// transforms E' (even ky) and O' (odd ky) of [k][kx][half][j], rows j and
+// j+ny/2 of the inverse y transform are E'_j + w_ny^-j O'_j and
+// E'_j - w_ny^-j O'_j.
+template <typename R, int N1, int N2, bool YS>
 __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
@@ -1125,6 +1325,37 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
     const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + jb;
     const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.px.tw : (const void*)a.px.twf);
     // c2r pack into the block tile [m][row], loads batched per thread
+    if constexpr (YS) {
+        constexpr int TH = TJ / 2, LB2 = 2;
+        static_assert((N * TH) % (LB2 * G::NT) == 0, "pack batches");
+        const int ny2 = ny / 2, j0 = blockIdx.x * TH;
+        const T* sp = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + j0;
+        const T* twy = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.py.tw : (const void*)a.py.twf);
+        for (int t0 = threadIdx.x; t0 < N * TH; t0 += LB2 * G::NT) {
+            T ek[LB2], ok[LB2], ec[LB2], oc[LB2];
+#pragma unroll
+            for (int q = 0; q < LB2; ++q) {
+                const int t = t0 + q * G::NT;
+                const int kk = t / TH, rr = t - kk * TH;
+                ek[q] = ld_l2(&sp[(long)kk * ny + rr], plast);
+                ok[q] = ld_l2(&sp[(long)kk * ny + ny2 + rr], plast);
+                ec[q] = ld_l2(&sp[(long)(N - kk) * ny + rr], plast);
+                oc[q] = ld_l2(&sp[(long)(N - kk) * ny + ny2 + rr], plast);
+            }
+#pragma unroll
+            for (int q = 0; q < LB2; ++q) {
+                const int t = t0 + q * G::NT;
+                const int kk = t / TH, rr = t - kk * TH;
+                const double2 w = __ldg(a.twx + kk);
+                const T wx = mk<R>((R)w.x, (R)w.y);
+                T wy = __ldg(twy + j0 + rr);
+                wy.y = -wy.y;   // w_ny^-j
+                const T ok2 = cmul(ok[q], wy), oc2 = cmul(oc[q], wy);
+                tb[kk * G::LD + rr] = c2r_pack<R>(cadd(ek[q], ok2), cadd(ec[q], oc2), wx, kk == 0);
+                tb[kk * G::LD + rr + TH] = c2r_pack<R>(csub(ek[q], ok2), csub(ec[q], oc2), wx, kk == 0);
+            }
+        }
+    } else {
     constexpr int LB = 4;
     static_assert((N * TJ) % (LB * G::NT) == 0, "pack batches");
     for (int t0 = threadIdx.x; t0 < N * TJ; t0 += LB * G::NT) {
@@ -1144,6 +1375,7 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
             tb[kk * G::LD + rr] = c2r_pack<R>(xk[q], xc[q], mk<R>((R)w.x, (R)w.y), kk == 0);
         }
     }
+    }
     __syncthreads();
     T v[N1];
 #pragma unroll
@@ -1161,7 +1393,7 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
     for (int k1 = 0; k1 < N1; ++k1) t1[k1 * (N2 + 1) + tl] = v[k1];
     __syncwarp();
     const double sc = a.scale;
-    double* out = a.out + (long)inst * a.sN + (long)k * nx * ny + (long)(jb + row) * nx;
+    double* out = a.out + (long)inst * a.sN + (long)k * nx * ny + (long)rowreg_row<TJ, YS>(blockIdx.x, row, ny) * nx;
 #pragma unroll
     for (int r = 0; r < N1 / N2; ++r) {
         const int k1 = tl + N2 * r;
@@ -1324,8 +1556,12 @@ static cudaError_t launch_rows_reg_t(const PlaneArgs& a, bool fwd, cudaStream_t 
     using G = RowReg<N1, N2>;
     const dim3 g(a.ny / G::TJ, (a.kcount ? a.kcount : a.nz) * std::max(1, a.batch));
     const size_t sm = G::elems * sizeof(cpx<R>);
-    if (fwd) return launch_pdl(k_rows_fwd_reg<R, N1, N2>, g, dim3(G::NT), sm, s, a);
-    return launch_pdl(k_rows_inv_reg<R, N1, N2>, g, dim3(G::NT), sm, s, a);
+    if (a.ysplit) {
+        if (fwd) return launch_pdl(k_rows_fwd_reg<R, N1, N2, true>, g, dim3(G::NT), sm, s, a);
+        return launch_pdl(k_rows_inv_reg<R, N1, N2, true>, g, dim3(G::NT), sm, s, a);
+    }
+    if (fwd) return launch_pdl(k_rows_fwd_reg<R, N1, N2, false>, g, dim3(G::NT), sm, s, a);
+    return launch_pdl(k_rows_inv_reg<R, N1, N2, false>, g, dim3(G::NT), sm, s, a);
     return cudaGetLastError();
 }
 // The register rows pass when nx/2 has a two-factor split, else false.  The
@@ -1360,6 +1596,10 @@ static cudaError_t launch_split_m(const PlaneArgs& a, bool fwd, cudaStream_t s) 
         if (e != cudaSuccess) return e;
         if (!ylines_reg<R>(ay, -1, a.scale, s, &e))
             e = launch_pdl(k_ylines<R, MY>, glines, dim3(kPlaneThreads), sml, s, ay, -1, a.scale);
+    } else if (fwd && a.ysplit) {   // the y transforms run inside k_colsolve
+        if (!rows_reg<R>(a, true, s, &e)) return cudaErrorInvalidValue;
+    } else if (a.ysplit) {
+        if (!rows_reg<R>(a, false, s, &e)) return cudaErrorInvalidValue;
     } else if (fwd) {
         if (!rows_reg<R>(a, true, s, &e)) e = launch_pdl(k_rows_fwd<R, MX>, grows, dim3(kPlaneThreads), smr, s, a);
         if (e != cudaSuccess) return e;
@@ -1427,14 +1667,19 @@ static cudaError_t setup_t() {
     if ((e = max_dynamic_smem(k_ylines_reg<R, 8, 8>))) return e;
     if ((e = max_dynamic_smem(k_ylines_reg<R, 16, 8>))) return e;
     if ((e = max_dynamic_smem(k_ylines_reg<R, 16, 16>))) return e;
-    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 8, 8>))) return e;
-    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 16, 8>))) return e;
-    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 16, 16>))) return e;
-    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 8, 8>))) return e;
-    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8>))) return e;
-    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16>))) return e;
+#define PS3D_ROWS_SETUP(YS)                                                   \
+    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 8, 8, YS>))) return e;       \
+    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 16, 8, YS>))) return e;      \
+    if ((e = max_dynamic_smem(k_rows_fwd_reg<R, 16, 16, YS>))) return e;     \
+    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 8, 8, YS>))) return e;       \
+    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 8, YS>))) return e;      \
+    if ((e = max_dynamic_smem(k_rows_inv_reg<R, 16, 16, YS>))) return e;
+    PS3D_ROWS_SETUP(false)
+    PS3D_ROWS_SETUP(true)
+#undef PS3D_ROWS_SETUP
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
     if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
+    if ((e = max_dynamic_smem(k_colsolve))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
     if ((e = setup_m<R, 16>())) return e;

@@ -317,8 +317,9 @@ void ps3d_server::worker_loop() {
             --active;
             if (done && !stopping) idle.push_back({g[0]->prm, (int)g.size(), std::move(done), gfoot});
             else used -= gfoot;
-            // keep at most max_active idle contexts
-            while ((int)idle.size() > max_active) {
+            // keep at most 2 max_active idle contexts (with batching, groups of
+            // different sizes of one grid each keep theirs)
+            while ((int)idle.size() > 2 * max_active) {
                 evicted.push_back(std::move(idle.front().ctx));
                 used -= idle.front().footprint;
                 idle.pop_front();

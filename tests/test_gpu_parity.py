@@ -319,6 +319,39 @@ def test_mixed_precision_200_steps():
     assert max(err.values()) < TOL_MIXED, err
 
 
+@pytest.mark.parametrize("ysplit", ["1", "0"])
+@pytest.mark.parametrize("shape", [(128, 64, 32), (128, 128, 48), (256, 32, 17)])
+def test_mixed_ysplit_solve(shape, ysplit, plane_impl, monkeypatch):
+    """The mixed rigid-lid solve with the y transforms split at the rows
+    passes and run inside k_colsolve together with the vertical solve (odd
+    nz included), against the oracle after 20 steps, and the same solve on
+    the y-lines passes and k_thomas2.  The split applies to the rows + y-lines
+    implementation only."""
+    if ysplit == "1" and plane_impl != "rows+lines":
+        pytest.skip("the y-split solve runs on the rows + y-lines implementation")
+    monkeypatch.setenv("PS3D_YSPLIT", ysplit)
+    p = cf.eddy_params(*shape, precision=abi.PS3D_MIXED)
+    f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=2)
+    p64 = p.copy()
+    p64.precision = abi.PS3D_FP64
+    o = Oracle(p64)
+    load_oracle(o, f)
+    m = Model(p)
+    assert ("rows+colsolve" in m.describe()) == (ysplit == "1"), m.describe()
+    upload_from_oracle(m, o)
+    o.integrate(20)
+    m.run(20)
+    err = compare_state(m, o)
+    assert max(err.values()) < TOL_MIXED, err
+    # an explicit (cold) solve of the stepped state: the velocity is already
+    # divergence free to round-off, so the new p is round-off too and only
+    # the velocity and buoyancy are compared
+    o.pressure_solver()
+    m.pressure_solver()
+    err = compare_state(m, o, names=FIELDS)
+    assert max(err.values()) < TOL_MIXED, err
+
+
 def test_bad_params_rejected():
     p = small_params(33, 32, 16)
     with pytest.raises(PS3DError) as ei:
