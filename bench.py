@@ -14,9 +14,11 @@ oracle restatement timed on this host's cores.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 (torchrun): every rank runs an independent replica on its own GPU
-(weak scaling; the z-slab decomposition of one grid is exercised by its own
-tests, not here); value = all ranks' grid-point-steps over the slowest
-rank's time.
+(weak scaling); value = all ranks' grid-point-steps over the slowest rank's
+time.  With --slab, the N ranks instead share one grid in z-slabs
+(ps3d_b200.slab.DistSlab over NCCL: all-to-all transposes to column slabs,
+halo planes between neighbours; strong scaling): value = the grid's
+grid-point-steps over the slowest rank's time.
 
 `value` is the median of five windows of exactly K steps each, replayed as
 CUDA graphs with per-kernel profiling off (what a user's ps3d_integrate
@@ -374,6 +376,38 @@ def ensemble_run(dev, pg, world, n_members=256, steps=200, seed=3):
                     "serial arm steps one member at a time (one context per size, state uploaded per member)"}
 
 
+def slab_levels(nz, world, rank):
+    """The global levels rank `rank` of `world` owns in a z-slab run."""
+    nzl = nz // world
+    return rank * nzl, nzl
+
+
+def slab_run(precision, steps, warmup, dev, pg, world, rank):
+    """One grid over `world` ranks in z-slabs (DistSlab, NCCL): each rank
+    uploads its levels of the jets state, runs `warmup` steps, then `steps`
+    steps timed with CUDA events on its slab stream; max over ranks."""
+    import torch
+    from ps3d_b200 import configs as cf
+    from ps3d_b200.slab import DistSlab
+    p = cf.jets_params(NX, NY, NZ, precision=precision)
+    f = jets_state(p)
+    k0, nzl = slab_levels(NZ, world, rank)
+    sl = slice(k0 + 2, k0 + 2 + nzl)
+    d = DistSlab(p, dev)
+    d.upload(*[np.ascontiguousarray(f[n][sl, 2:-2, 2:-2]) for n in ("u", "v", "w", "b")])
+    d.step(warmup)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg, dev)
+    e0.record(d.stream)
+    d.step(steps)
+    e1.record(d.stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), pg, dev)
+    out = d.download()
+    d.close()
+    return ms, out
+
+
 def fp64_gemm_peak(dev, n=8192, reps=5):
     """FP64 throughput denominator measured here: torch.matmul in float64
     (cuBLAS DGEMM) on n x n operands, best of `reps`, 2 n^3 flop each."""
@@ -488,6 +522,8 @@ def main():
     ap.add_argument("--ensemble", type=int, default=1, help="also run the batched-ensemble workload")
     ap.add_argument("--serve", type=int, default=1, help="also run the serving workload")
     ap.add_argument("--projection", type=int, default=1, help="also time the normal-mode projection")
+    ap.add_argument("--slab", action="store_true",
+                    help="one grid over the N ranks in z-slabs (strong scaling) instead of N replicas")
     args = ap.parse_args()
     set_grid(args.nx, args.ny, args.nz)
     unit = "grid-point-steps/s"
@@ -512,6 +548,8 @@ def main():
         return
 
     world, rank, local, pg = dist_setup()
+    if args.slab:
+        return slab_main(args, world, rank, local, pg, metric, unit)
     import torch
     from ps3d_b200 import build as b
     from ps3d_b200 import abi
@@ -622,6 +660,45 @@ def main():
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def slab_main(args, world, rank, local, pg, metric, unit):
+    """bench.py --slab: the mixed path's time step on one grid shared by the
+    ranks in z-slabs (strong scaling), FP64 beside it."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from ps3d_b200 import abi
+    from ps3d_b200 import build as b
+    b.build()
+    torch.cuda.set_device(local)
+    if pg is None:   # one rank: a process group of one for DistSlab's collectives
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29641")
+        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    if NZ % world or NZ // world < 2:
+        raise SystemExit(f"--slab: nz={NZ} does not split into {world} slabs of >= 2 levels")
+    npts = NX * NY * NZ
+    res = {}
+    for name, prec in (("mixed", abi.PS3D_MIXED), ("fp64", abi.PS3D_FP64)):
+        ms, _ = slab_run(prec, args.steps, args.warmup, local, pg, world, rank)
+        res[name] = ms
+    ms = res["mixed"]
+    line = {"metric": metric + " (one grid in z-slabs)", "value": npts * args.steps / (ms * 1e-3), "unit": unit,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32+f64 (FP64 state/AB/tridiagonal)", "data": "synthetic (seeded jets + 1e-3 b noise)",
+            "config": {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "parallelism": f"z-slabs x{world}",
+                       "path": "mixed", "levels_per_rank": NZ // world,
+                       "l2": "inputs larger than L2 (state > 1 GB)" if npts >= 2 ** 23 else "small case"},
+            "fp64": {"value": npts * args.steps / (res["fp64"] * 1e-3), "ms_per_step": res["fp64"] / args.steps},
+            "timing": "CUDA events on each rank's slab stream around exactly `steps` steps, max over ranks"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
 
 
 if __name__ == "__main__":

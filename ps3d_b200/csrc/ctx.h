@@ -75,7 +75,11 @@ struct Ctx {
     // except w, whose tendency is dominated by the buoyancy term b/dsqr that
     // the pressure gradient nearly cancels (rounding it to FP32 costs ~1e-5
     // relative in w within 100 steps)
-    size_t tsz(int f) const { return (mixed && f != 2) ? sizeof(float) : sizeof(double); }
+    size_t tsz(int f) const { return (hist32 && f != 2) ? sizeof(float) : sizeof(double); }
+    // the mixed path's stored history in FP32 (the default); PS3D_MIXED_HISTORY=64
+    // keeps it in FP64, a diagnostic that separates the history's rounding
+    // from the FP32 transforms' in the mixed path's error budget
+    bool hist32 = false;
     int batch = 1;            // instances of this grid stepped together (ensembles)
     // CUDA graphs of three consecutive steps (tau and the state buffers both
     // cycle with period 3), replayed by advance() for constant parameters: one

@@ -250,6 +250,10 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     rigid = P.enable_vertical_boundaries != 0;
     mixed = P.precision == PS3D_MIXED || P.precision == PS3D_MIXED_REFINED;
     refine_full = P.precision == PS3D_MIXED_REFINED;
+    {
+        const char* h = std::getenv("PS3D_MIXED_HISTORY");
+        hist32 = mixed && !(h && h[0] == '6');
+    }
     // a z-slab's local grid (split_solve) never transforms along its own z:
     // the slab driver solves whole columns of the global grid
     const bool zfft = !rigid && !split_solve;
@@ -508,7 +512,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         a.uo = (double*)state[0][nxt[0]].p; a.vo = (double*)state[1][nxt[1]].p;
         a.wo = (double*)state[2][nxt[2]].p; a.bo = (double*)state[3][nxt[3]].p;
         a.do_ab = 1;
-        LAUNCH(PS3D_K_STEP, launch_step(a, mixed, stream));
+        LAUNCH(PS3D_K_STEP, launch_step(a, hist32, stream));
         for (int f = 0; f < 4; ++f) cur[f] = nxt[f];
         pending = false;   // consumed by the step kernel
         if (split_solve) return PS3D_OK;
@@ -739,7 +743,7 @@ int Ctx::autotune() {
             }
             a.uo = (double*)state[0][(cur[0] + 1) % 3].p; a.vo = (double*)state[1][(cur[1] + 1) % 3].p;
             a.wo = (double*)state[2][(cur[2] + 1) % 3].p; a.bo = (double*)state[3][(cur[3] + 1) % 3].p;
-            CK(launch_step(a, mixed, stream));
+            CK(launch_step(a, hist32, stream));
             return PS3D_OK;
         });
         if (t < bestk) { bestk = t; bestkc = kc; }
