@@ -107,6 +107,7 @@ struct PlaneArgs {
     // vertical solve are then one kernel, k_colsolve (launch_colsolve)
     int ysplit;
     FFTPlan pyh;                   // ysplit: the half-length y plan (length ny/2)
+    int zrev;                      // the rows passes walk the planes top down (set by the launchers)
 };
 // spectral layout of a plane configuration: 0 [k][ky][kx], 1 [k][kx][ky]
 inline int spectral_layout(const PlaneArgs& a) { return a.impl != 0; }

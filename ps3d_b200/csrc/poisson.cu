@@ -874,7 +874,9 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     const int jb = blockIdx.x * tj;
     const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
     const int inst = blockIdx.y / kcnt;
-    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    // spectral level; zrev walks the planes top down (the step kernel before
+    // the forward pass wrote the top levels last, so some are still in L2)
+    const int kl = a.zrev ? kcnt - 1 - (int)(blockIdx.y - inst * kcnt) : (int)(blockIdx.y - inst * kcnt);
     const int k = a.kbeg + kl;                    // real-field level
     const long ioff = (long)inst * a.sN;
     const double* au = a.u + ioff;
@@ -1105,8 +1107,10 @@ struct YReg {
     static constexpr int LS = N1 * (N2 + 1) + 1;              // tile stride of a line (elements)
 };
 
+// four resident blocks in FP32 (64 registers, no spills; 80 and three
+// blocks without the bound), two in FP64 (128 registers; capping them spills)
 template <typename R, int N1, int N2>
-__global__ void __launch_bounds__(kPlaneThreads, 2) k_ylines_reg(const PlaneArgs a, long nlines, int sign,
+__global__ void __launch_bounds__(kPlaneThreads, sizeof(R) == 4 ? 4 : 2) k_ylines_reg(const PlaneArgs a, long nlines, int sign,
                                                                  double scale) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
@@ -1218,7 +1222,9 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
     const int jb = blockIdx.x * TJ;
     const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
     const int inst = blockIdx.y / kcnt;
-    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    // spectral level; zrev walks the planes top down (the step kernel before
+    // the forward pass wrote the top levels last, so some are still in L2)
+    const int kl = a.zrev ? kcnt - 1 - (int)(blockIdx.y - inst * kcnt) : (int)(blockIdx.y - inst * kcnt);
     const int k = a.kbeg + kl;                    // real-field level
     const long ioff = (long)inst * a.sN;
     const double* asrc = a.src ? a.src + ioff : nullptr;
@@ -1320,7 +1326,9 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const Plane
     const int jb = blockIdx.x * TJ;
     const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
     const int inst = blockIdx.y / kcnt;
-    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    // spectral level; zrev walks the planes top down (the step kernel before
+    // the forward pass wrote the top levels last, so some are still in L2)
+    const int kl = a.zrev ? kcnt - 1 - (int)(blockIdx.y - inst * kcnt) : (int)(blockIdx.y - inst * kcnt);
     const int k = a.kbeg + kl;                    // real-field level
     const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)kl * a.nxh * ny + jb;
     const T* tw = reinterpret_cast<const T*>(sizeof(R) == 8 ? (const void*)a.px.tw : (const void*)a.px.twf);
@@ -1431,7 +1439,9 @@ __global__ void __launch_bounds__(kPlaneThreads, plane_min_blocks<MAXR>()) k_row
     const int jb = blockIdx.x * tj;
     const int kcnt = a.kcount ? a.kcount : nz;   // levels of the window (z-slab)
     const int inst = blockIdx.y / kcnt;
-    const int kl = blockIdx.y - inst * kcnt;     // spectral level
+    // spectral level; zrev walks the planes top down (the step kernel before
+    // the forward pass wrote the top levels last, so some are still in L2)
+    const int kl = a.zrev ? kcnt - 1 - (int)(blockIdx.y - inst * kcnt) : (int)(blockIdx.y - inst * kcnt);
     const int k = a.kbeg + kl;                    // real-field level
     const long plane = (long)nx * ny;
     const T* spec = reinterpret_cast<const T*>(a.spec) + (long)inst * a.sM + (long)kl * nxh * ny;
@@ -1626,6 +1636,15 @@ template <typename R>
 static cudaError_t launch_split_t(const PlaneArgs& a0, bool fwd, cudaStream_t s) {
     PlaneArgs a = a0;
     a.l2hint = l2hint_mode();
+    // the forward rows pass walks the planes top down (PS3D_ZREV=0: bottom
+    // up): the step kernel wrote the top levels last, so some are still in
+    // L2 (FP64 forward transform 109 -> 103 us at 256x256x128; the inverse
+    // pass top down measured slower, 58 -> 62 us, and keeps the bottom-up order)
+    static const int zrev = [] {
+        const char* e = std::getenv("PS3D_ZREV");
+        return e && e[0] == '0' ? 0 : 1;
+    }();
+    a.zrev = fwd ? zrev : 0;
     a.fd_n2 = make_fastdiv(a.nx / 2);
     a.fd_ny = make_fastdiv(a.ny);
     a.fd_tj = make_fastdiv(a.tj);

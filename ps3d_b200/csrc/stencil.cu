@@ -18,6 +18,7 @@
 // one offset add per field.  Face fluxes are recomputed per
 // point instead of being stored, so the kernel reads each state word once
 // from HBM and writes tendencies and the new state once.
+#include <cstdlib>
 #include "engine.h"
 
 namespace ps3d {
@@ -494,6 +495,7 @@ static cudaError_t launch_step_t(const StepArgs& a0, cudaStream_t s) {
     a.hdx = 0.5 * a.rdx; a.hdy = 0.5 * a.rdy; a.hdz = 0.5 * a.rdz;
     a.qdx = 0.25 * a.rdx; a.qdy = 0.25 * a.rdy; a.qdz = 0.25 * a.rdz;
     a.qf0 = 0.25 * a.f0; a.hN0sq = 0.5 * a.N0sq;
+
     const int kcnt = a.kcount ? a.kcount : a.nz;
     const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
     dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((kcnt + kchunk - 1) / kchunk) * std::max(1, a.batch));
@@ -515,9 +517,17 @@ static cudaError_t launch_step_tt(const StepArgs& a, cudaStream_t s) {
 template <typename TT>
 static cudaError_t step_setup_tt() {
     cudaError_t e;
+    // PS3D_STEP_CARVEOUT=<percent>: the shared-memory share of the unified
+    // L1/shared storage the step kernels ask for (a hint to the driver)
+    const char* cv = std::getenv("PS3D_STEP_CARVEOUT");
+    const int carve = cv ? std::atoi(cv) : -1;
 #define S(H, W, G)                                                                                        \
     if ((e = cudaFuncSetAttribute(k_step<TT, 8, H, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
                                   (int)sizeof(StepSmem<TT, 8, G ? 6 : 4>))))                              \
+        return e;                                                                                         \
+    if (carve >= 0 &&                                                                                     \
+        (e = cudaFuncSetAttribute(k_step<TT, 8, H, W, G>, cudaFuncAttributePreferredSharedMemoryCarveout,  \
+                                  carve)))                                                                \
         return e;
     S(true, true, true) S(true, true, false) S(true, false, true) S(true, false, false)
     S(false, true, true) S(false, true, false) S(false, false, true) S(false, false, false)
