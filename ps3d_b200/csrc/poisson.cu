@@ -1175,20 +1175,24 @@ __global__ void __launch_bounds__(kPlaneThreads, sizeof(R) == 4 ? 4 : 2) k_yline
 // ---------------------------------------------------------------------------
 constexpr int kRowsRegTJ = 16;
 
-template <int N1, int N2>
+template <int N1, int N2, typename R = float>
 struct RowReg {
     static constexpr int N = N1 * N2;
     static constexpr int TJ = kRowsRegTJ;
     static constexpr int NT = TJ * N2;                    // threads per block
-    // Tile pitches chosen against shared-memory bank conflicts (8-byte
-    // complex FP32 elements take two 4-byte banks; a half-warp's 16 lanes
-    // are served together).  With N2 = 8 a half-warp spans two rows, so the
-    // rows' transpose tiles start 16 banks apart (LS = 8 mod 16 elements);
-    // in the block tile [m][row] the lanes of a row step through m, so its
+    // Tile pitches chosen against shared-memory bank conflicts.  FP32
+    // complex elements take two 4-byte banks and a half-warp's 16 lanes are
+    // served together: with N2 = 8 a half-warp spans two rows, so the rows'
+    // transpose tiles start 16 banks apart (LS = 8 mod 16 elements), and in
+    // the block tile [m][row], where the lanes of a row step through m, the
     // pitch is TJ + 2 (4 banks per step of m, the two rows 2 banks apart).
+    // FP64 complex elements take four banks and a quarter-warp of 8 lanes
+    // (one row) is served together: the block tile's pitch is TJ + 1 (4
+    // banks per step of m), and the row tiles need no spacing.
+    static constexpr bool F32 = sizeof(R) == 4;
     static constexpr int LS0 = N1 * (N2 + 1);
-    static constexpr int LS = N2 == 8 ? LS0 + (24 - LS0 % 16) % 16 : LS0 + 1;   // transpose tile stride of a row
-    static constexpr int LD = TJ + 2;                     // block tile [m][row] pitch
+    static constexpr int LS = (F32 && N2 == 8) ? LS0 + (24 - LS0 % 16) % 16 : LS0 + 1;   // transpose tile stride of a row
+    static constexpr int LD = F32 ? TJ + 2 : TJ + 1;      // block tile [m][row] pitch
     static constexpr size_t T1 = (size_t)TJ * LS, T2 = (size_t)N * LD;
     static constexpr size_t elems = T1 > T2 ? T1 : T2;
 };
@@ -1207,12 +1211,12 @@ __device__ __forceinline__ int rowreg_row(int jb_block, int r, int ny) {
 }
 
 template <typename R, int N1, int N2, bool YS>
-__global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const PlaneArgs a) {
+__global__ void __launch_bounds__(RowReg<N1, N2, R>::NT) k_rows_fwd_reg(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
     const unsigned long long pfield = pol_field(a.l2hint), pkeep = pol_keep(a.l2hint);
     using T = cpx<R>;
-    using G = RowReg<N1, N2>;
+    using G = RowReg<N1, N2, R>;
     constexpr int N = G::N, TJ = G::TJ;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tb = reinterpret_cast<T*>(smem_raw);
@@ -1311,12 +1315,12 @@ __global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_fwd_reg(const Plane
 // j+ny/2 of the inverse y transform are E'_j + w_ny^-j O'_j and
 // E'_j - w_ny^-j O'_j.
 template <typename R, int N1, int N2, bool YS>
-__global__ void __launch_bounds__(RowReg<N1, N2>::NT) k_rows_inv_reg(const PlaneArgs a) {
+__global__ void __launch_bounds__(RowReg<N1, N2, R>::NT) k_rows_inv_reg(const PlaneArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
     const unsigned long long plast = pol_last(a.l2hint);
     using T = cpx<R>;
-    using G = RowReg<N1, N2>;
+    using G = RowReg<N1, N2, R>;
     constexpr int N = G::N, TJ = G::TJ;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tb = reinterpret_cast<T*>(smem_raw);
@@ -1563,7 +1567,7 @@ bool rows_in_registers(int nx, int ny) {
 }
 template <typename R, int N1, int N2>
 static cudaError_t launch_rows_reg_t(const PlaneArgs& a, bool fwd, cudaStream_t s) {
-    using G = RowReg<N1, N2>;
+    using G = RowReg<N1, N2, R>;
     const dim3 g(a.ny / G::TJ, (a.kcount ? a.kcount : a.nz) * std::max(1, a.batch));
     const size_t sm = G::elems * sizeof(cpx<R>);
     if (a.ysplit) {

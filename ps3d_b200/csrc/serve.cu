@@ -368,7 +368,10 @@ PS3D_API int ps3d_server_destroy(ps3d_server* s) {
         s->stopping = true;
         for (auto& q : s->queue) { q->state = kCancelled; q->status = PS3D_ERR_CANCELLED; }
         s->queue.clear();
-        for (auto& kv : s->all) kv.second->cancel.store(1);
+        for (auto& kv : s->all) {
+            kv.second->cancel.store(1);
+            if (kv.second->group) kv.second->group->cancel.store(1);   // a running batched group stops too
+        }
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
