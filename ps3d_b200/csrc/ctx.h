@@ -230,6 +230,14 @@ struct Ctx {
     // no longer holds the previous step's pressure of this trajectory
     void state_replaced() { ++version; p_warm = false; }
     int step(int itt, int tau, int taum1, int taum2);
+    // Grouped step launches (an ensemble's groups in one step-kernel launch):
+    // with defer_step set, step() of a fused step does the step kernel's
+    // bookkeeping and writes its arguments to *defer_step instead of
+    // launching it; the caller launches the kernel, then step_finish() runs
+    // the rest of the step (the pressure solve) on this context's stream.
+    StepArgs* defer_step = nullptr;
+    bool fused_step() const;
+    int step_finish() { return pressure_solve(lazy_correction, true); }
     int poisson_once(double* out, double beta, bool lazy = false, const double* pc = nullptr);
     int pressure_solve(bool lazy = false, bool warm = false);
     int materialize();        // apply a pending correction so the state arrays hold the true state

@@ -463,6 +463,16 @@ DevBuf* Ctx::fieldset(int which) {
 // ---------------------------------------------------------------------------
 // integrate (integrate.f90:2-115)
 // ---------------------------------------------------------------------------
+// the step runs the fused kernel: no biharmonic stages, no host callback,
+// no background flow together with harmonic friction
+bool Ctx::fused_step() const {
+    const bool bg = (fkind & PS3D_FORCE_BACKGROUND) != 0;
+    const bool cb = (fkind & PS3D_FORCE_CALLBACK) != 0 && fn != nullptr;
+    const bool bih = P.Ahbi > 0. || P.Avbi > 0. || P.Khbi > 0. || P.Kvbi > 0.;
+    const bool harm = P.Ah > 0. || P.Av > 0. || P.Kh > 0. || P.Kv > 0.;
+    return !bih && !cb && !(bg && harm);
+}
+
 int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
     StepArgs a{};
     a.nx = nx; a.ny = ny; a.nz = nz;
@@ -494,7 +504,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         a.wm_on = 1; a.wm_c = std::cos(omega * t); a.wm_s = std::sin(omega * t);
         for (int f = 0; f < 4; ++f) { a.wr[f] = (const double*)wr[f].p; a.wi[f] = (const double*)wi[f].p; }
     }
-    const bool fused = !bih && !cb && !(bg && harm);
+    const bool fused = fused_step();
     if (split_solve && (!fused || wm || bg)) return PS3D_ERR_UNSUPPORTED;   // z-slabs: the fused step, no forcing
     if (!fused) {
         int rc = materialize();
@@ -512,10 +522,11 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         a.uo = (double*)state[0][nxt[0]].p; a.vo = (double*)state[1][nxt[1]].p;
         a.wo = (double*)state[2][nxt[2]].p; a.bo = (double*)state[3][nxt[3]].p;
         a.do_ab = 1;
-        LAUNCH(PS3D_K_STEP, launch_step(a, hist32, stream));
+        if (defer_step) *defer_step = a;   // launched by the caller, with other grids
+        else LAUNCH(PS3D_K_STEP, launch_step(a, hist32, stream));
         for (int f = 0; f < 4; ++f) cur[f] = nxt[f];
         pending = false;   // consumed by the step kernel
-        if (split_solve) return PS3D_OK;
+        if (split_solve || defer_step) return PS3D_OK;
     } else {
         if (mixed || batch > 1) return PS3D_ERR_UNSUPPORTED;   // generic path: FP64 tendencies, one grid
         int old[4], B[4], Cb[4];

@@ -67,6 +67,17 @@ struct StepArgs {
     double hdx, hdy, hdz, qdx, qdy, qdz, qf0, hN0sq;
 };
 
+// One step-kernel launch over the grids of several groups (an ensemble's
+// members of uneven sizes).  The table is a kernel parameter (sizeof ~11 KB,
+// below the 32 KB parameter limit of CUDA 12.1+).
+constexpr int kMaxStepGroups = 16;
+struct StepGroups {
+    StepArgs a[kMaxStepGroups];                    // each group's arguments (launcher-derived fields set)
+    int blk0[kMaxStepGroups + 1];                  // first block of each group in the launch
+    int gx[kMaxStepGroups], gy[kMaxStepGroups];    // column tiles along x and y of each group's grid
+    int n;
+};
+
 // Plane-FFT kernels (divergence + forward 2D FFT, inverse 2D FFT) for one grid.
 struct PlaneArgs {
     int nx, ny, nz, nxh;
@@ -140,6 +151,12 @@ int l2hint_mode();
 
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s);
 cudaError_t step_setup();   // opts the step kernels in to their dynamic shared memory
+// which fused step kernel a launch of `a` runs (friction, wavemaker,
+// background-flow bits); grids of one grouped launch must agree
+int step_flavour(const StepArgs& a);
+// one launch of the step kernel over n <= kMaxStepGroups grids, each as
+// launch_step(a[g], fp32_tendencies) would step it
+cudaError_t launch_step_groups(const StepArgs* a, int n, bool fp32_tendencies, cudaStream_t s);
 cudaError_t launch_biharmonic_h(const double* cur, const double* old, double* out, int nx, int ny, int nz,
                                 double Hmix, double rdx, double rdy, double dt, cudaStream_t s);
 cudaError_t launch_biharmonic_v(const double* cur, const double* old, double* out, int nx, int ny, int nz,

@@ -10,6 +10,7 @@
 // consecutive steps of every group are captured into a single CUDA graph —
 // one branch per group — that is replayed (tau and the state buffers cycle
 // with period 3).
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -27,6 +28,7 @@ struct ps3d_ensemble {
     std::vector<std::pair<int, int>> where;   // member -> (group, index in group)
     cudaGraphExec_t gexec = nullptr;
     bool graph_valid = false;
+    bool grouped = false;                    // the groups' step kernels in one launch
     int itt = 0;
     ~ps3d_ensemble() {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -41,9 +43,61 @@ namespace {
 
 bool same_params(const ps3d_params& a, const ps3d_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
 
+// The groups' step kernels as one launch on the ensemble stream
+// (PS3D_ENSEMBLE_GROUPED=1 at creation; measured slower than one launch per
+// group on its own stream, so off by default): every group runs the fused
+// step (no generic friction or callback path), in one precision,
+// unprofiled, and there are at most kMaxStepGroups of them.
+bool grouped_step(const ps3d_ensemble* e) {
+    const size_t G = e->groups.size();
+    if (!e->grouped || G < 2 || G > (size_t)ps3d::kMaxStepGroups) return false;
+    for (auto& g : e->groups)
+        if (!g->fused_step() || g->prof || g->split_solve || g->hist32 != e->groups[0]->hist32) return false;
+    return true;
+}
+
 // one step of every group: each group's stream waits for the ensemble
-// stream, runs its step, and the ensemble stream waits for every group
+// stream, runs its step, and the ensemble stream waits for every group.
+// Grouped: the step kernels of all groups run first, as one launch on the
+// ensemble stream, and the groups' streams then run their pressure solves.
 int step_all(ps3d_ensemble* e) {
+    if (grouped_step(e)) {
+        const size_t G = e->groups.size();
+        ps3d::StepArgs args[ps3d::kMaxStepGroups];
+        for (size_t q = 0; q < G; ++q) {
+            Ctx& g = *e->groups[q];
+            g.defer_step = &args[q];
+            const int rc = g.step(g.itt, g.tau, g.taum1, g.taum2);
+            g.defer_step = nullptr;
+            if (rc) return rc;
+        }
+        bool same = true;
+        for (size_t q = 1; q < G; ++q) same = same && ps3d::step_flavour(args[q]) == ps3d::step_flavour(args[0]);
+        const bool f32 = e->groups[0]->hist32;
+        if (same) {
+            if (ps3d::launch_step_groups(args, (int)G, f32, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+            ++e->groups[0]->launches;
+        } else {
+            for (size_t q = 0; q < G; ++q) {
+                if (ps3d::launch_step(args[q], f32, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+                ++e->groups[q]->launches;
+            }
+        }
+        if (cudaEventRecord(e->fork, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+        for (size_t q = 0; q < G; ++q) {
+            Ctx& g = *e->groups[q];
+            if (cudaStreamWaitEvent(g.stream, e->fork, 0) != cudaSuccess) return PS3D_ERR_CUDA;
+            const int rc = g.step_finish();
+            if (rc) return rc;
+            g.rotate();
+            g.time = g.time + g.P.dt;
+            ++g.itt;
+            if (cudaEventRecord(e->joins[q], g.stream) != cudaSuccess) return PS3D_ERR_CUDA;
+            if (cudaStreamWaitEvent(e->stream, e->joins[q], 0) != cudaSuccess) return PS3D_ERR_CUDA;
+        }
+        ++e->itt;
+        return PS3D_OK;
+    }
     if (cudaEventRecord(e->fork, e->stream) != cudaSuccess) return PS3D_ERR_CUDA;
     for (size_t q = 0; q < e->groups.size(); ++q) {
         Ctx& g = *e->groups[q];
@@ -102,6 +156,12 @@ int capture(ps3d_ensemble* e) {
 }
 
 int advance(ps3d_ensemble* e, int nsteps) {
+    // the ensemble stream (where grouped step kernels run) waits for what the
+    // groups' streams hold (uploads, the previous call's work)
+    for (size_t q = 0; q < e->groups.size(); ++q) {
+        if (cudaEventRecord(e->joins[q], e->groups[q]->stream) != cudaSuccess) return PS3D_ERR_CUDA;
+        if (cudaStreamWaitEvent(e->stream, e->joins[q], 0) != cudaSuccess) return PS3D_ERR_CUDA;
+    }
     while (nsteps > 0) {
         if (nsteps >= 3 && e->itt >= 2 && all_graphable(e)) {
             bool same = true;
@@ -171,6 +231,10 @@ int ps3d::ensemble_create(const ps3d_params* members, int n, int device, bool tu
     if (cudaSetDevice(device) != cudaSuccess) return PS3D_ERR_CUDA;
     std::unique_ptr<ps3d_ensemble> e(new ps3d_ensemble());
     e->device = device;
+    {
+        const char* v = std::getenv("PS3D_ENSEMBLE_GROUPED");
+        e->grouped = v && v[0] == '1';
+    }
     if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) return PS3D_ERR_CUDA;
     // group members with identical parameters, in first-seen order
     std::vector<int> gid(n, -1);

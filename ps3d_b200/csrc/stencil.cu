@@ -216,22 +216,22 @@ out = F(0, 0, 0) + dt * ((e - em) * rdx + (n - nm) * rdy + (t - tm) * rdz);     
 // read field f at offsets (di, dj) in ring slot s
 #define SM(fi, s, dj, di) sm.pl[fi][s][(ty + 1 + (dj)) * (kTX + 2) + (tx + 1 + (di))]
 
+// One block's column tile (bx, by) and z chunk / instance bz of the grid
+// described by `a`.
 template <typename TT, int BY, bool HARM, bool WM, bool BG>
-__global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) {
+__device__ __forceinline__ void step_tile(const StepArgs& a, int kchunk, int bx, int by, int bz) {
     using TW = double;   // stored w tendencies stay FP64 in both paths
     constexpr int NF = BG ? 6 : 4;
     extern __shared__ __align__(16) unsigned char step_smem_raw[];
     StepSmem<TT, BY, NF>& sm = *reinterpret_cast<StepSmem<TT, BY, NF>*>(step_smem_raw);
-    pdl_trigger();
-    pdl_wait();   // the state, p and history were written by the preceding kernels
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * BY;
+    const int i0 = bx * kTX, j0 = by * BY;
     const int kcnt = a.kcount ? a.kcount : nz;           // levels stepped (a z-slab's interior)
     const int kofs = a.kofs, nzg = a.nzg ? a.nzg : nz;   // global level k + kofs of nzg (rigid-lid masks)
     const int nzc = (kcnt + kchunk - 1) / kchunk;
-    const int inst = blockIdx.z / nzc;
-    const int kb = a.kbeg + (blockIdx.z - inst * nzc) * kchunk;
+    const int inst = bz / nzc;
+    const int kb = a.kbeg + (bz - inst * nzc) * kchunk;
     const int ke = min(a.kbeg + kcnt, kb + kchunk);
     const long ioff = (long)inst * a.sN;
     const int i = i0 + tx, j = j0 + ty;
@@ -316,6 +316,28 @@ __global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) 
         }
         __syncthreads();
     }
+}
+
+template <typename TT, int BY, bool HARM, bool WM, bool BG>
+__global__ void __launch_bounds__(kTX* BY) k_step(const StepArgs a, int kchunk) {
+    pdl_trigger();
+    pdl_wait();   // the state, p and history were written by the preceding kernels
+    step_tile<TT, BY, HARM, WM, BG>(a, kchunk, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// One launch over the grids of several groups (an ensemble's members of
+// uneven sizes): block b belongs to the group g with blk0[g] <= b <
+// blk0[g+1] and runs that group's tile as k_step would.  The table rides in
+// the kernel's parameter space (captured by value into a CUDA graph).
+template <typename TT, int BY, bool HARM, bool WM, bool BG>
+__global__ void __launch_bounds__(kTX* BY, BG ? 2 : 4) k_step_groups(const __grid_constant__ StepGroups m) {
+    pdl_trigger();
+    pdl_wait();
+    int g = 0;
+    while (g + 1 < m.n && (int)blockIdx.x >= m.blk0[g + 1]) ++g;
+    const int l = blockIdx.x - m.blk0[g];
+    const int gx = m.gx[g], gy = m.gy[g];
+    step_tile<TT, BY, HARM, WM, BG>(m.a[g], m.a[g].kchunk, l % gx, (l / gx) % gy, l / (gx * gy));
 }
 
 // ---------------------------------------------------------------------------
@@ -489,18 +511,69 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v, double
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <typename TT, int BY, bool HARM, bool WM, bool BG>
-static cudaError_t launch_step_t(const StepArgs& a0, cudaStream_t s) {
-    StepArgs a = a0;
+// the launcher-derived fields of a step and its grid of blocks
+static dim3 prep_step(StepArgs& a, int by) {
     a.hdx = 0.5 * a.rdx; a.hdy = 0.5 * a.rdy; a.hdz = 0.5 * a.rdz;
     a.qdx = 0.25 * a.rdx; a.qdy = 0.25 * a.rdy; a.qdz = 0.25 * a.rdz;
     a.qf0 = 0.25 * a.f0; a.hN0sq = 0.5 * a.N0sq;
-
     const int kcnt = a.kcount ? a.kcount : a.nz;
-    const int kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
-    dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + BY - 1) / BY, ((kcnt + kchunk - 1) / kchunk) * std::max(1, a.batch));
+    a.kchunk = a.kchunk > 0 ? std::min(a.kchunk, kcnt) : (kcnt <= 16 ? kcnt : 8);
+    return dim3((a.nx + kTX - 1) / kTX, (a.ny + by - 1) / by, ((kcnt + a.kchunk - 1) / a.kchunk) * std::max(1, a.batch));
+}
+
+template <typename TT, int BY, bool HARM, bool WM, bool BG>
+static cudaError_t launch_step_t(const StepArgs& a0, cudaStream_t s) {
+    StepArgs a = a0;
+    const dim3 grid = prep_step(a, BY);
     return launch_pdl(k_step<TT, BY, HARM, WM, BG>, grid, dim3(kTX, BY), sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s, a,
-                      kchunk);
+                      a.kchunk);
+}
+
+template <typename TT, int BY, bool HARM, bool WM, bool BG>
+static cudaError_t launch_step_groups_t(const StepArgs* in, int n, cudaStream_t s) {
+    static_assert(sizeof(StepGroups) <= 32000, "grouped step table exceeds the kernel parameter space");
+    StepGroups m{};
+    m.n = n;
+    long blocks = 0;
+    for (int g = 0; g < n; ++g) {
+        m.a[g] = in[g];
+        const dim3 gr = prep_step(m.a[g], BY);
+        m.gx[g] = (int)gr.x; m.gy[g] = (int)gr.y;
+        m.blk0[g] = (int)blocks;
+        blocks += (long)gr.x * gr.y * gr.z;
+    }
+    if (blocks > 0x7fffffffL) return cudaErrorInvalidValue;
+    m.blk0[n] = (int)blocks;
+    return launch_pdl(k_step_groups<TT, BY, HARM, WM, BG>, dim3((unsigned)blocks), dim3(kTX, BY),
+                      sizeof(StepSmem<TT, BY, BG ? 6 : 4>), s, m);
+}
+
+int step_flavour(const StepArgs& a) {
+    return (a.harm_uvw || a.harm_b ? 1 : 0) | (a.wm_on ? 2 : 0) | (a.ub ? 4 : 0);
+}
+
+template <typename TT>
+static cudaError_t launch_step_groups_tt(const StepArgs* a, int n, cudaStream_t s) {
+    if (n < 1 || n > kMaxStepGroups) return cudaErrorInvalidValue;
+    const int fl = step_flavour(a[0]);
+    for (int g = 1; g < n; ++g)
+        if (step_flavour(a[g]) != fl) return cudaErrorInvalidValue;
+#define L(H, W, G) return launch_step_groups_t<TT, 8, H, W, G>(a, n, s)
+    switch (fl) {
+        case 0: L(false, false, false);
+        case 1: L(true, false, false);
+        case 2: L(false, true, false);
+        case 3: L(true, true, false);
+        case 4: L(false, false, true);
+        case 5: L(true, false, true);
+        case 6: L(false, true, true);
+        default: L(true, true, true);
+    }
+#undef L
+}
+
+cudaError_t launch_step_groups(const StepArgs* a, int n, bool fp32_tendencies, cudaStream_t s) {
+    return fp32_tendencies ? launch_step_groups_tt<float>(a, n, s) : launch_step_groups_tt<double>(a, n, s);
 }
 
 template <typename TT>
@@ -523,6 +596,10 @@ static cudaError_t step_setup_tt() {
     const int carve = cv ? std::atoi(cv) : -1;
 #define S(H, W, G)                                                                                        \
     if ((e = cudaFuncSetAttribute(k_step<TT, 8, H, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                  (int)sizeof(StepSmem<TT, 8, G ? 6 : 4>))))                              \
+        return e;                                                                                         \
+    if ((e = cudaFuncSetAttribute(k_step_groups<TT, 8, H, W, G>,                                       \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                            \
                                   (int)sizeof(StepSmem<TT, 8, G ? 6 : 4>))))                              \
         return e;                                                                                         \
     if (carve >= 0 &&                                                                                     \

@@ -73,6 +73,56 @@ def test_ensemble_members_match_oracle(precision, tol):
     ens.close()
 
 
+@pytest.mark.parametrize("precision,tol_single,tol_oracle",
+                         [(abi.PS3D_FP64, 1e-11, 1e-11), (abi.PS3D_MIXED, 1e-8, 1e-5)])
+def test_grouped_step_launch(precision, tol_single, tol_oracle, monkeypatch):
+    """PS3D_ENSEMBLE_GROUPED=1: the step kernels of all size groups run as one
+    launch (the groups' arguments in a table).  That kernel is compiled apart
+    from the single-grid one, so its floating-point contractions may differ:
+    members agree with lone runs to round-off (FP64; the mixed path's FP32
+    history carries a flipped rounding further) and with the oracle at the
+    parity tolerances."""
+    from oracle.binding import Oracle
+    monkeypatch.setenv("PS3D_AUTOTUNE", "0")
+    monkeypatch.setenv("PS3D_ENSEMBLE_GROUPED", "1")
+    sizes = [(32, 32, 16), (64, 32, 16), (32, 32, 16), (64, 64, 16)]
+    members = [cf.eddy_params(*s, precision=precision) for s in sizes]
+    amps = [0.08, 0.15, 0.2, 0.1]
+    fields = [_member_fields(p, a, seed=20 + i) for i, (p, a) in enumerate(zip(members, amps))]
+    ens = Ensemble(members)
+    assert ens.info()["groups"] == 3
+    for i, f in enumerate(fields):
+        ens.upload(i, f["u"], f["v"], f["w"], f["b"])
+    nsteps = 11      # eager start, graph replays, eager remainder
+    l0 = ens.info()["launches"]
+    ens.integrate(nsteps)
+    per_step = (ens.info()["launches"] - l0) / nsteps
+    for i, (p, f) in enumerate(zip(members, fields)):
+        m = Model(p)
+        m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+        m.run(nsteps)
+        ref = m.download(tendencies=False)
+        got = ens.download(i)
+        o = Oracle(cf.eddy_params(*sizes[i]))
+        for n in ("u", "v", "w", "b"):
+            o.field(n)[...] = f[n]
+        o.integrate(nsteps)
+        for n in ("u", "v", "w", "b", "p"):
+            assert rel(got[n], ref[n]) < tol_single, (i, n, rel(got[n], ref[n]))
+            assert rel(got[n], o.field(n)) < tol_oracle, (i, n, rel(got[n], o.field(n)))
+        m.close()
+    ens.close()
+    monkeypatch.setenv("PS3D_ENSEMBLE_GROUPED", "0")
+    ens = Ensemble(members)
+    for i, f in enumerate(fields):
+        ens.upload(i, f["u"], f["v"], f["w"], f["b"])
+    l0 = ens.info()["launches"]
+    ens.integrate(nsteps)
+    # one step-kernel launch per step instead of one per group
+    assert (ens.info()["launches"] - l0) / nsteps == pytest.approx(per_step + 2)
+    ens.close()
+
+
 def test_graph_replay_matches_eager():
     """ps3d_integrate replays 3-step CUDA graphs; the result equals stepping
     one call at a time."""
