@@ -398,14 +398,14 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     // the y-split solve (k_colsolve) for the mixed rigid-lid path, with
     // PS3D_YSPLIT=1, where the register rows passes and its shared memory
     // take the grid (not for z-slabs, whose column slabs take the natural
-    // layout).  Off by default: at 256x256x128 it measured 486 us per step
-    // against 468 us for the y-lines passes and k_thomas2 (one 183 KB block
-    // per SM leaves its vertical solves eight warps to hide the FP64 chain)
+    // layout).  Off by default: at 256x256x128 it measured 461 us per step
+    // (two-CTA k_colsolve2; 486 us with the one-CTA k_colsolve) against
+    // 452 us for the y-lines passes and k_thomas2
     {
         const char* ys = std::getenv("PS3D_YSPLIT");
         const bool want = ys && ys[0] == '1';
         if (want && mixed && rigid && !split_solve && pa32.impl == 1 && rows_in_registers(nx, ny) &&
-            colsolve_fits(nz, ny) && fft_length_ok(ny / 2)) {
+            (colsolve_fits(nz, ny) || colsolve2_fits(nz, ny)) && fft_length_ok(ny / 2)) {
             CK(plyh.build(ny / 2, 0));
             int mr = 1;
             for (int q = 0; q < plyh.plan.nst; ++q) mr = std::max(mr, plyh.plan.r[q]);

@@ -192,6 +192,7 @@ int thomas_threads(int nz);
 // (FP32 spectra); p: the forward plane arguments (scale, half-length plan)
 cudaError_t launch_colsolve(const PlaneArgs& p, const ColumnArgs& c, cudaStream_t s);
 bool colsolve_fits(int nz, int ny);
+bool colsolve2_fits(int nz, int ny);   // the two-CTA cluster form (half the levels per CTA)
 // periodic z solve; zsolve_fits(nz, fp32) false: too tall for a block's shared memory
 cudaError_t launch_zsolve(const ColumnArgs& a, bool fp32, cudaStream_t s);
 bool zsolve_fits(int nz, bool fp32);

@@ -771,12 +771,198 @@ __global__ void __launch_bounds__(kCsThreads) k_colsolve(const ColSolveArgs a) {
     }
 }
 
+// The same solve split over a cluster of two CTAs by levels: CTA 0 holds
+// levels 0 .. H-1, CTA 1 levels nz-1 down to H (its local level q is level
+// nz-1-q), so each runs the y transforms of half the levels, and each
+// eliminates one end of the two-ended factorisation over its own levels:
+// the top-down chain (c', d') in CTA 0 and the bottom-up chain (c', d'') in
+// CTA 1, through the same pivots (the matrix is persymmetric).  The halves
+// meet through distributed shared memory: each CTA writes its end value
+// d'(m) or d''(jb) into the other's shared memory, one cluster barrier, and
+// both form the middle 2x2 solve from the same operands, so x(m) and
+// x(m+1) come out as in k_colsolve and k_thomas2, bit for bit.  The (0,0)
+// recurrence runs through CTA 0's levels, passes (p(H-2), p(H-1), f(H-1))
+// across, and CTA 1 continues after the barrier.  Half the shared memory of
+// k_colsolve per CTA: two clusters' CTAs fit an SM.
+constexpr int kCs2KC = 16;
+
+PS3D_HD size_t colsolve2_smem(int nz, int ny) {
+    const int ny2 = ny / 2, H = (nz + 1) / 2, nch = (H + kCs2KC - 1) / kCs2KC;
+    return align16((size_t)ny2 * (H | 1) * sizeof(float2)) +         // spectra [j][q]
+           align16((size_t)nch * 2 * 2 * ny2 * sizeof(double)) +      // checkpoints [chunk][2][column part]
+           align16((size_t)6 * 2 * ny2 * sizeof(double)) +            // own end values, pivots, exchange
+           plan_tables_bytes(ny2, sizeof(float2));
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kCsThreads, 2) k_colsolve2(const ColSolveArgs a) {
+    using T = float2;
+    pdl_trigger();
+    pdl_wait();   // inputs written by the preceding kernels
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    extern __shared__ __align__(16) unsigned char cs2_raw[];
+    const int nz = a.nz, ny = a.ny, ny2 = ny / 2, nxh = a.nxh;
+    const int H = (nz + 1) / 2, Bc = nz - H, m = H - 1, jb = Bc - 1;
+    const int L = rank == 0 ? H : Bc;   // levels held; chain index jj = local level q
+    const int ld = H | 1;
+    const int nch = (L + kCs2KC - 1) / kCs2KC;
+    const int ncp = 2 * ny2;            // column parts
+    unsigned char* base = cs2_raw;
+    T* buf = reinterpret_cast<T*>(base);                                   // [j][q], pitch ld
+    base += align16((size_t)ny2 * ld * sizeof(T));
+    double* ck = reinterpret_cast<double*>(base);                          // [chunk][2][cp]
+    base += align16((size_t)((H + kCs2KC - 1) / kCs2KC) * 2 * ncp * sizeof(double));
+    double* own = reinterpret_cast<double*>(base);                         // [0] end value, [1] c'(m), [2] c'(jb)
+    double* xch = own + 3 * ncp;                                           // [3][cp]: written by the other CTA
+    base += align16((size_t)6 * ncp * sizeof(double));
+    const PlanTables<float> ty = stage_plan<float>(a.ph, base);
+    const int units = nxh * 2;
+    const int pair = blockIdx.x >> 1;
+    const int inst = pair / units, u = pair - inst * units;
+    const int kx = u >> 1, half = u & 1;
+    T* g = reinterpret_cast<T*>(a.spec) + (long)inst * a.sM + (long)kx * ny + half * ny2;
+    const long ls = (long)nxh * ny;   // level stride
+    const unsigned long long pk = pol_keep(a.l2hint), pl = pol_last(a.l2hint);
+    const float sc = (float)a.scale;
+    for (int t = threadIdx.x; t < L * ny2; t += kCsThreads) {
+        const int q = t / ny2, j = t - q * ny2;
+        const int k = rank == 0 ? q : nz - 1 - q;
+        buf[j * ld + q] = cscale(ld_l2(&g[(long)k * ls + j], pl), sc);
+    }
+    fft_batch<false, float, 16>(buf, ld, L, a.ph, -1, ty.tw);   // synchronises before and after
+    cluster.sync();   // the other CTA is running before its shared memory is written
+    const int tid = threadIdx.x;
+    float* bf = reinterpret_cast<float*>(buf);
+    double* peer = cluster.map_shared_rank(xch, rank ^ 1);
+    const double fxa = a.fxa;
+    // pivot level jj: cp(0) = c/b_end, cp(jj) = c / (b_mid - cp(jj-1) a); d the chain's own value
+    // (d' from the top in CTA 0, d'' from the bottom in CTA 1)
+    auto elim = [&](int jj, double dv, double bend, double bmid, double& cp, double& d) {
+        if (jj == 0) {
+            cp = fxa / bend;
+            d = dv / bend;
+        } else {
+            const double r = rcp_newton(bmid - cp * fxa);
+            cp = fxa * r;
+            d = (dv - d * fxa) * r;
+        }
+    };
+    // ---- forward eliminations over this CTA's levels
+    for (int p0 = 0; p0 < ny2; p0 += kCsThreads / 2) {
+        const int p = p0 + (tid >> 1), part = tid & 1, c = 2 * p + part;
+        if (p < ny2) {
+            float* col = bf + (size_t)p * ld * 2 + part;   // local level q at col[2 q]
+            const int ky = 2 * ty.ipos[p] + half;
+            const double ks = a.hkx[kx] + a.hky[ky];
+            if (!(ks > 0)) {
+                if (rank == 0) {
+                    // (0,0): p(1) = 0, p(2) = f(1) dz^2 dsqr, p(k+1) = 2p(k) - p(k-1) + f(k) dz^2 dsqr
+                    double x0 = 0.0, x1 = 0.0, fprev = 0.0;
+                    for (int q = 0; q < H; ++q) {
+                        const double xk = q == 0 ? 0.0 : 2 * x1 - x0 + fprev * a.dz2dsqr;
+                        fprev = (double)col[2 * q];
+                        x0 = x1; x1 = xk;
+                        col[2 * q] = (float)xk;
+                    }
+                    peer[c] = x0; peer[ncp + c] = x1; peer[2 * ncp + c] = fprev;
+                }
+            } else {
+                const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+                double cp = 0.0, d = 0.0, cp_jb = 0.0;
+                for (int ch = 0; ch < nch; ++ch) {
+                    ck[(size_t)(ch * 2) * ncp + c] = cp;
+                    ck[(size_t)(ch * 2 + 1) * ncp + c] = d;
+#pragma unroll
+                    for (int q = 0; q < kCs2KC; ++q) {
+                        const int jj = ch * kCs2KC + q;
+                        if (jj < L) {
+                            elim(jj, (double)col[2 * jj], bend, bmid, cp, d);
+                            if (jj == jb) cp_jb = cp;
+                        }
+                    }
+                }
+                // c'(m): CTA 1 ends at jb, one level short of m when nz is odd
+                double cp_m = cp;
+                if (rank == 1 && m > jb) {
+                    double dd = 0.0;
+                    elim(m, 0.0, bend, bmid, cp_m, dd);
+                }
+                own[c] = d; own[ncp + c] = cp_m; own[2 * ncp + c] = cp_jb;
+                peer[c] = d;
+            }
+        }
+    }
+    cluster.sync();   // both ends' values delivered
+    for (int p0 = 0; p0 < ny2; p0 += kCsThreads / 2) {
+        const int p = p0 + (tid >> 1), part = tid & 1, c = 2 * p + part;
+        if (p < ny2) {
+            float* col = bf + (size_t)p * ld * 2 + part;
+            const int ky = 2 * ty.ipos[p] + half;
+            const double ks = a.hkx[kx] + a.hky[ky];
+            if (!(ks > 0)) {
+                if (rank == 1) {
+                    double x0 = xch[c], x1 = xch[ncp + c], fprev = xch[2 * ncp + c];
+                    for (int k = H; k < nz; ++k) {
+                        const int q = nz - 1 - k;
+                        const double xk = 2 * x1 - x0 + fprev * a.dz2dsqr;
+                        fprev = (double)col[2 * q];
+                        x0 = x1; x1 = xk;
+                        col[2 * q] = (float)xk;
+                    }
+                }
+            } else {
+                const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
+                const double dp_m = rank == 0 ? own[c] : xch[c];
+                const double dq_jb = rank == 0 ? xch[c] : own[c];
+                const double cp_m = own[ncp + c], cp_jb = own[2 * ncp + c];
+                const double xt = (dp_m - cp_m * dq_jb) / (1.0 - cp_m * cp_jb);   // x(m)
+                double x = rank == 0 ? xt : dq_jb - cp_jb * xt;                     // CTA 1: x(m+1)
+                const int top = rank == 0 ? m : jb;   // the chain's last level holds x as formed
+                for (int ch = nch - 1; ch >= 0; --ch) {
+                    const int jc = ch * kCs2KC;
+                    double cpv = ck[(size_t)(ch * 2) * ncp + c], dv = ck[(size_t)(ch * 2 + 1) * ncp + c];
+                    double cpl[kCs2KC], dl[kCs2KC];
+#pragma unroll
+                    for (int q = 0; q < kCs2KC; ++q) {
+                        const int jj = jc + q;
+                        if (jj < L) elim(jj, (double)col[2 * jj], bend, bmid, cpv, dv);
+                        cpl[q] = cpv; dl[q] = dv;
+                    }
+#pragma unroll
+                    for (int q = kCs2KC - 1; q >= 0; --q) {
+                        const int jj = jc + q;
+                        if (jj < L) {
+                            if (jj < top) x = dl[q] - cpl[q] * x;
+                            col[2 * jj] = (float)x;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    fft_batch<true, float, 16>(buf, ld, L, a.ph, +1, ty.tw);
+    for (int t = threadIdx.x; t < L * ny2; t += kCsThreads) {
+        const int q = t / ny2, j = t - q * ny2;
+        const int k = rank == 0 ? q : nz - 1 - q;
+        st_l2(&g[(long)k * ls + j], buf[j * ld + q], pk);
+    }
+}
+
 bool colsolve_fits(int nz, int ny) {
     return ny % 16 == 0 && colsolve_smem(nz, ny) <= 227 * 1024 - 64;
 }
 
+bool colsolve2_fits(int nz, int ny) {
+    return ny % 16 == 0 && colsolve2_smem(nz, ny) <= 227 * 1024 - 64;
+}
+
 cudaError_t launch_colsolve(const PlaneArgs& p, const ColumnArgs& c, cudaStream_t s) {
-    if (!colsolve_fits(c.nz, c.ny) || plan_max_radix(p.py) > 16) return cudaErrorInvalidValue;
+    // the two-CTA form where it fits, unless PS3D_COLSOLVE=1 pins the one-CTA form
+    const char* fv = std::getenv("PS3D_COLSOLVE");
+    const int form = fv ? std::atoi(fv) : 2;
+    const bool two = form != 1 && colsolve2_fits(c.nz, c.ny);
+    if (!two && !colsolve_fits(c.nz, c.ny)) return cudaErrorInvalidValue;
+    if (plan_max_radix(p.pyh) > 16) return cudaErrorInvalidValue;
     ColSolveArgs a{};
     a.nz = c.nz; a.ny = c.ny; a.nxh = c.nxh;
     a.spec = c.spec; a.sM = c.sM; a.batch = std::max(1, c.batch);
@@ -786,6 +972,7 @@ cudaError_t launch_colsolve(const PlaneArgs& p, const ColumnArgs& c, cudaStream_
     a.fxa = c.fxa; a.dz2dsqr = c.dz2dsqr;
     a.l2hint = l2hint_mode();
     const dim3 g((unsigned)(c.nxh * 2 * a.batch)), b(kCsThreads);
+    if (two) return launch_pdl(k_colsolve2, dim3(2 * g.x), b, colsolve2_smem(c.nz, c.ny), s, a);
     return launch_pdl(k_colsolve, g, b, colsolve_smem(c.nz, c.ny), s, a);
 }
 
@@ -1703,6 +1890,7 @@ static cudaError_t setup_t() {
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
     if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
     if ((e = max_dynamic_smem(k_colsolve))) return e;
+    if ((e = max_dynamic_smem(k_colsolve2))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, false>))) return e;
     if ((e = setup_m<R, 16>())) return e;

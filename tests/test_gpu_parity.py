@@ -352,6 +352,34 @@ def test_mixed_ysplit_solve(shape, ysplit, plane_impl, monkeypatch):
     assert max(err.values()) < TOL_MIXED, err
 
 
+@pytest.mark.parametrize("shape", [(128, 64, 32), (128, 32, 17), (128, 64, 2), (128, 32, 3)])
+def test_colsolve_two_cta_form_matches_one_cta(shape, monkeypatch):
+    """k_colsolve2 splits each half-line's levels over a cluster of two CTAs
+    (each eliminates one end, the ends meet through distributed shared
+    memory); it runs the same operations as the one-CTA k_colsolve, so the
+    steps and an explicit solve agree bit for bit (odd nz and nz = 2, 3
+    included)."""
+    monkeypatch.setenv("PS3D_YSPLIT", "1")
+    monkeypatch.setenv("PS3D_PLANE_IMPL", "1")
+    monkeypatch.setenv("PS3D_AUTOTUNE", "0")
+    p = cf.eddy_params(*shape, precision=abi.PS3D_MIXED)
+    f = cf.add_noise(p, cf.eddy_fields(p), "b", rel=1e-3, seed=5)
+    out = {}
+    for form in ("1", "2"):
+        monkeypatch.setenv("PS3D_COLSOLVE", form)
+        m = Model(p)
+        assert "rows+colsolve" in m.describe(), m.describe()
+        m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+        m.run(7)
+        st = m.download(tendencies=False)
+        m.pressure_solver()
+        out[form] = (st, m.download(tendencies=False))
+        m.close()
+    for a, b in zip(out["1"], out["2"]):
+        for n in ("u", "v", "w", "b", "p"):
+            assert np.array_equal(a[n], b[n]), (shape, n, rel(a[n], b[n]))
+
+
 def test_bad_params_rejected():
     p = small_params(33, 32, 16)
     with pytest.raises(PS3DError) as ei:
