@@ -334,8 +334,10 @@ PS3D_API int ps3d_ensemble_info(ps3d_ensemble* e, int* ngroups, long long* launc
  * (PACK_STATE, exchange, UNPACK_STATE).  ps3d_slab_group_step does all of it
  * for the ranks of one process (device copies; one GPU or several).
  * Upload/download take the rank's interior levels, [nzl][ny][nx] doubles,
- * x fastest (no halos).  Rigid lid and the fused step only
- * (PS3D_ERR_UNSUPPORTED otherwise).                                        */
+ * x fastest (no halos).  Rigid lid or triply periodic, the fused step
+ * (Laplacian friction, wavemaker and background-flow forcing; not
+ * biharmonic friction, a host callback, or background flow together with
+ * Laplacian friction: PS3D_ERR_UNSUPPORTED).                               */
 #define PS3D_SLAB_TENDENCY     0
 #define PS3D_SLAB_PACK_STATE   1
 #define PS3D_SLAB_UNPACK_STATE 2
@@ -359,6 +361,13 @@ PS3D_API int ps3d_slab_bind(ps3d_slab* s, void* xbuf, void* colbuf, void* hsend,
 PS3D_API int ps3d_slab_upload(ps3d_slab* s, const double* u, const double* v, const double* w, const double* b);
 /* applies the pending pressure correction first; waits for the stream      */
 PS3D_API int ps3d_slab_download(ps3d_slab* s, double* u, double* v, double* w, double* b, double* p);
+/* set_forcing (lee_wave1.f90:232-332; config.f90:224-237) for the rank's
+ * levels: kind PS3D_FORCE_WAVEMAKER and/or PS3D_FORCE_BACKGROUND (NONE
+ * clears).  Every field pointer of f (NULL = zero field) holds the rank's
+ * levels with one halo level each side, [nzl+2][ny][nx] doubles: global
+ * levels k0-1 .. k0+nzl, taken periodically in z (the rigid-lid masks never
+ * read the wrapped levels).  The callback kind is not supported on slabs.   */
+PS3D_API int ps3d_slab_set_forcing(ps3d_slab* s, const ps3d_forcing* f);
 PS3D_API int ps3d_slab_phase(ps3d_slab* s, int phase);
 PS3D_API int ps3d_slab_sync(ps3d_slab* s);
 PS3D_API int ps3d_slab_group_step(ps3d_slab* const* ranks, int n, int nsteps);

@@ -505,7 +505,7 @@ int Ctx::step(int itt_, int tau_, int taum1_, int taum2_) {
         for (int f = 0; f < 4; ++f) { a.wr[f] = (const double*)wr[f].p; a.wi[f] = (const double*)wi[f].p; }
     }
     const bool fused = fused_step();
-    if (split_solve && (!fused || wm || bg)) return PS3D_ERR_UNSUPPORTED;   // z-slabs: the fused step, no forcing
+    if (split_solve && !fused) return PS3D_ERR_UNSUPPORTED;   // z-slabs: the fused step only
     if (!fused) {
         int rc = materialize();
         if (rc) return rc;

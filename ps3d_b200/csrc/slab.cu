@@ -36,8 +36,9 @@
 // caller's: NCCL all-to-all and send/receive between processes (the Python
 // driver, ps3d_b200/slab.py), or ps3d_slab_group_step for contexts in one
 // process, which copies device to device.  Supported: rigid lid or triply
-// periodic, FP64 and mixed, the fused step (Laplacian friction, no
-// biharmonic, no forcing).
+// periodic, FP64 and mixed, the fused step (Laplacian friction, the
+// wavemaker and background-flow forcing of set_forcing on the rank's levels
+// and one halo level each side; no biharmonic friction, no host callback).
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -442,6 +443,54 @@ PS3D_API int ps3d_slab_download(ps3d_slab* s, double* u, double* v, double* w, d
     const size_t bytes = (size_t)s->nzl * s->plane * sizeof(double);
     for (int q = 0; q < 5; ++q)
         if (f[q]) CK(cudaMemcpy(f[q], s->lvl(q < 4 ? c.field(q) : (double*)c.p.p, 1), bytes, cudaMemcpyDeviceToHost));
+    return PS3D_OK;
+    SGUARD_END
+}
+
+PS3D_API int ps3d_slab_set_forcing(ps3d_slab* s, const ps3d_forcing* f) {
+    SGUARD_BEGIN
+    if (!s) return PS3D_ERR_BADPARAM;
+    Ctx& c = *s->ctx;
+    cudaSetDevice(c.device);
+    CK(cudaStreamSynchronize(c.stream));
+    for (int q = 0; q < 4; ++q) { c.wr[q].release(); c.wi[q].release(); }
+    c.ub.release(); c.bb.release();
+    c.invalidate_graph();
+    ++c.forcing_gen;
+    c.fkind = 0; c.fn = nullptr; c.user = nullptr;
+    if (!f || f->kind == PS3D_FORCE_NONE) return PS3D_OK;
+    if (f->kind & ~(PS3D_FORCE_WAVEMAKER | PS3D_FORCE_BACKGROUND | PS3D_FORCE_CALLBACK)) return PS3D_ERR_BADPARAM;
+    if (f->kind & PS3D_FORCE_CALLBACK) return PS3D_ERR_UNSUPPORTED;
+    // local arrays: levels 0 .. nzl+2 as the state's (halo 0, interior 1 .. nzl, halo nzl+1; the
+    // second upper halo, which only p uses, stays zero)
+    const size_t nloc = (size_t)(s->nzl + 3) * s->plane * sizeof(double);
+    const size_t nin = (size_t)(s->nzl + 2) * s->plane * sizeof(double);
+    auto put = [&](DevBuf& d, const double* h) -> cudaError_t {
+        cudaError_t e = d.alloc(nloc);
+        if (e) return e;
+        if ((e = cudaMemset(d.p, 0, nloc))) return e;
+        return h ? cudaMemcpy(d.p, h, nin, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    c.omega = f->omega;
+    if (f->kind & PS3D_FORCE_WAVEMAKER) {
+        const double* r[4] = {f->u_r, f->v_r, f->w_r, f->b_r};
+        const double* im[4] = {f->u_i, f->v_i, f->w_i, f->b_i};
+        for (int q = 0; q < 4; ++q) {
+            if (r[q]) CK(put(c.wr[q], r[q]));
+            if (im[q]) CK(put(c.wi[q], im[q]));
+        }
+    }
+    if (f->kind & PS3D_FORCE_BACKGROUND) {
+        CK(put(c.ub, f->u_back));
+        CK(put(c.bb, f->b_back));
+    }
+    c.fkind = f->kind;
+    if (!c.fused_step()) {   // background flow with Laplacian friction: the generic step
+        for (int q = 0; q < 4; ++q) { c.wr[q].release(); c.wi[q].release(); }
+        c.ub.release(); c.bb.release();
+        c.fkind = 0;
+        return PS3D_ERR_UNSUPPORTED;
+    }
     return PS3D_OK;
     SGUARD_END
 }

@@ -20,8 +20,10 @@ import ctypes as C
 
 import numpy as np
 
-from .abi import PS3D_FP64, Params
+from .abi import PS3D_FORCE_NONE, PS3D_FP64, Forcing, Params
 from .model import _check, load
+
+FORCING_FIELDS = ("u_r", "v_r", "w_r", "b_r", "u_i", "v_i", "w_i", "b_i", "u_back", "b_back")
 
 PHASE = {"tendency": 0, "pack_state": 1, "unpack_state": 2, "forward": 3, "vsolve": 4, "inverse": 5,
          "pack_p": 6, "unpack_p": 7, "end_step": 8}
@@ -48,6 +50,7 @@ def _lib():
     L.ps3d_slab_phase.argtypes = [vp, C.c_int]
     L.ps3d_slab_sync.argtypes = [vp]
     L.ps3d_slab_group_step.argtypes = [C.POINTER(vp), C.c_int, C.c_int]
+    L.ps3d_slab_set_forcing.argtypes = [vp, C.POINTER(Forcing)]
     L._slab_argtypes = True
     return L
 
@@ -105,6 +108,29 @@ class Slab:
                "ps3d_slab_download")
         return out
 
+    def set_forcing(self, kind=PS3D_FORCE_NONE, omega=0.0, **fields):
+        """set_forcing on this rank's levels: kind (wavemaker and/or background
+        flow), omega, and whole-grid interior fields [nz][ny][nx] named as
+        Model.set_forcing names them (u_r .. b_i, u_back, b_back; absent =
+        zero).  The rank keeps its levels and one level each side, periodic
+        in z."""
+        f = Forcing()
+        f.kind = kind
+        f.omega = omega
+        nz = self.params.nz
+        lev = [(self.k0 - 1 + q) % nz for q in range(self.nzl + 2)]
+        keep = []
+        for name in FORCING_FIELDS:
+            a = fields.get(name)
+            if a is None:
+                continue
+            a = np.asarray(a, dtype=np.float64)
+            assert a.shape == (nz, self.params.ny, self.params.nx), (name, a.shape)
+            loc = np.ascontiguousarray(a[lev])
+            keep.append(loc)
+            setattr(f, name, _dp(loc))
+        _check(self.L.ps3d_slab_set_forcing(self.h, C.byref(f)), "ps3d_slab_set_forcing")
+
     def phase(self, name):
         _check(self.L.ps3d_slab_phase(self.h, PHASE[name]), "ps3d_slab_phase " + name)
 
@@ -137,6 +163,11 @@ class SlabGroup:
         for s in self.ranks:
             sl = slice(s.k0, s.k0 + s.nzl)
             s.upload(u[sl], v[sl], w[sl], b[sl])
+
+    def set_forcing(self, kind=PS3D_FORCE_NONE, omega=0.0, **fields):
+        """Whole-grid interior forcing fields [nz][ny][nx] (Slab.set_forcing)."""
+        for s in self.ranks:
+            s.set_forcing(kind, omega, **fields)
 
     def step(self, nsteps=1):
         arr = (C.c_void_p * len(self.ranks))(*[s.h.value for s in self.ranks])
@@ -219,6 +250,11 @@ class DistSlab:
         """This rank's interior levels [nzl][ny][nx]."""
         self.slab.upload(u, v, w, b)
         self.need_halo = True
+
+    def set_forcing(self, kind=PS3D_FORCE_NONE, omega=0.0, **fields):
+        """Whole-grid interior forcing fields [nz][ny][nx]; this rank keeps
+        its levels and one level each side (Slab.set_forcing)."""
+        self.slab.set_forcing(kind, omega, **fields)
 
     def _halo(self, which):
         s = self.slab

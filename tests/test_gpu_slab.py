@@ -129,6 +129,50 @@ def test_periodic_slabs_match_single_grid(nranks, precision, tol, monkeypatch):
     assert max(err.values()) < tol, err
 
 
+@pytest.mark.parametrize("precision,tol", [(abi.PS3D_FP64, TOL), (abi.PS3D_MIXED, 1e-10)])
+@pytest.mark.parametrize("nranks", [2, 4])
+def test_forced_slabs_match_single_grid(nranks, precision, tol, monkeypatch):
+    """The lee-wave case (triply periodic, background flow and wavemaker,
+    lee_wave1.f90:232-332) in z-slabs: each rank holds the forcing fields of
+    its levels and one halo level each side (the background terms read the
+    levels above and below)."""
+    monkeypatch.setenv("PS3D_TUNE", "im1,C1,rc8,tj16,ly16,pol0,kc8")
+    p = cf.lee_wave_params(64, 32, 32, precision=precision)
+    fr = cf.lee_wave_forcing(p, seed=3, amp=1e-4)
+    f = random_state(p, seed=19, amp=0.02)
+    kind = abi.PS3D_FORCE_WAVEMAKER | abi.PS3D_FORCE_BACKGROUND
+    monkeypatch.setenv("PS3D_PLANE_IMPL", "1")
+    m = Model(p)
+    m.set_forcing(kind, fr["omega"], **{n: fr[n] for n in ("w_r", "w_i", "u_back", "b_back")})
+    m.upload(**{n: f[n] for n in "uvwb"})
+    m.run(8)
+    ref = {n: _interior(a) for n, a in m.download(tendencies=False).items() if n in NAMES}
+    m.close()
+    g = SlabGroup(p, nranks)
+    g.set_forcing(kind, fr["omega"], **{n: _interior(fr[n]) for n in ("w_r", "w_i", "u_back", "b_back")})
+    g.upload(*[_interior(f[n]) for n in "uvwb"])
+    g.step(8)
+    got = g.download()
+    g.close()
+    assert np.abs(got["w"]).max() > 0.0
+    err = {n: rel(got[n], ref[n]) for n in NAMES}
+    assert max(err.values()) < tol, err
+
+
+def test_slab_forcing_rejects_callback_and_background_with_friction():
+    p = small_params(32, 32, 16, rigid=True)   # Laplacian friction on
+    s = Slab(p, 2, 0)
+    z = np.zeros((16, 32, 32))
+    with pytest.raises(PS3DError) as e:
+        s.set_forcing(abi.PS3D_FORCE_BACKGROUND, 0.0, u_back=z)
+    assert e.value.status == abi.PS3D_ERR_UNSUPPORTED
+    with pytest.raises(PS3DError) as e:
+        s.set_forcing(abi.PS3D_FORCE_CALLBACK)
+    assert e.value.status == abi.PS3D_ERR_UNSUPPORTED
+    s.set_forcing(abi.PS3D_FORCE_WAVEMAKER, 1e-3, w_r=z)   # the wavemaker alone takes the fused step
+    s.close()
+
+
 @pytest.mark.parametrize("rigid", [True, False])
 def test_slabs_match_oracle(rigid):
     """Four slabs of one grid against the CPU oracle, 10 AB3 steps."""
