@@ -437,47 +437,69 @@ def projection_run(dev, nx=256, ny=256, nz=64):
     """normal_mode_projection (diag_opt_balance.f90:288-310) on a rigid-lid
     eddy of the largest serving size: forward transform (4 plane FFTs + 4
     vertical-mode transforms), eigen projection, backward transform.  Median
-    of 5 timed calls; the vertical-mode transform's FP64 roofline from a
-    profiled call (2 nz^2 flop per complex multiply-add, i.e. 4 nz^2 per
-    complex column, against the FP64 GEMM throughput measured here by cuBLAS
-    DGEMM; the nominal B200 figure is 40 TFLOP/s)."""
+    of 5 timed calls in each form of the vertical-mode transform: the dense
+    FP64 product (the engine's choice up to nz = 64; 4 nz^2 flop per complex
+    column, against the FP64 GEMM throughput measured here by cuBLAS DGEMM)
+    and the FFT of length 2 nz (above nz = 64; an HBM-bound pass: the column
+    data read and written once, against the measured copy bandwidth)."""
     import torch
     from ps3d_b200 import configs as cf
     from ps3d_b200.model import Model
     p = cf.eddy_params(nx, ny, nz)
     f = cf.eddy_fields(p)
-    m = Model(p, device=dev)
-    m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
-    m.normal_mode_projection()
-    st = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t = []
-    for _ in range(5):
-        e0.record(st)
-        m.normal_mode_projection()
-        e1.record(st)
-        e1.synchronize()
-        t.append(e0.elapsed_time(e1))
-    m.profile(True)
-    m.normal_mode_projection()
-    kern = m.profile_read()
-    m.profile(False)
-    m.close()
-    ms_v, n_v = kern["vmode"]
     ncol = (nx // 2 + 1) * ny
-    flop = 4.0 * nz * nz * ncol            # per launch
-    per = ms_v / max(n_v, 1)
+
+    def measure(form):
+        old = os.environ.get("PS3D_VMODE_FORM")
+        os.environ["PS3D_VMODE_FORM"] = form
+        try:
+            m = Model(p, device=dev)
+        finally:
+            if old is None:
+                del os.environ["PS3D_VMODE_FORM"]
+            else:
+                os.environ["PS3D_VMODE_FORM"] = old
+        m.upload(**{n: f[n] for n in ("u", "v", "w", "b")})
+        m.normal_mode_projection()
+        st = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{dev}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t = []
+        for _ in range(5):
+            e0.record(st)
+            m.normal_mode_projection()
+            e1.record(st)
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1))
+        m.profile(True)
+        m.normal_mode_projection()
+        kern = m.profile_read()
+        m.profile(False)
+        m.close()
+        ms_v, n_v = kern["vmode"]
+        return t, kern, ms_v / max(n_v, 1), int(n_v)
+
+    t_d, kern_d, per_d, n_d = measure("1")
+    t_f, kern_f, per_f, n_f = measure("2")
+    nbytes = 2 * 16 * ncol * nz            # per launch: the columns read and written once
+    flop = 4.0 * nz * nz * ncol            # per launch of the dense product
     try:
         peak_fp64, peak_kind = fp64_gemm_peak(dev), "measured: cuBLAS FP64 GEMM 8192^3, best of 5"
     except Exception:
         peak_fp64, peak_kind = 40.0, "nominal B200 FP64"
-    return {"grid": [nx, ny, nz], "ms_median": float(np.median(t)), "ms_windows": t,
-            "vmode": {"launches": int(n_v), "ms_per_launch": per, "flop_per_launch": flop,
-                      "achieved_tflops": flop / (per * 1e-3) / 1e12 if n_v else None,
-                      "peak_tflops": peak_fp64, "peak_kind": peak_kind,
-                      "frac": (flop / (per * 1e-3) / 1e12) / peak_fp64 if n_v else None,
-                      "bytes_per_launch": 2 * 16 * ncol * nz},
-            "kernels_ms": {k: v[0] for k, v in kern.items() if v[1]}}
+    hbm, hbm_kind = peaks()
+    dense = {"ms_median": float(np.median(t_d)), "ms_windows": t_d, "ms_per_launch": per_d, "launches": n_d,
+             "flop_per_launch": flop, "achieved_tflops": flop / (per_d * 1e-3) / 1e12 if n_d else None,
+             "peak_tflops": peak_fp64, "peak_kind": peak_kind,
+             "frac": (flop / (per_d * 1e-3) / 1e12) / peak_fp64 if n_d else None}
+    fft = {"ms_median": float(np.median(t_f)), "ms_windows": t_f, "ms_per_launch": per_f, "launches": n_f,
+           "bytes_per_launch": nbytes, "achieved_gbs": nbytes / (per_f * 1e-3) / 1e9 if n_f else None,
+           "peak_gbs": hbm, "peak_kind": hbm_kind,
+           "frac": (nbytes / (per_f * 1e-3) / 1e9) / hbm if n_f else None}
+    default = "fft" if nz > 64 else "dense"
+    chosen = fft if default == "fft" else dense
+    return {"grid": [nx, ny, nz], "ms_median": chosen["ms_median"], "vmode_form": default,
+            "vmode_dense": dense, "vmode_fft": fft,
+            "kernels_ms": {k: v[0] for k, v in (kern_f if default == "fft" else kern_d).items() if v[1]}}
 
 
 def serve_run(dev, n_requests=40, rate_hz=50.0, max_active=8, max_batch=8):

@@ -359,6 +359,23 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
         const std::vector<double> phi2 = with_t(phi), psi2 = with_t(psi), psib2 = with_t(psib);
         CK(up(m_phi, phi2.data(), phi2.size() * 8)); CK(up(m_psi, psi2.data(), psi2.size() * 8));
         CK(up(m_psib, psib2.data(), psib2.size() * 8));
+        // the same transforms by FFT of length 2 nz where the length factors
+        // and nz > 64: at 256x256x128 90.6 us per transform against 202 us
+        // for the dense product, at 256x256x64 52 against 49 us.
+        // PS3D_VMODE_FORM=0|1 keeps the dense products, =2 takes the FFT
+        const char* vf = std::getenv("PS3D_VMODE_FORM");
+        const bool want_fft = vf && (vf[0] == '0' || vf[0] == '1') ? false : (nz > 64 || (vf && vf[0] == '2'));
+        if (want_fft && vert_dtt_fits(nz)) {
+            CK(pl2z.build(2 * nz, 2));   // radix-8 first: the transform's radix-8 build
+            int mr = 1;
+            for (int q = 0; q < pl2z.plan.nst; ++q) mr = std::max(mr, pl2z.plan.r[q]);
+            if (mr <= 8) {
+                std::vector<double2> tw(nz);
+                for (int j = 0; j < nz; ++j) tw[j] = make_double2(std::cos(pi * j / (2.0 * nz)), std::sin(pi * j / (2.0 * nz)));
+                CK(up(t_dtw, tw.data(), nz * 16));
+                vmode_fft = true;
+            }
+        }
     }
     // plane kernel shapes
     PlaneArgs base{};
@@ -942,9 +959,30 @@ int Ctx::pressure_solve(bool lazy, bool warm) {
 // ---------------------------------------------------------------------------
 // forward_transform / backward_transform (diag_balance.f90:421-462)
 // ---------------------------------------------------------------------------
+// the vertical-mode transform of field f (u, v: phi; w: psi; b: psib) of one
+// instance: analysis (fwd, my_fft_vert_mode, scale dz) or synthesis
+// (my_ifft_vert_mode), by FFT or as the dense product
+int Ctx::vmode_transform(const double2* in, double2* out, int f, bool fwd) {
+    const DevBuf* modes[4] = {&m_phi, &m_phi, &m_psi, &m_psib};
+    if (vmode_fft) {
+        VertDttArgs d{};
+        d.in = in; d.out = out; d.nz = nz; d.ncol = M2;
+        d.scale = fwd ? P.dz : 1.0;
+        d.plan = pl2z.plan;
+        d.tw = (const double2*)t_dtw.p;
+        d.c0 = std::sqrt(1.0 / P.Lz); d.c1 = std::sqrt(2.0 / P.Lz);
+        const int kind = f < 2 ? 0 : (f == 2 ? 1 : 2);
+        LAUNCH(PS3D_K_VMODE, launch_vert_dtt(d, kind, fwd, stream));
+        return PS3D_OK;
+    }
+    // the forward product takes the transposed matrix, the buffer's second half
+    const double* A = (const double*)modes[f]->p + (fwd ? (size_t)nz * nz : 0);
+    LAUNCH(PS3D_K_VMODE, launch_vert_mode(in, out, A, nz, M2, fwd ? P.dz : 1.0, stream));
+    return PS3D_OK;
+}
+
 int Ctx::forward_transform(const double* const* in) {
     CK(ensure_spectral4());
-    const DevBuf* modes[4] = {&m_phi, &m_phi, &m_psi, &m_psib};
     for (int f = 0; f < 4; ++f) {
         PlaneArgs a = pa64;
         a.mode = 1; a.src = in[f]; a.scale = P.dx * P.dy;
@@ -953,9 +991,10 @@ int Ctx::forward_transform(const double* const* in) {
         LAUNCH(PS3D_K_OTHER, launch_plane_fwd(a, false, stream));
         if (rigid) {
             // A = the transposed matrix, the second half of the mode buffer
-            for (int m = 0; m < batch; ++m)
-                LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)qtmp.p + m * M, (double2*)spec4[f].p + m * M,
-                                                      (const double*)modes[f]->p + (size_t)nz * nz, nz, M2, P.dz, stream));
+            for (int m = 0; m < batch; ++m) {
+                int rc = vmode_transform((const double2*)qtmp.p + m * M, (double2*)spec4[f].p + m * M, f, true);
+                if (rc) return rc;
+            }
         } else {
             ColumnArgs c{};
             c.nx = nx; c.ny = ny; c.nz = nz; c.nxh = nxh; c.spec = spec4[f].p;
@@ -967,13 +1006,13 @@ int Ctx::forward_transform(const double* const* in) {
     return PS3D_OK;
 }
 int Ctx::backward_transform(double* const* out) {
-    const DevBuf* modes[4] = {&m_phi, &m_phi, &m_psi, &m_psib};
     for (int f = 0; f < 4; ++f) {
         void* src = spec4[f].p;
         if (rigid) {
-            for (int m = 0; m < batch; ++m)
-                LAUNCH(PS3D_K_VMODE, launch_vert_mode((const double2*)spec4[f].p + m * M, (double2*)qtmp.p + m * M,
-                                                      (const double*)modes[f]->p, nz, M2, 1.0, stream));
+            for (int m = 0; m < batch; ++m) {
+                int rc = vmode_transform((const double2*)spec4[f].p + m * M, (double2*)qtmp.p + m * M, f, false);
+                if (rc) return rc;
+            }
             src = qtmp.p;
         } else {
             ColumnArgs c{};

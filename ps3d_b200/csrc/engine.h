@@ -222,6 +222,22 @@ cudaError_t launch_vert_mode(const double2* in, double2* out, const double* A, i
                              cudaStream_t s);
 bool vert_mode_fits(int nz);
 cudaError_t modes_setup();   // per device, before the first launch_vert_mode
+// The rigid-lid vertical-mode transforms by FFT of length 2 nz (modes.cu):
+// kind 0 = phi (DCT-II / DCT-III), 1 = psi (DST-I), 2 = psib (DST-II / DST-III)
+struct VertDttArgs {
+    const double2* in;
+    double2* out;
+    int nz;
+    long ncol;          // columns: levels are ncol apart
+    double scale;       // forward: dz; backward: 1
+    FFTPlan plan;       // length 2 nz, radices <= 8 (radix-8-first plan)
+    const double2* tw;  // e^{i pi j / 2 nz}, j = 0 .. nz-1
+    double c0, c1;      // sqrt(1/Lz) (phi's mode 0), sqrt(2/Lz) (every other mode)
+    int cols;           // columns per block (set by the launcher)
+};
+bool fft_length_ok(int n);
+bool vert_dtt_fits(int nz);
+cudaError_t launch_vert_dtt(const VertDttArgs& a, int kind, bool fwd, cudaStream_t s);
 
 // layout.cu: host halo layout <-> device interior layout (h_dev holds the
 // whole host array, (nx+4)*(ny+4)*(nz+4) doubles)

@@ -218,10 +218,15 @@ def test_projection(rigid, mode):
     assert max(err.values()) < TOL_KERNEL, err
 
 
-@pytest.mark.parametrize("nz", [33, 64, 128])
-def test_normal_mode_projection_tall_rigid(nz):
-    """Rigid-lid projection through the vertical-mode transforms at nz = 128
-    (the tiled FP64 product), 64 and an odd 33 (the unpaired-load path)."""
+@pytest.mark.parametrize("form", ["fft", "dense"])
+@pytest.mark.parametrize("nz", [33, 60, 64, 128])
+def test_normal_mode_projection_tall_rigid(nz, form, monkeypatch):
+    """Rigid-lid projection through the vertical-mode transforms at nz = 128,
+    64 and 60 (by FFT of length 2 nz, PS3D_VMODE_FORM=2, the default above
+    nz = 64: the mode matrices are sampled sines and cosines; or the dense
+    FP64 product, PS3D_VMODE_FORM=1) and an odd 33 (2 nz = 66 has a factor
+    11: the dense product, its unpaired-load path, in both cases)."""
+    monkeypatch.setenv("PS3D_VMODE_FORM", ("1" if nz % 2 == 0 else "0") if form == "dense" else "2")
     p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
     o, m = _pair(p, smooth_state(p, seed=15))
     o.project(abi.PS3D_PROJ_NORMAL_MODE)
