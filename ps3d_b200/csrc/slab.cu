@@ -66,6 +66,10 @@ struct ps3d_slab {
     ps3d::DevPlan plz;              // triply periodic: the global z transform
     DevBuf hkz;                     // ... and hat_ksqr(kz)/dsqr of the global levels
     int pass = 0;                   // solve pass: 0 full solve, 1 residual solve (mixed path)
+    cudaEvent_t ev = nullptr;       // ps3d_slab_group_step: marks this rank's stream for the others
+    ~ps3d_slab() {
+        if (ev) cudaEventDestroy(ev);
+    }
 
     // solve passes of the next step: 1 in FP64; in the mixed path 2 on a cold
     // start (full solve, then the residual one), else 1 (the residual solve
@@ -208,7 +212,7 @@ int slab_end_step(ps3d_slab* s) {
     return PS3D_OK;
 }
 
-// device-to-device copies between contexts of one process (any devices)
+// host waits for every rank's stream (the end of ps3d_slab_group_step)
 int sync_all(ps3d_slab* const* r, int n) {
     for (int q = 0; q < n; ++q) {
         cudaSetDevice(r[q]->ctx->device);
@@ -218,31 +222,50 @@ int sync_all(ps3d_slab* const* r, int n) {
     return PS3D_OK;
 }
 
+// The group driver orders the ranks' streams with events, without host
+// synchronisation: mark(q) records rank q's event on its stream, after(q, p)
+// makes rank q's stream wait for rank p's last mark.  Every wait on a mark is
+// issued (host order) before that event is recorded again.
+cudaError_t mark(const ps3d_slab* s) { return cudaEventRecord(s->ev, s->ctx->stream); }
+cudaError_t after(const ps3d_slab* s, const ps3d_slab* p) { return cudaStreamWaitEvent(s->ctx->stream, p->ev, 0); }
+
 int transport_halo(ps3d_slab* const* r, int n, int which) {
-    int rc = sync_all(r, n);
-    if (rc) return rc;
     const size_t pb = (size_t)r[0]->plane * sizeof(double);
     const int nd = kDown[which], nu = kUp[which];
+    for (int q = 0; q < n; ++q) { cudaSetDevice(r[q]->ctx->device); CK(mark(r[q])); }   // packed
     for (int q = 0; q < n; ++q) {
         const ps3d_slab* below = r[(q + n - 1) % n];
         const ps3d_slab* above = r[(q + 1) % n];
         char* in = (char*)r[q]->hrecv;
         cudaSetDevice(r[q]->ctx->device);
+        CK(after(r[q], below));
+        CK(after(r[q], above));
         // from below: what it sent up; from above: what it sent down
         CK(cudaMemcpyAsync(in, (const char*)below->hsend + nd * pb, nu * pb, cudaMemcpyDefault, r[q]->ctx->stream));
         CK(cudaMemcpyAsync(in + nu * pb, above->hsend, nd * pb, cudaMemcpyDefault, r[q]->ctx->stream));
     }
-    return sync_all(r, n);
+    // a rank's send planes are read by its neighbours' copies: it packs
+    // again only after those
+    for (int q = 0; q < n; ++q) { cudaSetDevice(r[q]->ctx->device); CK(mark(r[q])); }
+    for (int q = 0; q < n; ++q) {
+        cudaSetDevice(r[q]->ctx->device);
+        CK(after(r[q], r[(q + n - 1) % n]));
+        CK(after(r[q], r[(q + 1) % n]));
+    }
+    return PS3D_OK;
 }
 
 int transport_columns(ps3d_slab* const* r, int n, bool forward) {
-    int rc = sync_all(r, n);
-    if (rc) return rc;
     const size_t es = r[0]->es();
+    if (forward)
+        for (int q = 0; q < n; ++q) { cudaSetDevice(r[q]->ctx->device); CK(mark(r[q])); }   // packed
     for (int d = 0; d < n; ++d) {
         cudaSetDevice(r[d]->ctx->device);
+        if (forward)
+            for (int q = 0; q < n; ++q)
+                if (q != d) CK(after(r[d], r[q]));
         for (int q = 0; q < n; ++q) {
-            // the block of rank q's levels and rank d's columns
+            // the block of rank q's levels and rank d's columns, moved on rank d's stream
             const size_t bytes = (size_t)r[q]->nzl * r[d]->ccnt[d] * es;
             if (forward)
                 CK(cudaMemcpyAsync((char*)r[d]->colbuf + (size_t)q * r[q]->nzl * r[d]->ccnt[d] * es,
@@ -254,7 +277,16 @@ int transport_columns(ps3d_slab* const* r, int n, bool forward) {
                                    cudaMemcpyDefault, r[d]->ctx->stream));
         }
     }
-    return sync_all(r, n);
+    if (!forward) {
+        // every rank unpacks only after every rank's blocks have landed in its xbuf
+        for (int d = 0; d < n; ++d) { cudaSetDevice(r[d]->ctx->device); CK(mark(r[d])); }
+        for (int q = 0; q < n; ++q) {
+            cudaSetDevice(r[q]->ctx->device);
+            for (int d = 0; d < n; ++d)
+                if (d != q) CK(after(r[q], r[d]));
+        }
+    }
+    return PS3D_OK;
 }
 
 int group_halo(ps3d_slab* const* r, int n, int which) {
@@ -358,6 +390,7 @@ PS3D_API int ps3d_slab_create(const ps3d_params* global, int nranks, int rank, i
     CK(s->own_hs.alloc(s->hbytes()));
     CK(s->own_hr.alloc(s->hbytes()));
     s->xbuf = s->own_x.p; s->colbuf = s->own_col.p; s->hsend = s->own_hs.p; s->hrecv = s->own_hr.p;
+    CK(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming));
     *out = s.release();
     return PS3D_OK;
     SGUARD_END
