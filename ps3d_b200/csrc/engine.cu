@@ -746,10 +746,29 @@ int Ctx::autotune() {
     }
     bestpa.batch = 1;
     pa = bestpa;
-    // step kernel z chunk
+    // step kernel z chunk: 4, 8, 16, 32 and the chunk that best fills the
+    // last wave of blocks (cost ~ waves x (kc + 2) plane loads per block:
+    // at 256x256x128, kc 15 gives 2304 blocks, 3.9 waves of 592, against
+    // kc 16's 2048 blocks, 3.5 waves: 308 against 314 us)
+    std::vector<int> kcs = {4, 8, 16, 32};
+    {
+        StepArgs q{};
+        q.harm_uvw = (P.Ah > 0. || P.Av > 0.); q.harm_b = (P.Kh > 0. || P.Kv > 0.);
+        q.wm_on = (fkind & PS3D_FORCE_WAVEMAKER) ? 1 : 0;
+        const long slots = (long)prop.multiProcessorCount * step_resident(q, hist32);
+        const long tiles = (long)((nx + 31) / 32) * ((ny + 7) / 8) * std::max(1, batch);
+        double bestc = 1e300;
+        int mkc = 16;
+        for (int kc = 4; kc <= std::min(nz, 48); ++kc) {
+            const long blocks = tiles * ((nz + kc - 1) / kc);
+            const double c = (double)((blocks + slots - 1) / slots) * (kc + 2);
+            if (c < bestc * (1 - 1e-9)) { bestc = c; mkc = kc; }
+        }
+        if (std::find(kcs.begin(), kcs.end(), mkc) == kcs.end()) kcs.push_back(mkc);
+    }
     float bestk = 1e30f;
     int bestkc = kchunk;
-    for (int kc : {4, 8, 16, 32}) {
+    for (int kc : kcs) {
         if (kc > nz) continue;
         kchunk = kc;
         const float t = timeit([&]() -> int {

@@ -154,6 +154,8 @@ cudaError_t step_setup();   // opts the step kernels in to their dynamic shared 
 // which fused step kernel a launch of `a` runs (friction, wavemaker,
 // background-flow bits); grids of one grouped launch must agree
 int step_flavour(const StepArgs& a);
+// resident blocks per SM of the step kernel launch_step(a) would run
+int step_resident(const StepArgs& a, bool fp32_tendencies);
 // one launch of the step kernel over n <= kMaxStepGroups grids, each as
 // launch_step(a[g], fp32_tendencies) would step it
 cudaError_t launch_step_groups(const StepArgs* a, int n, bool fp32_tendencies, cudaStream_t s);

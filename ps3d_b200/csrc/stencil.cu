@@ -618,6 +618,32 @@ cudaError_t step_setup() {
     return e != cudaSuccess ? e : step_setup_tt<float>();
 }
 
+// resident blocks per SM of the fused step kernel that launch_step(a) runs
+template <typename TT>
+static int step_resident_tt(const StepArgs& a) {
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+#define R(H, W, G)                                                                                            \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<TT, 8, H, W, G>, kTX * 8,                   \
+                                                      sizeof(StepSmem<TT, 8, G ? 6 : 4>));
+    switch (step_flavour(a)) {
+        case 0: R(false, false, false) break;
+        case 1: R(true, false, false) break;
+        case 2: R(false, true, false) break;
+        case 3: R(true, true, false) break;
+        case 4: R(false, false, true) break;
+        case 5: R(true, false, true) break;
+        case 6: R(false, true, true) break;
+        default: R(true, true, true) break;
+    }
+#undef R
+    if (e != cudaSuccess) { cudaGetLastError(); return 1; }
+    return n > 0 ? n : 1;
+}
+int step_resident(const StepArgs& a, bool fp32_tendencies) {
+    return fp32_tendencies ? step_resident_tt<float>(a) : step_resident_tt<double>(a);
+}
+
 cudaError_t launch_step(const StepArgs& a, bool fp32_tendencies, cudaStream_t s) {
     return fp32_tendencies ? launch_step_tt<float>(a, s) : launch_step_tt<double>(a, s);
 }
