@@ -235,6 +235,24 @@ def test_normal_mode_projection_tall_rigid(nz, form, monkeypatch):
     assert max(err.values()) < TOL_KERNEL, err
 
 
+def test_opt_balance_tall_rigid():
+    """Optimal balance on a rigid-lid grid of 96 levels, whose vertical-mode
+    transforms run by FFT of length 2 nz (the engine's form above nz = 64),
+    against the oracle's dense products."""
+    p = small_params(32, 16, 96, rigid=True, dt=600.0, Lz=6000.0)
+    f = smooth_state(p, seed=21)
+    o, m = _pair(p, f)
+    opt = abi.OptBal(period=5.5 * p.dt, average=3.5 * p.dt, max_itts=2, average_times=2, tol=0.0,
+                     enable_time_ave=0, adopt=0)
+    n_o, it_o = o.opt_balance(opt)
+    n_m, it_m = m.diag_opt_balance(opt)
+    assert it_o == it_m == 2
+    assert abs(n_m - n_o) <= 1e-9 * abs(n_o) + 1e-300
+    got = m.get_fields(abi.PS3D_FIELDS_BALANCED)
+    err = {n: rel(got[n], o.field(n + "_bal")) for n in FIELDS if np.abs(o.field(n + "_bal")).max() > 0}
+    assert max(err.values()) < TOL64, err
+
+
 @pytest.mark.parametrize("time_ave", [False, True])
 def test_opt_balance(time_ave):
     p = small_params(32, 32, 8, rigid=True, dt=600.0)
