@@ -1743,9 +1743,9 @@ int ps3d_describe(ps3d_ctx* ctx, char* buf, int len) {
     const Ctx& C = ctx->impl;
     const ps3d::PlaneArgs& pa = C.mixed ? C.pa32 : C.pa64;
     std::snprintf(buf, len, "grid=%dx%dx%d precision=%s batch=%d plane_impl=%s plane_cluster=%d row_chunk=%d tj=%d ly=%d "
-                  "fft_x=%d stages fft_y=%d stages kchunk=%d tuned=%s", C.nx, C.ny, C.nz, C.refine_full ? "mixed_refined" : C.mixed ? "mixed" : "fp64",
+                  "fft_x=%d stages fft_y=%d stages kchunk=%d vmode=%s tuned=%s", C.nx, C.ny, C.nz, C.refine_full ? "mixed_refined" : C.mixed ? "mixed" : "fp64",
                   C.batch, pa.impl == 2 ? "pipe+lines" : pa.ysplit ? "rows+colsolve" : pa.impl ? "rows+lines" : "cluster", pa.C, pa.row_chunk, pa.tj, pa.ly, pa.px.nst, pa.py.nst,
-                  C.kchunk, C.tuned.empty() ? "default" : C.tuned.c_str());
+                  C.kchunk, !C.rigid ? "z-fft" : C.vmode_fft ? "fft" : "dense", C.tuned.empty() ? "default" : C.tuned.c_str());
     return PS3D_OK;
 }
 

@@ -229,6 +229,7 @@ def test_normal_mode_projection_tall_rigid(nz, form, monkeypatch):
     monkeypatch.setenv("PS3D_VMODE_FORM", ("1" if nz % 2 == 0 else "0") if form == "dense" else "2")
     p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
     o, m = _pair(p, smooth_state(p, seed=15))
+    assert ("vmode=fft" in m.describe()) == (form == "fft" and nz != 33), m.describe()
     o.project(abi.PS3D_PROJ_NORMAL_MODE)
     m.project(abi.PS3D_PROJ_NORMAL_MODE)
     err = compare_state(m, o, names=FIELDS)
