@@ -361,6 +361,14 @@ PS3D_API int ps3d_slab_bind(ps3d_slab* s, void* xbuf, void* colbuf, void* hsend,
 PS3D_API int ps3d_slab_upload(ps3d_slab* s, const double* u, const double* v, const double* w, const double* b);
 /* applies the pending pressure correction first; waits for the stream      */
 PS3D_API int ps3d_slab_download(ps3d_slab* s, double* u, double* v, double* w, double* b, double* p);
+/* diagnose (diagnose.F90:2-61) over the rank's levels, for a global
+ * reduction (global_sum / global_max, parallel_mpi.f90:37-67): the sums of
+ * the kinetic and potential energy density over the rank's points (divide
+ * the ranks' total by nx ny nz), |u_h| max, |w| max, and 1 where a value is
+ * not finite.  Applies the pending pressure correction first; the values
+ * are filled whatever the state, so every rank takes part in the reduction. */
+PS3D_API int ps3d_slab_diagnose(ps3d_slab* s, double* ke_sum, double* pe_sum, double* umax, double* wmax,
+                                int* nonfinite);
 /* set_forcing (lee_wave1.f90:232-332; config.f90:224-237) for the rank's
  * levels: kind PS3D_FORCE_WAVEMAKER and/or PS3D_FORCE_BACKGROUND (NONE
  * clears).  Every field pointer of f (NULL = zero field) holds the rank's

@@ -251,7 +251,8 @@ cudaError_t launch_to_halo(const void* src, double* h_dev, int nx, int ny, int n
 struct DiagOut { double ke, pe, umax, wmax; unsigned flags; };
 cudaError_t launch_diagnose(const double* u, const double* v, const double* w, const double* b, const double* p,
                             int nx, int ny, int nz, double dsqr, double N0, double dz,
-                            double* partials, int nblk, DiagOut* out_dev, cudaStream_t s);
+                            double* partials, int nblk, DiagOut* out_dev, cudaStream_t s,
+                            int kofs = 0);
 cudaError_t launch_norm(const double* const* x, const double* const* y, long n, double dsqr, double N0sq,
                         double* partials, int nblk, double* out_dev, cudaStream_t s);
 cudaError_t launch_axpby(double* y, const double* x, long n, double a, double b, cudaStream_t s);

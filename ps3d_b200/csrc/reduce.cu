@@ -35,7 +35,8 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], const bool (&is_ma
 __global__ void __launch_bounds__(kRedThreads) k_diag_partial(const double* __restrict__ u, const double* __restrict__ v,
                                                               const double* __restrict__ w, const double* __restrict__ b,
                                                               const double* __restrict__ p, int nx, int ny, int nz,
-                                                              double dsqr, double N0, double dz, double* partials) {
+                                                              double dsqr, double N0, double dz, int kofs,
+                                                              double* partials) {
     __shared__ double sh[32 * 5];
     const long N = (long)nx * ny * nz, plane = (long)nx * ny;
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};   // ke, pe, umax, wmax, nonfinite
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(kRedThreads) k_diag_partial(const double* __re
         acc[3] = fmax(acc[3], fabs(ww));
         acc[0] = acc[0] + 0.5 * (uu * uu + vv * vv + dsqr * (ww * ww));
         if (N0 > 0.0) acc[1] = acc[1] + 0.5 * (bb * bb) * rN2;
-        else acc[1] = acc[1] + bb * ((double)(g / plane) + 0.5) * dz;
+        else acc[1] = acc[1] + bb * ((double)(g / plane + kofs) + 0.5) * dz;   // level k + kofs of the grid
     }
     block_reduce<5>(acc, mx, sh);
     if (threadIdx.x == 0)
@@ -76,8 +77,8 @@ __global__ void __launch_bounds__(kRedThreads) k_diag_final(const double* partia
 
 cudaError_t launch_diagnose(const double* u, const double* v, const double* w, const double* b, const double* p,
                             int nx, int ny, int nz, double dsqr, double N0, double dz,
-                            double* partials, int nblk, DiagOut* out_dev, cudaStream_t s) {
-    k_diag_partial<<<nblk, kRedThreads, 0, s>>>(u, v, w, b, p, nx, ny, nz, dsqr, N0, dz, partials);
+                            double* partials, int nblk, DiagOut* out_dev, cudaStream_t s, int kofs) {
+    k_diag_partial<<<nblk, kRedThreads, 0, s>>>(u, v, w, b, p, nx, ny, nz, dsqr, N0, dz, kofs, partials);
     k_diag_final<<<1, kRedThreads, 0, s>>>(partials, nblk, (long)nx * ny * nz, out_dev);
     return cudaGetLastError();
 }

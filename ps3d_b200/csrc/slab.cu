@@ -457,18 +457,54 @@ PS3D_API int ps3d_slab_upload(ps3d_slab* s, const double* u, const double* v, co
     SGUARD_END
 }
 
+// the pending correction of the interior and of both state halo planes (p is
+// valid one level below and two above), so the halos stay consistent
+static int apply_pending(ps3d_slab* s) {
+    Ctx& c = *s->ctx;
+    if (c.pending) {
+        CK(ps3d::launch_correct(c.field(0), c.field(1), c.field(2), c.pcor, c.nx, c.ny, c.nz, 1, c.dtp,
+                                c.dtp / c.P.dsqr, 1.0 / c.P.dx, 1.0 / c.P.dy, 1.0 / c.P.dz, c.stream, 1, 0, s->nzl + 2,
+                                s->k0 - 1, s->nzg));
+        c.pending = false;
+    }
+    return PS3D_OK;
+}
+
+PS3D_API int ps3d_slab_diagnose(ps3d_slab* s, double* ke_sum, double* pe_sum, double* umax, double* wmax,
+                                int* nonfinite) {
+    SGUARD_BEGIN
+    if (!s) return PS3D_ERR_BADPARAM;
+    Ctx& c = *s->ctx;
+    cudaSetDevice(c.device);
+    int rc = apply_pending(s);
+    if (rc) return rc;
+    // the interior levels 1 .. nzl; the potential energy of the N0 = 0 form
+    // weighs b by the global level k0 + k
+    ps3d::DiagOut* d = (ps3d::DiagOut*)c.red_out.p;
+    CK(ps3d::launch_diagnose(s->lvl(c.field(0), 1), s->lvl(c.field(1), 1), s->lvl(c.field(2), 1),
+                             s->lvl(c.field(3), 1), s->lvl((double*)c.p.p, 1), c.nx, c.ny, s->nzl, c.P.dsqr, c.P.N0,
+                             c.P.dz, (double*)c.red_partials.p, c.nred, d, c.stream, s->k0));
+    ps3d::DiagOut h{};
+    CK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    if ((rc = c.sync())) return rc;
+    const double n = (double)s->nzl * (double)s->plane;   // the kernel returned means over these points
+    if (ke_sum) *ke_sum = h.ke * n;
+    if (pe_sum) *pe_sum = h.pe * n;
+    if (umax) *umax = h.umax;
+    if (wmax) *wmax = h.wmax;
+    if (nonfinite) *nonfinite = h.flags ? 1 : 0;
+    return PS3D_OK;
+    SGUARD_END
+}
+
 PS3D_API int ps3d_slab_download(ps3d_slab* s, double* u, double* v, double* w, double* b, double* p) {
     SGUARD_BEGIN
     if (!s) return PS3D_ERR_BADPARAM;
     Ctx& c = *s->ctx;
     cudaSetDevice(c.device);
-    if (c.pending) {
-        // the pending correction of the interior and of both state halo planes
-        // (p is valid one level below and two above), so the halos stay consistent
-        CK(ps3d::launch_correct(c.field(0), c.field(1), c.field(2), c.pcor, c.nx, c.ny, c.nz, 1, c.dtp,
-                                c.dtp / c.P.dsqr, 1.0 / c.P.dx, 1.0 / c.P.dy, 1.0 / c.P.dz, c.stream, 1, 0, s->nzl + 2,
-                                s->k0 - 1, s->nzg));
-        c.pending = false;
+    {
+        int rc0 = apply_pending(s);
+        if (rc0) return rc0;
     }
     int rc = c.sync();
     if (rc) return rc;

@@ -20,7 +20,7 @@ import ctypes as C
 
 import numpy as np
 
-from .abi import PS3D_FORCE_NONE, PS3D_FP64, Forcing, Params
+from .abi import PS3D_ERR_NONFINITE, PS3D_FORCE_NONE, PS3D_FP64, Forcing, Params
 from .model import _check, load
 
 FORCING_FIELDS = ("u_r", "v_r", "w_r", "b_r", "u_i", "v_i", "w_i", "b_i", "u_back", "b_back")
@@ -51,12 +51,23 @@ def _lib():
     L.ps3d_slab_sync.argtypes = [vp]
     L.ps3d_slab_group_step.argtypes = [C.POINTER(vp), C.c_int, C.c_int]
     L.ps3d_slab_set_forcing.argtypes = [vp, C.POINTER(Forcing)]
+    L.ps3d_slab_diagnose.argtypes = [vp, dp, dp, dp, dp, C.POINTER(C.c_int)]
     L._slab_argtypes = True
     return L
 
 
 def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def combine_diagnostics(parts, npoints):
+    """diagnose over the whole grid from the ranks' (ke_sum, pe_sum, umax,
+    wmax, nonfinite): global sums divided by the grid's points, global maxima
+    (global_sum / global_max, parallel_mpi.f90:37-67).  Returns (ke, pe,
+    umax, wmax, nonfinite)."""
+    ke = sum(q[0] for q in parts) / npoints
+    pe = sum(q[1] for q in parts) / npoints
+    return ke, pe, max(q[2] for q in parts), max(q[3] for q in parts), max(int(q[4]) for q in parts)
 
 
 class Slab:
@@ -131,6 +142,13 @@ class Slab:
             setattr(f, name, _dp(loc))
         _check(self.L.ps3d_slab_set_forcing(self.h, C.byref(f)), "ps3d_slab_set_forcing")
 
+    def diagnose_partial(self):
+        """This rank's (ke_sum, pe_sum, umax, wmax, nonfinite) over its levels."""
+        ke, pe, um, wm, nf = C.c_double(), C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        _check(self.L.ps3d_slab_diagnose(self.h, C.byref(ke), C.byref(pe), C.byref(um), C.byref(wm), C.byref(nf)),
+               "ps3d_slab_diagnose")
+        return ke.value, pe.value, um.value, wm.value, nf.value
+
     def phase(self, name):
         _check(self.L.ps3d_slab_phase(self.h, PHASE[name]), "ps3d_slab_phase " + name)
 
@@ -172,6 +190,15 @@ class SlabGroup:
     def step(self, nsteps=1):
         arr = (C.c_void_p * len(self.ranks))(*[s.h.value for s in self.ranks])
         _check(self.L.ps3d_slab_group_step(arr, len(self.ranks), nsteps), "ps3d_slab_group_step")
+
+    def diagnose(self):
+        """(ke, pe, umax, wmax) of the whole grid; raises PS3DError
+        (PS3D_ERR_NONFINITE) where a value is not finite, as Model.diagnose."""
+        p = self.params
+        ke, pe, um, wm, nf = combine_diagnostics([s.diagnose_partial() for s in self.ranks], p.nx * p.ny * p.nz)
+        if nf:
+            _check(PS3D_ERR_NONFINITE, "ps3d_slab_diagnose")
+        return ke, pe, um, wm
 
     def download(self):
         parts = [s.download() for s in self.ranks]
@@ -282,6 +309,27 @@ class DistSlab:
                 s.phase("inverse")
                 self._halo(1)
             s.phase("end_step")
+
+    def diagnose(self):
+        """(ke, pe, umax, wmax) of the whole grid: every rank's partial sums
+        and maxima reduced over the process group (sums, then maxima)."""
+        import torch.distributed as dist
+        torch = self.torch
+        p = self.slab.params
+        ke, pe, um, wm, nf = self.slab.diagnose_partial()
+        dev = self.xbuf.device
+        sums = torch.tensor([ke, pe], dtype=torch.float64, device=dev)
+        maxs = torch.tensor([um, wm, float(nf)], dtype=torch.float64, device=dev)
+        with torch.cuda.stream(self.stream):
+            dist.all_reduce(sums, op=dist.ReduceOp.SUM, group=self.group)
+            dist.all_reduce(maxs, op=dist.ReduceOp.MAX, group=self.group)
+        self.stream.synchronize()
+        n = p.nx * p.ny * p.nz
+        ke, pe, um, wm, nf = combine_diagnostics([(sums[0].item(), sums[1].item(), maxs[0].item(), maxs[1].item(),
+                                                   int(maxs[2].item()))], n)
+        if nf:
+            _check(PS3D_ERR_NONFINITE, "ps3d_slab_diagnose")
+        return ke, pe, um, wm
 
     def download(self):
         return self.slab.download()

@@ -225,9 +225,38 @@ def test_dist_slab_nccl_single_rank(precision, monkeypatch):
         d = DistSlab(p, 0)
         d.upload(*[_interior(f[n]) for n in "uvwb"])
         d.step(4)
+        diag = d.diagnose()
         got = d.download()
         d.close()
     finally:
         dist.destroy_process_group()
     err = {n: rel(got[n], ref[n]) for n in NAMES}
     assert max(err.values()) < (TOL if precision == abi.PS3D_FP64 else 1e-10), err
+    m = Model(p)
+    m.upload(**{n: f[n] for n in "uvwb"})
+    m.run(4)
+    want = m.diagnose()
+    m.close()
+    assert np.allclose(diag, want, rtol=1e-10, atol=0.0), (diag, want)
+
+
+@pytest.mark.parametrize("n0", [1e-3, 0.0])
+@pytest.mark.parametrize("nranks", [1, 2, 4])
+def test_slab_diagnose_matches_single_grid(nranks, n0, monkeypatch):
+    """diagnose of a grid in slabs: the ranks' partial sums and maxima over
+    their levels, combined, against diagnose of the grid on one context
+    (with N0 = 0 the potential energy weighs b by the global level)."""
+    monkeypatch.setenv("PS3D_PLANE_IMPL", "1")
+    p = small_params(64, 32, 32, rigid=True, N0=n0)
+    f = random_state(p, seed=23, amp=0.05)
+    m = Model(p)
+    m.upload(**{n: f[n] for n in "uvwb"})
+    m.run(5)
+    want = m.diagnose()
+    m.close()
+    g = SlabGroup(p, nranks)
+    g.upload(*[_interior(f[n]) for n in "uvwb"])
+    g.step(5)
+    got = g.diagnose()
+    g.close()
+    assert np.allclose(got, want, rtol=1e-11, atol=0.0), (got, want)

@@ -71,3 +71,26 @@ def test_slab_transports_gloo(world):
     for p in procs:
         p.join(timeout=60)
     assert res == {r: "ok" for r in range(world)}, res
+
+
+def test_combine_diagnostics_matches_whole_grid():
+    """The ranks' partial sums and maxima combine to the whole grid's
+    diagnose values (global_sum / global_max, parallel_mpi.f90:37-67)."""
+    import numpy as np
+    from ps3d_b200.slab import combine_diagnostics
+    rng = np.random.default_rng(4)
+    nz, ny, nx, nr = 8, 4, 6, 4
+    u, v, w, b = (rng.standard_normal((nz, ny, nx)) for _ in range(4))
+    dsqr, n0 = 0.5, 2e-3
+
+    def part(sl):
+        ke = 0.5 * (u[sl] ** 2 + v[sl] ** 2 + dsqr * w[sl] ** 2).sum()
+        pe = 0.5 * (b[sl] ** 2).sum() / n0 ** 2
+        return ke, pe, np.sqrt(u[sl] ** 2 + v[sl] ** 2).max(), np.abs(w[sl]).max(), 0
+    parts = [part(slice(r * nz // nr, (r + 1) * nz // nr)) for r in range(nr)]
+    whole = part(slice(0, nz))
+    ke, pe, um, wm, nf = combine_diagnostics(parts, nx * ny * nz)
+    assert np.isclose(ke, whole[0] / (nx * ny * nz), rtol=1e-14)
+    assert np.isclose(pe, whole[1] / (nx * ny * nz), rtol=1e-14)
+    assert um == whole[2] and wm == whole[3] and nf == 0
+    assert combine_diagnostics(parts[:1] + [(0.0, 0.0, 0.0, 0.0, 1)], 1)[4] == 1
