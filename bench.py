@@ -548,6 +548,8 @@ def main():
     ap.add_argument("--ensemble", type=int, default=1, help="also run the batched-ensemble workload")
     ap.add_argument("--serve", type=int, default=1, help="also run the serving workload")
     ap.add_argument("--projection", type=int, default=1, help="also time the normal-mode projection")
+    ap.add_argument("--projection-grid", default="256x256x64",
+                    help="grid of the projection timing, NXxNYxNZ (rigid-lid eddy)")
     ap.add_argument("--slab", action="store_true",
                     help="one grid over the N ranks in z-slabs (strong scaling) instead of N replicas")
     args = ap.parse_args()
@@ -675,7 +677,8 @@ def main():
     if args.ensemble:
         line["ensemble"] = ensemble_run(dev, pg, world)
     if args.projection:
-        line["projection"] = projection_run(dev)
+        pg_nx, pg_ny, pg_nz = (int(x) for x in args.projection_grid.split("x"))
+        line["projection"] = projection_run(dev, pg_nx, pg_ny, pg_nz)
     if args.serve:
         line["serving"] = serve_run(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
