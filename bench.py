@@ -438,10 +438,10 @@ def projection_run(dev, nx=256, ny=256, nz=64):
     eddy of the largest serving size: forward transform (4 plane FFTs + 4
     vertical-mode transforms), eigen projection, backward transform.  Median
     of 5 timed calls in each form of the vertical-mode transform: the dense
-    FP64 product (the engine's choice up to nz = 64; 4 nz^2 flop per complex
-    column, against the FP64 GEMM throughput measured here by cuBLAS DGEMM)
-    and the FFT of length 2 nz (above nz = 64; an HBM-bound pass: the column
-    data read and written once, against the measured copy bandwidth)."""
+    FP64 product (4 nz^2 flop per complex column, against the FP64 GEMM
+    throughput measured here by cuBLAS DGEMM) and the FFTs (the engine's
+    choice; an HBM-bound pass: the column data read and written once,
+    against the measured copy bandwidth)."""
     import torch
     from ps3d_b200 import configs as cf
     from ps3d_b200.model import Model
@@ -495,7 +495,7 @@ def projection_run(dev, nx=256, ny=256, nz=64):
            "bytes_per_launch": nbytes, "achieved_gbs": nbytes / (per_f * 1e-3) / 1e9 if n_f else None,
            "peak_gbs": hbm, "peak_kind": hbm_kind,
            "frac": (nbytes / (per_f * 1e-3) / 1e9) / hbm if n_f else None}
-    default = "fft" if nz > 64 else "dense"
+    default = "fft"
     chosen = fft if default == "fft" else dense
     return {"grid": [nx, ny, nz], "ms_median": chosen["ms_median"], "vmode_form": default,
             "vmode_dense": dense, "vmode_fft": fft,

@@ -150,6 +150,7 @@ struct Ctx {
     DevBuf t_kx, t_ky, t_kz, t_hkx, t_hky, t_hkz, t_ex, t_ey, t_ez, t_px, t_py, t_pz, t_sz, t_cz, t_hkz_ds;
     DevBuf m_phi, m_psi, m_psib;
     DevPlan pl2z;               // rigid lid: length 2 nz, the vertical-mode transforms by FFT
+    DevPlan pl1z;               // ... and length nz (phi and psib for even nz)
     DevBuf t_dtw;               // ... and e^{i pi j / 2 nz}, j = 0 .. nz-1
     bool vmode_fft = false;     // the vertical-mode transforms run by FFT (launch_vert_dtt)
     int vmode_transform(const double2* in, double2* out, int f, bool fwd);

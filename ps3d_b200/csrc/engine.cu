@@ -359,12 +359,14 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
         const std::vector<double> phi2 = with_t(phi), psi2 = with_t(psi), psib2 = with_t(psib);
         CK(up(m_phi, phi2.data(), phi2.size() * 8)); CK(up(m_psi, psi2.data(), psi2.size() * 8));
         CK(up(m_psib, psib2.data(), psib2.size() * 8));
-        // the same transforms by FFT of length 2 nz where the length factors
-        // and nz > 64: at 256x256x128 90.6 us per transform against 202 us
-        // for the dense product, at 256x256x64 52 against 49 us.
-        // PS3D_VMODE_FORM=0|1 keeps the dense products, =2 takes the FFT
+        // the same transforms by FFT where 2 nz factors: phi and psib by
+        // FFTs of length nz (even nz), psi by one of length 2 nz.  Per
+        // transform at 256x256x128 79 us (average of the three) against 202
+        // us for the dense product, at 256x256x64 40 against 48 us.
+        // PS3D_VMODE_FORM=0|1 keeps the dense products, =3 takes length 2 nz
+        // for every field
         const char* vf = std::getenv("PS3D_VMODE_FORM");
-        const bool want_fft = vf && (vf[0] == '0' || vf[0] == '1') ? false : (nz > 64 || (vf && vf[0] == '2'));
+        const bool want_fft = !(vf && (vf[0] == '0' || vf[0] == '1'));
         if (want_fft && vert_dtt_fits(nz)) {
             CK(pl2z.build(2 * nz, 2));   // radix-8 first: the transform's radix-8 build
             int mr = 1;
@@ -374,6 +376,14 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
                 for (int j = 0; j < nz; ++j) tw[j] = make_double2(std::cos(pi * j / (2.0 * nz)), std::sin(pi * j / (2.0 * nz)));
                 CK(up(t_dtw, tw.data(), nz * 16));
                 vmode_fft = true;
+                // phi and psib by FFTs of length nz (even nz; PS3D_VMODE_FORM=3
+                // keeps the length-2nz extension for every field)
+                if (nz % 2 == 0 && fft_length_ok(nz) && !(vf && vf[0] == '3')) {
+                    CK(pl1z.build(nz, 2));
+                    int mr1 = 1;
+                    for (int q = 0; q < pl1z.plan.nst; ++q) mr1 = std::max(mr1, pl1z.plan.r[q]);
+                    if (mr1 > 8) pl1z.plan.n = 0;
+                }
             }
         }
     }
@@ -988,6 +998,7 @@ int Ctx::vmode_transform(const double2* in, double2* out, int f, bool fwd) {
         d.in = in; d.out = out; d.nz = nz; d.ncol = M2;
         d.scale = fwd ? P.dz : 1.0;
         d.plan = pl2z.plan;
+        d.plan1 = pl1z.plan;
         d.tw = (const double2*)t_dtw.p;
         d.c0 = std::sqrt(1.0 / P.Lz); d.c1 = std::sqrt(2.0 / P.Lz);
         const int kind = f < 2 ? 0 : (f == 2 ? 1 : 2);

@@ -233,6 +233,7 @@ struct VertDttArgs {
     long ncol;          // columns: levels are ncol apart
     double scale;       // forward: dz; backward: 1
     FFTPlan plan;       // length 2 nz, radices <= 8 (radix-8-first plan)
+    FFTPlan plan1;      // length nz, radices <= 8 (phi and psib for even nz; n = 0: none)
     const double2* tw;  // e^{i pi j / 2 nz}, j = 0 .. nz-1
     double c0, c1;      // sqrt(1/Lz) (phi's mode 0), sqrt(2/Lz) (every other mode)
     int cols;           // columns per block (set by the launcher)

@@ -230,10 +230,10 @@ __global__ void __launch_bounds__(kVmThreads) k_vert_mode_staged(const double2* 
 // hold both to the oracle).  A block takes kDttCols columns, buf[e][column]
 // as fft_batch lays lines out (its radix-8 build: 80 registers, three
 // blocks per SM), and walks the column tiles with the grid's stride.
-// Measured per transform: 52 us against 49 us for the dense product at
-// 256x256x64, 90.6 against 202 us at 256x256x128, 162 against 1012 us at
-// 256x128x256; both are bound at nz = 64 by reading columns as 256-512 byte
-// rows one plane apart, so the engine takes the FFT form above nz = 64.
+// Measured per transform with every field at length 2 nz: 52 us against 49
+// us for the dense product at 256x256x64, 90 against 202 us at
+// 256x256x128, 162 against 1012 us at 256x128x256; k_vert_dttn below
+// halves the length for phi and psib.
 constexpr int kDttCols = 16;
 constexpr int kDttThreads = 256;
 
@@ -304,6 +304,87 @@ __global__ void __launch_bounds__(kDttThreads, 3) k_vert_dtt(const VertDttArgs a
     }
 }
 
+// phi and psib (kinds 0 and 2) for even nz by FFTs of length nz (Makhoul
+// 1980, "A fast cosine transform in one and multiple dimensions", its
+// even/odd reordering, carried over to complex data): half the transform
+// length of the extension form.
+//   DCT-II   v = [x_0, x_2, .., x_{N-2}, x_{N-1}, .., x_3, x_1], V = FFT_N(v),
+//            X_j = ((P.x + Q.x) + i (P.y - Q.y)) / 2 with P = e^{-i pi j/2N} V_j,
+//            Q = e^{-i pi j/2N} conj(V_{N-j}) (the real and imaginary parts
+//            of the data separated through V_j and V_{N-j})
+//   DST-II   X_j = DCT-II((-1)^k x_k)_{N-j}
+//   DCT-III  V_0 = 2 Z_0, V_j = e^{i pi j/2N} (Z_j - i Z_{N-j}), v = IFFT_N(V)/2,
+//            x_{2n} = v_n, x_{2n+1} = v_{N-1-n}
+//   DST-III  x_k = (-1)^k DCT-III(Z')_k with Z'_j = Z_{N-j}, Z'_0 = 0
+size_t vert_dttn_smem(int nz, int cols) {
+    return align16((size_t)nz * (cols | 1) * sizeof(double2)) + plan_tables_bytes(nz, sizeof(double2));
+}
+
+template <int KIND, bool FWD>
+__global__ void __launch_bounds__(kDttThreads, 3) k_vert_dttn(const VertDttArgs a) {
+    static_assert(KIND == 0 || KIND == 2, "phi and psib");
+    using T = double2;
+    extern __shared__ __align__(16) unsigned char dttn_raw[];
+    const int N = a.nz, H = a.nz / 2, C = a.cols, ld = a.cols | 1;
+    T* buf = reinterpret_cast<T*>(dttn_raw);
+    const PlanTables<double> tp = stage_plan<double>(a.plan1, dttn_raw + align16((size_t)N * ld * sizeof(T)));
+    const long ncol = a.ncol;
+    const long ntiles = (ncol + C - 1) / C;
+    for (long ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const long c0 = ti * C;
+        const int nl = (int)min((long)C, ncol - c0);
+        __syncthreads();   // the previous tile is stored (and the tables staged)
+        for (int t = threadIdx.x; t < N * C; t += blockDim.x) {
+            const int e = t / C, l = t - e * C;
+            T v = make_double2(0.0, 0.0);
+            if (l < nl) {
+                const T* col = a.in + c0 + l;
+                if (FWD) {
+                    // v_e = x_{2e} (e < N/2), x_{2(N-1-e)+1} (e >= N/2); DST-II's (-1)^k on the odd ones
+                    if (e < H) v = col[(long)(2 * e) * ncol];
+                    else v = cscale(col[(long)(2 * (N - 1 - e) + 1) * ncol], KIND == 0 ? 1.0 : -1.0);
+                } else {
+                    // Z_j (phi: the weighted input; psib: Z'_j = c1 in_{N-j}, Z'_0 = 0) and Z_{N-j}
+                    auto z = [&](int j) -> T {
+                        if (j <= 0 || j >= N) return (KIND == 0 && j == 0) ? cscale(col[0], a.c0) : make_double2(0.0, 0.0);
+                        return cscale(col[(long)(KIND == 0 ? j : N - j) * ncol], a.c1);
+                    };
+                    if (e == 0) v = cscale(z(0), 2.0);
+                    else {
+                        const T d = csub(z(e), cmul_si(z(N - e), 1));   // Z_j - i Z_{N-j}
+                        v = cmul(d, a.tw[e]);
+                    }
+                }
+            }
+            buf[e * ld + l] = v;
+        }
+        fft_batch<false, double, 8>(buf, ld, C, a.plan1, FWD ? -1 : +1, tp.tw);   // synchronises
+        for (int t = threadIdx.x; t < N * C; t += blockDim.x) {
+            const int j = t / C, l = t - j * C;
+            if (l >= nl) continue;
+            T o;
+            if (FWD) {
+                // element jp of the DCT-II (phi: jp = j; psib: jp = N - j, and mode 0 is zero)
+                const int jp = KIND == 0 ? j : N - j;
+                if (KIND == 2 && j == 0) {
+                    o = make_double2(0.0, 0.0);
+                } else {
+                    const T w = cconj(a.tw[jp]);
+                    const T P = cmul(buf[tp.pos[jp] * ld + l], w);
+                    const T Q = cmul(cconj(buf[tp.pos[(N - jp) % N] * ld + l]), w);
+                    const double wt = (KIND == 0 && j == 0) ? a.c0 : a.c1;
+                    o = cscale(make_double2(P.x + Q.x, P.y - Q.y), 0.5 * a.scale * wt);
+                }
+            } else {
+                // x_{2n} = v_n, x_{2n+1} = v_{N-1-n}; DST-III's (-1)^k
+                const int n = (j & 1) ? N - 1 - (j >> 1) : (j >> 1);
+                o = cscale(buf[tp.pos[n] * ld + l], (KIND == 2 && (j & 1) ? -0.5 : 0.5) * a.scale);
+            }
+            a.out[(long)j * ncol + c0 + l] = o;
+        }
+    }
+}
+
 // opts the transform in to its dynamic shared memory on the current device
 cudaError_t modes_setup() {
     cudaError_t e = cudaFuncSetAttribute(k_vert_mode<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -315,6 +396,11 @@ cudaError_t modes_setup() {
         return e;
     DTT_ATTR(0, true) DTT_ATTR(1, true) DTT_ATTR(2, true) DTT_ATTR(0, false) DTT_ATTR(1, false) DTT_ATTR(2, false)
 #undef DTT_ATTR
+#define DTTN_ATTR(K, F)                                                                                        \
+    if ((e = cudaFuncSetAttribute(k_vert_dttn<K, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) \
+        return e;
+    DTTN_ATTR(0, true) DTTN_ATTR(2, true) DTTN_ATTR(0, false) DTTN_ATTR(2, false)
+#undef DTTN_ATTR
     return cudaFuncSetAttribute(k_vert_mode<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
@@ -361,12 +447,27 @@ cudaError_t launch_vert_dtt(const VertDttArgs& a0, int kind, bool fwd, cudaStrea
     if (!vert_dtt_fits(a.nz) || a.plan.n != 2 * a.nz || kind < 0 || kind > 2) return cudaErrorInvalidValue;
     for (int q = 0; q < a.plan.nst; ++q)
         if (a.plan.r[q] > 8) return cudaErrorInvalidValue;   // the radix-8 build
-    const size_t sm = vert_dtt_smem(a.nz, a.cols);
+    // phi and psib by FFTs of length nz where nz is even and that plan is set
+    const bool half = kind != 1 && a.nz % 2 == 0 && a.plan1.n == a.nz && vert_dttn_smem(a.nz, a.cols) <= 227 * 1024;
+    if (half)
+        for (int q = 0; q < a.plan1.nst; ++q)
+            if (a.plan1.r[q] > 8) return cudaErrorInvalidValue;
+    const size_t sm = half ? vert_dttn_smem(a.nz, a.cols) : vert_dtt_smem(a.nz, a.cols);
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const long ntiles = (a.ncol + a.cols - 1) / a.cols;
     const int per = std::max(1, (int)((227 * 1024) / (sm + 1024)));
     const int blocks = (int)std::min<long>(ntiles, (long)nsm * std::min(per, 8));
+    if (half) {
+        if (kind == 0) {
+            if (fwd) k_vert_dttn<0, true><<<blocks, kDttThreads, sm, s>>>(a);
+            else k_vert_dttn<0, false><<<blocks, kDttThreads, sm, s>>>(a);
+        } else {
+            if (fwd) k_vert_dttn<2, true><<<blocks, kDttThreads, sm, s>>>(a);
+            else k_vert_dttn<2, false><<<blocks, kDttThreads, sm, s>>>(a);
+        }
+        return cudaGetLastError();
+    }
 #define DTT_L(K)                                                                                   \
     if (kind == K) {                                                                               \
         if (fwd) k_vert_dtt<K, true><<<blocks, kDttThreads, sm, s>>>(a);                          \

@@ -218,18 +218,20 @@ def test_projection(rigid, mode):
     assert max(err.values()) < TOL_KERNEL, err
 
 
-@pytest.mark.parametrize("form", ["fft", "dense"])
+@pytest.mark.parametrize("form", ["fft", "fft2n", "dense"])
 @pytest.mark.parametrize("nz", [33, 60, 64, 128])
 def test_normal_mode_projection_tall_rigid(nz, form, monkeypatch):
     """Rigid-lid projection through the vertical-mode transforms at nz = 128,
-    64 and 60 (by FFT of length 2 nz, PS3D_VMODE_FORM=2, the default above
-    nz = 64: the mode matrices are sampled sines and cosines; or the dense
-    FP64 product, PS3D_VMODE_FORM=1) and an odd 33 (2 nz = 66 has a factor
-    11: the dense product, its unpaired-load path, in both cases)."""
-    monkeypatch.setenv("PS3D_VMODE_FORM", ("1" if nz % 2 == 0 else "0") if form == "dense" else "2")
+    64 and 60, by FFT (PS3D_VMODE_FORM=2, the default where 2 nz factors:
+    the mode matrices are sampled sines and cosines; phi and psib by FFTs of
+    length nz, psi by one of length 2 nz; =3 every field by length 2 nz) or
+    as the dense FP64 product (PS3D_VMODE_FORM=1), and an odd 33 (2 nz = 66
+    has a factor 11: the dense product, its unpaired-load path, in every
+    case)."""
+    monkeypatch.setenv("PS3D_VMODE_FORM", {"dense": "1" if nz % 2 == 0 else "0", "fft": "2", "fft2n": "3"}[form])
     p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
     o, m = _pair(p, smooth_state(p, seed=15))
-    assert ("vmode=fft" in m.describe()) == (form == "fft" and nz != 33), m.describe()
+    assert ("vmode=fft" in m.describe()) == (form != "dense" and nz != 33), m.describe()
     o.project(abi.PS3D_PROJ_NORMAL_MODE)
     m.project(abi.PS3D_PROJ_NORMAL_MODE)
     err = compare_state(m, o, names=FIELDS)
@@ -238,8 +240,7 @@ def test_normal_mode_projection_tall_rigid(nz, form, monkeypatch):
 
 def test_opt_balance_tall_rigid():
     """Optimal balance on a rigid-lid grid of 96 levels, whose vertical-mode
-    transforms run by FFT of length 2 nz (the engine's form above nz = 64),
-    against the oracle's dense products."""
+    transforms run by FFT, against the oracle's dense products."""
     p = small_params(32, 16, 96, rigid=True, dt=600.0, Lz=6000.0)
     f = smooth_state(p, seed=21)
     o, m = _pair(p, f)
