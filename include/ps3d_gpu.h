@@ -428,6 +428,9 @@ PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch, long long m
 /* stats[6] = {active, queued, bytes in use, peak bytes, peak active, budget} */
 PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats);
 PS3D_API long long ps3d_server_footprint(const ps3d_params* prm);
+/* request contexts created, and taken from the idle pool (a pooled context
+ * of k instances serves a group of up to k same-parameter requests)        */
+PS3D_API int ps3d_server_context_stats(ps3d_server* s, long long* created, long long* reused);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,7 @@ struct Ctx {
     // from the FP32 transforms' in the mixed path's error budget
     bool hist32 = false;
     int batch = 1;            // instances of this grid stepped together (ensembles)
+    int cap = 1;              // instances the buffers hold (batch <= cap; set_active_batch)
     // CUDA graphs of three consecutive steps (tau and the state buffers both
     // cycle with period 3), replayed by advance() for constant parameters: one
     // per phase of the cycle (slot tau - 1), so that calls of any length keep
@@ -235,6 +236,9 @@ struct Ctx {
     // no longer holds the previous step's pressure of this trajectory
     void state_replaced() { ++version; p_warm = false; }
     int step(int itt, int tau, int taum1, int taum2);
+    // run the first b <= cap instances (a pooled serving context of cap
+    // instances taking a smaller group); captured graphs are kept per batch
+    int set_active_batch(int b);
     // Grouped step launches (an ensemble's groups in one step-kernel launch):
     // with defer_step set, step() of a fused step does the step kernel's
     // bookkeeping and writes its arguments to *defer_step instead of

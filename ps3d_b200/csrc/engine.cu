@@ -243,6 +243,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
     P = prm;
     device = dev;
     batch = nbatch < 1 ? 1 : nbatch;
+    cap = batch;
     nx = P.nx; ny = P.ny; nz = P.nz; nxh = nx / 2 + 1;
     N = (long)nx * ny * nz;
     M2 = (long)nxh * ny;
@@ -452,7 +453,7 @@ int Ctx::init(const ps3d_params& prm, int dev, int nbatch, cudaStream_t use_stre
 cudaError_t Ctx::ensure_spectral4() {
     if (spec4[0].p) return cudaSuccess;
     cudaError_t e;
-    const long MB = M * batch;   // projections of a batched context cover every instance
+    const long MB = M * cap;   // projections of a batched context cover every instance it holds
     for (int f = 0; f < 4; ++f) if ((e = spec4[f].alloc(MB * sizeof(double2)))) return e;
     if ((e = g0base.alloc(MB * sizeof(double2)))) return e;
     if ((e = cudaMemset(g0base.p, 0, MB * sizeof(double2)))) return e;
@@ -464,9 +465,9 @@ cudaError_t Ctx::ensure_fieldset(int which) {
     if (!s) return cudaErrorInvalidValue;
     if (s[0].p) return cudaSuccess;
     for (int f = 0; f < 4; ++f) {
-        cudaError_t e = s[f].alloc(N * batch * sizeof(double));
+        cudaError_t e = s[f].alloc(N * cap * sizeof(double));
         if (e) return e;
-        if ((e = cudaMemsetAsync(s[f].p, 0, N * batch * sizeof(double), stream))) return e;
+        if ((e = cudaMemsetAsync(s[f].p, 0, N * cap * sizeof(double), stream))) return e;
     }
     return cudaSuccess;
 }
@@ -1191,6 +1192,7 @@ int Ctx::opt_time_ave(int set, int n_end_ave) {
 // pool) replays them without capturing again.
 struct RampGraph {
     ps3d_params P_at{};   // the step parameters at capture (Ro excepted: ramped)
+    int batch = 1;        // instances its launches step
     long forcing_gen = 0;
     int n_end = 0;
     double Ro_loc = 0.0, dt_loc = 0.0, period = 0.0;
@@ -1227,7 +1229,7 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
     Pk.Ro = 0.0;
     RampGraph* g = nullptr;
     for (RampGraph& c : cache)
-        if (c.backward == backward && std::equal(c.cur_in, c.cur_in + 4, cur) && c.pend_in == pending &&
+        if (c.backward == backward && c.batch == batch && std::equal(c.cur_in, c.cur_in + 4, cur) && c.pend_in == pending &&
             c.pcor_in == pcor && c.dtp_in == dtp && c.warm_in == p_warm && c.n_end == n_end && c.Ro_loc == Ro_loc &&
             c.dt_loc == dt_loc && c.period == period && c.forcing_gen == forcing_gen &&
             std::memcmp(&c.P_at, &Pk, sizeof(Pk)) == 0)
@@ -1235,6 +1237,7 @@ int Ctx::ramp_run(bool backward, int n_end, double Ro_loc, double dt_loc, double
     if (!g) {
         RampGraph n;
         n.backward = backward;
+        n.batch = batch;
         n.P_at = Pk; n.n_end = n_end; n.Ro_loc = Ro_loc; n.dt_loc = dt_loc; n.period = period;
         n.forcing_gen = forcing_gen;
         std::copy(cur, cur + 4, n.cur_in);
@@ -1283,6 +1286,15 @@ void release_ramp_graphs(std::vector<RampGraph>* g) {
     for (RampGraph& r : *g)
         if (r.exec) cudaGraphExecDestroy(r.exec);
     delete g;
+}
+
+int Ctx::set_active_batch(int b) {
+    if (b < 1 || b > cap) return PS3D_ERR_BADPARAM;
+    if (b != batch) {
+        batch = b;
+        invalidate_graph();   // the main-loop graphs step the old batch
+    }
+    return PS3D_OK;
 }
 
 int Ctx::reset_request() {
@@ -1430,8 +1442,8 @@ int Ctx::opt_balance(const ps3d_optbal& O, double* final_norm, int* iters) {
 cudaError_t Ctx::ensure_saved_tail() {
     if (saved_p.p) return cudaSuccess;
     cudaError_t e;
-    if ((e = saved_p.alloc(N * batch * sizeof(double)))) return e;
-    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * batch * tsz(f)))) return e;
+    if ((e = saved_p.alloc(N * cap * sizeof(double)))) return e;
+    for (int f = 0; f < 4; ++f) if ((e = saved_tend[f].alloc(3 * N * cap * tsz(f)))) return e;
     return cudaSuccess;
 }
 

@@ -92,7 +92,7 @@ static size_t footprint_of(const ps3d_params& p) {
 
 struct IdleCtx {
     ps3d_params prm;
-    int batch;
+    int batch;                  // instances the context holds (serves groups of up to this many)
     std::unique_ptr<Ctx> ctx;
     size_t footprint;
 };
@@ -103,6 +103,7 @@ struct ps3d_server {
     size_t budget = 0, used = 0, peak_used = 0;
     int max_active = 1, active = 0, peak_active = 0;
     int max_batch = 1;          // same-parameter requests run together (ps3d_server_set_batching)
+    std::atomic<long long> created{0}, reused{0};   // request contexts created, and taken from the pool
     long batch_points = 1L << 22;   // ... while the group's grid points stay within this
     long long next_id = 1;
     bool stopping = false;
@@ -171,8 +172,11 @@ std::unique_ptr<Ctx> ps3d_server::run(std::vector<std::shared_ptr<Request>>& g, 
     std::unique_ptr<Ctx> cp = std::move(reuse);
     int rc = PS3D_OK;
     if (cp) {
+        ++reused;
         rc = cp->reset_request();
+        if (!rc) rc = cp->set_active_batch(nb);
     } else {
+        ++created;
         cp.reset(new Ctx());
         // no autotuning runs here: they would time their candidates while
         // other requests share the GPU, and one context at a time (the
@@ -242,7 +246,11 @@ void ps3d_server::worker_loop() {
                     const std::shared_ptr<Request>& q = queue.front();
                     std::vector<std::shared_ptr<Request>> cand{q};
                     const long qpts = (long)q->prm.nx * q->prm.ny * q->prm.nz;
-                    if (max_batch > 1 && batchable(*q))
+                    // group only when more requests wait than slots are free: with
+                    // free slots, lone requests run side by side on their own
+                    // streams, and a group would take that concurrency away
+                    const bool backlog = (long)queue.size() > (long)(max_active - active);
+                    if (max_batch > 1 && backlog && batchable(*q))
                         for (size_t k = 1; k < queue.size() && (int)cand.size() < max_batch &&
                                            (long)(cand.size() + 1) * qpts <= batch_points;
                              ++k)
@@ -258,9 +266,13 @@ void ps3d_server::worker_loop() {
                     while (cand.size() & (cand.size() - 1)) cand.pop_back();
                     const int nb = (int)cand.size();
                     const size_t foot = nb * q->footprint;
+                    // an idle context of the same parameters holding at least nb
+                    // instances, the smallest such (a group runs the first nb)
                     long hit = -1;
-                    for (size_t i = 0; i < idle.size() && hit < 0 && q->kind == 0; ++i)
-                        if (idle[i].batch == nb && same_params(idle[i].prm, q->prm)) hit = (long)i;
+                    for (size_t i = 0; i < idle.size() && q->kind == 0; ++i)
+                        if (idle[i].batch >= nb && same_params(idle[i].prm, q->prm) &&
+                            (hit < 0 || idle[i].batch < idle[hit].batch))
+                            hit = (long)i;
                     bool fits = hit >= 0;
                     while (!fits && !idle.empty() && used + foot > budget) {   // no hit: free idle ones
                         evicted.push_back(std::move(idle.front().ctx));
@@ -315,7 +327,10 @@ void ps3d_server::worker_loop() {
                 r->group.reset();
             }
             --active;
-            if (done && !stopping) idle.push_back({g[0]->prm, (int)g.size(), std::move(done), gfoot});
+            if (done && !stopping) {
+                const int capn = done->cap;
+                idle.push_back({g[0]->prm, capn, std::move(done), gfoot});
+            }
             else used -= gfoot;
             // keep at most 2 max_active idle contexts (with batching, groups of
             // different sizes of one grid each keep theirs)
@@ -584,6 +599,13 @@ PS3D_API int ps3d_server_stats(ps3d_server* s, double* stats) {
 }
 
 PS3D_API long long ps3d_server_footprint(const ps3d_params* prm) { return prm ? (long long)footprint_of(*prm) : -1; }
+
+PS3D_API int ps3d_server_context_stats(ps3d_server* s, long long* created, long long* reused) {
+    if (!s) return PS3D_ERR_BADPARAM;
+    if (created) *created = s->created.load();
+    if (reused) *reused = s->reused.load();
+    return PS3D_OK;
+}
 
 PS3D_API int ps3d_server_set_batching(ps3d_server* s, int max_batch, long long max_points) {
     if (!s || max_batch < 1 || max_points < 0) return PS3D_ERR_BADPARAM;

@@ -38,6 +38,7 @@ def _lib():
         L.ps3d_server_footprint.restype = C.c_longlong
         L.ps3d_server_footprint.argtypes = [C.POINTER(Params)]
         L.ps3d_server_set_batching.argtypes = [vp, C.c_int, C.c_longlong]
+        L.ps3d_server_context_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L._srv_ready = True
     return L
 
@@ -145,8 +146,10 @@ class Server:
     def stats(self):
         s = (C.c_double * 6)()
         self.L.ps3d_server_stats(self.h, s)
+        c, r = C.c_longlong(), C.c_longlong()
+        self.L.ps3d_server_context_stats(self.h, C.byref(c), C.byref(r))
         return {"active": int(s[0]), "queued": int(s[1]), "bytes": s[2], "peak_bytes": s[3],
-                "peak_active": int(s[4]), "budget": s[5]}
+                "peak_active": int(s[4]), "budget": s[5], "contexts_created": c.value, "contexts_reused": r.value}
 
 
 # --------------------------------------------------------------------------

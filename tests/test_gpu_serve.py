@@ -267,6 +267,38 @@ def test_batched_requests_match_alone(precision, monkeypatch):
     assert abs(got[-1].queue_ms - got[0].queue_ms) < 50.0
 
 
+def test_pooled_context_serves_smaller_groups(monkeypatch):
+    """A pooled context created for a group of four serves a later group of
+    two and a lone request of the same parameters (the first instances of
+    its buffers): no new context, and each result bit for bit its result
+    alone."""
+    monkeypatch.setenv("PS3D_AUTOTUNE", "0")
+    p, opt, f = _req((32, 32, 16), ramp=6, iters=2)
+    states = [{k: v * a for k, v in f.items()} for a in (1.0, 1.7, 0.6, 2.5)]
+    s = Server(max_active=1)
+    alone = [s.wait(s.submit(p, opt, st)) for st in states]
+    s.close()
+    s = Server(max_active=1, max_batch=4)
+    blocker = s.submit(*_req((64, 32, 16)))
+    four = [s.submit(p, opt, st) for st in states]
+    assert s.wait(blocker).status == 0
+    got4 = [s.wait(t) for t in four]
+    c0 = s.stats()["contexts_created"]
+    blocker = s.submit(*_req((64, 32, 16)))
+    two = [s.submit(p, opt, st) for st in states[:2]]
+    assert s.wait(blocker).status == 0
+    got2 = [s.wait(t) for t in two]
+    got1 = s.wait(s.submit(p, opt, states[3]))
+    st = s.stats()
+    s.close()
+    # the second blocker and the groups of two and one took pooled contexts
+    assert st["contexts_created"] == c0, st
+    for a, g in list(zip(alone, got4)) + list(zip(alone[:2], got2)) + [(alone[3], got1)]:
+        assert g.status == 0 and g.iters == a.iters and g.norm == a.norm
+        for n in ("u", "v", "w", "b"):
+            assert np.array_equal(g.fields[n], a.fields[n]), n
+
+
 def test_batched_group_member_cancelled_and_nonfinite(monkeypatch):
     """In a batched group a cancelled member reports PS3D_ERR_CANCELLED and
     a member whose state turns non-finite fails alone; the others finish
