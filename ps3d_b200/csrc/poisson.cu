@@ -479,18 +479,42 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas(const ColumnArgs a
 // it bounds the kernel.  Checkpoints (cp, dp, dq) before every chunk of 8
 // pivot levels in shared memory; each chunk's values recomputed on the way
 // back as in k_thomas.
+//
+// Two instantiation switches, neither of which changes an operation or its
+// order (every form gives the same bits):
+//   FULL  nz is even and nz/2 a multiple of the chunk: both halves end on a
+//         chunk boundary, so no level needs a bounds test, and the first
+//         pivot level and the meeting level sit at fixed positions of the
+//         first and the last chunk;
+//   RTAB  the forward sweep parks every level's reciprocal pivot r in shared
+//         memory ([level][complex column]: the two parts of a column form the
+//         same r), and the backward sweep takes it from there (cp = fxa r)
+//         instead of forming it again; the checkpoints then hold (dp, dq).
+//         Blocks of kThomas2RThreads threads, so that the table, H x 32
+//         doubles, leaves eight blocks an SM.
+// Level offsets are 32-bit (the launcher checks nz x level stride < 2^32).
+constexpr int kThomas2RThreads = 64;
+
 PS3D_HD size_t thomas2_smem(int nz, int threads) {
     const int h = (nz + 1) / 2;
     return (size_t)((h + kThomasChunk - 1) / kThomasChunk + 1) * threads * (sizeof(double2) + sizeof(double));
 }
+PS3D_HD size_t thomas2r_smem(int nz, int threads) {
+    const int h = (nz + 1) / 2;
+    return (size_t)((h + kThomasChunk - 1) / kThomasChunk + 1) * threads * sizeof(double2) +
+           (size_t)h * (threads / 2) * sizeof(double);
+}
 
-template <typename R>
-__global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs a) {
+template <typename R, bool FULL, bool RTAB>
+__global__ void __launch_bounds__(RTAB ? kThomas2RThreads : kThomasThreads, RTAB ? 8 : 4) k_thomas2(const ColumnArgs a) {
     pdl_trigger();
     pdl_wait();   // inputs written by the preceding kernels
     const unsigned long long pk = pol_keep(a.l2hint);   // the inverse y lines read the solution
     constexpr int KC = kThomasChunk;
-    extern __shared__ double2 ck2[];   // [chunk][thread] (cp, dp), then [chunk][thread] dq
+#define IN(cond) (FULL || (cond))
+    // checkpoints [chunk][thread]: (cp, dp) and, after them, dq (RTAB: (dp, dq));
+    // RTAB: then the reciprocal pivots [level][complex column]
+    extern __shared__ double2 ck2[];
     const int nz = a.nz;
     const int H = (nz + 1) / 2;   // pivot levels: top 0 .. H-1, bottom nz-1 .. nz-Bc
     const int Bc = nz - H;
@@ -498,6 +522,8 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
     const int nch = (H + KC - 1) / KC;
     const int T = blockDim.x, tid = threadIdx.x;
     double* ckq = reinterpret_cast<double*>(ck2 + (size_t)(nch + 1) * T);
+    double* rt = ckq + (tid >> 1);   // RTAB: level jj's r at rt[jj * (T / 2)]
+    const int rts = T >> 1;
     const long ncols = a.ncl ? a.ncl : (long)a.nxh * a.ny;   // columns held (a column slab: ncl)
     const long gid = blockIdx.x * (long)T + tid;
     if (gid >= 2 * ncols * a.batch) return;
@@ -506,7 +532,8 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
     const unsigned inst = fdiv(cb, a.fd_ncols);
     const unsigned c = cb - inst * (unsigned)ncols;
     R* col = reinterpret_cast<R*>(a.spec) + 2 * ((long)inst * a.sM + c) + part;
-    const long ls = 2 * ncols;   // level stride in R
+    const unsigned ls = (unsigned)(2 * ncols);   // level stride in R
+    R* const bot0 = col + (size_t)(nz - 1) * ls;
     const unsigned cg = c + (unsigned)a.col0;   // global column: its wavenumbers
     const unsigned q0 = fdiv(cg, a.layout ? a.fd_ny : a.fd_nxh);
     const int i = a.layout ? (int)q0 : (int)(cg - q0 * (unsigned)a.nxh);
@@ -520,14 +547,14 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
         R nxt[KC];
 #pragma unroll
         for (int q = 0; q < KC; ++q)
-            if (q < nz) nxt[q] = ld_l2(&col[(long)q * ls], pk);
+            if (q < nz) nxt[q] = ld_l2(&col[(unsigned)q * ls], pk);
         for (int kb = 0; kb < nz; kb += KC) {
             R d[KC];
 #pragma unroll
             for (int q = 0; q < KC; ++q) d[q] = nxt[q];
 #pragma unroll
             for (int q = 0; q < KC; ++q)
-                if (kb + KC + q < nz) nxt[q] = ld_l2(&col[(long)(kb + KC + q) * ls], pk);
+                if (kb + KC + q < nz) nxt[q] = ld_l2(&col[(unsigned)(kb + KC + q) * ls], pk);
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
                 const int k = kb + q;
@@ -535,26 +562,27 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
                     const double xk = k == 0 ? 0.0 : 2 * x1 - x0 + fprev * h;
                     fprev = (double)d[q];
                     x0 = x1; x1 = xk;
-                    st_l2(&col[(long)k * ls], (R)xk, pk);
+                    st_l2(&col[(unsigned)k * ls], (R)xk, pk);
                 }
             }
         }
         return;
     }
     const double bend = -ks - fxa, bmid = -ks - 2 * fxa;
-    // pivot level jj (from either end) with the top value dt and the bottom
+    // pivot level jj (first: jj == 0) with the top value dt and the bottom
     // value db: cp(1) = c/b(1), dp(1) = d(1)/b(1); r = 1/(b - cp a),
-    // cp = c r, dp = (d - dp a) r (the bottom chain the same with its own d)
-    auto elim = [&](int jj, double dt, double db, double& cp, double& dp, double& dq) {
-        if (jj == 0) {
+    // cp = c r, dp = (d - dp a) r (the bottom chain the same with its own d;
+    // both: level jj has a bottom partner)
+    auto elim = [&](bool first, bool both, double dt, double db, double& cp, double& dp, double& dq, double& r) {
+        if (first) {
             cp = fxa / bend;
             dp = dt / bend;
             dq = db / bend;
         } else {
-            const double r = rcp_newton(bmid - cp * fxa);
+            r = rcp_newton(bmid - cp * fxa);
             cp = fxa * r;
             dp = (dt - dp * fxa) * r;
-            if (jj < Bc) dq = (db - dq * fxa) * r;
+            if (both) dq = (db - dq * fxa) * r;
         }
     };
     // the chunk of pivot levels jc .. jc+KC-1: top levels jc.., bottom levels nz-1-jc..
@@ -562,8 +590,9 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
 #pragma unroll
         for (int q = 0; q < KC; ++q) {
             const int jj = jc + q;
-            if (jj < H) top[q] = ld_l2(&col[(long)jj * ls], pk);
-            if (jj < Bc) bot[q] = ld_l2(&col[(long)(nz - 1 - jj) * ls], pk);
+            const unsigned o = (unsigned)jj * ls;
+            if (IN(jj < H)) top[q] = ld_l2(col + o, pk);
+            if (IN(jj < Bc)) bot[q] = ld_l2(bot0 - o, pk);
         }
     };
     double cp = 0.0, dp = 0.0, dq = 0.0, cp_jb = 0.0, dq_jb = 0.0;
@@ -577,14 +606,21 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
 #pragma unroll
         for (int q = 0; q < KC; ++q) { dt[q] = nt[q]; db[q] = nb[q]; }
         if (ch + 1 < nch) load(jc + KC, nt, nb);
-        ck2[ch * T + tid] = make_double2(cp, dp);   // before pivot level jc
-        ckq[ch * T + tid] = dq;
+        if constexpr (RTAB) {
+            ck2[ch * T + tid] = make_double2(dp, dq);   // before pivot level jc
+        } else {
+            ck2[ch * T + tid] = make_double2(cp, dp);
+            ckq[ch * T + tid] = dq;
+        }
 #pragma unroll
         for (int q = 0; q < KC; ++q) {
             const int jj = jc + q;
-            if (jj < H) {
-                elim(jj, (double)dt[q], (double)db[q], cp, dp, dq);
-                if (jj == jb) { cp_jb = cp; dq_jb = dq; }
+            if (IN(jj < H)) {
+                const bool first = q == 0 && ch == 0;
+                double r = 0.0;
+                elim(first, IN(jj < Bc), (double)dt[q], (double)db[q], cp, dp, dq, r);
+                if (RTAB && !first) rt[jj * rts] = r;
+                if (FULL ? (q == KC - 1 && ch == nch - 1) : (jj == jb)) { cp_jb = cp; dq_jb = dq; }
             }
         }
     }
@@ -602,10 +638,22 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
         double cpl[KC], dpl[KC], dql[KC];
         {
             const double2 c0 = ck2[ch * T + tid];
-            double cpv = c0.x, dpv = c0.y, dqv = ckq[ch * T + tid];
+            double cpv = RTAB ? 0.0 : c0.x, dpv = RTAB ? c0.x : c0.y, dqv = RTAB ? c0.y : ckq[ch * T + tid];
 #pragma unroll
             for (int q = 0; q < KC; ++q) {
-                if (jc + q < H) elim(jc + q, (double)dt[q], (double)db[q], cpv, dpv, dqv);
+                const int jj = jc + q;
+                if (IN(jj < H)) {
+                    const bool first = q == 0 && ch == 0;
+                    if (RTAB && !first) {
+                        const double r = rt[jj * rts];
+                        cpv = fxa * r;
+                        dpv = ((double)dt[q] - dpv * fxa) * r;
+                        if (IN(jj < Bc)) dqv = ((double)db[q] - dqv * fxa) * r;
+                    } else {
+                        double r;
+                        elim(first, IN(jj < Bc), (double)dt[q], (double)db[q], cpv, dpv, dqv, r);
+                    }
+                }
                 cpl[q] = cpv;
                 dpl[q] = dpv;
                 dql[q] = dqv;
@@ -614,16 +662,19 @@ __global__ void __launch_bounds__(kThomasThreads, 4) k_thomas2(const ColumnArgs 
 #pragma unroll
         for (int q = KC - 1; q >= 0; --q) {
             const int jj = jc + q;
-            if (jj < H) {
-                if (jj < m) xt = dpl[q] - cpl[q] * xt;
-                st_l2(&col[(long)jj * ls], (R)xt, pk);
-                if (jj <= jb) {
-                    if (jj < jb) xb = dql[q] - cpl[q] * xb;
-                    st_l2(&col[(long)(nz - 1 - jj) * ls], (R)xb, pk);
+            if (IN(jj < H)) {
+                const unsigned o = (unsigned)jj * ls;
+                const bool mid = FULL ? (q == KC - 1 && ch == nch - 1) : (jj >= m);   // the meeting level
+                if (!mid) xt = dpl[q] - cpl[q] * xt;
+                st_l2(col + o, (R)xt, pk);
+                if (IN(jj <= jb)) {
+                    if (FULL ? !mid : (jj < jb)) xb = dql[q] - cpl[q] * xb;
+                    st_l2(bot0 - o, (R)xb, pk);
                 }
             }
         }
     }
+#undef IN
 }
 
 // ---------------------------------------------------------------------------
@@ -1888,7 +1939,10 @@ static cudaError_t setup_t() {
     PS3D_ROWS_SETUP(true)
 #undef PS3D_ROWS_SETUP
     if ((e = cudaFuncSetAttribute(k_zsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))) return e;
-    if ((e = max_dynamic_smem(k_thomas2<R>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R, false, false>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R, true, false>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R, false, true>))) return e;
+    if ((e = max_dynamic_smem(k_thomas2<R, true, true>))) return e;
     if ((e = max_dynamic_smem(k_colsolve))) return e;
     if ((e = max_dynamic_smem(k_colsolve2))) return e;
     if ((e = max_dynamic_smem(k_thomas<R, true>))) return e;
@@ -1975,15 +2029,30 @@ cudaError_t launch_thomas(const ColumnArgs& a0, bool fp32, cudaStream_t s) {
     a.fd_nxh = make_fastdiv(a.nxh);
     // the two-ended form with two threads per column where 4 blocks of 128
     // fit an SM, else the one-ended form with as many threads per block as
-    // its checkpoints allow; PS3D_THOMAS_FORM=0|2 pins one
+    // its checkpoints allow; PS3D_THOMAS_FORM=0|2|3 pins one (3: the
+    // two-ended form with its pivot table); PS3D_THOMAS_FULL=0 keeps the
+    // bounds-tested instantiation of the two-ended form on every grid
     const char* pin = std::getenv("PS3D_THOMAS_FORM");
-    if ((!pin && thomas2_smem(a.nz, kThomasThreads) <= 56 * 1024) ||
-        (pin && pin[0] == '2' && thomas2_smem(a.nz, kThomasThreads) <= 227 * 1024 - 64)) {
-        const long nthreads = 2 * ncols * std::max(1, a.batch);
-        const dim3 g((unsigned)((nthreads + kThomasThreads - 1) / kThomasThreads)), b(kThomasThreads);
-        const size_t sm2 = thomas2_smem(a.nz, kThomasThreads);
-        if (fp32) return launch_pdl(k_thomas2<float>, g, b, sm2, s, a);
-        return launch_pdl(k_thomas2<double>, g, b, sm2, s, a);
+    const char* fe = std::getenv("PS3D_THOMAS_FULL");
+    const int form = pin ? pin[0] - '0' : (thomas2_smem(a.nz, kThomasThreads) <= 56 * 1024 ? 2 : 0);
+    const bool off32 = (long)a.nz * 2 * ncols < (1L << 32);   // 32-bit level offsets
+    const bool full = a.nz % (2 * kThomasChunk) == 0 && !(fe && fe[0] == '0');
+    const long n2 = 2 * ncols * std::max(1, a.batch);
+    if (form == 3 && off32 && thomas2r_smem(a.nz, kThomas2RThreads) <= 227 * 1024 - 64) {
+        const dim3 g((unsigned)((n2 + kThomas2RThreads - 1) / kThomas2RThreads)), b(kThomas2RThreads);
+        const size_t sm = thomas2r_smem(a.nz, kThomas2RThreads);
+        if (full) return fp32 ? launch_pdl(k_thomas2<float, true, true>, g, b, sm, s, a)
+                              : launch_pdl(k_thomas2<double, true, true>, g, b, sm, s, a);
+        return fp32 ? launch_pdl(k_thomas2<float, false, true>, g, b, sm, s, a)
+                    : launch_pdl(k_thomas2<double, false, true>, g, b, sm, s, a);
+    }
+    if (form == 2 && off32 && thomas2_smem(a.nz, kThomasThreads) <= 227 * 1024 - 64) {
+        const dim3 g((unsigned)((n2 + kThomasThreads - 1) / kThomasThreads)), b(kThomasThreads);
+        const size_t sm = thomas2_smem(a.nz, kThomasThreads);
+        if (full) return fp32 ? launch_pdl(k_thomas2<float, true, false>, g, b, sm, s, a)
+                              : launch_pdl(k_thomas2<double, true, false>, g, b, sm, s, a);
+        return fp32 ? launch_pdl(k_thomas2<float, false, false>, g, b, sm, s, a)
+                    : launch_pdl(k_thomas2<double, false, false>, g, b, sm, s, a);
     }
     const int nt = thomas_threads(a.nz);
     if (nt == 0 || ncols < 1) return cudaErrorInvalidValue;

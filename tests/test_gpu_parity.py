@@ -52,20 +52,46 @@ def test_pressure_solver(rigid, shape, plane_impl):
     assert max(err.values()) < TOL_KERNEL, err
 
 
-@pytest.mark.parametrize("thomas_form", ["0", "2"])
-@pytest.mark.parametrize("nz", [40, 64, 100, 129])
+@pytest.mark.parametrize("thomas_form", ["0", "2", "2g", "3", "3g"])
+@pytest.mark.parametrize("nz", [40, 64, 100, 128, 129])
 def test_pressure_solver_tall_columns(nz, thomas_form, monkeypatch):
-    """Rigid-lid solve on columns split into several segments: nz = 64 fills
-    every segment, 40 and 100 leave the last one short, 129 leaves trailing
-    segments empty; both forms of the vertical solve (one-ended and
-    two-ended, a thread per column part)."""
-    monkeypatch.setenv("PS3D_THOMAS_FORM", thomas_form)
+    """Rigid-lid solve on columns split into several segments: nz = 64 and
+    128 fill every segment (the full-chunk instantiation), 40 and 100 leave
+    the last one short, 129 leaves trailing segments empty; every form of
+    the vertical solve: one-ended (0), two-ended (2), two-ended with its
+    pivot table (3), the two-ended ones also in their bounds-tested
+    instantiation on every grid (g)."""
+    monkeypatch.setenv("PS3D_THOMAS_FORM", thomas_form[0])
+    monkeypatch.setenv("PS3D_THOMAS_FULL", "0" if thomas_form.endswith("g") else "1")
     p = small_params(32, 16, nz, rigid=True, Lz=1000.0 * nz / 16)
     o, m = _pair(p, random_state(p, seed=3))
     o.pressure_solver()
     m.pressure_solver()
     err = compare_state(m, o)
     assert max(err.values()) < TOL_KERNEL, err
+
+
+@pytest.mark.parametrize("precision", [abi.PS3D_FP64, abi.PS3D_MIXED])
+def test_vertical_solve_forms_bit_identical(precision, monkeypatch):
+    """The two-ended vertical solve's instantiations (bounds-tested or full
+    chunks; pivots formed in both sweeps or parked in a table by the
+    forward sweep) run the same FP64 operations in the same order, so they
+    give the same bits, on FP64 and on FP32 spectra."""
+    p = small_params(64, 32, 128, rigid=True, Lz=8000.0)
+    p.precision = precision
+    f = random_state(p, seed=5)
+    out = {}
+    for form, full in (("2", "0"), ("2", "1"), ("3", "0"), ("3", "1")):
+        monkeypatch.setenv("PS3D_THOMAS_FORM", form)
+        monkeypatch.setenv("PS3D_THOMAS_FULL", full)
+        m = Model(p)
+        m.upload(**f)
+        m.pressure_solver()
+        out[form + full] = m.download(tendencies=False)
+        m.close()
+    for k, v in out.items():
+        for n in ("u", "v", "w", "p"):
+            assert np.array_equal(v[n], out["20"][n]), (k, n)
 
 
 def test_pressure_solver_divergence_free():
