@@ -1,7 +1,8 @@
 """ctypes binding of the CPU oracle — TEST INFRASTRUCTURE.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
-this module, and only as the checker.  The library under test never does.
+this module, and only to check the CUDA engine's results against it.  The
+library under test never does.
 Field arrays are halo-padded (nz+4, ny+4, nx+4) float64 views (C order z,y,x,
 which is the reference's Fortran column-major (x,y,z) layout).
 """

@@ -2,8 +2,8 @@
  * ps3d_oracle.cpp — TEST INFRASTRUCTURE, not the product.
  *
  * A CPU, FP64, loop-for-loop restatement of the ceden/ps3D hot path, used only
- * as the checker by tests/, __graft_entry__.smoke() and the cpu_baseline leg
- * of bench.py.  Nothing in the shipped library links or calls this file.
+ * to check the CUDA engine's results, by tests/, __graft_entry__.smoke() and
+ * the cpu_baseline leg of bench.py.  Nothing in the shipped library links or calls this file.
  *
  * Parity status: the reference itself cannot be built here (Fortran, MPI,
  * P3DFFT, FFTW and netCDF are absent) and ships no tests or golden vectors,

@@ -1,6 +1,6 @@
 """Committed golden fixtures (tests/golden/make_golden.py).
 
-CPU: the oracle reproduces them (regression pin of the checker).
+CPU: the oracle reproduces them (a regression pin of the oracle itself).
 GPU: the engine reproduces them through the C ABI without the oracle.
 """
 import os
